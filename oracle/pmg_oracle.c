@@ -1,0 +1,750 @@
+/* CPU restatement of the reference PMG path (oracle, test infrastructure).
+ * See pmg_oracle.h for conventions. Each routine cites the reference routine
+ * it restates; the per-point arithmetic of the smoothers, matvecs, residuals
+ * and transfers keeps the reference's operation order so that single-kernel
+ * FP64 results can be compared bit for bit. The prolongation and Galerkin
+ * builders are a generic formulation of the same operators (see the comments
+ * there) and agree with the reference to rounding.
+ */
+#include "pmg_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define IX(nx, ny, i, j, k)                                                    \
+  (((size_t)((k)-1) * (size_t)(ny) + (size_t)((j)-1)) * (size_t)(nx) +          \
+   (size_t)((i)-1))
+
+/* Index of the stored upper diagonal for a neighbour offset (ex,ey,ez), or 0
+ * when the offset is not an upper one. 1..13 = oE oN uC oNE oNW uE uW uN uS
+ * uNE uNW uSE uSW. */
+static int upper_slot(int ex, int ey, int ez) {
+  if (ez == 1) {
+    static const int t[3][3] = {/* ey=-1 */ {13, 9, 12},
+                                /* ey= 0 */ {7, 3, 6},
+                                /* ey=+1 */ {11, 8, 10}};
+    return t[ey + 1][ex + 1];
+  }
+  if (ez == 0 && ey == 1)
+    return ex == 1 ? 4 : (ex == 0 ? 2 : 5);
+  if (ez == 0 && ey == 0 && ex == 1)
+    return 1;
+  return 0;
+}
+
+/* Positive coupling between fine point (i,j,k) and (i+ex, j+ey, k+ez) of a
+ * symmetric 14-diagonal operator: the lower half is read from the upper
+ * diagonal stored at the neighbour (pmgc/matvecd.h:208-236). */
+static double coupling(const pmgo_op *A, int nx, int ny, int i, int j, int k,
+                       int ex, int ey, int ez) {
+  int s = upper_slot(ex, ey, ez);
+  if (s) {
+    const double *a = A->a[s];
+    return a ? a[IX(nx, ny, i, j, k)] : 0.0;
+  }
+  s = upper_slot(-ex, -ey, -ez);
+  const double *a = A->a[s];
+  return a ? a[IX(nx, ny, i + ex, j + ey, k + ez)] : 0.0;
+}
+
+/* ------------------------------------------------------------------------
+ * Gauss-Seidel smoothers
+ * ---------------------------------------------------------------------- */
+
+/* Red-black GS on the 7-point operator: Vgsrb7x, pmgc/gsd.cc:61-111.
+ * Colour c of each sweep updates (i+j+k)%2 == (1-iad)*c + iad*(1-c) on the
+ * 1-based interior; zero_init drops the neighbour sum in the very first
+ * colour only (the flag is cleared after each colour, gsd.cc:108). */
+void pmgo_gsrb7x(int nx, int ny, int nz, const double *oC, const double *cc,
+                 const double *fc, const double *oE, const double *oN,
+                 const double *uC, double *x, int itmax, int iadjoint,
+                 int zero_init) {
+  const size_t sy = (size_t)nx, sz = (size_t)nx * ny;
+  for (int it = 1; it <= itmax; ++it) {
+    for (int c = 0; c <= 1; ++c) {
+      const int want = (1 - iadjoint) * c + iadjoint * (1 - c);
+      const double keep = zero_init ? 0.0 : 1.0;
+      for (int k = 2; k <= nz - 1; ++k)
+        for (int j = 2; j <= ny - 1; ++j)
+          for (int i = 2; i <= nx - 1; ++i) {
+            if ((i + j + k) % 2 != want)
+              continue;
+            const size_t p = IX(nx, ny, i, j, k);
+            const double s = oN[p] * x[p + sy] + oN[p - sy] * x[p - sy] +
+                             oE[p] * x[p + 1] + oE[p - 1] * x[p - 1] +
+                             uC[p - sz] * x[p - sz] + uC[p] * x[p + sz];
+            x[p] = (fc[p] + keep * s) / (oC[p] + cc[p]);
+          }
+      zero_init = 0;
+    }
+  }
+}
+
+/* The 27-point neighbour sums in the reference's order: tmpO (8 in-plane),
+ * tmpU (9 above), tmpD (9 below); pmgc/gsd.cc:171-204,
+ * pmgc/matvecd.cc:142-170. */
+static void sums27(const double *const *a, const double *x, size_t p,
+                   size_t sy, size_t sz, double *tO, double *tU, double *tD) {
+  const double *oE = a[1], *oN = a[2], *uC = a[3], *oNE = a[4], *oNW = a[5];
+  const double *uE = a[6], *uW = a[7], *uN = a[8], *uS = a[9], *uNE = a[10];
+  const double *uNW = a[11], *uSE = a[12], *uSW = a[13];
+  *tO = +oN[p] * x[p + sy] + oN[p - sy] * x[p - sy] + oE[p] * x[p + 1] +
+        oE[p - 1] * x[p - 1] + oNE[p] * x[p + 1 + sy] +
+        oNW[p] * x[p - 1 + sy] + oNW[p + 1 - sy] * x[p + 1 - sy] +
+        oNE[p - 1 - sy] * x[p - 1 - sy];
+  *tU = +uC[p] * x[p + sz] + uN[p] * x[p + sy + sz] + uS[p] * x[p - sy + sz] +
+        uE[p] * x[p + 1 + sz] + uW[p] * x[p - 1 + sz] +
+        uNE[p] * x[p + 1 + sy + sz] + uNW[p] * x[p - 1 + sy + sz] +
+        uSE[p] * x[p + 1 - sy + sz] + uSW[p] * x[p - 1 - sy + sz];
+  *tD = +uC[p - sz] * x[p - sz] + uS[p + sy - sz] * x[p + sy - sz] +
+        uN[p - sy - sz] * x[p - sy - sz] + uW[p + 1 - sz] * x[p + 1 - sz] +
+        uE[p - 1 - sz] * x[p - 1 - sz] +
+        uSW[p + 1 + sy - sz] * x[p + 1 + sy - sz] +
+        uSE[p - 1 + sy - sz] * x[p - 1 + sy - sz] +
+        uNW[p + 1 - sy - sz] * x[p + 1 - sy - sz] +
+        uNE[p - 1 - sy - sz] * x[p - 1 - sy - sz];
+}
+
+/* Eight-colour GS on the 27-point operator: Vgsrb27x, pmgc/gsd.cc:114-212.
+ * Colour (i%2) + 2(j%2) + 4(k%2) on 1-based indices, visited in the order
+ * c*(1-iad) + iad*(7-c); zero_init clears the whole array first
+ * (gsd.cc:154-156). */
+void pmgo_gsrb27x(int nx, int ny, int nz, const double *const *a,
+                  const double *cc, const double *fc, double *x, int itmax,
+                  int iadjoint, int zero_init) {
+  const size_t sy = (size_t)nx, sz = (size_t)nx * ny;
+  if (zero_init)
+    memset(x, 0, sizeof(double) * (size_t)nx * ny * nz);
+  for (int it = 1; it <= itmax; ++it)
+    for (int c = 0; c < 8; ++c) {
+      const int want = c * (1 - iadjoint) + iadjoint * (7 - c);
+      for (int k = 2; k <= nz - 1; ++k)
+        for (int j = 2; j <= ny - 1; ++j)
+          for (int i = 2; i <= nx - 1; ++i) {
+            if ((i % 2) + 2 * (j % 2) + 4 * (k % 2) != want)
+              continue;
+            const size_t p = IX(nx, ny, i, j, k);
+            double tO, tU, tD;
+            sums27(a, x, p, sy, sz, &tO, &tU, &tD);
+            x[p] = (fc[p] + (tO + tU + tD)) / (a[0][p] + cc[p]);
+          }
+    }
+}
+
+/* ------------------------------------------------------------------------
+ * Matrix-vector products and residuals
+ * ---------------------------------------------------------------------- */
+
+/* y = A x on the interior with the reference's rounding order:
+ * 7-point Vmatvec7_1s / matveckernel7 (pmgc/matvecd.cc:62-90,
+ * pmgc/matvecd.h:118-139); 27-point Vmatvec27_1s / matveckernel27
+ * (pmgc/matvecd.cc:104-176, pmgc/matvecd.h:180-240). */
+static double apply_at(int nx, int ny, const pmgo_op *A, const double *cc,
+                       const double *x, int i, int j, int k) {
+  const size_t sy = (size_t)nx, sz = (size_t)nx * ny;
+  const size_t p = IX(nx, ny, i, j, k);
+  const double *const *a = A->a;
+  const double ccp = cc ? cc[p] : 0.0;
+  if (A->kind == 7) {
+    const double *oC = a[0], *oE = a[1], *oN = a[2], *uC = a[3];
+    return -oN[p] * x[p + sy] - oN[p - sy] * x[p - sy] - oE[p] * x[p + 1] -
+           oE[p - 1] * x[p - 1] - uC[p - sz] * x[p - sz] - uC[p] * x[p + sz] +
+           (oC[p] + ccp) * x[p];
+  }
+  double tO, tU, tD;
+  sums27(a, x, p, sy, sz, &tO, &tU, &tD);
+  /* the reference negates every product; -(a*b) is exact, so summing the
+   * negated products equals negating the positive sum term by term */
+  return (-tO) + (-tU) + (-tD) + (a[0][p] + ccp) * x[p];
+}
+
+void pmgo_matvec(int nx, int ny, int nz, const pmgo_op *A, const double *cc,
+                 const double *x, double *y) {
+  for (int k = 2; k <= nz - 1; ++k)
+    for (int j = 2; j <= ny - 1; ++j)
+      for (int i = 2; i <= nx - 1; ++i)
+        y[IX(nx, ny, i, j, k)] = apply_at(nx, ny, A, cc, x, i, j, k);
+}
+
+/* r = f - A x in the rounding order of Vmresid7_1s / Vmresid27_1s
+ * (pmgc/matvecd.cc:382-411, 426-495): f plus the positive neighbour sums,
+ * minus the centre term. */
+void pmgo_mresid(int nx, int ny, int nz, const pmgo_op *A, const double *cc,
+                 const double *fc, const double *x, double *r) {
+  const size_t sy = (size_t)nx, sz = (size_t)nx * ny;
+  const double *const *a = A->a;
+  for (int k = 2; k <= nz - 1; ++k)
+    for (int j = 2; j <= ny - 1; ++j)
+      for (int i = 2; i <= nx - 1; ++i) {
+        const size_t p = IX(nx, ny, i, j, k);
+        const double ccp = cc ? cc[p] : 0.0;
+        if (A->kind == 7) {
+          const double *oC = a[0], *oE = a[1], *oN = a[2], *uC = a[3];
+          r[p] = fc[p] + oN[p] * x[p + sy] + oN[p - sy] * x[p - sy] +
+                 oE[p] * x[p + 1] + oE[p - 1] * x[p - 1] +
+                 uC[p - sz] * x[p - sz] + uC[p] * x[p + sz] -
+                 (oC[p] + ccp) * x[p];
+        } else {
+          double tO, tU, tD;
+          sums27(a, x, p, sy, sz, &tO, &tU, &tD);
+          r[p] = fc[p] + tO + tU + tD - (a[0][p] + ccp) * x[p];
+        }
+      }
+}
+
+/* Defect of the class: r = f - map(x) with map = matveckernel7/27 and cc = 0
+ * (Subtract_Convolve_map, Convolution.h:123-146; get_map,
+ * PBE_pmgc_class.h:619-698). Interior only. */
+void pmgo_defect(int nx, int ny, int nz, const pmgo_op *A, const double *f,
+                 const double *x, double *r) {
+  for (int k = 2; k <= nz - 1; ++k)
+    for (int j = 2; j <= ny - 1; ++j)
+      for (int i = 2; i <= nx - 1; ++i) {
+        const size_t p = IX(nx, ny, i, j, k);
+        r[p] = f[p] - apply_at(nx, ny, A, NULL, x, i, j, k);
+      }
+}
+
+/* sqrt(sum over the interior of (f - A x)^2 / (nx*ny*nz)): the class's
+ * compute_residual_2 (Convolution.h:156-185; num_values counts the shell). */
+double pmgo_residual2(int nx, int ny, int nz, const pmgo_op *A,
+                      const double *f, const double *x) {
+  double s = 0.0;
+  for (int k = 2; k <= nz - 1; ++k)
+    for (int j = 2; j <= ny - 1; ++j)
+      for (int i = 2; i <= nx - 1; ++i) {
+        const size_t p = IX(nx, ny, i, j, k);
+        const double d = f[p] - apply_at(nx, ny, A, NULL, x, i, j, k);
+        s += d * d;
+      }
+  return sqrt(s / ((double)nx * ny * nz));
+}
+
+/* Hackbusch-Reusken damping (r . x) / (x . A x) over the interior:
+ * get_ideal_lambda, MultigridDomain.h:327-359 (accumulators start at 0). */
+double pmgo_ideal_lambda(int nx, int ny, int nz, const pmgo_op *A,
+                         const double *x, const double *r) {
+  double up = 0.0, lo = 0.0;
+  for (int k = 2; k <= nz - 1; ++k)
+    for (int j = 2; j <= ny - 1; ++j)
+      for (int i = 2; i <= nx - 1; ++i) {
+        const size_t p = IX(nx, ny, i, j, k);
+        up += r[p] * x[p];
+        lo += x[p] * apply_at(nx, ny, A, NULL, x, i, j, k);
+      }
+  return up / lo;
+}
+
+/* ------------------------------------------------------------------------
+ * Grid transfers
+ * ---------------------------------------------------------------------- */
+
+/* Offsets of the nine in-plane prolongation stencils in list order
+ * C N S E W NE NW SE SW, and the plane order o (dz=0), u (+1), d (-1). */
+static const int kPlaneDx[9] = {0, 0, 0, 1, -1, 1, -1, 1, -1};
+static const int kPlaneDy[9] = {0, 1, -1, 0, 0, 1, 1, -1, -1};
+static const int kPlaneDz[3] = {0, 1, -1};
+
+/* Slot in the 27-array list of the prolongation weight for fine offset
+ * (dx,dy,dz) from the coarse point's fine image. */
+static int pslot(int dx, int dy, int dz) {
+  int s = 0;
+  for (; s < 9; ++s)
+    if (kPlaneDx[s] == dx && kPlaneDy[s] == dy)
+      break;
+  const int plane = dz == 0 ? 0 : (dz == 1 ? 1 : 2);
+  return plane * 9 + s;
+}
+
+/* Restriction r_c = P^T r_f: Vrestrc2, pmgc/matvecd.cc:696-799. Coarse
+ * interior (i,j,k) reads fine (ii,jj,kk) = 2(i,j,k)-1 and its 26 neighbours;
+ * sums tmpO, tmpU, tmpD in list order. */
+void pmgo_restrc2(int nxf, int nyf, int nzf, int nxc, int nyc, int nzc,
+                  const double *xin, double *xout, const double *const *P) {
+  (void)nzf;
+  for (int k = 2; k <= nzc - 1; ++k)
+    for (int j = 2; j <= nyc - 1; ++j)
+      for (int i = 2; i <= nxc - 1; ++i) {
+        const size_t pc = IX(nxc, nyc, i, j, k);
+        const int ii = 2 * i - 1, jj = 2 * j - 1, kk = 2 * k - 1;
+        double t[3];
+        for (int pl = 0; pl < 3; ++pl) {
+          double s = 0.0;
+          for (int q = 0; q < 9; ++q) {
+            const double w = P[pl * 9 + q][pc];
+            const double v = xin[IX(nxf, nyf, ii + kPlaneDx[q],
+                                    jj + kPlaneDy[q], kk + kPlaneDz[pl])];
+            s = q == 0 ? w * v : s + w * v;
+          }
+          t[pl] = s;
+        }
+        xout[pc] = t[0] + t[1] + t[2];
+      }
+}
+
+/* Prolongation e_f = P e_c: VinterpPMG2, pmgc/matvecd.cc:820-964. Each
+ * coarse (ii,jj,kk) in [1, n_c-1]^3 writes the eight fine points
+ * (2ii-1+{0,1}, 2jj-1+{0,1}, 2kk-1+{0,1}); fine index n_f is never written. */
+void pmgo_interp2(int nxc, int nyc, int nzc, int nxf, int nyf, int nzf,
+                  const double *xin, double *xout, const double *const *P) {
+  (void)nzf;
+#define PC(name, a, b, c) P[name][IX(nxc, nyc, a, b, c)]
+#define XC(a, b, c) xin[IX(nxc, nyc, a, b, c)]
+#define XF(a, b, c) xout[IX(nxf, nyf, a, b, c)]
+  enum { oPC, oPN, oPS, oPE, oPW, oPNE, oPNW, oPSE, oPSW,
+         uPC, uPN, uPS, uPE, uPW, uPNE, uPNW, uPSE, uPSW,
+         dPC, dPN, dPS, dPE, dPW, dPNE, dPNW, dPSE, dPSW };
+  for (int kk = 1; kk <= nzc - 1; ++kk)
+    for (int jj = 1; jj <= nyc - 1; ++jj)
+      for (int ii = 1; ii <= nxc - 1; ++ii) {
+        const int i = 2 * ii - 1, j = 2 * jj - 1, k = 2 * kk - 1;
+        /* a fine point on a coarse point */
+        XF(i, j, k) = XC(ii, jj, kk);
+        /* fine points between two coarse points along x, y, z */
+        XF(i + 1, j, k) = PC(oPE, ii, jj, kk) * XC(ii, jj, kk) +
+                          PC(oPW, ii + 1, jj, kk) * XC(ii + 1, jj, kk);
+        XF(i, j + 1, k) = PC(oPN, ii, jj, kk) * XC(ii, jj, kk) +
+                          PC(oPS, ii, jj + 1, kk) * XC(ii, jj + 1, kk);
+        XF(i, j, k + 1) = PC(uPC, ii, jj, kk) * XC(ii, jj, kk) +
+                          PC(dPC, ii, jj, kk + 1) * XC(ii, jj, kk + 1);
+        /* fine points in the middle of four coarse points (xy, xz, yz) */
+        XF(i + 1, j + 1, k) = PC(oPNE, ii, jj, kk) * XC(ii, jj, kk) +
+                              PC(oPNW, ii + 1, jj, kk) * XC(ii + 1, jj, kk) +
+                              PC(oPSE, ii, jj + 1, kk) * XC(ii, jj + 1, kk) +
+                              PC(oPSW, ii + 1, jj + 1, kk) *
+                                  XC(ii + 1, jj + 1, kk);
+        XF(i + 1, j, k + 1) = PC(uPE, ii, jj, kk) * XC(ii, jj, kk) +
+                              PC(uPW, ii + 1, jj, kk) * XC(ii + 1, jj, kk) +
+                              PC(dPE, ii, jj, kk + 1) * XC(ii, jj, kk + 1) +
+                              PC(dPW, ii + 1, jj, kk + 1) *
+                                  XC(ii + 1, jj, kk + 1);
+        XF(i, j + 1, k + 1) = PC(uPN, ii, jj, kk) * XC(ii, jj, kk) +
+                              PC(uPS, ii, jj + 1, kk) * XC(ii, jj + 1, kk) +
+                              PC(dPN, ii, jj, kk + 1) * XC(ii, jj, kk + 1) +
+                              PC(dPS, ii, jj + 1, kk + 1) *
+                                  XC(ii, jj + 1, kk + 1);
+        /* the fine point in the middle of eight coarse points */
+        XF(i + 1, j + 1, k + 1) =
+            +PC(uPNE, ii, jj, kk) * XC(ii, jj, kk) +
+            PC(uPNW, ii + 1, jj, kk) * XC(ii + 1, jj, kk) +
+            PC(uPSE, ii, jj + 1, kk) * XC(ii, jj + 1, kk) +
+            PC(uPSW, ii + 1, jj + 1, kk) * XC(ii + 1, jj + 1, kk) +
+            PC(dPNE, ii, jj, kk + 1) * XC(ii, jj, kk + 1) +
+            PC(dPNW, ii + 1, jj, kk + 1) * XC(ii + 1, jj, kk + 1) +
+            PC(dPSE, ii, jj + 1, kk + 1) * XC(ii, jj + 1, kk + 1) +
+            PC(dPSW, ii + 1, jj + 1, kk + 1) * XC(ii + 1, jj + 1, kk + 1);
+      }
+#undef PC
+#undef XC
+#undef XF
+}
+
+/* ------------------------------------------------------------------------
+ * Operator-based prolongation (VbuildPb_op7 pmgc/buildPd.cc:173-555,
+ * VbuildPb_op27 :579-1091), restated as one rule for every fine neighbour
+ * f = c + d of a coarse point's fine image c, d in {-1,0,1}^3 \ {0}:
+ *
+ *   S    = axes with d_a != 0 (the directions being interpolated across),
+ *   P_d  = [ sum_{e in N(d)} a(f, f+e) * w(proj(d+e)) ]
+ *          / [ oC(f) - sum_{e in L(d)} a(f, f+e) ],
+ *   N(d) = { e : e_a in {0, -d_a} for a in S, not all zero on S,
+ *                e_b in {-1,0,1} for b not in S }     (couplings toward c),
+ *   L(d) = { e != 0 : e_a = 0 for a in S }            (lumped onto the
+ *                                                       diagonal),
+ *   proj(v) keeps v on S and zeroes it elsewhere, w(0) = 1 and w(v) = P_v.
+ *
+ * Faces (|S|=1) come first, then edges (|S|=2), then corners (|S|=3), so
+ * every w on the right is already known. a(.,.) is the positive coupling of
+ * the fine operator (7- or 27-point); the 7-point reference formulas are the
+ * same rule with only axis couplings present.
+ * ---------------------------------------------------------------------- */
+void pmgo_buildP_op(int nxf, int nyf, int nzf, int nxc, int nyc, int nzc,
+                    const pmgo_op *A, double *const *P) {
+  (void)nzf;
+  for (int kk = 2; kk <= nzc - 1; ++kk)
+    for (int jj = 2; jj <= nyc - 1; ++jj)
+      for (int ii = 2; ii <= nxc - 1; ++ii) {
+        const size_t pc = IX(nxc, nyc, ii, jj, kk);
+        const int ci = 2 * ii - 1, cj = 2 * jj - 1, ck = 2 * kk - 1;
+        double w[27];
+        for (int s = 0; s < 27; ++s)
+          w[s] = 0.0;
+        w[pslot(0, 0, 0)] = 1.0;
+        for (int order = 1; order <= 3; ++order)
+          for (int dz = -1; dz <= 1; ++dz)
+            for (int dy = -1; dy <= 1; ++dy)
+              for (int dx = -1; dx <= 1; ++dx) {
+                const int d[3] = {dx, dy, dz};
+                if ((dx != 0) + (dy != 0) + (dz != 0) != order)
+                  continue;
+                const int fi = ci + dx, fj = cj + dy, fk = ck + dz;
+                double num = 0.0, lump = 0.0;
+                for (int ez = -1; ez <= 1; ++ez)
+                  for (int ey = -1; ey <= 1; ++ey)
+                    for (int ex = -1; ex <= 1; ++ex) {
+                      const int e[3] = {ex, ey, ez};
+                      if (!ex && !ey && !ez)
+                        continue;
+                      int toward = 1, on_s = 0;
+                      for (int a = 0; a < 3; ++a) {
+                        if (d[a] == 0)
+                          continue;
+                        if (e[a] != 0 && e[a] != -d[a])
+                          toward = 0;
+                        if (e[a] != 0)
+                          on_s = 1;
+                      }
+                      double cpl = coupling(A, nxf, nyf, fi, fj, fk, ex, ey,
+                                            ez);
+                      /* Reference quirk kept for parity: for uPE of the
+                       * 27-point builder the coupling to (i, j, k) — the
+                       * coarse point's own fine image, offset (-1,0,-1) from
+                       * f — is read as uS(i+1, j+1, k), the coupling of f
+                       * to (i+1, j+1, k) (pmgc/buildPd.cc uPE numerator,
+                       * first line). uPNE and uPSE inherit it through uPE. */
+                      if (A->kind == 27 && dx == 1 && dy == 0 && dz == 1 &&
+                          ex == -1 && ey == 0 && ez == -1)
+                        cpl = coupling(A, nxf, nyf, fi, fj, fk, 0, 1, -1);
+                      if (!on_s) {
+                        lump += cpl;
+                      } else if (toward) {
+                        int v[3];
+                        for (int a = 0; a < 3; ++a)
+                          v[a] = d[a] ? d[a] + e[a] : 0;
+                        num += cpl * w[pslot(v[0], v[1], v[2])];
+                      }
+                    }
+                const double diag = A->a[0][IX(nxf, nyf, fi, fj, fk)];
+                w[pslot(dx, dy, dz)] = num / (diag - lump);
+              }
+        for (int s = 0; s < 27; ++s)
+          P[s][pc] = w[s];
+      }
+}
+
+/* Constant weights 1, 1/2, 1/4, 1/8 by the number of nonzero offset
+ * components: VbuildPb_trilin, pmgc/buildPd.cc:63-153. */
+void pmgo_buildP_trilin(int nxc, int nyc, int nzc, double *const *P) {
+  for (int kk = 2; kk <= nzc - 1; ++kk)
+    for (int jj = 2; jj <= nyc - 1; ++jj)
+      for (int ii = 2; ii <= nxc - 1; ++ii) {
+        const size_t pc = IX(nxc, nyc, ii, jj, kk);
+        for (int pl = 0; pl < 3; ++pl)
+          for (int q = 0; q < 9; ++q) {
+            const int nnz =
+                (kPlaneDx[q] != 0) + (kPlaneDy[q] != 0) + (kPlaneDz[pl] != 0);
+            P[pl * 9 + q][pc] = 1.0 / (double)(1 << nnz);
+          }
+      }
+}
+
+/* ------------------------------------------------------------------------
+ * Galerkin coarse operator A_c = P^T A_f P (VbuildG_7, pmgc/buildGd.cc:
+ * 438-1361; VbuildG_27, :1364-3274), computed from its definition: for a
+ * coarse point C and an upper direction D (or D = 0),
+ *
+ *   A_c(C, C+D) = sum_{d, e} P_d(C) * A_f(c+d, c+d+e) * P_{d+e-2D}(C+D)
+ *
+ * over d in {-1,0,1}^3 (fine support of C) and fine couplings e with
+ * d+e-2D in {-1,0,1}^3 (the fine point lies in the support of C+D).
+ * A_f(f,f) = oC(f), A_f(f,g) = -a(f,g). The stored coarse entries are
+ * XoC = A_c(C,C) and X<dir> = -A_c(C, C+dir), on the coarse interior.
+ * ---------------------------------------------------------------------- */
+static const int kUpper[14][3] = {
+    {0, 0, 0},  {1, 0, 0},  {0, 1, 0},   {0, 0, 1},  {1, 1, 0},
+    {-1, 1, 0}, {1, 0, 1},  {-1, 0, 1},  {0, 1, 1},  {0, -1, 1},
+    {1, 1, 1},  {-1, 1, 1}, {1, -1, 1},  {-1, -1, 1}};
+
+void pmgo_buildG(int nxf, int nyf, int nzf, int nxc, int nyc, int nzc,
+                 const double *const *P, const pmgo_op *A,
+                 double *const *out) {
+  (void)nzf;
+  for (int kk = 2; kk <= nzc - 1; ++kk)
+    for (int jj = 2; jj <= nyc - 1; ++jj)
+      for (int ii = 2; ii <= nxc - 1; ++ii) {
+        const size_t pc = IX(nxc, nyc, ii, jj, kk);
+        const int ci = 2 * ii - 1, cj = 2 * jj - 1, ck = 2 * kk - 1;
+        for (int s = 0; s < 14; ++s) {
+          const int *D = kUpper[s];
+          const size_t pn = IX(nxc, nyc, ii + D[0], jj + D[1], kk + D[2]);
+          double acc = 0.0;
+          for (int dz = -1; dz <= 1; ++dz)
+            for (int dy = -1; dy <= 1; ++dy)
+              for (int dx = -1; dx <= 1; ++dx) {
+                const double pw = P[pslot(dx, dy, dz)][pc];
+                const int fi = ci + dx, fj = cj + dy, fk = ck + dz;
+                for (int ez = -1; ez <= 1; ++ez)
+                  for (int ey = -1; ey <= 1; ++ey)
+                    for (int ex = -1; ex <= 1; ++ex) {
+                      const int tx = dx + ex - 2 * D[0];
+                      const int ty = dy + ey - 2 * D[1];
+                      const int tz = dz + ez - 2 * D[2];
+                      if (tx < -1 || tx > 1 || ty < -1 || ty > 1 || tz < -1 ||
+                          tz > 1)
+                        continue;
+                      double af;
+                      if (!ex && !ey && !ez)
+                        af = A->a[0][IX(nxf, nyf, fi, fj, fk)];
+                      else
+                        af = -coupling(A, nxf, nyf, fi, fj, fk, ex, ey, ez);
+                      if (af == 0.0)
+                        continue;
+                      acc += pw * af * P[pslot(tx, ty, tz)][pn];
+                    }
+              }
+          out[s][pc] = s == 0 ? acc : -acc;
+        }
+      }
+}
+
+/* ------------------------------------------------------------------------
+ * Coarsest-level CG of the class (CG_solver, CG_Solver.h:45-242, run by
+ * solve_by_cg<1>, PBE_pmgc_class.h:856-860): warm start from x, interior
+ * dot products, absolute stop sqrt(r.r) <= thresh, the first test taking
+ * the square root twice (CG_Solver.h:135,140), return when the first p.Ap
+ * is zero. An iteration cap (absent in the reference, which would loop
+ * forever on stagnation) bounds the loop; returns the iterations run.
+ * ---------------------------------------------------------------------- */
+int pmgo_cg(int nx, int ny, int nz, const pmgo_op *A, const double *rhs,
+            double *x, double thresh) {
+  const size_t n = (size_t)nx * ny * nz;
+  double *r = calloc(n, sizeof(double));
+  double *p = calloc(n, sizeof(double));
+  double *ap = calloc(n, sizeof(double));
+  int it = 0;
+  if (!r || !p || !ap)
+    goto done;
+  pmgo_defect(nx, ny, nz, A, rhs, x, r);
+  memcpy(p, r, n * sizeof(double));
+  double rs = 0.0, pap = 0.0;
+  for (int k = 2; k <= nz - 1; ++k)
+    for (int j = 2; j <= ny - 1; ++j)
+      for (int i = 2; i <= nx - 1; ++i) {
+        const size_t q = IX(nx, ny, i, j, k);
+        rs += r[q] * r[q];
+      }
+  for (int k = 2; k <= nz - 1; ++k)
+    for (int j = 2; j <= ny - 1; ++j)
+      for (int i = 2; i <= nx - 1; ++i)
+        pap += apply_at(nx, ny, A, NULL, p, i, j, k) * p[IX(nx, ny, i, j, k)];
+  if (pap == 0.0)
+    goto done;
+  double alpha = rs / pap;
+  double res = sqrt(sqrt(rs));
+  while (res > thresh && it < 100000) {
+    ++it;
+    pmgo_matvec(nx, ny, nz, A, NULL, p, ap);
+    double rsn = 0.0;
+    for (int k = 2; k <= nz - 1; ++k)
+      for (int j = 2; j <= ny - 1; ++j)
+        for (int i = 2; i <= nx - 1; ++i) {
+          const size_t q = IX(nx, ny, i, j, k);
+          x[q] += alpha * p[q];
+          r[q] -= alpha * ap[q];
+        }
+    for (int k = 2; k <= nz - 1; ++k)
+      for (int j = 2; j <= ny - 1; ++j)
+        for (int i = 2; i <= nx - 1; ++i) {
+          const size_t q = IX(nx, ny, i, j, k);
+          rsn += r[q] * r[q];
+        }
+    const double beta = rs == 0.0 ? 0.0 : rsn / rs;
+    rs = rsn;
+    for (int k = 2; k <= nz - 1; ++k)
+      for (int j = 2; j <= ny - 1; ++j)
+        for (int i = 2; i <= nx - 1; ++i) {
+          const size_t q = IX(nx, ny, i, j, k);
+          p[q] = r[q] + beta * p[q];
+        }
+    pap = 0.0;
+    for (int k = 2; k <= nz - 1; ++k)
+      for (int j = 2; j <= ny - 1; ++j)
+        for (int i = 2; i <= nx - 1; ++i)
+          pap +=
+              apply_at(nx, ny, A, NULL, p, i, j, k) * p[IX(nx, ny, i, j, k)];
+    alpha = pap == 0.0 ? 0.0 : rs / pap;
+    res = sqrt(rs);
+  }
+done:
+  free(r);
+  free(p);
+  free(ap);
+  return it;
+}
+
+/* ------------------------------------------------------------------------
+ * Hierarchy and V-cycle of the class (buildmultilevelops,
+ * PBE_pmgc_class.h:351-617; v_cycle :1070-1114)
+ * ---------------------------------------------------------------------- */
+typedef struct {
+  int n;
+  double *op[14]; /* level operator; finest uses 4 (7-point) */
+  double *P[27];  /* prolongation from this level to the next finer one */
+  double *x, *f, *r, *zero;
+  pmgo_op A;
+} olevel;
+
+typedef struct {
+  int nlev;
+  olevel lv[16]; /* 1-based: lv[1] coarsest .. lv[nlev] finest */
+} ohier;
+
+static void hier_free(ohier *h) {
+  for (int L = 1; L <= h->nlev; ++L) {
+    olevel *v = &h->lv[L];
+    for (int s = 0; s < 14; ++s)
+      free(v->op[s]);
+    for (int s = 0; s < 27; ++s)
+      free(v->P[s]);
+    free(v->x);
+    free(v->f);
+    free(v->r);
+    free(v->zero);
+  }
+}
+
+static int hier_build(ohier *h, int base, int nlev, const double *oC,
+                      const double *oE, const double *oN, const double *uC,
+                      int trilinear) {
+  memset(h, 0, sizeof(*h));
+  h->nlev = nlev;
+  if (nlev < 2 || nlev > 15)
+    return -1;
+  for (int L = 1; L <= nlev; ++L) {
+    olevel *v = &h->lv[L];
+    v->n = base * (1 << L) + 1;
+    const size_t n3 = (size_t)v->n * v->n * v->n;
+    const int nops = L == nlev ? 4 : 14;
+    for (int s = 0; s < nops; ++s)
+      if (!(v->op[s] = calloc(n3, sizeof(double))))
+        return -1;
+    if (L < nlev)
+      for (int s = 0; s < 27; ++s)
+        if (!(v->P[s] = calloc(n3, sizeof(double))))
+          return -1;
+    if (!(v->x = calloc(n3, sizeof(double))) ||
+        !(v->f = calloc(n3, sizeof(double))) ||
+        !(v->r = calloc(n3, sizeof(double))) ||
+        !(v->zero = calloc(n3, sizeof(double))))
+      return -1;
+    v->A.kind = L == nlev ? 7 : 27;
+    for (int s = 0; s < 14; ++s)
+      v->A.a[s] = v->op[s];
+  }
+  olevel *fine = &h->lv[nlev];
+  const size_t n3 = (size_t)fine->n * fine->n * fine->n;
+  memcpy(fine->op[0], oC, n3 * sizeof(double));
+  memcpy(fine->op[1], oE, n3 * sizeof(double));
+  memcpy(fine->op[2], oN, n3 * sizeof(double));
+  memcpy(fine->op[3], uC, n3 * sizeof(double));
+  for (int L = nlev; L >= 2; --L) {
+    olevel *f = &h->lv[L], *c = &h->lv[L - 1];
+    if (trilinear)
+      pmgo_buildP_trilin(c->n, c->n, c->n, c->P);
+    else
+      pmgo_buildP_op(f->n, f->n, f->n, c->n, c->n, c->n, &f->A, c->P);
+    pmgo_buildG(f->n, f->n, f->n, c->n, c->n, c->n,
+                (const double *const *)c->P, &f->A, c->op);
+  }
+  return 0;
+}
+
+static void smooth(ohier *h, int L, int zero_init) {
+  olevel *v = &h->lv[L];
+  if (L == h->nlev)
+    pmgo_gsrb7x(v->n, v->n, v->n, v->op[0], v->zero, v->f, v->op[1],
+                v->op[2], v->op[3], v->x, 1, 0, zero_init);
+  else
+    pmgo_gsrb27x(v->n, v->n, v->n, (const double *const *)v->op, v->zero,
+                 v->f, v->x, 1, 0, zero_init);
+}
+
+static void vcycle(ohier *h, int L, int as_preconditioner) {
+  olevel *v = &h->lv[L];
+  if (L == 1) {
+    pmgo_cg(v->n, v->n, v->n, &v->A, v->f, v->x, 1e-8);
+    return;
+  }
+  olevel *c = &h->lv[L - 1];
+  int zero_init = (L != h->nlev) || as_preconditioner;
+  for (int s = 0; s < 2; ++s) {
+    smooth(h, L, zero_init);
+    zero_init = 0;
+  }
+  pmgo_defect(v->n, v->n, v->n, &v->A, v->f, v->x, v->r);
+  pmgo_restrc2(v->n, v->n, v->n, c->n, c->n, c->n, v->r, c->f,
+               (const double *const *)c->P);
+  vcycle(h, L - 1, 0);
+  const double omega =
+      pmgo_ideal_lambda(c->n, c->n, c->n, &c->A, c->x, c->f);
+  pmgo_interp2(c->n, c->n, c->n, v->n, v->n, v->n, c->x, v->r,
+               (const double *const *)c->P);
+  /* x = x + omega * e over the whole padded array (Domain.h:602-623) */
+  const size_t n3 = (size_t)v->n * v->n * v->n;
+  for (size_t q = 0; q < n3; ++q)
+    v->x[q] = v->x[q] + omega * v->r[q];
+  for (int s = 0; s < 2; ++s)
+    smooth(h, L, 0);
+}
+
+int pmgo_solve(int base, int nlev, const double *oC, const double *oE,
+               const double *oN, const double *uC, const double *f,
+               const double *x0, double tol, int max_cycles, int trilinear,
+               double *x_out, double *hist) {
+  ohier h;
+  if (hier_build(&h, base, nlev, oC, oE, oN, uC, trilinear) != 0) {
+    hier_free(&h);
+    return -1;
+  }
+  olevel *fine = &h.lv[nlev];
+  const int n = fine->n;
+  const size_t n3 = (size_t)n * n * n;
+  memcpy(fine->f, f, n3 * sizeof(double));
+  memcpy(fine->x, x0, n3 * sizeof(double));
+  const double r0 = pmgo_residual2(n, n, n, &fine->A, fine->f, fine->x);
+  if (hist)
+    hist[0] = r0;
+  int c = 0;
+  while (c < max_cycles) {
+    vcycle(&h, nlev, 0);
+    ++c;
+    const double r = pmgo_residual2(n, n, n, &fine->A, fine->f, fine->x);
+    if (hist)
+      hist[c] = r;
+    if (r / r0 < tol)
+      break;
+  }
+  if (x_out)
+    memcpy(x_out, fine->x, n3 * sizeof(double));
+  hier_free(&h);
+  return c;
+}
+
+long pmgo_hierarchy(int base, int nlev, const double *oC, const double *oE,
+                    const double *oN, const double *uC, int trilinear,
+                    double *out, long cap) {
+  long need = 0;
+  for (int L = nlev - 1; L >= 1; --L) {
+    const long n = base * (1L << L) + 1;
+    need += 41 * n * n * n;
+  }
+  if (cap < need)
+    return -1;
+  ohier h;
+  if (hier_build(&h, base, nlev, oC, oE, oN, uC, trilinear) != 0) {
+    hier_free(&h);
+    return -1;
+  }
+  double *o = out;
+  for (int L = nlev - 1; L >= 1; --L) {
+    olevel *v = &h.lv[L];
+    const size_t n3 = (size_t)v->n * v->n * v->n;
+    for (int s = 0; s < 27; ++s, o += n3)
+      memcpy(o, v->P[s], n3 * sizeof(double));
+    for (int s = 0; s < 14; ++s, o += n3)
+      memcpy(o, v->op[s], n3 * sizeof(double));
+  }
+  hier_free(&h);
+  return need;
+}

@@ -1,0 +1,86 @@
+/* CPU restatement of the reference PMG path (oracle, test infrastructure).
+ *
+ * Plain C99, double precision, single thread. This is the checker that
+ * tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use; the
+ * product (multigrid_b200/) never links or calls it.
+ *
+ * Every function restates one reference routine and cites it. Grid arrays use
+ * the reference layout: nx*ny*nz doubles with a one-point shell, x fastest,
+ * 1-based (i,j,k) -> ((k-1)*ny + (j-1))*nx + (i-1)  (pmgc/vmatrix.h:79-80).
+ *
+ * Operators are held as 14 "upper" diagonals (oC oE oN uC oNE oNW uE uW uN uS
+ * uNE uNW uSE uSW, pmgc/buildGd.h:281-494); a 7-point operator sets only
+ * oC oE oN uC and leaves the other ten NULL. Off-diagonal entries are stored
+ * as positive couplings: A(p, p+d) = -coef. Prolongations are 27 arrays on
+ * the coarse grid in the order oPC oPN oPS oPE oPW oPNE oPNW oPSE oPSW,
+ * uP*, dP* (pmgc/matvecd.cc:696-704).
+ */
+#ifndef PMG_ORACLE_H
+#define PMG_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* 14-diagonal operator; kind 7 or 27. */
+typedef struct {
+  int kind;
+  const double *a[14];
+} pmgo_op;
+
+/* ---- single kernels ------------------------------------------------- */
+void pmgo_gsrb7x(int nx, int ny, int nz, const double *oC, const double *cc,
+                 const double *fc, const double *oE, const double *oN,
+                 const double *uC, double *x, int itmax, int iadjoint,
+                 int zero_init);
+void pmgo_gsrb27x(int nx, int ny, int nz, const double *const *a14,
+                  const double *cc, const double *fc, double *x, int itmax,
+                  int iadjoint, int zero_init);
+void pmgo_matvec(int nx, int ny, int nz, const pmgo_op *A, const double *cc,
+                 const double *x, double *y);
+void pmgo_mresid(int nx, int ny, int nz, const pmgo_op *A, const double *cc,
+                 const double *fc, const double *x, double *r);
+void pmgo_restrc2(int nxf, int nyf, int nzf, int nxc, int nyc, int nzc,
+                  const double *xin, double *xout, const double *const *p27);
+void pmgo_interp2(int nxc, int nyc, int nzc, int nxf, int nyf, int nzf,
+                  const double *xin, double *xout, const double *const *p27);
+void pmgo_buildP_op(int nxf, int nyf, int nzf, int nxc, int nyc, int nzc,
+                    const pmgo_op *A, double *const *p27);
+void pmgo_buildP_trilin(int nxc, int nyc, int nzc, double *const *p27);
+void pmgo_buildG(int nxf, int nyf, int nzf, int nxc, int nyc, int nzc,
+                 const double *const *p27, const pmgo_op *A,
+                 double *const *out14);
+
+/* ---- the class's map-based helpers ---------------------------------- */
+void pmgo_defect(int nx, int ny, int nz, const pmgo_op *A, const double *f,
+                 const double *x, double *r);
+double pmgo_residual2(int nx, int ny, int nz, const pmgo_op *A,
+                      const double *f, const double *x);
+double pmgo_ideal_lambda(int nx, int ny, int nz, const pmgo_op *A,
+                         const double *x, const double *r);
+int pmgo_cg(int nx, int ny, int nz, const pmgo_op *A, const double *rhs,
+            double *x, double thresh);
+
+/* ---- whole solve ----------------------------------------------------- */
+/* Fine inputs as in the reference class: oC has kappa^2 folded in, x0 holds
+ * the Dirichlet boundary on its shell. Levels: n_L = base*2^L + 1.
+ * trilinear selects constant prolongation weights. Returns V-cycles run or a
+ * negative value on allocation failure. hist[0..cycles] gets the residual
+ * norms. */
+int pmgo_solve(int base, int nlev, const double *oC, const double *oE,
+               const double *oN, const double *uC, const double *f,
+               const double *x0, double tol, int max_cycles, int trilinear,
+               double *x_out, double *hist);
+
+/* Hierarchy in the layout of pmgref_hierarchy: for L = nlev-1 .. 1, the 27
+ * prolongation arrays then the 14 operator arrays of level L. Returns the
+ * number of doubles written, or -1 if cap is too small. */
+long pmgo_hierarchy(int base, int nlev, const double *oC, const double *oE,
+                    const double *oN, const double *uC, int trilinear,
+                    double *out, long cap);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

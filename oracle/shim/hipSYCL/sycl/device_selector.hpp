@@ -1,0 +1,3 @@
+// Forwarding header of the host oracle shim (test infrastructure).
+#pragma once
+#include <sycl/sycl.hpp>
