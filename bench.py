@@ -1,0 +1,404 @@
+"""Benchmark: linearized PB solves/s with the B200 PMG solver.
+
+A step is one PB solve of the workload from device-resident fine-level
+inputs: load the fine level (device copy), build the Galerkin hierarchy,
+V-cycles until the relative residual is below 1e-10. The default workload is
+the 257^3 grid (5 levels, 0.4 A, synthetic 5000-atom molecule) solved in
+mixed precision (float V-cycles inside double iterative refinement); the
+same run also times the plain FP64 solve.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
+                  [--workload pb257|pb161|pb65] [--precision mixed|fp64]
+
+--impl reference times the reference's own PMG class on the host cores
+(oracle/_ref, built from the reference sources; the CPU restatement when it
+is absent) on bounded samples of the same workload. Under torchrun every rank
+solves its own replica (the solve does not shard); value = all ranks'
+solves / max rank time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "PB solves/s at rel. residual 1e-10"
+UNIT = "solves/s"
+TOL = 1e-10
+MAX_CYCLES = 100
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="pb257")
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,"
+              "clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.dev}",
+                 f"--query-gpu={self.FIELDS}", "--format=csv,noheader",
+                 "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [],
+                    "samples": 0}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append(parts)
+            except Exception:
+                pass
+        os.unlink(self.path)
+        sm = [float(r[1].split()[0]) for r in rows if r[1].split()[0]
+              .replace(".", "").isdigit()]
+        mx = [float(r[2].split()[0]) for r in rows if r[2].split()[0]
+              .replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4)
+                          if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing
+# ---------------------------------------------------------------------------
+def dist_setup(args):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(
+            seconds=600), device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(world, value: float) -> float:
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: reference class (or the restatement) on bounded samples
+# ---------------------------------------------------------------------------
+def cpu_sample(w, fine, fp64_cycles: int):
+    """Times hierarchy build + 2 V-cycles of the reference on host cores and
+    extrapolates to a full solve of fp64_cycles V-cycles."""
+    from oracle.oracle import Reference, Restatement, reference_available
+    cores = os.cpu_count() or 1
+    if reference_available(omp=True):
+        os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+        ref = Reference(omp=True)
+        kind, threads = "reference", cores
+        t0 = time.perf_counter()
+        ref.cycles(w.base, w.nlev, fine, 0)
+        t_build = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        ref.cycles(w.base, w.nlev, fine, 2)
+        t_cyc = (time.perf_counter() - t0 - t_build) / 2
+    else:
+        ref = Restatement()
+        kind, threads = "port", 1
+        t0 = time.perf_counter()
+        ref.solve(w.base, w.nlev, fine, tol=0.0, max_cycles=0)
+        t_build = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        ref.solve(w.base, w.nlev, fine, tol=0.0, max_cycles=2)
+        t_cyc = (time.perf_counter() - t0 - t_build) / 2
+    t_solve = t_build + fp64_cycles * max(t_cyc, 0.0)
+    return {
+        "value": 1.0 / t_solve, "unit": UNIT, "cores": threads, "kind": kind,
+        "sample": (f"{w.name}: hierarchy build ({t_build:.2f} s) + 2 FP64 "
+                   f"V-cycles ({t_cyc:.2f} s each), extrapolated to "
+                   f"{fp64_cycles} cycles"),
+    }
+
+
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from multigrid_b200.molecule import WORKLOADS
+    from multigrid_b200.problem import setup_fine
+    w = WORKLOADS[args.workload]
+    fine = setup_fine(w.n, w.h, w.atoms(), w.physics)
+    cycles = {"pb65": 13, "pb161": 16, "pb257": 16}.get(w.name, 16)
+    for _ in range(max(0, min(args.warmup, 1))):
+        pass
+    samples = [cpu_sample(w, fine, cycles) for _ in range(max(1, min(
+        args.steps, 2)))]
+    v = statistics.median(s["value"] for s in samples)
+    base = dict(samples[-1])
+    base["value"] = v
+    out = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT,
+        "n_gpus": world, "steps": len(samples), "warmup": 0,
+        "ms_per_step": 1000.0 / v, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": workload_config(w, "fp64"),
+        "cpu_baseline": base,
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out))
+    return 0
+
+
+def workload_config(w, precision):
+    return {
+        "workload": (f"{w.name}: {w.n}^3 grid, {w.nlev} levels, h {w.h} A, "
+                     f"{w.natoms}-atom synthetic molecule, linearized PBE, "
+                     f"Galerkin PMG V-cycles to rel. residual 1e-10"),
+        "grid": w.n, "levels": w.nlev, "spacing_A": w.h, "atoms": w.natoms,
+        "precision": precision, "tol": TOL,
+        "l2_flush": "inputs larger than L2 (fine level 4+2 arrays of n^3)",
+    }
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+
+    world, rank, local = dist_setup(args)
+    from multigrid_b200 import PBELinearProblem, pmgc
+    from multigrid_b200.molecule import WORKLOADS
+    from multigrid_b200.problem import setup_fine
+
+    w = WORKLOADS[args.workload]
+    atoms = w.atoms()
+    fine = setup_fine(w.n, w.h, atoms, w.physics)
+    keys = ("oC", "oE", "oN", "uC", "f", "x0")
+    dev = {k: torch.from_numpy(fine[k]).cuda() for k in keys}
+    n3 = w.n ** 3
+
+    def make(precision):
+        p = PBELinearProblem(w.base, w.nlev, w.box, precision, w.physics)
+        return p
+
+    def step(p, inputs):
+        p.set_fine(*[inputs[k] for k in keys])
+        p.buildmultilevelops()
+        return p.solve(TOL, MAX_CYCLES)
+
+    results = {}
+    for precision in (args.precision, "fp64" if args.precision == "mixed"
+                      else "mixed"):
+        p = make(precision)
+        stream = torch.cuda.ExternalStream(p.stream)
+        for _ in range(args.warmup):
+            res = step(p, dev)
+        torch.cuda.synchronize()
+        barrier(world)
+        clocks = ClockSampler(torch.cuda.current_device())
+        if precision == args.precision:
+            clocks.start()
+            time.sleep(0.3)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        cyc = []
+        e0.record(stream)
+        for _ in range(args.steps):
+            res = step(p, dev)
+            cyc.append(res.cycles)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        ck = clocks.stop() if precision == args.precision else None
+        barrier(world)
+        ms = max_over_ranks(world, ms)
+        x = p.potential().ravel()
+        results[precision] = dict(ms=ms, cycles=cyc, relres=res.relres,
+                                  x=x, clocks=ck, p=p, stream=stream)
+
+    prim = results[args.precision]
+    value = world * args.steps / (prim["ms"] / 1000.0)
+
+    # end to end through the public API from pinned host buffers
+    p = prim["p"]
+    stream = prim["stream"]
+    host = {k: torch.from_numpy(fine[k]).pin_memory() for k in keys}
+    out_host = torch.empty(n3, dtype=torch.float64).pin_memory()
+    import ctypes
+    from multigrid_b200 import _lib
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    k_e2e = max(1, min(args.steps, 5))
+    barrier(world)
+    e0.record(stream)
+    for _ in range(k_e2e):
+        step(p, host)
+        _lib.check("pmg_get_potential", _lib.lib.pmg_get_potential(
+            p._h, ctypes.c_void_p(out_host.data_ptr())))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(world, e0.elapsed_time(e1))
+    e2e = {"value": world * k_e2e / (e2e_ms / 1000.0), "unit": UNIT,
+           "h2d_bytes_per_step": 6 * n3 * 8, "d2h_bytes_per_step": n3 * 8}
+
+    # dominant kernel: the finest-level red-black smoother (one sweep of two
+    # colours), timed with CUDA events on its stream
+    peak, peak_kind = peaks()
+    xs = dev["x0"].clone()
+    if args.precision == "mixed":
+        arr = {k: dev[k].float() for k in keys}
+        xs = xs.float()
+        esz = 4
+    else:
+        arr = dev
+        esz = 8
+    s2 = torch.cuda.Stream()
+    reps = 20
+    with torch.cuda.stream(s2):
+        for _ in range(3):
+            pmgc.Vgsrb7x(w.n, w.n, w.n, arr["oC"], None, arr["f"], arr["oE"],
+                         arr["oN"], arr["uC"], xs, 1, stream=s2)
+        a0 = torch.cuda.Event(enable_timing=True)
+        a1 = torch.cuda.Event(enable_timing=True)
+        a0.record(s2)
+        for _ in range(reps):
+            pmgc.Vgsrb7x(w.n, w.n, w.n, arr["oC"], None, arr["f"], arr["oE"],
+                         arr["oN"], arr["uC"], xs, 1, stream=s2)
+        a1.record(s2)
+    torch.cuda.synchronize()
+    sweep_ms = a0.elapsed_time(a1) / reps
+    alg_bytes = 7 * n3 * esz  # 4 coefficients + f + x read, x written
+    achieved = alg_bytes / (sweep_ms / 1000.0) / 1e9
+    roofline = {"bound": "hbm", "kernel": "gs7_color_kernel (one sweep)",
+                "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": None,
+                "peak_source": peak_kind,
+                "algorithmic_bytes_per_launch": alg_bytes}
+
+    # error of the mixed solve against the FP64 solve of the same run
+    xm, xd = results["mixed"]["x"], results["fp64"]["x"]
+    err = {"rel_l2": float(np.linalg.norm(xm - xd) / np.linalg.norm(xd)),
+           "max_norm": float(np.abs(xm - xd).max() / np.abs(xd).max())}
+
+    cpu = None
+    if world == 1 and rank == 0 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_sample(w, fine, results["fp64"]["cycles"][-1])
+        except Exception as e:  # reported, never silently replaced
+            cpu = {"error": str(e)}
+
+    fp64_value = world * args.steps / (results["fp64"]["ms"] / 1000.0)
+    mixed_value = world * args.steps / (results["mixed"]["ms"] / 1000.0)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": prim["ms"] / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+f64" if args.precision == "mixed" else "f64",
+            "data": "synthetic",
+            "config": dict(workload_config(w, args.precision),
+                           parallelism=f"replicas x{world}"),
+            "cycles": prim["cycles"][-1],
+            "relres": prim["relres"],
+            "fp64": {"value": fp64_value, "cycles":
+                     results["fp64"]["cycles"][-1],
+                     "ms_per_step": results["fp64"]["ms"] / args.steps},
+            "mixed": {"value": mixed_value, "cycles":
+                      results["mixed"]["cycles"][-1],
+                      "ms_per_step": results["mixed"]["ms"] / args.steps,
+                      "error_vs_fp64": err},
+            "mixed_speedup_vs_fp64": mixed_value / fp64_value,
+            "fine_unknowns_x_cycles_per_s": value * (w.n - 2) ** 3 *
+            prim["cycles"][-1],
+            "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
+            "clocks": prim["clocks"],
+        }
+        print(json.dumps(line))
+    for r in results.values():
+        r["p"].close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,322 @@
+/* pmg_b200 — C ABI of the B200-native PMG (Galerkin multigrid) solver for
+ * the linearized Poisson-Boltzmann equation.
+ *
+ * Drop-in boundary for the reference's pmgc kernels and its
+ * pmgc_solver::PBE_linear_problem class (jabruniessner/multigrid, ported from
+ * APBS pmgc). Each entry point below names the reference routine it replaces
+ * as file:line in that project.
+ *
+ * Conventions (all entry points):
+ *  - Grid arrays are the reference's: nx*ny*nz values including the
+ *    one-point Dirichlet shell, x fastest, 1-based
+ *    VAT3(m,i,j,k) = m[(k-1)*ny*nx + (j-1)*nx + (i-1)] (pmgc/vmatrix.h:79-80).
+ *  - Kernel entry points take DEVICE pointers and a CUDA stream in place of
+ *    the reference's sycl::queue&; they are asynchronous on that stream, like
+ *    the reference's in-order queue. Entry points that return a scalar to the
+ *    host synchronise the stream, as the reference's reductions do (.wait()).
+ *  - The caller owns every array passed in; the library never frees caller
+ *    memory. Unused APBS arguments of the reference (ipc, rpc) are dropped.
+ *  - Every function returns a pmg_status: 0 on success, negative on error;
+ *    pmg_last_error() describes the last failure on the calling thread.
+ *  - _d entry points compute in double, _f in float.
+ */
+#ifndef PMG_B200_H
+#define PMG_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+struct CUstream_st;
+typedef struct CUstream_st *pmg_stream_t; /* == cudaStream_t */
+
+typedef enum {
+  PMG_OK = 0,
+  PMG_ERR_ARG = -1,      /* invalid size, null pointer, bad option        */
+  PMG_ERR_CUDA = -2,     /* a CUDA call failed (see pmg_last_error)      */
+  PMG_ERR_NOMEM = -3,    /* device allocation failed                      */
+  PMG_ERR_DIVERGED = -4, /* residual became NaN/Inf or stagnated          */
+  PMG_ERR_TIMEOUT = -5,  /* a bounded device wait or iteration cap ran out */
+  PMG_ERR_BUDGET = -6,   /* admission refused: device-memory budget       */
+  PMG_ERR_STATE = -7     /* call out of order (e.g. solve before build)   */
+} pmg_status;
+
+/* Human-readable description of the last error on this thread. */
+const char *pmg_last_error(void);
+/* Library version string. */
+const char *pmg_version(void);
+
+/* ======================================================================
+ * pmgc kernels (device pointers, stream-ordered)
+ * ==================================================================== */
+
+/* Red-black Gauss-Seidel on the 7-point operator, itmax sweeps of two
+ * colours; colour c updates (i+j+k)%2 == (1-iadjoint)*c + iadjoint*(1-c);
+ * zero_init drops the neighbour sum in the first colour.
+ * Replaces pmgc::Vgsrb7x, pmgc/gsd.cc:60-111. cc may be NULL (= 0). */
+int pmg_Vgsrb7x_d(int nx, int ny, int nz, const double *oC, const double *cc,
+                  const double *fc, const double *oE, const double *oN,
+                  const double *uC, double *x, int itmax, int iadjoint,
+                  int zero_init, pmg_stream_t stream);
+int pmg_Vgsrb7x_f(int nx, int ny, int nz, const float *oC, const float *cc,
+                  const float *fc, const float *oE, const float *oN,
+                  const float *uC, float *x, int itmax, int iadjoint,
+                  int zero_init, pmg_stream_t stream);
+
+/* Eight-colour Gauss-Seidel on the 27-point operator; colour
+ * (i%2)+2(j%2)+4(k%2) visited in order c*(1-iadjoint) + iadjoint*(7-c);
+ * zero_init clears x first. Argument order follows the reference
+ * (x, itmax, zero_initialize, iadjoint).
+ * Replaces pmgc::Vgsrb27x, pmgc/gsd.cc:113-212. cc may be NULL. */
+int pmg_Vgsrb27x_d(int nx, int ny, int nz, const double *oC, const double *cc,
+                   const double *fc, const double *oE, const double *oN,
+                   const double *uC, const double *oNE, const double *oNW,
+                   const double *uE, const double *uW, const double *uN,
+                   const double *uS, const double *uNE, const double *uNW,
+                   const double *uSE, const double *uSW, double *x, int itmax,
+                   int zero_init, int iadjoint, pmg_stream_t stream);
+int pmg_Vgsrb27x_f(int nx, int ny, int nz, const float *oC, const float *cc,
+                   const float *fc, const float *oE, const float *oN,
+                   const float *uC, const float *oNE, const float *oNW,
+                   const float *uE, const float *uW, const float *uN,
+                   const float *uS, const float *uNE, const float *uNW,
+                   const float *uSE, const float *uSW, float *x, int itmax,
+                   int zero_init, int iadjoint, pmg_stream_t stream);
+
+/* y = A x on the interior (7-point). Replaces pmgc::Vmatvec7_1s,
+ * pmgc/matvecd.cc:61-90 (and the class map matveckernel7,
+ * pmgc/matvecd.h:117-138). */
+int pmg_Vmatvec7_1s_d(int nx, int ny, int nz, const double *oC,
+                      const double *cc, const double *oE, const double *oN,
+                      const double *uC, const double *x, double *y,
+                      pmg_stream_t stream);
+/* y = A x on the interior (27-point). Replaces pmgc::Vmatvec27_1s,
+ * pmgc/matvecd.cc:103-176 (and matveckernel27, pmgc/matvecd.h:179-240). */
+int pmg_Vmatvec27_1s_d(int nx, int ny, int nz, const double *oC,
+                       const double *cc, const double *oE, const double *oN,
+                       const double *uC, const double *oNE, const double *oNW,
+                       const double *uE, const double *uW, const double *uN,
+                       const double *uS, const double *uNE, const double *uNW,
+                       const double *uSE, const double *uSW, const double *x,
+                       double *y, pmg_stream_t stream);
+
+/* r = f - A x on the interior (7-point). Replaces pmgc::Vmresid7_1s,
+ * pmgc/matvecd.cc:381-411. */
+int pmg_Vmresid7_1s_d(int nx, int ny, int nz, const double *oC,
+                      const double *cc, const double *fc, const double *oE,
+                      const double *oN, const double *uC, const double *x,
+                      double *r, pmg_stream_t stream);
+/* r = f - A x on the interior (27-point). Replaces pmgc::Vmresid27_1s,
+ * pmgc/matvecd.cc:425-495. */
+int pmg_Vmresid27_1s_d(int nx, int ny, int nz, const double *oC,
+                       const double *cc, const double *fc, const double *oE,
+                       const double *oN, const double *uC, const double *oNE,
+                       const double *oNW, const double *uE, const double *uW,
+                       const double *uN, const double *uS, const double *uNE,
+                       const double *uNW, const double *uSE, const double *uSW,
+                       const double *x, double *r, pmg_stream_t stream);
+
+/* Restriction xout = P^T xin on the coarse interior.
+ * Replaces pmgc::Vrestrc2, pmgc/matvecd.cc:695-799. */
+int pmg_Vrestrc2_d(int nxf, int nyf, int nzf, int nxc, int nyc, int nzc,
+                   const double *xin, double *xout, const double *oPC,
+                   const double *oPN, const double *oPS, const double *oPE,
+                   const double *oPW, const double *oPNE, const double *oPNW,
+                   const double *oPSE, const double *oPSW, const double *uPC,
+                   const double *uPN, const double *uPS, const double *uPE,
+                   const double *uPW, const double *uPNE, const double *uPNW,
+                   const double *uPSE, const double *uPSW, const double *dPC,
+                   const double *dPN, const double *dPS, const double *dPE,
+                   const double *dPW, const double *dPNE, const double *dPNW,
+                   const double *dPSE, const double *dPSW,
+                   pmg_stream_t stream);
+
+/* Operator-based interpolation xout = P xin: every coarse (ii,jj,kk) in
+ * [1,n_c-1]^3 writes its eight fine points.
+ * Replaces pmgc::VinterpPMG2, pmgc/matvecd.cc:819-964. */
+int pmg_VinterpPMG2_d(int nxc, int nyc, int nzc, int nxf, int nyf, int nzf,
+                      const double *xin, double *xout, const double *oPC,
+                      const double *oPN, const double *oPS, const double *oPE,
+                      const double *oPW, const double *oPNE, const double *oPNW,
+                      const double *oPSE, const double *oPSW, const double *uPC,
+                      const double *uPN, const double *uPS, const double *uPE,
+                      const double *uPW, const double *uPNE, const double *uPNW,
+                      const double *uPSE, const double *uPSW, const double *dPC,
+                      const double *dPN, const double *dPS, const double *dPE,
+                      const double *dPW, const double *dPNE, const double *dPNW,
+                      const double *dPSE, const double *dPSW,
+                      pmg_stream_t stream);
+
+/* Operator-based prolongation from a 7-point fine operator (27 outputs on
+ * the coarse grid). Replaces pmgc::VbuildPb_op7, pmgc/buildPd.cc:172-555. */
+int pmg_VbuildPb_op7_d(int nxf, int nyf, int nzf, int nxc, int nyc, int nzc,
+                       const double *oC, const double *oE, const double *oN,
+                       const double *uC, double *oPC, double *oPN,
+                       double *oPS, double *oPE, double *oPW, double *oPNE,
+                       double *oPNW, double *oPSE, double *oPSW, double *uPC,
+                       double *uPN, double *uPS, double *uPE, double *uPW,
+                       double *uPNE, double *uPNW, double *uPSE, double *uPSW,
+                       double *dPC, double *dPN, double *dPS, double *dPE,
+                       double *dPW, double *dPNE, double *dPNW, double *dPSE,
+                       double *dPSW, pmg_stream_t stream);
+/* Operator-based prolongation from a 27-point fine operator.
+ * Replaces pmgc::VbuildPb_op27, pmgc/buildPd.cc:578-1091. */
+int pmg_VbuildPb_op27_d(int nxf, int nyf, int nzf, int nxc, int nyc, int nzc,
+                        const double *oC, const double *oE, const double *oN,
+                        const double *uC, const double *oNE,
+                        const double *oNW, const double *uE, const double *uW,
+                        const double *uN, const double *uS, const double *uNE,
+                        const double *uNW, const double *uSE,
+                        const double *uSW, double *oPC, double *oPN,
+                        double *oPS, double *oPE, double *oPW, double *oPNE,
+                        double *oPNW, double *oPSE, double *oPSW, double *uPC,
+                        double *uPN, double *uPS, double *uPE, double *uPW,
+                        double *uPNE, double *uPNW, double *uPSE, double *uPSW,
+                        double *dPC, double *dPN, double *dPS, double *dPE,
+                        double *dPW, double *dPNE, double *dPNW, double *dPSE,
+                        double *dPSW, pmg_stream_t stream);
+/* Constant (trilinear) prolongation weights.
+ * Replaces pmgc::VbuildPb_trilin, pmgc/buildPd.cc:62-153. */
+int pmg_VbuildPb_trilin_d(int nxf, int nyf, int nzf, int nxc, int nyc,
+                          int nzc, double *oPC, double *oPN, double *oPS,
+                          double *oPE, double *oPW, double *oPNE, double *oPNW,
+                          double *oPSE, double *oPSW, double *uPC, double *uPN,
+                          double *uPS, double *uPE, double *uPW, double *uPNE,
+                          double *uPNW, double *uPSE, double *uPSW,
+                          double *dPC, double *dPN, double *dPS, double *dPE,
+                          double *dPW, double *dPNE, double *dPNW,
+                          double *dPSE, double *dPSW, pmg_stream_t stream);
+
+/* Galerkin coarse operator A_c = P^T A_f P from a 7-point fine operator:
+ * 14 coarse diagonals XoC..XuSW. Replaces pmgc::VbuildG_7,
+ * pmgc/buildGd.cc:437-1361. p27 = the 27 prolongation arrays in list order,
+ * out14 = the 14 outputs (host arrays of device pointers). */
+int pmg_VbuildG_7_d(int nxf, int nyf, int nzf, int nxc, int nyc, int nzc,
+                    const double *const *p27, const double *oC,
+                    const double *oE, const double *oN, const double *uC,
+                    double *const *out14, pmg_stream_t stream);
+/* Galerkin coarse operator from a 27-point fine operator (a14 = fine
+ * diagonals oC..uSW). Replaces pmgc::VbuildG_27, pmgc/buildGd.cc:1363-3274. */
+int pmg_VbuildG_27_d(int nxf, int nyf, int nzf, int nxc, int nyc, int nzc,
+                     const double *const *p27, const double *const *a14,
+                     double *const *out14, pmg_stream_t stream);
+
+/* ======================================================================
+ * Class-level helpers of PBE_linear_problem (device pointers)
+ * ==================================================================== */
+
+/* Coarsest-level CG exactly as the class runs it: warm start from x,
+ * absolute stop sqrt(r.r) <= thresh (the first test on sqrt(sqrt(r.r))),
+ * early exit when the first p.Ap is 0, at most max_iters iterations (the
+ * reference has no cap). a14 = 14 diagonals (host array of device
+ * pointers). *iters (host) gets the iteration count. One CTA; grids up to
+ * 33^3. Synchronises the stream. Replaces cg_solver::CG_solver with
+ * thresh_criterion, CG_Solver.h:45-242, as called by solve_by_cg,
+ * PBE_pmgc_class.h:856-860. */
+int pmg_cg_level_d(int nx, int ny, int nz, const double *const *a14,
+                   const double *rhs, double *x, double thresh, int max_iters,
+                   int *iters, pmg_stream_t stream);
+
+/* ======================================================================
+ * Fine-level set-up from atoms (host)
+ * ==================================================================== */
+
+/* Physical parameters of a linearized PB problem. */
+typedef struct {
+  double eps_in;         /* solute dielectric (reference: epsilon_p)        */
+  double eps_out;        /* solvent dielectric (reference: epsilon_r)       */
+  double ionic_strength; /* 1:1 salt, mol/l                                 */
+  double ion_radius;     /* Angstrom, inflates the ion-exclusion spheres    */
+  double temperature;    /* K                                               */
+  double probe_radius;   /* Angstrom; 0 = van der Waals dielectric boundary */
+} pmg_physics;
+
+/* Inverse Debye length (1/Angstrom) and the vacuum permittivity in the
+ * reference's reduced units (e^2 / (kT Angstrom)); KappaA and epsilon,
+ * scientific_quantities.h:8-55. Either output may be NULL. */
+int pmg_kappa(const pmg_physics *phys, double *kappa, double *eps0);
+
+/* Builds the fine level of an n^3 grid with spacing h (host arrays, n^3
+ * doubles each) from natoms rows (x, y, z, radius, charge) in the grid's
+ * frame (grid point (i0,i1,i2) sits at (i0 h, i1 h, i2 h); coordinate 0 lies
+ * on the slowest array axis, as the reference's Position[0]):
+ *   oE oN uC  eps/h^2 at the staggered points (x fastest: oE), eps_in inside
+ *             the solute, eps_out outside;
+ *   oC        sum of the six face coefficients plus kappa^2 eps_out outside
+ *             the ion-exclusion spheres (interior only);
+ *   f         trilinear charges q / eps0 / h^3;
+ *   x0        multiple Debye-Hueckel boundary values on the shell, 0 inside.
+ * Replaces initialize_epsilons, set_up_rhs and initialize_boundary of the
+ * class, PBE_pmgc_class.h:141-349 (probe_radius 0 reproduces them). */
+int pmg_setup_fine(int n, double h, const double *atoms, int natoms,
+                   const pmg_physics *phys, double *oC, double *oE,
+                   double *oN, double *uC, double *f, double *x0);
+
+/* ======================================================================
+ * Problem handle: PBE_linear_problem<base, nlev, box> with runtime sizes
+ * (PBE_pmgc_class.h:112-1174). Level L has n_L = base*2^L + 1 points per
+ * axis; level nlev is the finest, level 1 the coarsest (CG).
+ * ==================================================================== */
+
+typedef struct pmg_problem pmg_problem;
+
+typedef enum {
+  PMG_PREC_FP64 = 0,  /* V-cycles in double (the reference's arithmetic)  */
+  PMG_PREC_MIXED = 1  /* float V-cycles inside double iterative refinement */
+} pmg_precision;
+
+/* Creates a problem on the current CUDA device; allocates its hierarchy.
+ * stream may be NULL (a private stream is created). */
+int pmg_problem_create(int base, int nlev, double box, int precision,
+                       pmg_stream_t stream, pmg_problem **out);
+/* Frees the handle and everything it allocated. */
+int pmg_problem_destroy(pmg_problem *p);
+/* Device bytes held by a problem of this shape (for admission control). */
+long long pmg_problem_bytes(int base, int nlev, int precision);
+
+/* Loads the fine level: oC (kappa^2 folded in), oE, oN, uC, the right-hand
+ * side f and the initial iterate x0 whose shell holds the boundary values.
+ * Pointers may be host or device memory (copied). Replaces filling the
+ * class's maps by initialize_epsilons / set_up_rhs / initialize_boundary,
+ * PBE_pmgc_class.h:191-349. */
+int pmg_problem_set_fine(pmg_problem *p, const double *oC, const double *oE,
+                         const double *oN, const double *uC, const double *f,
+                         const double *x0);
+
+/* Builds the Galerkin hierarchy (P then A_c per level); trilinear != 0 uses
+ * constant weights. Replaces buildmultilevelops, PBE_pmgc_class.h:351-617. */
+int pmg_build_hierarchy(pmg_problem *p, int trilinear);
+
+/* One V-cycle of the class (v_cycle, PBE_pmgc_class.h:1070-1114); with
+ * as_preconditioner != 0 every level is zero-initialised. FP64 problems
+ * only. */
+int pmg_vcycle(pmg_problem *p, int as_preconditioner);
+
+/* sqrt(sum_interior (f - A x)^2 / n^3) of the finest level; synchronises.
+ * Replaces compute_residual_2, PBE_pmgc_class.h:768-772. */
+int pmg_compute_residual_2(pmg_problem *p, double *out);
+
+/* Solves to compute_residual_2()/r0 < tol with at most max_cycles V-cycles
+ * (FP64) or refinement steps (mixed). *cycles and *relres (host) get the
+ * cycles run and the final relative residual; hist (host, may be NULL,
+ * max_cycles+1 entries) the residual norm per cycle. Returns
+ * PMG_ERR_DIVERGED on NaN/Inf or stagnation. */
+int pmg_solve(pmg_problem *p, double tol, int max_cycles, int *cycles,
+              double *relres, double *hist);
+
+/* Copies the finest iterate (n^3 doubles incl. shell) to dst (host or
+ * device). */
+int pmg_get_potential(pmg_problem *p, double *dst);
+
+/* Copies level L's hierarchy out (host or device dst): 27 prolongation
+ * arrays then 14 operator arrays, n_L^3 doubles each; L in [1, nlev-1]. */
+int pmg_get_level(pmg_problem *p, int level, double *dst);
+
+/* The class's stream (for callers that enqueue around a solve). */
+pmg_stream_t pmg_problem_stream(pmg_problem *p);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PMG_B200_H */

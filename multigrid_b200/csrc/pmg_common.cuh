@@ -1,0 +1,135 @@
+// Shared device helpers for the PMG kernels (sm_100a).
+//
+// Grid layout is the reference's (pmgc/vmatrix.h:79-80): an nx*ny*nz array
+// per quantity with a one-point Dirichlet shell, x fastest, 1-based
+// (i,j,k) -> ((k-1)*ny + (j-1))*nx + (i-1). Grids are at most 1025 points per
+// axis, so every linear index fits in 32 bits.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/pmg_b200.h"
+
+namespace pmg {
+
+constexpr int kMaxN = 1025;
+
+struct Dims {
+  int nx, ny, nz;
+  __host__ __device__ int sy() const { return nx; }
+  __host__ __device__ int sz() const { return nx * ny; }
+  __host__ __device__ int at(int i, int j, int k) const {
+    return ((k - 1) * ny + (j - 1)) * nx + (i - 1);
+  }
+  __host__ __device__ long count() const { return (long)nx * ny * nz; }
+};
+
+// The 14 upper diagonals of a symmetric 27-point operator in the reference's
+// order oC oE oN uC oNE oNW uE uW uN uS uNE uNW uSE uSW; a 7-point operator
+// uses the first four.
+template <typename T> struct Op14 {
+  const T *a[14];
+};
+template <typename T> struct Op14W {
+  T *a[14];
+};
+// The 27 prolongation arrays: oP{C,N,S,E,W,NE,NW,SE,SW}, uP*, dP*.
+template <typename T> struct P27 {
+  const T *p[27];
+};
+template <typename T> struct P27W {
+  T *p[27];
+};
+
+enum OpSlot {
+  kOC = 0, kOE, kON, kUC, kONE, kONW, kUE, kUW, kUN, kUS, kUNE, kUNW, kUSE,
+  kUSW
+};
+
+// Slot of the stored upper diagonal for a neighbour offset, 0 when the offset
+// points to the lower half (read from the neighbour) or is the centre.
+__host__ __device__ constexpr int upper_slot(int ex, int ey, int ez) {
+  return ez == 1
+             ? (ey == -1 ? (ex == -1 ? kUSW : ex == 0 ? kUS : kUSE)
+                : ey == 0 ? (ex == -1 ? kUW : ex == 0 ? kUC : kUE)
+                          : (ex == -1 ? kUNW : ex == 0 ? kUN : kUNE))
+         : (ez == 0 && ey == 1) ? (ex == -1 ? kONW : ex == 0 ? kON : kONE)
+         : (ez == 0 && ey == 0 && ex == 1) ? kOE
+                                           : 0;
+}
+
+// Slot in the 27-array prolongation list of fine offset (dx,dy,dz) from a
+// coarse point's fine image: plane (o: dz=0, u: +1, d: -1) * 9 + in-plane
+// position C N S E W NE NW SE SW.
+__host__ __device__ constexpr int pslot(int dx, int dy, int dz) {
+  return (dz == 0 ? 0 : dz == 1 ? 9 : 18) +
+         (dy == 0 ? (dx == 0 ? 0 : dx == 1 ? 3 : 4)
+          : dy == 1 ? (dx == 0 ? 1 : dx == 1 ? 5 : 6)
+                    : (dx == 0 ? 2 : dx == 1 ? 7 : 8));
+}
+
+// Positive coupling between point p and p + (ex,ey,ez) of a symmetric
+// operator; the lower half is read from the upper diagonal stored at the
+// neighbour (pmgc/matvecd.h:208-236). Offsets are compile-time after
+// unrolling.
+template <typename T>
+__device__ __forceinline__ T coupling(const Op14<T> &A, const Dims &d, int p,
+                                      int ex, int ey, int ez) {
+  const int s = upper_slot(ex, ey, ez);
+  if (s) {
+    const T *a = A.a[s];
+    return a ? a[p] : T(0);
+  }
+  const int s2 = upper_slot(-ex, -ey, -ez);
+  const T *a = A.a[s2];
+  return a ? a[p + ex + ey * d.sy() + ez * d.sz()] : T(0);
+}
+
+// Block-wide sum of one value per thread into thread 0 (any blockDim that is
+// a multiple of 32, at most 1024). `sh` needs 32 entries.
+template <typename T> __device__ __forceinline__ T block_sum(T v, T *sh) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
+    v += __shfl_down_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0)
+    sh[w] = v;
+  __syncthreads();
+  const int nw = (blockDim.x + 31) >> 5;
+  v = (threadIdx.x < nw) ? sh[threadIdx.x] : T(0);
+  if (w == 0) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+      v += __shfl_down_sync(0xffffffffu, v, o);
+  }
+  return v;
+}
+
+} // namespace pmg
+
+// Host-side error plumbing: every entry point returns a pmg_status.
+#define PMG_CUDA_TRY(expr)                                                     \
+  do {                                                                         \
+    cudaError_t _e = (expr);                                                   \
+    if (_e != cudaSuccess) {                                                   \
+      pmg::set_last_error(_e, #expr, __FILE__, __LINE__);                      \
+      return PMG_ERR_CUDA;                                                     \
+    }                                                                          \
+  } while (0)
+
+#define PMG_LAUNCH_CHECK()                                                     \
+  do {                                                                         \
+    cudaError_t _e = cudaGetLastError();                                       \
+    if (_e != cudaSuccess) {                                                   \
+      pmg::set_last_error(_e, "kernel launch", __FILE__, __LINE__);            \
+      return PMG_ERR_CUDA;                                                     \
+    }                                                                          \
+  } while (0)
+
+namespace pmg {
+void set_last_error(cudaError_t e, const char *what, const char *file,
+                    int line);
+void set_last_message(const char *msg);
+} // namespace pmg

@@ -1,0 +1,532 @@
+// Non-template kernels and the per-kernel C-ABI entry points (pmgc names).
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+
+#include "build_kernels.cuh"
+#include "launch.cuh"
+#include "reduce_kernels.cuh"
+
+namespace pmg {
+
+// ---------------------------------------------------------------------------
+// error plumbing
+// ---------------------------------------------------------------------------
+static thread_local char g_last_error[512] = "no error";
+
+void set_last_error(cudaError_t e, const char *what, const char *file,
+                    int line) {
+  snprintf(g_last_error, sizeof(g_last_error), "%s failed: %s (%s:%d)", what,
+           cudaGetErrorString(e), file, line);
+}
+void set_last_message(const char *msg) {
+  snprintf(g_last_error, sizeof(g_last_error), "%s", msg);
+}
+
+// ---------------------------------------------------------------------------
+// non-template kernels
+// ---------------------------------------------------------------------------
+__global__ void add_correction_kernel(Dims d, double *__restrict__ x,
+                                      const float *__restrict__ e) {
+  const Interior t = interior_point(d);
+  if (!t.ok)
+    return;
+  const int p = d.at(t.i, t.j, t.k);
+  x[p] = x[p] + (double)e[p];
+}
+
+__global__ void buildP_trilin_kernel(Dims dc, P27W<double> P) {
+  const Interior t = interior_point(dc);
+  if (!t.ok)
+    return;
+  const int pc = dc.at(t.i, t.j, t.k);
+#pragma unroll
+  for (int dz = -1; dz <= 1; ++dz)
+#pragma unroll
+    for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
+      for (int dx = -1; dx <= 1; ++dx) {
+        const int nnz = (dx != 0) + (dy != 0) + (dz != 0);
+        P.p[pslot(dx, dy, dz)][pc] = 1.0 / (double)(1 << nnz);
+      }
+}
+
+__global__ void __launch_bounds__(1024)
+    cg_level_kernel(Dims d, Op14<double> A, const double *__restrict__ rhs,
+                    double *__restrict__ x, double *__restrict__ r,
+                    double *__restrict__ p, double thresh, int max_iters,
+                    int *__restrict__ status) {
+  __shared__ double sh[32];
+  __shared__ double bc;
+  const int m = (d.nx - 2) * (d.ny - 2) * (d.nz - 2);
+  const int sy = d.sy(), sz = d.sz();
+  const int tid = threadIdx.x, nt = blockDim.x;
+  auto bsum = [&](double v) {
+    v = block_sum(v, sh);
+    if (tid == 0)
+      bc = v;
+    __syncthreads();
+    const double out = bc;
+    __syncthreads();
+    return out;
+  };
+
+  // r = rhs - A x; p = r
+  for (int q = tid; q < m; q += nt) {
+    int i, j, k;
+    interior_coords(d, q, i, j, k);
+    const int c = d.at(i, j, k);
+    const double v = rhs[c] - apply27(A, (const double *)nullptr, x, c, sy, sz);
+    r[c] = v;
+    p[c] = v;
+  }
+  __syncthreads();
+  double acc = 0.0;
+  for (int q = tid; q < m; q += nt) {
+    int i, j, k;
+    interior_coords(d, q, i, j, k);
+    const int c = d.at(i, j, k);
+    acc += r[c] * r[c];
+  }
+  double rs = bsum(acc);
+  acc = 0.0;
+  for (int q = tid; q < m; q += nt) {
+    int i, j, k;
+    interior_coords(d, q, i, j, k);
+    const int c = d.at(i, j, k);
+    acc += apply27(A, (const double *)nullptr, p, c, sy, sz) * p[c];
+  }
+  double pap = bsum(acc);
+  int it = 0;
+  double res = 0.0;
+  if (pap != 0.0) {
+    double alpha = rs / pap;
+    res = sqrt(sqrt(rs));
+    while (res > thresh && it < max_iters) {
+      ++it;
+      for (int q = tid; q < m; q += nt) {
+        int i, j, k;
+        interior_coords(d, q, i, j, k);
+        const int c = d.at(i, j, k);
+        const double ap = apply27(A, (const double *)nullptr, p, c, sy, sz);
+        x[c] += alpha * p[c];
+        r[c] -= alpha * ap;
+      }
+      __syncthreads();
+      acc = 0.0;
+      for (int q = tid; q < m; q += nt) {
+        int i, j, k;
+        interior_coords(d, q, i, j, k);
+        const int c = d.at(i, j, k);
+        acc += r[c] * r[c];
+      }
+      const double rsn = bsum(acc);
+      const double beta = rs == 0.0 ? 0.0 : rsn / rs;
+      rs = rsn;
+      for (int q = tid; q < m; q += nt) {
+        int i, j, k;
+        interior_coords(d, q, i, j, k);
+        const int c = d.at(i, j, k);
+        p[c] = r[c] + beta * p[c];
+      }
+      __syncthreads();
+      acc = 0.0;
+      for (int q = tid; q < m; q += nt) {
+        int i, j, k;
+        interior_coords(d, q, i, j, k);
+        const int c = d.at(i, j, k);
+        acc += apply27(A, (const double *)nullptr, p, c, sy, sz) * p[c];
+      }
+      pap = bsum(acc);
+      alpha = pap == 0.0 ? 0.0 : rs / pap;
+      res = sqrt(rs);
+    }
+  }
+  if (tid == 0) {
+    status[0] = it;
+    status[1] = (it >= max_iters && res > thresh) ? 1 : 0;
+  }
+}
+
+} // namespace pmg
+
+using namespace pmg;
+
+// ---------------------------------------------------------------------------
+// argument checks
+// ---------------------------------------------------------------------------
+static bool bad_dims(int nx, int ny, int nz) {
+  return nx < 3 || ny < 3 || nz < 3 || nx > kMaxN || ny > kMaxN ||
+         nz > kMaxN;
+}
+static bool bad_pair(int nxf, int nyf, int nzf, int nxc, int nyc, int nzc) {
+  return bad_dims(nxf, nyf, nzf) || bad_dims(nxc, nyc, nzc) ||
+         nxf != 2 * nxc - 1 || nyf != 2 * nyc - 1 || nzf != 2 * nzc - 1;
+}
+#define PMG_REQUIRE(cond, msg)                                                 \
+  do {                                                                         \
+    if (!(cond)) {                                                             \
+      set_last_message(msg);                                                   \
+      return PMG_ERR_ARG;                                                      \
+    }                                                                          \
+  } while (0)
+
+template <typename T>
+static Op14<T> op7(const T *oC, const T *oE, const T *oN, const T *uC) {
+  Op14<T> A{};
+  A.a[kOC] = oC;
+  A.a[kOE] = oE;
+  A.a[kON] = oN;
+  A.a[kUC] = uC;
+  return A;
+}
+template <typename T>
+static Op14<T> op27(const T *oC, const T *oE, const T *oN, const T *uC,
+                    const T *oNE, const T *oNW, const T *uE, const T *uW,
+                    const T *uN, const T *uS, const T *uNE, const T *uNW,
+                    const T *uSE, const T *uSW) {
+  return Op14<T>{{oC, oE, oN, uC, oNE, oNW, uE, uW, uN, uS, uNE, uNW, uSE,
+                  uSW}};
+}
+template <typename T> static bool any_null(const Op14<T> &A, int n) {
+  for (int s = 0; s < n; ++s)
+    if (!A.a[s])
+      return true;
+  return false;
+}
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+const char *pmg_last_error(void) { return g_last_error; }
+const char *pmg_version(void) { return "pmg_b200 0.1 (sm_100a)"; }
+
+#define GS7_BODY(T)                                                            \
+  PMG_REQUIRE(!bad_dims(nx, ny, nz), "Vgsrb7x: grid size out of range");       \
+  PMG_REQUIRE(oC && fc && oE && oN && uC && x, "Vgsrb7x: null array");         \
+  PMG_REQUIRE(itmax >= 0, "Vgsrb7x: itmax < 0");                               \
+  return launch_gs7<T>(Dims{nx, ny, nz}, oC, cc, fc, oE, oN, uC, x, itmax,    \
+                       iadjoint, zero_init, (cudaStream_t)stream);
+
+int pmg_Vgsrb7x_d(int nx, int ny, int nz, const double *oC, const double *cc,
+                  const double *fc, const double *oE, const double *oN,
+                  const double *uC, double *x, int itmax, int iadjoint,
+                  int zero_init, pmg_stream_t stream) {
+  GS7_BODY(double)
+}
+int pmg_Vgsrb7x_f(int nx, int ny, int nz, const float *oC, const float *cc,
+                  const float *fc, const float *oE, const float *oN,
+                  const float *uC, float *x, int itmax, int iadjoint,
+                  int zero_init, pmg_stream_t stream) {
+  GS7_BODY(float)
+}
+
+#define GS27_BODY(T)                                                           \
+  PMG_REQUIRE(!bad_dims(nx, ny, nz), "Vgsrb27x: grid size out of range");      \
+  const Op14<T> A =                                                            \
+      op27<T>(oC, oE, oN, uC, oNE, oNW, uE, uW, uN, uS, uNE, uNW, uSE, uSW);  \
+  PMG_REQUIRE(!any_null(A, 14) && fc && x, "Vgsrb27x: null array");            \
+  PMG_REQUIRE(itmax >= 0, "Vgsrb27x: itmax < 0");                              \
+  return launch_gs27<T>(Dims{nx, ny, nz}, A, cc, fc, x, itmax, iadjoint,      \
+                        zero_init, (cudaStream_t)stream);
+
+int pmg_Vgsrb27x_d(int nx, int ny, int nz, const double *oC, const double *cc,
+                   const double *fc, const double *oE, const double *oN,
+                   const double *uC, const double *oNE, const double *oNW,
+                   const double *uE, const double *uW, const double *uN,
+                   const double *uS, const double *uNE, const double *uNW,
+                   const double *uSE, const double *uSW, double *x, int itmax,
+                   int zero_init, int iadjoint, pmg_stream_t stream) {
+  GS27_BODY(double)
+}
+int pmg_Vgsrb27x_f(int nx, int ny, int nz, const float *oC, const float *cc,
+                   const float *fc, const float *oE, const float *oN,
+                   const float *uC, const float *oNE, const float *oNW,
+                   const float *uE, const float *uW, const float *uN,
+                   const float *uS, const float *uNE, const float *uNW,
+                   const float *uSE, const float *uSW, float *x, int itmax,
+                   int zero_init, int iadjoint, pmg_stream_t stream) {
+  GS27_BODY(float)
+}
+
+int pmg_Vmatvec7_1s_d(int nx, int ny, int nz, const double *oC,
+                      const double *cc, const double *oE, const double *oN,
+                      const double *uC, const double *x, double *y,
+                      pmg_stream_t stream) {
+  PMG_REQUIRE(!bad_dims(nx, ny, nz), "Vmatvec7_1s: grid size out of range");
+  PMG_REQUIRE(oC && oE && oN && uC && x && y, "Vmatvec7_1s: null array");
+  const Dims d{nx, ny, nz};
+  matvec_kernel<7, double><<<interior_grid(d), interior_block(),
+                             0, (cudaStream_t)stream>>>(
+      d, op7(oC, oE, oN, uC), cc, x, y);
+  PMG_LAUNCH_CHECK();
+  return PMG_OK;
+}
+
+int pmg_Vmatvec27_1s_d(int nx, int ny, int nz, const double *oC,
+                       const double *cc, const double *oE, const double *oN,
+                       const double *uC, const double *oNE, const double *oNW,
+                       const double *uE, const double *uW, const double *uN,
+                       const double *uS, const double *uNE, const double *uNW,
+                       const double *uSE, const double *uSW, const double *x,
+                       double *y, pmg_stream_t stream) {
+  PMG_REQUIRE(!bad_dims(nx, ny, nz), "Vmatvec27_1s: grid size out of range");
+  const Op14<double> A =
+      op27(oC, oE, oN, uC, oNE, oNW, uE, uW, uN, uS, uNE, uNW, uSE, uSW);
+  PMG_REQUIRE(!any_null(A, 14) && x && y, "Vmatvec27_1s: null array");
+  const Dims d{nx, ny, nz};
+  matvec_kernel<27, double><<<interior_grid(d), interior_block(), 0,
+                              (cudaStream_t)stream>>>(d, A, cc, x, y);
+  PMG_LAUNCH_CHECK();
+  return PMG_OK;
+}
+
+int pmg_Vmresid7_1s_d(int nx, int ny, int nz, const double *oC,
+                      const double *cc, const double *fc, const double *oE,
+                      const double *oN, const double *uC, const double *x,
+                      double *r, pmg_stream_t stream) {
+  PMG_REQUIRE(!bad_dims(nx, ny, nz), "Vmresid7_1s: grid size out of range");
+  PMG_REQUIRE(oC && fc && oE && oN && uC && x && r,
+              "Vmresid7_1s: null array");
+  const Dims d{nx, ny, nz};
+  mresid_kernel<7, double><<<interior_grid(d), interior_block(), 0,
+                             (cudaStream_t)stream>>>(
+      d, op7(oC, oE, oN, uC), cc, fc, x, r);
+  PMG_LAUNCH_CHECK();
+  return PMG_OK;
+}
+
+int pmg_Vmresid27_1s_d(int nx, int ny, int nz, const double *oC,
+                       const double *cc, const double *fc, const double *oE,
+                       const double *oN, const double *uC, const double *oNE,
+                       const double *oNW, const double *uE, const double *uW,
+                       const double *uN, const double *uS, const double *uNE,
+                       const double *uNW, const double *uSE, const double *uSW,
+                       const double *x, double *r, pmg_stream_t stream) {
+  PMG_REQUIRE(!bad_dims(nx, ny, nz), "Vmresid27_1s: grid size out of range");
+  const Op14<double> A =
+      op27(oC, oE, oN, uC, oNE, oNW, uE, uW, uN, uS, uNE, uNW, uSE, uSW);
+  PMG_REQUIRE(!any_null(A, 14) && fc && x && r, "Vmresid27_1s: null array");
+  const Dims d{nx, ny, nz};
+  mresid_kernel<27, double><<<interior_grid(d), interior_block(), 0,
+                              (cudaStream_t)stream>>>(d, A, cc, fc, x, r);
+  PMG_LAUNCH_CHECK();
+  return PMG_OK;
+}
+
+#define P27_ARGS                                                               \
+  oPC, oPN, oPS, oPE, oPW, oPNE, oPNW, oPSE, oPSW, uPC, uPN, uPS, uPE, uPW,    \
+      uPNE, uPNW, uPSE, uPSW, dPC, dPN, dPS, dPE, dPW, dPNE, dPNW, dPSE, dPSW
+
+int pmg_Vrestrc2_d(int nxf, int nyf, int nzf, int nxc, int nyc, int nzc,
+                   const double *xin, double *xout, const double *oPC,
+                   const double *oPN, const double *oPS, const double *oPE,
+                   const double *oPW, const double *oPNE, const double *oPNW,
+                   const double *oPSE, const double *oPSW, const double *uPC,
+                   const double *uPN, const double *uPS, const double *uPE,
+                   const double *uPW, const double *uPNE, const double *uPNW,
+                   const double *uPSE, const double *uPSW, const double *dPC,
+                   const double *dPN, const double *dPS, const double *dPE,
+                   const double *dPW, const double *dPNE, const double *dPNW,
+                   const double *dPSE, const double *dPSW,
+                   pmg_stream_t stream) {
+  PMG_REQUIRE(!bad_pair(nxf, nyf, nzf, nxc, nyc, nzc),
+              "Vrestrc2: sizes must satisfy n_f = 2 n_c - 1");
+  const P27<double> P{{P27_ARGS}};
+  for (int s = 0; s < 27; ++s)
+    PMG_REQUIRE(P.p[s], "Vrestrc2: null prolongation array");
+  PMG_REQUIRE(xin && xout, "Vrestrc2: null array");
+  const Dims dc{nxc, nyc, nzc};
+  restrict_kernel<double, double><<<interior_grid(dc), interior_block(), 0,
+                                    (cudaStream_t)stream>>>(
+      Dims{nxf, nyf, nzf}, dc, xin, xout, P);
+  PMG_LAUNCH_CHECK();
+  return PMG_OK;
+}
+
+int pmg_VinterpPMG2_d(int nxc, int nyc, int nzc, int nxf, int nyf, int nzf,
+                      const double *xin, double *xout, const double *oPC,
+                      const double *oPN, const double *oPS, const double *oPE,
+                      const double *oPW, const double *oPNE, const double *oPNW,
+                      const double *oPSE, const double *oPSW, const double *uPC,
+                      const double *uPN, const double *uPS, const double *uPE,
+                      const double *uPW, const double *uPNE, const double *uPNW,
+                      const double *uPSE, const double *uPSW, const double *dPC,
+                      const double *dPN, const double *dPS, const double *dPE,
+                      const double *dPW, const double *dPNE, const double *dPNW,
+                      const double *dPSE, const double *dPSW,
+                      pmg_stream_t stream) {
+  PMG_REQUIRE(!bad_pair(nxf, nyf, nzf, nxc, nyc, nzc),
+              "VinterpPMG2: sizes must satisfy n_f = 2 n_c - 1");
+  const P27<double> P{{P27_ARGS}};
+  for (int s = 0; s < 27; ++s)
+    PMG_REQUIRE(P.p[s], "VinterpPMG2: null prolongation array");
+  PMG_REQUIRE(xin && xout, "VinterpPMG2: null array");
+  const Dims dc{nxc, nyc, nzc};
+  interp_kernel<double><<<interp_grid(dc), interior_block(), 0,
+                          (cudaStream_t)stream>>>(dc, Dims{nxf, nyf, nzf},
+                                                  xin, xout, P);
+  PMG_LAUNCH_CHECK();
+  return PMG_OK;
+}
+
+int pmg_VbuildPb_op7_d(int nxf, int nyf, int nzf, int nxc, int nyc, int nzc,
+                       const double *oC, const double *oE, const double *oN,
+                       const double *uC, double *oPC, double *oPN,
+                       double *oPS, double *oPE, double *oPW, double *oPNE,
+                       double *oPNW, double *oPSE, double *oPSW, double *uPC,
+                       double *uPN, double *uPS, double *uPE, double *uPW,
+                       double *uPNE, double *uPNW, double *uPSE, double *uPSW,
+                       double *dPC, double *dPN, double *dPS, double *dPE,
+                       double *dPW, double *dPNE, double *dPNW, double *dPSE,
+                       double *dPSW, pmg_stream_t stream) {
+  PMG_REQUIRE(!bad_pair(nxf, nyf, nzf, nxc, nyc, nzc),
+              "VbuildPb_op7: sizes must satisfy n_f = 2 n_c - 1");
+  PMG_REQUIRE(oC && oE && oN && uC, "VbuildPb_op7: null operator array");
+  const P27W<double> P{{P27_ARGS}};
+  for (int s = 0; s < 27; ++s)
+    PMG_REQUIRE(P.p[s], "VbuildPb_op7: null prolongation array");
+  return launch_buildP(Dims{nxf, nyf, nzf}, Dims{nxc, nyc, nzc}, 7,
+                       op7(oC, oE, oN, uC), P, (cudaStream_t)stream);
+}
+
+int pmg_VbuildPb_op27_d(int nxf, int nyf, int nzf, int nxc, int nyc, int nzc,
+                        const double *oC, const double *oE, const double *oN,
+                        const double *uC, const double *oNE,
+                        const double *oNW, const double *uE, const double *uW,
+                        const double *uN, const double *uS, const double *uNE,
+                        const double *uNW, const double *uSE,
+                        const double *uSW, double *oPC, double *oPN,
+                        double *oPS, double *oPE, double *oPW, double *oPNE,
+                        double *oPNW, double *oPSE, double *oPSW, double *uPC,
+                        double *uPN, double *uPS, double *uPE, double *uPW,
+                        double *uPNE, double *uPNW, double *uPSE, double *uPSW,
+                        double *dPC, double *dPN, double *dPS, double *dPE,
+                        double *dPW, double *dPNE, double *dPNW, double *dPSE,
+                        double *dPSW, pmg_stream_t stream) {
+  PMG_REQUIRE(!bad_pair(nxf, nyf, nzf, nxc, nyc, nzc),
+              "VbuildPb_op27: sizes must satisfy n_f = 2 n_c - 1");
+  const Op14<double> A =
+      op27(oC, oE, oN, uC, oNE, oNW, uE, uW, uN, uS, uNE, uNW, uSE, uSW);
+  PMG_REQUIRE(!any_null(A, 14), "VbuildPb_op27: null operator array");
+  const P27W<double> P{{P27_ARGS}};
+  for (int s = 0; s < 27; ++s)
+    PMG_REQUIRE(P.p[s], "VbuildPb_op27: null prolongation array");
+  return launch_buildP(Dims{nxf, nyf, nzf}, Dims{nxc, nyc, nzc}, 27, A, P,
+                       (cudaStream_t)stream);
+}
+
+int pmg_VbuildPb_trilin_d(int nxf, int nyf, int nzf, int nxc, int nyc,
+                          int nzc, double *oPC, double *oPN, double *oPS,
+                          double *oPE, double *oPW, double *oPNE, double *oPNW,
+                          double *oPSE, double *oPSW, double *uPC, double *uPN,
+                          double *uPS, double *uPE, double *uPW, double *uPNE,
+                          double *uPNW, double *uPSE, double *uPSW,
+                          double *dPC, double *dPN, double *dPS, double *dPE,
+                          double *dPW, double *dPNE, double *dPNW,
+                          double *dPSE, double *dPSW, pmg_stream_t stream) {
+  PMG_REQUIRE(!bad_pair(nxf, nyf, nzf, nxc, nyc, nzc),
+              "VbuildPb_trilin: sizes must satisfy n_f = 2 n_c - 1");
+  const P27W<double> P{{P27_ARGS}};
+  for (int s = 0; s < 27; ++s)
+    PMG_REQUIRE(P.p[s], "VbuildPb_trilin: null prolongation array");
+  const Dims dc{nxc, nyc, nzc};
+  buildP_trilin_kernel<<<interior_grid(dc), interior_block(), 0,
+                         (cudaStream_t)stream>>>(dc, P);
+  PMG_LAUNCH_CHECK();
+  return PMG_OK;
+}
+
+int pmg_VbuildG_7_d(int nxf, int nyf, int nzf, int nxc, int nyc, int nzc,
+                    const double *const *p27, const double *oC,
+                    const double *oE, const double *oN, const double *uC,
+                    double *const *out14, pmg_stream_t stream) {
+  PMG_REQUIRE(!bad_pair(nxf, nyf, nzf, nxc, nyc, nzc),
+              "VbuildG_7: sizes must satisfy n_f = 2 n_c - 1");
+  PMG_REQUIRE(p27 && out14 && oC && oE && oN && uC, "VbuildG_7: null array");
+  P27<double> P;
+  Op14W<double> out;
+  for (int s = 0; s < 27; ++s) {
+    P.p[s] = p27[s];
+    PMG_REQUIRE(P.p[s], "VbuildG_7: null prolongation array");
+  }
+  for (int s = 0; s < 14; ++s) {
+    out.a[s] = out14[s];
+    PMG_REQUIRE(out.a[s], "VbuildG_7: null output array");
+  }
+  return launch_buildG(Dims{nxf, nyf, nzf}, Dims{nxc, nyc, nzc}, 7, P,
+                       op7(oC, oE, oN, uC), out, (cudaStream_t)stream);
+}
+
+int pmg_VbuildG_27_d(int nxf, int nyf, int nzf, int nxc, int nyc, int nzc,
+                     const double *const *p27, const double *const *a14,
+                     double *const *out14, pmg_stream_t stream) {
+  PMG_REQUIRE(!bad_pair(nxf, nyf, nzf, nxc, nyc, nzc),
+              "VbuildG_27: sizes must satisfy n_f = 2 n_c - 1");
+  PMG_REQUIRE(p27 && a14 && out14, "VbuildG_27: null array");
+  P27<double> P;
+  Op14<double> A;
+  Op14W<double> out;
+  for (int s = 0; s < 27; ++s) {
+    P.p[s] = p27[s];
+    PMG_REQUIRE(P.p[s], "VbuildG_27: null prolongation array");
+  }
+  for (int s = 0; s < 14; ++s) {
+    A.a[s] = a14[s];
+    out.a[s] = out14[s];
+    PMG_REQUIRE(A.a[s] && out.a[s], "VbuildG_27: null operator array");
+  }
+  return launch_buildG(Dims{nxf, nyf, nzf}, Dims{nxc, nyc, nzc}, 27, P, A,
+                       out, (cudaStream_t)stream);
+}
+
+int pmg_cg_level_d(int nx, int ny, int nz, const double *const *a14,
+                   const double *rhs, double *x, double thresh, int max_iters,
+                   int *iters, pmg_stream_t stream) {
+  PMG_REQUIRE(!bad_dims(nx, ny, nz) && nx <= 33 && ny <= 33 && nz <= 33,
+              "cg_level: grid must be at most 33^3");
+  PMG_REQUIRE(a14 && rhs && x && max_iters >= 0, "cg_level: bad argument");
+  Op14<double> A;
+  for (int s = 0; s < 14; ++s) {
+    A.a[s] = a14[s];
+    PMG_REQUIRE(A.a[s], "cg_level: null operator array");
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  const Dims d{nx, ny, nz};
+  const size_t n3 = (size_t)d.count();
+  // r, p (zero shells) and the two status words, stream-ordered.
+  char *ws = nullptr;
+  const size_t bytes = 2 * n3 * sizeof(double) + 2 * sizeof(int);
+  PMG_CUDA_TRY(cudaMallocAsync((void **)&ws, bytes, s));
+  int rc = PMG_OK;
+  int host_status[2] = {0, 0};
+  double *r = (double *)ws, *p = r + n3;
+  int *status = (int *)(p + n3);
+  cudaError_t e = cudaMemsetAsync(ws, 0, bytes, s);
+  if (e == cudaSuccess) {
+    cg_level_kernel<<<1, 1024, 0, s>>>(d, A, rhs, x, r, p, thresh, max_iters,
+                                       status);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(host_status, status, sizeof(host_status),
+                        cudaMemcpyDeviceToHost, s);
+  cudaFreeAsync(ws, s);
+  if (e == cudaSuccess)
+    e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) {
+    set_last_error(e, "cg_level", __FILE__, __LINE__);
+    return PMG_ERR_CUDA;
+  }
+  if (iters)
+    *iters = host_status[0];
+  if (host_status[1]) {
+    set_last_message("cg_level: iteration cap reached above the threshold");
+    rc = PMG_ERR_TIMEOUT;
+  }
+  return rc;
+}
+
+} // extern "C"

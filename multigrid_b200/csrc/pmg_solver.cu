@@ -1,0 +1,608 @@
+// Problem handle: the PBE_linear_problem class (PBE_pmgc_class.h:112-1174)
+// with runtime sizes, its Galerkin hierarchy resident in one device arena,
+// the V-cycle, and the FP64 / mixed-precision solves.
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <new>
+
+#include "build_kernels.cuh"
+#include "launch.cuh"
+#include "reduce_kernels.cuh"
+
+namespace pmg {
+
+constexpr int kMaxLevels = 12;
+constexpr int kCgMaxIters = 20000;
+
+struct LevelBuf {
+  int n = 0;
+  Dims d{};
+  long n3 = 0;
+  double *op[14] = {};
+  double *P[27] = {}; // prolongation from this level to level+1
+  double *x = nullptr, *f = nullptr, *r = nullptr;
+  float *op32[14] = {};
+  float *P32[27] = {};
+  float *x32 = nullptr, *f32 = nullptr, *r32 = nullptr;
+  double *omega = nullptr; // damping computed on this level (device)
+
+  Op14<double> A64(int nops) const {
+    Op14<double> A{};
+    for (int s = 0; s < nops; ++s)
+      A.a[s] = op[s];
+    return A;
+  }
+  Op14<float> A32(int nops) const {
+    Op14<float> A{};
+    for (int s = 0; s < nops; ++s)
+      A.a[s] = op32[s];
+    return A;
+  }
+  P27<double> Pc() const {
+    P27<double> p;
+    for (int s = 0; s < 27; ++s)
+      p.p[s] = P[s];
+    return p;
+  }
+  P27<float> Pc32() const {
+    P27<float> p;
+    for (int s = 0; s < 27; ++s)
+      p.p[s] = P32[s];
+    return p;
+  }
+};
+
+// Two-pass arena planner: the first pass (base == nullptr) only counts.
+struct Arena {
+  char *base = nullptr;
+  size_t off = 0;
+  template <typename T> T *take(long count) {
+    off = (off + 255) & ~size_t(255);
+    T *p = base ? reinterpret_cast<T *>(base + off) : nullptr;
+    off += sizeof(T) * (size_t)count;
+    return p;
+  }
+};
+
+} // namespace pmg
+
+using namespace pmg;
+
+struct pmg_problem {
+  int base = 0, nlev = 0, precision = 0;
+  double box = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  char *arena = nullptr;
+  size_t arena_bytes = 0;
+  LevelBuf lv[kMaxLevels + 1];
+  double *cg_r = nullptr, *cg_p = nullptr;
+  int *cg_status = nullptr;
+  ReduceSlot red_norm{}, red_lambda{};
+  double *h_pinned = nullptr; // [0] residual sum, [1..] spare
+  int *h_status = nullptr;
+  bool fine_set = false, built = false;
+  // One V-cycle (plus the residual norm) captured as a CUDA graph.
+  cudaGraphExec_t cycle_exec = nullptr;
+};
+
+namespace {
+
+int level_n(int base, int L) { return base * (1 << L) + 1; }
+
+// Lays out every device array of a problem; with a.base == nullptr only
+// counts bytes.
+void plan(pmg_problem *p, Arena &a) {
+  const bool mixed = p->precision == PMG_PREC_MIXED;
+  for (int L = 1; L <= p->nlev; ++L) {
+    LevelBuf &v = p->lv[L];
+    v.n = level_n(p->base, L);
+    v.d = Dims{v.n, v.n, v.n};
+    v.n3 = v.d.count();
+    const bool fine = L == p->nlev;
+    const int nops = fine ? 4 : 14;
+    for (int s = 0; s < 14; ++s)
+      v.op[s] = s < nops ? a.take<double>(v.n3) : nullptr;
+    for (int s = 0; s < 27; ++s)
+      v.P[s] = fine ? nullptr : a.take<double>(v.n3);
+    // The mixed path keeps double iterates only on the finest level (x64,
+    // f) and on level 1 (the double CG).
+    const bool need64 = !mixed || fine || L == 1;
+    v.x = need64 ? a.take<double>(v.n3) : nullptr;
+    v.f = need64 ? a.take<double>(v.n3) : nullptr;
+    v.r = (mixed && L > 1) ? nullptr : a.take<double>(v.n3);
+    v.omega = a.take<double>(1);
+    if (mixed) {
+      for (int s = 0; s < 14; ++s)
+        v.op32[s] = (L > 1 && s < nops) ? a.take<float>(v.n3) : nullptr;
+      for (int s = 0; s < 27; ++s)
+        v.P32[s] = fine ? nullptr : a.take<float>(v.n3);
+      v.x32 = a.take<float>(v.n3);
+      v.f32 = a.take<float>(v.n3);
+      v.r32 = L > 1 ? a.take<float>(v.n3) : nullptr;
+    }
+  }
+  const long n1 = p->lv[1].n3;
+  p->cg_r = a.take<double>(n1);
+  p->cg_p = a.take<double>(n1);
+  p->cg_status = a.take<int>(2);
+  for (ReduceSlot *s : {&p->red_norm, &p->red_lambda}) {
+    s->partials = a.take<double>(2 * kReduceBlocks);
+    s->ticket = a.take<unsigned int>(1);
+    s->result = a.take<double>(2);
+  }
+}
+
+int check_shape(int base, int nlev) {
+  if (base < 1 || nlev < 2 || nlev > kMaxLevels)
+    return PMG_ERR_ARG;
+  if ((long)base * (1L << nlev) + 1 > kMaxN)
+    return PMG_ERR_ARG;
+  return PMG_OK;
+}
+
+// ---- V-cycle pieces (FP64) ------------------------------------------------
+
+int smooth64(pmg_problem *p, int L, int zero_init) {
+  LevelBuf &v = p->lv[L];
+  if (L == p->nlev)
+    return launch_gs7<double>(v.d, v.op[kOC], nullptr, v.f, v.op[kOE],
+                              v.op[kON], v.op[kUC], v.x, 1, 0, zero_init,
+                              p->stream);
+  return launch_gs27<double>(v.d, v.A64(14), nullptr, v.f, v.x, 1, 0,
+                             zero_init, p->stream);
+}
+
+int cg_level1(pmg_problem *p, const double *rhs, double *x) {
+  LevelBuf &v = p->lv[1];
+  cg_level_kernel<<<1, 1024, 0, p->stream>>>(v.d, v.A64(14), rhs, x, p->cg_r,
+                                             p->cg_p, 1e-8, kCgMaxIters,
+                                             p->cg_status);
+  PMG_LAUNCH_CHECK();
+  return PMG_OK;
+}
+
+int vcycle64(pmg_problem *p, int L, int as_preconditioner) {
+  cudaStream_t s = p->stream;
+  LevelBuf &v = p->lv[L];
+  if (L == 1)
+    return cg_level1(p, v.f, v.x);
+  LevelBuf &c = p->lv[L - 1];
+  const int kind = L == p->nlev ? 7 : 27;
+  int rc;
+  int zero_init = (L != p->nlev) || as_preconditioner;
+  for (int it = 0; it < 2; ++it) {
+    if ((rc = smooth64(p, L, zero_init)))
+      return rc;
+    zero_init = 0;
+  }
+  if (kind == 7)
+    defect_kernel<7, double><<<interior_grid(v.d), interior_block(), 0, s>>>(
+        v.d, v.A64(4), v.f, v.x, v.r);
+  else
+    defect_kernel<27, double><<<interior_grid(v.d), interior_block(), 0, s>>>(
+        v.d, v.A64(14), v.f, v.x, v.r);
+  restrict_kernel<double, double>
+      <<<interior_grid(c.d), interior_block(), 0, s>>>(v.d, c.d, v.r, c.f,
+                                                       c.Pc());
+  PMG_LAUNCH_CHECK();
+  if ((rc = vcycle64(p, L - 1, 0)))
+    return rc;
+  ideal_lambda_kernel<double><<<kReduceBlocks, kReduceThreads, 0, s>>>(
+      c.d, c.A64(14), c.x, c.f, p->red_lambda, c.omega);
+  interp_kernel<double><<<interp_grid(c.d), interior_block(), 0, s>>>(
+      c.d, v.d, c.x, v.r, c.Pc());
+  axpy_full_kernel<double><<<flat_grid(v.n3), 256, 0, s>>>(v.n3, v.x, v.r,
+                                                           c.omega);
+  PMG_LAUNCH_CHECK();
+  for (int it = 0; it < 2; ++it)
+    if ((rc = smooth64(p, L, 0)))
+      return rc;
+  return PMG_OK;
+}
+
+// Residual sum of squares of the finest level into red_norm.result[0] and
+// then into pinned host memory (not synchronised here).
+int residual_norm_async(pmg_problem *p) {
+  LevelBuf &v = p->lv[p->nlev];
+  defect_norm_kernel<7, double, double>
+      <<<kReduceBlocks, kReduceThreads, 0, p->stream>>>(
+          v.d, v.A64(4), v.f, v.x, (double *)nullptr, p->red_norm);
+  PMG_LAUNCH_CHECK();
+  PMG_CUDA_TRY(cudaMemcpyAsync(p->h_pinned, p->red_norm.result,
+                               sizeof(double), cudaMemcpyDeviceToHost,
+                               p->stream));
+  return PMG_OK;
+}
+
+double norm_from_sum(const pmg_problem *p, double s) {
+  const double n3 = (double)p->lv[p->nlev].n3;
+  return sqrt(s / n3);
+}
+
+// ---- mixed precision -------------------------------------------------------
+
+int smooth32(pmg_problem *p, int L, int zero_init) {
+  LevelBuf &v = p->lv[L];
+  if (L == p->nlev)
+    return launch_gs7<float>(v.d, v.op32[kOC], nullptr, v.f32, v.op32[kOE],
+                             v.op32[kON], v.op32[kUC], v.x32, 1, 0, zero_init,
+                             p->stream);
+  return launch_gs27<float>(v.d, v.A32(14), nullptr, v.f32, v.x32, 1, 0,
+                            zero_init, p->stream);
+}
+
+// V-cycle in float on the correction equation, every level zero-started
+// (v_cycle with as_preconditioner, PBE_pmgc_class.h:1070-1114); level 1 in
+// double.
+int vcycle32(pmg_problem *p, int L) {
+  cudaStream_t s = p->stream;
+  LevelBuf &v = p->lv[L];
+  if (L == 1) {
+    convert_kernel<float, double><<<flat_grid(v.n3), 256, 0, s>>>(v.n3, v.f32,
+                                                                 v.f);
+    PMG_CUDA_TRY(cudaMemsetAsync(v.x, 0, sizeof(double) * v.n3, s));
+    return cg_level1(p, v.f, v.x);
+  }
+  LevelBuf &c = p->lv[L - 1];
+  const int kind = L == p->nlev ? 7 : 27;
+  int rc;
+  if ((rc = smooth32(p, L, 1)))
+    return rc;
+  if ((rc = smooth32(p, L, 0)))
+    return rc;
+  if (kind == 7)
+    defect_kernel<7, float><<<interior_grid(v.d), interior_block(), 0, s>>>(
+        v.d, v.A32(4), v.f32, v.x32, v.r32);
+  else
+    defect_kernel<27, float><<<interior_grid(v.d), interior_block(), 0, s>>>(
+        v.d, v.A32(14), v.f32, v.x32, v.r32);
+  restrict_kernel<float, float>
+      <<<interior_grid(c.d), interior_block(), 0, s>>>(v.d, c.d, v.r32, c.f32,
+                                                       c.Pc32());
+  PMG_LAUNCH_CHECK();
+  if ((rc = vcycle32(p, L - 1)))
+    return rc;
+  if (L - 1 == 1) {
+    ideal_lambda_kernel<double><<<kReduceBlocks, kReduceThreads, 0, s>>>(
+        c.d, c.A64(14), c.x, c.f, p->red_lambda, c.omega);
+    convert_kernel<double, float><<<flat_grid(c.n3), 256, 0, s>>>(c.n3, c.x,
+                                                                 c.x32);
+  } else {
+    ideal_lambda_kernel<float><<<kReduceBlocks, kReduceThreads, 0, s>>>(
+        c.d, c.A32(14), c.x32, c.f32, p->red_lambda, c.omega);
+  }
+  interp_kernel<float><<<interp_grid(c.d), interior_block(), 0, s>>>(
+      c.d, v.d, c.x32, v.r32, c.Pc32());
+  axpy_full_kernel<float><<<flat_grid(v.n3), 256, 0, s>>>(v.n3, v.x32, v.r32,
+                                                          c.omega);
+  PMG_LAUNCH_CHECK();
+  for (int it = 0; it < 2; ++it)
+    if ((rc = smooth32(p, L, 0)))
+      return rc;
+  return PMG_OK;
+}
+
+// r64 = f - A x64 on the finest level, written as float into f32 (the
+// correction equation's right-hand side), its sum of squares into red_norm
+// and pinned host memory.
+int mixed_residual_async(pmg_problem *p) {
+  LevelBuf &v = p->lv[p->nlev];
+  defect_norm_kernel<7, double, float>
+      <<<kReduceBlocks, kReduceThreads, 0, p->stream>>>(
+          v.d, v.A64(4), v.f, v.x, v.f32, p->red_norm);
+  PMG_LAUNCH_CHECK();
+  PMG_CUDA_TRY(cudaMemcpyAsync(p->h_pinned, p->red_norm.result,
+                               sizeof(double), cudaMemcpyDeviceToHost,
+                               p->stream));
+  return PMG_OK;
+}
+
+// One refinement step: float V-cycle on the correction, x64 += e, new
+// residual.
+int mixed_step(pmg_problem *p) {
+  LevelBuf &v = p->lv[p->nlev];
+  int rc;
+  if ((rc = vcycle32(p, p->nlev)))
+    return rc;
+  add_correction_kernel<<<interior_grid(v.d), interior_block(), 0,
+                          p->stream>>>(v.d, v.x, v.x32);
+  PMG_LAUNCH_CHECK();
+  return mixed_residual_async(p);
+}
+
+// Captures one cycle (FP64: V-cycle + residual; mixed: refinement step) as a
+// CUDA graph on first use.
+int ensure_graph(pmg_problem *p) {
+  if (p->cycle_exec)
+    return PMG_OK;
+  cudaGraph_t g = nullptr;
+  PMG_CUDA_TRY(
+      cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal));
+  int rc;
+  if (p->precision == PMG_PREC_MIXED) {
+    rc = mixed_step(p);
+  } else {
+    rc = vcycle64(p, p->nlev, 0);
+    if (!rc)
+      rc = residual_norm_async(p);
+  }
+  cudaError_t e = cudaStreamEndCapture(p->stream, &g);
+  if (rc)
+    return rc;
+  if (e != cudaSuccess) {
+    set_last_error(e, "cudaStreamEndCapture", __FILE__, __LINE__);
+    return PMG_ERR_CUDA;
+  }
+  e = cudaGraphInstantiate(&p->cycle_exec, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) {
+    p->cycle_exec = nullptr;
+    set_last_error(e, "cudaGraphInstantiate", __FILE__, __LINE__);
+    return PMG_ERR_CUDA;
+  }
+  return PMG_OK;
+}
+
+} // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+long long pmg_problem_bytes(int base, int nlev, int precision) {
+  if (check_shape(base, nlev))
+    return -1;
+  pmg_problem tmp;
+  tmp.base = base;
+  tmp.nlev = nlev;
+  tmp.precision = precision;
+  Arena a;
+  plan(&tmp, a);
+  return (long long)a.off;
+}
+
+int pmg_problem_create(int base, int nlev, double box, int precision,
+                       pmg_stream_t stream, pmg_problem **out) {
+  if (!out || check_shape(base, nlev) ||
+      (precision != PMG_PREC_FP64 && precision != PMG_PREC_MIXED)) {
+    set_last_message("pmg_problem_create: bad argument");
+    return PMG_ERR_ARG;
+  }
+  *out = nullptr;
+  pmg_problem *p = new (std::nothrow) pmg_problem();
+  if (!p)
+    return PMG_ERR_NOMEM;
+  p->base = base;
+  p->nlev = nlev;
+  p->box = box;
+  p->precision = precision;
+  Arena a;
+  plan(p, a);
+  p->arena_bytes = a.off;
+  cudaError_t e = cudaMalloc((void **)&p->arena, p->arena_bytes);
+  if (e != cudaSuccess) {
+    delete p;
+    set_last_error(e, "cudaMalloc(problem arena)", __FILE__, __LINE__);
+    return PMG_ERR_NOMEM;
+  }
+  Arena b;
+  b.base = p->arena;
+  plan(p, b);
+  if (stream) {
+    p->stream = (cudaStream_t)stream;
+  } else {
+    e = cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking);
+    p->own_stream = e == cudaSuccess;
+  }
+  if (e == cudaSuccess)
+    e = cudaMallocHost((void **)&p->h_pinned, 4 * sizeof(double));
+  if (e == cudaSuccess)
+    e = cudaMemsetAsync(p->arena, 0, p->arena_bytes, p->stream);
+  if (e == cudaSuccess)
+    e = cudaStreamSynchronize(p->stream);
+  if (e != cudaSuccess) {
+    set_last_error(e, "pmg_problem_create", __FILE__, __LINE__);
+    pmg_problem_destroy(p);
+    return PMG_ERR_CUDA;
+  }
+  *out = p;
+  return PMG_OK;
+}
+
+int pmg_problem_destroy(pmg_problem *p) {
+  if (!p)
+    return PMG_OK;
+  if (p->stream)
+    cudaStreamSynchronize(p->stream);
+  if (p->cycle_exec)
+    cudaGraphExecDestroy(p->cycle_exec);
+  if (p->arena)
+    cudaFree(p->arena);
+  if (p->h_pinned)
+    cudaFreeHost(p->h_pinned);
+  if (p->own_stream)
+    cudaStreamDestroy(p->stream);
+  delete p;
+  return PMG_OK;
+}
+
+pmg_stream_t pmg_problem_stream(pmg_problem *p) {
+  return p ? (pmg_stream_t)p->stream : nullptr;
+}
+
+int pmg_problem_set_fine(pmg_problem *p, const double *oC, const double *oE,
+                         const double *oN, const double *uC, const double *f,
+                         const double *x0) {
+  if (!p || !oC || !oE || !oN || !uC || !f || !x0) {
+    set_last_message("pmg_problem_set_fine: null argument");
+    return PMG_ERR_ARG;
+  }
+  LevelBuf &v = p->lv[p->nlev];
+  const size_t b = sizeof(double) * v.n3;
+  const double *src[6] = {oC, oE, oN, uC, f, x0};
+  double *dst[6] = {v.op[kOC], v.op[kOE], v.op[kON], v.op[kUC], v.f, v.x};
+  for (int q = 0; q < 6; ++q)
+    PMG_CUDA_TRY(
+        cudaMemcpyAsync(dst[q], src[q], b, cudaMemcpyDefault, p->stream));
+  p->fine_set = true;
+  p->built = false;
+  return PMG_OK;
+}
+
+int pmg_build_hierarchy(pmg_problem *p, int trilinear) {
+  if (!p)
+    return PMG_ERR_ARG;
+  if (!p->fine_set) {
+    set_last_message("pmg_build_hierarchy: fine level not set");
+    return PMG_ERR_STATE;
+  }
+  cudaStream_t s = p->stream;
+  int rc;
+  for (int L = p->nlev; L >= 2; --L) {
+    LevelBuf &f = p->lv[L], &c = p->lv[L - 1];
+    const int kind = L == p->nlev ? 7 : 27;
+    P27W<double> Pw;
+    for (int q = 0; q < 27; ++q)
+      Pw.p[q] = c.P[q];
+    if (trilinear) {
+      buildP_trilin_kernel<<<interior_grid(c.d), interior_block(), 0, s>>>(
+          c.d, Pw);
+      PMG_LAUNCH_CHECK();
+    } else if ((rc = launch_buildP(f.d, c.d, kind, f.A64(kind == 7 ? 4 : 14),
+                                   Pw, s))) {
+      return rc;
+    }
+    Op14W<double> out;
+    for (int q = 0; q < 14; ++q)
+      out.a[q] = c.op[q];
+    if ((rc = launch_buildG(f.d, c.d, kind, c.Pc(),
+                            f.A64(kind == 7 ? 4 : 14), out, s)))
+      return rc;
+  }
+  if (p->precision == PMG_PREC_MIXED) {
+    for (int L = 1; L <= p->nlev; ++L) {
+      LevelBuf &v = p->lv[L];
+      const unsigned g = flat_grid(v.n3);
+      for (int q = 0; q < 14; ++q)
+        if (v.op32[q])
+          convert_kernel<double, float><<<g, 256, 0, s>>>(v.n3, v.op[q],
+                                                         v.op32[q]);
+      for (int q = 0; q < 27; ++q)
+        if (v.P32[q])
+          convert_kernel<double, float><<<g, 256, 0, s>>>(v.n3, v.P[q],
+                                                         v.P32[q]);
+    }
+    PMG_LAUNCH_CHECK();
+  }
+  p->built = true;
+  return PMG_OK;
+}
+
+int pmg_vcycle(pmg_problem *p, int as_preconditioner) {
+  if (!p)
+    return PMG_ERR_ARG;
+  if (!p->built) {
+    set_last_message("pmg_vcycle: hierarchy not built");
+    return PMG_ERR_STATE;
+  }
+  if (p->precision != PMG_PREC_FP64) {
+    set_last_message("pmg_vcycle: FP64 problems only");
+    return PMG_ERR_ARG;
+  }
+  return vcycle64(p, p->nlev, as_preconditioner);
+}
+
+int pmg_compute_residual_2(pmg_problem *p, double *out) {
+  if (!p || !out)
+    return PMG_ERR_ARG;
+  if (!p->fine_set)
+    return PMG_ERR_STATE;
+  int rc = residual_norm_async(p);
+  if (rc)
+    return rc;
+  PMG_CUDA_TRY(cudaStreamSynchronize(p->stream));
+  *out = norm_from_sum(p, p->h_pinned[0]);
+  return PMG_OK;
+}
+
+int pmg_solve(pmg_problem *p, double tol, int max_cycles, int *cycles,
+              double *relres, double *hist) {
+  if (!p || max_cycles < 0)
+    return PMG_ERR_ARG;
+  if (!p->built) {
+    set_last_message("pmg_solve: hierarchy not built");
+    return PMG_ERR_STATE;
+  }
+  const bool mixed = p->precision == PMG_PREC_MIXED;
+  int rc = mixed ? mixed_residual_async(p) : residual_norm_async(p);
+  if (rc)
+    return rc;
+  PMG_CUDA_TRY(cudaStreamSynchronize(p->stream));
+  const double r0 = norm_from_sum(p, p->h_pinned[0]);
+  if (hist)
+    hist[0] = r0;
+  if (!isfinite(r0)) {
+    if (cycles)
+      *cycles = 0;
+    if (relres)
+      *relres = r0;
+    set_last_message("pmg_solve: initial residual is not finite");
+    return PMG_ERR_DIVERGED;
+  }
+  if ((rc = ensure_graph(p)))
+    return rc;
+  int c = 0;
+  double r = r0;
+  rc = PMG_OK;
+  while (c < max_cycles && r0 > 0.0) {
+    PMG_CUDA_TRY(cudaGraphLaunch(p->cycle_exec, p->stream));
+    PMG_CUDA_TRY(cudaStreamSynchronize(p->stream));
+    ++c;
+    r = norm_from_sum(p, p->h_pinned[0]);
+    if (hist)
+      hist[c] = r;
+    if (!isfinite(r) || r > 1e6 * r0) {
+      set_last_message("pmg_solve: residual diverged");
+      rc = PMG_ERR_DIVERGED;
+      break;
+    }
+    if (r / r0 < tol)
+      break;
+  }
+  if (cycles)
+    *cycles = c;
+  if (relres)
+    *relres = r0 > 0.0 ? r / r0 : 0.0;
+  return rc;
+}
+
+int pmg_get_potential(pmg_problem *p, double *dst) {
+  if (!p || !dst)
+    return PMG_ERR_ARG;
+  LevelBuf &v = p->lv[p->nlev];
+  PMG_CUDA_TRY(cudaMemcpyAsync(dst, v.x, sizeof(double) * v.n3,
+                               cudaMemcpyDefault, p->stream));
+  PMG_CUDA_TRY(cudaStreamSynchronize(p->stream));
+  return PMG_OK;
+}
+
+int pmg_get_level(pmg_problem *p, int level, double *dst) {
+  if (!p || !dst || level < 1 || level >= p->nlev)
+    return PMG_ERR_ARG;
+  LevelBuf &v = p->lv[level];
+  const size_t b = sizeof(double) * v.n3;
+  for (int q = 0; q < 27; ++q)
+    PMG_CUDA_TRY(cudaMemcpyAsync(dst + q * v.n3, v.P[q], b, cudaMemcpyDefault,
+                                 p->stream));
+  for (int q = 0; q < 14; ++q)
+    PMG_CUDA_TRY(cudaMemcpyAsync(dst + (27 + q) * v.n3, v.op[q], b,
+                                 cudaMemcpyDefault, p->stream));
+  PMG_CUDA_TRY(cudaStreamSynchronize(p->stream));
+  return PMG_OK;
+}
+
+} // extern "C"

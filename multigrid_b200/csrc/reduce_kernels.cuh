@@ -1,0 +1,155 @@
+// Reductions of the PMG path (defect norm, Hackbusch-Reusken damping) and
+// the single-CTA coarsest-level CG.
+//
+// Reductions are deterministic: a fixed grid of blocks accumulates per-thread
+// partials over a fixed grid-stride partition, each block writes its partial,
+// and the last block to finish (atomic ticket) sums the partials in block
+// order. The result therefore depends only on the problem, never on timing or
+// on other work sharing the GPU.
+#pragma once
+
+#include "stencil_kernels.cuh"
+
+namespace pmg {
+
+constexpr int kReduceBlocks = 296; // 2 per SM on 148 SMs
+constexpr int kReduceThreads = 256;
+
+// Device scratch of one reduction site: partials[kReduceBlocks * NV],
+// ticket counter (zero between uses), result[NV].
+struct ReduceSlot {
+  double *partials;
+  unsigned int *ticket;
+  double *result;
+};
+
+__device__ __forceinline__ void interior_coords(const Dims &d, int q, int &i,
+                                                int &j, int &k) {
+  const int mx = d.nx - 2, my = d.ny - 2;
+  const int r = q / mx;
+  i = q - r * mx + 2;
+  k = r / my;
+  j = r - k * my + 2;
+  k += 2;
+}
+
+// Finishes a reduction of NV values: called by every block after it has
+// computed its block sums v[] (valid in thread 0). The last block sums all
+// partials in block order and writes result[]; when ratio != nullptr it also
+// stores result[0] / result[1] there (NV == 2).
+template <int NV>
+__device__ void reduce_finish(const double (&v)[NV], ReduceSlot s,
+                              double *ratio) {
+  __shared__ bool last;
+  __shared__ double sh[32];
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int q = 0; q < NV; ++q)
+      s.partials[blockIdx.x * NV + q] = v[q];
+    __threadfence();
+    const unsigned t = atomicAdd(s.ticket, 1u);
+    last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!last)
+    return;
+  __threadfence();
+#pragma unroll
+  for (int q = 0; q < NV; ++q) {
+    double acc = 0.0;
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x)
+      acc += ((volatile double *)s.partials)[b * NV + q];
+    acc = block_sum(acc, sh);
+    if (threadIdx.x == 0)
+      s.result[q] = acc;
+  }
+  if (threadIdx.x == 0) {
+    if (ratio)
+      *ratio = s.result[0] / s.result[1];
+    *s.ticket = 0u;
+  }
+}
+
+// sum over the interior of (f - A x)^2 with the defect of the class
+// (f - map(x), Convolution.h:137-139 and 170-175); optionally stores the
+// defect (cast to Tout) into r. Accumulates in double.
+template <int KIND, typename T, typename Tout>
+__global__ void __launch_bounds__(kReduceThreads)
+    defect_norm_kernel(Dims d, Op14<T> A, const T *__restrict__ f,
+                       const T *__restrict__ x, Tout *__restrict__ r,
+                       ReduceSlot s) {
+  __shared__ double sh[32];
+  const int m = (d.nx - 2) * (d.ny - 2) * (d.nz - 2);
+  const int sy = d.sy(), sz = d.sz();
+  double acc = 0.0;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < m;
+       q += gridDim.x * blockDim.x) {
+    int i, j, k;
+    interior_coords(d, q, i, j, k);
+    const int p = d.at(i, j, k);
+    const T dv = f[p] - apply_op<KIND>(A, (const T *)nullptr, x, p, sy, sz);
+    if (r)
+      r[p] = (Tout)dv;
+    acc += (double)dv * (double)dv;
+  }
+  double v[1] = {block_sum(acc, sh)};
+  reduce_finish<1>(v, s, nullptr);
+}
+
+// Defect only (no reduction): r = f - map(x) on the interior
+// (Subtract_Convolve_map, Convolution.h:123-146).
+template <int KIND, typename T>
+__global__ void __launch_bounds__(256)
+    defect_kernel(Dims d, Op14<T> A, const T *__restrict__ f,
+                  const T *__restrict__ x, T *__restrict__ r) {
+  const Interior t = interior_point(d);
+  if (!t.ok)
+    return;
+  const int p = d.at(t.i, t.j, t.k);
+  r[p] = f[p] - apply_op<KIND>(A, (const T *)nullptr, x, p, d.sy(), d.sz());
+}
+
+// Hackbusch-Reusken damping w = (r . x) / (x . A x) over the interior of a
+// 27-point level (get_ideal_lambda, MultigridDomain.h:327-352), accumulated
+// in double; the last block stores w.
+template <typename T>
+__global__ void __launch_bounds__(kReduceThreads)
+    ideal_lambda_kernel(Dims d, Op14<T> A, const T *__restrict__ x,
+                        const T *__restrict__ r, ReduceSlot s,
+                        double *__restrict__ w) {
+  __shared__ double sh[32];
+  const int m = (d.nx - 2) * (d.ny - 2) * (d.nz - 2);
+  const int sy = d.sy(), sz = d.sz();
+  double up = 0.0, lo = 0.0;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < m;
+       q += gridDim.x * blockDim.x) {
+    int i, j, k;
+    interior_coords(d, q, i, j, k);
+    const int p = d.at(i, j, k);
+    up += (double)r[p] * (double)x[p];
+    lo += (double)x[p] *
+          (double)apply27(A, (const T *)nullptr, x, p, sy, sz);
+  }
+  double v[2];
+  v[0] = block_sum(up, sh);
+  v[1] = block_sum(lo, sh);
+  reduce_finish<2>(v, s, w);
+}
+
+// Coarsest-level CG of the class, one CTA (CG_solver, CG_Solver.h:45-242 via
+// solve_by_cg<1>, PBE_pmgc_class.h:856-860):
+//   r = rhs - A x; p = r; rs = r.r; pAp = (A p).p; stop if pAp == 0;
+//   alpha = rs/pAp; res = sqrt(sqrt(rs));
+//   while res > thresh: x += alpha p; r -= alpha A p; rs' = r.r;
+//     beta = rs'/rs (0 if rs == 0); p = r + beta p; pAp = (A p).p;
+//     alpha = rs/pAp (0 if pAp == 0); res = sqrt(rs)
+// bounded by max_iters (the reference loops without a cap). r and p are
+// scratch arrays whose shells are zero. status[0] = iterations,
+// status[1] = 1 when the cap stopped the loop above the threshold.
+__global__ void __launch_bounds__(1024)
+    cg_level_kernel(Dims d, Op14<double> A, const double *__restrict__ rhs,
+                    double *__restrict__ x, double *__restrict__ r,
+                    double *__restrict__ p, double thresh, int max_iters,
+                    int *__restrict__ status);
+
+} // namespace pmg

@@ -1,0 +1,286 @@
+// Stencil kernels of the PMG V-cycle: Gauss-Seidel smoothers, matvec,
+// residual and defect, restriction, interpolation, axpy.
+//
+// Every kernel evaluates the per-point arithmetic in the reference's operation
+// order (products and sums rounded separately: the library is built with
+// --fmad=false), so a double-precision launch reproduces the reference kernel
+// bit for bit on the same inputs. Cited per kernel.
+#pragma once
+
+#include "pmg_common.cuh"
+
+namespace pmg {
+
+// ---------------------------------------------------------------------------
+// Per-point operators
+// ---------------------------------------------------------------------------
+
+// Positive neighbour sums of the 27-point operator in the reference order:
+// tmpO (8 in-plane), tmpU (9 above), tmpD (9 below), pmgc/gsd.cc:171-204.
+template <typename T>
+__device__ __forceinline__ void sums27(const Op14<T> &A, const T *x, int p,
+                                       int sy, int sz, T &tO, T &tU, T &tD) {
+  const T *const *a = A.a;
+  tO = a[kON][p] * x[p + sy] + a[kON][p - sy] * x[p - sy] +
+       a[kOE][p] * x[p + 1] + a[kOE][p - 1] * x[p - 1] +
+       a[kONE][p] * x[p + 1 + sy] + a[kONW][p] * x[p - 1 + sy] +
+       a[kONW][p + 1 - sy] * x[p + 1 - sy] +
+       a[kONE][p - 1 - sy] * x[p - 1 - sy];
+  tU = a[kUC][p] * x[p + sz] + a[kUN][p] * x[p + sy + sz] +
+       a[kUS][p] * x[p - sy + sz] + a[kUE][p] * x[p + 1 + sz] +
+       a[kUW][p] * x[p - 1 + sz] + a[kUNE][p] * x[p + 1 + sy + sz] +
+       a[kUNW][p] * x[p - 1 + sy + sz] + a[kUSE][p] * x[p + 1 - sy + sz] +
+       a[kUSW][p] * x[p - 1 - sy + sz];
+  tD = a[kUC][p - sz] * x[p - sz] + a[kUS][p + sy - sz] * x[p + sy - sz] +
+       a[kUN][p - sy - sz] * x[p - sy - sz] +
+       a[kUW][p + 1 - sz] * x[p + 1 - sz] +
+       a[kUE][p - 1 - sz] * x[p - 1 - sz] +
+       a[kUSW][p + 1 + sy - sz] * x[p + 1 + sy - sz] +
+       a[kUSE][p - 1 + sy - sz] * x[p - 1 + sy - sz] +
+       a[kUNW][p + 1 - sy - sz] * x[p + 1 - sy - sz] +
+       a[kUNE][p - 1 - sy - sz] * x[p - 1 - sy - sz];
+}
+
+// (A x)(p) as matveckernel7 / Vmatvec7_1s compute it
+// (pmgc/matvecd.h:131-137, pmgc/matvecd.cc:81-88); cc may be null (= 0).
+template <typename T>
+__device__ __forceinline__ T apply7(const Op14<T> &A, const T *cc, const T *x,
+                                    int p, int sy, int sz) {
+  const T *oC = A.a[kOC], *oE = A.a[kOE], *oN = A.a[kON], *uC = A.a[kUC];
+  const T c = cc ? cc[p] : T(0);
+  return -oN[p] * x[p + sy] - oN[p - sy] * x[p - sy] - oE[p] * x[p + 1] -
+         oE[p - 1] * x[p - 1] - uC[p - sz] * x[p - sz] - uC[p] * x[p + sz] +
+         (oC[p] + c) * x[p];
+}
+
+// (A x)(p) as matveckernel27 / Vmatvec27_1s compute it
+// (pmgc/matvecd.h:208-239, pmgc/matvecd.cc:142-174): the reference subtracts
+// each product from a negated running sum, which rounds exactly like the
+// negated positive sum.
+template <typename T>
+__device__ __forceinline__ T apply27(const Op14<T> &A, const T *cc,
+                                     const T *x, int p, int sy, int sz) {
+  T tO, tU, tD;
+  sums27(A, x, p, sy, sz, tO, tU, tD);
+  const T c = cc ? cc[p] : T(0);
+  return (-tO) + (-tU) + (-tD) + (A.a[kOC][p] + c) * x[p];
+}
+
+template <int KIND, typename T>
+__device__ __forceinline__ T apply_op(const Op14<T> &A, const T *cc,
+                                      const T *x, int p, int sy, int sz) {
+  if constexpr (KIND == 7)
+    return apply7(A, cc, x, p, sy, sz);
+  else
+    return apply27(A, cc, x, p, sy, sz);
+}
+
+// ---------------------------------------------------------------------------
+// Gauss-Seidel colour sweeps
+// ---------------------------------------------------------------------------
+
+// One colour of the red-black sweep on the 7-point operator (Vgsrb7x,
+// pmgc/gsd.cc:85-107): updates the interior points with (i+j+k)%2 == want;
+// keep = 0 drops the neighbour sum (zero_initialize). One thread per point of
+// the colour; blockIdx.z is the plane.
+template <typename T>
+__global__ void __launch_bounds__(256)
+    gs7_color_kernel(Dims d, const T *__restrict__ oC, const T *__restrict__ cc,
+                     const T *__restrict__ fc, const T *__restrict__ oE,
+                     const T *__restrict__ oN, const T *__restrict__ uC, T *x,
+                     int want, T keep) {
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
+  const int k = blockIdx.z + 2;
+  if (j > d.ny - 1)
+    return;
+  const int i = 2 + ((2 + j + k + want) & 1) +
+                2 * (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (i > d.nx - 1)
+    return;
+  const int sy = d.sy(), sz = d.sz();
+  const int p = d.at(i, j, k);
+  const T s = oN[p] * x[p + sy] + oN[p - sy] * x[p - sy] + oE[p] * x[p + 1] +
+              oE[p - 1] * x[p - 1] + uC[p - sz] * x[p - sz] +
+              uC[p] * x[p + sz];
+  const T c = cc ? cc[p] : T(0);
+  x[p] = (fc[p] + keep * s) / (oC[p] + c);
+}
+
+// One colour of the eight-colour sweep on the 27-point operator (Vgsrb27x,
+// pmgc/gsd.cc:161-209): updates the interior points whose index parities are
+// (want&1, want>>1&1, want>>2&1).
+template <typename T>
+__global__ void __launch_bounds__(256)
+    gs27_color_kernel(Dims d, Op14<T> A, const T *__restrict__ cc,
+                      const T *__restrict__ fc, T *x, int want) {
+  const int i = 2 + (want & 1) +
+                2 * (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  const int j = 2 + ((want >> 1) & 1) +
+                2 * (int)(blockIdx.y * blockDim.y + threadIdx.y);
+  const int k = 2 + ((want >> 2) & 1) + 2 * (int)blockIdx.z;
+  if (i > d.nx - 1 || j > d.ny - 1 || k > d.nz - 1)
+    return;
+  const int sy = d.sy(), sz = d.sz();
+  const int p = d.at(i, j, k);
+  T tO, tU, tD;
+  sums27(A, x, p, sy, sz, tO, tU, tD);
+  const T c = cc ? cc[p] : T(0);
+  x[p] = (fc[p] + (tO + tU + tD)) / (A.a[kOC][p] + c);
+}
+
+// ---------------------------------------------------------------------------
+// matvec / residual / defect
+// ---------------------------------------------------------------------------
+
+// Interior launch helper: blockIdx.z is the plane, (x, y) cover the row.
+struct Interior {
+  int i, j, k;
+  bool ok;
+};
+__device__ __forceinline__ Interior interior_point(const Dims &d) {
+  Interior t;
+  t.i = blockIdx.x * blockDim.x + threadIdx.x + 2;
+  t.j = blockIdx.y * blockDim.y + threadIdx.y + 2;
+  t.k = blockIdx.z + 2;
+  t.ok = t.i <= d.nx - 1 && t.j <= d.ny - 1;
+  return t;
+}
+
+// y = A x (Vmatvec7_1s / Vmatvec27_1s).
+template <int KIND, typename T>
+__global__ void __launch_bounds__(256)
+    matvec_kernel(Dims d, Op14<T> A, const T *__restrict__ cc,
+                  const T *__restrict__ x, T *__restrict__ y) {
+  const Interior t = interior_point(d);
+  if (!t.ok)
+    return;
+  const int p = d.at(t.i, t.j, t.k);
+  y[p] = apply_op<KIND>(A, cc, x, p, d.sy(), d.sz());
+}
+
+// r = f - A x in the order of Vmresid7_1s / Vmresid27_1s
+// (pmgc/matvecd.cc:402-409, 491-493).
+template <int KIND, typename T>
+__global__ void __launch_bounds__(256)
+    mresid_kernel(Dims d, Op14<T> A, const T *__restrict__ cc,
+                  const T *__restrict__ fc, const T *__restrict__ x,
+                  T *__restrict__ r) {
+  const Interior t = interior_point(d);
+  if (!t.ok)
+    return;
+  const int sy = d.sy(), sz = d.sz();
+  const int p = d.at(t.i, t.j, t.k);
+  const T c = cc ? cc[p] : T(0);
+  if constexpr (KIND == 7) {
+    const T *oC = A.a[kOC], *oE = A.a[kOE], *oN = A.a[kON], *uC = A.a[kUC];
+    r[p] = fc[p] + oN[p] * x[p + sy] + oN[p - sy] * x[p - sy] +
+           oE[p] * x[p + 1] + oE[p - 1] * x[p - 1] + uC[p - sz] * x[p - sz] +
+           uC[p] * x[p + sz] - (oC[p] + c) * x[p];
+  } else {
+    T tO, tU, tD;
+    sums27(A, x, p, sy, sz, tO, tU, tD);
+    r[p] = fc[p] + tO + tU + tD - (A.a[kOC][p] + c) * x[p];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Grid transfers
+// ---------------------------------------------------------------------------
+
+// Restriction xout = P^T xin on the coarse interior (Vrestrc2,
+// pmgc/matvecd.cc:755-794): plane sums over C N S E W NE NW SE SW at the
+// fine planes kk, kk+1, kk-1, then tmpO + tmpU + tmpD.
+template <typename Tin, typename Tout>
+__global__ void __launch_bounds__(256)
+    restrict_kernel(Dims df, Dims dc, const Tin *__restrict__ xin,
+                    Tout *__restrict__ xout, P27<Tin> P) {
+  const Interior t = interior_point(dc);
+  if (!t.ok)
+    return;
+  const int pc = dc.at(t.i, t.j, t.k);
+  const int sy = df.sy(), sz = df.sz();
+  const int f0 = df.at(2 * t.i - 1, 2 * t.j - 1, 2 * t.k - 1);
+  Tin pl[3];
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    const int b = q * 9;
+    const int f = f0 + (q == 0 ? 0 : q == 1 ? sz : -sz);
+    pl[q] = P.p[b + 0][pc] * xin[f] + P.p[b + 1][pc] * xin[f + sy] +
+            P.p[b + 2][pc] * xin[f - sy] + P.p[b + 3][pc] * xin[f + 1] +
+            P.p[b + 4][pc] * xin[f - 1] + P.p[b + 5][pc] * xin[f + 1 + sy] +
+            P.p[b + 6][pc] * xin[f - 1 + sy] +
+            P.p[b + 7][pc] * xin[f + 1 - sy] +
+            P.p[b + 8][pc] * xin[f - 1 - sy];
+  }
+  xout[pc] = (Tout)(pl[0] + pl[1] + pl[2]);
+}
+
+// Interpolation xout = P xin (VinterpPMG2, pmgc/matvecd.cc:878-960): one
+// thread per coarse cell (ii,jj,kk) in [1, n_c-1]^3 writing its eight fine
+// points.
+template <typename T>
+__global__ void __launch_bounds__(256)
+    interp_kernel(Dims dc, Dims df, const T *__restrict__ xin,
+                  T *__restrict__ xout, P27<T> P) {
+  const int ii = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int jj = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int kk = blockIdx.z + 1;
+  if (ii > dc.nx - 1 || jj > dc.ny - 1)
+    return;
+  const int cy = dc.sy(), cz = dc.sz();
+  const int fy = df.sy(), fz = df.sz();
+  const int c = dc.at(ii, jj, kk);
+  const int f = df.at(2 * ii - 1, 2 * jj - 1, 2 * kk - 1);
+  const T *const *p = P.p;
+  // P slots: oPC 0 oPN 1 oPS 2 oPE 3 oPW 4 oPNE 5 oPNW 6 oPSE 7 oPSW 8,
+  // u* +9, d* +18.
+  const T x000 = xin[c], x100 = xin[c + 1], x010 = xin[c + cy],
+          x001 = xin[c + cz], x110 = xin[c + 1 + cy], x101 = xin[c + 1 + cz],
+          x011 = xin[c + cy + cz], x111 = xin[c + 1 + cy + cz];
+  xout[f] = x000;
+  xout[f + 1] = p[3][c] * x000 + p[4][c + 1] * x100;
+  xout[f + fy] = p[1][c] * x000 + p[2][c + cy] * x010;
+  xout[f + fz] = p[9][c] * x000 + p[18][c + cz] * x001;
+  xout[f + 1 + fy] = p[5][c] * x000 + p[6][c + 1] * x100 +
+                     p[7][c + cy] * x010 + p[8][c + 1 + cy] * x110;
+  xout[f + 1 + fz] = p[12][c] * x000 + p[13][c + 1] * x100 +
+                     p[21][c + cz] * x001 + p[22][c + 1 + cz] * x101;
+  xout[f + fy + fz] = p[10][c] * x000 + p[11][c + cy] * x010 +
+                      p[19][c + cz] * x001 + p[20][c + cy + cz] * x011;
+  xout[f + 1 + fy + fz] =
+      p[14][c] * x000 + p[15][c + 1] * x100 + p[16][c + cy] * x010 +
+      p[17][c + 1 + cy] * x110 + p[23][c + cz] * x001 +
+      p[24][c + 1 + cz] * x101 + p[25][c + cy + cz] * x011 +
+      p[26][c + 1 + cy + cz] * x111;
+}
+
+// ---------------------------------------------------------------------------
+// Elementwise
+// ---------------------------------------------------------------------------
+
+// x = x + w * e over all n entries, w read from device memory
+// (add_and_multiply_domains, Domain.h:602-623).
+template <typename T>
+__global__ void axpy_full_kernel(long n, T *__restrict__ x,
+                                 const T *__restrict__ e,
+                                 const double *__restrict__ w) {
+  const T ww = (T)(*w);
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n;
+       q += (long)gridDim.x * blockDim.x)
+    x[q] = x[q] + ww * e[q];
+}
+
+// dst = (Tout)src over n entries.
+template <typename Tin, typename Tout>
+__global__ void convert_kernel(long n, const Tin *__restrict__ src,
+                               Tout *__restrict__ dst) {
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n;
+       q += (long)gridDim.x * blockDim.x)
+    dst[q] = (Tout)src[q];
+}
+
+// x64 += (double)e32 on the interior (mixed-precision refinement update).
+__global__ void add_correction_kernel(Dims d, double *__restrict__ x,
+                                      const float *__restrict__ e);
+
+} // namespace pmg

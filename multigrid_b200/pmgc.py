@@ -1,0 +1,142 @@
+"""The pmgc kernels under the reference's names, on torch CUDA tensors.
+
+Each function calls the matching C-ABI entry point of libpmg_b200.so with the
+tensors' device pointers and the current torch stream (or `stream`), in the
+reference's argument order minus the unused APBS arguments (ipc, rpc) and
+with the sycl::queue replaced by a stream. Arrays are flat, n^3 long, with
+the reference's layout (x fastest, one-point shell). cc may be None (zero).
+
+  Vgsrb7x        pmgc/gsd.cc:60-111        Vgsrb27x     pmgc/gsd.cc:113-212
+  Vmatvec7_1s    pmgc/matvecd.cc:61-90     Vmatvec27_1s pmgc/matvecd.cc:103-176
+  Vmresid7_1s    pmgc/matvecd.cc:381-411   Vmresid27_1s pmgc/matvecd.cc:425-495
+  Vrestrc2       pmgc/matvecd.cc:695-799   VinterpPMG2  pmgc/matvecd.cc:819-964
+  VbuildPb_op7   pmgc/buildPd.cc:172-555   VbuildPb_op27 pmgc/buildPd.cc:578-1091
+  VbuildPb_trilin pmgc/buildPd.cc:62-153   VbuildG_7    pmgc/buildGd.cc:437-1361
+  VbuildG_27     pmgc/buildGd.cc:1363-3274
+  cg_level       CG_Solver.h:45-242 as run by PBE_pmgc_class.h:856-860
+"""
+from __future__ import annotations
+
+import ctypes
+
+import torch
+
+from . import _lib
+
+OP14 = ("oC", "oE", "oN", "uC", "oNE", "oNW", "uE", "uW", "uN", "uS", "uNE",
+        "uNW", "uSE", "uSW")
+P27 = ("oPC", "oPN", "oPS", "oPE", "oPW", "oPNE", "oPNW", "oPSE", "oPSW",
+       "uPC", "uPN", "uPS", "uPE", "uPW", "uPNE", "uPNW", "uPSE", "uPSW",
+       "dPC", "dPN", "dPS", "dPE", "dPW", "dPNE", "dPNW", "dPSE", "dPSW")
+
+
+def _p(t):
+    if t is None:
+        return None
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise TypeError("pmgc kernels take CUDA tensors")
+    if not t.is_contiguous():
+        raise ValueError("pmgc kernels take contiguous tensors")
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _s(stream):
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return ctypes.c_void_p(getattr(stream, "cuda_stream", stream))
+
+
+def _sfx(t):
+    if t.dtype == torch.float64:
+        return "_d"
+    if t.dtype == torch.float32:
+        return "_f"
+    raise TypeError("float32 or float64 tensors only")
+
+
+def _pp(ts):
+    return (ctypes.c_void_p * len(ts))(*[t.data_ptr() for t in ts])
+
+
+def Vgsrb7x(nx, ny, nz, oC, cc, fc, oE, oN, uC, x, itmax, iadjoint=0,
+            zero_init=False, stream=None):
+    _lib.call("pmg_Vgsrb7x" + _sfx(x), nx, ny, nz, _p(oC), _p(cc), _p(fc),
+              _p(oE), _p(oN), _p(uC), _p(x), int(itmax), int(iadjoint),
+              int(zero_init), _s(stream))
+
+
+def Vgsrb27x(nx, ny, nz, op14, cc, fc, x, itmax, zero_init=False, iadjoint=0,
+             stream=None):
+    """op14: the 14 diagonals oC..uSW (a sequence of tensors)."""
+    a = [_p(t) for t in op14]
+    _lib.call("pmg_Vgsrb27x" + _sfx(x), nx, ny, nz, a[0], _p(cc), _p(fc),
+              *a[1:], _p(x), int(itmax), int(zero_init), int(iadjoint),
+              _s(stream))
+
+
+def Vmatvec7_1s(nx, ny, nz, oC, cc, oE, oN, uC, x, y, stream=None):
+    _lib.call("pmg_Vmatvec7_1s_d", nx, ny, nz, _p(oC), _p(cc), _p(oE),
+              _p(oN), _p(uC), _p(x), _p(y), _s(stream))
+
+
+def Vmatvec27_1s(nx, ny, nz, op14, cc, x, y, stream=None):
+    a = [_p(t) for t in op14]
+    _lib.call("pmg_Vmatvec27_1s_d", nx, ny, nz, a[0], _p(cc), *a[1:], _p(x),
+              _p(y), _s(stream))
+
+
+def Vmresid7_1s(nx, ny, nz, oC, cc, fc, oE, oN, uC, x, r, stream=None):
+    _lib.call("pmg_Vmresid7_1s_d", nx, ny, nz, _p(oC), _p(cc), _p(fc),
+              _p(oE), _p(oN), _p(uC), _p(x), _p(r), _s(stream))
+
+
+def Vmresid27_1s(nx, ny, nz, op14, cc, fc, x, r, stream=None):
+    a = [_p(t) for t in op14]
+    _lib.call("pmg_Vmresid27_1s_d", nx, ny, nz, a[0], _p(cc), _p(fc),
+              *a[1:], _p(x), _p(r), _s(stream))
+
+
+def Vrestrc2(nxf, nyf, nzf, nxc, nyc, nzc, xin, xout, p27, stream=None):
+    _lib.call("pmg_Vrestrc2_d", nxf, nyf, nzf, nxc, nyc, nzc, _p(xin),
+              _p(xout), *[_p(t) for t in p27], _s(stream))
+
+
+def VinterpPMG2(nxc, nyc, nzc, nxf, nyf, nzf, xin, xout, p27, stream=None):
+    _lib.call("pmg_VinterpPMG2_d", nxc, nyc, nzc, nxf, nyf, nzf, _p(xin),
+              _p(xout), *[_p(t) for t in p27], _s(stream))
+
+
+def VbuildPb_op7(nxf, nyf, nzf, nxc, nyc, nzc, oC, oE, oN, uC, p27,
+                 stream=None):
+    _lib.call("pmg_VbuildPb_op7_d", nxf, nyf, nzf, nxc, nyc, nzc, _p(oC),
+              _p(oE), _p(oN), _p(uC), *[_p(t) for t in p27], _s(stream))
+
+
+def VbuildPb_op27(nxf, nyf, nzf, nxc, nyc, nzc, op14, p27, stream=None):
+    _lib.call("pmg_VbuildPb_op27_d", nxf, nyf, nzf, nxc, nyc, nzc,
+              *[_p(t) for t in op14], *[_p(t) for t in p27], _s(stream))
+
+
+def VbuildPb_trilin(nxf, nyf, nzf, nxc, nyc, nzc, p27, stream=None):
+    _lib.call("pmg_VbuildPb_trilin_d", nxf, nyf, nzf, nxc, nyc, nzc,
+              *[_p(t) for t in p27], _s(stream))
+
+
+def VbuildG_7(nxf, nyf, nzf, nxc, nyc, nzc, p27, oC, oE, oN, uC, out14,
+              stream=None):
+    _lib.call("pmg_VbuildG_7_d", nxf, nyf, nzf, nxc, nyc, nzc, _pp(p27),
+              _p(oC), _p(oE), _p(oN), _p(uC), _pp(out14), _s(stream))
+
+
+def VbuildG_27(nxf, nyf, nzf, nxc, nyc, nzc, p27, op14, out14, stream=None):
+    _lib.call("pmg_VbuildG_27_d", nxf, nyf, nzf, nxc, nyc, nzc, _pp(p27),
+              _pp(op14), _pp(out14), _s(stream))
+
+
+def cg_level(nx, ny, nz, op14, rhs, x, thresh=1e-8, max_iters=20000,
+             stream=None) -> int:
+    """Coarsest-level CG of the class; returns the iteration count."""
+    it = ctypes.c_int()
+    _lib.call("pmg_cg_level_d", nx, ny, nz, _pp(op14), _p(rhs), _p(x),
+              float(thresh), int(max_iters), ctypes.byref(it), _s(stream))
+    return it.value

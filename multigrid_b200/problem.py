@@ -1,0 +1,209 @@
+"""Host mirror of the reference's PBE_linear_problem (PBE_pmgc_class.h:112-1174).
+
+The reference fixes its grid at compile time as template parameters
+<base_length, nlev, box_length>; here they are constructor arguments. The
+method names follow the class: initialize_boundary / initialize_epsilons /
+set_up_rhs (set-up from atoms), buildmultilevelops, v_cycle,
+compute_residual_2, plus solve(), which runs the V-cycle loop the reference's
+drivers write by hand (PBE_pmgc_class_test.cc:150-162). All work happens in
+libpmg_b200.so on the current CUDA device.
+"""
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+
+import numpy as np
+
+from . import _lib
+from .molecule import REFERENCE_PHYSICS, grid_step, level_n
+
+
+def physics_struct(physics: dict) -> _lib.PmgPhysics:
+    return _lib.PmgPhysics(**{k: float(physics[k]) for k in (
+        "eps_in", "eps_out", "ionic_strength", "ion_radius", "temperature",
+        "probe_radius")})
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(_lib.PD)
+
+
+def setup_fine(n: int, h: float, atoms: np.ndarray, physics: dict) -> dict:
+    """Fine-level arrays (oC, oE, oN, uC, f, x0; n^3 doubles each, x fastest)
+    from atoms (rows x, y, z, radius, charge in the grid frame)."""
+    atoms = np.ascontiguousarray(atoms, dtype=np.float64)
+    out = {k: np.empty(n ** 3) for k in ("oC", "oE", "oN", "uC", "f", "x0")}
+    ph = physics_struct(physics)
+    _lib.check("pmg_setup_fine", _lib.lib.pmg_setup_fine(
+        n, h, _dptr(atoms), int(atoms.shape[0]), ctypes.byref(ph),
+        *[_dptr(out[k]) for k in ("oC", "oE", "oN", "uC", "f", "x0")]))
+    return out
+
+
+def kappa(physics: dict) -> tuple[float, float]:
+    """(kappa [1/A], eps0 [reduced units]) of the physics."""
+    k = ctypes.c_double()
+    e = ctypes.c_double()
+    ph = physics_struct(physics)
+    _lib.check("pmg_kappa", _lib.lib.pmg_kappa(ctypes.byref(ph),
+                                               ctypes.byref(k),
+                                               ctypes.byref(e)))
+    return k.value, e.value
+
+
+@dataclasses.dataclass
+class SolveResult:
+    cycles: int
+    relres: float
+    history: np.ndarray  # residual norm before and after each cycle
+
+
+PRECISIONS = {"fp64": _lib.PREC_FP64, "mixed": _lib.PREC_MIXED}
+
+
+class PBELinearProblem:
+    """PBE_linear_problem<base, nlev, box> with runtime sizes.
+
+    precision: "fp64" (the reference's arithmetic) or "mixed" (float
+    V-cycles inside double iterative refinement; double residual, norms and
+    coarsest CG).
+    """
+
+    def __init__(self, base: int, nlev: int, box: float,
+                 precision: str = "fp64", physics: dict | None = None,
+                 stream: int | None = None):
+        self.base, self.nlev, self.box = int(base), int(nlev), float(box)
+        self.n = level_n(self.base, self.nlev)
+        self.grid_step = grid_step(self.base, self.nlev, self.box)
+        self.precision = precision
+        self.physics = dict(physics or REFERENCE_PHYSICS)
+        self._atoms = None
+        self._fine = None
+        h = ctypes.c_void_p()
+        _lib.check("pmg_problem_create", _lib.lib.pmg_problem_create(
+            self.base, self.nlev, self.box, PRECISIONS[precision],
+            ctypes.c_void_p(stream or 0), ctypes.byref(h)))
+        self._h = h
+
+    # -- lifetime ----------------------------------------------------------
+    def close(self) -> None:
+        if self._h:
+            _lib.lib.pmg_problem_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @staticmethod
+    def device_bytes(base: int, nlev: int, precision: str = "fp64") -> int:
+        return int(_lib.lib.pmg_problem_bytes(base, nlev,
+                                              PRECISIONS[precision]))
+
+    @property
+    def stream(self) -> int:
+        return int(_lib.lib.pmg_problem_stream(self._h) or 0)
+
+    # -- set-up (PBE_pmgc_class.h:191-349) ----------------------------------
+    def _setup_from_atoms(self, atoms) -> None:
+        atoms = np.ascontiguousarray(atoms, dtype=np.float64)
+        if self._atoms is None or not np.array_equal(self._atoms, atoms):
+            self._atoms = atoms
+            self._fine = setup_fine(self.n, self.grid_step, atoms,
+                                    self.physics)
+            self.set_fine(**self._fine)
+
+    def initialize_boundary(self, atoms) -> None:
+        """Debye-Hueckel boundary values on the finest shell."""
+        self._setup_from_atoms(atoms)
+
+    def initialize_epsilons(self, atoms) -> None:
+        """Dielectric, kappa and centre coefficients of the finest level."""
+        self._setup_from_atoms(atoms)
+
+    def set_up_rhs(self, atoms) -> None:
+        """Trilinear charge distribution on the finest level."""
+        self._setup_from_atoms(atoms)
+
+    def set_fine(self, oC, oE, oN, uC, f, x0) -> None:
+        """Loads the finest level from host (numpy) or device (torch)
+        arrays of n^3 doubles."""
+        keep = []
+
+        def ptr(a):
+            if hasattr(a, "data_ptr"):
+                assert a.dtype.is_floating_point and a.element_size() == 8
+                assert a.numel() == self.n ** 3 and a.is_contiguous()
+                return ctypes.c_void_p(a.data_ptr())
+            a = np.ascontiguousarray(a, dtype=np.float64).reshape(-1)
+            assert a.size == self.n ** 3
+            keep.append(a)
+            return ctypes.c_void_p(a.ctypes.data)
+
+        ptrs = [ptr(a) for a in (oC, oE, oN, uC, f, x0)]
+        _lib.check("pmg_problem_set_fine",
+                   _lib.lib.pmg_problem_set_fine(self._h, *ptrs))
+        # pmg_problem_set_fine is stream-ordered; host buffers must live
+        # until the copies finish.
+        self.synchronize()
+        del keep
+
+    def synchronize(self) -> None:
+        import torch  # noqa: F401  (CUDA context of the process)
+        torch.cuda.current_stream()  # make sure CUDA is initialised
+        torch.cuda.ExternalStream(self.stream).synchronize()
+
+    # -- multigrid ------------------------------------------------------------
+    def buildmultilevelops(self, trilinear: bool = False) -> None:
+        """Galerkin hierarchy (PBE_pmgc_class.h:351-617)."""
+        _lib.check("pmg_build_hierarchy",
+                   _lib.lib.pmg_build_hierarchy(self._h, int(trilinear)))
+
+    def v_cycle(self, as_preconditioner: bool = False) -> None:
+        """One V-cycle (PBE_pmgc_class.h:1070-1114); fp64 problems."""
+        _lib.check("pmg_vcycle",
+                   _lib.lib.pmg_vcycle(self._h, int(as_preconditioner)))
+
+    def compute_residual_2(self) -> float:
+        """sqrt(sum (f - A x)^2 / n^3) on the finest level."""
+        out = ctypes.c_double()
+        _lib.check("pmg_compute_residual_2",
+                   _lib.lib.pmg_compute_residual_2(self._h, ctypes.byref(out)))
+        return out.value
+
+    def solve(self, tol: float = 1e-10, max_cycles: int = 100) -> SolveResult:
+        """V-cycles (fp64) or refinement steps (mixed) until
+        compute_residual_2() / r0 < tol."""
+        hist = np.zeros(max_cycles + 1)
+        cycles = ctypes.c_int()
+        rel = ctypes.c_double()
+        _lib.check("pmg_solve", _lib.lib.pmg_solve(
+            self._h, tol, max_cycles, ctypes.byref(cycles), ctypes.byref(rel),
+            _dptr(hist)))
+        return SolveResult(cycles.value, rel.value, hist[:cycles.value + 1])
+
+    # -- results ----------------------------------------------------------------
+    def potential(self) -> np.ndarray:
+        """Finest iterate, shape (n, n, n) indexed [k, j, i] (x fastest)."""
+        out = np.empty(self.n ** 3)
+        _lib.check("pmg_get_potential", _lib.lib.pmg_get_potential(
+            self._h, ctypes.c_void_p(out.ctypes.data)))
+        return out.reshape(self.n, self.n, self.n)
+
+    def get_level(self, level: int) -> tuple[np.ndarray, np.ndarray]:
+        """(P (27, n_L^3), A (14, n_L^3)) of coarse level L in [1, nlev-1]."""
+        nl = level_n(self.base, level) ** 3
+        out = np.empty(41 * nl)
+        _lib.check("pmg_get_level", _lib.lib.pmg_get_level(
+            self._h, level, ctypes.c_void_p(out.ctypes.data)))
+        out = out.reshape(41, nl)
+        return out[:27], out[27:]

@@ -1,0 +1,151 @@
+"""Generates the golden fixtures of tests/golden/ from the reference itself.
+
+Runs the reference's own PBE_pmgc_class.h and pmgc kernels, compiled against
+the host SYCL shim (oracle/_ref/libpmgc_ref.so, built by `make -C oracle`
+from the reference tree), on small seeded inputs and stores inputs and
+outputs as compressed .npz files. The reference tree is only needed to
+regenerate them:
+
+    make -C oracle -j8 && python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(
+    os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+from oracle.oracle import Reference  # noqa: E402
+from multigrid_b200.molecule import synthetic_atoms  # noqa: E402
+
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+
+def random_op27(rng, n):
+    """Diagonally dominant symmetric 27-point operator (14 diagonals)."""
+    a = [rng.uniform(0.5, 2.0, n ** 3) for _ in range(14)]
+    a[0] = rng.uniform(28.0, 40.0, n ** 3)
+    return a
+
+
+def kernels(ref: Reference) -> None:
+    L = ref.lib
+    import ctypes
+    D = ctypes.POINTER(ctypes.c_double)
+
+    def d(a):
+        return a.ctypes.data_as(D)
+
+    def pp(arrs):
+        return (D * len(arrs))(*[d(a) for a in arrs])
+
+    rng = np.random.default_rng(20261203)
+    nf, nc = 9, 5
+    op27 = random_op27(rng, nf)
+    op7 = [rng.uniform(20.0, 30.0, nf ** 3)] + [
+        rng.uniform(0.5, 2.0, nf ** 3) for _ in range(3)]
+    cc = rng.uniform(0.0, 0.5, nf ** 3)
+    f = rng.normal(0.0, 1.0, nf ** 3)
+    x0 = rng.normal(0.0, 1.0, nf ** 3)
+    out = dict(nf=nf, nc=nc, op27=np.stack(op27), op7=np.stack(op7), cc=cc,
+               f=f, x0=x0)
+    for name, iad, zi in (("a0z0", 0, 0), ("a1z0", 1, 0), ("a0z1", 0, 1)):
+        x = x0.copy()
+        L.pmgref_Vgsrb7x(nf, nf, nf, d(op7[0]), d(cc), d(f), d(op7[1]),
+                         d(op7[2]), d(op7[3]), d(x), 2, iad, zi)
+        out["gs7_" + name] = x
+        x = x0.copy()
+        L.pmgref_Vgsrb27x(nf, nf, nf, pp(op27), d(cc), d(f), d(x), 2, iad, zi)
+        out["gs27_" + name] = x
+    y = np.zeros(nf ** 3)
+    L.pmgref_Vmatvec7_1s(nf, nf, nf, d(op7[0]), d(cc), d(op7[1]), d(op7[2]),
+                         d(op7[3]), d(x0), d(y))
+    out["matvec7"] = y.copy()
+    y[:] = 0
+    L.pmgref_Vmatvec27_1s(nf, nf, nf, pp(op27), d(cc), d(x0), d(y))
+    out["matvec27"] = y.copy()
+    y[:] = 0
+    L.pmgref_Vmresid7_1s(nf, nf, nf, d(op7[0]), d(cc), d(f), d(op7[1]),
+                         d(op7[2]), d(op7[3]), d(x0), d(y))
+    out["mresid7"] = y.copy()
+    y[:] = 0
+    L.pmgref_Vmresid27_1s(nf, nf, nf, pp(op27), d(cc), d(f), d(x0), d(y))
+    out["mresid27"] = y.copy()
+    # prolongation / Galerkin builders
+    P7 = [np.zeros(nc ** 3) for _ in range(27)]
+    L.pmgref_VbuildPb_op7(nf, nf, nf, nc, nc, nc, d(op7[0]), d(op7[1]),
+                          d(op7[2]), d(op7[3]), pp(P7))
+    out["P_op7"] = np.stack(P7)
+    P27 = [np.zeros(nc ** 3) for _ in range(27)]
+    L.pmgref_VbuildPb_op27(nf, nf, nf, nc, nc, nc, pp(op27), pp(P27))
+    out["P_op27"] = np.stack(P27)
+    Pt = [np.zeros(nc ** 3) for _ in range(27)]
+    L.pmgref_VbuildPb_trilin(nf, nf, nf, nc, nc, nc, pp(Pt))
+    out["P_trilin"] = np.stack(Pt)
+    Prand = [rng.uniform(0.05, 1.0, nc ** 3) for _ in range(27)]
+    out["P_rand"] = np.stack(Prand)
+    G7 = [np.zeros(nc ** 3) for _ in range(14)]
+    L.pmgref_VbuildG_7(nf, nf, nf, nc, nc, nc, pp(Prand), d(op7[0]),
+                       d(op7[1]), d(op7[2]), d(op7[3]), pp(G7))
+    out["G7"] = np.stack(G7)
+    G27 = [np.zeros(nc ** 3) for _ in range(14)]
+    L.pmgref_VbuildG_27(nf, nf, nf, nc, nc, nc, pp(Prand), pp(op27), pp(G27))
+    out["G27"] = np.stack(G27)
+    # transfers
+    xc = rng.normal(0.0, 1.0, nc ** 3)
+    e = np.zeros(nf ** 3)
+    L.pmgref_VinterpPMG2(nc, nc, nc, nf, nf, nf, d(xc), d(e), pp(Prand))
+    out["xc"] = xc
+    out["interp"] = e
+    rc_ = np.zeros(nc ** 3)
+    L.pmgref_Vrestrc2(nf, nf, nf, nc, nc, nc, d(x0), d(rc_), pp(Prand))
+    out["restrict"] = rc_
+    np.savez_compressed(os.path.join(OUT, "kernels_n9.npz"), **out)
+
+
+def problems(ref: Reference) -> None:
+    # set-up from atoms at the reference's constants, then hierarchy and
+    # solve on the same grid: (base 2, nlev 3) = 17^3 and (4, 3) = 33^3
+    for base, nlev, box, natoms, seed in ((2, 3, 8.0, 12, 11),
+                                          (4, 3, 16.0, 40, 12)):
+        n = base * 2 ** nlev + 1
+        atoms = synthetic_atoms(natoms, box / 5, seed, (box / 2,) * 3)
+        fine = ref.setup(base, nlev, atoms, 0.15, 2.0)
+        x, cycles, hist = ref.solve(base, nlev, fine, tol=1e-10,
+                                    max_cycles=60)
+        xt, ct, ht = ref.solve(base, nlev, fine, tol=1e-10, max_cycles=60,
+                               trilinear=True)
+        hier = ref.hierarchy(base, nlev, fine)
+        out = dict(base=base, nlev=nlev, box=box, atoms=atoms,
+                   ionic_strength=0.15, ion_radius=2.0, x=x, cycles=cycles,
+                   hist=hist, x_trilin=xt, cycles_trilin=ct, hist_trilin=ht,
+                   **{"fine_" + k: v for k, v in fine.items()})
+        for L_, (P, A) in hier.items():
+            out[f"P{L_}"] = P
+            out[f"A{L_}"] = A
+        # coarsest-level CG of the class on level 1 of this hierarchy
+        P1, A1 = hier[1]
+        n1 = base * 2 + 1
+        rng = np.random.default_rng(seed)
+        rhs = rng.normal(0.0, 1.0, n1 ** 3)
+        xcg = np.zeros(n1 ** 3)
+        ref.cg_level1(base, nlev, [np.ascontiguousarray(a) for a in A1], rhs,
+                      xcg)
+        out["cg_rhs"] = rhs
+        out["cg_x"] = xcg
+        np.savez_compressed(os.path.join(OUT, f"problem_b{base}n{nlev}.npz"),
+                            **out)
+        print(f"b{base}n{nlev}: n={n} cycles={cycles} (trilinear {ct})")
+
+
+if __name__ == "__main__":
+    ref = Reference()
+    kernels(ref)
+    problems(ref)
+    for f in sorted(os.listdir(OUT)):
+        if f.endswith(".npz"):
+            print(f, os.path.getsize(os.path.join(OUT, f)))

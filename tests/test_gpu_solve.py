@@ -1,0 +1,151 @@
+"""Whole PMG solves on the GPU through the problem handle (C ABI) against
+the CPU restatement and the reference's golden solves.
+
+FP64: the potential must be within 1e-12 relative L2 of the oracle with the
+same number of V-cycles; the hierarchy bit-identical to the restatement's.
+Mixed precision (float V-cycles inside double refinement): within 1e-8
+relative L2 of the FP64 oracle at relative residual 1e-10.
+"""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+pytestmark = pytest.mark.gpu
+
+if not torch.cuda.is_available():  # pragma: no cover
+    pytest.skip("no CUDA device", allow_module_level=True)
+
+from conftest import fine_of  # noqa: E402
+from multigrid_b200 import PBELinearProblem, WORKLOADS  # noqa: E402
+from multigrid_b200._lib import PmgError  # noqa: E402
+from multigrid_b200.problem import setup_fine  # noqa: E402
+
+TOL_FP64 = 1e-12
+TOL_MIXED = 1e-8
+
+
+def rel_l2(a, b):
+    return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+
+@pytest.mark.parametrize("trilinear", [False, True])
+def test_fp64_solve_matches_reference(golden_problem, trilinear):
+    g = golden_problem
+    base, nlev, box = int(g["base"]), int(g["nlev"]), float(g["box"])
+    sfx = "_trilin" if trilinear else ""
+    with PBELinearProblem(base, nlev, box, "fp64") as p:
+        p.set_fine(**fine_of(g))
+        p.buildmultilevelops(trilinear=trilinear)
+        res = p.solve(tol=1e-10, max_cycles=60)
+        x = p.potential().ravel()
+    assert res.cycles == int(g["cycles" + sfx])
+    assert res.relres < 1e-10
+    assert rel_l2(x, g["x" + sfx]) <= TOL_FP64
+
+
+def test_hierarchy_bitexact_vs_restatement(golden_problem, restatement):
+    g = golden_problem
+    base, nlev, box = int(g["base"]), int(g["nlev"]), float(g["box"])
+    ho = restatement.hierarchy(base, nlev, fine_of(g))
+    with PBELinearProblem(base, nlev, box, "fp64") as p:
+        p.set_fine(**fine_of(g))
+        p.buildmultilevelops()
+        for L in range(1, nlev):
+            P, A = p.get_level(L)
+            assert np.array_equal(P, ho[L][0]), L
+            assert np.array_equal(A, ho[L][1]), L
+
+
+def test_single_vcycles_match_restatement(golden_problem, restatement):
+    g = golden_problem
+    base, nlev, box = int(g["base"]), int(g["nlev"]), float(g["box"])
+    with PBELinearProblem(base, nlev, box, "fp64") as p:
+        p.set_fine(**fine_of(g))
+        p.buildmultilevelops()
+        r0 = p.compute_residual_2()
+        for _ in range(3):
+            p.v_cycle()
+        r3 = p.compute_residual_2()
+        x = p.potential().ravel()
+    xo, c, hist = restatement.solve(base, nlev, fine_of(g), tol=0.0,
+                                    max_cycles=3)
+    assert c == 3
+    assert abs(r0 / hist[0] - 1) < 1e-12
+    assert abs(r3 / hist[3] - 1) < 1e-6
+    assert rel_l2(x, xo) <= TOL_FP64
+
+
+def test_mixed_solve_close_to_fp64(golden_problem):
+    g = golden_problem
+    base, nlev, box = int(g["base"]), int(g["nlev"]), float(g["box"])
+    with PBELinearProblem(base, nlev, box, "mixed") as p:
+        p.set_fine(**fine_of(g))
+        p.buildmultilevelops()
+        res = p.solve(tol=1e-10, max_cycles=60)
+        x = p.potential().ravel()
+    assert res.relres < 1e-10
+    assert res.cycles <= int(g["cycles"]) + 3
+    assert rel_l2(x, g["x"]) <= TOL_MIXED
+
+
+@pytest.fixture(scope="module")
+def pb65():
+    w = WORKLOADS["pb65"]
+    return w, setup_fine(w.n, w.h, w.atoms(), w.physics)
+
+
+def test_pb65_fp64_matches_restatement(pb65, restatement):
+    w, fine = pb65
+    xo, co, ho = restatement.solve(w.base, w.nlev, fine, tol=1e-10,
+                                   max_cycles=60)
+    with PBELinearProblem(w.base, w.nlev, w.box, "fp64") as p:
+        p.set_fine(**fine)
+        p.buildmultilevelops()
+        res = p.solve(tol=1e-10, max_cycles=60)
+        x = p.potential().ravel()
+    assert res.cycles == co
+    assert rel_l2(x, xo) <= TOL_FP64
+
+
+def test_pb65_mixed_error_vs_fp64_oracle(pb65, restatement):
+    w, fine = pb65
+    xo, co, _ = restatement.solve(w.base, w.nlev, fine, tol=1e-10,
+                                  max_cycles=60)
+    with PBELinearProblem(w.base, w.nlev, w.box, "mixed") as p:
+        p.set_fine(**fine)
+        p.buildmultilevelops()
+        res = p.solve(tol=1e-10, max_cycles=60)
+        x = p.potential().ravel()
+    assert res.relres < 1e-10
+    assert rel_l2(x, xo) <= TOL_MIXED
+    assert np.abs(x - xo).max() / np.abs(xo).max() <= TOL_MIXED
+
+
+def test_state_errors():
+    with PBELinearProblem(2, 3, 8.0, "fp64") as p:
+        with pytest.raises(PmgError) as e:
+            p.buildmultilevelops()
+        assert e.value.status == -7
+        with pytest.raises(PmgError) as e:
+            p.solve()
+        assert e.value.status == -7
+    with PBELinearProblem(2, 3, 8.0, "mixed") as p:
+        with pytest.raises(PmgError):
+            p.v_cycle()
+
+
+def test_nan_input_reports_divergence(golden_problem):
+    g = golden_problem
+    base, nlev, box = int(g["base"]), int(g["nlev"]), float(g["box"])
+    fine = fine_of(g)
+    f = fine["f"].copy()
+    n = base * 2 ** nlev + 1
+    f[(n // 2) * n * n + (n // 2) * n + n // 2] = np.nan
+    fine["f"] = f
+    with PBELinearProblem(base, nlev, box, "fp64") as p:
+        p.set_fine(**fine)
+        p.buildmultilevelops()
+        with pytest.raises(PmgError) as e:
+            p.solve(tol=1e-10, max_cycles=5)
+        assert e.value.status == -4

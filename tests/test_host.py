@@ -1,0 +1,127 @@
+"""Host-side logic that needs no GPU: the C ABI library loads and exports
+every declared symbol, argument checks reject bad calls before any CUDA work,
+grid-size rules are exact, synthetic molecules are well formed."""
+import ctypes
+import math
+
+import numpy as np
+import pytest
+
+from multigrid_b200 import _lib
+from multigrid_b200.molecule import (BATCH_SIZES, WORKLOADS, batch_grid,
+                                     batch_workloads, coarsen, grid_step,
+                                     level_n, levels_for, synthetic_atoms)
+
+
+def test_library_exports_header():
+    names = _lib.exported_symbols()
+    assert len(names) > 25
+    missing = [n for n in names if not hasattr(_lib.lib, n)]
+    assert not missing, missing
+
+
+def test_version():
+    assert b"sm_100a" in _lib.lib.pmg_version()
+
+
+V = ctypes.c_void_p
+
+
+def test_kernel_args_rejected_without_gpu():
+    # grid too small / mismatched coarse sizes / null arrays: PMG_ERR_ARG
+    p = V(16)  # never dereferenced: the size checks fail first
+    assert _lib.lib.pmg_Vgsrb7x_d(2, 9, 9, p, None, p, p, p, p, p, 1, 0, 0,
+                                  None) == -1
+    assert _lib.lib.pmg_Vgsrb7x_d(9, 9, 9, None, None, p, p, p, p, p, 1, 0, 0,
+                                  None) == -1
+    assert b"null" in _lib.lib.pmg_last_error()
+    args = [9, 9, 9, 4, 4, 4] + [p] * 29 + [None]
+    assert _lib.lib.pmg_Vrestrc2_d(*args) == -1
+    assert b"2 n_c - 1" in _lib.lib.pmg_last_error()
+    assert _lib.lib.pmg_Vgsrb27x_d(*([9, 9, 9] + [p] * 17 + [-1, 0, 0, None])
+                                   ) == -1
+
+
+def test_problem_bytes():
+    b = _lib.lib.pmg_problem_bytes(8, 5, 0)
+    # 257^3 finest level: 4 coefficients + x, f, r = 7 arrays at least
+    assert b > 7 * 257 ** 3 * 8
+    assert b < 4 * 2 ** 30
+    mixed = _lib.lib.pmg_problem_bytes(8, 5, 1)
+    assert mixed > b
+    assert _lib.lib.pmg_problem_bytes(0, 5, 0) == -1
+    assert _lib.lib.pmg_problem_bytes(64, 5, 0) == -1  # n > 1025
+
+
+def test_grid_rules():
+    assert level_n(4, 4) == 65 and level_n(5, 5) == 161
+    assert level_n(8, 5) == 257
+    for n in (9, 17, 65, 161, 257):
+        assert coarsen(n) == (n - 1) // 2 + 1
+    assert [level_n(8, L) for L in range(5, 0, -1)] == [257, 129, 65, 33, 17]
+    assert grid_step(8, 5, 102.4) == pytest.approx(0.4)
+    assert {n: levels_for(n) for n in BATCH_SIZES} == {
+        65: (2, 5), 97: (3, 5), 129: (2, 6), 161: (5, 5), 193: (3, 6),
+        225: (7, 5)}
+    assert batch_grid(5.0) == 65 and batch_grid(30.0) == 161
+    assert batch_grid(200.0) == 225
+
+
+def test_workloads():
+    w = WORKLOADS["pb257"]
+    assert (w.n, w.base, w.nlev) == (257, 8, 5)
+    assert w.box == pytest.approx(102.4)
+    assert WORKLOADS["pb65"].n == 65 and WORKLOADS["pb161"].n == 161
+    ws = batch_workloads(96)
+    assert len(ws) == 96
+    assert all(4 <= w.nlev <= 6 for w in ws)
+    assert all(200 <= w.natoms <= 6000 for w in ws)
+    assert {w.n for w in ws} <= set(BATCH_SIZES)
+
+
+def test_synthetic_atoms():
+    a = synthetic_atoms(500, 12.0, 0, (16.0, 16.0, 16.0))
+    b = synthetic_atoms(500, 12.0, 0, (16.0, 16.0, 16.0))
+    assert np.array_equal(a, b)
+    r = np.linalg.norm(a[:, :3] - 16.0, axis=1)
+    assert a.shape == (500, 5) and r.max() <= 12.0
+    assert a[:, 3].min() >= 1.2 and a[:, 3].max() <= 2.0
+    q = a[:, 4].sum()
+    assert abs(q - round(q)) < 1e-9
+    assert abs(np.std(a[:, 4]) - 0.4) < 0.05
+
+
+def test_setup_physics():
+    from multigrid_b200.problem import kappa
+    from multigrid_b200.molecule import DEFAULT_PHYSICS, REFERENCE_PHYSICS
+    k, e0 = kappa(REFERENCE_PHYSICS)
+    # Debye length of 0.15 M 1:1 salt at 298 K in water: ~7.85 A
+    assert 1 / k == pytest.approx(7.85, abs=0.05)
+    assert e0 == pytest.approx(1.42e-4, rel=0.01)
+    k2, _ = kappa(DEFAULT_PHYSICS)
+    assert k2 == pytest.approx(k * math.sqrt(78.4 / 78.54), rel=1e-12)
+
+
+def test_setup_probe_surface_contains_vdw():
+    from multigrid_b200.molecule import DEFAULT_PHYSICS
+    from multigrid_b200.problem import setup_fine
+    n, h = 33, 0.5
+    atoms = synthetic_atoms(30, 3.5, 5, (8.0, 8.0, 8.0))
+    vdw = setup_fine(n, h, atoms, dict(DEFAULT_PHYSICS, probe_radius=0.0))
+    ses = setup_fine(n, h, atoms, DEFAULT_PHYSICS)
+    inside_vdw = vdw["oE"] < DEFAULT_PHYSICS["eps_out"] / h ** 2
+    inside_ses = ses["oE"] < DEFAULT_PHYSICS["eps_out"] / h ** 2
+    # the molecular surface encloses the van der Waals volume and more
+    assert np.all(inside_ses[inside_vdw])
+    assert inside_ses.sum() > inside_vdw.sum()
+    # the rest of the set-up does not depend on the probe
+    for k in ("f", "x0"):
+        assert np.array_equal(vdw[k], ses[k])
+
+
+def test_setup_rejects_atoms_outside():
+    from multigrid_b200.molecule import DEFAULT_PHYSICS
+    from multigrid_b200.problem import setup_fine
+    with pytest.raises(_lib.PmgError):
+        setup_fine(9, 0.5, np.array([[10.0, 1.0, 1.0, 1.5, 1.0]]),
+                   DEFAULT_PHYSICS)

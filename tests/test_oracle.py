@@ -1,0 +1,179 @@
+"""The CPU restatement (oracle/pmg_oracle.c) against the reference's own
+outputs: the golden fixtures made by tests/golden/make_golden.py from the
+reference PMG class and pmgc kernels, and — where the reference-built oracle
+(oracle/_ref) is present — random cases run through it directly.
+
+Per-point kernels (smoothers, matvec, residual, transfers) keep the
+reference's operation order and must match bit for bit; the builders are a
+generic formulation and must match to rounding; whole solves to 1e-12
+relative L2 with the same number of cycles.
+"""
+import numpy as np
+import pytest
+
+from conftest import fine_of
+from oracle.oracle import Reference, reference_available
+
+TOL_BUILD = 1e-13   # builders: relative to the array's max magnitude
+TOL_SOLVE = 1e-12   # potential: relative L2
+
+
+def rel(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+def test_gs7_bitexact(restatement, golden_kernels):
+    g = golden_kernels
+    n, op7 = int(g["nf"]), g["op7"]
+    for name, iad, zi in (("a0z0", 0, 0), ("a1z0", 1, 0), ("a0z1", 0, 1)):
+        x = g["x0"].copy()
+        restatement.gsrb7x(n, op7[0], g["cc"], g["f"], op7[1], op7[2], op7[3],
+                           x, itmax=2, iadjoint=iad, zero_init=zi)
+        assert np.array_equal(x, g["gs7_" + name]), name
+
+
+def test_gs27_bitexact(restatement, golden_kernels):
+    g = golden_kernels
+    n = int(g["nf"])
+    op = [np.ascontiguousarray(a) for a in g["op27"]]
+    for name, iad, zi in (("a0z0", 0, 0), ("a1z0", 1, 0), ("a0z1", 0, 1)):
+        x = g["x0"].copy()
+        restatement.gsrb27x(n, op, g["cc"], g["f"], x, itmax=2, iadjoint=iad,
+                            zero_init=zi)
+        assert np.array_equal(x, g["gs27_" + name]), name
+
+
+def test_matvec_mresid_bitexact(restatement, golden_kernels):
+    g = golden_kernels
+    n = int(g["nf"])
+    op7 = [np.ascontiguousarray(a) for a in g["op7"]]
+    op27 = [np.ascontiguousarray(a) for a in g["op27"]]
+    for ops, key in ((op7, "7"), (op27, "27")):
+        y = np.zeros(n ** 3)
+        restatement.matvec(n, ops, g["cc"], g["x0"], y)
+        assert np.array_equal(y, g["matvec" + key])
+        r = np.zeros(n ** 3)
+        restatement.mresid(n, ops, g["cc"], g["f"], g["x0"], r)
+        assert np.array_equal(r, g["mresid" + key])
+
+
+def test_transfers_bitexact(restatement, golden_kernels):
+    g = golden_kernels
+    nf, nc = int(g["nf"]), int(g["nc"])
+    P = [np.ascontiguousarray(a) for a in g["P_rand"]]
+    e = np.zeros(nf ** 3)
+    restatement.interp2(nc, nf, g["xc"], e, P)
+    assert np.array_equal(e, g["interp"])
+    r = np.zeros(nc ** 3)
+    restatement.restrc2(nf, nc, g["x0"], r, P)
+    assert np.array_equal(r, g["restrict"])
+
+
+def test_build_prolongation(restatement, golden_kernels):
+    g = golden_kernels
+    nf, nc = int(g["nf"]), int(g["nc"])
+    for ops, key in (([np.ascontiguousarray(a) for a in g["op7"]], "P_op7"),
+                     ([np.ascontiguousarray(a) for a in g["op27"]], "P_op27")):
+        P = [np.zeros(nc ** 3) for _ in range(27)]
+        restatement.buildP_op(nf, nc, ops, P)
+        for s in range(27):
+            assert rel(P[s], g[key][s]) <= TOL_BUILD, (key, s)
+    P = [np.zeros(nc ** 3) for _ in range(27)]
+    restatement.buildP_trilin(nc, P)
+    assert np.array_equal(np.stack(P), g["P_trilin"])
+
+
+def test_build_galerkin(restatement, golden_kernels):
+    g = golden_kernels
+    nf, nc = int(g["nf"]), int(g["nc"])
+    P = [np.ascontiguousarray(a) for a in g["P_rand"]]
+    for ops, key in (([np.ascontiguousarray(a) for a in g["op7"]], "G7"),
+                     ([np.ascontiguousarray(a) for a in g["op27"]], "G27")):
+        out = [np.zeros(nc ** 3) for _ in range(14)]
+        restatement.buildG(nf, nc, P, ops, out)
+        for s in range(14):
+            assert rel(out[s], g[key][s]) <= TOL_BUILD, (key, s)
+
+
+def test_hierarchy(restatement, golden_problem):
+    g = golden_problem
+    base, nlev = int(g["base"]), int(g["nlev"])
+    hier = restatement.hierarchy(base, nlev, fine_of(g))
+    for L, (P, A) in hier.items():
+        for s in range(27):
+            assert rel(P[s], g[f"P{L}"][s]) <= TOL_BUILD, (L, "P", s)
+        for s in range(14):
+            assert rel(A[s], g[f"A{L}"][s]) <= 1e-12, (L, "A", s)
+
+
+def test_cg_level1(restatement, golden_problem):
+    g = golden_problem
+    base = int(g["base"])
+    n1 = 2 * base + 1
+    A1 = [np.ascontiguousarray(a) for a in g["A1"]]
+    x = np.zeros(n1 ** 3)
+    restatement.cg(n1, A1, g["cg_rhs"], x)
+    assert rel(x, g["cg_x"]) <= 1e-12
+
+
+@pytest.mark.parametrize("trilinear", [False, True])
+def test_solve(restatement, golden_problem, trilinear):
+    g = golden_problem
+    base, nlev = int(g["base"]), int(g["nlev"])
+    sfx = "_trilin" if trilinear else ""
+    x, cycles, hist = restatement.solve(base, nlev, fine_of(g), tol=1e-10,
+                                        max_cycles=60, trilinear=trilinear)
+    assert cycles == int(g["cycles" + sfx])
+    xr = g["x" + sfx]
+    assert np.linalg.norm(x - xr) / np.linalg.norm(xr) <= TOL_SOLVE
+    h = g["hist" + sfx]
+    # early residual norms agree closely; late ones are rounding-dominated
+    assert abs(hist[1] / h[1] - 1) < 1e-9
+
+
+def test_setup_matches_reference(golden_problem):
+    from multigrid_b200.molecule import REFERENCE_PHYSICS
+    from multigrid_b200.problem import setup_fine
+    g = golden_problem
+    base, nlev, box = int(g["base"]), int(g["nlev"]), float(g["box"])
+    n = base * 2 ** nlev + 1
+    out = setup_fine(n, box / (n - 1), g["atoms"], REFERENCE_PHYSICS)
+    for k in ("oC", "oE", "oN", "uC", "f", "x0"):
+        assert np.array_equal(out[k], g["fine_" + k]), k
+
+
+# -------- direct comparison with the reference-built oracle (if built) --------
+needs_ref = pytest.mark.skipif(not reference_available(),
+                               reason="oracle/_ref not built")
+
+
+@needs_ref
+@pytest.mark.parametrize("base,nlev", [(2, 3), (4, 2), (3, 4), (4, 4)])
+def test_solve_vs_reference(restatement, base, nlev):
+    from multigrid_b200.molecule import REFERENCE_PHYSICS, synthetic_atoms
+    from multigrid_b200.problem import setup_fine
+    ref = Reference()
+    n = base * 2 ** nlev + 1
+    h = 0.5
+    box = h * (n - 1)
+    atoms = synthetic_atoms(3 * n, box / 5, 100 + n, (box / 2,) * 3)
+    fine = setup_fine(n, h, atoms, REFERENCE_PHYSICS)
+    xr, cr, _ = ref.solve(base, nlev, fine, tol=1e-10, max_cycles=60)
+    xo, co, _ = restatement.solve(base, nlev, fine, tol=1e-10, max_cycles=60)
+    assert co == cr
+    assert np.linalg.norm(xo - xr) / np.linalg.norm(xr) <= TOL_SOLVE
+
+
+@needs_ref
+def test_setup_vs_reference_random():
+    from multigrid_b200.molecule import REFERENCE_PHYSICS, synthetic_atoms
+    from multigrid_b200.problem import setup_fine
+    ref = Reference()
+    for base, nlev, box in ((4, 3, 16.0), (4, 4, 32.0), (3, 4, 24.0)):
+        n = base * 2 ** nlev + 1
+        atoms = synthetic_atoms(60, box / 4, 7 + base, (box / 2,) * 3)
+        a = ref.setup(base, nlev, atoms, 0.15, 2.0)
+        b = setup_fine(n, box / (n - 1), atoms, REFERENCE_PHYSICS)
+        for k in a:
+            assert np.array_equal(a[k], b[k]), (base, nlev, k)
