@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--workload", default="pb257")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    # one precision, no end-to-end or kernel legs: a short run for profilers
+    ap.add_argument("--quick", action="store_true")
     return ap.parse_args()
 
 
@@ -264,8 +266,10 @@ def main():
         return p.solve(TOL, MAX_CYCLES)
 
     results = {}
-    for precision in (args.precision, "fp64" if args.precision == "mixed"
-                      else "mixed"):
+    precisions = [args.precision]
+    if not args.quick:
+        precisions.append("fp64" if args.precision == "mixed" else "mixed")
+    for precision in precisions:
         p = make(precision)
         stream = torch.cuda.ExternalStream(p.stream)
         for _ in range(args.warmup):
@@ -295,6 +299,14 @@ def main():
 
     prim = results[args.precision]
     value = world * args.steps / (prim["ms"] / 1000.0)
+    if args.quick:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT,
+                              "quick": True, "cycles": prim["cycles"][-1],
+                              "ms_per_step": prim["ms"] / args.steps}))
+        for r in results.values():
+            r["p"].close()
+        return 0
 
     # end to end through the public API from pinned host buffers
     p = prim["p"]
