@@ -312,6 +312,11 @@ int pmg_get_potential(pmg_problem *p, double *dst);
  * arrays then 14 operator arrays, n_L^3 doubles each; L in [1, nlev-1]. */
 int pmg_get_level(pmg_problem *p, int level, double *dst);
 
+/* Mixed precision: relative residual reduction at which the coarsest-level
+ * CG stops on each correction (default 1e-4; the FP64 path always runs the
+ * class's absolute 1e-8 test). */
+int pmg_problem_set_coarse_rtol(pmg_problem *p, double rtol);
+
 /* The class's stream (for callers that enqueue around a solve). */
 pmg_stream_t pmg_problem_stream(pmg_problem *p);
 

@@ -102,6 +102,7 @@ _sig("pmg_solve", c_int, _V, c_double, c_int, PI, PD, PD)
 _sig("pmg_get_potential", c_int, _V, _V)
 _sig("pmg_get_level", c_int, _V, c_int, _V)
 _sig("pmg_problem_stream", c_void_p, _V)
+_sig("pmg_problem_set_coarse_rtol", c_int, _V, c_double)
 
 
 def check(func: str, status: int) -> None:

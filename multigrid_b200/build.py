@@ -2,7 +2,7 @@
 
 The library is a plain shared object with a C ABI (include/pmg_b200.h);
 nothing in it depends on torch. Invoked by __graft_entry__.build() and
-usable directly: python -m multigrid_b200.build
+usable directly: python multigrid_b200/build.py [--force]
 """
 from __future__ import annotations
 

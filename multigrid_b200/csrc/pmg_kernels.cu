@@ -51,101 +51,142 @@ __global__ void buildP_trilin_kernel(Dims dc, P27W<double> P) {
       }
 }
 
+// Block-wide sum visible to every thread: warp shuffles, one partial per
+// warp in sh[0..31], one barrier, then every thread adds the 32 partials in
+// warp order (deterministic). Callers alternate between two sh buffers so
+// that a buffer is only rewritten after a later barrier.
+__device__ __forceinline__ double cg_allsum(double v, double *sh) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
+    v += __shfl_down_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0)
+    sh[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double t = 0.0;
+  const int nw = blockDim.x >> 5;
+  for (int w = 0; w < nw; ++w)
+    t += sh[w];
+  return t;
+}
+
+template <int K>
 __global__ void __launch_bounds__(1024)
     cg_level_kernel(Dims d, Op14<double> A, const double *__restrict__ rhs,
                     double *__restrict__ x, double *__restrict__ r,
-                    double *__restrict__ p, double thresh, int max_iters,
-                    int *__restrict__ status) {
-  __shared__ double sh[32];
-  __shared__ double bc;
+                    double *__restrict__ p, double *__restrict__ ap,
+                    double thresh, double rel_tol, int class_first_check,
+                    int max_iters, int *__restrict__ status) {
+  __shared__ double sh[2][32];
   const int m = (d.nx - 2) * (d.ny - 2) * (d.nz - 2);
   const int sy = d.sy(), sz = d.sz();
-  const int tid = threadIdx.x, nt = blockDim.x;
-  auto bsum = [&](double v) {
-    v = block_sum(v, sh);
-    if (tid == 0)
-      bc = v;
-    __syncthreads();
-    const double out = bc;
-    __syncthreads();
-    return out;
-  };
+  int c[K];
+#pragma unroll
+  for (int t = 0; t < K; ++t) {
+    const int q = threadIdx.x + t * blockDim.x;
+    int i = 2, j = 2, k = 2;
+    if (q < m)
+      interior_coords(d, q, i, j, k);
+    c[t] = q < m ? d.at(i, j, k) : -1;
+  }
+  const double *const nul = nullptr;
 
-  // r = rhs - A x; p = r
-  for (int q = tid; q < m; q += nt) {
-    int i, j, k;
-    interior_coords(d, q, i, j, k);
-    const int c = d.at(i, j, k);
-    const double v = rhs[c] - apply27(A, (const double *)nullptr, x, c, sy, sz);
-    r[c] = v;
-    p[c] = v;
-  }
-  __syncthreads();
+  // r = rhs - A x; p = r; rs = r.r
   double acc = 0.0;
-  for (int q = tid; q < m; q += nt) {
-    int i, j, k;
-    interior_coords(d, q, i, j, k);
-    const int c = d.at(i, j, k);
-    acc += r[c] * r[c];
-  }
-  double rs = bsum(acc);
+#pragma unroll
+  for (int t = 0; t < K; ++t)
+    if (c[t] >= 0) {
+      const double v = rhs[c[t]] - apply27(A, nul, x, c[t], sy, sz);
+      r[c[t]] = v;
+      p[c[t]] = v;
+      acc += v * v;
+    }
+  double rs = cg_allsum(acc, sh[0]);
+  // Ap and p.Ap (A p is kept: the next update needs exactly these values)
   acc = 0.0;
-  for (int q = tid; q < m; q += nt) {
-    int i, j, k;
-    interior_coords(d, q, i, j, k);
-    const int c = d.at(i, j, k);
-    acc += apply27(A, (const double *)nullptr, p, c, sy, sz) * p[c];
-  }
-  double pap = bsum(acc);
+#pragma unroll
+  for (int t = 0; t < K; ++t)
+    if (c[t] >= 0) {
+      const double v = apply27(A, nul, p, c[t], sy, sz);
+      ap[c[t]] = v;
+      acc += v * p[c[t]];
+    }
+  double pap = cg_allsum(acc, sh[1]);
   int it = 0;
   double res = 0.0;
   if (pap != 0.0) {
     double alpha = rs / pap;
-    res = sqrt(sqrt(rs));
-    while (res > thresh && it < max_iters) {
+    res = class_first_check ? sqrt(sqrt(rs)) : sqrt(rs);
+    const double stop = fmax(thresh, rel_tol * sqrt(rs));
+    while (res > stop && it < max_iters) {
       ++it;
-      for (int q = tid; q < m; q += nt) {
-        int i, j, k;
-        interior_coords(d, q, i, j, k);
-        const int c = d.at(i, j, k);
-        const double ap = apply27(A, (const double *)nullptr, p, c, sy, sz);
-        x[c] += alpha * p[c];
-        r[c] -= alpha * ap;
-      }
-      __syncthreads();
       acc = 0.0;
-      for (int q = tid; q < m; q += nt) {
-        int i, j, k;
-        interior_coords(d, q, i, j, k);
-        const int c = d.at(i, j, k);
-        acc += r[c] * r[c];
-      }
-      const double rsn = bsum(acc);
+#pragma unroll
+      for (int t = 0; t < K; ++t)
+        if (c[t] >= 0) {
+          x[c[t]] += alpha * p[c[t]];
+          const double v = r[c[t]] - alpha * ap[c[t]];
+          r[c[t]] = v;
+          acc += v * v;
+        }
+      const double rsn = cg_allsum(acc, sh[0]);
       const double beta = rs == 0.0 ? 0.0 : rsn / rs;
       rs = rsn;
-      for (int q = tid; q < m; q += nt) {
-        int i, j, k;
-        interior_coords(d, q, i, j, k);
-        const int c = d.at(i, j, k);
-        p[c] = r[c] + beta * p[c];
-      }
+#pragma unroll
+      for (int t = 0; t < K; ++t)
+        if (c[t] >= 0)
+          p[c[t]] = r[c[t]] + beta * p[c[t]];
       __syncthreads();
       acc = 0.0;
-      for (int q = tid; q < m; q += nt) {
-        int i, j, k;
-        interior_coords(d, q, i, j, k);
-        const int c = d.at(i, j, k);
-        acc += apply27(A, (const double *)nullptr, p, c, sy, sz) * p[c];
-      }
-      pap = bsum(acc);
+#pragma unroll
+      for (int t = 0; t < K; ++t)
+        if (c[t] >= 0) {
+          const double v = apply27(A, nul, p, c[t], sy, sz);
+          ap[c[t]] = v;
+          acc += v * p[c[t]];
+        }
+      pap = cg_allsum(acc, sh[1]);
       alpha = pap == 0.0 ? 0.0 : rs / pap;
       res = sqrt(rs);
     }
+    if (threadIdx.x == 0) {
+      status[0] = it;
+      status[1] = (it >= max_iters && res > stop) ? 1 : 0;
+    }
+  } else if (threadIdx.x == 0) {
+    status[0] = 0;
+    status[1] = 0;
   }
-  if (tid == 0) {
-    status[0] = it;
-    status[1] = (it >= max_iters && res > thresh) ? 1 : 0;
+}
+
+int launch_cg_level(const Dims &d, const Op14<double> &A, const double *rhs,
+                    double *x, double *r, double *p, double *ap,
+                    double thresh, double rel_tol, int class_first_check,
+                    int max_iters, int *status, cudaStream_t s) {
+  const long m = (long)(d.nx - 2) * (d.ny - 2) * (d.nz - 2);
+  const int k = (int)((m + 1023) / 1024);
+#define PMG_CG(K)                                                              \
+  cg_level_kernel<K><<<1, 1024, 0, s>>>(d, A, rhs, x, r, p, ap, thresh,       \
+                                        rel_tol, class_first_check,           \
+                                        max_iters, status)
+  if (k <= 1)
+    PMG_CG(1);
+  else if (k <= 2)
+    PMG_CG(2);
+  else if (k <= 4)
+    PMG_CG(4);
+  else if (k <= 8)
+    PMG_CG(8);
+  else if (k <= 16)
+    PMG_CG(16);
+  else if (k <= 32)
+    PMG_CG(32);
+  else {
+    set_last_message("cg_level: level too large for one CTA");
+    return PMG_ERR_ARG;
   }
+#undef PMG_CG
+  PMG_LAUNCH_CHECK();
+  return PMG_OK;
 }
 
 } // namespace pmg
@@ -496,19 +537,19 @@ int pmg_cg_level_d(int nx, int ny, int nz, const double *const *a14,
   cudaStream_t s = (cudaStream_t)stream;
   const Dims d{nx, ny, nz};
   const size_t n3 = (size_t)d.count();
-  // r, p (zero shells) and the two status words, stream-ordered.
+  // r, p, Ap (zero shells) and the two status words, stream-ordered.
   char *ws = nullptr;
-  const size_t bytes = 2 * n3 * sizeof(double) + 2 * sizeof(int);
+  const size_t bytes = 3 * n3 * sizeof(double) + 2 * sizeof(int);
   PMG_CUDA_TRY(cudaMallocAsync((void **)&ws, bytes, s));
   int rc = PMG_OK;
   int host_status[2] = {0, 0};
-  double *r = (double *)ws, *p = r + n3;
-  int *status = (int *)(p + n3);
+  double *r = (double *)ws, *p = r + n3, *ap = p + n3;
+  int *status = (int *)(ap + n3);
   cudaError_t e = cudaMemsetAsync(ws, 0, bytes, s);
   if (e == cudaSuccess) {
-    cg_level_kernel<<<1, 1024, 0, s>>>(d, A, rhs, x, r, p, thresh, max_iters,
-                                       status);
-    e = cudaGetLastError();
+    rc = launch_cg_level(d, A, rhs, x, r, p, ap, thresh, 0.0, 1, max_iters,
+                         status, s);
+    e = rc == PMG_OK ? cudaSuccess : cudaErrorLaunchFailure;
   }
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(host_status, status, sizeof(host_status),
@@ -516,6 +557,8 @@ int pmg_cg_level_d(int nx, int ny, int nz, const double *const *a14,
   cudaFreeAsync(ws, s);
   if (e == cudaSuccess)
     e = cudaStreamSynchronize(s);
+  if (rc != PMG_OK)
+    return rc;
   if (e != cudaSuccess) {
     set_last_error(e, "cg_level", __FILE__, __LINE__);
     return PMG_ERR_CUDA;

@@ -78,8 +78,11 @@ struct pmg_problem {
   char *arena = nullptr;
   size_t arena_bytes = 0;
   LevelBuf lv[kMaxLevels + 1];
-  double *cg_r = nullptr, *cg_p = nullptr;
+  double *cg_r = nullptr, *cg_p = nullptr, *cg_ap = nullptr;
   int *cg_status = nullptr;
+  // Relative stopping threshold of the coarsest CG on the mixed path's
+  // correction equation (the FP64 path keeps the class's absolute 1e-8).
+  double coarse_rtol = 1e-4;
   ReduceSlot red_norm{}, red_lambda{};
   double *h_pinned = nullptr; // [0] residual sum, [1..] spare
   int *h_status = nullptr;
@@ -127,6 +130,7 @@ void plan(pmg_problem *p, Arena &a) {
   const long n1 = p->lv[1].n3;
   p->cg_r = a.take<double>(n1);
   p->cg_p = a.take<double>(n1);
+  p->cg_ap = a.take<double>(n1);
   p->cg_status = a.take<int>(2);
   for (ReduceSlot *s : {&p->red_norm, &p->red_lambda}) {
     s->partials = a.take<double>(2 * kReduceBlocks);
@@ -155,13 +159,17 @@ int smooth64(pmg_problem *p, int L, int zero_init) {
                              zero_init, p->stream);
 }
 
+// Coarsest level: the class's CG (absolute 1e-8, first test on
+// sqrt(sqrt(r.r))) on the FP64 path; on the mixed path a zero-started CG to
+// coarse_rtol relative to its initial residual.
 int cg_level1(pmg_problem *p, const double *rhs, double *x) {
   LevelBuf &v = p->lv[1];
-  cg_level_kernel<<<1, 1024, 0, p->stream>>>(v.d, v.A64(14), rhs, x, p->cg_r,
-                                             p->cg_p, 1e-8, kCgMaxIters,
-                                             p->cg_status);
-  PMG_LAUNCH_CHECK();
-  return PMG_OK;
+  if (p->precision == PMG_PREC_MIXED)
+    return launch_cg_level(v.d, v.A64(14), rhs, x, p->cg_r, p->cg_p,
+                           p->cg_ap, 0.0, p->coarse_rtol, 0, kCgMaxIters,
+                           p->cg_status, p->stream);
+  return launch_cg_level(v.d, v.A64(14), rhs, x, p->cg_r, p->cg_p, p->cg_ap,
+                         1e-8, 0.0, 1, kCgMaxIters, p->cg_status, p->stream);
 }
 
 int vcycle64(pmg_problem *p, int L, int as_preconditioner) {
@@ -427,6 +435,19 @@ int pmg_problem_destroy(pmg_problem *p) {
   if (p->own_stream)
     cudaStreamDestroy(p->stream);
   delete p;
+  return PMG_OK;
+}
+
+int pmg_problem_set_coarse_rtol(pmg_problem *p, double rtol) {
+  if (!p || !(rtol >= 0.0) || rtol >= 1.0) {
+    set_last_message("pmg_problem_set_coarse_rtol: need 0 <= rtol < 1");
+    return PMG_ERR_ARG;
+  }
+  p->coarse_rtol = rtol;
+  if (p->cycle_exec) { // the captured cycle bakes the threshold in
+    cudaGraphExecDestroy(p->cycle_exec);
+    p->cycle_exec = nullptr;
+  }
   return PMG_OK;
 }
 

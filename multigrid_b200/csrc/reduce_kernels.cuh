@@ -138,18 +138,21 @@ __global__ void __launch_bounds__(kReduceThreads)
 
 // Coarsest-level CG of the class, one CTA (CG_solver, CG_Solver.h:45-242 via
 // solve_by_cg<1>, PBE_pmgc_class.h:856-860):
-//   r = rhs - A x; p = r; rs = r.r; pAp = (A p).p; stop if pAp == 0;
-//   alpha = rs/pAp; res = sqrt(sqrt(rs));
-//   while res > thresh: x += alpha p; r -= alpha A p; rs' = r.r;
-//     beta = rs'/rs (0 if rs == 0); p = r + beta p; pAp = (A p).p;
-//     alpha = rs/pAp (0 if pAp == 0); res = sqrt(rs)
-// bounded by max_iters (the reference loops without a cap). r and p are
-// scratch arrays whose shells are zero. status[0] = iterations,
-// status[1] = 1 when the cap stopped the loop above the threshold.
-__global__ void __launch_bounds__(1024)
-    cg_level_kernel(Dims d, Op14<double> A, const double *__restrict__ rhs,
-                    double *__restrict__ x, double *__restrict__ r,
-                    double *__restrict__ p, double thresh, int max_iters,
-                    int *__restrict__ status);
+//   r = rhs - A x; p = r; rs = r.r; Ap = A p; pAp = Ap.p; stop if pAp == 0;
+//   alpha = rs/pAp; res = sqrt(sqrt(rs)) (class_first_check) or sqrt(rs);
+//   while res > max(thresh, rel_tol sqrt(rs_0)):
+//     x += alpha p; r -= alpha Ap; rs' = r.r; beta = rs'/rs (0 if rs == 0);
+//     p = r + beta p; Ap = A p; pAp = Ap.p; alpha = rs/pAp (0 if pAp == 0);
+//     res = sqrt(rs)
+// bounded by max_iters (the reference loops without a cap). The reference
+// applies A to the same p twice per iteration; keeping Ap gives the same
+// values with one matvec. The class runs thresh = 1e-8, rel_tol = 0,
+// class_first_check = 1. r, p, Ap are scratch arrays whose shells are zero.
+// status[0] = iterations, status[1] = 1 when the cap stopped the loop above
+// the threshold. Grids up to 33^3 (at most 32 interior points per thread).
+int launch_cg_level(const Dims &d, const Op14<double> &A, const double *rhs,
+                    double *x, double *r, double *p, double *ap,
+                    double thresh, double rel_tol, int class_first_check,
+                    int max_iters, int *status, cudaStream_t s);
 
 } // namespace pmg

@@ -162,6 +162,11 @@ class PBELinearProblem:
         torch.cuda.current_stream()  # make sure CUDA is initialised
         torch.cuda.ExternalStream(self.stream).synchronize()
 
+    def set_coarse_rtol(self, rtol: float) -> None:
+        """Mixed precision: relative stop of the coarsest CG per correction."""
+        _lib.check("pmg_problem_set_coarse_rtol",
+                   _lib.lib.pmg_problem_set_coarse_rtol(self._h, float(rtol)))
+
     # -- multigrid ------------------------------------------------------------
     def buildmultilevelops(self, trilinear: bool = False) -> None:
         """Galerkin hierarchy (PBE_pmgc_class.h:351-617)."""
