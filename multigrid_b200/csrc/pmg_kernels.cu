@@ -4,6 +4,7 @@
 #include <string.h>
 
 #include "build_kernels.cuh"
+#include "gs27_tiled.cuh"
 #include "launch.cuh"
 #include "reduce_kernels.cuh"
 
@@ -236,6 +237,40 @@ template <typename T> static bool any_null(const Op14<T> &A, int n) {
   return false;
 }
 
+// Runs itmax eight-colour sweeps in place on x with the two-launch tiled
+// kernel; the ping-pong partner is a stream-ordered copy of x (same shell).
+template <typename T>
+static int gs27_inplace(const Dims &d, const Op14<T> &A, const T *cc,
+                        const T *fc, T *x, int itmax, int iadjoint,
+                        int zero_init, cudaStream_t s) {
+  if (itmax == 0) {
+    if (zero_init)
+      PMG_CUDA_TRY(cudaMemsetAsync(x, 0, sizeof(T) * d.count(), s));
+    return PMG_OK;
+  }
+  T *alt = nullptr;
+  const size_t bytes = sizeof(T) * d.count();
+  PMG_CUDA_TRY(cudaMallocAsync((void **)&alt, bytes, s));
+  int rc = PMG_OK;
+  cudaError_t e = cudaSuccess;
+  if (zero_init)
+    e = cudaMemsetAsync(x, 0, bytes, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(alt, x, bytes, cudaMemcpyDeviceToDevice, s);
+  if (e == cudaSuccess) {
+    T *res = nullptr;
+    rc = launch_gs27_pp<T>(d, A, cc, fc, x, alt, itmax, iadjoint, 0, s, &res);
+    if (rc == PMG_OK && res != x)
+      e = cudaMemcpyAsync(x, res, bytes, cudaMemcpyDeviceToDevice, s);
+  }
+  cudaFreeAsync(alt, s);
+  if (e != cudaSuccess) {
+    set_last_error(e, "Vgsrb27x", __FILE__, __LINE__);
+    return PMG_ERR_CUDA;
+  }
+  return rc;
+}
+
 // ---------------------------------------------------------------------------
 // C ABI
 // ---------------------------------------------------------------------------
@@ -270,8 +305,8 @@ int pmg_Vgsrb7x_f(int nx, int ny, int nz, const float *oC, const float *cc,
       op27<T>(oC, oE, oN, uC, oNE, oNW, uE, uW, uN, uS, uNE, uNW, uSE, uSW);  \
   PMG_REQUIRE(!any_null(A, 14) && fc && x, "Vgsrb27x: null array");            \
   PMG_REQUIRE(itmax >= 0, "Vgsrb27x: itmax < 0");                              \
-  return launch_gs27<T>(Dims{nx, ny, nz}, A, cc, fc, x, itmax, iadjoint,      \
-                        zero_init, (cudaStream_t)stream);
+  return gs27_inplace<T>(Dims{nx, ny, nz}, A, cc, fc, x, itmax, iadjoint,     \
+                         zero_init, (cudaStream_t)stream);
 
 int pmg_Vgsrb27x_d(int nx, int ny, int nz, const double *oC, const double *cc,
                    const double *fc, const double *oE, const double *oN,

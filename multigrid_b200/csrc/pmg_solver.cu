@@ -8,6 +8,7 @@
 #include <new>
 
 #include "build_kernels.cuh"
+#include "gs27_tiled.cuh"
 #include "launch.cuh"
 #include "reduce_kernels.cuh"
 
@@ -23,9 +24,11 @@ struct LevelBuf {
   double *op[14] = {};
   double *P[27] = {}; // prolongation from this level to level+1
   double *x = nullptr, *f = nullptr, *r = nullptr;
+  double *xalt = nullptr; // ping-pong partner of x for the 27-point smoother
   float *op32[14] = {};
   float *P32[27] = {};
   float *x32 = nullptr, *f32 = nullptr, *r32 = nullptr;
+  float *xalt32 = nullptr;
   double *omega = nullptr; // damping computed on this level (device)
 
   Op14<double> A64(int nops) const {
@@ -116,6 +119,8 @@ void plan(pmg_problem *p, Arena &a) {
     v.x = need64 ? a.take<double>(v.n3) : nullptr;
     v.f = need64 ? a.take<double>(v.n3) : nullptr;
     v.r = (mixed && L > 1) ? nullptr : a.take<double>(v.n3);
+    const bool smooth27 = !fine && L > 1;
+    v.xalt = (smooth27 && !mixed) ? a.take<double>(v.n3) : nullptr;
     v.omega = a.take<double>(1);
     if (mixed) {
       for (int s = 0; s < 14; ++s)
@@ -125,6 +130,7 @@ void plan(pmg_problem *p, Arena &a) {
       v.x32 = a.take<float>(v.n3);
       v.f32 = a.take<float>(v.n3);
       v.r32 = L > 1 ? a.take<float>(v.n3) : nullptr;
+      v.xalt32 = smooth27 ? a.take<float>(v.n3) : nullptr;
     }
   }
   const long n1 = p->lv[1].n3;
@@ -149,14 +155,24 @@ int check_shape(int base, int nlev) {
 
 // ---- V-cycle pieces (FP64) ------------------------------------------------
 
-int smooth64(pmg_problem *p, int L, int zero_init) {
+// nsweeps smoothing sweeps on level L (smooth_domain_sol,
+// PBE_pmgc_class.h:868-927): red-black on the finest level, eight-colour
+// (two-launch tiled, ping-pong through xalt) below. Every call uses an even
+// number of sweeps, so x ends in its own buffer.
+int smooth64(pmg_problem *p, int L, int nsweeps, int zero_init) {
   LevelBuf &v = p->lv[L];
   if (L == p->nlev)
     return launch_gs7<double>(v.d, v.op[kOC], nullptr, v.f, v.op[kOE],
-                              v.op[kON], v.op[kUC], v.x, 1, 0, zero_init,
-                              p->stream);
-  return launch_gs27<double>(v.d, v.A64(14), nullptr, v.f, v.x, 1, 0,
-                             zero_init, p->stream);
+                              v.op[kON], v.op[kUC], v.x, nsweeps, 0,
+                              zero_init, p->stream);
+  double *res = nullptr;
+  int rc = launch_gs27_pp<double>(v.d, v.A64(14), nullptr, v.f, v.x, v.xalt,
+                                  nsweeps, 0, zero_init, p->stream, &res);
+  if (rc == PMG_OK && res != v.x) {
+    set_last_message("smooth64: odd sweep count");
+    return PMG_ERR_STATE;
+  }
+  return rc;
 }
 
 // Coarsest level: the class's CG (absolute 1e-8, first test on
@@ -180,12 +196,9 @@ int vcycle64(pmg_problem *p, int L, int as_preconditioner) {
   LevelBuf &c = p->lv[L - 1];
   const int kind = L == p->nlev ? 7 : 27;
   int rc;
-  int zero_init = (L != p->nlev) || as_preconditioner;
-  for (int it = 0; it < 2; ++it) {
-    if ((rc = smooth64(p, L, zero_init)))
-      return rc;
-    zero_init = 0;
-  }
+  const int zero_init = (L != p->nlev) || as_preconditioner;
+  if ((rc = smooth64(p, L, 2, zero_init)))
+    return rc;
   if (kind == 7)
     defect_kernel<7, double><<<interior_grid(v.d), interior_block(), 0, s>>>(
         v.d, v.A64(4), v.f, v.x, v.r);
@@ -205,10 +218,7 @@ int vcycle64(pmg_problem *p, int L, int as_preconditioner) {
   axpy_full_kernel<double><<<flat_grid(v.n3), 256, 0, s>>>(v.n3, v.x, v.r,
                                                            c.omega);
   PMG_LAUNCH_CHECK();
-  for (int it = 0; it < 2; ++it)
-    if ((rc = smooth64(p, L, 0)))
-      return rc;
-  return PMG_OK;
+  return smooth64(p, L, 2, 0);
 }
 
 // Residual sum of squares of the finest level into red_norm.result[0] and
@@ -232,14 +242,21 @@ double norm_from_sum(const pmg_problem *p, double s) {
 
 // ---- mixed precision -------------------------------------------------------
 
-int smooth32(pmg_problem *p, int L, int zero_init) {
+int smooth32(pmg_problem *p, int L, int nsweeps, int zero_init) {
   LevelBuf &v = p->lv[L];
   if (L == p->nlev)
     return launch_gs7<float>(v.d, v.op32[kOC], nullptr, v.f32, v.op32[kOE],
-                             v.op32[kON], v.op32[kUC], v.x32, 1, 0, zero_init,
-                             p->stream);
-  return launch_gs27<float>(v.d, v.A32(14), nullptr, v.f32, v.x32, 1, 0,
-                            zero_init, p->stream);
+                             v.op32[kON], v.op32[kUC], v.x32, nsweeps, 0,
+                             zero_init, p->stream);
+  float *res = nullptr;
+  int rc = launch_gs27_pp<float>(v.d, v.A32(14), nullptr, v.f32, v.x32,
+                                 v.xalt32, nsweeps, 0, zero_init, p->stream,
+                                 &res);
+  if (rc == PMG_OK && res != v.x32) {
+    set_last_message("smooth32: odd sweep count");
+    return PMG_ERR_STATE;
+  }
+  return rc;
 }
 
 // V-cycle in float on the correction equation, every level zero-started
@@ -257,9 +274,7 @@ int vcycle32(pmg_problem *p, int L) {
   LevelBuf &c = p->lv[L - 1];
   const int kind = L == p->nlev ? 7 : 27;
   int rc;
-  if ((rc = smooth32(p, L, 1)))
-    return rc;
-  if ((rc = smooth32(p, L, 0)))
+  if ((rc = smooth32(p, L, 2, 1)))
     return rc;
   if (kind == 7)
     defect_kernel<7, float><<<interior_grid(v.d), interior_block(), 0, s>>>(
@@ -287,10 +302,7 @@ int vcycle32(pmg_problem *p, int L) {
   axpy_full_kernel<float><<<flat_grid(v.n3), 256, 0, s>>>(v.n3, v.x32, v.r32,
                                                           c.omega);
   PMG_LAUNCH_CHECK();
-  for (int it = 0; it < 2; ++it)
-    if ((rc = smooth32(p, L, 0)))
-      return rc;
-  return PMG_OK;
+  return smooth32(p, L, 2, 0);
 }
 
 // r64 = f - A x64 on the finest level, written as float into f32 (the

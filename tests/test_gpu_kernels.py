@@ -157,7 +157,7 @@ def test_builders_bitexact_vs_restatement(restatement, nf):
             assert np.array_equal(H(out[s]), oo[s]), (kind, s)
 
 
-@pytest.mark.parametrize("n", [17, 33, 65])
+@pytest.mark.parametrize("n", [17, 33, 65, 97])
 def test_smoothers_bitexact_large(restatement, n):
     c = rand_case(n, 100 + n)
     for iad, zi in ((0, 0), (1, 1)):
