@@ -317,6 +317,18 @@ int pmg_get_level(pmg_problem *p, int level, double *dst);
  * class's absolute 1e-8 test). */
 int pmg_problem_set_coarse_rtol(pmg_problem *p, double rtol);
 
+/* Phase timing: with on != 0, pmg_solve records CUDA events around every
+ * phase of every cycle (inside the captured cycle graph) and accumulates the
+ * elapsed times. */
+int pmg_problem_set_profiling(pmg_problem *p, int on);
+/* Accumulated phase times (ms) and counts; slot = level * 8 + phase with
+ * phase 0 pre-smoothing, 1 defect, 2 restriction, 3 coarsest solve,
+ * 4 damping, 5 interpolation, 6 x += w e, 7 post-smoothing; level 0 holds
+ * 0 finest-level residual norm, 1 refinement update. Returns the number of
+ * slots; reset != 0 clears the accumulators. */
+int pmg_problem_profile(pmg_problem *p, double *ms, long long *counts,
+                        int cap, int reset);
+
 /* The class's stream (for callers that enqueue around a solve). */
 pmg_stream_t pmg_problem_stream(pmg_problem *p);
 

@@ -9,6 +9,7 @@
 
 #include "build_kernels.cuh"
 #include "gs27_tiled.cuh"
+#include "gs7_fused.cuh"
 #include "launch.cuh"
 #include "reduce_kernels.cuh"
 
@@ -16,6 +17,7 @@ namespace pmg {
 
 constexpr int kMaxLevels = 12;
 constexpr int kCgMaxIters = 20000;
+constexpr int kProfSlots = 8 * (kMaxLevels + 1);
 
 struct LevelBuf {
   int n = 0;
@@ -92,6 +94,12 @@ struct pmg_problem {
   bool fine_set = false, built = false;
   // One V-cycle (plus the residual norm) captured as a CUDA graph.
   cudaGraphExec_t cycle_exec = nullptr;
+  // phase timing (pmg_problem_set_profiling)
+  bool prof_on = false;
+  cudaEvent_t prof_ev[2][kProfSlots] = {};
+  bool prof_used[kProfSlots] = {};
+  double prof_ms[kProfSlots] = {};
+  long prof_count[kProfSlots] = {};
 };
 
 namespace {
@@ -119,8 +127,9 @@ void plan(pmg_problem *p, Arena &a) {
     v.x = need64 ? a.take<double>(v.n3) : nullptr;
     v.f = need64 ? a.take<double>(v.n3) : nullptr;
     v.r = (mixed && L > 1) ? nullptr : a.take<double>(v.n3);
-    const bool smooth27 = !fine && L > 1;
-    v.xalt = (smooth27 && !mixed) ? a.take<double>(v.n3) : nullptr;
+    // ping-pong partners of the smoothers (levels 2 .. nlev)
+    const bool smoothed = L > 1;
+    v.xalt = (smoothed && !mixed) ? a.take<double>(v.n3) : nullptr;
     v.omega = a.take<double>(1);
     if (mixed) {
       for (int s = 0; s < 14; ++s)
@@ -130,7 +139,7 @@ void plan(pmg_problem *p, Arena &a) {
       v.x32 = a.take<float>(v.n3);
       v.f32 = a.take<float>(v.n3);
       v.r32 = L > 1 ? a.take<float>(v.n3) : nullptr;
-      v.xalt32 = smooth27 ? a.take<float>(v.n3) : nullptr;
+      v.xalt32 = smoothed ? a.take<float>(v.n3) : nullptr;
     }
   }
   const long n1 = p->lv[1].n3;
@@ -153,26 +162,56 @@ int check_shape(int base, int nlev) {
   return PMG_OK;
 }
 
+// ---- phase timing ------------------------------------------------------------
+// Optional CUDA-event timing of every V-cycle phase, recorded inside the
+// captured cycle graph. Slot = level * 8 + phase; level 0 holds the
+// finest-level residual (0), the refinement update (1) and conversions (2).
+enum Phase {
+  kPhPre = 0, kPhDefect, kPhRestrict, kPhCoarse, kPhLambda, kPhInterp,
+  kPhAxpy, kPhPost
+};
+enum GlobalPhase { kPhResidual = 0, kPhCorrect = 1, kPhConvert = 2 };
+
+void prof_begin(pmg_problem *p, int slot) {
+  if (p->prof_on)
+    cudaEventRecord(p->prof_ev[0][slot], p->stream);
+}
+void prof_end(pmg_problem *p, int slot) {
+  if (p->prof_on) {
+    cudaEventRecord(p->prof_ev[1][slot], p->stream);
+    p->prof_used[slot] = true;
+  }
+}
+void prof_collect(pmg_problem *p) {
+  if (!p->prof_on)
+    return;
+  for (int q = 0; q < kProfSlots; ++q)
+    if (p->prof_used[q]) {
+      float ms = 0.f;
+      if (cudaEventElapsedTime(&ms, p->prof_ev[0][q], p->prof_ev[1][q]) ==
+          cudaSuccess) {
+        p->prof_ms[q] += ms;
+        p->prof_count[q] += 1;
+      }
+    }
+}
+
 // ---- V-cycle pieces (FP64) ------------------------------------------------
 
 // nsweeps smoothing sweeps on level L (smooth_domain_sol,
-// PBE_pmgc_class.h:868-927): red-black on the finest level, eight-colour
-// (two-launch tiled, ping-pong through xalt) below. Every call uses an even
-// number of sweeps, so x ends in its own buffer.
-int smooth64(pmg_problem *p, int L, int nsweeps, int zero_init) {
+// PBE_pmgc_class.h:868-927): fused red-black on the finest level, two-launch
+// eight-colour below; both ping-pong between x and xalt. *cur is the buffer
+// holding the iterate on entry and on return.
+int smooth64(pmg_problem *p, int L, int nsweeps, int zero_init,
+             double **cur) {
   LevelBuf &v = p->lv[L];
+  double *alt = *cur == v.x ? v.xalt : v.x;
   if (L == p->nlev)
-    return launch_gs7<double>(v.d, v.op[kOC], nullptr, v.f, v.op[kOE],
-                              v.op[kON], v.op[kUC], v.x, nsweeps, 0,
-                              zero_init, p->stream);
-  double *res = nullptr;
-  int rc = launch_gs27_pp<double>(v.d, v.A64(14), nullptr, v.f, v.x, v.xalt,
-                                  nsweeps, 0, zero_init, p->stream, &res);
-  if (rc == PMG_OK && res != v.x) {
-    set_last_message("smooth64: odd sweep count");
-    return PMG_ERR_STATE;
-  }
-  return rc;
+    return launch_gs7_fused<double>(v.d, v.op[kOC], nullptr, v.f, v.op[kOE],
+                                    v.op[kON], v.op[kUC], *cur, alt, nsweeps,
+                                    0, zero_init, p->stream, cur);
+  return launch_gs27_pp<double>(v.d, v.A64(14), nullptr, v.f, *cur, alt,
+                                nsweeps, 0, zero_init, p->stream, cur);
 }
 
 // Coarsest level: the class's CG (absolute 1e-8, first test on
@@ -188,46 +227,75 @@ int cg_level1(pmg_problem *p, const double *rhs, double *x) {
                          1e-8, 0.0, 1, kCgMaxIters, p->cg_status, p->stream);
 }
 
+// v_cycle of the class (PBE_pmgc_class.h:1070-1114) on level L.
 int vcycle64(pmg_problem *p, int L, int as_preconditioner) {
   cudaStream_t s = p->stream;
   LevelBuf &v = p->lv[L];
-  if (L == 1)
-    return cg_level1(p, v.f, v.x);
+  const int sl = L * 8;
+  if (L == 1) {
+    prof_begin(p, sl + kPhCoarse);
+    int rc = cg_level1(p, v.f, v.x);
+    prof_end(p, sl + kPhCoarse);
+    return rc;
+  }
   LevelBuf &c = p->lv[L - 1];
   const int kind = L == p->nlev ? 7 : 27;
   int rc;
+  double *x = v.x;
   const int zero_init = (L != p->nlev) || as_preconditioner;
-  if ((rc = smooth64(p, L, 2, zero_init)))
+  prof_begin(p, sl + kPhPre);
+  if ((rc = smooth64(p, L, 2, zero_init, &x)))
     return rc;
+  prof_end(p, sl + kPhPre);
+  prof_begin(p, sl + kPhDefect);
   if (kind == 7)
     defect_kernel<7, double><<<interior_grid(v.d), interior_block(), 0, s>>>(
-        v.d, v.A64(4), v.f, v.x, v.r);
+        v.d, v.A64(4), v.f, x, v.r);
   else
     defect_kernel<27, double><<<interior_grid(v.d), interior_block(), 0, s>>>(
-        v.d, v.A64(14), v.f, v.x, v.r);
+        v.d, v.A64(14), v.f, x, v.r);
+  prof_end(p, sl + kPhDefect);
+  prof_begin(p, sl + kPhRestrict);
   restrict_kernel<double, double>
       <<<interior_grid(c.d), interior_block(), 0, s>>>(v.d, c.d, v.r, c.f,
                                                        c.Pc());
+  prof_end(p, sl + kPhRestrict);
   PMG_LAUNCH_CHECK();
   if ((rc = vcycle64(p, L - 1, 0)))
     return rc;
+  prof_begin(p, sl + kPhLambda);
   ideal_lambda_kernel<double><<<kReduceBlocks, kReduceThreads, 0, s>>>(
       c.d, c.A64(14), c.x, c.f, p->red_lambda, c.omega);
+  prof_end(p, sl + kPhLambda);
+  prof_begin(p, sl + kPhInterp);
   interp_kernel<double><<<interp_grid(c.d), interior_block(), 0, s>>>(
       c.d, v.d, c.x, v.r, c.Pc());
-  axpy_full_kernel<double><<<flat_grid(v.n3), 256, 0, s>>>(v.n3, v.x, v.r,
+  prof_end(p, sl + kPhInterp);
+  prof_begin(p, sl + kPhAxpy);
+  axpy_full_kernel<double><<<flat_grid(v.n3), 256, 0, s>>>(v.n3, x, v.r,
                                                            c.omega);
+  prof_end(p, sl + kPhAxpy);
   PMG_LAUNCH_CHECK();
-  return smooth64(p, L, 2, 0);
+  prof_begin(p, sl + kPhPost);
+  if ((rc = smooth64(p, L, 2, 0, &x)))
+    return rc;
+  prof_end(p, sl + kPhPost);
+  if (x != v.x) {
+    set_last_message("vcycle64: iterate left the level's buffer");
+    return PMG_ERR_STATE;
+  }
+  return PMG_OK;
 }
 
 // Residual sum of squares of the finest level into red_norm.result[0] and
 // then into pinned host memory (not synchronised here).
 int residual_norm_async(pmg_problem *p) {
   LevelBuf &v = p->lv[p->nlev];
+  prof_begin(p, kPhResidual);
   defect_norm_kernel<7, double, double>
       <<<kReduceBlocks, kReduceThreads, 0, p->stream>>>(
           v.d, v.A64(4), v.f, v.x, (double *)nullptr, p->red_norm);
+  prof_end(p, kPhResidual);
   PMG_LAUNCH_CHECK();
   PMG_CUDA_TRY(cudaMemcpyAsync(p->h_pinned, p->red_norm.result,
                                sizeof(double), cudaMemcpyDeviceToHost,
@@ -242,21 +310,16 @@ double norm_from_sum(const pmg_problem *p, double s) {
 
 // ---- mixed precision -------------------------------------------------------
 
-int smooth32(pmg_problem *p, int L, int nsweeps, int zero_init) {
+int smooth32(pmg_problem *p, int L, int nsweeps, int zero_init, float **cur) {
   LevelBuf &v = p->lv[L];
+  float *alt = *cur == v.x32 ? v.xalt32 : v.x32;
   if (L == p->nlev)
-    return launch_gs7<float>(v.d, v.op32[kOC], nullptr, v.f32, v.op32[kOE],
-                             v.op32[kON], v.op32[kUC], v.x32, nsweeps, 0,
-                             zero_init, p->stream);
-  float *res = nullptr;
-  int rc = launch_gs27_pp<float>(v.d, v.A32(14), nullptr, v.f32, v.x32,
-                                 v.xalt32, nsweeps, 0, zero_init, p->stream,
-                                 &res);
-  if (rc == PMG_OK && res != v.x32) {
-    set_last_message("smooth32: odd sweep count");
-    return PMG_ERR_STATE;
-  }
-  return rc;
+    return launch_gs7_fused<float>(v.d, v.op32[kOC], nullptr, v.f32,
+                                   v.op32[kOE], v.op32[kON], v.op32[kUC],
+                                   *cur, alt, nsweeps, 0, zero_init,
+                                   p->stream, cur);
+  return launch_gs27_pp<float>(v.d, v.A32(14), nullptr, v.f32, *cur, alt,
+                               nsweeps, 0, zero_init, p->stream, cur);
 }
 
 // V-cycle in float on the correction equation, every level zero-started
@@ -265,29 +328,41 @@ int smooth32(pmg_problem *p, int L, int nsweeps, int zero_init) {
 int vcycle32(pmg_problem *p, int L) {
   cudaStream_t s = p->stream;
   LevelBuf &v = p->lv[L];
+  const int sl = L * 8;
   if (L == 1) {
+    prof_begin(p, sl + kPhCoarse);
     convert_kernel<float, double><<<flat_grid(v.n3), 256, 0, s>>>(v.n3, v.f32,
                                                                  v.f);
     PMG_CUDA_TRY(cudaMemsetAsync(v.x, 0, sizeof(double) * v.n3, s));
-    return cg_level1(p, v.f, v.x);
+    int rc = cg_level1(p, v.f, v.x);
+    prof_end(p, sl + kPhCoarse);
+    return rc;
   }
   LevelBuf &c = p->lv[L - 1];
   const int kind = L == p->nlev ? 7 : 27;
   int rc;
-  if ((rc = smooth32(p, L, 2, 1)))
+  float *x = v.x32;
+  prof_begin(p, sl + kPhPre);
+  if ((rc = smooth32(p, L, 2, 1, &x)))
     return rc;
+  prof_end(p, sl + kPhPre);
+  prof_begin(p, sl + kPhDefect);
   if (kind == 7)
     defect_kernel<7, float><<<interior_grid(v.d), interior_block(), 0, s>>>(
-        v.d, v.A32(4), v.f32, v.x32, v.r32);
+        v.d, v.A32(4), v.f32, x, v.r32);
   else
     defect_kernel<27, float><<<interior_grid(v.d), interior_block(), 0, s>>>(
-        v.d, v.A32(14), v.f32, v.x32, v.r32);
+        v.d, v.A32(14), v.f32, x, v.r32);
+  prof_end(p, sl + kPhDefect);
+  prof_begin(p, sl + kPhRestrict);
   restrict_kernel<float, float>
       <<<interior_grid(c.d), interior_block(), 0, s>>>(v.d, c.d, v.r32, c.f32,
                                                        c.Pc32());
+  prof_end(p, sl + kPhRestrict);
   PMG_LAUNCH_CHECK();
   if ((rc = vcycle32(p, L - 1)))
     return rc;
+  prof_begin(p, sl + kPhLambda);
   if (L - 1 == 1) {
     ideal_lambda_kernel<double><<<kReduceBlocks, kReduceThreads, 0, s>>>(
         c.d, c.A64(14), c.x, c.f, p->red_lambda, c.omega);
@@ -297,12 +372,25 @@ int vcycle32(pmg_problem *p, int L) {
     ideal_lambda_kernel<float><<<kReduceBlocks, kReduceThreads, 0, s>>>(
         c.d, c.A32(14), c.x32, c.f32, p->red_lambda, c.omega);
   }
+  prof_end(p, sl + kPhLambda);
+  prof_begin(p, sl + kPhInterp);
   interp_kernel<float><<<interp_grid(c.d), interior_block(), 0, s>>>(
       c.d, v.d, c.x32, v.r32, c.Pc32());
-  axpy_full_kernel<float><<<flat_grid(v.n3), 256, 0, s>>>(v.n3, v.x32, v.r32,
+  prof_end(p, sl + kPhInterp);
+  prof_begin(p, sl + kPhAxpy);
+  axpy_full_kernel<float><<<flat_grid(v.n3), 256, 0, s>>>(v.n3, x, v.r32,
                                                           c.omega);
+  prof_end(p, sl + kPhAxpy);
   PMG_LAUNCH_CHECK();
-  return smooth32(p, L, 2, 0);
+  prof_begin(p, sl + kPhPost);
+  if ((rc = smooth32(p, L, 2, 0, &x)))
+    return rc;
+  prof_end(p, sl + kPhPost);
+  if (x != v.x32) {
+    set_last_message("vcycle32: iterate left the level's buffer");
+    return PMG_ERR_STATE;
+  }
+  return PMG_OK;
 }
 
 // r64 = f - A x64 on the finest level, written as float into f32 (the
@@ -310,9 +398,11 @@ int vcycle32(pmg_problem *p, int L) {
 // and pinned host memory.
 int mixed_residual_async(pmg_problem *p) {
   LevelBuf &v = p->lv[p->nlev];
+  prof_begin(p, kPhResidual);
   defect_norm_kernel<7, double, float>
       <<<kReduceBlocks, kReduceThreads, 0, p->stream>>>(
           v.d, v.A64(4), v.f, v.x, v.f32, p->red_norm);
+  prof_end(p, kPhResidual);
   PMG_LAUNCH_CHECK();
   PMG_CUDA_TRY(cudaMemcpyAsync(p->h_pinned, p->red_norm.result,
                                sizeof(double), cudaMemcpyDeviceToHost,
@@ -327,8 +417,10 @@ int mixed_step(pmg_problem *p) {
   int rc;
   if ((rc = vcycle32(p, p->nlev)))
     return rc;
+  prof_begin(p, kPhCorrect);
   add_correction_kernel<<<interior_grid(v.d), interior_block(), 0,
                           p->stream>>>(v.d, v.x, v.x32);
+  prof_end(p, kPhCorrect);
   PMG_LAUNCH_CHECK();
   return mixed_residual_async(p);
 }
@@ -440,6 +532,10 @@ int pmg_problem_destroy(pmg_problem *p) {
     cudaStreamSynchronize(p->stream);
   if (p->cycle_exec)
     cudaGraphExecDestroy(p->cycle_exec);
+  for (int e = 0; e < 2; ++e)
+    for (int q = 0; q < kProfSlots; ++q)
+      if (p->prof_ev[e][q])
+        cudaEventDestroy(p->prof_ev[e][q]);
   if (p->arena)
     cudaFree(p->arena);
   if (p->h_pinned)
@@ -463,6 +559,40 @@ int pmg_problem_set_coarse_rtol(pmg_problem *p, double rtol) {
   return PMG_OK;
 }
 
+int pmg_problem_set_profiling(pmg_problem *p, int on) {
+  if (!p)
+    return PMG_ERR_ARG;
+  if (on && !p->prof_ev[0][0]) {
+    for (int e = 0; e < 2; ++e)
+      for (int q = 0; q < kProfSlots; ++q)
+        PMG_CUDA_TRY(cudaEventCreate(&p->prof_ev[e][q]));
+  }
+  if ((bool)on != p->prof_on && p->cycle_exec) {
+    cudaGraphExecDestroy(p->cycle_exec);
+    p->cycle_exec = nullptr;
+  }
+  p->prof_on = on != 0;
+  return PMG_OK;
+}
+
+int pmg_problem_profile(pmg_problem *p, double *ms, long long *counts,
+                        int cap, int reset) {
+  if (!p)
+    return PMG_ERR_ARG;
+  for (int q = 0; q < kProfSlots && q < cap; ++q) {
+    if (ms)
+      ms[q] = p->prof_ms[q];
+    if (counts)
+      counts[q] = p->prof_count[q];
+  }
+  if (reset)
+    for (int q = 0; q < kProfSlots; ++q) {
+      p->prof_ms[q] = 0.0;
+      p->prof_count[q] = 0;
+    }
+  return kProfSlots;
+}
+
 pmg_stream_t pmg_problem_stream(pmg_problem *p) {
   return p ? (pmg_stream_t)p->stream : nullptr;
 }
@@ -481,6 +611,10 @@ int pmg_problem_set_fine(pmg_problem *p, const double *oC, const double *oE,
   for (int q = 0; q < 6; ++q)
     PMG_CUDA_TRY(
         cudaMemcpyAsync(dst[q], src[q], b, cudaMemcpyDefault, p->stream));
+  // the smoother's ping-pong partner carries the same Dirichlet shell
+  if (v.xalt)
+    PMG_CUDA_TRY(cudaMemcpyAsync(v.xalt, v.x, b, cudaMemcpyDeviceToDevice,
+                                 p->stream));
   p->fine_set = true;
   p->built = false;
   return PMG_OK;
@@ -594,6 +728,7 @@ int pmg_solve(pmg_problem *p, double tol, int max_cycles, int *cycles,
   while (c < max_cycles && r0 > 0.0) {
     PMG_CUDA_TRY(cudaGraphLaunch(p->cycle_exec, p->stream));
     PMG_CUDA_TRY(cudaStreamSynchronize(p->stream));
+    prof_collect(p);
     ++c;
     r = norm_from_sum(p, p->h_pinned[0]);
     if (hist)

@@ -167,6 +167,33 @@ class PBELinearProblem:
         _lib.check("pmg_problem_set_coarse_rtol",
                    _lib.lib.pmg_problem_set_coarse_rtol(self._h, float(rtol)))
 
+    PHASES = ("pre-smooth", "defect", "restrict", "coarse-solve", "damping",
+              "interp", "axpy", "post-smooth")
+    GLOBAL_PHASES = ("residual", "refine-update")
+
+    def set_profiling(self, on: bool = True) -> None:
+        """Time every cycle phase with CUDA events inside the cycle graph."""
+        _lib.check("pmg_problem_set_profiling",
+                   _lib.lib.pmg_problem_set_profiling(self._h, int(on)))
+
+    def profile(self, reset: bool = False) -> dict:
+        """{(level, phase): (total ms, launches)} accumulated by solve();
+        level 0 holds the finest-level residual and refinement update."""
+        cap = 8 * 13
+        ms = np.zeros(cap)
+        cnt = np.zeros(cap, dtype=np.int64)
+        n = _lib.lib.pmg_problem_profile(
+            self._h, _dptr(ms), cnt.ctypes.data_as(
+                ctypes.POINTER(ctypes.c_longlong)), cap, int(reset))
+        out = {}
+        for q in range(min(n, cap)):
+            if cnt[q]:
+                L, ph = divmod(q, 8)
+                name = (self.GLOBAL_PHASES[ph] if L == 0 and ph < 2
+                        else self.PHASES[ph])
+                out[(L, name)] = (float(ms[q]), int(cnt[q]))
+        return out
+
     # -- multigrid ------------------------------------------------------------
     def buildmultilevelops(self, trilinear: bool = False) -> None:
         """Galerkin hierarchy (PBE_pmgc_class.h:351-617)."""
