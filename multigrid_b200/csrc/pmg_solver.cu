@@ -172,13 +172,17 @@ enum Phase {
 };
 enum GlobalPhase { kPhResidual = 0, kPhCorrect = 1, kPhConvert = 2 };
 
+// Inside stream capture a plain cudaEventRecord only orders work; the
+// external flag makes the captured node record the event for timing.
 void prof_begin(pmg_problem *p, int slot) {
   if (p->prof_on)
-    cudaEventRecord(p->prof_ev[0][slot], p->stream);
+    cudaEventRecordWithFlags(p->prof_ev[0][slot], p->stream,
+                             cudaEventRecordExternal);
 }
 void prof_end(pmg_problem *p, int slot) {
   if (p->prof_on) {
-    cudaEventRecord(p->prof_ev[1][slot], p->stream);
+    cudaEventRecordWithFlags(p->prof_ev[1][slot], p->stream,
+                             cudaEventRecordExternal);
     p->prof_used[slot] = true;
   }
 }
@@ -194,6 +198,8 @@ void prof_collect(pmg_problem *p) {
         p->prof_count[q] += 1;
       }
     }
+  // a failed query must not surface as the next launch's error
+  (void)cudaGetLastError();
 }
 
 // ---- V-cycle pieces (FP64) ------------------------------------------------
