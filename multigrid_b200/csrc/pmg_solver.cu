@@ -173,16 +173,23 @@ enum Phase {
 enum GlobalPhase { kPhResidual = 0, kPhCorrect = 1, kPhConvert = 2 };
 
 // Inside stream capture a plain cudaEventRecord only orders work; the
-// external flag makes the captured node record the event for timing.
+// external flag (valid only while capturing) makes the captured node record
+// the event for timing.
+void prof_record(pmg_problem *p, cudaEvent_t ev) {
+  cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+  cudaStreamIsCapturing(p->stream, &st);
+  if (st == cudaStreamCaptureStatusActive)
+    cudaEventRecordWithFlags(ev, p->stream, cudaEventRecordExternal);
+  else
+    cudaEventRecord(ev, p->stream);
+}
 void prof_begin(pmg_problem *p, int slot) {
   if (p->prof_on)
-    cudaEventRecordWithFlags(p->prof_ev[0][slot], p->stream,
-                             cudaEventRecordExternal);
+    prof_record(p, p->prof_ev[0][slot]);
 }
 void prof_end(pmg_problem *p, int slot) {
   if (p->prof_on) {
-    cudaEventRecordWithFlags(p->prof_ev[1][slot], p->stream,
-                             cudaEventRecordExternal);
+    prof_record(p, p->prof_ev[1][slot]);
     p->prof_used[slot] = true;
   }
 }
