@@ -5,7 +5,6 @@
 
 #include "build_kernels.cuh"
 #include "gs27_tiled.cuh"
-#include "gs7_fused.cuh"
 #include "launch.cuh"
 #include "reduce_kernels.cuh"
 
@@ -272,35 +271,6 @@ static int gs27_inplace(const Dims &d, const Op14<T> &A, const T *cc,
   return rc;
 }
 
-// itmax red-black sweeps in place on x with the fused kernel (two sweeps per
-// launch); the ping-pong partner is a stream-ordered copy of x.
-template <typename T>
-static int gs7_inplace(const Dims &d, const T *oC, const T *cc, const T *fc,
-                       const T *oE, const T *oN, const T *uC, T *x,
-                       int itmax, int iadjoint, int zero_init,
-                       cudaStream_t s) {
-  if (itmax == 0)
-    return PMG_OK;
-  T *alt = nullptr;
-  const size_t bytes = sizeof(T) * d.count();
-  PMG_CUDA_TRY(cudaMallocAsync((void **)&alt, bytes, s));
-  int rc = PMG_OK;
-  cudaError_t e = cudaMemcpyAsync(alt, x, bytes, cudaMemcpyDeviceToDevice, s);
-  if (e == cudaSuccess) {
-    T *res = nullptr;
-    rc = launch_gs7_fused<T>(d, oC, cc, fc, oE, oN, uC, x, alt, itmax,
-                             iadjoint, zero_init, s, &res);
-    if (rc == PMG_OK && res != x)
-      e = cudaMemcpyAsync(x, res, bytes, cudaMemcpyDeviceToDevice, s);
-  }
-  cudaFreeAsync(alt, s);
-  if (e != cudaSuccess) {
-    set_last_error(e, "Vgsrb7x", __FILE__, __LINE__);
-    return PMG_ERR_CUDA;
-  }
-  return rc;
-}
-
 // ---------------------------------------------------------------------------
 // C ABI
 // ---------------------------------------------------------------------------
@@ -313,8 +283,8 @@ const char *pmg_version(void) { return "pmg_b200 0.1 (sm_100a)"; }
   PMG_REQUIRE(!bad_dims(nx, ny, nz), "Vgsrb7x: grid size out of range");       \
   PMG_REQUIRE(oC && fc && oE && oN && uC && x, "Vgsrb7x: null array");         \
   PMG_REQUIRE(itmax >= 0, "Vgsrb7x: itmax < 0");                               \
-  return gs7_inplace<T>(Dims{nx, ny, nz}, oC, cc, fc, oE, oN, uC, x, itmax,   \
-                        iadjoint, zero_init, (cudaStream_t)stream);
+  return launch_gs7<T>(Dims{nx, ny, nz}, oC, cc, fc, oE, oN, uC, x, itmax,    \
+                       iadjoint, zero_init, (cudaStream_t)stream);
 
 int pmg_Vgsrb7x_d(int nx, int ny, int nz, const double *oC, const double *cc,
                   const double *fc, const double *oE, const double *oN,

@@ -9,7 +9,6 @@
 
 #include "build_kernels.cuh"
 #include "gs27_tiled.cuh"
-#include "gs7_fused.cuh"
 #include "launch.cuh"
 #include "reduce_kernels.cuh"
 
@@ -127,8 +126,8 @@ void plan(pmg_problem *p, Arena &a) {
     v.x = need64 ? a.take<double>(v.n3) : nullptr;
     v.f = need64 ? a.take<double>(v.n3) : nullptr;
     v.r = (mixed && L > 1) ? nullptr : a.take<double>(v.n3);
-    // ping-pong partners of the smoothers (levels 2 .. nlev)
-    const bool smoothed = L > 1;
+    // ping-pong partners of the eight-colour smoother (levels 2 .. nlev-1)
+    const bool smoothed = L > 1 && !fine;
     v.xalt = (smoothed && !mixed) ? a.take<double>(v.n3) : nullptr;
     v.omega = a.take<double>(1);
     if (mixed) {
@@ -212,17 +211,17 @@ void prof_collect(pmg_problem *p) {
 // ---- V-cycle pieces (FP64) ------------------------------------------------
 
 // nsweeps smoothing sweeps on level L (smooth_domain_sol,
-// PBE_pmgc_class.h:868-927): fused red-black on the finest level, two-launch
-// eight-colour below; both ping-pong between x and xalt. *cur is the buffer
-// holding the iterate on entry and on return.
+// PBE_pmgc_class.h:868-927): red-black in place on the finest level,
+// two-launch eight-colour (ping-pong between x and xalt) below. *cur is the
+// buffer holding the iterate on entry and on return.
 int smooth64(pmg_problem *p, int L, int nsweeps, int zero_init,
              double **cur) {
   LevelBuf &v = p->lv[L];
-  double *alt = *cur == v.x ? v.xalt : v.x;
   if (L == p->nlev)
-    return launch_gs7_fused<double>(v.d, v.op[kOC], nullptr, v.f, v.op[kOE],
-                                    v.op[kON], v.op[kUC], *cur, alt, nsweeps,
-                                    0, zero_init, p->stream, cur);
+    return launch_gs7<double>(v.d, v.op[kOC], nullptr, v.f, v.op[kOE],
+                              v.op[kON], v.op[kUC], *cur, nsweeps, 0,
+                              zero_init, p->stream);
+  double *alt = *cur == v.x ? v.xalt : v.x;
   return launch_gs27_pp<double>(v.d, v.A64(14), nullptr, v.f, *cur, alt,
                                 nsweeps, 0, zero_init, p->stream, cur);
 }
@@ -325,12 +324,11 @@ double norm_from_sum(const pmg_problem *p, double s) {
 
 int smooth32(pmg_problem *p, int L, int nsweeps, int zero_init, float **cur) {
   LevelBuf &v = p->lv[L];
-  float *alt = *cur == v.x32 ? v.xalt32 : v.x32;
   if (L == p->nlev)
-    return launch_gs7_fused<float>(v.d, v.op32[kOC], nullptr, v.f32,
-                                   v.op32[kOE], v.op32[kON], v.op32[kUC],
-                                   *cur, alt, nsweeps, 0, zero_init,
-                                   p->stream, cur);
+    return launch_gs7<float>(v.d, v.op32[kOC], nullptr, v.f32, v.op32[kOE],
+                             v.op32[kON], v.op32[kUC], *cur, nsweeps, 0,
+                             zero_init, p->stream);
+  float *alt = *cur == v.x32 ? v.xalt32 : v.x32;
   return launch_gs27_pp<float>(v.d, v.A32(14), nullptr, v.f32, *cur, alt,
                                nsweeps, 0, zero_init, p->stream, cur);
 }
@@ -624,10 +622,6 @@ int pmg_problem_set_fine(pmg_problem *p, const double *oC, const double *oE,
   for (int q = 0; q < 6; ++q)
     PMG_CUDA_TRY(
         cudaMemcpyAsync(dst[q], src[q], b, cudaMemcpyDefault, p->stream));
-  // the smoother's ping-pong partner carries the same Dirichlet shell
-  if (v.xalt)
-    PMG_CUDA_TRY(cudaMemcpyAsync(v.xalt, v.x, b, cudaMemcpyDeviceToDevice,
-                                 p->stream));
   p->fine_set = true;
   p->built = false;
   return PMG_OK;

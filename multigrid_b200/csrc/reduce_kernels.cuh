@@ -12,7 +12,7 @@
 
 namespace pmg {
 
-constexpr int kReduceBlocks = 296; // 2 per SM on 148 SMs
+constexpr int kReduceBlocks = 592; // 4 per SM on 148 SMs
 constexpr int kReduceThreads = 256;
 
 // Device scratch of one reduction site: partials[kReduceBlocks * NV],
@@ -72,25 +72,28 @@ __device__ void reduce_finish(const double (&v)[NV], ReduceSlot s,
 
 // sum over the interior of (f - A x)^2 with the defect of the class
 // (f - map(x), Convolution.h:137-139 and 170-175); optionally stores the
-// defect (cast to Tout) into r. Accumulates in double.
+// defect (cast to Tout) into r. Accumulates in double. Blocks take interior
+// rows (j, k) round robin, threads run along i (coalesced).
 template <int KIND, typename T, typename Tout>
 __global__ void __launch_bounds__(kReduceThreads)
     defect_norm_kernel(Dims d, Op14<T> A, const T *__restrict__ f,
                        const T *__restrict__ x, Tout *__restrict__ r,
                        ReduceSlot s) {
   __shared__ double sh[32];
-  const int m = (d.nx - 2) * (d.ny - 2) * (d.nz - 2);
+  const int my = d.ny - 2, rows = my * (d.nz - 2);
   const int sy = d.sy(), sz = d.sz();
   double acc = 0.0;
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < m;
-       q += gridDim.x * blockDim.x) {
-    int i, j, k;
-    interior_coords(d, q, i, j, k);
-    const int p = d.at(i, j, k);
-    const T dv = f[p] - apply_op<KIND>(A, (const T *)nullptr, x, p, sy, sz);
-    if (r)
-      r[p] = (Tout)dv;
-    acc += (double)dv * (double)dv;
+  for (int row = blockIdx.x; row < rows; row += gridDim.x) {
+    const int kk = row / my;
+    const int j = row - kk * my + 2, k = kk + 2;
+    for (int i = threadIdx.x + 2; i <= d.nx - 1; i += blockDim.x) {
+      const int p = d.at(i, j, k);
+      const T dv =
+          f[p] - apply_op<KIND>(A, (const T *)nullptr, x, p, sy, sz);
+      if (r)
+        r[p] = (Tout)dv;
+      acc += (double)dv * (double)dv;
+    }
   }
   double v[1] = {block_sum(acc, sh)};
   reduce_finish<1>(v, s, nullptr);
@@ -118,17 +121,18 @@ __global__ void __launch_bounds__(kReduceThreads)
                         const T *__restrict__ r, ReduceSlot s,
                         double *__restrict__ w) {
   __shared__ double sh[32];
-  const int m = (d.nx - 2) * (d.ny - 2) * (d.nz - 2);
+  const int my = d.ny - 2, rows = my * (d.nz - 2);
   const int sy = d.sy(), sz = d.sz();
   double up = 0.0, lo = 0.0;
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < m;
-       q += gridDim.x * blockDim.x) {
-    int i, j, k;
-    interior_coords(d, q, i, j, k);
-    const int p = d.at(i, j, k);
-    up += (double)r[p] * (double)x[p];
-    lo += (double)x[p] *
-          (double)apply27(A, (const T *)nullptr, x, p, sy, sz);
+  for (int row = blockIdx.x; row < rows; row += gridDim.x) {
+    const int kk = row / my;
+    const int j = row - kk * my + 2, k = kk + 2;
+    for (int i = threadIdx.x + 2; i <= d.nx - 1; i += blockDim.x) {
+      const int p = d.at(i, j, k);
+      up += (double)r[p] * (double)x[p];
+      lo += (double)x[p] *
+            (double)apply27(A, (const T *)nullptr, x, p, sy, sz);
+    }
   }
   double v[2];
   v[0] = block_sum(up, sh);

@@ -51,7 +51,7 @@ def levels_for(n: int, max_levels: int = 6, min_coarse: int = 5):
     n = base * 2^nlev + 1 and a coarsest grid of at least min_coarse
     points."""
     for L in range(max_levels, 1, -1):
-        if (n - 1) % (1 << L) == 0:
+        if (n - 1) % (1 << L) == 0 and (n - 1) >> L >= 1:
             base = (n - 1) >> L
             if 2 * base + 1 >= min_coarse:
                 return base, L

@@ -16,7 +16,7 @@ import dataclasses
 import numpy as np
 
 from . import _lib
-from .molecule import REFERENCE_PHYSICS, grid_step, level_n
+from .molecule import REFERENCE_PHYSICS, grid_step, level_n, levels_for
 
 
 def physics_struct(physics: dict) -> _lib.PmgPhysics:
@@ -72,7 +72,20 @@ class PBELinearProblem:
 
     def __init__(self, base: int, nlev: int, box: float,
                  precision: str = "fp64", physics: dict | None = None,
-                 stream: int | None = None):
+                 stream: int | None = None, hierarchy: str | None = None):
+        """hierarchy: "reference" keeps the class's levels (base * 2^L + 1,
+        L = 1..nlev); "deep" coarsens the same finest grid as far as a 5^3
+        coarsest level allows (levels_for), which makes the coarsest CG
+        cheap. Default: "reference" for fp64 (parity with the reference),
+        "deep" for mixed."""
+        n = level_n(int(base), int(nlev))
+        if hierarchy is None:
+            hierarchy = "deep" if precision == "mixed" else "reference"
+        if hierarchy == "deep":
+            base, nlev = levels_for(n, max_levels=12, min_coarse=5)
+        elif hierarchy != "reference":
+            raise ValueError(f"unknown hierarchy {hierarchy!r}")
+        self.hierarchy = hierarchy
         self.base, self.nlev, self.box = int(base), int(nlev), float(box)
         self.n = level_n(self.base, self.nlev)
         self.grid_step = grid_step(self.base, self.nlev, self.box)
