@@ -107,6 +107,29 @@ template <typename T> __device__ __forceinline__ T block_sum(T v, T *sh) {
   return v;
 }
 
+// block_sum for 2-D blocks (threads numbered x-fastest); result in the
+// first thread.
+template <typename T> __device__ __forceinline__ T block_sum_2d(T v, T *sh) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
+    v += __shfl_down_sync(0xffffffffu, v, o);
+  const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+  const int nt = blockDim.x * blockDim.y;
+  const int lane = tid & 31, w = tid >> 5;
+  __syncthreads();
+  if (lane == 0)
+    sh[w] = v;
+  __syncthreads();
+  const int nw = (nt + 31) >> 5;
+  v = (tid < nw) ? sh[tid] : T(0);
+  if (w == 0) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+      v += __shfl_down_sync(0xffffffffu, v, o);
+  }
+  return v;
+}
+
 } // namespace pmg
 
 // Host-side error plumbing: every entry point returns a pmg_status.

@@ -12,11 +12,12 @@
 
 namespace pmg {
 
-constexpr int kReduceBlocks = 592; // 4 per SM on 148 SMs
 constexpr int kReduceThreads = 256;
+// Interior reductions launch one thread per point (interior_grid, blocks of
+// 32 x 8) and keep one partial sum per block and reduced quantity.
 
-// Device scratch of one reduction site: partials[kReduceBlocks * NV],
-// ticket counter (zero between uses), result[NV].
+// Device scratch of one reduction site: partials[blocks * NV], ticket
+// counter (zero between uses), result[NV].
 struct ReduceSlot {
   double *partials;
   unsigned int *ticket;
@@ -37,18 +38,27 @@ __device__ __forceinline__ void interior_coords(const Dims &d, int q, int &i,
 // computed its block sums v[] (valid in thread 0). The last block sums all
 // partials in block order and writes result[]; when ratio != nullptr it also
 // stores result[0] / result[1] there (NV == 2).
+// Finishes a reduction of NV values: called by every block after it has
+// computed its block sums v[] (valid in thread 0). The last block sums all
+// partials in block order and writes result[]; when ratio != nullptr it also
+// stores result[0] / result[1] there (NV == 2).
 template <int NV>
 __device__ void reduce_finish(const double (&v)[NV], ReduceSlot s,
                               double *ratio) {
   __shared__ bool last;
   __shared__ double sh[32];
-  if (threadIdx.x == 0) {
+  const unsigned nb = gridDim.x * gridDim.y * gridDim.z;
+  const unsigned b = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y *
+                                                            blockIdx.z);
+  const unsigned tid = threadIdx.x + blockDim.x * threadIdx.y;
+  const unsigned nt = blockDim.x * blockDim.y;
+  if (tid == 0) {
 #pragma unroll
     for (int q = 0; q < NV; ++q)
-      s.partials[blockIdx.x * NV + q] = v[q];
+      s.partials[(size_t)b * NV + q] = v[q];
     __threadfence();
     const unsigned t = atomicAdd(s.ticket, 1u);
-    last = (t == gridDim.x - 1);
+    last = (t == nb - 1);
   }
   __syncthreads();
   if (!last)
@@ -57,13 +67,13 @@ __device__ void reduce_finish(const double (&v)[NV], ReduceSlot s,
 #pragma unroll
   for (int q = 0; q < NV; ++q) {
     double acc = 0.0;
-    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x)
-      acc += ((volatile double *)s.partials)[b * NV + q];
-    acc = block_sum(acc, sh);
-    if (threadIdx.x == 0)
+    for (unsigned k = tid; k < nb; k += nt)
+      acc += ((volatile double *)s.partials)[(size_t)k * NV + q];
+    acc = block_sum_2d(acc, sh);
+    if (tid == 0)
       s.result[q] = acc;
   }
-  if (threadIdx.x == 0) {
+  if (tid == 0) {
     if (ratio)
       *ratio = s.result[0] / s.result[1];
     *s.ticket = 0u;
@@ -72,30 +82,25 @@ __device__ void reduce_finish(const double (&v)[NV], ReduceSlot s,
 
 // sum over the interior of (f - A x)^2 with the defect of the class
 // (f - map(x), Convolution.h:137-139 and 170-175); optionally stores the
-// defect (cast to Tout) into r. Accumulates in double. Blocks take interior
-// rows (j, k) round robin, threads run along i (coalesced).
+// defect (cast to Tout) into r. Accumulates in double; one thread per
+// interior point (interior_grid).
 template <int KIND, typename T, typename Tout>
 __global__ void __launch_bounds__(kReduceThreads)
     defect_norm_kernel(Dims d, Op14<T> A, const T *__restrict__ f,
                        const T *__restrict__ x, Tout *__restrict__ r,
                        ReduceSlot s) {
   __shared__ double sh[32];
-  const int my = d.ny - 2, rows = my * (d.nz - 2);
-  const int sy = d.sy(), sz = d.sz();
+  const Interior t = interior_point(d);
   double acc = 0.0;
-  for (int row = blockIdx.x; row < rows; row += gridDim.x) {
-    const int kk = row / my;
-    const int j = row - kk * my + 2, k = kk + 2;
-    for (int i = threadIdx.x + 2; i <= d.nx - 1; i += blockDim.x) {
-      const int p = d.at(i, j, k);
-      const T dv =
-          f[p] - apply_op<KIND>(A, (const T *)nullptr, x, p, sy, sz);
-      if (r)
-        r[p] = (Tout)dv;
-      acc += (double)dv * (double)dv;
-    }
+  if (t.ok) {
+    const int p = d.at(t.i, t.j, t.k);
+    const T dv =
+        f[p] - apply_op<KIND>(A, (const T *)nullptr, x, p, d.sy(), d.sz());
+    if (r)
+      r[p] = (Tout)dv;
+    acc = (double)dv * (double)dv;
   }
-  double v[1] = {block_sum(acc, sh)};
+  double v[1] = {block_sum_2d(acc, sh)};
   reduce_finish<1>(v, s, nullptr);
 }
 
@@ -121,22 +126,17 @@ __global__ void __launch_bounds__(kReduceThreads)
                         const T *__restrict__ r, ReduceSlot s,
                         double *__restrict__ w) {
   __shared__ double sh[32];
-  const int my = d.ny - 2, rows = my * (d.nz - 2);
-  const int sy = d.sy(), sz = d.sz();
+  const Interior t = interior_point(d);
   double up = 0.0, lo = 0.0;
-  for (int row = blockIdx.x; row < rows; row += gridDim.x) {
-    const int kk = row / my;
-    const int j = row - kk * my + 2, k = kk + 2;
-    for (int i = threadIdx.x + 2; i <= d.nx - 1; i += blockDim.x) {
-      const int p = d.at(i, j, k);
-      up += (double)r[p] * (double)x[p];
-      lo += (double)x[p] *
-            (double)apply27(A, (const T *)nullptr, x, p, sy, sz);
-    }
+  if (t.ok) {
+    const int p = d.at(t.i, t.j, t.k);
+    up = (double)r[p] * (double)x[p];
+    lo = (double)x[p] *
+         (double)apply27(A, (const T *)nullptr, x, p, d.sy(), d.sz());
   }
   double v[2];
-  v[0] = block_sum(up, sh);
-  v[1] = block_sum(lo, sh);
+  v[0] = block_sum_2d(up, sh);
+  v[1] = block_sum_2d(lo, sh);
   reduce_finish<2>(v, s, w);
 }
 
