@@ -217,6 +217,21 @@ int pmg_cg_level_d(int nx, int ny, int nz, const double *const *a14,
                    const double *rhs, double *x, double thresh, int max_iters,
                    int *iters, pmg_stream_t stream);
 
+/* Same CG as pmg_cg_level_d, for callers that cannot let a library allocate
+ * device memory (an application that hands all device memory to its own
+ * pool, or must not meet allocator stalls or out-of-memory errors inside a
+ * time step). The work vectors live in a static device array of this
+ * library (about 118 KB, held by every GPU that loads the library until the
+ * process exits), so grids are limited to 17*17*17 points including the
+ * shell; larger grids return PMG_ERR_ARG. The first call on a device looks
+ * up the array's device address; make that first call before any stream
+ * capture. All calls on a device share the array: each call clears the part
+ * it uses, and calls that overlap on the GPU (e.g. on two streams) corrupt
+ * each other. Synchronises the stream. No counterpart in the reference. */
+int pmg_cg_level_noalloc_d(int nx, int ny, int nz, const double *const *a14,
+                           const double *rhs, double *x, double thresh,
+                           int max_iters, int *iters, pmg_stream_t stream);
+
 /* ======================================================================
  * Fine-level set-up from atoms (host)
  * ==================================================================== */

@@ -85,6 +85,8 @@ _sig("pmg_VbuildG_7_d", c_int, *([c_int] * 6 + [_PP, _V, _V, _V, _V, _PP, _V]))
 _sig("pmg_VbuildG_27_d", c_int, *([c_int] * 6 + [_PP, _PP, _PP, _V]))
 _sig("pmg_cg_level_d", c_int,
      *([c_int] * 3 + [_PP, _V, _V, c_double, c_int, PI, _V]))
+_sig("pmg_cg_level_noalloc_d", c_int,
+     *([c_int] * 3 + [_PP, _V, _V, c_double, c_int, PI, _V]))
 
 _sig("pmg_kappa", c_int, ctypes.POINTER(PmgPhysics), PD, PD)
 _sig("pmg_setup_fine", c_int, c_int, c_double, PD, c_int,

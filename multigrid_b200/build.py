@@ -18,7 +18,8 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(ROOT, "_build")
 LIB = os.path.join(HERE, "libpmg_b200.so")
 
-SOURCES = ["pmg_kernels.cu", "pmg_build.cu", "pmg_solver.cu", "pmg_setup.cc"]
+SOURCES = ["pmg_kernels.cu", "pmg_build.cu", "pmg_solver.cu", "pmg_setup.cc",
+           "pmg_noalloc.cu"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
