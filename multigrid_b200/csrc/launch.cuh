@@ -15,6 +15,10 @@ inline dim3 interior_block() { return dim3(32, 8, 1); }
 inline dim3 interior_grid(const Dims &d) {
   return dim3(cdiv(d.nx - 2, 32), cdiv(d.ny - 2, 8), (unsigned)(d.nz - 2));
 }
+// Reductions: one thread per interior column, 8 planes per block.
+inline dim3 reduce_grid(const Dims &d) {
+  return dim3(cdiv(d.nx - 2, 32), cdiv(d.ny - 2, 8), cdiv(d.nz - 2, 8));
+}
 // Interpolation: one thread per coarse cell (ii,jj,kk) in [1, n_c-1]^3.
 inline dim3 interp_grid(const Dims &dc) {
   return dim3(cdiv(dc.nx - 1, 32), cdiv(dc.ny - 1, 8), (unsigned)(dc.nz - 1));

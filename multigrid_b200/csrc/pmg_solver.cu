@@ -149,7 +149,7 @@ void plan(pmg_problem *p, Arena &a) {
   for (ReduceSlot *s : {&p->red_norm, &p->red_lambda}) {
     // partials of the largest interior launch
     const Dims &df = p->lv[p->nlev].d;
-    const dim3 g = interior_grid(df);
+    const dim3 g = reduce_grid(df);
     s->partials = a.take<double>(2L * g.x * g.y * g.z);
     s->ticket = a.take<unsigned int>(1);
     s->result = a.take<double>(2);
@@ -279,7 +279,7 @@ int vcycle64(pmg_problem *p, int L, int as_preconditioner) {
   if ((rc = vcycle64(p, L - 1, 0)))
     return rc;
   prof_begin(p, sl + kPhLambda);
-  ideal_lambda_kernel<double><<<interior_grid(c.d), interior_block(), 0, s>>>(
+  ideal_lambda_kernel<double><<<reduce_grid(c.d), interior_block(), 0, s>>>(
       c.d, c.A64(14), c.x, c.f, p->red_lambda, c.omega);
   prof_end(p, sl + kPhLambda);
   prof_begin(p, sl + kPhInterp);
@@ -308,7 +308,7 @@ int residual_norm_async(pmg_problem *p) {
   LevelBuf &v = p->lv[p->nlev];
   prof_begin(p, kPhResidual);
   defect_norm_kernel<7, double, double>
-      <<<interior_grid(v.d), interior_block(), 0, p->stream>>>(
+      <<<reduce_grid(v.d), interior_block(), 0, p->stream>>>(
           v.d, v.A64(4), v.f, v.x, (double *)nullptr, p->red_norm);
   prof_end(p, kPhResidual);
   PMG_LAUNCH_CHECK();
@@ -378,12 +378,12 @@ int vcycle32(pmg_problem *p, int L) {
     return rc;
   prof_begin(p, sl + kPhLambda);
   if (L - 1 == 1) {
-    ideal_lambda_kernel<double><<<interior_grid(c.d), interior_block(), 0, s>>>(
+    ideal_lambda_kernel<double><<<reduce_grid(c.d), interior_block(), 0, s>>>(
         c.d, c.A64(14), c.x, c.f, p->red_lambda, c.omega);
     convert_kernel<double, float><<<flat_grid(c.n3), 256, 0, s>>>(c.n3, c.x,
                                                                  c.x32);
   } else {
-    ideal_lambda_kernel<float><<<interior_grid(c.d), interior_block(), 0, s>>>(
+    ideal_lambda_kernel<float><<<reduce_grid(c.d), interior_block(), 0, s>>>(
         c.d, c.A32(14), c.x32, c.f32, p->red_lambda, c.omega);
   }
   prof_end(p, sl + kPhLambda);
@@ -414,7 +414,7 @@ int mixed_residual_async(pmg_problem *p) {
   LevelBuf &v = p->lv[p->nlev];
   prof_begin(p, kPhResidual);
   defect_norm_kernel<7, double, float>
-      <<<interior_grid(v.d), interior_block(), 0, p->stream>>>(
+      <<<reduce_grid(v.d), interior_block(), 0, p->stream>>>(
           v.d, v.A64(4), v.f, v.x, v.f32, p->red_norm);
   prof_end(p, kPhResidual);
   PMG_LAUNCH_CHECK();

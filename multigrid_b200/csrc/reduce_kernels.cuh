@@ -80,25 +80,35 @@ __device__ void reduce_finish(const double (&v)[NV], ReduceSlot s,
   }
 }
 
+// Reductions take one interior column (i, j) per thread and a run of
+// kReducePlanes planes per block (grid: reduce_grid), so each block's partial
+// covers enough points to amortise the final step.
+constexpr int kReducePlanes = 8;
+
 // sum over the interior of (f - A x)^2 with the defect of the class
 // (f - map(x), Convolution.h:137-139 and 170-175); optionally stores the
-// defect (cast to Tout) into r. Accumulates in double; one thread per
-// interior point (interior_grid).
+// defect (cast to Tout) into r. Accumulates in double.
 template <int KIND, typename T, typename Tout>
 __global__ void __launch_bounds__(kReduceThreads)
     defect_norm_kernel(Dims d, Op14<T> A, const T *__restrict__ f,
                        const T *__restrict__ x, Tout *__restrict__ r,
                        ReduceSlot s) {
   __shared__ double sh[32];
-  const Interior t = interior_point(d);
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
+  const int k0 = 2 + blockIdx.z * kReducePlanes;
+  const int k1 = min(k0 + kReducePlanes - 1, d.nz - 1);
+  const int sy = d.sy(), sz = d.sz();
   double acc = 0.0;
-  if (t.ok) {
-    const int p = d.at(t.i, t.j, t.k);
-    const T dv =
-        f[p] - apply_op<KIND>(A, (const T *)nullptr, x, p, d.sy(), d.sz());
-    if (r)
-      r[p] = (Tout)dv;
-    acc = (double)dv * (double)dv;
+  if (i <= d.nx - 1 && j <= d.ny - 1) {
+    for (int k = k0; k <= k1; ++k) {
+      const int p = d.at(i, j, k);
+      const T dv =
+          f[p] - apply_op<KIND>(A, (const T *)nullptr, x, p, sy, sz);
+      if (r)
+        r[p] = (Tout)dv;
+      acc += (double)dv * (double)dv;
+    }
   }
   double v[1] = {block_sum_2d(acc, sh)};
   reduce_finish<1>(v, s, nullptr);
@@ -126,13 +136,19 @@ __global__ void __launch_bounds__(kReduceThreads)
                         const T *__restrict__ r, ReduceSlot s,
                         double *__restrict__ w) {
   __shared__ double sh[32];
-  const Interior t = interior_point(d);
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
+  const int k0 = 2 + blockIdx.z * kReducePlanes;
+  const int k1 = min(k0 + kReducePlanes - 1, d.nz - 1);
+  const int sy = d.sy(), sz = d.sz();
   double up = 0.0, lo = 0.0;
-  if (t.ok) {
-    const int p = d.at(t.i, t.j, t.k);
-    up = (double)r[p] * (double)x[p];
-    lo = (double)x[p] *
-         (double)apply27(A, (const T *)nullptr, x, p, d.sy(), d.sz());
+  if (i <= d.nx - 1 && j <= d.ny - 1) {
+    for (int k = k0; k <= k1; ++k) {
+      const int p = d.at(i, j, k);
+      up += (double)r[p] * (double)x[p];
+      lo += (double)x[p] *
+            (double)apply27(A, (const T *)nullptr, x, p, sy, sz);
+    }
   }
   double v[2];
   v[0] = block_sum_2d(up, sh);
