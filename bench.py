@@ -238,6 +238,53 @@ def workload_config(w, precision):
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
+def phase_bytes(p, level: int, phase: str, esz: int) -> float | None:
+    """Algorithmic bytes moved by one occurrence of a cycle phase (counted in
+    arrays of the level's n^3 points; see the kernel table of the design
+    notes)."""
+    from multigrid_b200.molecule import level_n
+    n3 = float(level_n(p.base, level) ** 3) if level >= 1 else 0.0
+    nf3 = float(p.n ** 3)
+    fine = level == p.nlev
+    nc3 = float(level_n(p.base, level - 1) ** 3) if level >= 2 else 0.0
+    if level == 0:
+        if phase == "residual":  # 4 coefficients + f + x in double
+            return nf3 * (6 * 8 + (4 if p.precision == "mixed" else 0))
+        if phase == "refine-update":  # x64 read/write, e32 read
+            return nf3 * (8 + 4 + 8)
+        return None
+    arrays = {"pre-smooth": 2 * (7 if fine else 17),
+              "post-smooth": 2 * (7 if fine else 17),
+              "defect": 7 if fine else 17, "axpy": 3}
+    if phase in arrays:
+        return arrays[phase] * n3 * esz
+    if phase in ("restrict", "interp"):
+        return (n3 + 28 * nc3) * esz
+    if phase == "damping":  # on the level below, double accumulators
+        return 16 * nc3 * esz
+    return None
+
+
+def profile_solve(p, step, dev, esz):
+    """One extra solve with CUDA events recorded around every cycle phase
+    inside the cycle graph; returns per-phase averages and bandwidths."""
+    p.set_profiling(True)
+    p.profile(reset=True)
+    step(p, dev)
+    prof = p.profile(reset=True)
+    p.set_profiling(False)
+    rows = []
+    for (L, ph), (ms, cnt) in prof.items():
+        avg_ms = ms / cnt
+        b = phase_bytes(p, L, ph, esz if L != 1 else 8)
+        rows.append({"level": L, "phase": ph, "ms_total": ms, "count": cnt,
+                     "us_avg": 1000 * avg_ms,
+                     "gbs": (b / (avg_ms / 1000) / 1e9) if b else None,
+                     "bytes": b})
+    rows.sort(key=lambda r: -r["ms_total"])
+    return rows
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -245,7 +292,7 @@ def main():
     import torch
 
     world, rank, local = dist_setup(args)
-    from multigrid_b200 import PBELinearProblem, pmgc
+    from multigrid_b200 import PBELinearProblem
     from multigrid_b200.molecule import WORKLOADS
     from multigrid_b200.problem import setup_fine
 
@@ -255,10 +302,6 @@ def main():
     keys = ("oC", "oE", "oN", "uC", "f", "x0")
     dev = {k: torch.from_numpy(fine[k]).cuda() for k in keys}
     n3 = w.n ** 3
-
-    def make(precision):
-        p = PBELinearProblem(w.base, w.nlev, w.box, precision, w.physics)
-        return p
 
     def step(p, inputs):
         p.set_fine(*[inputs[k] for k in keys])
@@ -270,7 +313,7 @@ def main():
     if not args.quick:
         precisions.append("fp64" if args.precision == "mixed" else "mixed")
     for precision in precisions:
-        p = make(precision)
+        p = PBELinearProblem(w.base, w.nlev, w.box, precision, w.physics)
         stream = torch.cuda.ExternalStream(p.stream)
         for _ in range(args.warmup):
             res = step(p, dev)
@@ -283,19 +326,22 @@ def main():
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         cyc = []
+        l0 = p.launches
         e0.record(stream)
         for _ in range(args.steps):
             res = step(p, dev)
             cyc.append(res.cycles)
         e1.record(stream)
         torch.cuda.synchronize()
+        launches = p.launches - l0
         ms = e0.elapsed_time(e1)
         ck = clocks.stop() if precision == args.precision else None
         barrier(world)
         ms = max_over_ranks(world, ms)
         x = p.potential().ravel()
         results[precision] = dict(ms=ms, cycles=cyc, relres=res.relres,
-                                  x=x, clocks=ck, p=p, stream=stream)
+                                  x=x, clocks=ck, p=p, stream=stream,
+                                  launches=launches)
 
     prim = results[args.precision]
     value = world * args.steps / (prim["ms"] / 1000.0)
@@ -309,12 +355,12 @@ def main():
         return 0
 
     # end to end through the public API from pinned host buffers
+    import ctypes
+    from multigrid_b200 import _lib
     p = prim["p"]
     stream = prim["stream"]
     host = {k: torch.from_numpy(fine[k]).pin_memory() for k in keys}
     out_host = torch.empty(n3, dtype=torch.float64).pin_memory()
-    import ctypes
-    from multigrid_b200 import _lib
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     k_e2e = max(1, min(args.steps, 5))
@@ -330,41 +376,21 @@ def main():
     e2e = {"value": world * k_e2e / (e2e_ms / 1000.0), "unit": UNIT,
            "h2d_bytes_per_step": 6 * n3 * 8, "d2h_bytes_per_step": n3 * 8}
 
-    # dominant kernel: the finest-level red-black smoother (one sweep of two
-    # colours), timed with CUDA events on its stream
+    # per-phase timing of one more solve (CUDA events inside the cycle graph,
+    # on the solver's stream); the dominant bandwidth-bound phase gives the
+    # roofline
     peak, peak_kind = peaks()
-    xs = dev["x0"].clone()
-    if args.precision == "mixed":
-        arr = {k: dev[k].float() for k in keys}
-        xs = xs.float()
-        esz = 4
-    else:
-        arr = dev
-        esz = 8
-    s2 = torch.cuda.Stream()
-    reps = 20
-    with torch.cuda.stream(s2):
-        for _ in range(3):
-            pmgc.Vgsrb7x(w.n, w.n, w.n, arr["oC"], None, arr["f"], arr["oE"],
-                         arr["oN"], arr["uC"], xs, 1, stream=s2)
-        a0 = torch.cuda.Event(enable_timing=True)
-        a1 = torch.cuda.Event(enable_timing=True)
-        a0.record(s2)
-        for _ in range(reps):
-            pmgc.Vgsrb7x(w.n, w.n, w.n, arr["oC"], None, arr["f"], arr["oE"],
-                         arr["oN"], arr["uC"], xs, 1, stream=s2)
-        a1.record(s2)
-    torch.cuda.synchronize()
-    sweep_ms = a0.elapsed_time(a1) / reps
-    alg_bytes = 7 * n3 * esz  # 4 coefficients + f + x read, x written
-    achieved = alg_bytes / (sweep_ms / 1000.0) / 1e9
-    roofline = {"bound": "hbm", "kernel": "gs7_color_kernel (one sweep)",
-                "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": None,
+    esz = 4 if args.precision == "mixed" else 8
+    phases = profile_solve(p, step, dev, esz)
+    dom = next(r for r in phases if r["gbs"])
+    roofline = {"bound": "hbm",
+                "kernel": f"level {dom['level']} {dom['phase']}",
+                "achieved": dom["gbs"], "peak": peak, "unit": "GB/s",
+                "frac": dom["gbs"] / peak, "traffic": None,
                 "peak_source": peak_kind,
-                "algorithmic_bytes_per_launch": alg_bytes}
+                "algorithmic_bytes_per_launch": dom["bytes"],
+                "avg_launch_us": dom["us_avg"]}
 
-    # error of the mixed solve against the FP64 solve of the same run
     xm, xd = results["mixed"]["x"], results["fp64"]["x"]
     err = {"rel_l2": float(np.linalg.norm(xm - xd) / np.linalg.norm(xd)),
            "max_norm": float(np.abs(xm - xd).max() / np.abs(xd).max())}
@@ -387,20 +413,28 @@ def main():
             "dtype": "f32+f64" if args.precision == "mixed" else "f64",
             "data": "synthetic",
             "config": dict(workload_config(w, args.precision),
+                           levels_used=results[args.precision]["p"].nlev,
                            parallelism=f"replicas x{world}"),
             "cycles": prim["cycles"][-1],
             "relres": prim["relres"],
             "fp64": {"value": fp64_value, "cycles":
                      results["fp64"]["cycles"][-1],
-                     "ms_per_step": results["fp64"]["ms"] / args.steps},
+                     "ms_per_step": results["fp64"]["ms"] / args.steps,
+                     "levels": results["fp64"]["p"].nlev},
             "mixed": {"value": mixed_value, "cycles":
                       results["mixed"]["cycles"][-1],
                       "ms_per_step": results["mixed"]["ms"] / args.steps,
+                      "levels": results["mixed"]["p"].nlev,
                       "error_vs_fp64": err},
             "mixed_speedup_vs_fp64": mixed_value / fp64_value,
             "fine_unknowns_x_cycles_per_s": value * (w.n - 2) ** 3 *
             prim["cycles"][-1],
-            "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
+            "gpu_launches": prim["launches"],
+            "e2e": e2e, "roofline": roofline,
+            "phases_top": [{k: (round(v, 3) if isinstance(v, float) else v)
+                            for k, v in r.items() if k != "bytes"}
+                           for r in phases[:8]],
+            "cpu_baseline": cpu,
             "clocks": prim["clocks"],
         }
         print(json.dumps(line))

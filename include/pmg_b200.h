@@ -344,6 +344,10 @@ int pmg_problem_set_profiling(pmg_problem *p, int on);
 int pmg_problem_profile(pmg_problem *p, double *ms, long long *counts,
                         int cap, int reset);
 
+/* Kernels this problem has launched so far (hierarchy builds, residuals and
+ * every kernel node of each replayed cycle graph). */
+long long pmg_problem_launches(pmg_problem *p);
+
 /* The class's stream (for callers that enqueue around a solve). */
 pmg_stream_t pmg_problem_stream(pmg_problem *p);
 

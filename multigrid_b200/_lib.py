@@ -106,6 +106,7 @@ _sig("pmg_get_level", c_int, _V, c_int, _V)
 _sig("pmg_problem_stream", c_void_p, _V)
 _sig("pmg_problem_set_coarse_rtol", c_int, _V, c_double)
 _sig("pmg_problem_set_profiling", c_int, _V, c_int)
+_sig("pmg_problem_launches", c_ll, _V)
 _sig("pmg_problem_profile", c_int, _V, PD, ctypes.POINTER(c_ll), c_int, c_int)
 
 

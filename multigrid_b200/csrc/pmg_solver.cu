@@ -93,6 +93,9 @@ struct pmg_problem {
   bool fine_set = false, built = false;
   // One V-cycle (plus the residual norm) captured as a CUDA graph.
   cudaGraphExec_t cycle_exec = nullptr;
+  // kernel launches issued by this problem (build, solve, graph replays)
+  long long launches = 0;
+  long long cycle_kernels = 0; // kernel nodes in the captured cycle graph
   // phase timing (pmg_problem_set_profiling)
   bool prof_on = false;
   cudaEvent_t prof_ev[2][kProfSlots] = {};
@@ -462,6 +465,19 @@ int ensure_graph(pmg_problem *p) {
     set_last_error(e, "cudaStreamEndCapture", __FILE__, __LINE__);
     return PMG_ERR_CUDA;
   }
+  size_t nn = 0;
+  p->cycle_kernels = 0;
+  if (cudaGraphGetNodes(g, nullptr, &nn) == cudaSuccess && nn) {
+    cudaGraphNode_t *nodes = new cudaGraphNode_t[nn];
+    if (cudaGraphGetNodes(g, nodes, &nn) == cudaSuccess)
+      for (size_t q = 0; q < nn; ++q) {
+        cudaGraphNodeType t;
+        if (cudaGraphNodeGetType(nodes[q], &t) == cudaSuccess &&
+            t == cudaGraphNodeTypeKernel)
+          ++p->cycle_kernels;
+      }
+    delete[] nodes;
+  }
   e = cudaGraphInstantiate(&p->cycle_exec, g, 0);
   cudaGraphDestroy(g);
   if (e != cudaSuccess) {
@@ -607,6 +623,8 @@ int pmg_problem_profile(pmg_problem *p, double *ms, long long *counts,
   return kProfSlots;
 }
 
+long long pmg_problem_launches(pmg_problem *p) { return p ? p->launches : -1; }
+
 pmg_stream_t pmg_problem_stream(pmg_problem *p) {
   return p ? (pmg_stream_t)p->stream : nullptr;
 }
@@ -653,6 +671,7 @@ int pmg_build_hierarchy(pmg_problem *p, int trilinear) {
                                    Pw, s))) {
       return rc;
     }
+    p->launches += 2; // prolongation + Galerkin operator
     Op14W<double> out;
     for (int q = 0; q < 14; ++q)
       out.a[q] = c.op[q];
@@ -665,13 +684,17 @@ int pmg_build_hierarchy(pmg_problem *p, int trilinear) {
       LevelBuf &v = p->lv[L];
       const unsigned g = flat_grid(v.n3);
       for (int q = 0; q < 14; ++q)
-        if (v.op32[q])
+        if (v.op32[q]) {
           convert_kernel<double, float><<<g, 256, 0, s>>>(v.n3, v.op[q],
                                                          v.op32[q]);
+          ++p->launches;
+        }
       for (int q = 0; q < 27; ++q)
-        if (v.P32[q])
+        if (v.P32[q]) {
           convert_kernel<double, float><<<g, 256, 0, s>>>(v.n3, v.P[q],
                                                          v.P32[q]);
+          ++p->launches;
+        }
     }
     PMG_LAUNCH_CHECK();
   }
@@ -718,6 +741,7 @@ int pmg_solve(pmg_problem *p, double tol, int max_cycles, int *cycles,
   int rc = mixed ? mixed_residual_async(p) : residual_norm_async(p);
   if (rc)
     return rc;
+  ++p->launches;
   PMG_CUDA_TRY(cudaStreamSynchronize(p->stream));
   const double r0 = norm_from_sum(p, p->h_pinned[0]);
   if (hist)
@@ -737,6 +761,7 @@ int pmg_solve(pmg_problem *p, double tol, int max_cycles, int *cycles,
   rc = PMG_OK;
   while (c < max_cycles && r0 > 0.0) {
     PMG_CUDA_TRY(cudaGraphLaunch(p->cycle_exec, p->stream));
+    p->launches += p->cycle_kernels;
     PMG_CUDA_TRY(cudaStreamSynchronize(p->stream));
     prof_collect(p);
     ++c;

@@ -180,6 +180,11 @@ class PBELinearProblem:
         _lib.check("pmg_problem_set_coarse_rtol",
                    _lib.lib.pmg_problem_set_coarse_rtol(self._h, float(rtol)))
 
+    @property
+    def launches(self) -> int:
+        """Kernels launched by this problem so far."""
+        return int(_lib.lib.pmg_problem_launches(self._h))
+
     PHASES = ("pre-smooth", "defect", "restrict", "coarse-solve", "damping",
               "interp", "axpy", "post-smooth")
     GLOBAL_PHASES = ("residual", "refine-update")
