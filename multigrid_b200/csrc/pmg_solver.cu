@@ -8,6 +8,7 @@
 #include <new>
 
 #include "build_kernels.cuh"
+#include "bottom_cycle.cuh"
 #include "gs27_tiled.cuh"
 #include "launch.cuh"
 #include "reduce_kernels.cuh"
@@ -87,6 +88,9 @@ struct pmg_problem {
   // Relative stopping threshold of the coarsest CG on the mixed path's
   // correction equation (the FP64 path keeps the class's absolute 1e-8).
   double coarse_rtol = 1e-4;
+  // Mixed path: levels 1 .. bottom_top (n <= 17) run in one CTA
+  // (bottom_cycle_kernel); 0 when level 1 is too large.
+  int bottom_top = 0;
   ReduceSlot red_norm{}, red_lambda{};
   double *h_pinned = nullptr; // [0] residual sum, [1..] spare
   int *h_status = nullptr;
@@ -339,6 +343,33 @@ int smooth32(pmg_problem *p, int L, int nsweeps, int zero_init, float **cur) {
                                nsweeps, 0, zero_init, p->stream, cur);
 }
 
+// Arguments of the one-CTA cycle over levels 1 .. top.
+BottomArgs bottom_args(pmg_problem *p, int top) {
+  BottomArgs a{};
+  a.top = top;
+  for (int L = 1; L <= top; ++L) {
+    LevelBuf &v = p->lv[L];
+    BottomLevel &b = a.lv[L];
+    b.d = v.d;
+    b.A = v.A32(L > 1 ? 14 : 0);
+    b.P = v.Pc32();
+    b.x = v.x32;
+    b.f = v.f32;
+    b.r = v.r32;
+    b.omega = v.omega;
+  }
+  a.A1 = p->lv[1].A64(14);
+  a.x1 = p->lv[1].x;
+  a.f1 = p->lv[1].f;
+  a.cg_r = p->cg_r;
+  a.cg_p = p->cg_p;
+  a.cg_ap = p->cg_ap;
+  a.rtol = p->coarse_rtol;
+  a.max_iters = kCgMaxIters;
+  a.status = p->cg_status;
+  return a;
+}
+
 // V-cycle in float on the correction equation, every level zero-started
 // (v_cycle with as_preconditioner, PBE_pmgc_class.h:1070-1114); level 1 in
 // double.
@@ -359,6 +390,7 @@ int vcycle32(pmg_problem *p, int L) {
   const int kind = L == p->nlev ? 7 : 27;
   int rc;
   float *x = v.x32;
+  const bool bottom_below = L - 1 <= p->bottom_top;
   prof_begin(p, sl + kPhPre);
   if ((rc = smooth32(p, L, 2, 1, &x)))
     return rc;
@@ -377,10 +409,19 @@ int vcycle32(pmg_problem *p, int L) {
                                                        c.Pc32());
   prof_end(p, sl + kPhRestrict);
   PMG_LAUNCH_CHECK();
-  if ((rc = vcycle32(p, L - 1)))
+  if (bottom_below) {
+    // levels 1 .. L-1 in one CTA; it also leaves the damping of level L-1
+    prof_begin(p, sl + kPhCoarse);
+    bottom_cycle_kernel<<<1, 1024, 0, s>>>(bottom_args(p, L - 1));
+    prof_end(p, sl + kPhCoarse);
+    PMG_LAUNCH_CHECK();
+  } else if ((rc = vcycle32(p, L - 1))) {
     return rc;
+  }
   prof_begin(p, sl + kPhLambda);
-  if (L - 1 == 1) {
+  if (bottom_below) {
+    // damping computed by the bottom kernel
+  } else if (L - 1 == 1) {
     ideal_lambda_kernel<double><<<reduce_grid(c.d), interior_block(), 0, s>>>(
         c.d, c.A64(14), c.x, c.f, p->red_lambda, c.omega);
     convert_kernel<double, float><<<flat_grid(c.n3), 256, 0, s>>>(c.n3, c.x,
@@ -522,6 +563,10 @@ int pmg_problem_create(int base, int nlev, double box, int precision,
   p->nlev = nlev;
   p->box = box;
   p->precision = precision;
+  if (precision == PMG_PREC_MIXED)
+    for (int L = 1; L < nlev && L <= kBottomMaxLevels; ++L)
+      if (level_n(base, L) <= kBottomMaxN)
+        p->bottom_top = L;
   Arena a;
   plan(p, a);
   p->arena_bytes = a.off;
