@@ -2,6 +2,7 @@
 every declared symbol, argument checks reject bad calls before any CUDA work,
 grid-size rules are exact, synthetic molecules are well formed."""
 import ctypes
+import os
 import math
 
 import numpy as np
@@ -125,3 +126,17 @@ def test_setup_rejects_atoms_outside():
     with pytest.raises(_lib.PmgError):
         setup_fine(9, 0.5, np.array([[10.0, 1.0, 1.0, 1.5, 1.0]]),
                    DEFAULT_PHYSICS)
+
+
+def test_bench_reads_profiled_traffic():
+    """bench.py's roofline takes its DRAM traffic from the committed ncu
+    summary of the dominant kernel (bytes per launch x launches per phase)."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location(
+        "bench", os.path.join(os.path.dirname(__file__), "..", "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    t = bench.profiled_traffic("gs7_color_kernel", 4, "pb257", "mixed")
+    assert t is not None and t > 4 * 4.0e8
+    assert bench.profiled_traffic("no_such_kernel", 1, "pb257", "mixed") is None
+    assert bench.profiled_traffic(None, 1, "pb257", "mixed") is None
