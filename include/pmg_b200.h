@@ -312,12 +312,30 @@ int pmg_vcycle(pmg_problem *p, int as_preconditioner);
 int pmg_compute_residual_2(pmg_problem *p, double *out);
 
 /* Solves to compute_residual_2()/r0 < tol with at most max_cycles V-cycles
- * (FP64) or refinement steps (mixed). *cycles and *relres (host) get the
+ * (FP64) or refinement steps (mixed): the solve loop of the class's apps
+ * (PBE_pmgc_class_test.cc:124-146). *cycles and *relres (host) get the
  * cycles run and the final relative residual; hist (host, may be NULL,
  * max_cycles+1 entries) the residual norm per cycle. Returns
- * PMG_ERR_DIVERGED on NaN/Inf or stagnation. */
+ * PMG_ERR_DIVERGED on NaN/Inf or stagnation. Runs as one graph launch with
+ * the stop test on the GPU (pmg_solve_start + pmg_solve_finish) unless phase
+ * timing is on or max_cycles > 1024 (then one launch and one read-back per
+ * cycle); both take the same decisions. */
 int pmg_solve(pmg_problem *p, double tol, int max_cycles, int *cycles,
               double *relres, double *hist);
+
+/* Asynchronous solve (no reference counterpart; the class's loop is
+ * synchronous): enqueues the whole solve on the problem's stream as one
+ * graph launch whose while node repeats cycle + stop test on the GPU, and
+ * returns at once. 0 <= max_cycles <= 1024. One solve in flight per
+ * problem; independent problems on their own streams overlap on the
+ * device. */
+int pmg_solve_start(pmg_problem *p, double tol, int max_cycles);
+/* *done = 1 once the solve started by pmg_solve_start has finished on the
+ * GPU (also when none is in flight); never blocks. */
+int pmg_solve_poll(pmg_problem *p, int *done);
+/* Waits for the solve in flight and reports it like pmg_solve. */
+int pmg_solve_finish(pmg_problem *p, int *cycles, double *relres,
+                     double *hist);
 
 /* Copies the finest iterate (n^3 doubles incl. shell) to dst (host or
  * device). */

@@ -71,6 +71,20 @@ struct Arena {
   }
 };
 
+// Device-resident state of one solve (pmg_solve_start): parameters, the
+// residual history and the outcome, written by the solve graph's control
+// kernels and copied to pinned host memory at its end.
+constexpr int kMaxHist = 1024;
+struct SolveState {
+  double tol;
+  int max_cycles;
+  int cycles;
+  int status; // 0 running / converged / capped, 1 diverged, 2 r0 not finite
+  int pad;
+  double r0, r;
+  double hist[kMaxHist + 1];
+};
+
 } // namespace pmg
 
 using namespace pmg;
@@ -97,6 +111,14 @@ struct pmg_problem {
   bool fine_set = false, built = false;
   // One V-cycle (plus the residual norm) captured as a CUDA graph.
   cudaGraphExec_t cycle_exec = nullptr;
+  // A whole solve as one graph: initial residual, then a device-side while
+  // loop over cycles (conditional node), then the state copy to the host.
+  cudaGraphExec_t solve_exec = nullptr;
+  long long solve_pre_kernels = 0, solve_body_kernels = 0;
+  SolveState *d_state = nullptr; // arena
+  SolveState *h_state = nullptr; // pinned
+  cudaEvent_t done_ev = nullptr;
+  bool solve_pending = false;
   // kernel launches issued by this problem (build, solve, graph replays)
   long long launches = 0;
   long long cycle_kernels = 0; // kernel nodes in the captured cycle graph
@@ -153,6 +175,7 @@ void plan(pmg_problem *p, Arena &a) {
   p->cg_p = a.take<double>(n1);
   p->cg_ap = a.take<double>(n1);
   p->cg_status = a.take<int>(2);
+  p->d_state = a.take<SolveState>(1);
   for (ReduceSlot *s : {&p->red_norm, &p->red_lambda}) {
     // partials of the largest interior launch
     const Dims &df = p->lv[p->nlev].d;
@@ -311,7 +334,7 @@ int vcycle64(pmg_problem *p, int L, int as_preconditioner) {
 
 // Residual sum of squares of the finest level into red_norm.result[0] and
 // then into pinned host memory (not synchronised here).
-int residual_norm_async(pmg_problem *p) {
+int residual_norm_async(pmg_problem *p, bool to_host = true) {
   LevelBuf &v = p->lv[p->nlev];
   prof_begin(p, kPhResidual);
   defect_norm_kernel<7, double, double>
@@ -319,9 +342,10 @@ int residual_norm_async(pmg_problem *p) {
           v.d, v.A64(4), v.f, v.x, (double *)nullptr, p->red_norm);
   prof_end(p, kPhResidual);
   PMG_LAUNCH_CHECK();
-  PMG_CUDA_TRY(cudaMemcpyAsync(p->h_pinned, p->red_norm.result,
-                               sizeof(double), cudaMemcpyDeviceToHost,
-                               p->stream));
+  if (to_host)
+    PMG_CUDA_TRY(cudaMemcpyAsync(p->h_pinned, p->red_norm.result,
+                                 sizeof(double), cudaMemcpyDeviceToHost,
+                                 p->stream));
   return PMG_OK;
 }
 
@@ -454,7 +478,7 @@ int vcycle32(pmg_problem *p, int L) {
 // r64 = f - A x64 on the finest level, written as float into f32 (the
 // correction equation's right-hand side), its sum of squares into red_norm
 // and pinned host memory.
-int mixed_residual_async(pmg_problem *p) {
+int mixed_residual_async(pmg_problem *p, bool to_host = true) {
   LevelBuf &v = p->lv[p->nlev];
   prof_begin(p, kPhResidual);
   defect_norm_kernel<7, double, float>
@@ -462,15 +486,16 @@ int mixed_residual_async(pmg_problem *p) {
           v.d, v.A64(4), v.f, v.x, v.f32, p->red_norm);
   prof_end(p, kPhResidual);
   PMG_LAUNCH_CHECK();
-  PMG_CUDA_TRY(cudaMemcpyAsync(p->h_pinned, p->red_norm.result,
-                               sizeof(double), cudaMemcpyDeviceToHost,
-                               p->stream));
+  if (to_host)
+    PMG_CUDA_TRY(cudaMemcpyAsync(p->h_pinned, p->red_norm.result,
+                                 sizeof(double), cudaMemcpyDeviceToHost,
+                                 p->stream));
   return PMG_OK;
 }
 
 // One refinement step: float V-cycle on the correction, x64 += e, new
 // residual.
-int mixed_step(pmg_problem *p) {
+int mixed_step(pmg_problem *p, bool to_host = true) {
   LevelBuf &v = p->lv[p->nlev];
   int rc;
   if ((rc = vcycle32(p, p->nlev)))
@@ -480,7 +505,38 @@ int mixed_step(pmg_problem *p) {
                           p->stream>>>(v.d, v.x, v.x32);
   prof_end(p, kPhCorrect);
   PMG_LAUNCH_CHECK();
-  return mixed_residual_async(p);
+  return mixed_residual_async(p, to_host);
+}
+
+// Kernel nodes of a graph (conditional bodies are counted by their own
+// graph). The type query fails on conditional nodes; that failure is
+// expected and cleared, so call this with no other error pending.
+long long count_kernel_nodes(cudaGraph_t g) {
+  size_t nn = 0;
+  long long k = 0;
+  if (cudaGraphGetNodes(g, nullptr, &nn) == cudaSuccess && nn) {
+    cudaGraphNode_t *nodes = new cudaGraphNode_t[nn];
+    if (cudaGraphGetNodes(g, nodes, &nn) == cudaSuccess)
+      for (size_t q = 0; q < nn; ++q) {
+        cudaGraphNodeType t;
+        if (cudaGraphNodeGetType(nodes[q], &t) == cudaSuccess &&
+            t == cudaGraphNodeTypeKernel)
+          ++k;
+      }
+    delete[] nodes;
+  }
+  (void)cudaGetLastError();
+  return k;
+}
+
+// One cycle with its residual: FP64 V-cycle + residual norm, or the mixed
+// refinement step. to_host adds the copy of the residual sum to pinned
+// memory (the host-driven loop); the device-driven loop keeps it on the GPU.
+int cycle_with_residual(pmg_problem *p, bool to_host) {
+  if (p->precision == PMG_PREC_MIXED)
+    return mixed_step(p, to_host);
+  int rc = vcycle64(p, p->nlev, 0);
+  return rc ? rc : residual_norm_async(p, to_host);
 }
 
 // Captures one cycle (FP64: V-cycle + residual; mixed: refinement step) as a
@@ -491,34 +547,18 @@ int ensure_graph(pmg_problem *p) {
   cudaGraph_t g = nullptr;
   PMG_CUDA_TRY(
       cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal));
-  int rc;
-  if (p->precision == PMG_PREC_MIXED) {
-    rc = mixed_step(p);
-  } else {
-    rc = vcycle64(p, p->nlev, 0);
-    if (!rc)
-      rc = residual_norm_async(p);
-  }
+  int rc = cycle_with_residual(p, true);
   cudaError_t e = cudaStreamEndCapture(p->stream, &g);
-  if (rc)
+  if (rc) {
+    if (g)
+      cudaGraphDestroy(g);
     return rc;
+  }
   if (e != cudaSuccess) {
     set_last_error(e, "cudaStreamEndCapture", __FILE__, __LINE__);
     return PMG_ERR_CUDA;
   }
-  size_t nn = 0;
-  p->cycle_kernels = 0;
-  if (cudaGraphGetNodes(g, nullptr, &nn) == cudaSuccess && nn) {
-    cudaGraphNode_t *nodes = new cudaGraphNode_t[nn];
-    if (cudaGraphGetNodes(g, nodes, &nn) == cudaSuccess)
-      for (size_t q = 0; q < nn; ++q) {
-        cudaGraphNodeType t;
-        if (cudaGraphNodeGetType(nodes[q], &t) == cudaSuccess &&
-            t == cudaGraphNodeTypeKernel)
-          ++p->cycle_kernels;
-      }
-    delete[] nodes;
-  }
+  p->cycle_kernels = count_kernel_nodes(g);
   e = cudaGraphInstantiate(&p->cycle_exec, g, 0);
   cudaGraphDestroy(g);
   if (e != cudaSuccess) {
@@ -527,6 +567,184 @@ int ensure_graph(pmg_problem *p) {
     return PMG_ERR_CUDA;
   }
   return PMG_OK;
+}
+
+// ---- device-driven solve loop ----------------------------------------------
+// The class's solve loop (PBE_pmgc_class.h:1139-1152: r0, then V-cycles until
+// r / r0 < tol) with the decisions taken on the GPU: the stop test sets the
+// condition of a while node, so a whole solve is one graph launch with no
+// host round trip per cycle. The arithmetic of the test (sqrt of the sum over
+// n^3, the ratio, the divergence guard) is the host loop's.
+
+__global__ void solve_params_kernel(SolveState *st, double tol,
+                                    int max_cycles) {
+  st->tol = tol;
+  st->max_cycles = max_cycles;
+  st->cycles = 0;
+  st->status = 0;
+}
+
+__global__ void solve_init_kernel(SolveState *st, const double *sum,
+                                  double n3, cudaGraphConditionalHandle h) {
+  const double r0 = sqrt(sum[0] / n3);
+  st->r0 = r0;
+  st->r = r0;
+  st->hist[0] = r0;
+  const bool finite = isfinite(r0);
+  st->status = finite ? 0 : 2;
+  cudaGraphSetConditional(h, (finite && r0 > 0.0 && st->max_cycles > 0)
+                                 ? 1u
+                                 : 0u);
+}
+
+__global__ void solve_check_kernel(SolveState *st, const double *sum,
+                                   double n3, cudaGraphConditionalHandle h) {
+  const double r = sqrt(sum[0] / n3);
+  const int c = ++st->cycles;
+  if (c <= kMaxHist)
+    st->hist[c] = r;
+  st->r = r;
+  const double r0 = st->r0;
+  const bool diverged = !isfinite(r) || r > 1e6 * r0;
+  if (diverged)
+    st->status = 1;
+  const bool go = !diverged && !(r / r0 < st->tol) && c < st->max_cycles;
+  cudaGraphSetConditional(h, go ? 1u : 0u);
+}
+
+// Takes a pending runtime error left by a graph-building call that reports
+// through the last-error slot only, naming the step.
+int graph_step_ok(const char *step) {
+  const cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess)
+    return PMG_OK;
+  set_last_error(e, step, __FILE__, __LINE__);
+  return PMG_ERR_CUDA;
+}
+
+// Builds the solve graph: [initial residual, init] -> while(cond){cycle,
+// check} -> copy of the state to pinned memory.
+int ensure_solve_graph(pmg_problem *p) {
+  if (p->solve_exec)
+    return PMG_OK;
+  const bool mixed = p->precision == PMG_PREC_MIXED;
+  const double n3 = (double)p->lv[p->nlev].n3;
+  cudaGraph_t g = nullptr, body = nullptr;
+  cudaGraphConditionalHandle h;
+  cudaGraphNode_t cond = nullptr;
+  int rc = PMG_OK;
+  (void)cudaGetLastError();
+  cudaError_t e = cudaGraphCreate(&g, 0);
+  if (e == cudaSuccess)
+    e = cudaGraphConditionalHandleCreate(&h, g, 0,
+                                         cudaGraphCondAssignDefault);
+  if (e != cudaSuccess) {
+    if (g)
+      cudaGraphDestroy(g);
+    set_last_error(e, "solve graph: conditional handle", __FILE__, __LINE__);
+    return PMG_ERR_CUDA;
+  }
+  // head: initial residual and the init kernel, captured into g
+  e = cudaStreamBeginCaptureToGraph(p->stream, g, nullptr, nullptr, 0,
+                                    cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    rc = mixed ? mixed_residual_async(p, false)
+               : residual_norm_async(p, false);
+    if (!rc) {
+      solve_init_kernel<<<1, 1, 0, p->stream>>>(p->d_state,
+                                                p->red_norm.result, n3, h);
+      e = cudaGetLastError();
+      if (e != cudaSuccess) {
+        set_last_error(e, "solve graph: init kernel", __FILE__, __LINE__);
+        rc = PMG_ERR_CUDA;
+      }
+    }
+    const cudaGraphNode_t *deps = nullptr;
+    size_t ndeps = 0;
+    cudaStreamCaptureStatus cs;
+    if (!rc)
+      e = cudaStreamGetCaptureInfo(p->stream, &cs, nullptr, nullptr, &deps,
+                                   &ndeps);
+    if (!rc && e == cudaSuccess) {
+      cudaGraphNodeParams cp = {};
+      cp.type = cudaGraphNodeTypeConditional;
+      cp.conditional.handle = h;
+      cp.conditional.type = cudaGraphCondTypeWhile;
+      cp.conditional.size = 1;
+      e = cudaGraphAddNode(&cond, g, deps, ndeps, &cp);
+      if (e == cudaSuccess) {
+        body = cp.conditional.phGraph_out[0];
+        e = cudaStreamUpdateCaptureDependencies(
+            p->stream, &cond, 1, cudaStreamSetCaptureDependencies);
+      }
+    }
+    if (!rc && e == cudaSuccess)
+      e = cudaMemcpyAsync(p->h_state, p->d_state, sizeof(SolveState),
+                          cudaMemcpyDeviceToHost, p->stream);
+    cudaGraph_t out = nullptr;
+    const cudaError_t e2 = cudaStreamEndCapture(p->stream, &out);
+    if (e == cudaSuccess)
+      e = e2;
+  }
+  if (!rc && e == cudaSuccess)
+    rc = graph_step_ok("solve graph: head capture");
+  if (!rc && e == cudaSuccess)
+    p->solve_pre_kernels = count_kernel_nodes(g);
+  if (!rc && e == cudaSuccess) {
+    // body: one cycle and the stop test
+    e = cudaStreamBeginCaptureToGraph(p->stream, body, nullptr, nullptr, 0,
+                                      cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess)
+      rc = graph_step_ok("solve graph: body capture");
+    if (e == cudaSuccess && !rc) {
+      rc = cycle_with_residual(p, false);
+      if (!rc) {
+        solve_check_kernel<<<1, 1, 0, p->stream>>>(
+            p->d_state, p->red_norm.result, n3, h);
+        const cudaError_t ek = cudaGetLastError();
+        if (ek != cudaSuccess) {
+          set_last_error(ek, "solve graph: check kernel", __FILE__, __LINE__);
+          rc = PMG_ERR_CUDA;
+        }
+      }
+      cudaGraph_t out = nullptr;
+      const cudaError_t e2 = cudaStreamEndCapture(p->stream, &out);
+      if (e == cudaSuccess)
+        e = e2;
+    }
+  }
+  if (!rc && e == cudaSuccess) {
+    p->solve_body_kernels = count_kernel_nodes(body);
+    // the loop ends only through the check kernel: never instantiate a body
+    // without it
+    if (p->solve_body_kernels < 2) {
+      set_last_message("solve graph: loop body was not captured");
+      rc = PMG_ERR_STATE;
+    } else {
+      e = cudaGraphInstantiate(&p->solve_exec, g, 0);
+    }
+  }
+  cudaGraphDestroy(g);
+  if (rc)
+    return rc;
+  if (e != cudaSuccess) {
+    p->solve_exec = nullptr;
+    set_last_error(e, "solve graph", __FILE__, __LINE__);
+    return PMG_ERR_CUDA;
+  }
+  return PMG_OK;
+}
+
+// Drops the captured graphs (their kernels bake in thresholds and modes).
+void drop_graphs(pmg_problem *p) {
+  if (p->cycle_exec) {
+    cudaGraphExecDestroy(p->cycle_exec);
+    p->cycle_exec = nullptr;
+  }
+  if (p->solve_exec) {
+    cudaGraphExecDestroy(p->solve_exec);
+    p->solve_exec = nullptr;
+  }
 }
 
 } // namespace
@@ -588,6 +806,10 @@ int pmg_problem_create(int base, int nlev, double box, int precision,
   if (e == cudaSuccess)
     e = cudaMallocHost((void **)&p->h_pinned, 4 * sizeof(double));
   if (e == cudaSuccess)
+    e = cudaMallocHost((void **)&p->h_state, sizeof(SolveState));
+  if (e == cudaSuccess)
+    e = cudaEventCreateWithFlags(&p->done_ev, cudaEventDisableTiming);
+  if (e == cudaSuccess)
     e = cudaMemsetAsync(p->arena, 0, p->arena_bytes, p->stream);
   if (e == cudaSuccess)
     e = cudaStreamSynchronize(p->stream);
@@ -605,8 +827,11 @@ int pmg_problem_destroy(pmg_problem *p) {
     return PMG_OK;
   if (p->stream)
     cudaStreamSynchronize(p->stream);
-  if (p->cycle_exec)
-    cudaGraphExecDestroy(p->cycle_exec);
+  drop_graphs(p);
+  if (p->done_ev)
+    cudaEventDestroy(p->done_ev);
+  if (p->h_state)
+    cudaFreeHost(p->h_state);
   for (int e = 0; e < 2; ++e)
     for (int q = 0; q < kProfSlots; ++q)
       if (p->prof_ev[e][q])
@@ -627,10 +852,7 @@ int pmg_problem_set_coarse_rtol(pmg_problem *p, double rtol) {
     return PMG_ERR_ARG;
   }
   p->coarse_rtol = rtol;
-  if (p->cycle_exec) { // the captured cycle bakes the threshold in
-    cudaGraphExecDestroy(p->cycle_exec);
-    p->cycle_exec = nullptr;
-  }
+  drop_graphs(p); // the captured cycles bake the threshold in
   return PMG_OK;
 }
 
@@ -642,10 +864,8 @@ int pmg_problem_set_profiling(pmg_problem *p, int on) {
       for (int q = 0; q < kProfSlots; ++q)
         PMG_CUDA_TRY(cudaEventCreate(&p->prof_ev[e][q]));
   }
-  if ((bool)on != p->prof_on && p->cycle_exec) {
-    cudaGraphExecDestroy(p->cycle_exec);
-    p->cycle_exec = nullptr;
-  }
+  if ((bool)on != p->prof_on)
+    drop_graphs(p);
   p->prof_on = on != 0;
   return PMG_OK;
 }
@@ -774,14 +994,11 @@ int pmg_compute_residual_2(pmg_problem *p, double *out) {
   return PMG_OK;
 }
 
-int pmg_solve(pmg_problem *p, double tol, int max_cycles, int *cycles,
-              double *relres, double *hist) {
-  if (!p || max_cycles < 0)
-    return PMG_ERR_ARG;
-  if (!p->built) {
-    set_last_message("pmg_solve: hierarchy not built");
-    return PMG_ERR_STATE;
-  }
+// Host-driven loop: one cycle graph per launch and a residual read-back per
+// cycle (used with phase timing, whose event records cannot sit in a
+// conditional body, and for histories longer than the device state holds).
+static int solve_host_loop(pmg_problem *p, double tol, int max_cycles,
+                           int *cycles, double *relres, double *hist) {
   const bool mixed = p->precision == PMG_PREC_MIXED;
   int rc = mixed ? mixed_residual_async(p) : residual_norm_async(p);
   if (rc)
@@ -826,6 +1043,103 @@ int pmg_solve(pmg_problem *p, double tol, int max_cycles, int *cycles,
   if (relres)
     *relres = r0 > 0.0 ? r / r0 : 0.0;
   return rc;
+}
+
+int pmg_solve_start(pmg_problem *p, double tol, int max_cycles) {
+  if (!p || max_cycles < 0 || max_cycles > kMaxHist || !(tol >= 0.0)) {
+    set_last_message("pmg_solve_start: bad argument (0 <= max_cycles <= "
+                     "1024, tol >= 0)");
+    return PMG_ERR_ARG;
+  }
+  if (!p->built) {
+    set_last_message("pmg_solve_start: hierarchy not built");
+    return PMG_ERR_STATE;
+  }
+  if (p->solve_pending) {
+    set_last_message("pmg_solve_start: a solve is already in flight");
+    return PMG_ERR_STATE;
+  }
+  if (p->prof_on) {
+    set_last_message("pmg_solve_start: phase timing needs pmg_solve");
+    return PMG_ERR_STATE;
+  }
+  int rc = ensure_solve_graph(p);
+  if (rc)
+    return rc;
+  solve_params_kernel<<<1, 1, 0, p->stream>>>(p->d_state, tol, max_cycles);
+  PMG_LAUNCH_CHECK();
+  PMG_CUDA_TRY(cudaGraphLaunch(p->solve_exec, p->stream));
+  PMG_CUDA_TRY(cudaEventRecord(p->done_ev, p->stream));
+  p->solve_pending = true;
+  return PMG_OK;
+}
+
+int pmg_solve_poll(pmg_problem *p, int *done) {
+  if (!p || !done)
+    return PMG_ERR_ARG;
+  if (!p->solve_pending) {
+    *done = 1;
+    return PMG_OK;
+  }
+  const cudaError_t e = cudaEventQuery(p->done_ev);
+  if (e == cudaErrorNotReady) {
+    *done = 0;
+    return PMG_OK;
+  }
+  PMG_CUDA_TRY(e);
+  *done = 1;
+  return PMG_OK;
+}
+
+int pmg_solve_finish(pmg_problem *p, int *cycles, double *relres,
+                     double *hist) {
+  if (!p)
+    return PMG_ERR_ARG;
+  if (!p->solve_pending) {
+    set_last_message("pmg_solve_finish: no solve in flight");
+    return PMG_ERR_STATE;
+  }
+  p->solve_pending = false;
+  PMG_CUDA_TRY(cudaEventSynchronize(p->done_ev));
+  const SolveState &st = *p->h_state;
+  p->launches += 1 + p->solve_pre_kernels +
+                 (long long)st.cycles * p->solve_body_kernels;
+  if (cycles)
+    *cycles = st.cycles;
+  if (relres)
+    *relres = st.status == 2 ? st.r0 : (st.r0 > 0.0 ? st.r / st.r0 : 0.0);
+  if (hist)
+    for (int c = 0; c <= st.cycles && c <= kMaxHist; ++c)
+      hist[c] = st.hist[c];
+  if (st.status == 2) {
+    set_last_message("pmg_solve: initial residual is not finite");
+    return PMG_ERR_DIVERGED;
+  }
+  if (st.status == 1) {
+    set_last_message("pmg_solve: residual diverged");
+    return PMG_ERR_DIVERGED;
+  }
+  return PMG_OK;
+}
+
+int pmg_solve(pmg_problem *p, double tol, int max_cycles, int *cycles,
+              double *relres, double *hist) {
+  if (!p || max_cycles < 0)
+    return PMG_ERR_ARG;
+  if (!p->built) {
+    set_last_message("pmg_solve: hierarchy not built");
+    return PMG_ERR_STATE;
+  }
+  if (p->solve_pending) {
+    set_last_message("pmg_solve: a solve is already in flight");
+    return PMG_ERR_STATE;
+  }
+  if (p->prof_on || max_cycles > kMaxHist)
+    return solve_host_loop(p, tol, max_cycles, cycles, relres, hist);
+  int rc = pmg_solve_start(p, tol, max_cycles);
+  if (rc)
+    return rc;
+  return pmg_solve_finish(p, cycles, relres, hist);
 }
 
 int pmg_get_potential(pmg_problem *p, double *dst) {

@@ -241,6 +241,27 @@ class PBELinearProblem:
             _dptr(hist)))
         return SolveResult(cycles.value, rel.value, hist[:cycles.value + 1])
 
+    def solve_start(self, tol: float = 1e-10, max_cycles: int = 100) -> None:
+        """Enqueues the whole solve (one graph launch, stop test on the GPU)
+        and returns at once; finish with solve_finish()."""
+        _lib.check("pmg_solve_start", _lib.lib.pmg_solve_start(
+            self._h, tol, max_cycles))
+        self._pending_max = max_cycles
+
+    def solve_done(self) -> bool:
+        done = ctypes.c_int()
+        _lib.check("pmg_solve_poll", _lib.lib.pmg_solve_poll(
+            self._h, ctypes.byref(done)))
+        return bool(done.value)
+
+    def solve_finish(self) -> SolveResult:
+        hist = np.zeros(getattr(self, "_pending_max", 1024) + 1)
+        cycles = ctypes.c_int()
+        rel = ctypes.c_double()
+        _lib.check("pmg_solve_finish", _lib.lib.pmg_solve_finish(
+            self._h, ctypes.byref(cycles), ctypes.byref(rel), _dptr(hist)))
+        return SolveResult(cycles.value, rel.value, hist[:cycles.value + 1])
+
     # -- results ----------------------------------------------------------------
     def potential(self) -> np.ndarray:
         """Finest iterate, shape (n, n, n) indexed [k, j, i] (x fastest)."""

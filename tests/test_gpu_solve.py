@@ -149,3 +149,75 @@ def test_nan_input_reports_divergence(golden_problem):
         with pytest.raises(PmgError) as e:
             p.solve(tol=1e-10, max_cycles=5)
         assert e.value.status == -4
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_device_loop_equals_host_loop(pb65, precision):
+    """The one-launch solve (stop test on the GPU, while node) takes the same
+    decisions as the host-driven loop (one launch + read-back per cycle, used
+    under phase timing): same cycles, same residual history, same bits."""
+    w, fine = pb65
+    out = {}
+    for mode in ("device", "host"):
+        with PBELinearProblem(w.base, w.nlev, w.box, precision) as p:
+            p.set_profiling(mode == "host")
+            p.set_fine(**fine)
+            p.buildmultilevelops()
+            res = p.solve(tol=1e-10, max_cycles=60)
+            out[mode] = (res, p.potential().ravel().copy())
+    (rd, xd), (rh, xh) = out["device"], out["host"]
+    assert rd.cycles == rh.cycles > 0
+    assert np.array_equal(rd.history, rh.history)
+    assert np.array_equal(xd, xh)
+
+
+def test_async_solves_overlap_and_match_alone(pb65, golden_problem):
+    """Solves started together on their own streams (pmg_solve_start) give
+    exactly the results of the same solves run one at a time."""
+    w, fine = pb65
+    g = golden_problem
+    cases = [(w.base, w.nlev, w.box, fine, "mixed"),
+             (w.base, w.nlev, w.box, fine, "fp64"),
+             (int(g["base"]), int(g["nlev"]), float(g["box"]), fine_of(g),
+              "fp64"),
+             (int(g["base"]), int(g["nlev"]), float(g["box"]), fine_of(g),
+              "mixed")]
+    alone = []
+    for base, nlev, box, fi, prec in cases:
+        with PBELinearProblem(base, nlev, box, prec) as p:
+            p.set_fine(**fi)
+            p.buildmultilevelops()
+            r = p.solve(tol=1e-10, max_cycles=60)
+            alone.append((r.cycles, p.potential().ravel().copy()))
+    probs = [PBELinearProblem(b, n, bx, pr) for b, n, bx, _, pr in cases]
+    try:
+        for p, (_, _, _, fi, _) in zip(probs, cases):
+            p.set_fine(**fi)
+            p.buildmultilevelops()
+        for p in probs:
+            p.solve_start(tol=1e-10, max_cycles=60)
+        results = [p.solve_finish() for p in probs]
+        for p, r, (c, x) in zip(probs, results, alone):
+            assert r.cycles == c
+            assert np.array_equal(p.potential().ravel(), x)
+            assert p.solve_done()
+    finally:
+        for p in probs:
+            p.close()
+
+
+def test_zero_cycles_and_double_start(golden_problem):
+    g = golden_problem
+    with PBELinearProblem(int(g["base"]), int(g["nlev"]), float(g["box"]),
+                          "fp64") as p:
+        p.set_fine(**fine_of(g))
+        p.buildmultilevelops()
+        res = p.solve(tol=1e-10, max_cycles=0)
+        assert res.cycles == 0 and res.relres == 1.0
+        p.solve_start(tol=1e-10, max_cycles=3)
+        with pytest.raises(PmgError) as e:
+            p.solve_start(tol=1e-10, max_cycles=3)
+        assert e.value.status == -7
+        assert p.solve_finish().cycles == 3
+        with pytest.raises(PmgError):
+            p.solve_finish()
