@@ -369,6 +369,73 @@ long long pmg_problem_launches(pmg_problem *p);
 /* The class's stream (for callers that enqueue around a solve). */
 pmg_stream_t pmg_problem_stream(pmg_problem *p);
 
+/* ---- Serving: continuous batching of independent solves ------------------
+ * No reference counterpart: the reference solves one molecule per process
+ * (PBE_pmgc_class_test.cc:84-146). A server owns a worker thread that admits
+ * requests in arrival order against a device-memory budget (the bytes of
+ * every problem it holds, pmg_problem_bytes), keeps each admitted solve's
+ * hierarchy resident in its own problem (reused for later requests of the
+ * same grid and precision), runs up to max_inflight solves at once, each as
+ * one graph launch on its own stream (pmg_solve_start), so cycles of
+ * different grid sizes overlap on the device, and reports completions. A
+ * request's arithmetic does not depend on what else is in flight: its result
+ * is bit-identical alone and in the mix. */
+typedef struct pmg_server pmg_server;
+
+typedef struct pmg_request {
+  int base, nlev;          /* grid: n = base * 2^nlev + 1 per axis        */
+  double box;              /* domain edge (Angstrom)                      */
+  int precision;           /* pmg_precision                               */
+  const double *fine[6];   /* oC oE oN uC f x0, n^3 each, host or device; */
+                           /* valid until the request's completion        */
+  double *potential;       /* n^3 result (host or device), may be NULL    */
+  double tol;              /* relative residual target                    */
+  int max_cycles;          /* 0 .. 1024                                   */
+  long long tag;           /* caller's identifier, echoed back            */
+  int hierarchy;           /* 0: levels as given; 1: the deepest levels   */
+                           /* of the same grid (pmg_levels_for(n, 12, 5)) */
+} pmg_request;
+
+typedef struct pmg_completion {
+  long long tag;
+  int status;              /* pmg_status of the solve                    */
+  int cycles;
+  double relres;
+  double t_submit, t_admit, t_done; /* seconds since server creation      */
+  char message[160];       /* error text when status != PMG_OK            */
+} pmg_completion;
+
+typedef struct pmg_server_stats {
+  int queued, inflight, idle_problems;
+  long long held_bytes, peak_bytes, budget_bytes;
+  long long completed, created_problems, evicted_problems;
+} pmg_server_stats;
+
+/* (base, nlev) with n = base * 2^nlev + 1, the largest nlev <= max_levels
+ * whose coarsest grid 2 * base + 1 has at least min_coarse points (grid-size
+ * rule of Vcorsr, pmgc/mgsubd.cc:395-413, applied as far as it goes). */
+int pmg_levels_for(int n, int max_levels, int min_coarse, int *base,
+                   int *nlev);
+
+/* budget_bytes > 0; 1 <= max_inflight <= 256. Uses the current device. */
+int pmg_server_create(long long budget_bytes, int max_inflight,
+                      pmg_server **out);
+/* Enqueues a copy of *r; never blocks on the GPU. A request larger than the
+ * whole budget completes with PMG_ERR_BUDGET. */
+int pmg_server_submit(pmg_server *s, const pmg_request *r);
+/* Moves up to cap completions into out (*n of them), waiting up to
+ * timeout_s seconds for the first one (0: no wait). */
+int pmg_server_wait(pmg_server *s, pmg_completion *out, int cap, int *n,
+                    double timeout_s);
+int pmg_server_get_stats(pmg_server *s, pmg_server_stats *st);
+/* Finishes the queued and in-flight work, then frees everything. */
+int pmg_server_destroy(pmg_server *s);
+
+/* Batched solves: every request through one server with the given budget,
+ * all admitted as memory allows; out[i] belongs to reqs[i]. */
+int pmg_batch_solve(const pmg_request *reqs, int count, long long budget_bytes,
+                    int max_inflight, pmg_completion *out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -33,6 +33,7 @@ STATUS = {
     -4: "PMG_ERR_DIVERGED", -5: "PMG_ERR_TIMEOUT", -6: "PMG_ERR_BUDGET",
     -7: "PMG_ERR_STATE",
 }
+globals().update({name: code for code, name in STATUS.items()})
 PREC_FP64 = 0
 PREC_MIXED = 1
 

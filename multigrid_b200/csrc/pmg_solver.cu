@@ -908,6 +908,18 @@ int pmg_problem_set_fine(pmg_problem *p, const double *oC, const double *oE,
   for (int q = 0; q < 6; ++q)
     PMG_CUDA_TRY(
         cudaMemcpyAsync(dst[q], src[q], b, cudaMemcpyDefault, p->stream));
+  // A new problem starts from the state of a freshly constructed class: the
+  // coarse iterates are zero (the coarsest CG warm-starts from its level's
+  // iterate, so a previous solve's values would change the result).
+  for (int L = 1; L < p->nlev; ++L) {
+    LevelBuf &c = p->lv[L];
+    if (c.x)
+      PMG_CUDA_TRY(
+          cudaMemsetAsync(c.x, 0, sizeof(double) * c.n3, p->stream));
+    if (c.x32)
+      PMG_CUDA_TRY(
+          cudaMemsetAsync(c.x32, 0, sizeof(float) * c.n3, p->stream));
+  }
   p->fine_set = true;
   p->built = false;
   return PMG_OK;

@@ -221,3 +221,31 @@ def test_zero_cycles_and_double_start(golden_problem):
         assert p.solve_finish().cycles == 3
         with pytest.raises(PmgError):
             p.solve_finish()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_reused_handle_solves_like_a_fresh_one(golden_problem, precision):
+    """A second problem loaded into the same handle solves exactly like a
+    fresh handle (no state of the first solve, e.g. the warm start of the
+    coarsest CG, carries over)."""
+    g = golden_problem
+    base, nlev, box = int(g["base"]), int(g["nlev"]), float(g["box"])
+    fine = fine_of(g)
+    other = dict(fine)
+    other["f"] = fine["f"] * -0.5 + 0.1
+    with PBELinearProblem(base, nlev, box, precision) as p:
+        p.set_fine(**fine)
+        p.buildmultilevelops()
+        r1 = p.solve(tol=1e-10, max_cycles=60)
+        x1 = p.potential().ravel().copy()
+    with PBELinearProblem(base, nlev, box, precision) as p:
+        p.set_fine(**other)
+        p.buildmultilevelops()
+        p.solve(tol=1e-10, max_cycles=60)
+        p.set_fine(**fine)
+        p.buildmultilevelops()
+        r2 = p.solve(tol=1e-10, max_cycles=60)
+        x2 = p.potential().ravel().copy()
+    assert r1.cycles == r2.cycles
+    assert np.array_equal(r1.history, r2.history)
+    assert np.array_equal(x1, x2)

@@ -140,3 +140,28 @@ def test_bench_reads_profiled_traffic():
     assert t is not None and t > 4 * 4.0e8
     assert bench.profiled_traffic("no_such_kernel", 1, "pb257", "mixed") is None
     assert bench.profiled_traffic(None, 1, "pb257", "mixed") is None
+
+
+def test_server_rejects_bad_arguments_without_gpu():
+    from multigrid_b200.serve import Server
+    for budget, inflight in ((0, 4), (1 << 30, 0), (1 << 30, 1000)):
+        with pytest.raises(_lib.PmgError) as e:
+            Server(budget, inflight)
+        assert e.value.status == _lib.PMG_ERR_ARG
+
+
+def test_native_levels_rule_matches_python():
+    """The runtime's hierarchy rule (pmg_levels_for) and levels_for agree."""
+    import ctypes
+    from multigrid_b200 import serve  # noqa: F401  (declares the symbol)
+    from multigrid_b200.molecule import levels_for
+    for n in list(range(5, 300, 4)) + [129, 161, 193, 225, 257, 513]:
+        try:
+            want = levels_for(n, max_levels=12, min_coarse=5)
+        except ValueError:
+            want = None
+        b, L = ctypes.c_int(), ctypes.c_int()
+        rc = _lib.lib.pmg_levels_for(n, 12, 5, ctypes.byref(b),
+                                     ctypes.byref(L))
+        got = (b.value, L.value) if rc == 0 else None
+        assert got == want, n
