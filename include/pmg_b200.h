@@ -267,6 +267,17 @@ int pmg_setup_fine(int n, double h, const double *atoms, int natoms,
                    const pmg_physics *phys, double *oC, double *oE,
                    double *oN, double *uC, double *f, double *x0);
 
+/* The same set-up on the GPU into device arrays (n^3 doubles each),
+ * stream-ordered on `stream` (scratch from the stream-ordered allocator);
+ * atoms are host rows, validated like pmg_setup_fine. oE oN uC oC and f are
+ * bit-identical to pmg_setup_fine (same marking bounds and sums, charges
+ * summed per grid point in atom order); x0 uses CUDA's exp and agrees to a
+ * few ulp. */
+int pmg_setup_fine_d(int n, double h, const double *atoms, int natoms,
+                     const pmg_physics *phys, double *oC, double *oE,
+                     double *oN, double *uC, double *f, double *x0,
+                     pmg_stream_t stream);
+
 /* ======================================================================
  * Problem handle: PBE_linear_problem<base, nlev, box> with runtime sizes
  * (PBE_pmgc_class.h:112-1174). Level L has n_L = base*2^L + 1 points per
@@ -297,6 +308,13 @@ long long pmg_problem_bytes(int base, int nlev, int precision);
 int pmg_problem_set_fine(pmg_problem *p, const double *oC, const double *oE,
                          const double *oN, const double *uC, const double *f,
                          const double *x0);
+
+/* Loads the finest level from atoms with the GPU set-up (pmg_setup_fine_d
+ * at spacing box / (n - 1)) straight into the problem's arrays: only the
+ * atoms cross PCIe. Replaces the class's set-up chain (initialize_boundary,
+ * initialize_epsilons, set_up_rhs; PBE_pmgc_class.h:141-349). */
+int pmg_problem_set_atoms(pmg_problem *p, const double *atoms, int natoms,
+                          const pmg_physics *phys);
 
 /* Builds the Galerkin hierarchy (P then A_c per level); trilinear != 0 uses
  * constant weights. Replaces buildmultilevelops, PBE_pmgc_class.h:351-617. */

@@ -92,6 +92,10 @@ _sig("pmg_cg_level_noalloc_d", c_int,
 _sig("pmg_kappa", c_int, ctypes.POINTER(PmgPhysics), PD, PD)
 _sig("pmg_setup_fine", c_int, c_int, c_double, PD, c_int,
      ctypes.POINTER(PmgPhysics), PD, PD, PD, PD, PD, PD)
+_sig("pmg_setup_fine_d", c_int, c_int, c_double, PD, c_int,
+     ctypes.POINTER(PmgPhysics), _V, _V, _V, _V, _V, _V, _V)
+_sig("pmg_problem_set_atoms", c_int, _V, PD, c_int,
+     ctypes.POINTER(PmgPhysics))
 
 _sig("pmg_problem_create", c_int, c_int, c_int, c_double, c_int, _V,
      ctypes.POINTER(c_void_p))

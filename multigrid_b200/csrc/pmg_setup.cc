@@ -20,48 +20,13 @@
 
 #include "../../include/pmg_b200.h"
 
+#include "pmg_physics.h"
+
 namespace {
 
-// Physical constants of the reference (scientific_quantities.h:7-15).
-constexpr double kB = 1.380649e-23;
-constexpr double kE = 1.60217663e-19;
-constexpr double kEpsSI = 8.8541878128e-12;
-constexpr double kNA = 6.0221408e23;
-constexpr double kPi = 3.14159265358979323846;
-
-// Heron/Newton square root with the reference's stopping rule
-// |g^2 - x| <= 1e-13 x, starting from 1.0 (const_sqrt,
-// scientific_quantities.h:18-25); kept so kappa rounds like the reference.
-double newton_sqrt(double x, double guess = 1.0) {
-  if (x == 0)
-    return 0;
-  for (int it = 0; it < 2000; ++it) {
-    if (fabs(guess * guess - x) <= x * 1e-13)
-      return guess;
-    guess = (guess + x / guess) / 2;
-  }
-  return guess;
-}
-
-struct Physics {
-  double eps_in, eps_out, T, kappa, eps0;
-};
-
-Physics physics(const pmg_physics &ph) {
-  Physics p;
-  p.eps_in = ph.eps_in;
-  p.eps_out = ph.eps_out;
-  p.T = ph.temperature;
-  const double beta = 1 / (kB * p.T);
-  // vacuum permittivity in e^2 / (kT * Angstrom)
-  p.eps0 = kEpsSI * 1e-10 / (kE * kE) * kB * p.T;
-  // inverse Debye length in 1/Angstrom (Debye_length_inverse_squared,
-  // Kappa, KappaA: scientific_quantities.h:38-55); IS in mol/l
-  const double is_si = 1000 * ph.ionic_strength;
-  const double inv_sq = kE * kE * beta * 2 * is_si * kNA / (p.eps_out * kEpsSI);
-  p.kappa = newton_sqrt(inv_sq) * 1e-10;
-  return p;
-}
+using pmg::Physics;
+using pmg::physics;
+using pmg::kPi;
 
 struct Grid {
   int n;
@@ -169,20 +134,18 @@ void mark_probe_surface(const Grid &g, const double *atoms, int natoms,
     cell_of(&atoms[5 * a], ci);
     cells[((size_t)ci[2] * nc[1] + ci[1]) * nc[0] + ci[0]].push_back(a);
   }
-  const int kPts = 96;
-  const double golden = kPi * (3.0 - sqrt(5.0));
+  pmg::ProbeDir dirs[pmg::kProbePoints];
+  pmg::probe_directions(dirs);
   std::vector<double> probes;
   for (int a = 0; a < natoms; ++a) {
     const double R = atoms[5 * a + 3] + probe;
     int ci[3];
     cell_of(&atoms[5 * a], ci);
-    for (int s = 0; s < kPts; ++s) {
-      const double zz = 1 - 2 * (s + 0.5) / kPts;
-      const double rr = sqrt(std::max(0.0, 1 - zz * zz));
-      const double ph = golden * s;
-      const double pc[3] = {atoms[5 * a] + R * rr * cos(ph),
-                            atoms[5 * a + 1] + R * rr * sin(ph),
-                            atoms[5 * a + 2] + R * zz};
+    for (int s = 0; s < pmg::kProbePoints; ++s) {
+      const pmg::ProbeDir &u = dirs[s];
+      const double pc[3] = {atoms[5 * a] + R * u.rr * u.c,
+                            atoms[5 * a + 1] + R * u.rr * u.s,
+                            atoms[5 * a + 2] + R * u.zz};
       bool free = true;
       for (int dz = -1; dz <= 1 && free; ++dz)
         for (int dy = -1; dy <= 1 && free; ++dy)

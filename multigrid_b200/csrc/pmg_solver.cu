@@ -71,6 +71,12 @@ struct Arena {
   }
 };
 
+// Fine-level set-up from atoms on the GPU (pmg_setup_gpu.cu).
+int setup_fine_device(int n, double h, const double *atoms_host, int natoms,
+                      const pmg_physics *ph, double *oC, double *oE,
+                      double *oN, double *uC, double *f, double *x0,
+                      cudaStream_t st);
+
 // Device-resident state of one solve (pmg_solve_start): parameters, the
 // residual history and the outcome, written by the solve graph's control
 // kernels and copied to pinned host memory at its end.
@@ -747,6 +753,24 @@ void drop_graphs(pmg_problem *p) {
   }
 }
 
+// A new problem starts from the state of a freshly constructed class: the
+// coarse iterates are zero (the coarsest CG warm-starts from its level's
+// iterate, so a previous solve's values would change the result).
+int new_problem_loaded(pmg_problem *p) {
+  for (int L = 1; L < p->nlev; ++L) {
+    LevelBuf &c = p->lv[L];
+    if (c.x)
+      PMG_CUDA_TRY(
+          cudaMemsetAsync(c.x, 0, sizeof(double) * c.n3, p->stream));
+    if (c.x32)
+      PMG_CUDA_TRY(
+          cudaMemsetAsync(c.x32, 0, sizeof(float) * c.n3, p->stream));
+  }
+  p->fine_set = true;
+  p->built = false;
+  return PMG_OK;
+}
+
 } // namespace
 
 // ---------------------------------------------------------------------------
@@ -908,21 +932,23 @@ int pmg_problem_set_fine(pmg_problem *p, const double *oC, const double *oE,
   for (int q = 0; q < 6; ++q)
     PMG_CUDA_TRY(
         cudaMemcpyAsync(dst[q], src[q], b, cudaMemcpyDefault, p->stream));
-  // A new problem starts from the state of a freshly constructed class: the
-  // coarse iterates are zero (the coarsest CG warm-starts from its level's
-  // iterate, so a previous solve's values would change the result).
-  for (int L = 1; L < p->nlev; ++L) {
-    LevelBuf &c = p->lv[L];
-    if (c.x)
-      PMG_CUDA_TRY(
-          cudaMemsetAsync(c.x, 0, sizeof(double) * c.n3, p->stream));
-    if (c.x32)
-      PMG_CUDA_TRY(
-          cudaMemsetAsync(c.x32, 0, sizeof(float) * c.n3, p->stream));
+  return new_problem_loaded(p);
+}
+
+int pmg_problem_set_atoms(pmg_problem *p, const double *atoms, int natoms,
+                          const pmg_physics *phys) {
+  if (!p || !phys || natoms < 0 || (natoms > 0 && !atoms)) {
+    set_last_message("pmg_problem_set_atoms: bad argument");
+    return PMG_ERR_ARG;
   }
-  p->fine_set = true;
-  p->built = false;
-  return PMG_OK;
+  LevelBuf &v = p->lv[p->nlev];
+  const double h = p->box / (double)(v.n - 1);
+  const int rc = setup_fine_device(v.n, h, atoms, natoms, phys, v.op[kOC],
+                                   v.op[kOE], v.op[kON], v.op[kUC], v.f, v.x,
+                                   p->stream);
+  if (rc)
+    return rc;
+  return new_problem_loaded(p);
 }
 
 int pmg_build_hierarchy(pmg_problem *p, int trilinear) {

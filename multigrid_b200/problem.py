@@ -135,6 +135,19 @@ class PBELinearProblem:
                                     self.physics)
             self.set_fine(**self._fine)
 
+    def set_atoms(self, atoms, physics: dict | None = None) -> None:
+        """Loads the finest level from atoms with the GPU set-up
+        (pmg_problem_set_atoms): only the atoms cross PCIe. Equal to the host
+        set-up bit for bit except the Debye-Hueckel boundary values (CUDA's
+        exp, a few ulp)."""
+        atoms = np.ascontiguousarray(atoms, dtype=np.float64).reshape(-1, 5)
+        ph = physics_struct(physics or self.physics)
+        _lib.check("pmg_problem_set_atoms", _lib.lib.pmg_problem_set_atoms(
+            self._h, _dptr(atoms), len(atoms), ctypes.byref(ph)))
+        # the atoms are copied before the call returns (pageable source)
+        self._atoms = None
+        self._fine = None
+
     def initialize_boundary(self, atoms) -> None:
         """Debye-Hueckel boundary values on the finest shell."""
         self._setup_from_atoms(atoms)
