@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--workload", default="pb257")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    # skip the batched (96 molecules) and serving (Poisson load) legs
+    ap.add_argument("--no-extras", action="store_true")
     # one precision, no end-to-end or kernel legs: a short run for profilers
     ap.add_argument("--quick", action="store_true")
     return ap.parse_args()
@@ -212,6 +214,12 @@ def run_reference(args):
         return 0
     from multigrid_b200.molecule import WORKLOADS
     from multigrid_b200.problem import setup_fine
+    if args.workload not in WORKLOADS:
+        print(json.dumps({"impl": "reference", "unavailable":
+                          f"{args.workload}: the reference solves one "
+                          "molecule per process; its arm is timed on the "
+                          "single-solve workloads"}))
+        return 0
     w = WORKLOADS[args.workload]
     fine = setup_fine(w.n, w.h, w.atoms(), w.physics)
     # FP64 cycle count of this workload (used only by the extrapolated
@@ -330,13 +338,173 @@ def profile_solve(p, step, dev, esz):
     return rows
 
 
+# ---------------------------------------------------------------------------
+# batched solves and serving (molecules of the batched set)
+# ---------------------------------------------------------------------------
+def batch_molecules(count: int):
+    from multigrid_b200.molecule import batch_workloads
+    return [(w, w.atoms()) for w in batch_workloads(count)]
+
+
+def run_batch(count: int = 96, reps: int = 2, warm: int = 1) -> dict:
+    """`count` molecules of the batched set (97^3-161^3 grids, 200-6000
+    atoms), each a full solve from its atoms (GPU set-up, hierarchy,
+    V-cycles to 1e-10, potential copied out): all in flight at once through
+    the serving runtime (mixed and FP64), against the same solves one after
+    another through the problem handle (plain FP64). Wall time between
+    device synchronisations (the work spans many streams)."""
+    import ctypes
+    import torch
+    from multigrid_b200 import PBELinearProblem, _lib
+    from multigrid_b200.serve import Server
+    mols = batch_molecules(count)
+    outs = [torch.empty(w.n ** 3, dtype=torch.float64, device="cuda")
+            for w, _ in mols]
+    out = {"molecules": count,
+           "grids": sorted({w.n for w, _ in mols}),
+           "levels": sorted({w.nlev for w, _ in mols})}
+    for prec in ("mixed", "fp64"):
+        times, cycles = [], []
+        with Server(120 << 30, max_inflight=count) as srv:
+            for rep in range(warm + reps):
+                torch.cuda.synchronize()
+                t = time.perf_counter()
+                for i, (w, at) in enumerate(mols):
+                    srv.submit(w.base, w.nlev, w.box, None, prec,
+                               out=outs[i], tag=rep * count + i, atoms=at,
+                               physics=w.physics)
+                done = srv.drain(count)
+                torch.cuda.synchronize()
+                if rep >= warm:
+                    times.append(time.perf_counter() - t)
+                bad = [c.message for c in done if not c.ok]
+                if bad:
+                    raise RuntimeError(f"batched {prec} solve failed: {bad[0]}")
+                cycles = [c.cycles for c in done]
+            st = srv.stats()
+        t = statistics.median(times)
+        out[f"concurrent_{prec}"] = {
+            "solves_per_s": count / t, "ms": 1000 * t,
+            "cycles_min": min(cycles), "cycles_max": max(cycles),
+            "peak_device_gib": st["peak_bytes"] / 2 ** 30}
+    probs = {}
+    times = []
+    for rep in range(warm + reps):
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        for i, (w, at) in enumerate(mols):
+            key = (w.base, w.nlev)
+            if key not in probs:
+                probs[key] = PBELinearProblem(w.base, w.nlev, w.box, "fp64",
+                                              w.physics)
+            p = probs[key]
+            p.set_atoms(at)
+            p.buildmultilevelops()
+            p.solve(TOL, MAX_CYCLES)
+            _lib.check("pmg_get_potential", _lib.lib.pmg_get_potential(
+                p._h, ctypes.c_void_p(outs[i].data_ptr())))
+        torch.cuda.synchronize()
+        if rep >= warm:
+            times.append(time.perf_counter() - t)
+    for p in probs.values():
+        p.close()
+    t = statistics.median(times)
+    out["sequential_fp64"] = {"solves_per_s": count / t, "ms": 1000 * t}
+    out["speedup_concurrent_mixed_vs_sequential_fp64"] = (
+        out["concurrent_mixed"]["solves_per_s"] / (count / t))
+    return out
+
+
+def run_serving(count: int = 128,
+                loads=(0.25, 0.5, 0.75, 0.9, 1.1)) -> dict:
+    """Open-loop Poisson arrivals of PB solve requests (molecules of the
+    batched set, from atoms) at rates swept up to past saturation, through
+    the serving runtime with a 120 GB budget; p50/p99 latency (submit to
+    potential on the device) and achieved solves/s per rate, mixed and
+    FP64. Saturation = the closed-loop rate with every request in flight."""
+    import torch
+    from multigrid_b200.serve import Server, open_loop, percentile
+    from multigrid_b200.serve import poisson_arrivals
+    mols = batch_molecules(count)
+    outs = [torch.empty(w.n ** 3, dtype=torch.float64, device="cuda")
+            for w, _ in mols]
+    res = {"requests_per_rate": count, "budget_gb": 120}
+    for prec in ("mixed", "fp64"):
+        with Server(120 << 30, max_inflight=32) as srv:
+            def submit_one(s, i, prec=prec):
+                w, at = mols[i]
+                s.submit(w.base, w.nlev, w.box, None, prec, out=outs[i],
+                         tag=i, atoms=at, physics=w.physics)
+            # warm-up + capacity: everything in flight at once
+            for _ in range(2):
+                torch.cuda.synchronize()
+                t = time.perf_counter()
+                for i in range(count):
+                    submit_one(srv, i)
+                srv.drain(count)
+                cap = count / (time.perf_counter() - t)
+            rows = []
+            for k, f in enumerate(loads):
+                rate = f * cap
+                arr = poisson_arrivals(rate, count, seed=100 + k)
+                done, wall = open_loop(srv, arr, submit_one)
+                bad = [c.message for c in done if not c.ok]
+                if bad:
+                    raise RuntimeError(f"served {prec} solve failed: {bad[0]}")
+                lat = [1000 * c.latency for c in done]
+                rows.append({"offered_per_s": rate,
+                             "achieved_per_s": count / wall,
+                             "p50_ms": percentile(lat, 50),
+                             "p99_ms": percentile(lat, 99)})
+        res[prec] = {"saturation_per_s": cap, "rates": rows}
+    return res
+
+
+def run_mode(args, world: int, rank: int) -> int:
+    """--workload batch96 / serve: the batched or serving measurement alone
+    (every rank runs its own replica; rank 0 reports)."""
+    if args.workload == "batch96":
+        res = run_batch(96, reps=max(1, args.steps), warm=max(1, args.warmup))
+        value = res["concurrent_mixed"]["solves_per_s"]
+        line = {"metric": METRIC + " (batched)", "value": world * value,
+                "unit": UNIT, "n_gpus": world, "steps": max(1, args.steps),
+                "warmup": max(1, args.warmup),
+                "ms_per_step": res["concurrent_mixed"]["ms"],
+                "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32+f64",
+                "data": "synthetic",
+                "config": {"workload": "batch96: 96 synthetic molecules, "
+                           "200-6000 atoms, 0.5 A, grids 97-161^3, mixed, "
+                           "from atoms (GPU set-up), all in flight"},
+                "batch": res}
+    else:
+        res = run_serving(128)
+        value = res["mixed"]["saturation_per_s"]
+        line = {"metric": "PB solves/s at saturation; p50/p99 latency",
+                "value": world * value, "unit": UNIT, "n_gpus": world,
+                "steps": 1, "warmup": 2, "ms_per_step": 1000.0 / value,
+                "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32+f64",
+                "data": "synthetic",
+                "config": {"workload": "serve: open-loop Poisson arrivals "
+                           "of batched-set molecules, 120 GB budget"},
+                "serving": res}
+    if rank == 0:
+        print(json.dumps(line))
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    # concurrent solves run on many streams: give them hardware queues
+    os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
     import torch
 
     world, rank, local = dist_setup(args)
+    if args.workload in ("batch96", "serve"):
+        return run_mode(args, world, rank)
     from multigrid_b200 import PBELinearProblem
     from multigrid_b200.molecule import WORKLOADS
     from multigrid_b200.problem import setup_fine
@@ -418,8 +586,31 @@ def main():
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks(world, e0.elapsed_time(e1))
+    e2e_arrays = {"value": world * k_e2e / (e2e_ms / 1000.0), "unit": UNIT,
+                  "h2d_bytes_per_step": 6 * n3 * 8,
+                  "d2h_bytes_per_step": n3 * 8,
+                  "path": "fine-level arrays from pinned host memory "
+                          "(pmg_problem_set_fine), potential to host"}
+    # the class's own entry: atoms in (GPU set-up), potential out
+    atoms_host = np.ascontiguousarray(atoms)
+    barrier(world)
+    e0.record(stream)
+    for _ in range(k_e2e):
+        p.set_atoms(atoms_host)
+        p.buildmultilevelops()
+        p.solve(TOL, MAX_CYCLES)
+        _lib.check("pmg_get_potential", _lib.lib.pmg_get_potential(
+            p._h, ctypes.c_void_p(out_host.data_ptr())))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(world, e0.elapsed_time(e1))
     e2e = {"value": world * k_e2e / (e2e_ms / 1000.0), "unit": UNIT,
-           "h2d_bytes_per_step": 6 * n3 * 8, "d2h_bytes_per_step": n3 * 8}
+           "h2d_bytes_per_step": int(atoms_host.nbytes),
+           "d2h_bytes_per_step": n3 * 8,
+           "path": "atoms from host (pmg_problem_set_atoms: GPU set-up), "
+                   "hierarchy build, solve, potential to pinned host "
+                   "memory; the set-up is extra work the device-resident "
+                   "value excludes"}
 
     # per-phase timing of one more solve (CUDA events inside the cycle graph,
     # on the solver's stream); the dominant bandwidth-bound phase gives the
@@ -480,13 +671,17 @@ def main():
             "fine_unknowns_x_cycles_per_s": value * (w.n - 2) ** 3 *
             prim["cycles"][-1],
             "gpu_launches": prim["launches"],
-            "e2e": e2e, "roofline": roofline,
+            "e2e": e2e, "e2e_fine_arrays": e2e_arrays,
+            "roofline": roofline,
             "phases_top": [{k: (round(v, 3) if isinstance(v, float) else v)
                             for k, v in r.items() if k != "bytes"}
                            for r in phases[:8]],
             "cpu_baseline": cpu,
             "clocks": prim["clocks"],
         }
+        if world == 1 and not args.no_extras:
+            line["batch"] = run_batch(96)
+            line["serving"] = run_serving(128)
         print(json.dumps(line))
     for r in results.values():
         r["p"].close()

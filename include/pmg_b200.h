@@ -359,6 +359,16 @@ int pmg_solve_finish(pmg_problem *p, int *cycles, double *relres,
  * device). */
 int pmg_get_potential(pmg_problem *p, double *dst);
 
+/* pmg_get_potential without the wait: the copy is queued on the problem's
+ * stream (dst must stay valid until the stream reaches it). */
+int pmg_get_potential_async(pmg_problem *p, double *dst);
+
+/* Moves the problem to another stream (no solve may be in flight); work
+ * already queued on the old stream stays ordered before later work. The
+ * captured graphs are launched on whichever stream the problem has. NULL
+ * returns a problem created without a stream to the stream it created. */
+int pmg_problem_set_stream(pmg_problem *p, pmg_stream_t stream);
+
 /* Copies level L's hierarchy out (host or device dst): 27 prolongation
  * arrays then 14 operator arrays, n_L^3 doubles each; L in [1, nlev-1]. */
 int pmg_get_level(pmg_problem *p, int level, double *dst);
@@ -412,6 +422,12 @@ typedef struct pmg_request {
   long long tag;           /* caller's identifier, echoed back            */
   int hierarchy;           /* 0: levels as given; 1: the deepest levels   */
                            /* of the same grid (pmg_levels_for(n, 12, 5)) */
+  const double *atoms;     /* non-NULL: load the fine level from these    */
+                           /* host rows (x y z radius charge) with the GPU*/
+                           /* set-up (pmg_problem_set_atoms); fine[] is   */
+                           /* then ignored                                */
+  int natoms;
+  pmg_physics physics;     /* set-up parameters when atoms is non-NULL    */
 } pmg_request;
 
 typedef struct pmg_completion {
@@ -427,6 +443,10 @@ typedef struct pmg_server_stats {
   int queued, inflight, idle_problems;
   long long held_bytes, peak_bytes, budget_bytes;
   long long completed, created_problems, evicted_problems;
+  /* host time of the worker: issuing requests (set-up / load, build,
+   * solve launch) and retiring them (results copied out), total and
+   * longest single call, seconds */
+  double issue_s, issue_max_s, retire_s, retire_max_s;
 } pmg_server_stats;
 
 /* (base, nlev) with n = base * 2^nlev + 1, the largest nlev <= max_levels

@@ -155,4 +155,10 @@ namespace pmg {
 void set_last_error(cudaError_t e, const char *what, const char *file,
                     int line);
 void set_last_message(const char *msg);
+// Stream-ordered scratch of the library: a memory pool of its own per
+// device that keeps freed memory (release threshold: unlimited), so
+// allocations after the first never map memory again and synchronising a
+// stream never trims it (trimming can wait on work of other streams).
+cudaError_t scratch_alloc(void **ptr, size_t bytes, cudaStream_t s);
+cudaError_t scratch_free(void *ptr, cudaStream_t s);
 } // namespace pmg

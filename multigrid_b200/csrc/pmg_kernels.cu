@@ -1,3 +1,4 @@
+#include <mutex>
 // Non-template kernels and the per-kernel C-ABI entry points (pmgc names).
 #include <math.h>
 #include <stdio.h>
@@ -22,6 +23,52 @@ void set_last_error(cudaError_t e, const char *what, const char *file,
 }
 void set_last_message(const char *msg) {
   snprintf(g_last_error, sizeof(g_last_error), "%s", msg);
+}
+
+namespace {
+std::mutex g_pool_mutex;
+cudaMemPool_t g_pools[64] = {};
+} // namespace
+
+static cudaError_t scratch_pool(cudaMemPool_t *out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess)
+    return e;
+  if (dev < 0 || dev >= 64)
+    return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lk(g_pool_mutex);
+  if (!g_pools[dev]) {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool = nullptr;
+    e = cudaMemPoolCreate(&pool, &props);
+    if (e != cudaSuccess)
+      return e;
+    unsigned long long keep = ~0ull;
+    e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    if (e != cudaSuccess) {
+      cudaMemPoolDestroy(pool);
+      return e;
+    }
+    g_pools[dev] = pool;
+  }
+  *out = g_pools[dev];
+  return cudaSuccess;
+}
+
+cudaError_t scratch_alloc(void **ptr, size_t bytes, cudaStream_t s) {
+  cudaMemPool_t pool = nullptr;
+  const cudaError_t e = scratch_pool(&pool);
+  if (e != cudaSuccess)
+    return e;
+  return cudaMallocFromPoolAsync(ptr, bytes ? bytes : 1, pool, s);
+}
+
+cudaError_t scratch_free(void *ptr, cudaStream_t s) {
+  return cudaFreeAsync(ptr, s);
 }
 
 // ---------------------------------------------------------------------------
@@ -250,7 +297,7 @@ static int gs27_inplace(const Dims &d, const Op14<T> &A, const T *cc,
   }
   T *alt = nullptr;
   const size_t bytes = sizeof(T) * d.count();
-  PMG_CUDA_TRY(cudaMallocAsync((void **)&alt, bytes, s));
+  PMG_CUDA_TRY(scratch_alloc((void **)&alt, bytes, s));
   int rc = PMG_OK;
   cudaError_t e = cudaSuccess;
   if (zero_init)
@@ -263,7 +310,7 @@ static int gs27_inplace(const Dims &d, const Op14<T> &A, const T *cc,
     if (rc == PMG_OK && res != x)
       e = cudaMemcpyAsync(x, res, bytes, cudaMemcpyDeviceToDevice, s);
   }
-  cudaFreeAsync(alt, s);
+  scratch_free(alt, s);
   if (e != cudaSuccess) {
     set_last_error(e, "Vgsrb27x", __FILE__, __LINE__);
     return PMG_ERR_CUDA;
@@ -575,7 +622,7 @@ int pmg_cg_level_d(int nx, int ny, int nz, const double *const *a14,
   // r, p, Ap (zero shells) and the two status words, stream-ordered.
   char *ws = nullptr;
   const size_t bytes = 3 * n3 * sizeof(double) + 2 * sizeof(int);
-  PMG_CUDA_TRY(cudaMallocAsync((void **)&ws, bytes, s));
+  PMG_CUDA_TRY(scratch_alloc((void **)&ws, bytes, s));
   int rc = PMG_OK;
   int host_status[2] = {0, 0};
   double *r = (double *)ws, *p = r + n3, *ap = p + n3;
@@ -589,7 +636,7 @@ int pmg_cg_level_d(int nx, int ny, int nz, const double *const *a14,
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(host_status, status, sizeof(host_status),
                         cudaMemcpyDeviceToHost, s);
-  cudaFreeAsync(ws, s);
+  scratch_free(ws, s);
   if (e == cudaSuccess)
     e = cudaStreamSynchronize(s);
   if (rc != PMG_OK)

@@ -44,7 +44,21 @@ struct Slot {
 struct Flight {
   pmg_request req;
   Slot slot;
+  int lane = -1;
+  bool copy_queued = false; // the result copy is queued before the event
   double t_submit = 0, t_admit = 0;
+};
+
+// A lane: a stream an admitted request runs on, its completion event and a
+// pinned staging buffer for the request's atoms. One request per lane at a
+// time, so at most `lanes` requests are in flight; with at most as many
+// lanes as the device has hardware work queues
+// (CUDA_DEVICE_MAX_CONNECTIONS), no request queues behind another's solve.
+struct Lane {
+  cudaStream_t stream = nullptr;
+  cudaEvent_t done = nullptr;
+  double *pinned = nullptr;
+  size_t pinned_doubles = 0;
 };
 
 struct Queued {
@@ -68,10 +82,13 @@ struct pmg_server {
   bool stopping = false;
 
   // worker-owned (read under mu for stats)
+  std::vector<Lane> lanes;
+  std::vector<int> free_lanes;
   std::vector<Flight> inflight;
   std::list<Slot> idle; // front = most recently used
   long long held = 0, peak = 0;
   long long completed = 0, created = 0, evicted = 0;
+  double issue_s = 0, issue_max_s = 0, retire_s = 0, retire_max_s = 0;
 
   std::thread worker;
 
@@ -118,14 +135,56 @@ void resolve_levels(pmg_request &r) {
   }
 }
 
-// Issues set_fine -> build -> solve_start for a request on its problem.
-int issue(const pmg_request &r, pmg_problem *p) {
-  int rc = pmg_problem_set_fine(p, r.fine[0], r.fine[1], r.fine[2], r.fine[3],
-                                r.fine[4], r.fine[5]);
+// True when dst may be written by a copy queued on a stream: device,
+// managed or pinned host memory (pageable memory is copied synchronously
+// after the solve instead).
+bool async_target(const void *dst) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, dst) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged ||
+         a.type == cudaMemoryTypeHost;
+}
+
+// Issues load -> build -> solve_start (-> result copy) -> lane event for a
+// request on its problem, all on the lane's stream; never waits on the GPU.
+int issue(const pmg_request &r, pmg_problem *p, Lane &lane, Flight &f) {
+  int rc = pmg_problem_set_stream(p, lane.stream);
+  if (rc != PMG_OK)
+    return rc;
+  if (r.atoms) {
+    // stage the atoms in pinned memory so their copy is queued, not waited
+    // for (the lane's previous request has finished with the buffer)
+    const size_t need = 5 * (size_t)(r.natoms > 0 ? r.natoms : 1);
+    if (need > lane.pinned_doubles) {
+      if (lane.pinned)
+        cudaFreeHost(lane.pinned);
+      lane.pinned = nullptr;
+      lane.pinned_doubles = 0;
+      if (cudaMallocHost((void **)&lane.pinned, need * sizeof(double)) !=
+          cudaSuccess)
+        return PMG_ERR_NOMEM;
+      lane.pinned_doubles = need;
+    }
+    std::memcpy(lane.pinned, r.atoms, sizeof(double) * 5 * r.natoms);
+    rc = pmg_problem_set_atoms(p, lane.pinned, r.natoms, &r.physics);
+  } else {
+    rc = pmg_problem_set_fine(p, r.fine[0], r.fine[1], r.fine[2], r.fine[3],
+                              r.fine[4], r.fine[5]);
+  }
   if (rc == PMG_OK)
     rc = pmg_build_hierarchy(p, 0);
   if (rc == PMG_OK)
     rc = pmg_solve_start(p, r.tol, r.max_cycles);
+  f.copy_queued = false;
+  if (rc == PMG_OK && r.potential && async_target(r.potential)) {
+    rc = pmg_get_potential_async(p, r.potential);
+    f.copy_queued = rc == PMG_OK;
+  }
+  if (rc == PMG_OK && cudaEventRecord(lane.done, lane.stream) != cudaSuccess)
+    rc = PMG_ERR_CUDA;
   return rc;
 }
 
@@ -188,7 +247,7 @@ bool step(pmg_server *s) {
     Queued q;
     {
       std::lock_guard<std::mutex> lk(s->mu);
-      if (s->queue.empty() || (int)s->inflight.size() >= s->max_inflight)
+      if (s->queue.empty() || s->free_lanes.empty())
         break;
       q = s->queue.front();
     }
@@ -218,21 +277,33 @@ bool step(pmg_server *s) {
     if (rc == PMG_ERR_BUDGET)
       break; // wait for a completion to free memory
     const double t_admit = s->now();
+    Flight f;
+    {
+      std::lock_guard<std::mutex> lk(s->mu);
+      f.lane = s->free_lanes.back();
+      s->free_lanes.pop_back();
+    }
     if (rc == PMG_OK)
-      rc = issue(q.req, slot.prob);
+      rc = issue(q.req, slot.prob, s->lanes[f.lane], f);
+    const double dt_issue = s->now() - t_admit;
     std::lock_guard<std::mutex> lk(s->mu);
+    s->issue_s += dt_issue;
+    s->issue_max_s = std::max(s->issue_max_s, dt_issue);
     s->queue.pop_front();
     progress = true;
     if (rc != PMG_OK) {
-      if (slot.prob)
+      if (slot.prob) {
+        // let the lane drain what was queued before reusing it
+        cudaStreamSynchronize(s->lanes[f.lane].stream);
         release(s, slot, false);
+      }
+      s->free_lanes.push_back(f.lane);
       s->done.push_back(make_completion(q.req, rc, 0, 0.0, q.t_submit,
                                         t_admit, s->now()));
       ++s->completed;
       s->cv_done.notify_all();
       continue;
     }
-    Flight f;
     f.req = q.req;
     f.slot = slot;
     f.t_submit = q.t_submit;
@@ -242,25 +313,37 @@ bool step(pmg_server *s) {
   // retirement
   for (size_t i = 0; i < s->inflight.size();) {
     Flight &f = s->inflight[i];
-    int done = 0;
-    int rc = pmg_solve_poll(f.slot.prob, &done);
-    if (rc == PMG_OK && !done) {
+    const cudaError_t q = cudaEventQuery(s->lanes[f.lane].done);
+    if (q == cudaErrorNotReady) {
       ++i;
       continue;
     }
+    int rc = q == cudaSuccess ? PMG_OK : PMG_ERR_CUDA;
+    if (q != cudaSuccess)
+      (void)cudaGetLastError();
     int cycles = 0;
     double relres = 0.0;
+    const double t_ret = s->now();
     if (rc == PMG_OK)
       rc = pmg_solve_finish(f.slot.prob, &cycles, &relres, nullptr);
-    if ((rc == PMG_OK || rc == PMG_ERR_DIVERGED) && f.req.potential) {
+    if ((rc == PMG_OK || rc == PMG_ERR_DIVERGED) && f.req.potential &&
+        !f.copy_queued) {
       const int rc2 = pmg_get_potential(f.slot.prob, f.req.potential);
       if (rc == PMG_OK)
         rc = rc2;
     }
     pmg_completion c = make_completion(f.req, rc, cycles, relres, f.t_submit,
                                        f.t_admit, s->now());
+    // park the problem on its own stream while the lane is idle, so its next
+    // lane does not wait for whatever this lane runs next
+    if (pmg_problem_set_stream(f.slot.prob, nullptr) != PMG_OK && rc == PMG_OK)
+      rc = PMG_ERR_CUDA;
+    const double dt_ret = s->now() - t_ret;
     std::lock_guard<std::mutex> lk(s->mu);
+    s->retire_s += dt_ret;
+    s->retire_max_s = std::max(s->retire_max_s, dt_ret);
     release(s, f.slot, rc == PMG_OK || rc == PMG_ERR_DIVERGED);
+    s->free_lanes.push_back(f.lane);
     s->done.push_back(c);
     ++s->completed;
     s->inflight.erase(s->inflight.begin() + (long)i);
@@ -293,6 +376,14 @@ void worker_main(pmg_server *s) {
     s->held -= sl.bytes;
   }
   s->idle.clear();
+  for (Lane &l : s->lanes) {
+    cudaStreamSynchronize(l.stream);
+    cudaEventDestroy(l.done);
+    cudaStreamDestroy(l.stream);
+    if (l.pinned)
+      cudaFreeHost(l.pinned);
+  }
+  s->lanes.clear();
 }
 
 } // namespace
@@ -328,6 +419,24 @@ int pmg_server_create(long long budget_bytes, int max_inflight,
   s->budget = budget_bytes;
   s->max_inflight = max_inflight;
   s->t0 = Clock::now();
+  s->lanes.resize(max_inflight);
+  for (int l = 0; l < max_inflight; ++l) {
+    Lane &ln = s->lanes[l];
+    if (cudaStreamCreateWithFlags(&ln.stream, cudaStreamNonBlocking) !=
+            cudaSuccess ||
+        cudaEventCreateWithFlags(&ln.done, cudaEventDisableTiming) !=
+            cudaSuccess) {
+      for (Lane &x : s->lanes) {
+        if (x.done)
+          cudaEventDestroy(x.done);
+        if (x.stream)
+          cudaStreamDestroy(x.stream);
+      }
+      delete s;
+      return PMG_ERR_CUDA;
+    }
+    s->free_lanes.push_back(max_inflight - 1 - l);
+  }
   s->worker = std::thread(worker_main, s);
   *out = s;
   return PMG_OK;
@@ -339,9 +448,14 @@ int pmg_server_submit(pmg_server *s, const pmg_request *r) {
   if (r->max_cycles < 0 || r->max_cycles > 1024 || !(r->tol >= 0.0) ||
       (r->precision != PMG_PREC_FP64 && r->precision != PMG_PREC_MIXED))
     return PMG_ERR_ARG;
-  for (int q = 0; q < 6; ++q)
-    if (!r->fine[q])
+  if (r->atoms) {
+    if (r->natoms < 0)
       return PMG_ERR_ARG;
+  } else {
+    for (int q = 0; q < 6; ++q)
+      if (!r->fine[q])
+        return PMG_ERR_ARG;
+  }
   std::lock_guard<std::mutex> lk(s->mu);
   if (s->stopping)
     return PMG_ERR_STATE;
@@ -383,6 +497,10 @@ int pmg_server_get_stats(pmg_server *s, pmg_server_stats *st) {
   st->completed = s->completed;
   st->created_problems = s->created;
   st->evicted_problems = s->evicted;
+  st->issue_s = s->issue_s;
+  st->issue_max_s = s->issue_max_s;
+  st->retire_s = s->retire_s;
+  st->retire_max_s = s->retire_max_s;
   return PMG_OK;
 }
 

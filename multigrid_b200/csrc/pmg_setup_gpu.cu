@@ -20,7 +20,7 @@
 //             faces; exp() is CUDA's, so values agree with the host's to a
 //             few ulp.
 // All work is stream-ordered on the caller's stream; scratch comes from the
-// stream-ordered allocator.
+// library's stream-ordered pool.
 #include <cub/device/device_radix_sort.cuh>
 
 #include <vector>
@@ -290,12 +290,12 @@ struct Scratch {
   explicit Scratch(cudaStream_t st) : s(st) {}
   ~Scratch() {
     for (void *p : ptrs)
-      cudaFreeAsync(p, s);
+      scratch_free(p, s);
   }
   template <typename T> cudaError_t take(T **p, size_t count) {
     void *q = nullptr;
-    const cudaError_t e = cudaMallocAsync(&q, sizeof(T) * (count ? count : 1),
-                                          s);
+    const cudaError_t e = scratch_alloc(&q, sizeof(T) * (count ? count : 1),
+                                        s);
     if (e == cudaSuccess)
       ptrs.push_back(q);
     *p = (T *)q;

@@ -100,6 +100,7 @@ struct pmg_problem {
   double box = 0;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
+  cudaStream_t created_stream = nullptr; // destroyed with the problem
   char *arena = nullptr;
   size_t arena_bytes = 0;
   LevelBuf lv[kMaxLevels + 1];
@@ -826,6 +827,8 @@ int pmg_problem_create(int base, int nlev, double box, int precision,
   } else {
     e = cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking);
     p->own_stream = e == cudaSuccess;
+    if (p->own_stream)
+      p->created_stream = p->stream;
   }
   if (e == cudaSuccess)
     e = cudaMallocHost((void **)&p->h_pinned, 4 * sizeof(double));
@@ -864,8 +867,10 @@ int pmg_problem_destroy(pmg_problem *p) {
     cudaFree(p->arena);
   if (p->h_pinned)
     cudaFreeHost(p->h_pinned);
-  if (p->own_stream)
-    cudaStreamDestroy(p->stream);
+  if (p->created_stream) {
+    cudaStreamSynchronize(p->created_stream);
+    cudaStreamDestroy(p->created_stream);
+  }
   delete p;
   return PMG_OK;
 }
@@ -1187,6 +1192,40 @@ int pmg_get_potential(pmg_problem *p, double *dst) {
   PMG_CUDA_TRY(cudaMemcpyAsync(dst, v.x, sizeof(double) * v.n3,
                                cudaMemcpyDefault, p->stream));
   PMG_CUDA_TRY(cudaStreamSynchronize(p->stream));
+  return PMG_OK;
+}
+
+int pmg_get_potential_async(pmg_problem *p, double *dst) {
+  if (!p || !dst)
+    return PMG_ERR_ARG;
+  LevelBuf &v = p->lv[p->nlev];
+  PMG_CUDA_TRY(cudaMemcpyAsync(dst, v.x, sizeof(double) * v.n3,
+                               cudaMemcpyDefault, p->stream));
+  return PMG_OK;
+}
+
+int pmg_problem_set_stream(pmg_problem *p, pmg_stream_t stream) {
+  if (!p || (!stream && !p->created_stream)) {
+    set_last_message("pmg_problem_set_stream: null argument");
+    return PMG_ERR_ARG;
+  }
+  if (!stream)
+    stream = (pmg_stream_t)p->created_stream;
+  if (p->solve_pending) {
+    set_last_message("pmg_problem_set_stream: a solve is in flight");
+    return PMG_ERR_STATE;
+  }
+  if ((cudaStream_t)stream == p->stream)
+    return PMG_OK;
+  // work already queued on the old stream precedes work on the new one
+  cudaEvent_t ev = nullptr;
+  PMG_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  cudaError_t e = cudaEventRecord(ev, p->stream);
+  if (e == cudaSuccess)
+    e = cudaStreamWaitEvent((cudaStream_t)stream, ev, 0);
+  cudaEventDestroy(ev);
+  PMG_CUDA_TRY(e);
+  p->stream = (cudaStream_t)stream;
   return PMG_OK;
 }
 

@@ -33,7 +33,8 @@ class _Request(ctypes.Structure):
                 ("precision", c_int), ("fine", c_void_p * 6),
                 ("potential", c_void_p), ("tol", c_double),
                 ("max_cycles", c_int), ("tag", c_longlong),
-                ("hierarchy", c_int)]
+                ("hierarchy", c_int), ("atoms", c_void_p),
+                ("natoms", c_int), ("physics", _lib.PmgPhysics)]
 
 
 class _Completion(ctypes.Structure):
@@ -48,7 +49,9 @@ class _Stats(ctypes.Structure):
                 ("idle_problems", c_int), ("held_bytes", c_longlong),
                 ("peak_bytes", c_longlong), ("budget_bytes", c_longlong),
                 ("completed", c_longlong), ("created_problems", c_longlong),
-                ("evicted_problems", c_longlong)]
+                ("evicted_problems", c_longlong), ("issue_s", c_double),
+                ("issue_max_s", c_double), ("retire_s", c_double),
+                ("retire_max_s", c_double)]
 
 
 _V = c_void_p
@@ -104,13 +107,27 @@ def _completion(c: _Completion) -> Completion:
                       float(c.t_done), c.message.decode(errors="replace"))
 
 
-def _request(base, nlev, box, precision, fine, out, tol, max_cycles, tag):
+def _request(base, nlev, box, precision, fine, out, tol, max_cycles, tag,
+             atoms=None, physics=None):
+    """fine: dict of the six fine-level arrays, or None with `atoms`
+    (rows x y z radius charge, GPU set-up with `physics`)."""
     n3 = level_n(base, nlev) ** 3
     r = _Request()
     r.base, r.nlev, r.box = base, nlev, box
     r.precision = PRECISIONS[precision]
     keep = []
-    for q, k in enumerate(FINE_KEYS):
+    if atoms is not None:
+        from .problem import physics_struct
+        from .molecule import REFERENCE_PHYSICS
+        a = np.ascontiguousarray(atoms, dtype=np.float64).reshape(-1, 5)
+        if not len(a):  # no atoms: any valid non-null pointer
+            a = np.zeros(5)
+        keep.append(a)
+        r.atoms = a.ctypes.data
+        r.natoms = len(np.asarray(atoms).reshape(-1, 5))
+        r.physics = physics_struct(physics or REFERENCE_PHYSICS)
+        fine = None
+    for q, k in enumerate(FINE_KEYS if fine is not None else ()):
         a = fine[k]
         if isinstance(a, np.ndarray):
             a = np.ascontiguousarray(a, dtype=np.float64).ravel()
@@ -144,14 +161,17 @@ class Server:
         self._keep: dict[int, list] = {}
         self._next = 0
 
-    def submit(self, base: int, nlev: int, box: float, fine: dict,
+    def submit(self, base: int, nlev: int, box: float, fine: dict | None,
                precision: str = "mixed", out=None, tol: float = 1e-10,
-               max_cycles: int = 100, tag: int | None = None) -> int:
+               max_cycles: int = 100, tag: int | None = None, atoms=None,
+               physics: dict | None = None) -> int:
+        """Enqueues one solve: from the six fine-level arrays (`fine`), or
+        from `atoms` with the GPU set-up (fine=None)."""
         if tag is None:
             tag = self._next
         self._next = max(self._next, tag) + 1
         r, keep = _request(base, nlev, box, precision, fine, out, tol,
-                           max_cycles, tag)
+                           max_cycles, tag, atoms, physics)
         self._keep[tag] = keep
         _lib.check("pmg_server_submit",
                    _lib.lib.pmg_server_submit(self._h, ctypes.byref(r)))
@@ -212,11 +232,51 @@ def batch_solve(items: list[dict], budget_bytes: int, max_inflight: int = 96,
     keep = []
     for i, it in enumerate(items):
         r, k = _request(it["base"], it["nlev"], it["box"],
-                        it.get("precision", "mixed"), it["fine"],
-                        it.get("out"), tol, max_cycles, i)
+                        it.get("precision", "mixed"), it.get("fine"),
+                        it.get("out"), tol, max_cycles, i, it.get("atoms"),
+                        it.get("physics"))
         reqs[i] = r
         keep.append(k)
     out = (_Completion * max(1, len(items)))()
     _lib.check("pmg_batch_solve", _lib.lib.pmg_batch_solve(
         reqs, len(items), int(budget_bytes), int(max_inflight), out))
     return [_completion(out[i]) for i in range(len(items))]
+
+
+# ---------------------------------------------------------------------------
+# open-loop load (serving measurements)
+# ---------------------------------------------------------------------------
+def poisson_arrivals(rate: float, count: int, seed: int = 0) -> np.ndarray:
+    """Arrival times (s, from 0) of an open-loop Poisson stream: cumulative
+    exponential gaps of mean 1/rate."""
+    rng = np.random.default_rng(seed)
+    return np.cumsum(rng.exponential(1.0 / rate, size=count))
+
+
+def percentile(values, q: float) -> float:
+    """The q-th percentile (0..100) by the nearest-rank rule."""
+    v = np.sort(np.asarray(values, dtype=np.float64))
+    if not len(v):
+        return float("nan")
+    k = max(1, int(np.ceil(q / 100.0 * len(v))))
+    return float(v[k - 1])
+
+
+def open_loop(server: Server, arrivals: np.ndarray, submit_one,
+              timeout: float = 600.0) -> tuple[list[Completion], float]:
+    """Submits request i (submit_one(server, i)) at arrivals[i] seconds after
+    the start, collecting completions while it waits; returns every
+    completion and the wall time from the first arrival to the last
+    completion."""
+    import time
+    t0 = time.perf_counter()
+    done: list[Completion] = []
+    for i, t in enumerate(arrivals):
+        while True:
+            left = t0 + t - time.perf_counter()
+            if left <= 0:
+                break
+            done += server.wait(timeout=min(left, 0.002))
+        submit_one(server, i)
+    done += server.drain(len(arrivals) - len(done), timeout=timeout)
+    return done, time.perf_counter() - t0 - float(arrivals[0])

@@ -138,3 +138,36 @@ def test_device_inputs_and_batch_order(cases, alone):
         cyc, x = alone[i]
         assert c.cycles == cyc
         assert np.array_equal(it["out"].cpu().numpy(), x)
+
+
+def test_requests_from_atoms_match_problem_handle():
+    """Requests carrying atoms (GPU set-up in the worker) give the results of
+    PBELinearProblem.set_atoms + solve, alone and mixed with array
+    requests."""
+    w = WORKLOADS["pb65"]
+    atoms = w.atoms()
+    want = {}
+    for prec in ("fp64", "mixed"):
+        with PBELinearProblem(w.base, w.nlev, w.box, prec, w.physics) as p:
+            p.set_atoms(atoms)
+            p.buildmultilevelops()
+            r = p.solve(tol=1e-10, max_cycles=100)
+            want[prec] = (r.cycles, p.potential().ravel().copy())
+    fine = setup_fine(w.n, w.h, atoms, w.physics)
+    outs = {}
+    with Server(budget_bytes=8 << 30, max_inflight=8) as srv:
+        for i, prec in enumerate(("fp64", "mixed", "fp64", "mixed")):
+            outs[i] = np.empty(w.n ** 3)
+            if i < 2:
+                srv.submit(w.base, w.nlev, w.box, None, prec, out=outs[i],
+                           tag=i, atoms=atoms, physics=w.physics)
+            else:  # array requests in the same mix
+                srv.submit(w.base, w.nlev, w.box, fine, prec, out=outs[i],
+                           tag=i)
+        done = srv.drain(4)
+    for c in done:
+        assert c.ok, c.message
+        if c.tag < 2:
+            prec = ("fp64", "mixed")[c.tag]
+            assert c.cycles == want[prec][0]
+            assert np.array_equal(outs[c.tag], want[prec][1])

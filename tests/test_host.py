@@ -165,3 +165,13 @@ def test_native_levels_rule_matches_python():
                                      ctypes.byref(L))
         got = (b.value, L.value) if rc == 0 else None
         assert got == want, n
+
+
+def test_poisson_arrivals_and_percentiles():
+    from multigrid_b200.serve import percentile, poisson_arrivals
+    t = poisson_arrivals(200.0, 20000, seed=1)
+    assert np.all(np.diff(t) > 0)
+    assert abs(len(t) / t[-1] - 200.0) < 200.0 * 0.03
+    assert percentile([5, 1, 3, 2, 4], 50) == 3
+    assert percentile(list(range(1, 101)), 99) == 99
+    assert percentile([7.0], 99) == 7.0
