@@ -278,6 +278,19 @@ int pmg_setup_fine_d(int n, double h, const double *atoms, int natoms,
                      double *oN, double *uC, double *f, double *x0,
                      pmg_stream_t stream);
 
+/* ---- File formats ------------------------------------------------------
+ * PQR atoms (read_pqr_file, fileio.cc:10-53): every non-REMARK line of
+ * exactly ten fields gives one row (x, y, z, radius, charge) from fields
+ * 6-8, 10 and 9. With atoms == NULL only counts; returns PMG_ERR_ARG when
+ * the file cannot be read or holds more than cap atoms. */
+int pmg_read_pqr(const char *path, double *atoms, int cap, int *count);
+/* OpenDX grid file of an nx x ny x nz array in array order (x fastest), the
+ * reference's print_dx_to_stream (Domain.h:136-185): origin (xmin, ymin,
+ * zmin), spacing box_length / (nx - 1), three values per line. */
+int pmg_write_dx(const char *path, const double *values, int nx, int ny,
+                 int nz, double xmin, double ymin, double zmin,
+                 double box_length);
+
 /* ======================================================================
  * Problem handle: PBE_linear_problem<base, nlev, box> with runtime sizes
  * (PBE_pmgc_class.h:112-1174). Level L has n_L = base*2^L + 1 points per

@@ -175,3 +175,54 @@ def test_poisson_arrivals_and_percentiles():
     assert percentile([5, 1, 3, 2, 4], 50) == 3
     assert percentile(list(range(1, 101)), 99) == 99
     assert percentile([7.0], 99) == 7.0
+
+
+def test_pqr_reader(tmp_path):
+    """Lines of exactly ten fields other than REMARK are atoms: x y z from
+    fields 6-8, charge 9, radius 10; other lines are skipped."""
+    from multigrid_b200.fileio import read_pqr
+    p = tmp_path / "mol.pqr"
+    p.write_text(
+        "REMARK   1 generated for a reader test\n"
+        "\n"
+        "ATOM      1  N   ALA     1      1.000   2.000   3.000 -0.3000 1.8240\n"
+        "ATOM      2  CA  ALA     1     -4.500   0.250  10.125  0.1500 1.9080\n"
+        "HETATM    3  O   HOH\n"
+        "ATOM      4  C   ALA     1      7.000   8.000   9.000  0.5000 1.7000\n"
+        "TER\nEND\n")
+    a = read_pqr(str(p))
+    assert a.shape == (3, 5)
+    assert np.array_equal(a[1], [-4.5, 0.25, 10.125, 1.908, 0.15])
+    b = read_pqr(str(p), origin=(1.0, 2.0, 3.0))
+    assert np.array_equal(b[0], [0.0, 0.0, 0.0, 1.824, -0.3])
+    with pytest.raises(_lib.PmgError):
+        read_pqr(str(tmp_path / "missing.pqr"))
+
+
+def test_dx_writer_format(tmp_path):
+    """The reference's OpenDX layout: header, three values per line in array
+    order formatted as {:<+13e} plus a space, field trailer."""
+    from multigrid_b200.fileio import write_dx
+    v = np.arange(27, dtype=np.float64).reshape(3, 3, 3) * 0.5 - 3.0
+    v[0, 0, 1] = 1.5e-120
+    p = tmp_path / "pot.dx"
+    write_dx(str(p), v, origin=(-1.0, 2.0, 0.25), box_length=8.0)
+    fmt = lambda x: format(x, "<+13e") + " "  # noqa: E731
+    lines = [
+        "object 1 class gridpositions counts 3 3 3",
+        "origin " + fmt(-1.0) + fmt(2.0) + fmt(0.25),
+        "delta " + fmt(4.0) + fmt(0.0) + fmt(0.0),
+        "delta " + fmt(0.0) + fmt(4.0) + fmt(0.0),
+        "delta " + fmt(0.0) + fmt(0.0) + fmt(4.0),
+        "object 2 class gridconnections count 3 3 3",
+        "object 3 class array type double rank 0 items 27 data follows",
+    ]
+    flat = v.ravel()
+    for r in range(9):
+        lines.append("".join(fmt(x) for x in flat[3 * r:3 * r + 3]))
+    lines += ['attribute "dep" string "positions"',
+              'object "regular positions regular connections" class field',
+              'component "positions" value 1',
+              'component "connections" value 2',
+              'component "data" value 3']
+    assert p.read_text() == "\n".join(lines) + "\n"
