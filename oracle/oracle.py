@@ -59,8 +59,9 @@ class Restatement:
         L.pmgo_residual2.restype = ctypes.c_double
         L.pmgo_ideal_lambda.restype = ctypes.c_double
         L.pmgo_cg.restype = ctypes.c_int
-        for name in ("pmgo_solve", "pmgo_residual2", "pmgo_ideal_lambda"):
-            pass
+        L.pmgo_pcg.restype = ctypes.c_int
+        L.pmgo_pcg.argtypes = [ctypes.c_int, ctypes.c_int] + [D] * 6 + [
+            ctypes.c_int, ctypes.c_double, D, D]
         L.pmgo_solve.argtypes = [ctypes.c_int, ctypes.c_int] + [D] * 6 + [
             ctypes.c_double, ctypes.c_int, ctypes.c_int, D, D]
         L.pmgo_hierarchy.argtypes = [ctypes.c_int, ctypes.c_int] + [D] * 4 + [
@@ -151,6 +152,19 @@ class Restatement:
             raise MemoryError("pmgo_solve: allocation failed")
         return x, c, hist[:c + 1]
 
+    def pcg(self, base, nlev, fine: dict, max_iters, tol=0.0):
+        """MG-preconditioned CG (pmgo_pcg): (x, iterations, history)."""
+        n = base * 2 ** nlev + 1
+        x = np.empty(n ** 3)
+        hist = np.zeros(max_iters + 1)
+        args = [_d(np.ascontiguousarray(fine[k], dtype=np.float64).ravel())
+                for k in ("oC", "oE", "oN", "uC", "f", "x0")]
+        c = self.lib.pmgo_pcg(base, nlev, *args, max_iters, tol, _d(x),
+                              _d(hist))
+        if c < 0:
+            raise MemoryError("pmgo_pcg: allocation failed")
+        return x, c, hist[:c + 1]
+
     def hierarchy(self, base, nlev, fine: dict, trilinear=False):
         cap = sum(41 * (base * 2 ** L + 1) ** 3 for L in range(1, nlev))
         out = np.empty(cap)
@@ -223,6 +237,17 @@ class Reference:
         if rc != 0:
             raise KeyError(f"reference oracle has no ({base}, {nlev}) grid")
         return x, c.value, hist[:c.value + 1]
+
+    def pcg(self, base, nlev, fine: dict, iters: int):
+        """The app's MG-preconditioned CG for exactly `iters` iterations
+        (pmgref_pcg); returns the iterate."""
+        n = base * 2 ** nlev + 1
+        x = np.empty(n ** 3)
+        f = self._fine(fine)
+        rc = self.lib.pmgref_pcg(base, nlev, ctypes.byref(f), iters, _d(x))
+        if rc != 0:
+            raise KeyError(f"reference oracle has no ({base}, {nlev}) grid")
+        return x
 
     def cycles(self, base, nlev, fine: dict, ncycles: int):
         n = base * 2 ** nlev + 1

@@ -721,6 +721,106 @@ int pmgo_solve(int base, int nlev, const double *oC, const double *oE,
   return c;
 }
 
+/* MG-preconditioned CG on the finest level: CG_solver (CG_Solver.h:45-242)
+ * with the class as preconditioner (PBE_pmgc_class.h:1116-1133: rhs -> the
+ * class's finest rhs, one zero-started V-cycle, the class's finest iterate
+ * returned), as the app runs it (PBE_pmgc_class_with_non_zero_IS.cc:
+ * 118-131). The class's finest iterate has a zero shell there; x0 (with the
+ * Dirichlet shell) is the initial guess. Sums run over the interior in
+ * (k, j, i) order. Iterates until max_iters or, with tol > 0, until
+ * sqrt(sum r^2 / n^3) of the updated residual falls below tol times its
+ * initial value; hist[c] holds that norm after c iterations. Returns the
+ * iterations run, -1 on allocation failure. */
+static double dot_interior(int n, const double *a, const double *b) {
+  double s = 0.0;
+  for (int k = 2; k <= n - 1; ++k)
+    for (int j = 2; j <= n - 1; ++j)
+      for (int i = 2; i <= n - 1; ++i) {
+        const size_t p = IX(n, n, i, j, k);
+        s += a[p] * b[p];
+      }
+  return s;
+}
+
+static void mg_precondition(ohier *h, const double *r, double *s) {
+  olevel *fine = &h->lv[h->nlev];
+  const size_t n3 = (size_t)fine->n * fine->n * fine->n;
+  memcpy(fine->f, r, n3 * sizeof(double));
+  memset(fine->x, 0, n3 * sizeof(double));
+  vcycle(h, h->nlev, 1);
+  memcpy(s, fine->x, n3 * sizeof(double));
+}
+
+int pmgo_pcg(int base, int nlev, const double *oC, const double *oE,
+             const double *oN, const double *uC, const double *f,
+             const double *x0, int max_iters, double tol, double *x_out,
+             double *hist) {
+  ohier h;
+  if (hier_build(&h, base, nlev, oC, oE, oN, uC, 0) != 0) {
+    hier_free(&h);
+    return -1;
+  }
+  olevel *fine = &h.lv[nlev];
+  const int n = fine->n;
+  const size_t n3 = (size_t)n * n * n;
+  const pmgo_op *A = &fine->A;
+  double *x = malloc(n3 * sizeof(double)), *r = calloc(n3, sizeof(double));
+  double *s = calloc(n3, sizeof(double)), *pv = calloc(n3, sizeof(double));
+  double *ap = calloc(n3, sizeof(double));
+  if (!x || !r || !s || !pv || !ap) {
+    free(x); free(r); free(s); free(pv); free(ap);
+    hier_free(&h);
+    return -1;
+  }
+  memcpy(x, x0, n3 * sizeof(double));
+  pmgo_defect(n, n, n, A, f, x, r);
+  const double r0 = sqrt(dot_interior(n, r, r) / (double)n3);
+  if (hist)
+    hist[0] = r0;
+  mg_precondition(&h, r, s);
+  memcpy(pv, s, n3 * sizeof(double));
+  double rs = dot_interior(n, r, s);
+  pmgo_matvec(n, n, n, A, NULL, pv, ap);
+  double pap = dot_interior(n, ap, pv);
+  int c = 0;
+  if (pap != 0.0) {
+    double alpha = rs / pap;
+    while (c < max_iters) {
+      for (int k = 2; k <= n - 1; ++k)
+        for (int j = 2; j <= n - 1; ++j)
+          for (int i = 2; i <= n - 1; ++i) {
+            const size_t q = IX(n, n, i, j, k);
+            x[q] += alpha * pv[q];
+            r[q] -= alpha * ap[q];
+          }
+      mg_precondition(&h, r, s);
+      const double rs_next = dot_interior(n, r, s);
+      const double beta = rs == 0.0 ? 0.0 : rs_next / rs;
+      rs = rs_next;
+      for (int k = 2; k <= n - 1; ++k)
+        for (int j = 2; j <= n - 1; ++j)
+          for (int i = 2; i <= n - 1; ++i) {
+            const size_t q = IX(n, n, i, j, k);
+            pv[q] = s[q] + beta * pv[q];
+          }
+      pmgo_matvec(n, n, n, A, NULL, pv, ap);
+      pap = dot_interior(n, ap, pv);
+      alpha = pap == 0.0 ? 0.0 : rs / pap;
+      ++c;
+      const double rn = sqrt(dot_interior(n, r, r) / (double)n3);
+      if (hist)
+        hist[c] = rn;
+      if (tol > 0.0 && r0 > 0.0 && rn / r0 < tol)
+        break;
+    }
+  }
+  if (x_out)
+    memcpy(x_out, x, n3 * sizeof(double));
+  free(x); free(r); free(s); free(pv); free(ap);
+  hier_free(&h);
+  return c;
+}
+
 long pmgo_hierarchy(int base, int nlev, const double *oC, const double *oE,
                     const double *oN, const double *uC, int trilinear,
                     double *out, long cap) {

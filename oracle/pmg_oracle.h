@@ -75,6 +75,13 @@ int pmgo_solve(int base, int nlev, const double *oC, const double *oE,
 /* Hierarchy in the layout of pmgref_hierarchy: for L = nlev-1 .. 1, the 27
  * prolongation arrays then the 14 operator arrays of level L. Returns the
  * number of doubles written, or -1 if cap is too small. */
+/* MG-preconditioned CG on the finest level (CG_Solver.h:45-242 with the
+ * class as preconditioner, PBE_pmgc_class.h:1116-1133); see pmg_oracle.c. */
+int pmgo_pcg(int base, int nlev, const double *oC, const double *oE,
+             const double *oN, const double *uC, const double *f,
+             const double *x0, int max_iters, double tol, double *x_out,
+             double *hist);
+
 long pmgo_hierarchy(int base, int nlev, const double *oC, const double *oE,
                     const double *oN, const double *uC, int trilinear,
                     double *out, long cap);

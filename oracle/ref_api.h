@@ -75,6 +75,16 @@ int pmgref_setup(int base, int nlev, const double *atoms, int natoms,
                  double ionic_strength, double ion_radius, double *oC,
                  double *oE, double *oN, double *uC, double *f, double *x0);
 
+/* MG-preconditioned CG of the reference app
+ * (PBE_pmgc_class_with_non_zero_IS.cc:123-131): CG_solver
+ * (CG_Solver.h:45-242) on the finest level with the class as preconditioner
+ * (operator(), PBE_pmgc_class.h:1116-1133: one zero-started V-cycle),
+ * counting criterion of `iters` iterations. The class's own finest iterate
+ * starts at zero (the app never sets its boundary); x0 (with the Dirichlet
+ * shell) is the CG's initial guess. Writes the iterate to x_out. */
+int pmgref_pcg(int base, int nlev, const pmgref_fine *in, int iters,
+               double *x_out);
+
 /* Single pmgc kernels (pmgc/*.cc), called on host arrays. */
 int pmgref_Vgsrb7x(int nx, int ny, int nz, const double *oC, const double *cc,
                    const double *fc, const double *oE, const double *oN,

@@ -183,10 +183,33 @@ int setup(const double *atoms, int natoms, double ionic_strength,
   return 0;
 }
 
+// The app's MG-preconditioned CG (PBE_pmgc_class_with_non_zero_IS.cc:
+// 118-131): general CG solver over the class's finest map, the class itself
+// as preconditioner, counting criterion.
+int pcg(const pmgref_fine *in, int iters, double *x_out) {
+  auto p = make_problem(in);
+  build(*p, 0);
+  auto &sol = p->sol.template get_domain<kNlev>();
+  using D = std::remove_reference_t<decltype(sol)>;
+  D init_guess(Paddings::PERIODIC, oracle_queue(), 1),
+      rhs(Paddings::PERIODIC, oracle_queue(), 1);
+  put(init_guess, in->x0);
+  put(rhs, in->f);
+  // the app's class never gets a boundary: its finest iterate is zero
+  std::memset(sol.values_buff, 0, sizeof(::DataType) * sol.num_values);
+  auto main_solver = cg_solver::make_general_solver<::DataType>(sol);
+  cg_solver::counting_criterion counter((std::size_t)iters);
+  auto map = p->get_map();
+  main_solver(init_guess, rhs, map, counter, *p, false);
+  get(init_guess, x_out);
+  return 0;
+}
+
 struct registrar {
   registrar() {
     pmgref_register(pmgref_entry{(int)kBase, (int)kNlev, (double)kBox, solve,
-                                 cycles_only, hierarchy, cg_level1, setup});
+                                 cycles_only, hierarchy, cg_level1, setup,
+                                 pcg});
   }
 } the_registrar;
 

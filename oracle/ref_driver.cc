@@ -109,6 +109,15 @@ int pmgref_setup(int base, int nlev, const double *atoms, int natoms,
                   f, x0);
 }
 
+int pmgref_pcg(int base, int nlev, const pmgref_fine *in, int iters,
+               double *x_out) {
+  const pmgref_entry *e = find(base, nlev);
+  if (!e)
+    return -1;
+  quiet_cout q;
+  return e->pcg(in, iters, x_out);
+}
+
 int pmgref_Vgsrb7x(int nx, int ny, int nz, const double *oC, const double *cc,
                    const double *fc, const double *oE, const double *oN,
                    const double *uC, double *x, int itmax, int iadjoint,

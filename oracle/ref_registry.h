@@ -21,6 +21,7 @@ struct pmgref_entry {
   int (*setup)(const double *atoms, int natoms, double ionic_strength,
                double ion_radius, double *oC, double *oE, double *oN,
                double *uC, double *f, double *x0);
+  int (*pcg)(const pmgref_fine *in, int iters, double *x_out);
 };
 
 void pmgref_register(const pmgref_entry &e);

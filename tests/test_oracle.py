@@ -177,3 +177,31 @@ def test_setup_vs_reference_random():
         b = setup_fine(n, box / (n - 1), atoms, REFERENCE_PHYSICS)
         for k in a:
             assert np.array_equal(a[k], b[k]), (base, nlev, k)
+
+
+@pytest.mark.skipif(not reference_available(), reason="reference not built")
+@pytest.mark.parametrize("iters", [1, 3, 8])
+def test_pcg_restatement_matches_reference(golden_problem, restatement,
+                                           iters):
+    """The app's MG-preconditioned CG (CG_Solver.h:45-242 with the class as
+    preconditioner) after a fixed number of iterations, restatement against
+    the reference run through its own solver object."""
+    from oracle.oracle import Reference
+    g = golden_problem
+    base, nlev = int(g["base"]), int(g["nlev"])
+    fine = fine_of(g)
+    xo, c, _ = restatement.pcg(base, nlev, fine, iters)
+    xr = Reference().pcg(base, nlev, fine, iters)
+    assert c == iters
+    assert np.linalg.norm(xo - xr) <= 1e-13 * np.linalg.norm(xr)
+
+
+def test_pcg_restatement_converges_to_the_solve(golden_problem, restatement):
+    g = golden_problem
+    base, nlev = int(g["base"]), int(g["nlev"])
+    fine = fine_of(g)
+    xs, cs, _ = restatement.solve(base, nlev, fine, tol=1e-10)
+    xo, c, h = restatement.pcg(base, nlev, fine, 100, tol=1e-10)
+    assert 0 < c <= cs
+    assert h[-1] / h[0] < 1e-10
+    assert np.linalg.norm(xo - xs) <= 1e-9 * np.linalg.norm(xs)
