@@ -354,6 +354,21 @@ int pmg_compute_residual_2(pmg_problem *p, double *out);
 int pmg_solve(pmg_problem *p, double tol, int max_cycles, int *cycles,
               double *relres, double *hist);
 
+/* MG-preconditioned CG on the finest level, the reference app's outer
+ * solver (PBE_pmgc_class_with_non_zero_IS.cc:118-131: CG_solver,
+ * CG_Solver.h:45-242, with the class as preconditioner, operator(),
+ * PBE_pmgc_class.h:1116-1133 -- one zero-started V-cycle per application,
+ * FP64 or, for mixed problems, the float V-cycle). Starts from the loaded
+ * iterate and stops after max_iters (<= 1024) iterations or, with tol > 0,
+ * once sqrt(sum r^2 / n^3) of the recursively updated residual is below tol
+ * times its initial value (tol = 0: the app's counting criterion). The
+ * result replaces the finest iterate (pmg_get_potential); *iters, *relres
+ * and hist (max_iters + 1 entries, may be NULL) as for pmg_solve. The whole
+ * iteration is one graph launch (stop test on the GPU). Allocates 6 n^3
+ * doubles on first use. */
+int pmg_pcg_solve(pmg_problem *p, double tol, int max_iters, int *iters,
+                  double *relres, double *hist);
+
 /* Asynchronous solve (no reference counterpart; the class's loop is
  * synchronous): enqueues the whole solve on the problem's stream as one
  * graph launch whose while node repeats cycle + stop test on the GPU, and

@@ -11,6 +11,7 @@
 #include "bottom_cycle.cuh"
 #include "gs27_tiled.cuh"
 #include "launch.cuh"
+#include "pcg_kernels.cuh"
 #include "reduce_kernels.cuh"
 
 namespace pmg {
@@ -126,6 +127,19 @@ struct pmg_problem {
   SolveState *h_state = nullptr; // pinned
   cudaEvent_t done_ev = nullptr;
   bool solve_pending = false;
+  // MG-preconditioned CG on the finest level (allocated on first use):
+  // right-hand side, iterate, residual, preconditioned residual, search
+  // direction, A times it; three reduction slots; the iteration state.
+  struct {
+    char *mem = nullptr;
+    size_t bytes = 0;
+    double *b = nullptr, *xs = nullptr, *r = nullptr, *z = nullptr,
+           *pv = nullptr, *ap = nullptr;
+    ReduceSlot rr{}, rz{}, pap{};
+    PcgState *d_st = nullptr, *h_st = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    long long head_kernels = 0, body_kernels = 0;
+  } pcg;
   // kernel launches issued by this problem (build, solve, graph replays)
   long long launches = 0;
   long long cycle_kernels = 0; // kernel nodes in the captured cycle graph
@@ -629,14 +643,16 @@ int graph_step_ok(const char *step) {
   return PMG_ERR_CUDA;
 }
 
-// Builds the solve graph: [initial residual, init] -> while(cond){cycle,
-// check} -> copy of the state to pinned memory.
-int ensure_solve_graph(pmg_problem *p) {
-  if (p->solve_exec)
-    return PMG_OK;
-  const bool mixed = p->precision == PMG_PREC_MIXED;
-  const double n3 = (double)p->lv[p->nlev].n3;
-  cudaGraph_t g = nullptr, body = nullptr;
+// Builds [head] -> while (cond) { body } -> [tail] as one executable graph.
+// head(h), body(h) and tail() enqueue work on the problem's stream (captured)
+// and return a pmg_status; head and body launch the kernels that set the
+// while node's condition h. The loop ends only through body's stop test, so
+// a body whose capture yields fewer than two kernels is refused.
+template <class Head, class Body, class Tail>
+int build_loop_graph(pmg_problem *p, Head head, Body body, Tail tail,
+                     cudaGraphExec_t *exec, long long *head_kernels,
+                     long long *body_kernels) {
+  cudaGraph_t g = nullptr, bg = nullptr;
   cudaGraphConditionalHandle h;
   cudaGraphNode_t cond = nullptr;
   int rc = PMG_OK;
@@ -648,24 +664,15 @@ int ensure_solve_graph(pmg_problem *p) {
   if (e != cudaSuccess) {
     if (g)
       cudaGraphDestroy(g);
-    set_last_error(e, "solve graph: conditional handle", __FILE__, __LINE__);
+    set_last_error(e, "loop graph: conditional handle", __FILE__, __LINE__);
     return PMG_ERR_CUDA;
   }
-  // head: initial residual and the init kernel, captured into g
   e = cudaStreamBeginCaptureToGraph(p->stream, g, nullptr, nullptr, 0,
                                     cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
-    rc = mixed ? mixed_residual_async(p, false)
-               : residual_norm_async(p, false);
-    if (!rc) {
-      solve_init_kernel<<<1, 1, 0, p->stream>>>(p->d_state,
-                                                p->red_norm.result, n3, h);
-      e = cudaGetLastError();
-      if (e != cudaSuccess) {
-        set_last_error(e, "solve graph: init kernel", __FILE__, __LINE__);
-        rc = PMG_ERR_CUDA;
-      }
-    }
+    rc = head(h);
+    if (!rc)
+      rc = graph_step_ok("loop graph: head");
     const cudaGraphNode_t *deps = nullptr;
     size_t ndeps = 0;
     cudaStreamCaptureStatus cs;
@@ -680,40 +687,31 @@ int ensure_solve_graph(pmg_problem *p) {
       cp.conditional.size = 1;
       e = cudaGraphAddNode(&cond, g, deps, ndeps, &cp);
       if (e == cudaSuccess) {
-        body = cp.conditional.phGraph_out[0];
+        bg = cp.conditional.phGraph_out[0];
         e = cudaStreamUpdateCaptureDependencies(
             p->stream, &cond, 1, cudaStreamSetCaptureDependencies);
       }
     }
     if (!rc && e == cudaSuccess)
-      e = cudaMemcpyAsync(p->h_state, p->d_state, sizeof(SolveState),
-                          cudaMemcpyDeviceToHost, p->stream);
+      rc = tail();
     cudaGraph_t out = nullptr;
     const cudaError_t e2 = cudaStreamEndCapture(p->stream, &out);
     if (e == cudaSuccess)
       e = e2;
   }
   if (!rc && e == cudaSuccess)
-    rc = graph_step_ok("solve graph: head capture");
+    rc = graph_step_ok("loop graph: head capture");
   if (!rc && e == cudaSuccess)
-    p->solve_pre_kernels = count_kernel_nodes(g);
+    *head_kernels = count_kernel_nodes(g);
   if (!rc && e == cudaSuccess) {
-    // body: one cycle and the stop test
-    e = cudaStreamBeginCaptureToGraph(p->stream, body, nullptr, nullptr, 0,
+    e = cudaStreamBeginCaptureToGraph(p->stream, bg, nullptr, nullptr, 0,
                                       cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess)
-      rc = graph_step_ok("solve graph: body capture");
+      rc = graph_step_ok("loop graph: body capture");
     if (e == cudaSuccess && !rc) {
-      rc = cycle_with_residual(p, false);
-      if (!rc) {
-        solve_check_kernel<<<1, 1, 0, p->stream>>>(
-            p->d_state, p->red_norm.result, n3, h);
-        const cudaError_t ek = cudaGetLastError();
-        if (ek != cudaSuccess) {
-          set_last_error(ek, "solve graph: check kernel", __FILE__, __LINE__);
-          rc = PMG_ERR_CUDA;
-        }
-      }
+      rc = body(h);
+      if (!rc)
+        rc = graph_step_ok("loop graph: body");
       cudaGraph_t out = nullptr;
       const cudaError_t e2 = cudaStreamEndCapture(p->stream, &out);
       if (e == cudaSuccess)
@@ -721,25 +719,58 @@ int ensure_solve_graph(pmg_problem *p) {
     }
   }
   if (!rc && e == cudaSuccess) {
-    p->solve_body_kernels = count_kernel_nodes(body);
-    // the loop ends only through the check kernel: never instantiate a body
-    // without it
-    if (p->solve_body_kernels < 2) {
-      set_last_message("solve graph: loop body was not captured");
+    *body_kernels = count_kernel_nodes(bg);
+    if (*body_kernels < 2) {
+      set_last_message("loop graph: loop body was not captured");
       rc = PMG_ERR_STATE;
     } else {
-      e = cudaGraphInstantiate(&p->solve_exec, g, 0);
+      e = cudaGraphInstantiate(exec, g, 0);
     }
   }
   cudaGraphDestroy(g);
   if (rc)
     return rc;
   if (e != cudaSuccess) {
-    p->solve_exec = nullptr;
-    set_last_error(e, "solve graph", __FILE__, __LINE__);
+    *exec = nullptr;
+    set_last_error(e, "loop graph", __FILE__, __LINE__);
     return PMG_ERR_CUDA;
   }
   return PMG_OK;
+}
+
+// The solve graph: [initial residual, init] -> while (cond) {cycle, check}
+// -> copy of the state to pinned memory.
+int ensure_solve_graph(pmg_problem *p) {
+  if (p->solve_exec)
+    return PMG_OK;
+  const bool mixed = p->precision == PMG_PREC_MIXED;
+  const double n3 = (double)p->lv[p->nlev].n3;
+  auto head = [&](cudaGraphConditionalHandle h) -> int {
+    int rc = mixed ? mixed_residual_async(p, false)
+                   : residual_norm_async(p, false);
+    if (rc)
+      return rc;
+    solve_init_kernel<<<1, 1, 0, p->stream>>>(p->d_state,
+                                              p->red_norm.result, n3, h);
+    PMG_LAUNCH_CHECK();
+    return PMG_OK;
+  };
+  auto body = [&](cudaGraphConditionalHandle h) -> int {
+    int rc = cycle_with_residual(p, false);
+    if (rc)
+      return rc;
+    solve_check_kernel<<<1, 1, 0, p->stream>>>(p->d_state,
+                                               p->red_norm.result, n3, h);
+    PMG_LAUNCH_CHECK();
+    return PMG_OK;
+  };
+  auto tail = [&]() -> int {
+    PMG_CUDA_TRY(cudaMemcpyAsync(p->h_state, p->d_state, sizeof(SolveState),
+                                 cudaMemcpyDeviceToHost, p->stream));
+    return PMG_OK;
+  };
+  return build_loop_graph(p, head, body, tail, &p->solve_exec,
+                          &p->solve_pre_kernels, &p->solve_body_kernels);
 }
 
 // Drops the captured graphs (their kernels bake in thresholds and modes).
@@ -752,6 +783,132 @@ void drop_graphs(pmg_problem *p) {
     cudaGraphExecDestroy(p->solve_exec);
     p->solve_exec = nullptr;
   }
+  if (p->pcg.exec) {
+    cudaGraphExecDestroy(p->pcg.exec);
+    p->pcg.exec = nullptr;
+  }
+}
+
+// ---- MG-preconditioned CG ----------------------------------------------------
+
+int pcg_alloc(pmg_problem *p) {
+  if (p->pcg.mem)
+    return PMG_OK;
+  const LevelBuf &v = p->lv[p->nlev];
+  const dim3 g = reduce_grid(v.d);
+  const long blocks = (long)g.x * g.y * g.z;
+  Arena a;
+  for (int pass = 0; pass < 2; ++pass) {
+    a.off = 0;
+    double **vec[6] = {&p->pcg.b, &p->pcg.xs, &p->pcg.r, &p->pcg.z,
+                       &p->pcg.pv, &p->pcg.ap};
+    for (double **q : vec)
+      *q = a.take<double>(v.n3);
+    for (ReduceSlot *sl : {&p->pcg.rr, &p->pcg.rz, &p->pcg.pap}) {
+      sl->partials = a.take<double>(blocks);
+      sl->ticket = a.take<unsigned int>(1);
+      sl->result = a.take<double>(1);
+    }
+    p->pcg.d_st = a.take<PcgState>(1);
+    if (pass == 0) {
+      PMG_CUDA_TRY(cudaMalloc((void **)&p->pcg.mem, a.off));
+      p->pcg.bytes = a.off;
+      a.base = p->pcg.mem;
+    }
+  }
+  PMG_CUDA_TRY(cudaMemsetAsync(p->pcg.mem, 0, p->pcg.bytes, p->stream));
+  if (!p->pcg.h_st)
+    PMG_CUDA_TRY(cudaMallocHost((void **)&p->pcg.h_st, sizeof(PcgState)));
+  return PMG_OK;
+}
+
+// z = M r: one zero-started V-cycle on r (the class's operator(),
+// PBE_pmgc_class.h:1116-1133) -- FP64 V-cycle, or the float V-cycle of the
+// mixed path. The finest iterate (shell zero) and, for FP64, the finest
+// right-hand side are borrowed as the V-cycle's work arrays.
+int precondition(pmg_problem *p, const double *r, double *z) {
+  LevelBuf &v = p->lv[p->nlev];
+  cudaStream_t s = p->stream;
+  const size_t b = sizeof(double) * v.n3;
+  if (p->precision == PMG_PREC_MIXED) {
+    convert_kernel<double, float><<<flat_grid(v.n3), 256, 0, s>>>(v.n3, r,
+                                                                  v.f32);
+    PMG_LAUNCH_CHECK();
+    int rc = vcycle32(p, p->nlev);
+    if (rc)
+      return rc;
+    convert_kernel<float, double><<<flat_grid(v.n3), 256, 0, s>>>(v.n3,
+                                                                  v.x32, z);
+    PMG_LAUNCH_CHECK();
+    return PMG_OK;
+  }
+  PMG_CUDA_TRY(cudaMemcpyAsync(v.f, r, b, cudaMemcpyDeviceToDevice, s));
+  PMG_CUDA_TRY(cudaMemsetAsync(v.x, 0, b, s));
+  int rc = vcycle64(p, p->nlev, 1);
+  if (rc)
+    return rc;
+  PMG_CUDA_TRY(cudaMemcpyAsync(z, v.x, b, cudaMemcpyDeviceToDevice, s));
+  return PMG_OK;
+}
+
+// The PCG graph (CG_solver, CG_Solver.h:45-242, with the MG
+// preconditioner): head r = b - A x, z = M r, p = z, rs = r.z, Ap, pAp,
+// alpha; body x += alpha p, r -= alpha Ap, z = M r, beta, p = z + beta p,
+// Ap, pAp, alpha, stop test; tail: iterate and right-hand side back into
+// the problem, state to pinned memory.
+int ensure_pcg_graph(pmg_problem *p) {
+  if (p->pcg.exec)
+    return PMG_OK;
+  LevelBuf &v = p->lv[p->nlev];
+  cudaStream_t s = p->stream;
+  const double n3 = (double)v.n3;
+  const size_t b = sizeof(double) * v.n3;
+  auto &c = p->pcg;
+  const dim3 rg = reduce_grid(v.d), rb = interior_block();
+  auto head = [&](cudaGraphConditionalHandle h) -> int {
+    PMG_CUDA_TRY(cudaMemcpyAsync(c.xs, v.x, b, cudaMemcpyDeviceToDevice, s));
+    PMG_CUDA_TRY(cudaMemcpyAsync(c.b, v.f, b, cudaMemcpyDeviceToDevice, s));
+    defect_norm_kernel<7, double, double>
+        <<<rg, rb, 0, s>>>(v.d, v.A64(4), c.b, c.xs, c.r, c.rr);
+    PMG_LAUNCH_CHECK();
+    int rc = precondition(p, c.r, c.z);
+    if (rc)
+      return rc;
+    PMG_CUDA_TRY(cudaMemcpyAsync(c.pv, c.z, b, cudaMemcpyDeviceToDevice, s));
+    pcg_dot_kernel<<<rg, rb, 0, s>>>(v.d, c.r, c.z, c.rz);
+    pcg_matvec_dot_kernel<<<rg, rb, 0, s>>>(v.d, v.A64(4), c.pv, c.ap,
+                                            c.pap);
+    pcg_init_kernel<<<1, 1, 0, s>>>(c.d_st, c.rr.result, c.rz.result,
+                                    c.pap.result, n3, h);
+    PMG_LAUNCH_CHECK();
+    return PMG_OK;
+  };
+  auto body = [&](cudaGraphConditionalHandle h) -> int {
+    pcg_update_xr_kernel<<<rg, rb, 0, s>>>(v.d, c.pv, c.ap, c.xs, c.r,
+                                           c.d_st, c.rr);
+    PMG_LAUNCH_CHECK();
+    int rc = precondition(p, c.r, c.z);
+    if (rc)
+      return rc;
+    pcg_dot_kernel<<<rg, rb, 0, s>>>(v.d, c.r, c.z, c.rz);
+    pcg_beta_kernel<<<1, 1, 0, s>>>(c.d_st, c.rz.result);
+    pcg_update_p_kernel<<<rg, rb, 0, s>>>(v.d, c.z, c.pv, c.d_st);
+    pcg_matvec_dot_kernel<<<rg, rb, 0, s>>>(v.d, v.A64(4), c.pv, c.ap,
+                                            c.pap);
+    pcg_check_kernel<<<1, 1, 0, s>>>(c.d_st, c.pap.result, c.rr.result, n3,
+                                     h);
+    PMG_LAUNCH_CHECK();
+    return PMG_OK;
+  };
+  auto tail = [&]() -> int {
+    PMG_CUDA_TRY(cudaMemcpyAsync(v.x, c.xs, b, cudaMemcpyDeviceToDevice, s));
+    PMG_CUDA_TRY(cudaMemcpyAsync(v.f, c.b, b, cudaMemcpyDeviceToDevice, s));
+    PMG_CUDA_TRY(cudaMemcpyAsync(c.h_st, c.d_st, sizeof(PcgState),
+                                 cudaMemcpyDeviceToHost, s));
+    return PMG_OK;
+  };
+  return build_loop_graph(p, head, body, tail, &c.exec, &c.head_kernels,
+                          &c.body_kernels);
 }
 
 // A new problem starts from the state of a freshly constructed class: the
@@ -855,6 +1012,10 @@ int pmg_problem_destroy(pmg_problem *p) {
   if (p->stream)
     cudaStreamSynchronize(p->stream);
   drop_graphs(p);
+  if (p->pcg.mem)
+    cudaFree(p->pcg.mem);
+  if (p->pcg.h_st)
+    cudaFreeHost(p->pcg.h_st);
   if (p->done_ev)
     cudaEventDestroy(p->done_ev);
   if (p->h_state)
@@ -1183,6 +1344,52 @@ int pmg_solve(pmg_problem *p, double tol, int max_cycles, int *cycles,
   if (rc)
     return rc;
   return pmg_solve_finish(p, cycles, relres, hist);
+}
+
+int pmg_pcg_solve(pmg_problem *p, double tol, int max_iters, int *iters,
+                  double *relres, double *hist) {
+  if (!p || max_iters < 0 || max_iters > 1024 || !(tol >= 0.0)) {
+    set_last_message("pmg_pcg_solve: bad argument (0 <= max_iters <= 1024, "
+                     "tol >= 0)");
+    return PMG_ERR_ARG;
+  }
+  if (!p->built) {
+    set_last_message("pmg_pcg_solve: hierarchy not built");
+    return PMG_ERR_STATE;
+  }
+  if (p->solve_pending || p->prof_on) {
+    set_last_message("pmg_pcg_solve: a solve is in flight or phase timing "
+                     "is on");
+    return PMG_ERR_STATE;
+  }
+  int rc = pcg_alloc(p);
+  if (!rc)
+    rc = ensure_pcg_graph(p);
+  if (rc)
+    return rc;
+  pcg_params_kernel<<<1, 1, 0, p->stream>>>(p->pcg.d_st, tol, max_iters);
+  PMG_LAUNCH_CHECK();
+  PMG_CUDA_TRY(cudaGraphLaunch(p->pcg.exec, p->stream));
+  PMG_CUDA_TRY(cudaStreamSynchronize(p->stream));
+  const PcgState &st = *p->pcg.h_st;
+  p->launches += 1 + p->pcg.head_kernels +
+                 (long long)st.iters * p->pcg.body_kernels;
+  if (iters)
+    *iters = st.iters;
+  if (relres)
+    *relres = st.status == 2 ? st.r0 : (st.r0 > 0.0 ? st.rn / st.r0 : 0.0);
+  if (hist)
+    for (int c = 0; c <= st.iters && c <= 1024; ++c)
+      hist[c] = st.hist[c];
+  if (st.status == 2) {
+    set_last_message("pmg_pcg_solve: initial residual is not finite");
+    return PMG_ERR_DIVERGED;
+  }
+  if (st.status == 1) {
+    set_last_message("pmg_pcg_solve: residual diverged");
+    return PMG_ERR_DIVERGED;
+  }
+  return PMG_OK;
 }
 
 int pmg_get_potential(pmg_problem *p, double *dst) {

@@ -254,6 +254,19 @@ class PBELinearProblem:
             _dptr(hist)))
         return SolveResult(cycles.value, rel.value, hist[:cycles.value + 1])
 
+    def pcg_solve(self, tol: float = 1e-10,
+                  max_iters: int = 100) -> SolveResult:
+        """MG-preconditioned CG on the finest level (the app's outer solver:
+        CG_solver with this class as preconditioner); tol = 0 runs exactly
+        max_iters iterations."""
+        hist = np.zeros(max_iters + 1)
+        iters = ctypes.c_int()
+        rel = ctypes.c_double()
+        _lib.check("pmg_pcg_solve", _lib.lib.pmg_pcg_solve(
+            self._h, tol, max_iters, ctypes.byref(iters), ctypes.byref(rel),
+            _dptr(hist)))
+        return SolveResult(iters.value, rel.value, hist[:iters.value + 1])
+
     def solve_start(self, tol: float = 1e-10, max_cycles: int = 100) -> None:
         """Enqueues the whole solve (one graph launch, stop test on the GPU)
         and returns at once; finish with solve_finish()."""
