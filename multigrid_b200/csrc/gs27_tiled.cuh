@@ -27,17 +27,20 @@
 
 namespace pmg {
 
-constexpr int kT27 = 32;      // tile edge (x and y)
-constexpr int kH27 = 4;       // staged halo
-constexpr int kW27 = kT27 + 2 * kH27;
+constexpr int kH27 = 4; // staged halo
+// tile edges the launcher can use (x and y); threads per CTA by tile
+constexpr int kGs27Tiles[3] = {8, 16, 32};
+template <int TT> struct Gs27Tile {
+  static constexpr int W = TT + 2 * kH27;
+  static constexpr int THREADS = TT >= 32 ? 256 : TT >= 16 ? 128 : 64;
+};
 
-template <typename T>
+template <typename T, int w>
 __device__ __forceinline__ void sums27_tile(const Op14<T> &A, int p, int sy,
                                             int sz, const T *xc, const T *xd,
                                             const T *xu, T &tO, T &tU,
                                             T &tD) {
   const T *const *a = A.a;
-  constexpr int w = kW27;
   tO = a[kON][p] * xc[w] + a[kON][p - sy] * xc[-w] + a[kOE][p] * xc[1] +
        a[kOE][p - 1] * xc[-1] + a[kONE][p] * xc[1 + w] +
        a[kONW][p] * xc[-1 + w] + a[kONW][p + 1 - sy] * xc[1 - w] +
@@ -54,13 +57,15 @@ __device__ __forceinline__ void sums27_tile(const Op14<T> &A, int p, int sy,
        a[kUNE][p - 1 - sy - sz] * xd[-1 - w];
 }
 
-// One parity phase. kfirst: first plane of the parity (2 or 3); order: the
-// four sub-colours in visiting order, 2 bits each (step t in bits 2t..2t+1).
-template <typename T>
-__global__ void __launch_bounds__(256)
+// One parity phase on TT x TT tiles. kfirst: first plane of the parity (2 or
+// 3); order: the four sub-colours in visiting order, 2 bits each (step t in
+// bits 2t..2t+1).
+template <typename T, int TT>
+__global__ void __launch_bounds__(Gs27Tile<TT>::THREADS)
     gs27_phase_kernel(Dims d, Op14<T> A, const T *__restrict__ cc,
                       const T *__restrict__ fc, const T *__restrict__ own,
                       const T *nb, T *out, int kfirst, int order) {
+  constexpr int kT27 = TT, kW27 = Gs27Tile<TT>::W;
   __shared__ T xs[3][kW27 * kW27];
   const int ti0 = 2 + blockIdx.x * kT27;
   const int tj0 = 2 + blockIdx.y * kT27;
@@ -103,8 +108,8 @@ __global__ void __launch_bounds__(256)
       const int p = d.at(i, j, k);
       const int sidx = (i - i_lo) + kW27 * (j - j_lo);
       T tO, tU, tD;
-      sums27_tile(A, p, sy, sz, &xs[1][sidx], &xs[0][sidx], &xs[2][sidx], tO,
-                  tU, tD);
+      sums27_tile<T, kW27>(A, p, sy, sz, &xs[1][sidx], &xs[0][sidx],
+                           &xs[2][sidx], tO, tU, tD);
       const T c = cc ? cc[p] : T(0);
       xs[1][sidx] = (fc[p] + (tO + tU + tD)) / (A.a[kOC][p] + c);
     }
@@ -120,21 +125,37 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+template <typename T, int TT>
+void launch_gs27_phase(const Dims &d, const Op14<T> &A, const T *cc,
+                       const T *fc, const T *own, const T *nb, T *out,
+                       int kfirst, int order, int planes, cudaStream_t s) {
+  const unsigned tx = (unsigned)((d.nx - 2 + TT - 1) / TT);
+  const unsigned ty = (unsigned)((d.ny - 2 + TT - 1) / TT);
+  gs27_phase_kernel<T, TT>
+      <<<dim3(tx, ty, (unsigned)planes), Gs27Tile<TT>::THREADS, 0, s>>>(
+          d, A, cc, fc, own, nb, out, kfirst, order);
+}
+
+// Tile edge for a level: the tuned choice when pmg_build_hierarchy measured
+// one for this grid and element size (gs27_tune), else by size. Every tile
+// gives bit-identical results; only the speed differs.
+int gs27_tile_for(const Dims &d, int esize);
+
 // nsweeps eight-colour sweeps starting from x in `cur`, ping-ponging with
 // `alt` (whose shell must equal cur's). Returns the buffer holding the
-// result through *result.
+// result through *result. tile 0 picks gs27_tile_for.
 template <typename T>
 int launch_gs27_pp(const Dims &d, const Op14<T> &A, const T *cc, const T *fc,
                    T *cur, T *alt, int nsweeps, int iadjoint, int zero_init,
-                   cudaStream_t s, T **result) {
+                   cudaStream_t s, T **result, int tile = 0) {
   if (zero_init)
     PMG_CUDA_TRY(cudaMemsetAsync(cur, 0, sizeof(T) * d.count(), s));
+  if (tile == 0)
+    tile = gs27_tile_for(d, (int)sizeof(T));
   // visiting order of the colours c = sub + 4 * kpar
   const int first_par = iadjoint ? 1 : 0;
   const int order = iadjoint ? (3 | 2 << 2 | 1 << 4 | 0 << 6)
                              : (0 | 1 << 2 | 2 << 4 | 3 << 6);
-  const unsigned tx = (unsigned)((d.nx - 2 + kT27 - 1) / kT27);
-  const unsigned ty = (unsigned)((d.ny - 2 + kT27 - 1) / kT27);
   for (int sw = 0; sw < nsweeps; ++sw) {
     for (int ph = 0; ph < 2; ++ph) {
       const int par = ph == 0 ? first_par : 1 - first_par;
@@ -142,8 +163,16 @@ int launch_gs27_pp(const Dims &d, const Op14<T> &A, const T *cc, const T *fc,
       const int planes = kfirst > d.nz - 1 ? 0 : (d.nz - 1 - kfirst) / 2 + 1;
       if (planes == 0)
         continue;
-      gs27_phase_kernel<T><<<dim3(tx, ty, (unsigned)planes), 256, 0, s>>>(
-          d, A, cc, fc, cur, ph == 0 ? cur : alt, alt, kfirst, order);
+      const T *nb = ph == 0 ? cur : alt;
+      if (tile == 8)
+        launch_gs27_phase<T, 8>(d, A, cc, fc, cur, nb, alt, kfirst, order,
+                                planes, s);
+      else if (tile == 16)
+        launch_gs27_phase<T, 16>(d, A, cc, fc, cur, nb, alt, kfirst, order,
+                                 planes, s);
+      else
+        launch_gs27_phase<T, 32>(d, A, cc, fc, cur, nb, alt, kfirst, order,
+                                 planes, s);
     }
     T *t = cur;
     cur = alt;
@@ -153,5 +182,14 @@ int launch_gs27_pp(const Dims &d, const Op14<T> &A, const T *cc, const T *fc,
   *result = cur;
   return PMG_OK;
 }
+
+// Measures every tile edge on a level (two sweeps each, CUDA events, best of
+// three) and records the fastest for gs27_tile_for. x and alt are scratch
+// iterates of the level (same shell); synchronises the stream.
+template <typename T>
+int gs27_tune(const Dims &d, const Op14<T> &A, const T *fc, T *x, T *alt,
+              cudaStream_t s);
+void gs27_tile_record(const Dims &d, int esize, int tile);
+bool gs27_tile_known(const Dims &d, int esize);
 
 } // namespace pmg

@@ -1,3 +1,4 @@
+#include <map>
 #include <mutex>
 // Non-template kernels and the per-kernel C-ABI entry points (pmgc names).
 #include <math.h>
@@ -70,6 +71,88 @@ cudaError_t scratch_alloc(void **ptr, size_t bytes, cudaStream_t s) {
 cudaError_t scratch_free(void *ptr, cudaStream_t s) {
   return cudaFreeAsync(ptr, s);
 }
+
+// ---- tile edge of the 27-point smoother ------------------------------------
+namespace {
+std::mutex g_tile_mutex;
+std::map<std::pair<long, int>, int> g_tiles; // (nx*ny*nz key, esize) -> edge
+long tile_key(const Dims &d) {
+  return ((long)d.nx * 2048 + d.ny) * 2048 + d.nz;
+}
+} // namespace
+
+int gs27_tile_for(const Dims &d, int esize) {
+  {
+    std::lock_guard<std::mutex> lk(g_tile_mutex);
+    auto it = g_tiles.find({tile_key(d), esize});
+    if (it != g_tiles.end())
+      return it->second;
+  }
+  // untuned: enough CTAs for small levels, fewer halo points for large ones
+  const int n = d.nx < d.ny ? d.nx : d.ny;
+  return n >= 97 ? 32 : n >= 49 ? 16 : 8;
+}
+
+void gs27_tile_record(const Dims &d, int esize, int tile) {
+  std::lock_guard<std::mutex> lk(g_tile_mutex);
+  g_tiles[{tile_key(d), esize}] = tile;
+}
+
+bool gs27_tile_known(const Dims &d, int esize) {
+  std::lock_guard<std::mutex> lk(g_tile_mutex);
+  return g_tiles.count({tile_key(d), esize}) != 0;
+}
+
+template <typename T>
+int gs27_tune(const Dims &d, const Op14<T> &A, const T *fc, T *x, T *alt,
+              cudaStream_t s) {
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  PMG_CUDA_TRY(cudaEventCreate(&e0));
+  cudaError_t e = cudaEventCreate(&e1);
+  int best = 0;
+  float best_ms = 0.f;
+  for (int tile : kGs27Tiles) {
+    if (e != cudaSuccess)
+      break;
+    float ms_min = 0.f;
+    for (int rep = 0; rep < 4 && e == cudaSuccess; ++rep) {
+      T *res = nullptr;
+      e = cudaEventRecord(e0, s);
+      if (e == cudaSuccess &&
+          launch_gs27_pp<T>(d, A, nullptr, fc, x, alt, 2, 0, 0, s, &res,
+                            tile) != PMG_OK)
+        e = cudaErrorUnknown;
+      if (e == cudaSuccess)
+        e = cudaEventRecord(e1, s);
+      if (e == cudaSuccess)
+        e = cudaEventSynchronize(e1);
+      float ms = 0.f;
+      if (e == cudaSuccess)
+        e = cudaEventElapsedTime(&ms, e0, e1);
+      if (rep > 0 && (rep == 1 || ms < ms_min)) // first run warms up
+        ms_min = ms;
+    }
+    if (e == cudaSuccess && (best == 0 || ms_min < best_ms)) {
+      best = tile;
+      best_ms = ms_min;
+    }
+  }
+  cudaEventDestroy(e0);
+  if (e1)
+    cudaEventDestroy(e1);
+  if (e != cudaSuccess) {
+    set_last_error(e, "gs27_tune", __FILE__, __LINE__);
+    return PMG_ERR_CUDA;
+  }
+  gs27_tile_record(d, (int)sizeof(T), best);
+  return PMG_OK;
+}
+
+template int gs27_tune<float>(const Dims &, const Op14<float> &,
+                              const float *, float *, float *, cudaStream_t);
+template int gs27_tune<double>(const Dims &, const Op14<double> &,
+                               const double *, double *, double *,
+                               cudaStream_t);
 
 // ---------------------------------------------------------------------------
 // non-template kernels
