@@ -111,6 +111,8 @@ _sig("pmg_solve_start", c_int, _V, c_double, c_int)
 _sig("pmg_solve_poll", c_int, _V, PI)
 _sig("pmg_solve_finish", c_int, _V, PI, PD, PD)
 _sig("pmg_get_potential", c_int, _V, _V)
+_sig("pmg_get_potential_async", c_int, _V, _V)
+_sig("pmg_problem_set_stream", c_int, _V, _V)
 _sig("pmg_get_level", c_int, _V, c_int, _V)
 _sig("pmg_problem_stream", c_void_p, _V)
 _sig("pmg_problem_set_coarse_rtol", c_int, _V, c_double)
