@@ -289,8 +289,11 @@ def phase_bytes(p, level: int, phase: str, esz: int) -> float | None:
 # kernel launched by a cycle phase, and launches per phase occurrence
 def phase_kernel(p, level: int, phase: str):
     if phase in ("pre-smooth", "post-smooth"):
-        return ("gs7_color_kernel", 4) if level == p.nlev else (
-            "gs27_phase_kernel", 4)
+        if level < p.nlev:
+            return ("gs27_phase_kernel", 4)
+        # the mixed path's finest float level is colour-split
+        return ("gs7_split_color_kernel" if p.precision == "mixed"
+                else "gs7_color_kernel", 4)
     return {"residual": ("defect_norm_kernel", 1),
             "defect": ("defect_kernel", 1),
             "restrict": ("restrict_kernel", 1),

@@ -12,6 +12,7 @@
 #include "gs27_tiled.cuh"
 #include "launch.cuh"
 #include "pcg_kernels.cuh"
+#include "split_layout.cuh"
 #include "reduce_kernels.cuh"
 
 namespace pmg {
@@ -379,10 +380,10 @@ double norm_from_sum(const pmg_problem *p, double s) {
 
 int smooth32(pmg_problem *p, int L, int nsweeps, int zero_init, float **cur) {
   LevelBuf &v = p->lv[L];
-  if (L == p->nlev)
-    return launch_gs7<float>(v.d, v.op32[kOC], nullptr, v.f32, v.op32[kOE],
-                             v.op32[kON], v.op32[kUC], *cur, nsweeps, 0,
-                             zero_init, p->stream);
+  if (L == p->nlev) // colour-split layout (split_layout.cuh)
+    return launch_gs7_split<float>(v.d, v.op32[kOC], v.f32, v.op32[kOE],
+                                   v.op32[kON], v.op32[kUC], *cur, nsweeps, 0,
+                                   zero_init, p->stream);
   float *alt = *cur == v.x32 ? v.xalt32 : v.x32;
   return launch_gs27_pp<float>(v.d, v.A32(14), nullptr, v.f32, *cur, alt,
                                nsweeps, 0, zero_init, p->stream, cur);
@@ -441,9 +442,11 @@ int vcycle32(pmg_problem *p, int L) {
     return rc;
   prof_end(p, sl + kPhPre);
   prof_begin(p, sl + kPhDefect);
-  if (kind == 7)
-    defect_kernel<7, float><<<interior_grid(v.d), interior_block(), 0, s>>>(
-        v.d, v.A32(4), v.f32, x, v.r32);
+  if (kind == 7) // split arrays in, reference-layout defect out
+    defect7_split_kernel<float>
+        <<<interior_grid(v.d), interior_block(), 0, s>>>(
+            v.d, v.op32[kOC], v.op32[kOE], v.op32[kON], v.op32[kUC], v.f32, x,
+            v.r32);
   else
     defect_kernel<27, float><<<interior_grid(v.d), interior_block(), 0, s>>>(
         v.d, v.A32(14), v.f32, x, v.r32);
@@ -481,8 +484,12 @@ int vcycle32(pmg_problem *p, int L) {
       c.d, v.d, c.x32, v.r32, c.Pc32());
   prof_end(p, sl + kPhInterp);
   prof_begin(p, sl + kPhAxpy);
-  axpy_full_kernel<float><<<flat_grid(v.n3), 256, 0, s>>>(v.n3, x, v.r32,
-                                                          c.omega);
+  if (kind == 7) // the finest float iterate is split
+    axpy_split_kernel<float><<<flat_grid(v.n3), 256, 0, s>>>(v.d, x, v.r32,
+                                                             c.omega);
+  else
+    axpy_full_kernel<float><<<flat_grid(v.n3), 256, 0, s>>>(v.n3, x, v.r32,
+                                                            c.omega);
   prof_end(p, sl + kPhAxpy);
   PMG_LAUNCH_CHECK();
   prof_begin(p, sl + kPhPost);
@@ -502,7 +509,7 @@ int vcycle32(pmg_problem *p, int L) {
 int mixed_residual_async(pmg_problem *p, bool to_host = true) {
   LevelBuf &v = p->lv[p->nlev];
   prof_begin(p, kPhResidual);
-  defect_norm_kernel<7, double, float>
+  defect_norm_kernel<7, double, float, true>
       <<<reduce_grid(v.d), interior_block(), 0, p->stream>>>(
           v.d, v.A64(4), v.f, v.x, v.f32, p->red_norm);
   prof_end(p, kPhResidual);
@@ -522,8 +529,8 @@ int mixed_step(pmg_problem *p, bool to_host = true) {
   if ((rc = vcycle32(p, p->nlev)))
     return rc;
   prof_begin(p, kPhCorrect);
-  add_correction_kernel<<<interior_grid(v.d), interior_block(), 0,
-                          p->stream>>>(v.d, v.x, v.x32);
+  add_correction_split_kernel<<<interior_grid(v.d), interior_block(), 0,
+                                p->stream>>>(v.d, v.x, v.x32);
   prof_end(p, kPhCorrect);
   PMG_LAUNCH_CHECK();
   return mixed_residual_async(p, to_host);
@@ -831,14 +838,14 @@ int precondition(pmg_problem *p, const double *r, double *z) {
   cudaStream_t s = p->stream;
   const size_t b = sizeof(double) * v.n3;
   if (p->precision == PMG_PREC_MIXED) {
-    convert_kernel<double, float><<<flat_grid(v.n3), 256, 0, s>>>(v.n3, r,
-                                                                  v.f32);
+    to_split_kernel<double, float><<<flat_grid(v.n3), 256, 0, s>>>(v.d, r,
+                                                                   v.f32);
     PMG_LAUNCH_CHECK();
     int rc = vcycle32(p, p->nlev);
     if (rc)
       return rc;
-    convert_kernel<float, double><<<flat_grid(v.n3), 256, 0, s>>>(v.n3,
-                                                                  v.x32, z);
+    from_split_kernel<float, double><<<flat_grid(v.n3), 256, 0, s>>>(
+        v.d, v.x32, z);
     PMG_LAUNCH_CHECK();
     return PMG_OK;
   }
@@ -1154,8 +1161,12 @@ int pmg_build_hierarchy(pmg_problem *p, int trilinear) {
       const unsigned g = flat_grid(v.n3);
       for (int q = 0; q < 14; ++q)
         if (v.op32[q]) {
-          convert_kernel<double, float><<<g, 256, 0, s>>>(v.n3, v.op[q],
-                                                         v.op32[q]);
+          if (L == p->nlev) // the finest float operator is split
+            to_split_kernel<double, float><<<g, 256, 0, s>>>(v.d, v.op[q],
+                                                             v.op32[q]);
+          else
+            convert_kernel<double, float><<<g, 256, 0, s>>>(v.n3, v.op[q],
+                                                           v.op32[q]);
           ++p->launches;
         }
       for (int q = 0; q < 27; ++q)

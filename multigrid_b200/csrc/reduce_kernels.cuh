@@ -88,7 +88,7 @@ constexpr int kReducePlanes = 8;
 // sum over the interior of (f - A x)^2 with the defect of the class
 // (f - map(x), Convolution.h:137-139 and 170-175); optionally stores the
 // defect (cast to Tout) into r. Accumulates in double.
-template <int KIND, typename T, typename Tout>
+template <int KIND, typename T, typename Tout, bool SPLIT_OUT = false>
 __global__ void __launch_bounds__(kReduceThreads)
     defect_norm_kernel(Dims d, Op14<T> A, const T *__restrict__ f,
                        const T *__restrict__ x, Tout *__restrict__ r,
@@ -105,8 +105,14 @@ __global__ void __launch_bounds__(kReduceThreads)
       const int p = d.at(i, j, k);
       const T dv =
           f[p] - apply_op<KIND>(A, (const T *)nullptr, x, p, sy, sz);
-      if (r)
-        r[p] = (Tout)dv;
+      if (r) {
+        if constexpr (SPLIT_OUT) { // colour-split row layout (i-1 parity)
+          const int q = i - 1;
+          r[p - q + (q >> 1) + (q & 1) * ((d.nx + 1) / 2)] = (Tout)dv;
+        } else {
+          r[p] = (Tout)dv;
+        }
+      }
       acc += (double)dv * (double)dv;
     }
   }
