@@ -50,7 +50,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     # skip the batched (96 molecules) and serving (Poisson load) legs
     ap.add_argument("--no-extras", action="store_true")
-    # one precision, no end-to-end or kernel legs: a short run for profilers
+    # one precision, no end-to-end or kernel legs, cycles driven from the
+    # host: a short run for kernel profilers
     ap.add_argument("--quick", action="store_true")
     return ap.parse_args()
 
@@ -604,6 +605,10 @@ def main():
         precisions.append("fp64" if args.precision == "mixed" else "mixed")
     for precision in precisions:
         p = PBELinearProblem(w.base, w.nlev, w.box, precision, w.physics)
+        if args.quick:
+            # profiler runs: kernel profilers do not see kernels inside
+            # graphs with conditional nodes, so drive the cycles from the host
+            p.set_host_loop(True)
         stream = torch.cuda.ExternalStream(p.stream)
         for _ in range(args.warmup):
             res = step(p, dev)

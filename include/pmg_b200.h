@@ -406,6 +406,13 @@ int pmg_get_level(pmg_problem *p, int level, double *dst);
  * class's absolute 1e-8 test). */
 int pmg_problem_set_coarse_rtol(pmg_problem *p, double rtol);
 
+/* on != 0: pmg_solve drives its cycles from the host (one cycle-graph
+ * launch and one residual read-back per cycle) instead of the single graph
+ * with the device-side stop test; same decisions, same results. For tools
+ * that cannot look inside graphs with conditional nodes (kernel profilers).
+ * No reference counterpart. */
+int pmg_problem_set_host_loop(pmg_problem *p, int on);
+
 /* Phase timing: with on != 0, pmg_solve records CUDA events around every
  * phase of every cycle (inside the captured cycle graph) and accumulates the
  * elapsed times. */

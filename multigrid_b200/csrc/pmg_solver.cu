@@ -128,6 +128,7 @@ struct pmg_problem {
   SolveState *h_state = nullptr; // pinned
   cudaEvent_t done_ev = nullptr;
   bool solve_pending = false;
+  bool host_loop = false; // pmg_problem_set_host_loop
   // MG-preconditioned CG on the finest level (allocated on first use):
   // right-hand side, iterate, residual, preconditioned residual, search
   // direction, A times it; three reduction slots; the iteration state.
@@ -1053,6 +1054,13 @@ int pmg_problem_set_coarse_rtol(pmg_problem *p, double rtol) {
   return PMG_OK;
 }
 
+int pmg_problem_set_host_loop(pmg_problem *p, int on) {
+  if (!p)
+    return PMG_ERR_ARG;
+  p->host_loop = on != 0;
+  return PMG_OK;
+}
+
 int pmg_problem_set_profiling(pmg_problem *p, int on) {
   if (!p)
     return PMG_ERR_ARG;
@@ -1371,7 +1379,7 @@ int pmg_solve(pmg_problem *p, double tol, int max_cycles, int *cycles,
     set_last_message("pmg_solve: a solve is already in flight");
     return PMG_ERR_STATE;
   }
-  if (p->prof_on || max_cycles > kMaxHist)
+  if (p->prof_on || p->host_loop || max_cycles > kMaxHist)
     return solve_host_loop(p, tol, max_cycles, cycles, relres, hist);
   int rc = pmg_solve_start(p, tol, max_cycles);
   if (rc)

@@ -202,6 +202,14 @@ class PBELinearProblem:
               "interp", "axpy", "post-smooth")
     GLOBAL_PHASES = ("residual", "refine-update")
 
+    def set_host_loop(self, on: bool = True) -> None:
+        """Drive solve()'s cycles from the host (one graph launch per cycle)
+        instead of one graph with the stop test on the GPU: same results;
+        for kernel profilers, which cannot see kernels inside graphs with
+        conditional nodes."""
+        _lib.check("pmg_problem_set_host_loop",
+                   _lib.lib.pmg_problem_set_host_loop(self._h, int(on)))
+
     def set_profiling(self, on: bool = True) -> None:
         """Time every cycle phase with CUDA events inside the cycle graph."""
         _lib.check("pmg_problem_set_profiling",

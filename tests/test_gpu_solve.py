@@ -249,3 +249,20 @@ def test_reused_handle_solves_like_a_fresh_one(golden_problem, precision):
     assert r1.cycles == r2.cycles
     assert np.array_equal(r1.history, r2.history)
     assert np.array_equal(x1, x2)
+
+
+def test_host_loop_switch_gives_the_same_solve(golden_problem):
+    """pmg_problem_set_host_loop: the host-driven cycles (for profilers) and
+    the one-graph solve give the same bits."""
+    g = golden_problem
+    base, nlev, box = int(g["base"]), int(g["nlev"]), float(g["box"])
+    out = []
+    for host in (False, True):
+        with PBELinearProblem(base, nlev, box, "mixed") as p:
+            p.set_host_loop(host)
+            p.set_fine(**fine_of(g))
+            p.buildmultilevelops()
+            r = p.solve(tol=1e-10, max_cycles=60)
+            out.append((r.cycles, p.potential().ravel().copy()))
+    assert out[0][0] == out[1][0]
+    assert np.array_equal(out[0][1], out[1][1])

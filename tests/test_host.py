@@ -136,8 +136,8 @@ def test_bench_reads_profiled_traffic():
         "bench", os.path.join(os.path.dirname(__file__), "..", "bench.py"))
     bench = importlib.util.module_from_spec(spec)
     spec.loader.exec_module(bench)
-    t = bench.profiled_traffic("gs7_color_kernel", 4, "pb257", "mixed")
-    assert t is not None and t > 4 * 4.0e8
+    t = bench.profiled_traffic("gs7_split_color_kernel", 4, "pb257", "mixed")
+    assert t == pytest.approx(4 * 343670000)
     assert bench.profiled_traffic("no_such_kernel", 1, "pb257", "mixed") is None
     assert bench.profiled_traffic(None, 1, "pb257", "mixed") is None
 
