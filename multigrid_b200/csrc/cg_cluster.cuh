@@ -1,0 +1,237 @@
+// Coarsest-level CG on a cluster of CTAs with the operator held in shared
+// memory.
+//
+// The one-CTA CG (cg_level_kernel) streams the level's fourteen coefficient
+// arrays (17^3 doubles: 550 KB) from L2 through a single SM on every
+// iteration. Here a cluster of kCgCtas CTAs splits the level by planes: each
+// CTA keeps the coefficients of its planes (and of the plane below, for the
+// lower couplings) in its shared memory for the whole solve, holds its
+// points' x, r, A p in registers and its planes of p in shared memory, and
+// reads the neighbouring planes of p from the neighbouring CTAs' shared
+// memory (distributed shared memory). Dot products are block sums summed
+// over the cluster in rank order, so every CTA gets the same bits and takes
+// the same branch. The iteration is the class's CG (CG_solver,
+// CG_Solver.h:45-242, via solve_by_cg<1>): see launch_cg_level.
+#pragma once
+
+#include <cooperative_groups.h>
+
+#include "reduce_kernels.cuh"
+
+namespace pmg {
+
+constexpr int kCgCtas = 8;        // CTAs of the cluster
+constexpr int kCgThreads = 512;   // threads per CTA, one point each
+constexpr int kCgMaxPlanes = 2;   // interior planes per CTA
+constexpr int kCgMaxN = 17;       // points per axis (incl. shell)
+
+// first interior plane of CTA c (planes 2 .. nz-1 split evenly)
+__host__ __device__ inline int cg_plane_lo(int c, int nz) {
+  return 2 + (c * (nz - 2)) / kCgCtas;
+}
+
+// CTA holding interior plane k
+__host__ __device__ inline int cg_plane_owner(int k, int nz) {
+  int c = 0;
+  while (c + 1 < kCgCtas && cg_plane_lo(c + 1, nz) <= k)
+    ++c;
+  return c;
+}
+
+// bytes of dynamic shared memory for an nx x ny level
+inline size_t cg_cluster_smem(int nx, int ny) {
+  const size_t nxy = (size_t)nx * ny;
+  return sizeof(double) *
+         ((kCgMaxPlanes + 1) * 14 * nxy + kCgMaxPlanes * nxy + 2 * kCgCtas);
+}
+
+inline bool cg_cluster_fits(const Dims &d) {
+  return d.nx <= kCgMaxN && d.ny <= kCgMaxN && d.nz <= kCgMaxN &&
+         (d.nx - 2) * (d.ny - 2) * kCgMaxPlanes <= kCgThreads &&
+         d.nz - 2 <= kCgCtas * kCgMaxPlanes;
+}
+
+// Sum of v over the CTA, in every thread (warp sums, then the warps in
+// order); sh holds 32 doubles.
+__device__ __forceinline__ double cg_block_sum(double v, double *sh) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
+    v += __shfl_down_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0)
+    sh[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double t = 0.0;
+  const int nw = blockDim.x >> 5;
+  for (int w = 0; w < nw; ++w)
+    t += sh[w];
+  return t;
+}
+
+// (A v)(i, j, k) in apply27's order (sums27, then -tO - tU - tD + oC v); a(s,
+// di, dj, dk) the coupling slot s at the offset point, v(di, dj, dk) the
+// vector there.
+template <class CoefFn, class VecFn>
+__device__ __forceinline__ double apply27_at(CoefFn a, VecFn v) {
+  const double tO = a(kON, 0, 0, 0) * v(0, 1, 0) +
+                    a(kON, 0, -1, 0) * v(0, -1, 0) +
+                    a(kOE, 0, 0, 0) * v(1, 0, 0) +
+                    a(kOE, -1, 0, 0) * v(-1, 0, 0) +
+                    a(kONE, 0, 0, 0) * v(1, 1, 0) +
+                    a(kONW, 0, 0, 0) * v(-1, 1, 0) +
+                    a(kONW, 1, -1, 0) * v(1, -1, 0) +
+                    a(kONE, -1, -1, 0) * v(-1, -1, 0);
+  const double tU = a(kUC, 0, 0, 0) * v(0, 0, 1) +
+                    a(kUN, 0, 0, 0) * v(0, 1, 1) +
+                    a(kUS, 0, 0, 0) * v(0, -1, 1) +
+                    a(kUE, 0, 0, 0) * v(1, 0, 1) +
+                    a(kUW, 0, 0, 0) * v(-1, 0, 1) +
+                    a(kUNE, 0, 0, 0) * v(1, 1, 1) +
+                    a(kUNW, 0, 0, 0) * v(-1, 1, 1) +
+                    a(kUSE, 0, 0, 0) * v(1, -1, 1) +
+                    a(kUSW, 0, 0, 0) * v(-1, -1, 1);
+  const double tD = a(kUC, 0, 0, -1) * v(0, 0, -1) +
+                    a(kUS, 0, 1, -1) * v(0, 1, -1) +
+                    a(kUN, 0, -1, -1) * v(0, -1, -1) +
+                    a(kUW, 1, 0, -1) * v(1, 0, -1) +
+                    a(kUE, -1, 0, -1) * v(-1, 0, -1) +
+                    a(kUSW, 1, 1, -1) * v(1, 1, -1) +
+                    a(kUSE, -1, 1, -1) * v(-1, 1, -1) +
+                    a(kUNW, 1, -1, -1) * v(1, -1, -1) +
+                    a(kUNE, -1, -1, -1) * v(-1, -1, -1);
+  return (-tO) + (-tU) + (-tD) + (a(kOC, 0, 0, 0) + 0.0) * v(0, 0, 0);
+}
+
+__global__ void __cluster_dims__(kCgCtas, 1, 1) __launch_bounds__(kCgThreads)
+    cg_cluster_kernel(Dims d, Op14<double> A, const double *__restrict__ rhs,
+                      double *__restrict__ x, double thresh, double rel_tol,
+                      int class_first_check, int max_iters,
+                      int *__restrict__ status) {
+  namespace cgs = cooperative_groups;
+  cgs::cluster_group cluster = cgs::this_cluster();
+  extern __shared__ __align__(16) double cg_smem[];
+  const int nx = d.nx, ny = d.ny, nxy = nx * ny;
+  // [plane klo-1 .. khi][slot][j][i] coefficients, then p of klo .. khi,
+  // then two reduction slots per CTA rank
+  double *sA = cg_smem;
+  double *sP = sA + (kCgMaxPlanes + 1) * 14 * nxy;
+  double *sRed = sP + kCgMaxPlanes * nxy;
+  __shared__ double sh[32];
+
+  const int rank = (int)cluster.block_rank();
+  const int klo = cg_plane_lo(rank, d.nz);
+  const int khi = cg_plane_lo(rank + 1, d.nz) - 1; // may be < klo
+  const int nplanes = khi - klo + 1;
+  const int mi = nx - 2, mj = ny - 2;
+
+  // the coefficients of planes klo-1 .. khi, whole planes (shell included)
+  for (int q = threadIdx.x; q < (nplanes + 1) * 14 * nxy; q += blockDim.x) {
+    const int lk = q / (14 * nxy), rem = q - lk * 14 * nxy;
+    const int slot = rem / nxy, o = rem - slot * nxy;
+    const int k = klo - 1 + lk;
+    sA[q] = A.a[slot][(long)(k - 1) * nxy + o];
+  }
+  for (int q = threadIdx.x; q < kCgMaxPlanes * nxy; q += blockDim.x)
+    sP[q] = 0.0; // shells of p stay zero
+
+  // this thread's point
+  const int t = threadIdx.x;
+  const bool own = t < nplanes * mi * mj;
+  int i = 2, j = 2, k = klo;
+  if (own) {
+    const int lp = t / (mi * mj), r2 = t - lp * mi * mj;
+    j = 2 + r2 / mi;
+    i = 2 + r2 % mi;
+    k = klo + lp;
+  }
+  const int gi = d.at(i, j, k);
+  const int sl = (k - klo) * nxy + (j - 1) * nx + (i - 1); // in sP
+  // the CTAs holding the planes below and above this point's plane (when
+  // those are interior planes of another CTA)
+  const int rk_dn = cg_plane_owner(k - 1, d.nz);
+  const int rk_up = cg_plane_owner(k + 1, d.nz);
+
+  auto coef = [&](int slot, int di, int dj, int dk) -> double {
+    const int lk = k + dk - (klo - 1);
+    return sA[(lk * 14 + slot) * nxy + (j - 1 + dj) * nx + (i - 1 + di)];
+  };
+  // p at an offset: own planes from this CTA, the planes next to them from
+  // the CTA holding them, shell planes zero
+  auto pval = [&](int di, int dj, int dk) -> double {
+    const int kk = k + dk;
+    const int o = (j - 1 + dj) * nx + (i - 1 + di);
+    if (kk >= klo && kk <= khi)
+      return sP[(kk - klo) * nxy + o];
+    if (kk < 2 || kk > d.nz - 1)
+      return 0.0;
+    const int r = kk < klo ? rk_dn : rk_up;
+    const int rlo = cg_plane_lo(r, d.nz);
+    const double *remote = cluster.map_shared_rank(sP, r);
+    return remote[(kk - rlo) * nxy + o];
+  };
+  auto xval = [&](int di, int dj, int dk) -> double {
+    return x[gi + di + dj * nx + dk * nxy];
+  };
+  // cluster-wide sum in rank order (identical bits in every CTA)
+  auto cluster_sum = [&](double v, int slot) -> double {
+    const double b = cg_block_sum(v, sh);
+    if (threadIdx.x == 0)
+      sRed[slot * kCgCtas + 0] = b;
+    cluster.sync();
+    double s = 0.0;
+    for (int r = 0; r < kCgCtas; ++r)
+      s += cluster.map_shared_rank(sRed, r)[slot * kCgCtas];
+    __syncthreads(); // sh is reused by the next block sum
+    return s;
+  };
+
+  // r = rhs - A x; p = r; rs = r.r
+  double xv = 0.0, rv = 0.0, apv = 0.0;
+  __syncthreads(); // coefficients staged
+  if (own) {
+    xv = x[gi];
+    rv = rhs[gi] - apply27_at(coef, xval);
+    sP[sl] = rv;
+  }
+  double rs = cluster_sum(own ? rv * rv : 0.0, 0);
+  // Ap and p.Ap (p is visible to the neighbours after the sum's sync)
+  if (own)
+    apv = apply27_at(coef, pval);
+  double pap = cluster_sum(own ? apv * sP[sl] : 0.0, 1);
+  int it = 0;
+  double res = 0.0;
+  if (pap != 0.0) {
+    double alpha = rs / pap;
+    res = class_first_check ? sqrt(sqrt(rs)) : sqrt(rs);
+    const double stop = fmax(thresh, rel_tol * sqrt(rs));
+    while (res > stop && it < max_iters) {
+      ++it;
+      if (own) {
+        xv += alpha * sP[sl];
+        rv = rv - alpha * apv;
+      }
+      const double rsn = cluster_sum(own ? rv * rv : 0.0, 0);
+      const double beta = rs == 0.0 ? 0.0 : rsn / rs;
+      rs = rsn;
+      if (own)
+        sP[sl] = rv + beta * sP[sl];
+      cluster.sync(); // every CTA's new p before anyone reads it
+      if (own)
+        apv = apply27_at(coef, pval);
+      pap = cluster_sum(own ? apv * sP[sl] : 0.0, 1);
+      alpha = pap == 0.0 ? 0.0 : rs / pap;
+      res = sqrt(rs);
+    }
+    if (rank == 0 && threadIdx.x == 0) {
+      status[0] = it;
+      status[1] = (it >= max_iters && res > stop) ? 1 : 0;
+    }
+  } else if (rank == 0 && threadIdx.x == 0) {
+    status[0] = 0;
+    status[1] = 0;
+  }
+  if (own)
+    x[gi] = xv;
+  cluster.sync(); // no CTA leaves while another may still read its p
+}
+
+} // namespace pmg

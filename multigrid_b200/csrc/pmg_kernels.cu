@@ -10,6 +10,7 @@
 #include "launch.cuh"
 #include "reduce_kernels.cuh"
 #include "split_layout.cuh"
+#include "cg_cluster.cuh"
 
 namespace pmg {
 
@@ -303,6 +304,21 @@ int launch_cg_level(const Dims &d, const Op14<double> &A, const double *rhs,
                     double *x, double *r, double *p, double *ap,
                     double thresh, double rel_tol, int class_first_check,
                     int max_iters, int *status, cudaStream_t s) {
+  if (cg_cluster_fits(d)) {
+    // levels up to 17^3: a cluster with the operator in shared memory
+    const size_t smem = cg_cluster_smem(d.nx, d.ny);
+    static size_t configured = 0;
+    if (configured < smem) {
+      PMG_CUDA_TRY(cudaFuncSetAttribute(
+          cg_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+          (int)cg_cluster_smem(kCgMaxN, kCgMaxN)));
+      configured = cg_cluster_smem(kCgMaxN, kCgMaxN);
+    }
+    cg_cluster_kernel<<<kCgCtas, kCgThreads, smem, s>>>(
+        d, A, rhs, x, thresh, rel_tol, class_first_check, max_iters, status);
+    PMG_LAUNCH_CHECK();
+    return PMG_OK;
+  }
   const long m = (long)(d.nx - 2) * (d.ny - 2) * (d.nz - 2);
   const int k = (int)((m + 1023) / 1024);
 #define PMG_CG(K)                                                              \
