@@ -12,7 +12,10 @@
 // runs the four sub-colour steps there; step t also recomputes its
 // sub-colour on a halo of 3 - t points so that the next steps find new
 // values at the tile edge without talking to other CTAs. Coefficients are
-// read from global memory (each once per computed point).
+// read from global memory (each once per computed point). The x planes are
+// staged with cp.async (zero fill off the array), and every sub-colour step
+// walks a fixed (TT/2 + h)^2 grid of its points, so the slot-to-point map is
+// compile-time arithmetic.
 //
 // Reads and writes go to different buffers (ping-pong): the first-parity
 // launch reads `cur` and writes the first-parity planes of `alt`; the
@@ -35,26 +38,120 @@ template <int TT> struct Gs27Tile {
   static constexpr int THREADS = TT >= 32 ? 256 : TT >= 16 ? 128 : 64;
 };
 
-template <typename T, int w>
-__device__ __forceinline__ void sums27_tile(const Op14<T> &A, int p, int sy,
-                                            int sz, const T *xc, const T *xd,
-                                            const T *xu, T &tO, T &tU,
-                                            T &tD) {
+// B-byte cp.async into shared memory; reads nothing and writes zero when
+// `in` is false (gmem must still be a valid address)
+template <int B>
+__device__ __forceinline__ void cp_async_zfill(void *smem, const void *gmem,
+                                               bool in) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  const int n = in ? B : 0;
+  if constexpr (B == 4)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s),
+                 "l"(gmem), "r"(n)
+                 : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s),
+                 "l"(gmem), "r"(n)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::
+                   : "memory");
+}
+
+// The couplings, right-hand side and diagonal of one point; loaded in full
+// before any of it is used (fewer live registers than interleaving the loads
+// with the sums).
+template <typename T> struct Gs27Point {
+  T a[26]; // sums27's couplings in its order: tO (8), tU (9), tD (9)
+  T f, d;  // right-hand side, diagonal (oC + cc)
+};
+
+template <typename T>
+__device__ __forceinline__ void gs27_load(const Op14<T> &A, const T *cc,
+                                          const T *fc, int p, int sy, int sz,
+                                          Gs27Point<T> &c) {
   const T *const *a = A.a;
-  tO = a[kON][p] * xc[w] + a[kON][p - sy] * xc[-w] + a[kOE][p] * xc[1] +
-       a[kOE][p - 1] * xc[-1] + a[kONE][p] * xc[1 + w] +
-       a[kONW][p] * xc[-1 + w] + a[kONW][p + 1 - sy] * xc[1 - w] +
-       a[kONE][p - 1 - sy] * xc[-1 - w];
-  tU = a[kUC][p] * xu[0] + a[kUN][p] * xu[w] + a[kUS][p] * xu[-w] +
-       a[kUE][p] * xu[1] + a[kUW][p] * xu[-1] + a[kUNE][p] * xu[1 + w] +
-       a[kUNW][p] * xu[-1 + w] + a[kUSE][p] * xu[1 - w] +
-       a[kUSW][p] * xu[-1 - w];
-  tD = a[kUC][p - sz] * xd[0] + a[kUS][p + sy - sz] * xd[w] +
-       a[kUN][p - sy - sz] * xd[-w] + a[kUW][p + 1 - sz] * xd[1] +
-       a[kUE][p - 1 - sz] * xd[-1] + a[kUSW][p + 1 + sy - sz] * xd[1 + w] +
-       a[kUSE][p - 1 + sy - sz] * xd[-1 + w] +
-       a[kUNW][p + 1 - sy - sz] * xd[1 - w] +
-       a[kUNE][p - 1 - sy - sz] * xd[-1 - w];
+  c.a[0] = a[kON][p];
+  c.a[1] = a[kON][p - sy];
+  c.a[2] = a[kOE][p];
+  c.a[3] = a[kOE][p - 1];
+  c.a[4] = a[kONE][p];
+  c.a[5] = a[kONW][p];
+  c.a[6] = a[kONW][p + 1 - sy];
+  c.a[7] = a[kONE][p - 1 - sy];
+  c.a[8] = a[kUC][p];
+  c.a[9] = a[kUN][p];
+  c.a[10] = a[kUS][p];
+  c.a[11] = a[kUE][p];
+  c.a[12] = a[kUW][p];
+  c.a[13] = a[kUNE][p];
+  c.a[14] = a[kUNW][p];
+  c.a[15] = a[kUSE][p];
+  c.a[16] = a[kUSW][p];
+  c.a[17] = a[kUC][p - sz];
+  c.a[18] = a[kUS][p + sy - sz];
+  c.a[19] = a[kUN][p - sy - sz];
+  c.a[20] = a[kUW][p + 1 - sz];
+  c.a[21] = a[kUE][p - 1 - sz];
+  c.a[22] = a[kUSW][p + 1 + sy - sz];
+  c.a[23] = a[kUSE][p - 1 + sy - sz];
+  c.a[24] = a[kUNW][p + 1 - sy - sz];
+  c.a[25] = a[kUNE][p - 1 - sy - sz];
+  c.f = fc[p];
+  c.d = a[kOC][p] + (cc ? cc[p] : T(0));
+}
+
+// The new value from x staged around the point (xc: plane k, xd: k-1, xu:
+// k+1, rows w apart): (f + (tO + tU + tD)) / (oC + cc), sums27's order.
+template <typename T, int w>
+__device__ __forceinline__ T gs27_update(const Gs27Point<T> &c, const T *xc,
+                                         const T *xd, const T *xu) {
+  const T tO = c.a[0] * xc[w] + c.a[1] * xc[-w] + c.a[2] * xc[1] +
+               c.a[3] * xc[-1] + c.a[4] * xc[1 + w] + c.a[5] * xc[-1 + w] +
+               c.a[6] * xc[1 - w] + c.a[7] * xc[-1 - w];
+  const T tU = c.a[8] * xu[0] + c.a[9] * xu[w] + c.a[10] * xu[-w] +
+               c.a[11] * xu[1] + c.a[12] * xu[-1] + c.a[13] * xu[1 + w] +
+               c.a[14] * xu[-1 + w] + c.a[15] * xu[1 - w] +
+               c.a[16] * xu[-1 - w];
+  const T tD = c.a[17] * xd[0] + c.a[18] * xd[w] + c.a[19] * xd[-w] +
+               c.a[20] * xd[1] + c.a[21] * xd[-1] + c.a[22] * xd[1 + w] +
+               c.a[23] * xd[-1 + w] + c.a[24] * xd[1 - w] +
+               c.a[25] * xd[-1 - w];
+  return (c.f + (tO + tU + tD)) / c.d;
+}
+
+// Sub-colour step with halo H (step 3 - H of the phase): the points of the
+// step's sub-colour within H of the tile, a fixed NU x NU grid of them
+// clipped to the interior.
+template <typename T, int TT, int H>
+__device__ __forceinline__ void gs27_step(const Dims &d, const Op14<T> &A,
+                                          const T *cc, const T *fc, T *xs,
+                                          int ti0, int tj0, int k,
+                                          int order) {
+  constexpr int W = Gs27Tile<TT>::W, NT = Gs27Tile<TT>::THREADS;
+  constexpr int NU = TT / 2 + H, NQ = NU * NU;
+  const int sy = d.sy(), sz = d.sz();
+  const int s = (order >> (2 * (3 - H))) & 3;
+  const int pi = s & 1, pj = s >> 1;
+  // first point of the sub-colour at or after ti0 - H (tj0 - H)
+  const int ia = ti0 - H + ((pi - (ti0 - H)) & 1);
+  const int ja = tj0 - H + ((pj - (tj0 - H)) & 1);
+  const int i_lo = ti0 - kH27, j_lo = tj0 - kH27;
+  const int i_max = d.nx - 1, j_max = d.ny - 1;
+#pragma unroll
+  for (int m = 0; m < (NQ + NT - 1) / NT; ++m) {
+    const int q = threadIdx.x + m * NT;
+    const int v = q / NU, u = q - v * NU;
+    const int i = ia + 2 * u, j = ja + 2 * v;
+    if (q < NQ && i >= 2 && i <= i_max && j >= 2 && j <= j_max) {
+      const int sidx = W * W + (i - i_lo) + W * (j - j_lo);
+      Gs27Point<T> c;
+      gs27_load(A, cc, fc, d.at(i, j, k), sy, sz, c);
+      xs[sidx] = gs27_update<T, W>(c, &xs[sidx], &xs[sidx - W * W],
+                                   &xs[sidx + W * W]);
+    }
+  }
 }
 
 // One parity phase on TT x TT tiles. kfirst: first plane of the parity (2 or
@@ -65,63 +162,42 @@ __global__ void __launch_bounds__(Gs27Tile<TT>::THREADS)
     gs27_phase_kernel(Dims d, Op14<T> A, const T *__restrict__ cc,
                       const T *__restrict__ fc, const T *__restrict__ own,
                       const T *nb, T *out, int kfirst, int order) {
-  constexpr int kT27 = TT, kW27 = Gs27Tile<TT>::W;
-  __shared__ T xs[3][kW27 * kW27];
-  const int ti0 = 2 + blockIdx.x * kT27;
-  const int tj0 = 2 + blockIdx.y * kT27;
+  constexpr int W = Gs27Tile<TT>::W, NT = Gs27Tile<TT>::THREADS;
+  // planes k-1 (nb), k (own), k+1 (nb), W x W points each
+  __shared__ __align__(16) T xs[3 * W * W];
+  const int ti0 = 2 + blockIdx.x * TT, tj0 = 2 + blockIdx.y * TT;
   const int k = kfirst + 2 * blockIdx.z;
-  const int sy = d.sy(), sz = d.sz();
   const int i_lo = ti0 - kH27, j_lo = tj0 - kH27;
 
-  // stage planes k-1 (nb), k (own), k+1 (nb); points off the array are
-  // never read by an update and are set to zero
-  for (int q = threadIdx.x; q < 3 * kW27 * kW27; q += blockDim.x) {
-    const int pl = q / (kW27 * kW27);
-    const int rem = q - pl * kW27 * kW27;
-    const int jj = rem / kW27, ii = rem - jj * kW27;
-    const int i = i_lo + ii, j = j_lo + jj, kk = k - 1 + pl;
-    T v = T(0);
-    if (i >= 1 && i <= d.nx && j >= 1 && j <= d.ny) {
-      const int g = d.at(i, j, kk);
-      v = pl == 1 ? own[g] : nb[g];
-    }
-    xs[pl][rem] = v;
+  // points off the array are never read by an update and are set to zero
+  for (int q = threadIdx.x; q < 3 * W * W; q += NT) {
+    const int pl = q / (W * W), rem = q - pl * (W * W);
+    const int jj = rem / W, ii = rem - jj * W;
+    const int i = i_lo + ii, j = j_lo + jj;
+    const bool in = i >= 1 && i <= d.nx && j >= 1 && j <= d.ny;
+    const T *src = (pl == 1 ? own : nb) + (in ? d.at(i, j, k - 1 + pl) : 0);
+    cp_async_zfill<sizeof(T)>(&xs[q], src, in);
   }
+  cp_async_wait_all();
+  __syncthreads();
+  gs27_step<T, TT, 3>(d, A, cc, fc, xs, ti0, tj0, k, order);
+  __syncthreads();
+  gs27_step<T, TT, 2>(d, A, cc, fc, xs, ti0, tj0, k, order);
+  __syncthreads();
+  gs27_step<T, TT, 1>(d, A, cc, fc, xs, ti0, tj0, k, order);
+  __syncthreads();
+  gs27_step<T, TT, 0>(d, A, cc, fc, xs, ti0, tj0, k, order);
   __syncthreads();
 
+  // write the tile's interior points of plane k
   const int i_max = d.nx - 1, j_max = d.ny - 1;
 #pragma unroll
-  for (int t = 0; t < 4; ++t) {
-    const int s = (order >> (2 * t)) & 3;
-    const int h = 3 - t;
-    const int pi = s & 1, pj = (s >> 1) & 1;
-    // region of this step, clipped to the interior, first point of parity
-    int ia = max(ti0 - h, 2), ib = min(ti0 + kT27 - 1 + h, i_max);
-    int ja = max(tj0 - h, 2), jb = min(tj0 + kT27 - 1 + h, j_max);
-    ia += (pi - ia) & 1;
-    ja += (pj - ja) & 1;
-    const int ni = ib >= ia ? (ib - ia) / 2 + 1 : 0;
-    const int nj = jb >= ja ? (jb - ja) / 2 + 1 : 0;
-    for (int q = threadIdx.x; q < ni * nj; q += blockDim.x) {
-      const int qj = q / ni;
-      const int i = ia + 2 * (q - qj * ni), j = ja + 2 * qj;
-      const int p = d.at(i, j, k);
-      const int sidx = (i - i_lo) + kW27 * (j - j_lo);
-      T tO, tU, tD;
-      sums27_tile<T, kW27>(A, p, sy, sz, &xs[1][sidx], &xs[0][sidx],
-                           &xs[2][sidx], tO, tU, tD);
-      const T c = cc ? cc[p] : T(0);
-      xs[1][sidx] = (fc[p] + (tO + tU + tD)) / (A.a[kOC][p] + c);
-    }
-    __syncthreads();
-  }
-
-  // write the tile's interior points of plane k
-  for (int q = threadIdx.x; q < kT27 * kT27; q += blockDim.x) {
-    const int jj = q / kT27, ii = q - jj * kT27;
+  for (int m = 0; m < (TT * TT + NT - 1) / NT; ++m) {
+    const int q = threadIdx.x + m * NT;
+    const int jj = q / TT, ii = q - jj * TT;
     const int i = ti0 + ii, j = tj0 + jj;
-    if (i <= i_max && j <= j_max)
-      out[d.at(i, j, k)] = xs[1][(i - i_lo) + kW27 * (j - j_lo)];
+    if (q < TT * TT && i <= i_max && j <= j_max)
+      out[d.at(i, j, k)] = xs[W * W + (i - i_lo) + W * (j - j_lo)];
   }
 }
 
