@@ -38,27 +38,6 @@ template <int TT> struct Gs27Tile {
   static constexpr int THREADS = TT >= 32 ? 256 : TT >= 16 ? 128 : 64;
 };
 
-// B-byte cp.async into shared memory; reads nothing and writes zero when
-// `in` is false (gmem must still be a valid address)
-template <int B>
-__device__ __forceinline__ void cp_async_zfill(void *smem, const void *gmem,
-                                               bool in) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  const int n = in ? B : 0;
-  if constexpr (B == 4)
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s),
-                 "l"(gmem), "r"(n)
-                 : "memory");
-  else
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s),
-                 "l"(gmem), "r"(n)
-                 : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() {
-  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::
-                   : "memory");
-}
-
 // The couplings, right-hand side and diagonal of one point; loaded in full
 // before any of it is used (fewer live registers than interleaving the loads
 // with the sums).

@@ -42,6 +42,27 @@ template <typename T> struct P27W {
   T *p[27];
 };
 
+// B-byte cp.async into shared memory; reads nothing and writes zero when
+// `in` is false (gmem must still be a valid address)
+template <int B>
+__device__ __forceinline__ void cp_async_zfill(void *smem, const void *gmem,
+                                               bool in) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  const int n = in ? B : 0;
+  if constexpr (B == 4)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s),
+                 "l"(gmem), "r"(n)
+                 : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s),
+                 "l"(gmem), "r"(n)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::
+                   : "memory");
+}
+
 enum OpSlot {
   kOC = 0, kOE, kON, kUC, kONE, kONW, kUE, kUW, kUN, kUS, kUNE, kUNW, kUSE,
   kUSW

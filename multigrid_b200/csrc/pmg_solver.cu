@@ -8,6 +8,7 @@
 #include <new>
 
 #include "build_kernels.cuh"
+#include "bottom_cluster.cuh"
 #include "bottom_cycle.cuh"
 #include "gs27_tiled.cuh"
 #include "launch.cuh"
@@ -417,6 +418,28 @@ BottomArgs bottom_args(pmg_problem *p, int top) {
   return a;
 }
 
+// Levels 1 .. top of the mixed V-cycle in one launch: on a cluster with
+// every array in shared memory when they fit (bottom_cluster.cuh), else in
+// one CTA out of global memory (bottom_cycle.cuh).
+int launch_bottom(pmg_problem *p, int top) {
+  const BottomArgs a = bottom_args(p, top);
+  cudaStream_t s = p->stream;
+  if (bc_fits(a)) {
+    static bool configured = false;
+    if (!configured) {
+      PMG_CUDA_TRY(cudaFuncSetAttribute(
+          bottom_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+          (int)kBcMaxSmem));
+      configured = true;
+    }
+    bottom_cluster_kernel<<<kCgCtas, kBcThreads, bc_layout(a).total, s>>>(a);
+  } else {
+    bottom_cycle_kernel<<<1, 1024, 0, s>>>(a);
+  }
+  PMG_LAUNCH_CHECK();
+  return PMG_OK;
+}
+
 // V-cycle in float on the correction equation, every level zero-started
 // (v_cycle with as_preconditioner, PBE_pmgc_class.h:1070-1114); level 1 in
 // double.
@@ -461,7 +484,8 @@ int vcycle32(pmg_problem *p, int L) {
   if (bottom_below) {
     // levels 1 .. L-1 in one CTA; it also leaves the damping of level L-1
     prof_begin(p, sl + kPhCoarse);
-    bottom_cycle_kernel<<<1, 1024, 0, s>>>(bottom_args(p, L - 1));
+    if ((rc = launch_bottom(p, L - 1)))
+      return rc;
     prof_end(p, sl + kPhCoarse);
     PMG_LAUNCH_CHECK();
   } else if ((rc = vcycle32(p, L - 1))) {
