@@ -277,11 +277,13 @@ def phase_bytes(p, level: int, phase: str, esz: int) -> float | None:
         return None
     arrays = {"pre-smooth": 2 * (7 if fine else 17),
               "post-smooth": 2 * (7 if fine else 17),
-              "defect": 7 if fine else 17, "axpy": 3}
+              "defect": 7 if fine else 17}
     if phase in arrays:
         return arrays[phase] * n3 * esz
-    if phase in ("restrict", "interp"):
+    if phase == "restrict":  # fine r; coarse 27 P + f
         return (n3 + 28 * nc3) * esz
+    if phase == "interp":  # coarse x + 27 P; fine x read and written
+        return (2 * n3 + 28 * nc3) * esz
     if phase == "damping":  # on the level below, double accumulators
         return 16 * nc3 * esz
     return None
@@ -298,8 +300,7 @@ def phase_kernel(p, level: int, phase: str):
     return {"residual": ("defect_norm_kernel", 1),
             "defect": ("defect_kernel", 1),
             "restrict": ("restrict_kernel", 1),
-            "interp": ("interp_kernel", 1),
-            "axpy": ("axpy_full_kernel", 1)}.get(phase, (None, 0))
+            "interp": ("interp_add_kernel", 1)}.get(phase, (None, 0))
 
 
 def profiled_traffic(kernel: str | None, launches: int, workload: str,

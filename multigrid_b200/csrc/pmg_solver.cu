@@ -336,14 +336,12 @@ int vcycle64(pmg_problem *p, int L, int as_preconditioner) {
   ideal_lambda_kernel<double><<<reduce_grid(c.d), interior_block(), 0, s>>>(
       c.d, c.A64(14), c.x, c.f, p->red_lambda, c.omega);
   prof_end(p, sl + kPhLambda);
+  // x += w * (interpolated correction), one pass
   prof_begin(p, sl + kPhInterp);
-  interp_kernel<double><<<interp_grid(c.d), interior_block(), 0, s>>>(
-      c.d, v.d, c.x, v.r, c.Pc());
+  interp_add_kernel<double, false>
+      <<<interp_grid(c.d), interior_block(), 0, s>>>(c.d, v.d, c.x, c.Pc(), x,
+                                                     c.omega);
   prof_end(p, sl + kPhInterp);
-  prof_begin(p, sl + kPhAxpy);
-  axpy_full_kernel<double><<<flat_grid(v.n3), 256, 0, s>>>(v.n3, x, v.r,
-                                                           c.omega);
-  prof_end(p, sl + kPhAxpy);
   PMG_LAUNCH_CHECK();
   prof_begin(p, sl + kPhPost);
   if ((rc = smooth64(p, L, 2, 0, &x)))
@@ -504,18 +502,17 @@ int vcycle32(pmg_problem *p, int L) {
         c.d, c.A32(14), c.x32, c.f32, p->red_lambda, c.omega);
   }
   prof_end(p, sl + kPhLambda);
+  // x += w * (interpolated correction), one pass
   prof_begin(p, sl + kPhInterp);
-  interp_kernel<float><<<interp_grid(c.d), interior_block(), 0, s>>>(
-      c.d, v.d, c.x32, v.r32, c.Pc32());
-  prof_end(p, sl + kPhInterp);
-  prof_begin(p, sl + kPhAxpy);
   if (kind == 7) // the finest float iterate is split
-    axpy_split_kernel<float><<<flat_grid(v.n3), 256, 0, s>>>(v.d, x, v.r32,
-                                                             c.omega);
+    interp_add_kernel<float, true>
+        <<<interp_grid(c.d), interior_block(), 0, s>>>(c.d, v.d, c.x32,
+                                                       c.Pc32(), x, c.omega);
   else
-    axpy_full_kernel<float><<<flat_grid(v.n3), 256, 0, s>>>(v.n3, x, v.r32,
-                                                            c.omega);
-  prof_end(p, sl + kPhAxpy);
+    interp_add_kernel<float, false>
+        <<<interp_grid(c.d), interior_block(), 0, s>>>(c.d, v.d, c.x32,
+                                                       c.Pc32(), x, c.omega);
+  prof_end(p, sl + kPhInterp);
   PMG_LAUNCH_CHECK();
   prof_begin(p, sl + kPhPost);
   if ((rc = smooth32(p, L, 2, 0, &x)))

@@ -254,6 +254,60 @@ __global__ void __launch_bounds__(256)
       p[26][c + 1 + cy + cz] * x111;
 }
 
+// x = x + w * (interpolation of xin), fused: interp_kernel's eight values
+// per coarse cell (same order and arithmetic), each added at once to the
+// fine iterate as axpy_full_kernel adds it (add_and_multiply_domains,
+// Domain.h:602-623), so the correction never goes through memory. The fine
+// points the interpolation does not write (the last plane, row and column
+// of the shell) keep x: there the separate update adds w * 0. With SPLIT_X
+// the fine iterate is in the colour-split row layout (split_layout.cuh).
+template <typename T, bool SPLIT_X>
+__global__ void __launch_bounds__(256)
+    interp_add_kernel(Dims dc, Dims df, const T *__restrict__ xin,
+                      P27<T> P, T *__restrict__ x,
+                      const double *__restrict__ w) {
+  const int ii = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int jj = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int kk = blockIdx.z + 1;
+  if (ii > dc.nx - 1 || jj > dc.ny - 1)
+    return;
+  const T ww = (T)(*w);
+  const int cy = dc.sy(), cz = dc.sz();
+  const int fy = df.sy(), fz = df.sz();
+  const int c = dc.at(ii, jj, kk);
+  const int f = df.at(2 * ii - 1, 2 * jj - 1, 2 * kk - 1);
+  // fine points 2ii-1 and 2ii of a row: reference layout f, f + 1; split
+  // layout (i - 1 = 2ii-2 even, 2ii-1 odd) row + ii-1 and row + hx + ii-1
+  const int e0 = SPLIT_X ? f - (2 * ii - 2) + (ii - 1) : f;
+  const int e1 = SPLIT_X ? e0 + (df.nx + 1) / 2 : f + 1;
+  const T *const *p = P.p;
+  const T x000 = xin[c], x100 = xin[c + 1], x010 = xin[c + cy],
+          x001 = xin[c + cz], x110 = xin[c + 1 + cy], x101 = xin[c + 1 + cz],
+          x011 = xin[c + cy + cz], x111 = xin[c + 1 + cy + cz];
+  const T v000 = x000;
+  const T v100 = p[3][c] * x000 + p[4][c + 1] * x100;
+  const T v010 = p[1][c] * x000 + p[2][c + cy] * x010;
+  const T v001 = p[9][c] * x000 + p[18][c + cz] * x001;
+  const T v110 = p[5][c] * x000 + p[6][c + 1] * x100 + p[7][c + cy] * x010 +
+                 p[8][c + 1 + cy] * x110;
+  const T v101 = p[12][c] * x000 + p[13][c + 1] * x100 +
+                 p[21][c + cz] * x001 + p[22][c + 1 + cz] * x101;
+  const T v011 = p[10][c] * x000 + p[11][c + cy] * x010 +
+                 p[19][c + cz] * x001 + p[20][c + cy + cz] * x011;
+  const T v111 = p[14][c] * x000 + p[15][c + 1] * x100 +
+                 p[16][c + cy] * x010 + p[17][c + 1 + cy] * x110 +
+                 p[23][c + cz] * x001 + p[24][c + 1 + cz] * x101 +
+                 p[25][c + cy + cz] * x011 + p[26][c + 1 + cy + cz] * x111;
+  x[e0] = x[e0] + ww * v000;
+  x[e1] = x[e1] + ww * v100;
+  x[e0 + fy] = x[e0 + fy] + ww * v010;
+  x[e0 + fz] = x[e0 + fz] + ww * v001;
+  x[e1 + fy] = x[e1 + fy] + ww * v110;
+  x[e1 + fz] = x[e1 + fz] + ww * v101;
+  x[e0 + fy + fz] = x[e0 + fy + fz] + ww * v011;
+  x[e1 + fy + fz] = x[e1 + fy + fz] + ww * v111;
+}
+
 // ---------------------------------------------------------------------------
 // Elementwise
 // ---------------------------------------------------------------------------
