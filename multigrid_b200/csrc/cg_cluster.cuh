@@ -24,8 +24,8 @@ namespace pmg {
 // bytes of dynamic shared memory for an nx x ny level
 inline size_t cg_cluster_smem(int nx, int ny) {
   const size_t nxy = (size_t)nx * ny;
-  return sizeof(double) *
-         ((kCgMaxPlanes + 1) * 14 * nxy + kCgMaxPlanes * nxy + 2 * kCgCtas);
+  return sizeof(double) * ((kCgMaxPlanes + 1) * 14 * nxy +
+                           kCgMaxPlanes * nxy + 2 * kCgCtas + nxy);
 }
 
 inline bool cg_cluster_fits(const Dims &d) {
@@ -78,11 +78,12 @@ __global__ void __cluster_dims__(kCgCtas, 1, 1) __launch_bounds__(kCgThreads)
   extern __shared__ __align__(16) double cg_smem[];
   const int nx = d.nx, ny = d.ny, nxy = nx * ny;
   // [plane klo-1 .. khi][slot][j][i] coefficients, then p of klo .. khi,
-  // then two reduction slots per CTA rank
+  // then two sets of reduction slots (one per CTA rank), then a zero plane
   double *sA = cg_smem;
   double *sP = sA + (kCgMaxPlanes + 1) * 14 * nxy;
   double *sRed = sP + kCgMaxPlanes * nxy;
-  __shared__ double sh[32];
+  double *zp = sRed + 2 * kCgCtas;
+  __shared__ double sh[2 * 32];
 
   const int rank = (int)cluster.block_rank();
   const int klo = cg_plane_lo(rank, d.nz);
@@ -99,6 +100,8 @@ __global__ void __cluster_dims__(kCgCtas, 1, 1) __launch_bounds__(kCgThreads)
   }
   for (int q = threadIdx.x; q < kCgMaxPlanes * nxy; q += blockDim.x)
     sP[q] = 0.0; // shells of p stay zero
+  for (int q = threadIdx.x; q < nxy; q += blockDim.x)
+    zp[q] = 0.0;
 
   // this thread's point
   const int t = threadIdx.x;
@@ -112,42 +115,61 @@ __global__ void __cluster_dims__(kCgCtas, 1, 1) __launch_bounds__(kCgThreads)
   }
   const int gi = d.at(i, j, k);
   const int sl = (k - klo) * nxy + (j - 1) * nx + (i - 1); // in sP
-  // the CTAs holding the planes below and above this point's plane (when
-  // those are interior planes of another CTA)
-  const int rk_dn = cg_plane_owner(k - 1, d.nz);
-  const int rk_up = cg_plane_owner(k + 1, d.nz);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nw = blockDim.x >> 5;
 
   auto coef = [&](int slot, int di, int dj, int dk) -> double {
     const int lk = k + dk - (klo - 1);
     return sA[(lk * 14 + slot) * nxy + (j - 1 + dj) * nx + (i - 1 + di)];
   };
-  // p at an offset: own planes from this CTA, the planes next to them from
-  // the CTA holding them, shell planes zero
-  auto pval = [&](int di, int dj, int dk) -> double {
-    const int kk = k + dk;
-    const int o = (j - 1 + dj) * nx + (i - 1 + di);
-    if (kk >= klo && kk <= khi)
-      return sP[(kk - klo) * nxy + o];
+  // plane kk of p: this CTA's planes, the planes next to them from the CTA
+  // holding them (distributed shared memory), shell planes zero
+  auto p_plane = [&](int kk) -> const double * {
     if (kk < 2 || kk > d.nz - 1)
-      return 0.0;
-    const int r = kk < klo ? rk_dn : rk_up;
-    const int rlo = cg_plane_lo(r, d.nz);
-    const double *remote = cluster.map_shared_rank(sP, r);
-    return remote[(kk - rlo) * nxy + o];
+      return zp;
+    if (kk >= klo && kk <= khi)
+      return sP + (kk - klo) * nxy;
+    const int r = cg_plane_owner(kk, d.nz);
+    return cluster.map_shared_rank(sP, r) + (kk - cg_plane_lo(r, d.nz)) * nxy;
+  };
+  const double *p_c = sP + (k - klo) * nxy;
+  const double *p_dn = p_plane(k - 1), *p_up = p_plane(k + 1);
+  const int po = (j - 1) * nx + (i - 1);
+  auto pval = [&](int di, int dj, int dk) -> double {
+    const double *pl = dk == 0 ? p_c : dk < 0 ? p_dn : p_up;
+    return pl[po + dj * nx + di];
   };
   auto xval = [&](int di, int dj, int dk) -> double {
     return x[gi + di + dj * nx + dk * nxy];
   };
-  // cluster-wide sum in rank order (identical bits in every CTA)
+  // Cluster-wide sum in rank order, the same bits in every CTA: warp sums,
+  // the CTA's warp sums added by warp 0 (fixed shuffle tree) and pushed
+  // into slot `rank` of every CTA; after the barrier each thread adds its
+  // own CTA's kCgCtas slots in rank order. The two slot sets (and the two
+  // halves of sh) alternate; a set is written again only after two more
+  // cluster barriers, which every reader of its previous contents passed.
   auto cluster_sum = [&](double v, int slot) -> double {
-    const double b = cg_block_sum(v, sh);
-    if (threadIdx.x == 0)
-      sRed[slot * kCgCtas + 0] = b;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+      v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0)
+      sh[slot * 32 + warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+      double b = lane < nw ? sh[slot * 32 + lane] : 0.0;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1)
+        b += __shfl_down_sync(0xffffffffu, b, o);
+      b = __shfl_sync(0xffffffffu, b, 0);
+      // every lane stores (lanes 8 apart write the same value)
+      cluster.map_shared_rank(sRed, lane % kCgCtas)[slot * kCgCtas + rank] =
+          b;
+    }
     cluster.sync();
     double s = 0.0;
+#pragma unroll
     for (int r = 0; r < kCgCtas; ++r)
-      s += cluster.map_shared_rank(sRed, r)[slot * kCgCtas];
-    __syncthreads(); // sh is reused by the next block sum
+      s += sRed[slot * kCgCtas + r];
     return s;
   };
 
