@@ -600,6 +600,11 @@ def main():
         p.buildmultilevelops()
         return p.solve(TOL, MAX_CYCLES)
 
+    if args.quick:
+        # profiler runs: launches are serialised and replayed there, so the
+        # smoother's tile timings would mean nothing; use the size rule
+        from multigrid_b200 import _lib
+        _lib.check("pmg_set_autotune", _lib.lib.pmg_set_autotune(0))
     results = {}
     precisions = [args.precision]
     if not args.quick:

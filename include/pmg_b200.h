@@ -413,6 +413,17 @@ int pmg_problem_set_coarse_rtol(pmg_problem *p, double rtol);
  * No reference counterpart. */
 int pmg_problem_set_host_loop(pmg_problem *p, int on);
 
+/* Tile edge of the 27-point smoother, for the whole process. mode 1 (the
+ * default): pmg_build_hierarchy times the edges 8, 16 and 32 on each level
+ * size the first time it meets it and keeps the fastest (the size rule's
+ * edge unless another is more than 10% faster); mode 0: the size rule (32
+ * from 97 points per axis, 16 from 49, else 8); mode 8, 16 or 32: that
+ * edge everywhere. Every edge gives the same results. Use mode 0 under
+ * kernel profilers, which serialise and replay launches so that timings
+ * taken there mean nothing. Other modes: PMG_ERR_ARG. No reference
+ * counterpart. */
+int pmg_set_autotune(int mode);
+
 /* Phase timing: with on != 0, pmg_solve records CUDA events around every
  * phase of every cycle (inside the captured cycle graph) and accumulates the
  * elapsed times. */

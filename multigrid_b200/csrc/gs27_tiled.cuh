@@ -195,6 +195,11 @@ void launch_gs27_phase(const Dims &d, const Op14<T> &A, const T *cc,
 // one for this grid and element size (gs27_tune), else by size. Every tile
 // gives bit-identical results; only the speed differs.
 int gs27_tile_for(const Dims &d, int esize);
+// the edge used when nothing was measured: 32 from 97 points per axis, 16
+// from 49, else 8
+int gs27_tile_by_size(const Dims &d);
+// whether pmg_build_hierarchy measures tile edges (pmg_set_autotune mode 1)
+bool gs27_autotune_on();
 
 // nsweeps eight-colour sweeps starting from x in `cur`, ping-ponging with
 // `alt` (whose shell must equal cur's). Returns the buffer holding the
@@ -239,7 +244,8 @@ int launch_gs27_pp(const Dims &d, const Op14<T> &A, const T *cc, const T *fc,
 }
 
 // Measures every tile edge on a level (two sweeps each, CUDA events, best of
-// three) and records the fastest for gs27_tile_for. x and alt are scratch
+// three) and records the fastest for gs27_tile_for; the size rule's edge
+// is kept unless another is more than 10% faster. x and alt are scratch
 // iterates of the level (same shell); synchronises the stream.
 template <typename T>
 int gs27_tune(const Dims &d, const Op14<T> &A, const T *fc, T *x, T *alt,

@@ -78,6 +78,8 @@ cudaError_t scratch_free(void *ptr, cudaStream_t s) {
 namespace {
 std::mutex g_tile_mutex;
 std::map<std::pair<long, int>, int> g_tiles; // (nx*ny*nz key, esize) -> edge
+// 1: measured edges (default); 0: size rule; 8, 16, 32: that edge
+int g_tile_mode = 1; // guarded by g_tile_mutex
 long tile_key(const Dims &d) {
   return ((long)d.nx * 2048 + d.ny) * 2048 + d.nz;
 }
@@ -86,13 +88,24 @@ long tile_key(const Dims &d) {
 int gs27_tile_for(const Dims &d, int esize) {
   {
     std::lock_guard<std::mutex> lk(g_tile_mutex);
+    if (g_tile_mode != 1)
+      return g_tile_mode ? g_tile_mode : gs27_tile_by_size(d);
     auto it = g_tiles.find({tile_key(d), esize});
     if (it != g_tiles.end())
       return it->second;
   }
-  // untuned: enough CTAs for small levels, fewer halo points for large ones
+  return gs27_tile_by_size(d);
+}
+
+// untuned: enough CTAs for small levels, fewer halo points for large ones
+int gs27_tile_by_size(const Dims &d) {
   const int n = d.nx < d.ny ? d.nx : d.ny;
   return n >= 97 ? 32 : n >= 49 ? 16 : 8;
+}
+
+bool gs27_autotune_on() {
+  std::lock_guard<std::mutex> lk(g_tile_mutex);
+  return g_tile_mode == 1;
 }
 
 void gs27_tile_record(const Dims &d, int esize, int tile) {
@@ -112,7 +125,7 @@ int gs27_tune(const Dims &d, const Op14<T> &A, const T *fc, T *x, T *alt,
   PMG_CUDA_TRY(cudaEventCreate(&e0));
   cudaError_t e = cudaEventCreate(&e1);
   int best = 0;
-  float best_ms = 0.f;
+  float best_ms = 0.f, size_ms = 0.f;
   for (int tile : kGs27Tiles) {
     if (e != cudaSuccess)
       break;
@@ -138,7 +151,13 @@ int gs27_tune(const Dims &d, const Op14<T> &A, const T *fc, T *x, T *alt,
       best = tile;
       best_ms = ms_min;
     }
+    if (tile == gs27_tile_by_size(d))
+      size_ms = ms_min;
   }
+  // the size rule's edge stays unless another is clearly faster (timings
+  // taken while other work shares the GPU are noisy)
+  if (best != gs27_tile_by_size(d) && !(best_ms < 0.9f * size_ms))
+    best = gs27_tile_by_size(d);
   cudaEventDestroy(e0);
   if (e1)
     cudaEventDestroy(e1);
@@ -431,6 +450,16 @@ static int gs27_inplace(const Dims &d, const Op14<T> &A, const T *cc,
 // C ABI
 // ---------------------------------------------------------------------------
 extern "C" {
+
+int pmg_set_autotune(int mode) {
+  if (mode != 0 && mode != 1 && mode != 8 && mode != 16 && mode != 32) {
+    set_last_message("pmg_set_autotune: mode must be 0, 1, 8, 16 or 32");
+    return PMG_ERR_ARG;
+  }
+  std::lock_guard<std::mutex> lk(g_tile_mutex);
+  g_tile_mode = mode;
+  return PMG_OK;
+}
 
 const char *pmg_last_error(void) { return g_last_error; }
 const char *pmg_version(void) { return "pmg_b200 0.1 (sm_100a)"; }

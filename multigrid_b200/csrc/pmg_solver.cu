@@ -1214,14 +1214,14 @@ int pmg_build_hierarchy(pmg_problem *p, int trilinear) {
     LevelBuf &v = p->lv[L];
     const size_t n3 = (size_t)v.n3;
     if (p->precision == PMG_PREC_MIXED) {
-      if (L <= p->bottom_top || gs27_tile_known(v.d, 4))
+      if (L <= p->bottom_top || gs27_tile_known(v.d, 4) || !gs27_autotune_on())
         continue;
       if ((rc = gs27_tune<float>(v.d, v.A32(14), v.f32, v.x32, v.xalt32, s)))
         return rc;
       PMG_CUDA_TRY(cudaMemsetAsync(v.x32, 0, sizeof(float) * n3, s));
       PMG_CUDA_TRY(cudaMemsetAsync(v.xalt32, 0, sizeof(float) * n3, s));
     } else {
-      if (gs27_tile_known(v.d, 8))
+      if (gs27_tile_known(v.d, 8) || !gs27_autotune_on())
         continue;
       if ((rc = gs27_tune<double>(v.d, v.A64(14), v.f, v.x, v.xalt, s)))
         return rc;

@@ -266,3 +266,28 @@ def test_host_loop_switch_gives_the_same_solve(golden_problem):
             out.append((r.cycles, p.potential().ravel().copy()))
     assert out[0][0] == out[1][0]
     assert np.array_equal(out[0][1], out[1][1])
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_smoother_tile_edges_give_the_same_solve(pb65, precision):
+    """pmg_set_autotune: the 27-point smoother's tile edge (fixed 8, 16 or
+    32, the size rule, or measured) changes speed only: every choice gives
+    the same cycles and the same potential, bit for bit."""
+    from multigrid_b200 import _lib
+    w, fine = pb65
+    out = []
+    try:
+        for mode in (8, 16, 32, 0, 1):
+            _lib.check("pmg_set_autotune", _lib.lib.pmg_set_autotune(mode))
+            with PBELinearProblem(w.base, w.nlev, w.box, precision,
+                                  w.physics) as p:
+                p.set_fine(**fine)
+                p.buildmultilevelops()
+                r = p.solve(tol=1e-10, max_cycles=100)
+                out.append((r.cycles, p.potential().ravel().copy()))
+        assert _lib.lib.pmg_set_autotune(5) == _lib.PMG_ERR_ARG
+    finally:
+        _lib.lib.pmg_set_autotune(1)
+    for cyc, x in out[1:]:
+        assert cyc == out[0][0]
+        assert np.array_equal(x, out[0][1])
