@@ -413,6 +413,15 @@ int pmg_problem_set_coarse_rtol(pmg_problem *p, double rtol);
  * No reference counterpart. */
 int pmg_problem_set_host_loop(pmg_problem *p, int on);
 
+/* on != 0: choose kernels for many solves sharing the GPU rather than for
+ * the latency of this one: the mixed path's lowest levels run in one CTA
+ * instead of an 8-CTA cluster with its arrays in shared memory (a cluster
+ * starts only when eight SMs of one GPC are idle at once). Same arithmetic
+ * per point; the mixed results may differ in the last bits (sums in another
+ * order). The serving runtime sets it on the problems it creates. Default
+ * off. No reference counterpart. */
+int pmg_problem_set_throughput_mode(pmg_problem *p, int on);
+
 /* Tile edge of the 27-point smoother, for the whole process. mode 1 (the
  * default): pmg_build_hierarchy times the edges 8, 16 and 32 on each level
  * size the first time it meets it and keeps the fastest (the size rule's

@@ -212,10 +212,14 @@ int acquire(pmg_server *s, const pmg_request &r, Slot *slot) {
   if (s->held + need > s->budget)
     return PMG_ERR_BUDGET;
   pmg_problem *p = nullptr;
-  const int rc =
-      pmg_problem_create(r.base, r.nlev, r.box, r.precision, nullptr, &p);
+  int rc = pmg_problem_create(r.base, r.nlev, r.box, r.precision, nullptr, &p);
   if (rc != PMG_OK)
     return rc;
+  // many solves share the GPU here: kernels that do not wait for whole SMs
+  if ((rc = pmg_problem_set_throughput_mode(p, 1)) != PMG_OK) {
+    pmg_problem_destroy(p);
+    return rc;
+  }
   slot->prob = p;
   slot->base = r.base;
   slot->nlev = r.nlev;

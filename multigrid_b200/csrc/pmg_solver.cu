@@ -130,6 +130,7 @@ struct pmg_problem {
   cudaEvent_t done_ev = nullptr;
   bool solve_pending = false;
   bool host_loop = false; // pmg_problem_set_host_loop
+  bool throughput = false; // pmg_problem_set_throughput_mode
   // MG-preconditioned CG on the finest level (allocated on first use):
   // right-hand side, iterate, residual, preconditioned residual, search
   // direction, A times it; three reduction slots; the iteration state.
@@ -417,12 +418,15 @@ BottomArgs bottom_args(pmg_problem *p, int top) {
 }
 
 // Levels 1 .. top of the mixed V-cycle in one launch: on a cluster with
-// every array in shared memory when they fit (bottom_cluster.cuh), else in
-// one CTA out of global memory (bottom_cycle.cuh).
+// every array in shared memory when they fit (bottom_cluster.cuh), else, or
+// in throughput mode, in one CTA out of global memory (bottom_cycle.cuh).
+// The cluster is faster for a solve alone, but it can start only when eight
+// SMs of one GPC are idle at once, which many concurrent solves rarely
+// leave (measured: serving saturation 111 against 133 solves/s).
 int launch_bottom(pmg_problem *p, int top) {
   const BottomArgs a = bottom_args(p, top);
   cudaStream_t s = p->stream;
-  if (bc_fits(a)) {
+  if (!p->throughput && bc_fits(a)) {
     static bool configured = false;
     if (!configured) {
       PMG_CUDA_TRY(cudaFuncSetAttribute(
@@ -1079,6 +1083,15 @@ int pmg_problem_set_host_loop(pmg_problem *p, int on) {
   if (!p)
     return PMG_ERR_ARG;
   p->host_loop = on != 0;
+  return PMG_OK;
+}
+
+int pmg_problem_set_throughput_mode(pmg_problem *p, int on) {
+  if (!p)
+    return PMG_ERR_ARG;
+  if ((bool)on != p->throughput)
+    drop_graphs(p); // the captured cycles bake the kernel choice in
+  p->throughput = on != 0;
   return PMG_OK;
 }
 

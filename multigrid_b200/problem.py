@@ -210,6 +210,13 @@ class PBELinearProblem:
         _lib.check("pmg_problem_set_host_loop",
                    _lib.lib.pmg_problem_set_host_loop(self._h, int(on)))
 
+    def set_throughput_mode(self, on: bool = True) -> None:
+        """Choose kernels for many solves sharing the GPU (the serving
+        runtime's setting) rather than for this solve's latency; mixed
+        results may differ from the default mode in the last bits."""
+        _lib.check("pmg_problem_set_throughput_mode",
+                   _lib.lib.pmg_problem_set_throughput_mode(self._h, int(on)))
+
     def set_profiling(self, on: bool = True) -> None:
         """Time every cycle phase with CUDA events inside the cycle graph."""
         _lib.check("pmg_problem_set_profiling",

@@ -2,8 +2,8 @@
 
 The contract: a request's result does not depend on what else is in flight.
 Every solve here is compared bit for bit (potential and cycle count) with
-the same solve run alone through the problem handle; admission never holds
-more device memory than the budget.
+the same solve run alone through the problem handle in the server's
+throughput mode; admission never holds more device memory than the budget.
 """
 import numpy as np
 import pytest
@@ -42,6 +42,7 @@ def cases(golden_kernels):
 
 def solve_alone(base, nlev, box, fine, prec):
     with PBELinearProblem(base, nlev, box, prec) as p:
+        p.set_throughput_mode(True)  # the server's kernel choice
         p.set_fine(**fine)
         p.buildmultilevelops()
         r = p.solve(tol=1e-10, max_cycles=100)
@@ -149,6 +150,7 @@ def test_requests_from_atoms_match_problem_handle():
     want = {}
     for prec in ("fp64", "mixed"):
         with PBELinearProblem(w.base, w.nlev, w.box, prec, w.physics) as p:
+            p.set_throughput_mode(True)  # the server's kernel choice
             p.set_atoms(atoms)
             p.buildmultilevelops()
             r = p.solve(tol=1e-10, max_cycles=100)

@@ -291,3 +291,25 @@ def test_smoother_tile_edges_give_the_same_solve(pb65, precision):
     for cyc, x in out[1:]:
         assert cyc == out[0][0]
         assert np.array_equal(x, out[0][1])
+
+
+def test_throughput_mode_same_solve_within_tolerance(pb65):
+    """pmg_problem_set_throughput_mode: the mixed path's lowest levels in
+    one CTA instead of the cluster: the same cycle count and a potential
+    equal to rounding (sums in another order); FP64 is untouched."""
+    w, fine = pb65
+    out = {}
+    for prec in ("mixed", "fp64"):
+        for mode in (False, True):
+            with PBELinearProblem(w.base, w.nlev, w.box, prec,
+                                  w.physics) as p:
+                p.set_throughput_mode(mode)
+                p.set_fine(**fine)
+                p.buildmultilevelops()
+                r = p.solve(tol=1e-10, max_cycles=100)
+                out[prec, mode] = (r.cycles, p.potential().ravel().copy())
+    assert np.array_equal(out["fp64", False][1], out["fp64", True][1])
+    c0, x0 = out["mixed", False]
+    c1, x1 = out["mixed", True]
+    assert abs(c0 - c1) <= 1
+    assert np.linalg.norm(x1 - x0) <= 1e-9 * np.linalg.norm(x0)
