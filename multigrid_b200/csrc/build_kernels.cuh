@@ -24,7 +24,8 @@ namespace pmg {
 // f to (i,j,k) is read as uS(i+1,j+1,k).
 template <int KIND>
 __global__ void __launch_bounds__(128)
-    buildP_op_kernel(Dims df, Dims dc, Op14<double> A, P27W<double> P) {
+    buildP_op_kernel(Dims df, Dims dc, Op14<double> A, P27W<double> P,
+                     P27W<float> P32) {
   const int ii = blockIdx.x * blockDim.x + threadIdx.x + 2;
   const int jj = blockIdx.y * blockDim.y + threadIdx.y + 2;
   const int kk = blockIdx.z + 2;
@@ -86,6 +87,10 @@ __global__ void __launch_bounds__(128)
 #pragma unroll
   for (int s = 0; s < 27; ++s)
     P.p[s][pc] = w[s];
+  if (P32.p[0]) // the mixed path's float copy
+#pragma unroll
+    for (int s = 0; s < 27; ++s)
+      P32.p[s][pc] = (float)w[s];
 }
 
 // Constant weights 1, 1/2, 1/4, 1/8 (VbuildPb_trilin, pmgc/buildPd.cc:
@@ -153,10 +158,11 @@ __device__ __forceinline__ double galerkin_entry(const Dims &df,
   return S == 0 ? acc : -acc;
 }
 
+// out32 (all null: none) receives the float copy of each entry.
 template <int KIND>
 __global__ void __launch_bounds__(128)
     buildG_kernel(Dims df, Dims dc, P27<double> P, Op14<double> A,
-                  Op14W<double> out) {
+                  Op14W<double> out, Op14W<float> out32) {
   const int ii = blockIdx.x * blockDim.x + threadIdx.x + 2;
   const int jj = blockIdx.y * blockDim.y + threadIdx.y + 2;
   const int kk = blockIdx.z + 2;
@@ -164,20 +170,64 @@ __global__ void __launch_bounds__(128)
     return;
   const int pc = dc.at(ii, jj, kk);
   const int c0 = df.at(2 * ii - 1, 2 * jj - 1, 2 * kk - 1);
-  out.a[0][pc] = galerkin_entry<KIND, 0>(df, dc, P, A, pc, c0);
-  out.a[1][pc] = galerkin_entry<KIND, 1>(df, dc, P, A, pc, c0);
-  out.a[2][pc] = galerkin_entry<KIND, 2>(df, dc, P, A, pc, c0);
-  out.a[3][pc] = galerkin_entry<KIND, 3>(df, dc, P, A, pc, c0);
-  out.a[4][pc] = galerkin_entry<KIND, 4>(df, dc, P, A, pc, c0);
-  out.a[5][pc] = galerkin_entry<KIND, 5>(df, dc, P, A, pc, c0);
-  out.a[6][pc] = galerkin_entry<KIND, 6>(df, dc, P, A, pc, c0);
-  out.a[7][pc] = galerkin_entry<KIND, 7>(df, dc, P, A, pc, c0);
-  out.a[8][pc] = galerkin_entry<KIND, 8>(df, dc, P, A, pc, c0);
-  out.a[9][pc] = galerkin_entry<KIND, 9>(df, dc, P, A, pc, c0);
-  out.a[10][pc] = galerkin_entry<KIND, 10>(df, dc, P, A, pc, c0);
-  out.a[11][pc] = galerkin_entry<KIND, 11>(df, dc, P, A, pc, c0);
-  out.a[12][pc] = galerkin_entry<KIND, 12>(df, dc, P, A, pc, c0);
-  out.a[13][pc] = galerkin_entry<KIND, 13>(df, dc, P, A, pc, c0);
+  const bool f32 = out32.a[0] != nullptr; // the mixed path's float copy
+  double v;
+  v = galerkin_entry<KIND, 0>(df, dc, P, A, pc, c0);
+  out.a[0][pc] = v;
+  if (f32)
+    out32.a[0][pc] = (float)v;
+  v = galerkin_entry<KIND, 1>(df, dc, P, A, pc, c0);
+  out.a[1][pc] = v;
+  if (f32)
+    out32.a[1][pc] = (float)v;
+  v = galerkin_entry<KIND, 2>(df, dc, P, A, pc, c0);
+  out.a[2][pc] = v;
+  if (f32)
+    out32.a[2][pc] = (float)v;
+  v = galerkin_entry<KIND, 3>(df, dc, P, A, pc, c0);
+  out.a[3][pc] = v;
+  if (f32)
+    out32.a[3][pc] = (float)v;
+  v = galerkin_entry<KIND, 4>(df, dc, P, A, pc, c0);
+  out.a[4][pc] = v;
+  if (f32)
+    out32.a[4][pc] = (float)v;
+  v = galerkin_entry<KIND, 5>(df, dc, P, A, pc, c0);
+  out.a[5][pc] = v;
+  if (f32)
+    out32.a[5][pc] = (float)v;
+  v = galerkin_entry<KIND, 6>(df, dc, P, A, pc, c0);
+  out.a[6][pc] = v;
+  if (f32)
+    out32.a[6][pc] = (float)v;
+  v = galerkin_entry<KIND, 7>(df, dc, P, A, pc, c0);
+  out.a[7][pc] = v;
+  if (f32)
+    out32.a[7][pc] = (float)v;
+  v = galerkin_entry<KIND, 8>(df, dc, P, A, pc, c0);
+  out.a[8][pc] = v;
+  if (f32)
+    out32.a[8][pc] = (float)v;
+  v = galerkin_entry<KIND, 9>(df, dc, P, A, pc, c0);
+  out.a[9][pc] = v;
+  if (f32)
+    out32.a[9][pc] = (float)v;
+  v = galerkin_entry<KIND, 10>(df, dc, P, A, pc, c0);
+  out.a[10][pc] = v;
+  if (f32)
+    out32.a[10][pc] = (float)v;
+  v = galerkin_entry<KIND, 11>(df, dc, P, A, pc, c0);
+  out.a[11][pc] = v;
+  if (f32)
+    out32.a[11][pc] = (float)v;
+  v = galerkin_entry<KIND, 12>(df, dc, P, A, pc, c0);
+  out.a[12][pc] = v;
+  if (f32)
+    out32.a[12][pc] = (float)v;
+  v = galerkin_entry<KIND, 13>(df, dc, P, A, pc, c0);
+  out.a[13][pc] = v;
+  if (f32)
+    out32.a[13][pc] = (float)v;
 }
 
 } // namespace pmg

@@ -1174,6 +1174,7 @@ int pmg_build_hierarchy(pmg_problem *p, int trilinear) {
     return PMG_ERR_STATE;
   }
   cudaStream_t s = p->stream;
+  const bool mixed = p->precision == PMG_PREC_MIXED;
   int rc;
   for (int L = p->nlev; L >= 2; --L) {
     LevelBuf &f = p->lv[L], &c = p->lv[L - 1];
@@ -1181,12 +1182,22 @@ int pmg_build_hierarchy(pmg_problem *p, int trilinear) {
     P27W<double> Pw;
     for (int q = 0; q < 27; ++q)
       Pw.p[q] = c.P[q];
+    // the mixed path's float copies are written by the builders (interior
+    // entries; the shells stay zero from the arena's clearing)
+    P27W<float> P32w{};
+    Op14W<float> out32{};
+    if (mixed) {
+      for (int q = 0; q < 27; ++q)
+        P32w.p[q] = c.P32[q];
+      for (int q = 0; q < 14; ++q)
+        out32.a[q] = c.op32[q]; // null on level 1
+    }
     if (trilinear) {
       buildP_trilin_kernel<<<interior_grid(c.d), interior_block(), 0, s>>>(
           c.d, Pw);
       PMG_LAUNCH_CHECK();
     } else if ((rc = launch_buildP(f.d, c.d, kind, f.A64(kind == 7 ? 4 : 14),
-                                   Pw, s))) {
+                                   Pw, s, P32w))) {
       return rc;
     }
     p->launches += 2; // prolongation + Galerkin operator
@@ -1194,30 +1205,27 @@ int pmg_build_hierarchy(pmg_problem *p, int trilinear) {
     for (int q = 0; q < 14; ++q)
       out.a[q] = c.op[q];
     if ((rc = launch_buildG(f.d, c.d, kind, c.Pc(),
-                            f.A64(kind == 7 ? 4 : 14), out, s)))
+                            f.A64(kind == 7 ? 4 : 14), out, s, out32)))
       return rc;
   }
-  if (p->precision == PMG_PREC_MIXED) {
-    for (int L = 1; L <= p->nlev; ++L) {
-      LevelBuf &v = p->lv[L];
-      const unsigned g = flat_grid(v.n3);
-      for (int q = 0; q < 14; ++q)
-        if (v.op32[q]) {
-          if (L == p->nlev) // the finest float operator is split
-            to_split_kernel<double, float><<<g, 256, 0, s>>>(v.d, v.op[q],
-                                                             v.op32[q]);
-          else
-            convert_kernel<double, float><<<g, 256, 0, s>>>(v.n3, v.op[q],
-                                                           v.op32[q]);
+  if (mixed) {
+    LevelBuf &v = p->lv[p->nlev];
+    const unsigned g = flat_grid(v.n3);
+    for (int q = 0; q < 14; ++q)
+      if (v.op32[q]) { // the finest float operator is split
+        to_split_kernel<double, float><<<g, 256, 0, s>>>(v.d, v.op[q],
+                                                         v.op32[q]);
+        ++p->launches;
+      }
+    if (trilinear) // the trilinear builder writes double only
+      for (int L = 1; L < p->nlev; ++L) {
+        LevelBuf &c = p->lv[L];
+        for (int q = 0; q < 27; ++q) {
+          convert_kernel<double, float><<<flat_grid(c.n3), 256, 0, s>>>(
+              c.n3, c.P[q], c.P32[q]);
           ++p->launches;
         }
-      for (int q = 0; q < 27; ++q)
-        if (v.P32[q]) {
-          convert_kernel<double, float><<<g, 256, 0, s>>>(v.n3, v.P[q],
-                                                         v.P32[q]);
-          ++p->launches;
-        }
-    }
+      }
     PMG_LAUNCH_CHECK();
   }
   // tile edge of the 27-point smoother, measured once per grid size (every
