@@ -230,4 +230,42 @@ __global__ void __launch_bounds__(128)
     out32.a[13][pc] = (float)v;
 }
 
+// One Galerkin entry per thread (blockIdx.y: the output slot), for the
+// 27-point input, whose fourteen entries in one thread spill: a block
+// evaluates one entry's unrolled sum for 128 coarse points.
+template <int KIND>
+__global__ void __launch_bounds__(128)
+    buildG_entry_kernel(Dims df, Dims dc, P27<double> P, Op14<double> A,
+                        Op14W<double> out, Op14W<float> out32) {
+  const int mx = dc.nx - 2, my = dc.ny - 2;
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= mx * my * (dc.nz - 2))
+    return;
+  const int r = q / mx, kq = r / my;
+  const int ii = q - r * mx + 2, jj = r - kq * my + 2, kk = kq + 2;
+  const int pc = dc.at(ii, jj, kk);
+  const int c0 = df.at(2 * ii - 1, 2 * jj - 1, 2 * kk - 1);
+  const int S = blockIdx.y;
+  double v;
+  switch (S) {
+  case 0: v = galerkin_entry<KIND, 0>(df, dc, P, A, pc, c0); break;
+  case 1: v = galerkin_entry<KIND, 1>(df, dc, P, A, pc, c0); break;
+  case 2: v = galerkin_entry<KIND, 2>(df, dc, P, A, pc, c0); break;
+  case 3: v = galerkin_entry<KIND, 3>(df, dc, P, A, pc, c0); break;
+  case 4: v = galerkin_entry<KIND, 4>(df, dc, P, A, pc, c0); break;
+  case 5: v = galerkin_entry<KIND, 5>(df, dc, P, A, pc, c0); break;
+  case 6: v = galerkin_entry<KIND, 6>(df, dc, P, A, pc, c0); break;
+  case 7: v = galerkin_entry<KIND, 7>(df, dc, P, A, pc, c0); break;
+  case 8: v = galerkin_entry<KIND, 8>(df, dc, P, A, pc, c0); break;
+  case 9: v = galerkin_entry<KIND, 9>(df, dc, P, A, pc, c0); break;
+  case 10: v = galerkin_entry<KIND, 10>(df, dc, P, A, pc, c0); break;
+  case 11: v = galerkin_entry<KIND, 11>(df, dc, P, A, pc, c0); break;
+  case 12: v = galerkin_entry<KIND, 12>(df, dc, P, A, pc, c0); break;
+  default: v = galerkin_entry<KIND, 13>(df, dc, P, A, pc, c0); break;
+  }
+  out.a[S][pc] = v;
+  if (out32.a[0])
+    out32.a[S][pc] = (float)v;
+}
+
 } // namespace pmg

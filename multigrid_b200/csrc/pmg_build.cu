@@ -26,10 +26,13 @@ int launch_buildG(const Dims &df, const Dims &dc, int kind,
   const dim3 block(32, 4, 1);
   const dim3 grid(cdiv(dc.nx - 2, 32), cdiv(dc.ny - 2, 4),
                   (unsigned)(dc.nz - 2));
-  if (kind == 7)
+  if (kind == 7) {
     buildG_kernel<7><<<grid, block, 0, s>>>(df, dc, P, A, out, out32);
-  else
-    buildG_kernel<27><<<grid, block, 0, s>>>(df, dc, P, A, out, out32);
+  } else {
+    const long m = (long)(dc.nx - 2) * (dc.ny - 2) * (dc.nz - 2);
+    buildG_entry_kernel<27><<<dim3((unsigned)((m + 127) / 128), 14), 128, 0,
+                              s>>>(df, dc, P, A, out, out32);
+  }
   PMG_LAUNCH_CHECK();
   return PMG_OK;
 }
