@@ -19,6 +19,17 @@ inline dim3 interior_grid(const Dims &d) {
 inline dim3 reduce_grid(const Dims &d) {
   return dim3(cdiv(d.nx - 2, 32), cdiv(d.ny - 2, 8), cdiv(d.nz - 2, 8));
 }
+// The damping reduction on coarse levels: fewer planes per block on smaller
+// levels, so that they still launch enough blocks (33^3 with 8 planes per
+// block is 16 blocks).
+inline int lambda_planes(const Dims &d) {
+  const int n = d.nx < d.ny ? d.nx : d.ny;
+  return n >= 97 ? 4 : n >= 49 ? 2 : 1;
+}
+inline dim3 lambda_grid(const Dims &d) {
+  return dim3(cdiv(d.nx - 2, 32), cdiv(d.ny - 2, 8),
+              cdiv(d.nz - 2, lambda_planes(d)));
+}
 // Interpolation: one thread per coarse cell (ii,jj,kk) in [1, n_c-1]^3.
 inline dim3 interp_grid(const Dims &dc) {
   return dim3(cdiv(dc.nx - 1, 32), cdiv(dc.ny - 1, 8), (unsigned)(dc.nz - 1));

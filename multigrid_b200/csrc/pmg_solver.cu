@@ -5,6 +5,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <algorithm>
 #include <new>
 
 #include "build_kernels.cuh"
@@ -201,11 +202,16 @@ void plan(pmg_problem *p, Arena &a) {
   p->cg_ap = a.take<double>(n1);
   p->cg_status = a.take<int>(2);
   p->d_state = a.take<SolveState>(1);
+  // partials of the largest launch using each slot: the finest level's
+  // reductions, and the damping on any coarse level
+  const dim3 gf = reduce_grid(p->lv[p->nlev].d);
+  long blocks = (long)gf.x * gf.y * gf.z;
+  for (int L = 1; L < p->nlev; ++L) {
+    const dim3 g = lambda_grid(p->lv[L].d);
+    blocks = std::max(blocks, (long)g.x * g.y * g.z);
+  }
   for (ReduceSlot *s : {&p->red_norm, &p->red_lambda}) {
-    // partials of the largest interior launch
-    const Dims &df = p->lv[p->nlev].d;
-    const dim3 g = reduce_grid(df);
-    s->partials = a.take<double>(2L * g.x * g.y * g.z);
+    s->partials = a.take<double>(2L * blocks);
     s->ticket = a.take<unsigned int>(1);
     s->result = a.take<double>(2);
   }
@@ -334,8 +340,9 @@ int vcycle64(pmg_problem *p, int L, int as_preconditioner) {
   if ((rc = vcycle64(p, L - 1, 0)))
     return rc;
   prof_begin(p, sl + kPhLambda);
-  ideal_lambda_kernel<double><<<reduce_grid(c.d), interior_block(), 0, s>>>(
-      c.d, c.A64(14), c.x, c.f, p->red_lambda, c.omega);
+  ideal_lambda_kernel<double><<<lambda_grid(c.d), interior_block(), 0, s>>>(
+      c.d, c.A64(14), c.x, c.f, p->red_lambda, c.omega,
+      lambda_planes(c.d));
   prof_end(p, sl + kPhLambda);
   // x += w * (interpolated correction), one pass
   prof_begin(p, sl + kPhInterp);
@@ -497,13 +504,15 @@ int vcycle32(pmg_problem *p, int L) {
   if (bottom_below) {
     // damping computed by the bottom kernel
   } else if (L - 1 == 1) {
-    ideal_lambda_kernel<double><<<reduce_grid(c.d), interior_block(), 0, s>>>(
-        c.d, c.A64(14), c.x, c.f, p->red_lambda, c.omega);
+    ideal_lambda_kernel<double><<<lambda_grid(c.d), interior_block(), 0, s>>>(
+        c.d, c.A64(14), c.x, c.f, p->red_lambda, c.omega,
+        lambda_planes(c.d));
     convert_kernel<double, float><<<flat_grid(c.n3), 256, 0, s>>>(c.n3, c.x,
                                                                  c.x32);
   } else {
-    ideal_lambda_kernel<float><<<reduce_grid(c.d), interior_block(), 0, s>>>(
-        c.d, c.A32(14), c.x32, c.f32, p->red_lambda, c.omega);
+    ideal_lambda_kernel<float><<<lambda_grid(c.d), interior_block(), 0, s>>>(
+        c.d, c.A32(14), c.x32, c.f32, p->red_lambda, c.omega,
+        lambda_planes(c.d));
   }
   prof_end(p, sl + kPhLambda);
   // x += w * (interpolated correction), one pass

@@ -135,17 +135,18 @@ __global__ void __launch_bounds__(256)
 
 // Hackbusch-Reusken damping w = (r . x) / (x . A x) over the interior of a
 // 27-point level (get_ideal_lambda, MultigridDomain.h:327-352), accumulated
-// in double; the last block stores w.
+// in double; the last block stores w. Grid: lambda_grid, `planes` =
+// lambda_planes.
 template <typename T>
 __global__ void __launch_bounds__(kReduceThreads)
     ideal_lambda_kernel(Dims d, Op14<T> A, const T *__restrict__ x,
                         const T *__restrict__ r, ReduceSlot s,
-                        double *__restrict__ w) {
+                        double *__restrict__ w, int planes) {
   __shared__ double sh[32];
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
-  const int k0 = 2 + blockIdx.z * kReducePlanes;
-  const int k1 = min(k0 + kReducePlanes - 1, d.nz - 1);
+  const int k0 = 2 + blockIdx.z * planes;
+  const int k1 = min(k0 + planes - 1, d.nz - 1);
   const int sy = d.sy(), sz = d.sz();
   double up = 0.0, lo = 0.0;
   if (i <= d.nx - 1 && j <= d.ny - 1) {
