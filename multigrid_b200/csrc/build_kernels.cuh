@@ -230,22 +230,24 @@ __global__ void __launch_bounds__(128)
     out32.a[13][pc] = (float)v;
 }
 
-// One Galerkin entry per thread (blockIdx.y: the output slot), for the
-// 27-point input, whose fourteen entries in one thread spill: a block
-// evaluates one entry's unrolled sum for 128 coarse points.
+// One Galerkin entry per thread (blockIdx.x: the output slot, so the
+// fourteen blocks of the same 128 coarse points run back to back and share
+// the fine operator in L2), for the 27-point input, whose fourteen entries
+// in one thread spill: a block evaluates one entry's unrolled sum for 128
+// coarse points.
 template <int KIND>
 __global__ void __launch_bounds__(128)
     buildG_entry_kernel(Dims df, Dims dc, P27<double> P, Op14<double> A,
                         Op14W<double> out, Op14W<float> out32) {
   const int mx = dc.nx - 2, my = dc.ny - 2;
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  const int q = blockIdx.y * blockDim.x + threadIdx.x;
   if (q >= mx * my * (dc.nz - 2))
     return;
   const int r = q / mx, kq = r / my;
   const int ii = q - r * mx + 2, jj = r - kq * my + 2, kk = kq + 2;
   const int pc = dc.at(ii, jj, kk);
   const int c0 = df.at(2 * ii - 1, 2 * jj - 1, 2 * kk - 1);
-  const int S = blockIdx.y;
+  const int S = blockIdx.x;
   double v;
   switch (S) {
   case 0: v = galerkin_entry<KIND, 0>(df, dc, P, A, pc, c0); break;

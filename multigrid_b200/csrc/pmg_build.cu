@@ -30,7 +30,7 @@ int launch_buildG(const Dims &df, const Dims &dc, int kind,
     buildG_kernel<7><<<grid, block, 0, s>>>(df, dc, P, A, out, out32);
   } else {
     const long m = (long)(dc.nx - 2) * (dc.ny - 2) * (dc.nz - 2);
-    buildG_entry_kernel<27><<<dim3((unsigned)((m + 127) / 128), 14), 128, 0,
+    buildG_entry_kernel<27><<<dim3(14, (unsigned)((m + 127) / 128)), 128, 0,
                               s>>>(df, dc, P, A, out, out32);
   }
   PMG_LAUNCH_CHECK();
