@@ -256,9 +256,14 @@ __global__ void __launch_bounds__(kSetupThreads)
   for (int b0 = 0; b0 < natoms; b0 += kSetupThreads) {
     __syncthreads();
     const int b = b0 + threadIdx.x;
-    if (b < natoms)
-      for (int d = 0; d < 5; ++d)
+    if (b < natoms) {
+      for (int d = 0; d < 4; ++d)
         sa[5 * threadIdx.x + d] = atoms[5 * b + d];
+      // the atom's factor q / (pref (1 + kappa r)), once per atom: the
+      // same operations as inside the sum, so the same bits
+      sa[5 * threadIdx.x + 4] =
+          atoms[5 * b + 4] / (pref * (1 + kappa * atoms[5 * b + 3]));
+    }
     __syncthreads();
     const int nb = natoms - b0 < kSetupThreads ? natoms - b0 : kSetupThreads;
     if (active)
@@ -268,9 +273,7 @@ __global__ void __launch_bounds__(kSetupThreads)
         const double d1 = i1 * h - at[1];
         const double d2 = i2 * h - at[2];
         const double dist = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
-        const double rad = at[3];
-        acc += at[4] / (pref * (1 + kappa * rad)) *
-               exp(-kappa * (dist - rad)) / dist;
+        acc += at[4] * exp(-kappa * (dist - at[3])) / dist;
       }
   }
   if (active)
