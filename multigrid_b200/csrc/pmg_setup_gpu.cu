@@ -22,7 +22,10 @@
 // All work is stream-ordered on the caller's stream; scratch comes from the
 // library's stream-ordered pool.
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
 
+#include <algorithm>
+#include <cmath>
 #include <vector>
 
 #include "pmg_common.cuh"
@@ -91,64 +94,6 @@ __global__ void __launch_bounds__(kSetupThreads)
   }
 }
 
-// Probe centres on the sphere of radius r_a + probe around every atom; a
-// centre is kept when no other inflated sphere contains it
-// (d^2 < R_b^2 (1 - 1e-12), the host's test). Output rows (x, y, z).
-__global__ void __launch_bounds__(kSetupThreads)
-    probe_centres_kernel(const double *atoms, int natoms, double probe,
-                         const ProbeDir *dirs, double *centres,
-                         unsigned char *free_flag) {
-  __shared__ double sa[kSetupThreads * 4];
-  const long g = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  const long total = (long)natoms * kProbePoints;
-  const bool active = g < total;
-  const int a = active ? (int)(g / kProbePoints) : 0;
-  const int s = active ? (int)(g % kProbePoints) : 0;
-  double pc[3] = {0, 0, 0};
-  if (active) {
-    const double R = atoms[5 * a + 3] + probe;
-    const ProbeDir u = dirs[s];
-    pc[0] = atoms[5 * a] + R * u.rr * u.c;
-    pc[1] = atoms[5 * a + 1] + R * u.rr * u.s;
-    pc[2] = atoms[5 * a + 2] + R * u.zz;
-  }
-  bool free = true;
-  for (int b0 = 0; b0 < natoms; b0 += kSetupThreads) {
-    __syncthreads();
-    const int b = b0 + threadIdx.x;
-    if (b < natoms) {
-      sa[4 * threadIdx.x + 0] = atoms[5 * b + 0];
-      sa[4 * threadIdx.x + 1] = atoms[5 * b + 1];
-      sa[4 * threadIdx.x + 2] = atoms[5 * b + 2];
-      sa[4 * threadIdx.x + 3] = atoms[5 * b + 3] + probe;
-    }
-    __syncthreads();
-    const int nb = natoms - b0 < kSetupThreads ? natoms - b0 : kSetupThreads;
-    if (active && free)
-      for (int t = 0; t < nb; ++t) {
-        if (b0 + t == a)
-          continue;
-        const double Rb = sa[4 * t + 3];
-        double d2 = 0;
-        for (int d = 0; d < 3; ++d) {
-          const double e = pc[d] - sa[4 * t + d];
-          d2 += e * e;
-        }
-        if (d2 < Rb * Rb * (1 - 1e-12)) {
-          free = false;
-          break;
-        }
-      }
-  }
-  if (active) {
-    centres[3 * g + 0] = pc[0];
-    centres[3 * g + 1] = pc[1];
-    centres[3 * g + 2] = pc[2];
-    free_flag[g] = free ? 1 : 0;
-  }
-}
-
-// face = solute ? v_in : v_out, solute = inside || (sas && !carved)
 __global__ void face_from_masks_kernel(long count, const unsigned char *inside,
                                        const unsigned char *sas,
                                        const unsigned char *carved,
@@ -227,6 +172,83 @@ __global__ void charge_sum_kernel(const double *atoms, int nrec, double h,
     acc += charge * wt / vol;
   }
   f[keys[r]] = acc;
+}
+
+// Probe centres on the sphere of radius r_a + probe around every atom; a
+// centre is kept when no other inflated sphere contains it
+// (d^2 < R_b^2 (1 - 1e-12), the host's test). Output rows (x, y, z). The
+// atoms are found through a cell list: a centre lies within the largest
+// inflated radius (<= the cell edge) of any sphere containing it, so only
+// the 27 cells around it are searched; "kept" is an AND over atoms, so the
+// order of the atoms within a cell does not matter.
+__global__ void __launch_bounds__(kSetupThreads)
+    probe_centres_cells_kernel(const double *atoms, int natoms, double probe,
+                               const ProbeDir *dirs, double cell, int dim,
+                               const int *cell_start, const int *cell_atoms,
+                               double *centres, unsigned char *free_flag) {
+  const long g = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (g >= (long)natoms * kProbePoints)
+    return;
+  const int a = (int)(g / kProbePoints), s = (int)(g % kProbePoints);
+  const double R = atoms[5 * a + 3] + probe;
+  const ProbeDir u = dirs[s];
+  double pc[3];
+  pc[0] = atoms[5 * a] + R * u.rr * u.c;
+  pc[1] = atoms[5 * a + 1] + R * u.rr * u.s;
+  pc[2] = atoms[5 * a + 2] + R * u.zz;
+  int cc[3];
+  for (int d = 0; d < 3; ++d)
+    cc[d] = (int)floor(pc[d] / cell);
+  bool free = true;
+  for (int dz = -1; dz <= 1 && free; ++dz)
+    for (int dy = -1; dy <= 1 && free; ++dy)
+      for (int dx = -1; dx <= 1 && free; ++dx) {
+        const int c0 = cc[0] + dx, c1 = cc[1] + dy, c2 = cc[2] + dz;
+        if (c0 < 0 || c1 < 0 || c2 < 0 || c0 >= dim || c1 >= dim ||
+            c2 >= dim)
+          continue;
+        const int cid = (c2 * dim + c1) * dim + c0;
+        for (int q = cell_start[cid]; q < cell_start[cid + 1]; ++q) {
+          const int b = cell_atoms[q];
+          if (b == a)
+            continue;
+          const double Rb = atoms[5 * b + 3] + probe;
+          double d2 = 0;
+          for (int d = 0; d < 3; ++d) {
+            const double e = pc[d] - atoms[5 * b + d];
+            d2 += e * e;
+          }
+          if (d2 < Rb * Rb * (1 - 1e-12)) {
+            free = false;
+            break;
+          }
+        }
+      }
+  centres[3 * g + 0] = pc[0];
+  centres[3 * g + 1] = pc[1];
+  centres[3 * g + 2] = pc[2];
+  free_flag[g] = free ? 1 : 0;
+}
+
+// Cell list of the atoms: cell of each atom and per-cell counts
+__global__ void atom_cells_kernel(const double *atoms, int natoms, double cell,
+                                  int dim, int *cid, int *count) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= natoms)
+    return;
+  int c[3];
+  for (int d = 0; d < 3; ++d)
+    c[d] = min((int)floor(atoms[5 * a + d] / cell), dim - 1);
+  cid[a] = (c[2] * dim + c[1]) * dim + c[0];
+  atomicAdd(&count[cid[a]], 1);
+}
+
+// atoms into their cells' ranges (fill: a copy of the ranges' starts)
+__global__ void atom_scatter_kernel(int natoms, const int *cid, int *fill,
+                                    int *cell_atoms) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a < natoms)
+    cell_atoms[atomicAdd(&fill[cid[a]], 1)] = a;
 }
 
 // Multiple Debye-Hueckel values on the six faces (atoms in order); faces
@@ -360,10 +382,42 @@ int setup_fine_device(int n, double h, const double *atoms_host, int natoms,
     PMG_CUDA_TRY(cudaMemcpyAsync(d_dirs, dirs, sizeof(dirs),
                                  cudaMemcpyHostToDevice, st));
     const long np = (long)natoms * kProbePoints;
-    probe_centres_kernel<<<(unsigned)((np + kSetupThreads - 1) /
-                                      kSetupThreads),
-                           kSetupThreads, 0, st>>>(
-        d_atoms, natoms, ph->probe_radius, d_dirs, centres, free_flag);
+    const unsigned pgrid = (unsigned)((np + kSetupThreads - 1) / kSetupThreads);
+    // cell list of the atoms, built on the stream: edge >= the largest
+    // inflated radius, at most 64 cells per axis of the grid's extent
+    const double extent = h * (n - 1);
+    double cell = 0;
+    for (int a = 0; a < natoms; ++a)
+      cell = std::max(cell, atoms_host[5 * a + 3]);
+    cell = std::max(cell + ph->probe_radius, extent / 63);
+    const int dim = (int)(extent / cell) + 1;
+    const int ncells = dim * dim * dim;
+    int *d_cid = nullptr, *d_count = nullptr, *d_cstart = nullptr,
+        *d_fill = nullptr, *d_cat = nullptr;
+    PMG_CUDA_TRY(sc.take(&d_cid, (size_t)natoms));
+    PMG_CUDA_TRY(sc.take(&d_count, (size_t)ncells + 1));
+    PMG_CUDA_TRY(sc.take(&d_cstart, (size_t)ncells + 1));
+    PMG_CUDA_TRY(sc.take(&d_fill, (size_t)ncells + 1));
+    PMG_CUDA_TRY(sc.take(&d_cat, (size_t)natoms));
+    PMG_CUDA_TRY(
+        cudaMemsetAsync(d_count, 0, sizeof(int) * (ncells + 1), st));
+    atom_cells_kernel<<<(natoms + 255) / 256, 256, 0, st>>>(
+        d_atoms, natoms, cell, dim, d_cid, d_count);
+    size_t scan_bytes = 0;
+    PMG_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, d_count,
+                                               d_cstart, ncells + 1, st));
+    unsigned char *scan_tmp = nullptr;
+    PMG_CUDA_TRY(sc.take(&scan_tmp, scan_bytes));
+    PMG_CUDA_TRY(cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, d_count,
+                                               d_cstart, ncells + 1, st));
+    PMG_CUDA_TRY(cudaMemcpyAsync(d_fill, d_cstart,
+                                 sizeof(int) * (ncells + 1),
+                                 cudaMemcpyDeviceToDevice, st));
+    atom_scatter_kernel<<<(natoms + 255) / 256, 256, 0, st>>>(
+        natoms, d_cid, d_fill, d_cat);
+    probe_centres_cells_kernel<<<pgrid, kSetupThreads, 0, st>>>(
+        d_atoms, natoms, ph->probe_radius, d_dirs, cell, dim, d_cstart, d_cat,
+        centres, free_flag);
     PMG_LAUNCH_CHECK();
   }
 
