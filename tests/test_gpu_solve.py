@@ -313,3 +313,28 @@ def test_throughput_mode_same_solve_within_tolerance(pb65):
     c1, x1 = out["mixed", True]
     assert abs(c0 - c1) <= 1
     assert np.linalg.norm(x1 - x0) <= 1e-9 * np.linalg.norm(x0)
+
+
+@pytest.mark.parametrize("throughput", [False, True])
+@pytest.mark.parametrize("base,nlev", [(2, 2), (2, 3), (2, 4), (1, 5)])
+def test_mixed_lowest_levels_shapes(base, nlev, throughput):
+    """The mixed path runs its levels up to 17^3 in one launch (a cluster of
+    CTAs, or one CTA in throughput mode). Hierarchies whose top bottom level
+    is 1, 2, 3 and 4 levels up (9^3 over 5^3 ... 33^3 over a 3^3 coarsest
+    level): the solve reaches 1e-10 and its potential matches the FP64
+    solve's within 1e-8."""
+    from multigrid_b200.molecule import Workload, level_n
+    n = level_n(base, nlev)
+    w = Workload("shape", base, nlev, 0.8, 12, 0.25 * 0.8 * (n - 1), 11)
+    fine = setup_fine(w.n, w.h, w.atoms(), w.physics)
+    out = {}
+    for prec in ("fp64", "mixed"):
+        with PBELinearProblem(base, nlev, w.box, prec, w.physics) as p:
+            p.set_throughput_mode(throughput)
+            p.set_fine(**fine)
+            p.buildmultilevelops()
+            r = p.solve(tol=1e-10, max_cycles=100)
+            assert r.relres < 1e-10, (prec, r.cycles, r.relres)
+            out[prec] = p.potential().ravel().copy()
+    x0, x1 = out["fp64"], out["mixed"]
+    assert np.linalg.norm(x1 - x0) <= 1e-8 * np.linalg.norm(x0)
