@@ -7,6 +7,8 @@
 #pragma once
 
 #include <cuda_runtime.h>
+
+#include <atomic>
 #include <stdint.h>
 
 #include "../../include/pmg_b200.h"
@@ -162,6 +164,23 @@ template <typename T> __device__ __forceinline__ T block_sum_2d(T v, T *sh) {
       return PMG_ERR_CUDA;                                                     \
     }                                                                          \
   } while (0)
+
+// Raises Kernel's dynamic shared-memory limit to `bytes` on the current
+// device, once per device (the attribute belongs to the device's context).
+template <auto Kernel> cudaError_t set_smem_limit(int bytes) {
+  static std::atomic<int> done[64]; // per device: the limit set so far
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess)
+    return e;
+  if (dev >= 0 && dev < 64 && done[dev].load() >= bytes)
+    return cudaSuccess;
+  e = cudaFuncSetAttribute(Kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           bytes);
+  if (e == cudaSuccess && dev >= 0 && dev < 64)
+    done[dev].store(bytes);
+  return e;
+}
 
 #define PMG_LAUNCH_CHECK()                                                     \
   do {                                                                         \

@@ -326,13 +326,8 @@ int launch_cg_level(const Dims &d, const Op14<double> &A, const double *rhs,
   if (cg_cluster_fits(d)) {
     // levels up to 17^3: a cluster with the operator in shared memory
     const size_t smem = cg_cluster_smem(d.nx, d.ny);
-    static size_t configured = 0;
-    if (configured < smem) {
-      PMG_CUDA_TRY(cudaFuncSetAttribute(
-          cg_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-          (int)cg_cluster_smem(kCgMaxN, kCgMaxN)));
-      configured = cg_cluster_smem(kCgMaxN, kCgMaxN);
-    }
+    PMG_CUDA_TRY(set_smem_limit<cg_cluster_kernel>(
+        (int)cg_cluster_smem(kCgMaxN, kCgMaxN)));
     cg_cluster_kernel<<<kCgCtas, kCgThreads, smem, s>>>(
         d, A, rhs, x, thresh, rel_tol, class_first_check, max_iters, status);
     PMG_LAUNCH_CHECK();

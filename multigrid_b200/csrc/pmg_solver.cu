@@ -434,13 +434,7 @@ int launch_bottom(pmg_problem *p, int top) {
   const BottomArgs a = bottom_args(p, top);
   cudaStream_t s = p->stream;
   if (!p->throughput && bc_fits(a)) {
-    static bool configured = false;
-    if (!configured) {
-      PMG_CUDA_TRY(cudaFuncSetAttribute(
-          bottom_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-          (int)kBcMaxSmem));
-      configured = true;
-    }
+    PMG_CUDA_TRY(set_smem_limit<bottom_cluster_kernel>((int)kBcMaxSmem));
     bottom_cluster_kernel<<<kCgCtas, kBcThreads, bc_layout(a).total, s>>>(a);
   } else {
     bottom_cycle_kernel<<<1, 1024, 0, s>>>(a);
