@@ -64,22 +64,6 @@ __global__ void from_split_kernel(Dims d, const Tin *__restrict__ src,
     dst[g] = (Tout)src[sp.of_linear((int)g)];
 }
 
-// x (split) += w e (reference layout) over every entry, the padded-array
-// update of add_and_multiply_domains (Domain.h:602-623)
-template <typename T>
-__global__ void axpy_split_kernel(Dims d, T *__restrict__ x,
-                                  const T *__restrict__ e,
-                                  const double *__restrict__ w) {
-  const Split sp = Split::of(d);
-  const T ww = (T)(*w);
-  const long n = d.count();
-  for (long g = blockIdx.x * (long)blockDim.x + threadIdx.x; g < n;
-       g += (long)gridDim.x * blockDim.x) {
-    const int s = sp.of_linear((int)g);
-    x[s] = x[s] + ww * e[g];
-  }
-}
-
 // x64 (reference layout) += (double) e32 (split) on the interior
 __global__ void add_correction_split_kernel(Dims d, double *__restrict__ x,
                                             const float *__restrict__ e);

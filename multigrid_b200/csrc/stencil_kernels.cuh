@@ -312,18 +312,6 @@ __global__ void __launch_bounds__(256)
 // Elementwise
 // ---------------------------------------------------------------------------
 
-// x = x + w * e over all n entries, w read from device memory
-// (add_and_multiply_domains, Domain.h:602-623).
-template <typename T>
-__global__ void axpy_full_kernel(long n, T *__restrict__ x,
-                                 const T *__restrict__ e,
-                                 const double *__restrict__ w) {
-  const T ww = (T)(*w);
-  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n;
-       q += (long)gridDim.x * blockDim.x)
-    x[q] = x[q] + ww * e[q];
-}
-
 // dst = (Tout)src over n entries.
 template <typename Tin, typename Tout>
 __global__ void convert_kernel(long n, const Tin *__restrict__ src,
