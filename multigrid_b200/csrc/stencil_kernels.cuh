@@ -1,5 +1,5 @@
 // Stencil kernels of the PMG V-cycle: Gauss-Seidel smoothers, matvec,
-// residual and defect, restriction, interpolation, axpy.
+// residual and defect, restriction, interpolation (with the damped update).
 //
 // Every kernel evaluates the per-point arithmetic in the reference's operation
 // order (products and sums rounded separately: the library is built with
@@ -256,10 +256,11 @@ __global__ void __launch_bounds__(256)
 
 // x = x + w * (interpolation of xin), fused: interp_kernel's eight values
 // per coarse cell (same order and arithmetic), each added at once to the
-// fine iterate as axpy_full_kernel adds it (add_and_multiply_domains,
-// Domain.h:602-623), so the correction never goes through memory. The fine
-// points the interpolation does not write (the last plane, row and column
-// of the shell) keep x: there the separate update adds w * 0. With SPLIT_X
+// fine iterate as the damped update of the padded array adds it, x + w e
+// (add_and_multiply_domains, Domain.h:602-623), so the correction never
+// goes through memory. The fine points the interpolation does not write
+// (the last plane, row and column of the shell) keep x: there the padded
+// update adds w * 0, e being zero there. With SPLIT_X
 // the fine iterate is in the colour-split row layout (split_layout.cuh).
 template <typename T, bool SPLIT_X>
 __global__ void __launch_bounds__(256)
