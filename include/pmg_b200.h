@@ -90,6 +90,11 @@ int pmg_Vmatvec7_1s_d(int nx, int ny, int nz, const double *oC,
                       const double *cc, const double *oE, const double *oN,
                       const double *uC, const double *x, double *y,
                       pmg_stream_t stream);
+/* The same on float arrays. */
+int pmg_Vmatvec7_1s_f(int nx, int ny, int nz, const float *oC,
+                      const float *cc, const float *oE, const float *oN,
+                      const float *uC, const float *x, float *y,
+                      pmg_stream_t stream);
 /* y = A x on the interior (27-point). Replaces pmgc::Vmatvec27_1s,
  * pmgc/matvecd.cc:103-176 (and matveckernel27, pmgc/matvecd.h:179-240). */
 int pmg_Vmatvec27_1s_d(int nx, int ny, int nz, const double *oC,
@@ -99,6 +104,14 @@ int pmg_Vmatvec27_1s_d(int nx, int ny, int nz, const double *oC,
                        const double *uS, const double *uNE, const double *uNW,
                        const double *uSE, const double *uSW, const double *x,
                        double *y, pmg_stream_t stream);
+/* The same on float arrays. */
+int pmg_Vmatvec27_1s_f(int nx, int ny, int nz, const float *oC,
+                       const float *cc, const float *oE, const float *oN,
+                       const float *uC, const float *oNE, const float *oNW,
+                       const float *uE, const float *uW, const float *uN,
+                       const float *uS, const float *uNE, const float *uNW,
+                       const float *uSE, const float *uSW, const float *x,
+                       float *y, pmg_stream_t stream);
 
 /* r = f - A x on the interior (7-point). Replaces pmgc::Vmresid7_1s,
  * pmgc/matvecd.cc:381-411. */
@@ -106,6 +119,11 @@ int pmg_Vmresid7_1s_d(int nx, int ny, int nz, const double *oC,
                       const double *cc, const double *fc, const double *oE,
                       const double *oN, const double *uC, const double *x,
                       double *r, pmg_stream_t stream);
+/* The same on float arrays. */
+int pmg_Vmresid7_1s_f(int nx, int ny, int nz, const float *oC,
+                      const float *cc, const float *fc, const float *oE,
+                      const float *oN, const float *uC, const float *x,
+                      float *r, pmg_stream_t stream);
 /* r = f - A x on the interior (27-point). Replaces pmgc::Vmresid27_1s,
  * pmgc/matvecd.cc:425-495. */
 int pmg_Vmresid27_1s_d(int nx, int ny, int nz, const double *oC,
@@ -115,6 +133,14 @@ int pmg_Vmresid27_1s_d(int nx, int ny, int nz, const double *oC,
                        const double *uN, const double *uS, const double *uNE,
                        const double *uNW, const double *uSE, const double *uSW,
                        const double *x, double *r, pmg_stream_t stream);
+/* The same on float arrays. */
+int pmg_Vmresid27_1s_f(int nx, int ny, int nz, const float *oC,
+                       const float *cc, const float *fc, const float *oE,
+                       const float *oN, const float *uC, const float *oNE,
+                       const float *oNW, const float *uE, const float *uW,
+                       const float *uN, const float *uS, const float *uNE,
+                       const float *uNW, const float *uSE, const float *uSW,
+                       const float *x, float *r, pmg_stream_t stream);
 
 /* Restriction xout = P^T xin on the coarse interior.
  * Replaces pmgc::Vrestrc2, pmgc/matvecd.cc:695-799. */
@@ -129,6 +155,19 @@ int pmg_Vrestrc2_d(int nxf, int nyf, int nzf, int nxc, int nyc, int nzc,
                    const double *dPN, const double *dPS, const double *dPE,
                    const double *dPW, const double *dPNE, const double *dPNW,
                    const double *dPSE, const double *dPSW,
+                   pmg_stream_t stream);
+/* The same on float arrays. */
+int pmg_Vrestrc2_f(int nxf, int nyf, int nzf, int nxc, int nyc, int nzc,
+                   const float *xin, float *xout, const float *oPC,
+                   const float *oPN, const float *oPS, const float *oPE,
+                   const float *oPW, const float *oPNE, const float *oPNW,
+                   const float *oPSE, const float *oPSW, const float *uPC,
+                   const float *uPN, const float *uPS, const float *uPE,
+                   const float *uPW, const float *uPNE, const float *uPNW,
+                   const float *uPSE, const float *uPSW, const float *dPC,
+                   const float *dPN, const float *dPS, const float *dPE,
+                   const float *dPW, const float *dPNE, const float *dPNW,
+                   const float *dPSE, const float *dPSW,
                    pmg_stream_t stream);
 
 /* Operator-based interpolation xout = P xin: every coarse (ii,jj,kk) in
@@ -145,6 +184,19 @@ int pmg_VinterpPMG2_d(int nxc, int nyc, int nzc, int nxf, int nyf, int nzf,
                       const double *dPN, const double *dPS, const double *dPE,
                       const double *dPW, const double *dPNE, const double *dPNW,
                       const double *dPSE, const double *dPSW,
+                      pmg_stream_t stream);
+/* The same on float arrays. */
+int pmg_VinterpPMG2_f(int nxc, int nyc, int nzc, int nxf, int nyf, int nzf,
+                      const float *xin, float *xout, const float *oPC,
+                      const float *oPN, const float *oPS, const float *oPE,
+                      const float *oPW, const float *oPNE, const float *oPNW,
+                      const float *oPSE, const float *oPSW, const float *uPC,
+                      const float *uPN, const float *uPS, const float *uPE,
+                      const float *uPW, const float *uPNE, const float *uPNW,
+                      const float *uPSE, const float *uPSW, const float *dPC,
+                      const float *dPN, const float *dPS, const float *dPE,
+                      const float *dPW, const float *dPNE, const float *dPNW,
+                      const float *dPSE, const float *dPSW,
                       pmg_stream_t stream);
 
 /* Operator-based prolongation from a 7-point fine operator (27 outputs on

@@ -72,12 +72,13 @@ _sig("pmg_Vgsrb7x_f", c_int, *_GS7)
 _GS27 = [c_int] * 3 + [_V] * 17 + [c_int] * 3 + [_V]
 _sig("pmg_Vgsrb27x_d", c_int, *_GS27)
 _sig("pmg_Vgsrb27x_f", c_int, *_GS27)
-_sig("pmg_Vmatvec7_1s_d", c_int, *([c_int] * 3 + [_V] * 7 + [_V]))
-_sig("pmg_Vmatvec27_1s_d", c_int, *([c_int] * 3 + [_V] * 17 + [_V]))
-_sig("pmg_Vmresid7_1s_d", c_int, *([c_int] * 3 + [_V] * 8 + [_V]))
-_sig("pmg_Vmresid27_1s_d", c_int, *([c_int] * 3 + [_V] * 18 + [_V]))
-_sig("pmg_Vrestrc2_d", c_int, *([c_int] * 6 + [_V] * 29 + [_V]))
-_sig("pmg_VinterpPMG2_d", c_int, *([c_int] * 6 + [_V] * 29 + [_V]))
+for _t in ("_d", "_f"):
+    _sig("pmg_Vmatvec7_1s" + _t, c_int, *([c_int] * 3 + [_V] * 7 + [_V]))
+    _sig("pmg_Vmatvec27_1s" + _t, c_int, *([c_int] * 3 + [_V] * 17 + [_V]))
+    _sig("pmg_Vmresid7_1s" + _t, c_int, *([c_int] * 3 + [_V] * 8 + [_V]))
+    _sig("pmg_Vmresid27_1s" + _t, c_int, *([c_int] * 3 + [_V] * 18 + [_V]))
+    _sig("pmg_Vrestrc2" + _t, c_int, *([c_int] * 6 + [_V] * 29 + [_V]))
+    _sig("pmg_VinterpPMG2" + _t, c_int, *([c_int] * 6 + [_V] * 29 + [_V]))
 _sig("pmg_VbuildPb_op7_d", c_int, *([c_int] * 6 + [_V] * 31 + [_V]))
 _sig("pmg_VbuildPb_op27_d", c_int, *([c_int] * 6 + [_V] * 41 + [_V]))
 _sig("pmg_VbuildPb_trilin_d", c_int, *([c_int] * 6 + [_V] * 27 + [_V]))

@@ -444,6 +444,134 @@ static int gs27_inplace(const Dims &d, const Op14<T> &A, const T *cc,
 // ---------------------------------------------------------------------------
 // C ABI
 // ---------------------------------------------------------------------------
+// Kernel entry points, for double (_d) and float (_f) arrays.
+#define P27_ARGS                                                               \
+  oPC, oPN, oPS, oPE, oPW, oPNE, oPNW, oPSE, oPSW, uPC, uPN, uPS, uPE, uPW,    \
+      uPNE, uPNW, uPSE, uPSW, dPC, dPN, dPS, dPE, dPW, dPNE, dPNW, dPSE, dPSW
+
+template <typename T>
+static int entry_Vmatvec7_1s(int nx, int ny, int nz, const T *oC,
+                      const T *cc, const T *oE, const T *oN,
+                      const T *uC, const T *x, T *y,
+                      pmg_stream_t stream) {
+  PMG_REQUIRE(!bad_dims(nx, ny, nz), "Vmatvec7_1s: grid size out of range");
+  PMG_REQUIRE(oC && oE && oN && uC && x && y, "Vmatvec7_1s: null array");
+  const Dims d{nx, ny, nz};
+  matvec_kernel<7, T><<<interior_grid(d), interior_block(),
+                             0, (cudaStream_t)stream>>>(
+      d, op7(oC, oE, oN, uC), cc, x, y);
+  PMG_LAUNCH_CHECK();
+  return PMG_OK;
+}
+
+template <typename T>
+static int entry_Vmatvec27_1s(int nx, int ny, int nz, const T *oC,
+                       const T *cc, const T *oE, const T *oN,
+                       const T *uC, const T *oNE, const T *oNW,
+                       const T *uE, const T *uW, const T *uN,
+                       const T *uS, const T *uNE, const T *uNW,
+                       const T *uSE, const T *uSW, const T *x,
+                       T *y, pmg_stream_t stream) {
+  PMG_REQUIRE(!bad_dims(nx, ny, nz), "Vmatvec27_1s: grid size out of range");
+  const Op14<T> A =
+      op27(oC, oE, oN, uC, oNE, oNW, uE, uW, uN, uS, uNE, uNW, uSE, uSW);
+  PMG_REQUIRE(!any_null(A, 14) && x && y, "Vmatvec27_1s: null array");
+  const Dims d{nx, ny, nz};
+  matvec_kernel<27, T><<<interior_grid(d), interior_block(), 0,
+                              (cudaStream_t)stream>>>(d, A, cc, x, y);
+  PMG_LAUNCH_CHECK();
+  return PMG_OK;
+}
+
+template <typename T>
+static int entry_Vmresid7_1s(int nx, int ny, int nz, const T *oC,
+                      const T *cc, const T *fc, const T *oE,
+                      const T *oN, const T *uC, const T *x,
+                      T *r, pmg_stream_t stream) {
+  PMG_REQUIRE(!bad_dims(nx, ny, nz), "Vmresid7_1s: grid size out of range");
+  PMG_REQUIRE(oC && fc && oE && oN && uC && x && r,
+              "Vmresid7_1s: null array");
+  const Dims d{nx, ny, nz};
+  mresid_kernel<7, T><<<interior_grid(d), interior_block(), 0,
+                             (cudaStream_t)stream>>>(
+      d, op7(oC, oE, oN, uC), cc, fc, x, r);
+  PMG_LAUNCH_CHECK();
+  return PMG_OK;
+}
+
+template <typename T>
+static int entry_Vmresid27_1s(int nx, int ny, int nz, const T *oC,
+                       const T *cc, const T *fc, const T *oE,
+                       const T *oN, const T *uC, const T *oNE,
+                       const T *oNW, const T *uE, const T *uW,
+                       const T *uN, const T *uS, const T *uNE,
+                       const T *uNW, const T *uSE, const T *uSW,
+                       const T *x, T *r, pmg_stream_t stream) {
+  PMG_REQUIRE(!bad_dims(nx, ny, nz), "Vmresid27_1s: grid size out of range");
+  const Op14<T> A =
+      op27(oC, oE, oN, uC, oNE, oNW, uE, uW, uN, uS, uNE, uNW, uSE, uSW);
+  PMG_REQUIRE(!any_null(A, 14) && fc && x && r, "Vmresid27_1s: null array");
+  const Dims d{nx, ny, nz};
+  mresid_kernel<27, T><<<interior_grid(d), interior_block(), 0,
+                              (cudaStream_t)stream>>>(d, A, cc, fc, x, r);
+  PMG_LAUNCH_CHECK();
+  return PMG_OK;
+}
+
+template <typename T>
+static int entry_Vrestrc2(int nxf, int nyf, int nzf, int nxc, int nyc, int nzc,
+                   const T *xin, T *xout, const T *oPC,
+                   const T *oPN, const T *oPS, const T *oPE,
+                   const T *oPW, const T *oPNE, const T *oPNW,
+                   const T *oPSE, const T *oPSW, const T *uPC,
+                   const T *uPN, const T *uPS, const T *uPE,
+                   const T *uPW, const T *uPNE, const T *uPNW,
+                   const T *uPSE, const T *uPSW, const T *dPC,
+                   const T *dPN, const T *dPS, const T *dPE,
+                   const T *dPW, const T *dPNE, const T *dPNW,
+                   const T *dPSE, const T *dPSW,
+                   pmg_stream_t stream) {
+  PMG_REQUIRE(!bad_pair(nxf, nyf, nzf, nxc, nyc, nzc),
+              "Vrestrc2: sizes must satisfy n_f = 2 n_c - 1");
+  const P27<T> P{{P27_ARGS}};
+  for (int s = 0; s < 27; ++s)
+    PMG_REQUIRE(P.p[s], "Vrestrc2: null prolongation array");
+  PMG_REQUIRE(xin && xout, "Vrestrc2: null array");
+  const Dims dc{nxc, nyc, nzc};
+  restrict_kernel<T, T><<<interior_grid(dc), interior_block(), 0,
+                                    (cudaStream_t)stream>>>(
+      Dims{nxf, nyf, nzf}, dc, xin, xout, P);
+  PMG_LAUNCH_CHECK();
+  return PMG_OK;
+}
+
+template <typename T>
+static int entry_VinterpPMG2(int nxc, int nyc, int nzc, int nxf, int nyf,
+                      int nzf, const T *xin, T *xout, const T *oPC,
+                      const T *oPN, const T *oPS, const T *oPE,
+                      const T *oPW, const T *oPNE, const T *oPNW,
+                      const T *oPSE, const T *oPSW, const T *uPC,
+                      const T *uPN, const T *uPS, const T *uPE,
+                      const T *uPW, const T *uPNE, const T *uPNW,
+                      const T *uPSE, const T *uPSW, const T *dPC,
+                      const T *dPN, const T *dPS, const T *dPE,
+                      const T *dPW, const T *dPNE, const T *dPNW,
+                      const T *dPSE, const T *dPSW,
+                      pmg_stream_t stream) {
+  PMG_REQUIRE(!bad_pair(nxf, nyf, nzf, nxc, nyc, nzc),
+              "VinterpPMG2: sizes must satisfy n_f = 2 n_c - 1");
+  const P27<T> P{{P27_ARGS}};
+  for (int s = 0; s < 27; ++s)
+    PMG_REQUIRE(P.p[s], "VinterpPMG2: null prolongation array");
+  PMG_REQUIRE(xin && xout, "VinterpPMG2: null array");
+  const Dims dc{nxc, nyc, nzc};
+  interp_kernel<T><<<interp_grid(dc), interior_block(), 0,
+                          (cudaStream_t)stream>>>(dc, Dims{nxf, nyf, nzf},
+                                                  xin, xout, P);
+  PMG_LAUNCH_CHECK();
+  return PMG_OK;
+}
+
 extern "C" {
 
 int pmg_set_autotune(int mode) {
@@ -511,14 +639,15 @@ int pmg_Vmatvec7_1s_d(int nx, int ny, int nz, const double *oC,
                       const double *cc, const double *oE, const double *oN,
                       const double *uC, const double *x, double *y,
                       pmg_stream_t stream) {
-  PMG_REQUIRE(!bad_dims(nx, ny, nz), "Vmatvec7_1s: grid size out of range");
-  PMG_REQUIRE(oC && oE && oN && uC && x && y, "Vmatvec7_1s: null array");
-  const Dims d{nx, ny, nz};
-  matvec_kernel<7, double><<<interior_grid(d), interior_block(),
-                             0, (cudaStream_t)stream>>>(
-      d, op7(oC, oE, oN, uC), cc, x, y);
-  PMG_LAUNCH_CHECK();
-  return PMG_OK;
+  return entry_Vmatvec7_1s<double>(nx, ny, nz, oC, cc, oE, oN, uC, x, y,
+      stream);
+}
+
+int pmg_Vmatvec7_1s_f(int nx, int ny, int nz, const float *oC,
+                      const float *cc, const float *oE, const float *oN,
+                      const float *uC, const float *x, float *y,
+                      pmg_stream_t stream) {
+  return entry_Vmatvec7_1s<float>(nx, ny, nz, oC, cc, oE, oN, uC, x, y, stream);
 }
 
 int pmg_Vmatvec27_1s_d(int nx, int ny, int nz, const double *oC,
@@ -528,30 +657,35 @@ int pmg_Vmatvec27_1s_d(int nx, int ny, int nz, const double *oC,
                        const double *uS, const double *uNE, const double *uNW,
                        const double *uSE, const double *uSW, const double *x,
                        double *y, pmg_stream_t stream) {
-  PMG_REQUIRE(!bad_dims(nx, ny, nz), "Vmatvec27_1s: grid size out of range");
-  const Op14<double> A =
-      op27(oC, oE, oN, uC, oNE, oNW, uE, uW, uN, uS, uNE, uNW, uSE, uSW);
-  PMG_REQUIRE(!any_null(A, 14) && x && y, "Vmatvec27_1s: null array");
-  const Dims d{nx, ny, nz};
-  matvec_kernel<27, double><<<interior_grid(d), interior_block(), 0,
-                              (cudaStream_t)stream>>>(d, A, cc, x, y);
-  PMG_LAUNCH_CHECK();
-  return PMG_OK;
+  return entry_Vmatvec27_1s<double>(nx, ny, nz, oC, cc, oE, oN, uC, oNE, oNW,
+      uE, uW, uN, uS, uNE, uNW, uSE, uSW, x, y, stream);
+}
+
+int pmg_Vmatvec27_1s_f(int nx, int ny, int nz, const float *oC,
+                       const float *cc, const float *oE, const float *oN,
+                       const float *uC, const float *oNE, const float *oNW,
+                       const float *uE, const float *uW, const float *uN,
+                       const float *uS, const float *uNE, const float *uNW,
+                       const float *uSE, const float *uSW, const float *x,
+                       float *y, pmg_stream_t stream) {
+  return entry_Vmatvec27_1s<float>(nx, ny, nz, oC, cc, oE, oN, uC, oNE, oNW, uE,
+      uW, uN, uS, uNE, uNW, uSE, uSW, x, y, stream);
 }
 
 int pmg_Vmresid7_1s_d(int nx, int ny, int nz, const double *oC,
                       const double *cc, const double *fc, const double *oE,
                       const double *oN, const double *uC, const double *x,
                       double *r, pmg_stream_t stream) {
-  PMG_REQUIRE(!bad_dims(nx, ny, nz), "Vmresid7_1s: grid size out of range");
-  PMG_REQUIRE(oC && fc && oE && oN && uC && x && r,
-              "Vmresid7_1s: null array");
-  const Dims d{nx, ny, nz};
-  mresid_kernel<7, double><<<interior_grid(d), interior_block(), 0,
-                             (cudaStream_t)stream>>>(
-      d, op7(oC, oE, oN, uC), cc, fc, x, r);
-  PMG_LAUNCH_CHECK();
-  return PMG_OK;
+  return entry_Vmresid7_1s<double>(nx, ny, nz, oC, cc, fc, oE, oN, uC, x, r,
+      stream);
+}
+
+int pmg_Vmresid7_1s_f(int nx, int ny, int nz, const float *oC,
+                      const float *cc, const float *fc, const float *oE,
+                      const float *oN, const float *uC, const float *x,
+                      float *r, pmg_stream_t stream) {
+  return entry_Vmresid7_1s<float>(nx, ny, nz, oC, cc, fc, oE, oN, uC, x, r,
+      stream);
 }
 
 int pmg_Vmresid27_1s_d(int nx, int ny, int nz, const double *oC,
@@ -561,20 +695,20 @@ int pmg_Vmresid27_1s_d(int nx, int ny, int nz, const double *oC,
                        const double *uN, const double *uS, const double *uNE,
                        const double *uNW, const double *uSE, const double *uSW,
                        const double *x, double *r, pmg_stream_t stream) {
-  PMG_REQUIRE(!bad_dims(nx, ny, nz), "Vmresid27_1s: grid size out of range");
-  const Op14<double> A =
-      op27(oC, oE, oN, uC, oNE, oNW, uE, uW, uN, uS, uNE, uNW, uSE, uSW);
-  PMG_REQUIRE(!any_null(A, 14) && fc && x && r, "Vmresid27_1s: null array");
-  const Dims d{nx, ny, nz};
-  mresid_kernel<27, double><<<interior_grid(d), interior_block(), 0,
-                              (cudaStream_t)stream>>>(d, A, cc, fc, x, r);
-  PMG_LAUNCH_CHECK();
-  return PMG_OK;
+  return entry_Vmresid27_1s<double>(nx, ny, nz, oC, cc, fc, oE, oN, uC, oNE,
+      oNW, uE, uW, uN, uS, uNE, uNW, uSE, uSW, x, r, stream);
 }
 
-#define P27_ARGS                                                               \
-  oPC, oPN, oPS, oPE, oPW, oPNE, oPNW, oPSE, oPSW, uPC, uPN, uPS, uPE, uPW,    \
-      uPNE, uPNW, uPSE, uPSW, dPC, dPN, dPS, dPE, dPW, dPNE, dPNW, dPSE, dPSW
+int pmg_Vmresid27_1s_f(int nx, int ny, int nz, const float *oC,
+                       const float *cc, const float *fc, const float *oE,
+                       const float *oN, const float *uC, const float *oNE,
+                       const float *oNW, const float *uE, const float *uW,
+                       const float *uN, const float *uS, const float *uNE,
+                       const float *uNW, const float *uSE, const float *uSW,
+                       const float *x, float *r, pmg_stream_t stream) {
+  return entry_Vmresid27_1s<float>(nx, ny, nz, oC, cc, fc, oE, oN, uC, oNE, oNW,
+      uE, uW, uN, uS, uNE, uNW, uSE, uSW, x, r, stream);
+}
 
 int pmg_Vrestrc2_d(int nxf, int nyf, int nzf, int nxc, int nyc, int nzc,
                    const double *xin, double *xout, const double *oPC,
@@ -588,18 +722,28 @@ int pmg_Vrestrc2_d(int nxf, int nyf, int nzf, int nxc, int nyc, int nzc,
                    const double *dPW, const double *dPNE, const double *dPNW,
                    const double *dPSE, const double *dPSW,
                    pmg_stream_t stream) {
-  PMG_REQUIRE(!bad_pair(nxf, nyf, nzf, nxc, nyc, nzc),
-              "Vrestrc2: sizes must satisfy n_f = 2 n_c - 1");
-  const P27<double> P{{P27_ARGS}};
-  for (int s = 0; s < 27; ++s)
-    PMG_REQUIRE(P.p[s], "Vrestrc2: null prolongation array");
-  PMG_REQUIRE(xin && xout, "Vrestrc2: null array");
-  const Dims dc{nxc, nyc, nzc};
-  restrict_kernel<double, double><<<interior_grid(dc), interior_block(), 0,
-                                    (cudaStream_t)stream>>>(
-      Dims{nxf, nyf, nzf}, dc, xin, xout, P);
-  PMG_LAUNCH_CHECK();
-  return PMG_OK;
+  return entry_Vrestrc2<double>(nxf, nyf, nzf, nxc, nyc, nzc, xin, xout, oPC,
+      oPN, oPS, oPE, oPW, oPNE, oPNW, oPSE, oPSW, uPC, uPN, uPS, uPE, uPW, uPNE,
+      uPNW, uPSE, uPSW, dPC, dPN, dPS, dPE, dPW, dPNE, dPNW, dPSE, dPSW,
+      stream);
+}
+
+int pmg_Vrestrc2_f(int nxf, int nyf, int nzf, int nxc, int nyc, int nzc,
+                   const float *xin, float *xout, const float *oPC,
+                   const float *oPN, const float *oPS, const float *oPE,
+                   const float *oPW, const float *oPNE, const float *oPNW,
+                   const float *oPSE, const float *oPSW, const float *uPC,
+                   const float *uPN, const float *uPS, const float *uPE,
+                   const float *uPW, const float *uPNE, const float *uPNW,
+                   const float *uPSE, const float *uPSW, const float *dPC,
+                   const float *dPN, const float *dPS, const float *dPE,
+                   const float *dPW, const float *dPNE, const float *dPNW,
+                   const float *dPSE, const float *dPSW,
+                   pmg_stream_t stream) {
+  return entry_Vrestrc2<float>(nxf, nyf, nzf, nxc, nyc, nzc, xin, xout, oPC,
+      oPN, oPS, oPE, oPW, oPNE, oPNW, oPSE, oPSW, uPC, uPN, uPS, uPE, uPW, uPNE,
+      uPNW, uPSE, uPSW, dPC, dPN, dPS, dPE, dPW, dPNE, dPNW, dPSE, dPSW,
+      stream);
 }
 
 int pmg_VinterpPMG2_d(int nxc, int nyc, int nzc, int nxf, int nyf, int nzf,
@@ -614,18 +758,28 @@ int pmg_VinterpPMG2_d(int nxc, int nyc, int nzc, int nxf, int nyf, int nzf,
                       const double *dPW, const double *dPNE, const double *dPNW,
                       const double *dPSE, const double *dPSW,
                       pmg_stream_t stream) {
-  PMG_REQUIRE(!bad_pair(nxf, nyf, nzf, nxc, nyc, nzc),
-              "VinterpPMG2: sizes must satisfy n_f = 2 n_c - 1");
-  const P27<double> P{{P27_ARGS}};
-  for (int s = 0; s < 27; ++s)
-    PMG_REQUIRE(P.p[s], "VinterpPMG2: null prolongation array");
-  PMG_REQUIRE(xin && xout, "VinterpPMG2: null array");
-  const Dims dc{nxc, nyc, nzc};
-  interp_kernel<double><<<interp_grid(dc), interior_block(), 0,
-                          (cudaStream_t)stream>>>(dc, Dims{nxf, nyf, nzf},
-                                                  xin, xout, P);
-  PMG_LAUNCH_CHECK();
-  return PMG_OK;
+  return entry_VinterpPMG2<double>(nxc, nyc, nzc, nxf, nyf, nzf, xin, xout, oPC,
+      oPN, oPS, oPE, oPW, oPNE, oPNW, oPSE, oPSW, uPC, uPN, uPS, uPE, uPW, uPNE,
+      uPNW, uPSE, uPSW, dPC, dPN, dPS, dPE, dPW, dPNE, dPNW, dPSE, dPSW,
+      stream);
+}
+
+int pmg_VinterpPMG2_f(int nxc, int nyc, int nzc, int nxf, int nyf, int nzf,
+                      const float *xin, float *xout, const float *oPC,
+                      const float *oPN, const float *oPS, const float *oPE,
+                      const float *oPW, const float *oPNE, const float *oPNW,
+                      const float *oPSE, const float *oPSW, const float *uPC,
+                      const float *uPN, const float *uPS, const float *uPE,
+                      const float *uPW, const float *uPNE, const float *uPNW,
+                      const float *uPSE, const float *uPSW, const float *dPC,
+                      const float *dPN, const float *dPS, const float *dPE,
+                      const float *dPW, const float *dPNE, const float *dPNW,
+                      const float *dPSE, const float *dPSW,
+                      pmg_stream_t stream) {
+  return entry_VinterpPMG2<float>(nxc, nyc, nzc, nxf, nyf, nzf, xin, xout, oPC,
+      oPN, oPS, oPE, oPW, oPNE, oPNW, oPSE, oPSW, uPC, uPN, uPS, uPE, uPW, uPNE,
+      uPNW, uPSE, uPSW, dPC, dPN, dPS, dPE, dPW, dPNE, dPNW, dPSE, dPSW,
+      stream);
 }
 
 int pmg_VbuildPb_op7_d(int nxf, int nyf, int nzf, int nxc, int nyc, int nzc,

@@ -75,35 +75,35 @@ def Vgsrb27x(nx, ny, nz, op14, cc, fc, x, itmax, zero_init=False, iadjoint=0,
 
 
 def Vmatvec7_1s(nx, ny, nz, oC, cc, oE, oN, uC, x, y, stream=None):
-    _lib.call("pmg_Vmatvec7_1s_d", nx, ny, nz, _p(oC), _p(cc), _p(oE),
-              _p(oN), _p(uC), _p(x), _p(y), _s(stream))
+    _lib.call("pmg_Vmatvec7_1s" + _sfx(x), nx, ny, nz, _p(oC), _p(cc),
+              _p(oE), _p(oN), _p(uC), _p(x), _p(y), _s(stream))
 
 
 def Vmatvec27_1s(nx, ny, nz, op14, cc, x, y, stream=None):
     a = [_p(t) for t in op14]
-    _lib.call("pmg_Vmatvec27_1s_d", nx, ny, nz, a[0], _p(cc), *a[1:], _p(x),
-              _p(y), _s(stream))
+    _lib.call("pmg_Vmatvec27_1s" + _sfx(x), nx, ny, nz, a[0], _p(cc),
+              *a[1:], _p(x), _p(y), _s(stream))
 
 
 def Vmresid7_1s(nx, ny, nz, oC, cc, fc, oE, oN, uC, x, r, stream=None):
-    _lib.call("pmg_Vmresid7_1s_d", nx, ny, nz, _p(oC), _p(cc), _p(fc),
-              _p(oE), _p(oN), _p(uC), _p(x), _p(r), _s(stream))
+    _lib.call("pmg_Vmresid7_1s" + _sfx(x), nx, ny, nz, _p(oC), _p(cc),
+              _p(fc), _p(oE), _p(oN), _p(uC), _p(x), _p(r), _s(stream))
 
 
 def Vmresid27_1s(nx, ny, nz, op14, cc, fc, x, r, stream=None):
     a = [_p(t) for t in op14]
-    _lib.call("pmg_Vmresid27_1s_d", nx, ny, nz, a[0], _p(cc), _p(fc),
-              *a[1:], _p(x), _p(r), _s(stream))
+    _lib.call("pmg_Vmresid27_1s" + _sfx(x), nx, ny, nz, a[0], _p(cc),
+              _p(fc), *a[1:], _p(x), _p(r), _s(stream))
 
 
 def Vrestrc2(nxf, nyf, nzf, nxc, nyc, nzc, xin, xout, p27, stream=None):
-    _lib.call("pmg_Vrestrc2_d", nxf, nyf, nzf, nxc, nyc, nzc, _p(xin),
-              _p(xout), *[_p(t) for t in p27], _s(stream))
+    _lib.call("pmg_Vrestrc2" + _sfx(xin), nxf, nyf, nzf, nxc, nyc, nzc,
+              _p(xin), _p(xout), *[_p(t) for t in p27], _s(stream))
 
 
 def VinterpPMG2(nxc, nyc, nzc, nxf, nyf, nzf, xin, xout, p27, stream=None):
-    _lib.call("pmg_VinterpPMG2_d", nxc, nyc, nzc, nxf, nyf, nzf, _p(xin),
-              _p(xout), *[_p(t) for t in p27], _s(stream))
+    _lib.call("pmg_VinterpPMG2" + _sfx(xin), nxc, nyc, nzc, nxf, nyf, nzf,
+              _p(xin), _p(xout), *[_p(t) for t in p27], _s(stream))
 
 
 def VbuildPb_op7(nxf, nyf, nzf, nxc, nyc, nzc, oC, oE, oN, uC, p27,

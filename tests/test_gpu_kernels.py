@@ -198,6 +198,46 @@ def test_float_smoothers_track_double():
     assert rel(H(xf), H(xd)) < 1e-5
 
 
+def test_float_kernels_track_double():
+    """The _f matvec, residual and transfer entry points against the _d ones
+    on the same float-rounded inputs: only the arithmetic's precision
+    differs, so each result agrees to 1e-5 of its maximum."""
+    nf, nc = 33, 17
+    c = rand_case(nf, 11)
+    r32 = [np.float32(a).astype(np.float64)
+           for a in c["op7"] + c["op27"] + [c["cc"], c["f"], c["x0"]]]
+    o7d, o27d = r32[:4], r32[4:18]
+    cc, f, x = r32[18:]
+
+    def both(call, n_out):
+        got = []
+        for dt in (torch.float64, torch.float32):
+            y = torch.zeros(n_out, dtype=dt, device=DEV)
+            call(lambda a: T(a, dt), y)
+            got.append(H(y))
+        assert np.abs(got[0]).max() > 0
+        assert rel(got[1], got[0]) < 1e-5
+        return got
+
+    both(lambda t, y: pmgc.Vmatvec7_1s(nf, nf, nf, t(o7d[0]), t(cc),
+                                       t(o7d[1]), t(o7d[2]), t(o7d[3]),
+                                       t(x), y), nf ** 3)
+    both(lambda t, y: pmgc.Vmatvec27_1s(nf, nf, nf, [t(a) for a in o27d],
+                                        t(cc), t(x), y), nf ** 3)
+    both(lambda t, y: pmgc.Vmresid7_1s(nf, nf, nf, t(o7d[0]), t(cc), t(f),
+                                       t(o7d[1]), t(o7d[2]), t(o7d[3]),
+                                       t(x), y), nf ** 3)
+    both(lambda t, y: pmgc.Vmresid27_1s(nf, nf, nf, [t(a) for a in o27d],
+                                        t(cc), t(f), t(x), y), nf ** 3)
+    P = [np.float32(c["rng"].uniform(0.05, 1.0, nc ** 3)).astype(np.float64)
+         for _ in range(27)]
+    xc = np.float32(c["rng"].normal(size=nc ** 3)).astype(np.float64)
+    both(lambda t, y: pmgc.Vrestrc2(nf, nf, nf, nc, nc, nc, t(x), y,
+                                    [t(a) for a in P]), nc ** 3)
+    both(lambda t, y: pmgc.VinterpPMG2(nc, nc, nc, nf, nf, nf, t(xc), y,
+                                       [t(a) for a in P]), nf ** 3)
+
+
 def test_cg_level_matches_reference(golden_problem, restatement):
     g = golden_problem
     base = int(g["base"])
