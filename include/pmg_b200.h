@@ -239,6 +239,26 @@ int pmg_VbuildPb_trilin_d(int nxf, int nyf, int nzf, int nxc, int nyc,
                           double *dPW, double *dPNE, double *dPNW,
                           double *dPSE, double *dPSW, pmg_stream_t stream);
 
+/* Box-method (finite volume) fine operator of the APBS driver from the
+ * coefficient maps on a tensor mesh: oC, cc, fc, oE, oN, uC on the interior
+ * (the shell is not written) from the mesh lines xf (nx), yf (ny), zf (nz),
+ * the Dirichlet values gxcf (ny*nz*2), gycf (nx*nz*2), gzcf (nx*ny*2; side
+ * 1 = low face, 2 = high face), the face maps a1cf, a2cf, a3cf, the kappa
+ * map ccf and the source fcf (all device arrays). Host bookkeeping as the
+ * reference: ipc[9..11] = ipkey, 7, 1 (ipc may be NULL, else 12 ints) and
+ * *numdia = 4 (may be NULL); the unused rpc is dropped. Every interior plane
+ * is built (the reference's launch takes its k extent from ny, the same when
+ * ny == nz).
+ * Replaces pmgc::VbuildA_fv, pmgc/buildAd.cc:63-212. */
+int pmg_VbuildA_fv_d(int nx, int ny, int nz, int ipkey, int *numdia, int *ipc,
+                     double *oC, double *cc, double *fc, double *oE,
+                     double *oN, double *uC, const double *xf,
+                     const double *yf, const double *zf, const double *gxcf,
+                     const double *gycf, const double *gzcf,
+                     const double *a1cf, const double *a2cf,
+                     const double *a3cf, const double *ccf, const double *fcf,
+                     pmg_stream_t stream);
+
 /* Galerkin coarse operator A_c = P^T A_f P from a 7-point fine operator:
  * 14 coarse diagonals XoC..XuSW. Replaces pmgc::VbuildG_7,
  * pmgc/buildGd.cc:437-1361. p27 = the 27 prolongation arrays in list order,
@@ -252,6 +272,45 @@ int pmg_VbuildG_7_d(int nxf, int nyf, int nzf, int nxc, int nyc, int nzc,
 int pmg_VbuildG_27_d(int nxf, int nyf, int nzf, int nxc, int nyc, int nzc,
                      const double *const *p27, const double *const *a14,
                      double *const *out14, pmg_stream_t stream);
+
+/* ======================================================================
+ * APBS-style entry points: packed operators (device pointers)
+ *
+ * ac holds the operator's diagonals as consecutive columns of nx*ny*nz
+ * doubles: oC oE oN uC for a 7-point operator, oC oE oN uC oNE oNW uE uW uN
+ * uS uNE uNW uSE uSW for a 27-point one. ipc is a host array of at least 11
+ * ints whose ipc[10] (the reference's VAT(ipc, 11)) is 7 or 27, as
+ * pmg_VbuildA_fv_d leaves it. The unused rpc is dropped.
+ * ==================================================================== */
+
+/* y = A x on the interior, dispatched on ipc[10].
+ * Replaces pmgc::Vmatvec, pmgc/matvecd.cc:244-260. */
+int pmg_Vmatvec_d(int nx, int ny, int nz, const int *ipc, const double *ac,
+                  const double *cc, const double *x, double *y,
+                  pmg_stream_t stream);
+
+/* r = f - A x on the interior, dispatched on ipc[10].
+ * Replaces pmgc::Vmresid, pmgc/matvecd.cc:513-529. */
+int pmg_Vmresid_d(int nx, int ny, int nz, const int *ipc, const double *ac,
+                  const double *cc, const double *fc, const double *x,
+                  double *r, pmg_stream_t stream);
+
+/* Hestenes-Stiefel conjugate gradient from the initial x: r = f - A x,
+ * then iterations until ||r|| / ||r_0|| <= errtol or itmax iterations
+ * (*iters, host, gets the count). p, ap, r are work arrays of nx*ny*nz
+ * doubles (r ends as the last residual); only interior points are read or
+ * written. With itmax <= 0 and iresid == 0 nothing runs. Reads one scalar
+ * back per iteration (synchronises the stream each time), as the reference
+ * does. The reference's dot product returns x.x instead of x.y and its axpy
+ * starts its range at index 0 (pmgc/mikpckd.cc:115-129, 192-222); this
+ * implements the algorithm they document: p.Ap in the step length and
+ * updates on the interior. omega and iadjoint, unused by the reference's
+ * CG, are dropped.
+ * Replaces pmgc::Vcghs, pmgc/cgd.cc:60-125. */
+int pmg_Vcghs_d(int nx, int ny, int nz, const int *ipc, const double *ac,
+                const double *cc, const double *fc, double *x, double *p,
+                double *ap, double *r, int itmax, int *iters, double errtol,
+                int iresid, pmg_stream_t stream);
 
 /* ======================================================================
  * Class-level helpers of PBE_linear_problem (device pointers)

@@ -82,6 +82,12 @@ for _t in ("_d", "_f"):
 _sig("pmg_VbuildPb_op7_d", c_int, *([c_int] * 6 + [_V] * 31 + [_V]))
 _sig("pmg_VbuildPb_op27_d", c_int, *([c_int] * 6 + [_V] * 41 + [_V]))
 _sig("pmg_VbuildPb_trilin_d", c_int, *([c_int] * 6 + [_V] * 27 + [_V]))
+_sig("pmg_VbuildA_fv_d", c_int, *([c_int] * 4 + [PI, PI] + [_V] * 17 + [_V]))
+_sig("pmg_Vmatvec_d", c_int, *([c_int] * 3 + [PI] + [_V] * 4 + [_V]))
+_sig("pmg_Vmresid_d", c_int, *([c_int] * 3 + [PI] + [_V] * 5 + [_V]))
+_sig("pmg_Vcghs_d", c_int, *([c_int] * 3 + [PI] + [_V] * 7 + [c_int, PI,
+                                                               c_double,
+                                                               c_int, _V]))
 _PP = ctypes.POINTER(c_void_p)
 _sig("pmg_VbuildG_7_d", c_int, *([c_int] * 6 + [_PP, _V, _V, _V, _V, _PP, _V]))
 _sig("pmg_VbuildG_27_d", c_int, *([c_int] * 6 + [_PP, _PP, _PP, _V]))

@@ -20,7 +20,7 @@ LIB = os.path.join(HERE, "libpmg_b200.so")
 
 SOURCES = ["pmg_kernels.cu", "pmg_build.cu", "pmg_solver.cu", "pmg_setup.cc",
            "pmg_noalloc.cu", "pmg_runtime.cc", "pmg_setup_gpu.cu",
-           "pmg_io.cc"]
+           "pmg_io.cc", "pmg_apbs.cu"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

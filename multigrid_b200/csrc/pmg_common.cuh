@@ -165,6 +165,23 @@ template <typename T> __device__ __forceinline__ T block_sum_2d(T v, T *sh) {
     }                                                                          \
   } while (0)
 
+// Argument check of an entry point: the message, then PMG_ERR_ARG.
+#define PMG_REQUIRE(cond, msg)                                                 \
+  do {                                                                         \
+    if (!(cond)) {                                                             \
+      pmg::set_last_message(msg);                                              \
+      return PMG_ERR_ARG;                                                      \
+    }                                                                          \
+  } while (0)
+
+namespace pmg {
+// Grid sizes an entry point accepts: 3 to kMaxN points per axis.
+inline bool bad_dims(int nx, int ny, int nz) {
+  return nx < 3 || ny < 3 || nz < 3 || nx > kMaxN || ny > kMaxN ||
+         nz > kMaxN;
+}
+} // namespace pmg
+
 // Raises Kernel's dynamic shared-memory limit to `bytes` on the current
 // device, once per device (the attribute belongs to the device's context).
 template <auto Kernel> cudaError_t set_smem_limit(int bytes) {

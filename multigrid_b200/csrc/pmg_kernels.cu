@@ -5,6 +5,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include "box_builder.cuh"
 #include "build_kernels.cuh"
 #include "gs27_tiled.cuh"
 #include "launch.cuh"
@@ -367,21 +368,10 @@ using namespace pmg;
 // ---------------------------------------------------------------------------
 // argument checks
 // ---------------------------------------------------------------------------
-static bool bad_dims(int nx, int ny, int nz) {
-  return nx < 3 || ny < 3 || nz < 3 || nx > kMaxN || ny > kMaxN ||
-         nz > kMaxN;
-}
 static bool bad_pair(int nxf, int nyf, int nzf, int nxc, int nyc, int nzc) {
   return bad_dims(nxf, nyf, nzf) || bad_dims(nxc, nyc, nzc) ||
          nxf != 2 * nxc - 1 || nyf != 2 * nyc - 1 || nzf != 2 * nzc - 1;
 }
-#define PMG_REQUIRE(cond, msg)                                                 \
-  do {                                                                         \
-    if (!(cond)) {                                                             \
-      set_last_message(msg);                                                   \
-      return PMG_ERR_ARG;                                                      \
-    }                                                                          \
-  } while (0)
 
 template <typename T>
 static Op14<T> op7(const T *oC, const T *oE, const T *oN, const T *uC) {
@@ -845,6 +835,36 @@ int pmg_VbuildPb_trilin_d(int nxf, int nyf, int nzf, int nxc, int nyc,
   const Dims dc{nxc, nyc, nzc};
   buildP_trilin_kernel<<<interior_grid(dc), interior_block(), 0,
                          (cudaStream_t)stream>>>(dc, P);
+  PMG_LAUNCH_CHECK();
+  return PMG_OK;
+}
+
+int pmg_VbuildA_fv_d(int nx, int ny, int nz, int ipkey, int *numdia, int *ipc,
+                     double *oC, double *cc, double *fc, double *oE,
+                     double *oN, double *uC, const double *xf,
+                     const double *yf, const double *zf, const double *gxcf,
+                     const double *gycf, const double *gzcf,
+                     const double *a1cf, const double *a2cf,
+                     const double *a3cf, const double *ccf, const double *fcf,
+                     pmg_stream_t stream) {
+  PMG_REQUIRE(!bad_dims(nx, ny, nz), "VbuildA_fv: grid size out of range");
+  const BoxMaps m{xf, yf, zf, gxcf, gycf, gzcf, a1cf, a2cf, a3cf, ccf, fcf};
+  const BoxOps o{oC, cc, fc, oE, oN, uC};
+  PMG_REQUIRE(m.xf && m.yf && m.zf && m.gx && m.gy && m.gz && m.a1 && m.a2 &&
+                  m.a3 && m.cc && m.fc,
+              "VbuildA_fv: null input array");
+  PMG_REQUIRE(o.oC && o.cc && o.fc && o.oE && o.oN && o.uC,
+              "VbuildA_fv: null output array");
+  if (ipc) {
+    ipc[9] = ipkey;
+    ipc[10] = 7; // stencil points
+    ipc[11] = 1;
+  }
+  if (numdia)
+    *numdia = 4; // stored diagonals
+  const Dims d{nx, ny, nz};
+  buildA_fv_kernel<<<interior_grid(d), interior_block(), 0,
+                     (cudaStream_t)stream>>>(d, m, o);
   PMG_LAUNCH_CHECK();
   return PMG_OK;
 }

@@ -38,10 +38,6 @@ __device__ __forceinline__ void interior_coords(const Dims &d, int q, int &i,
 // computed its block sums v[] (valid in thread 0). The last block sums all
 // partials in block order and writes result[]; when ratio != nullptr it also
 // stores result[0] / result[1] there (NV == 2).
-// Finishes a reduction of NV values: called by every block after it has
-// computed its block sums v[] (valid in thread 0). The last block sums all
-// partials in block order and writes result[]; when ratio != nullptr it also
-// stores result[0] / result[1] there (NV == 2).
 template <int NV>
 __device__ void reduce_finish(const double (&v)[NV], ReduceSlot s,
                               double *ratio) {

@@ -158,8 +158,26 @@ __global__ void __launch_bounds__(256)
   y[p] = apply_op<KIND>(A, cc, x, p, d.sy(), d.sz());
 }
 
-// r = f - A x in the order of Vmresid7_1s / Vmresid27_1s
-// (pmgc/matvecd.cc:402-409, 491-493).
+// (f - A x)(p) in the order of Vmresid7_1s / Vmresid27_1s
+// (pmgc/matvecd.cc:402-409, 491-493); cc may be null (= 0).
+template <int KIND, typename T>
+__device__ __forceinline__ T resid_at(const Op14<T> &A, const T *cc,
+                                      const T *fc, const T *x, int p, int sy,
+                                      int sz) {
+  const T c = cc ? cc[p] : T(0);
+  if constexpr (KIND == 7) {
+    const T *oC = A.a[kOC], *oE = A.a[kOE], *oN = A.a[kON], *uC = A.a[kUC];
+    return fc[p] + oN[p] * x[p + sy] + oN[p - sy] * x[p - sy] +
+           oE[p] * x[p + 1] + oE[p - 1] * x[p - 1] + uC[p - sz] * x[p - sz] +
+           uC[p] * x[p + sz] - (oC[p] + c) * x[p];
+  } else {
+    T tO, tU, tD;
+    sums27(A, x, p, sy, sz, tO, tU, tD);
+    return fc[p] + tO + tU + tD - (A.a[kOC][p] + c) * x[p];
+  }
+}
+
+// r = f - A x on the interior (Vmresid7_1s / Vmresid27_1s).
 template <int KIND, typename T>
 __global__ void __launch_bounds__(256)
     mresid_kernel(Dims d, Op14<T> A, const T *__restrict__ cc,
@@ -168,19 +186,8 @@ __global__ void __launch_bounds__(256)
   const Interior t = interior_point(d);
   if (!t.ok)
     return;
-  const int sy = d.sy(), sz = d.sz();
   const int p = d.at(t.i, t.j, t.k);
-  const T c = cc ? cc[p] : T(0);
-  if constexpr (KIND == 7) {
-    const T *oC = A.a[kOC], *oE = A.a[kOE], *oN = A.a[kON], *uC = A.a[kUC];
-    r[p] = fc[p] + oN[p] * x[p + sy] + oN[p - sy] * x[p - sy] +
-           oE[p] * x[p + 1] + oE[p - 1] * x[p - 1] + uC[p - sz] * x[p - sz] +
-           uC[p] * x[p + sz] - (oC[p] + c) * x[p];
-  } else {
-    T tO, tU, tD;
-    sums27(A, x, p, sy, sz, tO, tU, tD);
-    r[p] = fc[p] + tO + tU + tD - (A.a[kOC][p] + c) * x[p];
-  }
+  r[p] = resid_at<KIND>(A, cc, fc, x, p, d.sy(), d.sz());
 }
 
 // ---------------------------------------------------------------------------

@@ -13,6 +13,9 @@ the reference's layout (x fastest, one-point shell). cc may be None (zero).
   VbuildPb_op7   pmgc/buildPd.cc:172-555   VbuildPb_op27 pmgc/buildPd.cc:578-1091
   VbuildPb_trilin pmgc/buildPd.cc:62-153   VbuildG_7    pmgc/buildGd.cc:437-1361
   VbuildG_27     pmgc/buildGd.cc:1363-3274
+  VbuildA_fv     pmgc/buildAd.cc:63-212
+  Vmatvec        pmgc/matvecd.cc:244-260   Vmresid      pmgc/matvecd.cc:513-529
+  Vcghs          pmgc/cgd.cc:60-125 (packed operators, APBS layer)
   cg_level       CG_Solver.h:45-242 as run by PBE_pmgc_class.h:856-860
 """
 from __future__ import annotations
@@ -122,6 +125,21 @@ def VbuildPb_trilin(nxf, nyf, nzf, nxc, nyc, nzc, p27, stream=None):
               *[_p(t) for t in p27], _s(stream))
 
 
+def VbuildA_fv(nx, ny, nz, ipkey, oC, cc, fc, oE, oN, uC, xf, yf, zf, gxcf,
+               gycf, gzcf, a1cf, a2cf, a3cf, ccf, fcf, stream=None):
+    """Box-method fine operator (outputs oC..uC written on the interior).
+    Returns (ipc, numdia): the 12-int bookkeeping array (ipc[9..11] =
+    ipkey, 7, 1) and the stored-diagonal count 4."""
+    ipc = (ctypes.c_int * 12)()
+    numdia = ctypes.c_int(-1)
+    _lib.call("pmg_VbuildA_fv_d", nx, ny, nz, int(ipkey),
+              ctypes.byref(numdia), ipc,
+              *[_p(t) for t in (oC, cc, fc, oE, oN, uC, xf, yf, zf, gxcf,
+                                gycf, gzcf, a1cf, a2cf, a3cf, ccf, fcf)],
+              _s(stream))
+    return list(ipc), numdia.value
+
+
 def VbuildG_7(nxf, nyf, nzf, nxc, nyc, nzc, p27, oC, oE, oN, uC, out14,
               stream=None):
     _lib.call("pmg_VbuildG_7_d", nxf, nyf, nzf, nxc, nyc, nzc, _pp(p27),
@@ -131,6 +149,39 @@ def VbuildG_7(nxf, nyf, nzf, nxc, nyc, nzc, p27, oC, oE, oN, uC, out14,
 def VbuildG_27(nxf, nyf, nzf, nxc, nyc, nzc, p27, op14, out14, stream=None):
     _lib.call("pmg_VbuildG_27_d", nxf, nyf, nzf, nxc, nyc, nzc, _pp(p27),
               _pp(op14), _pp(out14), _s(stream))
+
+
+def _packed(ac):
+    """ac: a contiguous (4 or 14, n^3) tensor of diagonals -> ipc, pointer."""
+    if ac.dim() != 2 or ac.shape[0] not in (4, 14):
+        raise ValueError("ac must have 4 (7-point) or 14 (27-point) rows")
+    ipc = (ctypes.c_int * 12)()
+    ipc[10] = 7 if ac.shape[0] == 4 else 27
+    return ipc, _p(ac)
+
+
+def Vmatvec(nx, ny, nz, ac, cc, x, y, stream=None):
+    """y = A x with the packed operator ac (rows oC oE oN uC [oNE .. uSW])."""
+    ipc, a = _packed(ac)
+    _lib.call("pmg_Vmatvec_d", nx, ny, nz, ipc, a, _p(cc), _p(x), _p(y),
+              _s(stream))
+
+
+def Vmresid(nx, ny, nz, ac, cc, fc, x, r, stream=None):
+    ipc, a = _packed(ac)
+    _lib.call("pmg_Vmresid_d", nx, ny, nz, ipc, a, _p(cc), _p(fc), _p(x),
+              _p(r), _s(stream))
+
+
+def Vcghs(nx, ny, nz, ac, cc, fc, x, p, ap, r, itmax, errtol, iresid=0,
+          stream=None):
+    """APBS conjugate gradient from x (updated); returns the iterations."""
+    ipc, a = _packed(ac)
+    it = ctypes.c_int(-1)
+    _lib.call("pmg_Vcghs_d", nx, ny, nz, ipc, a, _p(cc), _p(fc), _p(x),
+              _p(p), _p(ap), _p(r), int(itmax), ctypes.byref(it),
+              ctypes.c_double(errtol), int(iresid), _s(stream))
+    return it.value
 
 
 def cg_level(nx, ny, nz, op14, rhs, x, thresh=1e-8, max_iters=20000,

@@ -116,6 +116,34 @@ class Restatement:
     def buildP_trilin(self, nc, p27):
         self.lib.pmgo_buildP_trilin(nc, nc, nc, _pp(p27))
 
+    def cghs(self, nx, ny, nz, ops, cc, fc, x, itmax, errtol, iresid=0):
+        """APBS CG (Vcghs) from x (updated in place); returns (iters, r)."""
+        o = self.op(ops)
+        n3 = nx * ny * nz
+        p, ap, r = np.zeros(n3), np.zeros(n3), np.zeros(n3)
+        self.lib.pmgo_cghs.argtypes = [ctypes.c_int] * 3 + [
+            ctypes.POINTER(_PmgoOp)] + [D] * 6 + [ctypes.c_int,
+                                                  ctypes.c_double,
+                                                  ctypes.c_int]
+        it = self.lib.pmgo_cghs(nx, ny, nz, ctypes.byref(o), _d(cc), _d(fc),
+                                _d(x), _d(p), _d(ap), _d(r), int(itmax),
+                                float(errtol), int(iresid))
+        return it, r
+
+    BOX_IN = ("xf", "yf", "zf", "gxcf", "gycf", "gzcf", "a1cf", "a2cf",
+              "a3cf", "ccf", "fcf")
+
+    def buildA_fv(self, nx, ny, nz, ipkey, inputs, out6):
+        """Box-method fine builder; inputs: dict of BOX_IN arrays, out6:
+        oC cc fc oE oN uC (written on the interior). Returns (ipc,
+        numdia)."""
+        ipc = (ctypes.c_int * 12)()
+        numdia = ctypes.c_int(-1)
+        self.lib.pmgo_buildA_fv(nx, ny, nz, ipkey, ctypes.byref(numdia), ipc,
+                                *[_d(a) for a in out6],
+                                *[_d(inputs[k]) for k in self.BOX_IN])
+        return np.array(ipc[:], dtype=np.int32), numdia.value
+
     def buildG(self, nf, nc, p27, ops, out14):
         o = self.op(ops)
         self.lib.pmgo_buildG(nf, nf, nf, nc, nc, nc, _pp(p27),

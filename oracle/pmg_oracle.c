@@ -439,6 +439,76 @@ void pmgo_buildP_trilin(int nxc, int nyc, int nzc, double *const *P) {
       }
 }
 
+/* Box-method (finite volume) fine operator of the APBS driver from the
+ * harmonic coefficient maps: VbuildA_fv, pmgc/buildAd.cc:63-212. Mesh
+ * coordinates xf/yf/zf are 1-based per axis; the boundary maps are
+ * gx(j,k,side) on ny x nz x 2, gy(i,k,side) on nx x nz x 2, gz(i,j,side) on
+ * nx x ny x 2 (side 1: low face, 2: high face). Every interior point gets
+ * the face weights (product of the two transverse widths over four times
+ * the normal width), the control volume (three widths over eight), the
+ * scaled source and kappa term, the diagonal as the six weighted coupling
+ * sum, the upper couplings zeroed on the high faces, and the Dirichlet
+ * values of boundary neighbours moved into fc in the order E, N, U, W, S, D.
+ * The expressions keep the reference's operand order. All interior planes
+ * are built; the reference's launch takes its k extent from ny
+ * (buildAd.cc:116), which is the same for ny == nz. ipc[9..11] get ipkey, 7
+ * and 1, *numdia 4 (buildAd.cc:102-107). */
+void pmgo_buildA_fv(int nx, int ny, int nz, int ipkey, int *numdia, int *ipc,
+                    double *oC, double *cc, double *fc, double *oE,
+                    double *oN, double *uC, const double *xf,
+                    const double *yf, const double *zf, const double *gxcf,
+                    const double *gycf, const double *gzcf,
+                    const double *a1cf, const double *a2cf,
+                    const double *a3cf, const double *ccf,
+                    const double *fcf) {
+  if (ipc) {
+    ipc[9] = ipkey;
+    ipc[10] = 7;
+    ipc[11] = 1;
+  }
+  if (numdia)
+    *numdia = 4;
+  const double diag = 1.0;
+  for (int k = 2; k <= nz - 1; ++k)
+    for (int j = 2; j <= ny - 1; ++j)
+      for (int i = 2; i <= nx - 1; ++i) {
+        const size_t p = IX(nx, ny, i, j, k);
+        const size_t pw = IX(nx, ny, i - 1, j, k);
+        const size_t ps = IX(nx, ny, i, j - 1, k);
+        const size_t pd = IX(nx, ny, i, j, k - 1);
+        const double hzm1 = zf[k - 1] - zf[k - 2], hz = zf[k] - zf[k - 1];
+        const double hym1 = yf[j - 1] - yf[j - 2], hy = yf[j] - yf[j - 1];
+        const double hxm1 = xf[i - 1] - xf[i - 2], hx = xf[i] - xf[i - 1];
+        const double wE = diag * (hym1 + hy) * (hzm1 + hz) / (4.0 * hx);
+        const double wW = diag * (hym1 + hy) * (hzm1 + hz) / (4.0 * hxm1);
+        const double wN = diag * (hxm1 + hx) * (hzm1 + hz) / (4.0 * hy);
+        const double wS = diag * (hxm1 + hx) * (hzm1 + hz) / (4.0 * hym1);
+        const double wU = diag * (hxm1 + hx) * (hym1 + hy) / (4.0 * hz);
+        const double wD = diag * (hxm1 + hx) * (hym1 + hy) / (4.0 * hzm1);
+        const double vol =
+            diag * (hxm1 + hx) * (hym1 + hy) * (hzm1 + hz) / 8.0;
+        double f = vol * fcf[p];
+        cc[p] = vol * ccf[p];
+        oC[p] = wE * a1cf[p] + wW * a1cf[pw] + wN * a2cf[p] + wS * a2cf[ps] +
+                wU * a3cf[p] + wD * a3cf[pd];
+        const int e = i != nx - 1, n = j != ny - 1, u = k != nz - 1;
+        const int w = i != 2, s = j != 2, d = k != 2;
+        oE[p] = e * wE * a1cf[p];
+        f += (1 - e) * wE * a1cf[p] *
+             gxcf[(size_t)ny * nz + (size_t)(k - 1) * ny + (j - 1)];
+        oN[p] = n * wN * a2cf[p];
+        f += (1 - n) * wN * a2cf[p] *
+             gycf[(size_t)nx * nz + (size_t)(k - 1) * nx + (i - 1)];
+        uC[p] = u * wU * a3cf[p];
+        f += (1 - u) * wU * a3cf[p] *
+             gzcf[(size_t)nx * ny + (size_t)(j - 1) * nx + (i - 1)];
+        f += (1 - w) * wW * a1cf[pw] * gxcf[(size_t)(k - 1) * ny + (j - 1)];
+        f += (1 - s) * wS * a2cf[ps] * gycf[(size_t)(k - 1) * nx + (i - 1)];
+        f += (1 - d) * wD * a3cf[pd] * gzcf[(size_t)(j - 1) * nx + (i - 1)];
+        fc[p] = f;
+      }
+}
+
 /* ------------------------------------------------------------------------
  * Galerkin coarse operator A_c = P^T A_f P (VbuildG_7, pmgc/buildGd.cc:
  * 438-1361; VbuildG_27, :1364-3274), computed from its definition: for a
@@ -506,6 +576,69 @@ void pmgo_buildG(int nxf, int nyf, int nzf, int nxc, int nyc, int nzc,
  * is zero. An iteration cap (absent in the reference, which would loop
  * forever on stagnation) bounds the loop; returns the iterations run.
  * ---------------------------------------------------------------------- */
+/* Interior dot product (the documented Vxdot, pmgc/mikpckd.cc:192-222,
+ * whose reference body sums x.x instead), serial order. */
+static double idot(int nx, int ny, int nz, const double *a, const double *b) {
+  double s = 0.0;
+  for (int k = 2; k <= nz - 1; ++k)
+    for (int j = 2; j <= ny - 1; ++j)
+      for (int i = 2; i <= nx - 1; ++i) {
+        const size_t q = IX(nx, ny, i, j, k);
+        s += a[q] * b[q];
+      }
+  return s;
+}
+
+/* Hestenes-Stiefel CG of the APBS layer: Vcghs, pmgc/cgd.cc:60-125, with
+ * the dot products and axpys it documents (x.y; interior updates, where the
+ * reference's Vxaxpy starts its range at index 0, mikpckd.cc:115-129).
+ * r = f - A x (Vmresid order), denom = ||r||; loop: stop when
+ * ||r||/denom <= errtol or iters >= itmax; p = r on the first step, else
+ * p += (1/beta) r then p *= beta (beta = rho_k / rho_{k-1}); ap = A p
+ * (Vmatvec order, cc included); alpha = rho_k / p.ap; x += alpha p;
+ * r += (-alpha) ap. p, ap, r are caller work arrays; returns the count. */
+int pmgo_cghs(int nx, int ny, int nz, const pmgo_op *A, const double *cc,
+              const double *fc, double *x, double *p, double *ap, double *r,
+              int itmax, double errtol, int iresid) {
+  int iters = 0;
+  if (iters >= itmax && iresid == 0)
+    return 0;
+  pmgo_mresid(nx, ny, nz, A, cc, fc, x, r);
+  const double denom = sqrt(idot(nx, ny, nz, r, r));
+  if (denom == 0.0 || iters >= itmax)
+    return 0;
+  double rhok1 = 0.0;
+  for (;;) {
+    const double rhok2 = idot(nx, ny, nz, r, r);
+    if (sqrt(rhok2) / denom <= errtol || iters >= itmax)
+      break;
+    for (int k = 2; k <= nz - 1; ++k)
+      for (int j = 2; j <= ny - 1; ++j)
+        for (int i = 2; i <= nx - 1; ++i) {
+          const size_t q = IX(nx, ny, i, j, k);
+          if (iters == 0) {
+            p[q] = r[q];
+          } else {
+            const double beta = rhok2 / rhok1, inv = 1.0 / beta;
+            p[q] = (p[q] + inv * r[q]) * beta;
+          }
+        }
+    pmgo_matvec(nx, ny, nz, A, cc, p, ap);
+    const double alpha = rhok2 / idot(nx, ny, nz, p, ap);
+    rhok1 = rhok2;
+    const double malpha = -alpha;
+    for (int k = 2; k <= nz - 1; ++k)
+      for (int j = 2; j <= ny - 1; ++j)
+        for (int i = 2; i <= nx - 1; ++i) {
+          const size_t q = IX(nx, ny, i, j, k);
+          x[q] += alpha * p[q];
+          r[q] = r[q] + malpha * ap[q];
+        }
+    ++iters;
+  }
+  return iters;
+}
+
 int pmgo_cg(int nx, int ny, int nz, const pmgo_op *A, const double *rhs,
             double *x, double thresh) {
   const size_t n = (size_t)nx * ny * nz;

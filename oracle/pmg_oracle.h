@@ -47,6 +47,20 @@ void pmgo_interp2(int nxc, int nyc, int nzc, int nxf, int nyf, int nzf,
 void pmgo_buildP_op(int nxf, int nyf, int nzf, int nxc, int nyc, int nzc,
                     const pmgo_op *A, double *const *p27);
 void pmgo_buildP_trilin(int nxc, int nyc, int nzc, double *const *p27);
+/* Hestenes-Stiefel CG of the APBS layer (Vcghs, documented dot/axpy);
+ * returns the iteration count. */
+int pmgo_cghs(int nx, int ny, int nz, const pmgo_op *A, const double *cc,
+              const double *fc, double *x, double *p, double *ap, double *r,
+              int itmax, double errtol, int iresid);
+/* Box-method fine operator from coefficient maps (VbuildA_fv). */
+void pmgo_buildA_fv(int nx, int ny, int nz, int ipkey, int *numdia, int *ipc,
+                    double *oC, double *cc, double *fc, double *oE,
+                    double *oN, double *uC, const double *xf,
+                    const double *yf, const double *zf, const double *gxcf,
+                    const double *gycf, const double *gzcf,
+                    const double *a1cf, const double *a2cf,
+                    const double *a3cf, const double *ccf,
+                    const double *fcf);
 void pmgo_buildG(int nxf, int nyf, int nzf, int nxc, int nyc, int nzc,
                  const double *const *p27, const pmgo_op *A,
                  double *const *out14);

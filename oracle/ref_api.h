@@ -125,6 +125,18 @@ int pmgref_VbuildG_27(int nxf, int nyf, int nzf, int nxc, int nyc, int nzc,
                       const double *const *p27, const double *const *op14,
                       double *const *out14);
 
+/* The reference's box-method fine builder VbuildA_fv
+ * (pmgc/buildAd.cc:63-212) as compiled: ipc needs 12 ints (it writes
+ * ipc[9..11]), numdia one; rpc is unused by it. */
+int pmgref_VbuildA_fv(int nx, int ny, int nz, int ipkey, int *numdia,
+                      int *ipc, double *oC, double *cc, double *fc,
+                      double *oE, double *oN, double *uC, const double *xf,
+                      const double *yf, const double *zf, const double *gxcf,
+                      const double *gycf, const double *gzcf,
+                      const double *a1cf, const double *a2cf,
+                      const double *a3cf, const double *ccf,
+                      const double *fcf);
+
 #ifdef __cplusplus
 }
 #endif

@@ -3,6 +3,7 @@
 // wrappers over the reference's pmgc kernels. See ref_api.h.
 #include "ref_registry.h"
 
+#include "pmgc/buildAd.h"
 #include "pmgc/buildGd.h"
 #include "pmgc/buildPd.h"
 #include "pmgc/gsd.h"
@@ -248,6 +249,22 @@ int pmgref_VbuildG_27(int nxf, int nyf, int nzf, int nxc, int nyc, int nzc,
                       m(a[8]), m(a[9]), m(a[10]), m(a[11]), m(a[12]), m(a[13]),
                       o[0], o[1], o[2], o[3], o[4], o[5], o[6], o[7], o[8],
                       o[9], o[10], o[11], o[12], o[13], kq());
+  return 0;
+}
+
+int pmgref_VbuildA_fv(int nx, int ny, int nz, int ipkey, int *numdia,
+                      int *ipc, double *oC, double *cc, double *fc,
+                      double *oE, double *oN, double *uC, const double *xf,
+                      const double *yf, const double *zf, const double *gxcf,
+                      const double *gycf, const double *gzcf,
+                      const double *a1cf, const double *a2cf,
+                      const double *a3cf, const double *ccf,
+                      const double *fcf) {
+  quiet_cout q;
+  pmgc::VbuildA_fv<D>(&nx, &ny, &nz, &ipkey, numdia, ipc, nullptr, oC, cc,
+                      fc, oE, oN, uC, m(xf), m(yf), m(zf), m(gxcf), m(gycf),
+                      m(gzcf), m(a1cf), m(a2cf), m(a3cf), m(ccf), m(fcf),
+                      kq());
   return 0;
 }
 

@@ -26,6 +26,23 @@ def golden_kernels():
     return load_golden("kernels_n9.npz")
 
 
+@pytest.fixture(scope="session")
+def golden_box():
+    return load_golden("buildA_fv.npz")
+
+
+def box_case(g, tag):
+    """One VbuildA_fv case of buildA_fv.npz: sizes, ipkey, the input maps,
+    the pre-filled output arrays and the reference's outputs."""
+    nx, ny, nz = (int(g[f"{tag}_{k}"]) for k in ("nx", "ny", "nz"))
+    inputs = {k: np.ascontiguousarray(g[f"{tag}_{k}"])
+              for k in ("xf", "yf", "zf", "gxcf", "gycf", "gzcf", "a1cf",
+                        "a2cf", "a3cf", "ccf", "fcf")}
+    return dict(n=(nx, ny, nz), ipkey=int(g[f"{tag}_ipkey"]), inputs=inputs,
+                init=g[f"{tag}_init"], out=g[f"{tag}_out"],
+                ipc=g[f"{tag}_ipc"], numdia=int(g[f"{tag}_numdia"]))
+
+
 @pytest.fixture(scope="session", params=["problem_b2n3.npz",
                                          "problem_b4n3.npz"])
 def golden_problem(request):

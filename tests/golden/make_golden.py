@@ -6,7 +6,9 @@ from the reference tree), on small seeded inputs and stores inputs and
 outputs as compressed .npz files. The reference tree is only needed to
 regenerate them:
 
-    make -C oracle -j8 && python tests/golden/make_golden.py
+    make -C oracle -j8 && python tests/golden/make_golden.py [group ...]
+
+(groups: kernels, problems, box_operator; all by default).
 """
 from __future__ import annotations
 
@@ -142,10 +144,63 @@ def problems(ref: Reference) -> None:
         print(f"b{base}n{nlev}: n={n} cycles={cycles} (trilinear {ct})")
 
 
+def box_inputs(rng, nx, ny, nz):
+    """Inputs of the APBS box-method builder: non-uniform mesh lines,
+    dielectric-like face maps, kappa and source maps, boundary values, and
+    output arrays pre-filled with noise (the shell must stay untouched)."""
+    def mesh(n):
+        return np.cumsum(rng.uniform(0.3, 0.7, n)) - 5.0
+    return dict(
+        nx=nx, ny=ny, nz=nz, ipkey=3,
+        xf=mesh(nx), yf=mesh(ny), zf=mesh(nz),
+        gxcf=rng.normal(0.0, 1.0, ny * nz * 2),
+        gycf=rng.normal(0.0, 1.0, nx * nz * 2),
+        gzcf=rng.normal(0.0, 1.0, nx * ny * 2),
+        a1cf=rng.uniform(2.0, 80.0, nx * ny * nz),
+        a2cf=rng.uniform(2.0, 80.0, nx * ny * nz),
+        a3cf=rng.uniform(2.0, 80.0, nx * ny * nz),
+        ccf=rng.uniform(0.0, 0.5, nx * ny * nz),
+        fcf=rng.normal(0.0, 1.0, nx * ny * nz),
+        init=rng.normal(0.0, 1.0, (6, nx * ny * nz)))
+
+
+def box_operator(ref: Reference) -> None:
+    """VbuildA_fv (pmgc/buildAd.cc:63-212) on a cube and on a grid with
+    nx != ny (the reference's launch takes its k extent from ny, so nz ==
+    ny keeps every plane built)."""
+    import ctypes
+    D = ctypes.POINTER(ctypes.c_double)
+
+    def d(a):
+        return a.ctypes.data_as(D)
+
+    rng = np.random.default_rng(20261204)
+    out = {}
+    for tag, (nx, ny, nz) in (("c9", (9, 9, 9)), ("r11", (11, 9, 9))):
+        c = box_inputs(rng, nx, ny, nz)
+        o = c["init"].copy()
+        ipc = (ctypes.c_int * 12)()
+        numdia = ctypes.c_int(-1)
+        ref.lib.pmgref_VbuildA_fv(
+            nx, ny, nz, c["ipkey"], ctypes.byref(numdia), ipc,
+            *[d(o[s]) for s in range(6)],
+            *[d(c[k]) for k in ("xf", "yf", "zf", "gxcf", "gycf", "gzcf",
+                                "a1cf", "a2cf", "a3cf", "ccf", "fcf")])
+        for k, v in c.items():
+            out[f"{tag}_{k}"] = v
+        out[f"{tag}_out"] = o  # oC cc fc oE oN uC
+        out[f"{tag}_ipc"] = np.array(ipc[:], dtype=np.int32)
+        out[f"{tag}_numdia"] = numdia.value
+    np.savez_compressed(os.path.join(OUT, "buildA_fv.npz"), **out)
+
+
+GROUPS = {"kernels": kernels, "problems": problems,
+          "box_operator": box_operator}
+
 if __name__ == "__main__":
     ref = Reference()
-    kernels(ref)
-    problems(ref)
+    for name in sys.argv[1:] or list(GROUPS):
+        GROUPS[name](ref)
     for f in sorted(os.listdir(OUT)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(OUT, f)))

@@ -238,6 +238,80 @@ def test_float_kernels_track_double():
                                        [t(a) for a in P]), nf ** 3)
 
 
+def _box_gpu(c):
+    """Runs pmg_VbuildA_fv_d on a box_case-style dict; returns the six
+    outputs (oC cc fc oE oN uC) and the host bookkeeping."""
+    out = [T(a) for a in c["init"]]
+    inp = [T(c["inputs"][k]) for k in ("xf", "yf", "zf", "gxcf", "gycf",
+                                       "gzcf", "a1cf", "a2cf", "a3cf", "ccf",
+                                       "fcf")]
+    ipc, numdia = pmgc.VbuildA_fv(*c["n"], c["ipkey"], *out, *inp)
+    return np.stack([H(t) for t in out]), ipc, numdia
+
+
+@pytest.mark.parametrize("tag", ["c9", "r11"])
+def test_box_builder_matches_reference(golden_box, tag):
+    """VbuildA_fv (pmgc/buildAd.cc:63-212) bit for bit against the
+    reference's outputs; the shell keeps the caller's values."""
+    from conftest import box_case
+    c = box_case(golden_box, tag)
+    got, ipc, numdia = _box_gpu(c)
+    assert np.array_equal(got, c["out"])
+    assert ipc == list(c["ipc"]) and numdia == c["numdia"]
+
+
+@pytest.mark.parametrize("n", [(33, 33, 33), (65, 49, 40)])
+def test_box_builder_bitexact_vs_restatement(restatement, n):
+    from tests.golden.make_golden import box_inputs
+    c = box_inputs(np.random.default_rng(sum(n)), *n)
+    want = [np.ascontiguousarray(a) for a in c["init"].copy()]
+    restatement.buildA_fv(*n, 2, c, want)
+    got, _, _ = _box_gpu(dict(n=n, ipkey=2, inputs=c, init=c["init"]))
+    assert np.array_equal(got, np.stack(want))
+
+
+def test_packed_matvec_mresid_match_reference(golden_kernels):
+    """Vmatvec / Vmresid with the operator packed as APBS keeps it
+    (matvecd.cc:244-260, 513-529), dispatched on ipc[10]."""
+    g = golden_kernels
+    n = int(g["nf"])
+    cc, f, x = T(g["cc"]), T(g["f"]), T(g["x0"])
+    for key, ac in (("7", T(g["op7"])), ("27", T(g["op27"]))):
+        y = torch.zeros(n ** 3, dtype=torch.float64, device=DEV)
+        pmgc.Vmatvec(n, n, n, ac, cc, x, y)
+        assert np.array_equal(H(y), g["matvec" + key])
+        y.zero_()
+        pmgc.Vmresid(n, n, n, ac, cc, f, x, y)
+        assert np.array_equal(H(y), g["mresid" + key])
+
+
+@pytest.mark.parametrize("kind,n", [(7, 17), (7, 33), (27, 17)])
+def test_cghs_matches_restatement(restatement, kind, n):
+    """Vcghs (cgd.cc:60-125): the same iteration count as the CPU
+    restatement and the iterate within 1e-12 of it (the sums are ordered
+    differently); the stop by count; itmax 0 does nothing."""
+    from test_oracle import spd_case
+    ops, cc, f = spd_case(n, kind, n + kind)
+    x0 = np.random.default_rng(n).normal(size=n ** 3) * 0.1
+    xo = x0.copy()
+    it_o, _ = restatement.cghs(n, n, n, ops, cc, f, xo, 500, 1e-10)
+    ac = T(np.stack(ops))
+    work = [torch.zeros(n ** 3, dtype=torch.float64, device=DEV)
+            for _ in range(3)]
+    x = T(x0)
+    it = pmgc.Vcghs(n, n, n, ac, T(cc), T(f), x, *work, 500, 1e-10)
+    assert it == it_o and 0 < it < 500
+    assert rel(H(x), xo) <= 1e-12
+    x = T(x0)
+    assert pmgc.Vcghs(n, n, n, ac, T(cc), T(f), x, *work, 3, 1e-10) == 3
+    x = T(x0)
+    assert pmgc.Vcghs(n, n, n, ac, T(cc), T(f), x, *work, 0, 1e-10) == 0
+    assert np.array_equal(H(x), x0)
+    z = torch.zeros(n ** 3, dtype=torch.float64, device=DEV)
+    assert pmgc.Vcghs(n, n, n, ac, T(cc), z, z.clone(), *work, 10,
+                      1e-10) == 0
+
+
 def test_cg_level_matches_reference(golden_problem, restatement):
     g = golden_problem
     base = int(g["base"])

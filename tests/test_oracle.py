@@ -11,8 +11,8 @@ relative L2 with the same number of cycles.
 import numpy as np
 import pytest
 
-from conftest import fine_of
-from oracle.oracle import Reference, reference_available
+from conftest import box_case, fine_of
+from oracle.oracle import Reference, Restatement, reference_available
 
 TOL_BUILD = 1e-13   # builders: relative to the array's max magnitude
 TOL_SOLVE = 1e-12   # potential: relative L2
@@ -94,6 +94,89 @@ def test_build_galerkin(restatement, golden_kernels):
         restatement.buildG(nf, nc, P, ops, out)
         for s in range(14):
             assert rel(out[s], g[key][s]) <= TOL_BUILD, (key, s)
+
+
+@pytest.mark.parametrize("tag", ["c9", "r11"])
+def test_box_builder_bitexact(restatement, golden_box, tag):
+    """VbuildA_fv (pmgc/buildAd.cc:63-212): operator, kappa term, source
+    with the Dirichlet values folded in, bit for bit; shell untouched; the
+    ipc/numdia bookkeeping."""
+    c = box_case(golden_box, tag)
+    out = [np.ascontiguousarray(a) for a in c["init"].copy()]
+    ipc, numdia = restatement.buildA_fv(*c["n"], c["ipkey"], c["inputs"],
+                                        out)
+    assert np.array_equal(np.stack(out), c["out"])
+    assert np.array_equal(ipc, c["ipc"]) and numdia == c["numdia"]
+
+
+@pytest.mark.skipif(not reference_available(), reason="oracle/_ref not built")
+def test_box_builder_vs_reference_random():
+    import ctypes
+    from tests.golden.make_golden import box_inputs
+    rng = np.random.default_rng(77)
+    c = box_inputs(rng, 13, 17, 17)
+    want = c["init"].copy()
+    got = [np.ascontiguousarray(a) for a in c["init"].copy()]
+    ref = Reference()
+    D = ctypes.POINTER(ctypes.c_double)
+    ipc = (ctypes.c_int * 12)()
+    nd = ctypes.c_int()
+    ref.lib.pmgref_VbuildA_fv(
+        13, 17, 17, 5, ctypes.byref(nd), ipc,
+        *[want[s].ctypes.data_as(D) for s in range(6)],
+        *[c[k].ctypes.data_as(D) for k in Restatement.BOX_IN])
+    ipc2, nd2 = Restatement().buildA_fv(13, 17, 17, 5, c, got)
+    assert np.array_equal(np.stack(got), want)
+    assert list(ipc2) == list(ipc) and nd2 == nd.value
+
+
+def spd_case(n, kind, seed):
+    """A symmetric positive definite operator (strictly diagonally dominant,
+    positive couplings), kappa map, right-hand side; zero shell."""
+    rng = np.random.default_rng(seed)
+    cols = 4 if kind == 7 else 14
+    ops = [rng.uniform(0.5, 2.0, n ** 3) for _ in range(cols)]
+    ops[0] = rng.uniform(60.0, 80.0, n ** 3)
+    return ops, rng.uniform(0.0, 0.5, n ** 3), rng.normal(size=n ** 3)
+
+
+def dense_operator(n, ops, cc):
+    """The interior block of A as a dense matrix (x fastest), from the
+    restatement's matvec applied to unit vectors."""
+    m = (n - 2) ** 3
+    idx = [((k * n) + j) * n + i for k in range(1, n - 1)
+           for j in range(1, n - 1) for i in range(1, n - 1)]
+    A = np.empty((m, m))
+    r = Restatement()
+    for c, q in enumerate(idx):
+        e = np.zeros(n ** 3)
+        e[q] = 1.0
+        y = np.zeros(n ** 3)
+        r.matvec(n, ops, cc, e, y)
+        A[:, c] = y[idx]
+    return A, idx
+
+
+@pytest.mark.parametrize("kind", [7, 27])
+def test_cghs_restatement_solves_the_system(restatement, kind):
+    """Vcghs (pmgc/cgd.cc:60-125) as documented converges to the solution
+    of the interior system with a zero shell; the counted iterations stop
+    at the tolerance and at itmax."""
+    n = 7
+    ops, cc, f = spd_case(n, kind, 5 + kind)
+    A, idx = dense_operator(n, ops, cc)
+    assert np.allclose(A, A.T)
+    want = np.linalg.solve(A, f[idx])
+    x = np.zeros(n ** 3)
+    it, r = restatement.cghs(n, n, n, ops, cc, f, x, 200, 1e-12)
+    assert 0 < it < 200
+    assert np.abs(x[idx] - want).max() <= 1e-10 * np.abs(want).max()
+    assert np.sqrt(np.sum(r[idx] ** 2)) <= 1e-12 * np.sqrt(np.sum(f[idx] ** 2))
+    x3 = np.zeros(n ** 3)
+    assert restatement.cghs(n, n, n, ops, cc, f, x3, 3, 1e-12)[0] == 3
+    x0 = np.zeros(n ** 3)
+    assert restatement.cghs(n, n, n, ops, cc, f, x0, 0, 1e-12)[0] == 0
+    assert not x0.any()
 
 
 def test_hierarchy(restatement, golden_problem):
