@@ -298,8 +298,9 @@ int pmg_Vmresid_d(int nx, int ny, int nz, const int *ipc, const double *ac,
 /* Hestenes-Stiefel conjugate gradient from the initial x: r = f - A x,
  * then iterations until ||r|| / ||r_0|| <= errtol or itmax iterations
  * (*iters, host, gets the count). p, ap, r are work arrays of nx*ny*nz
- * doubles (r ends as the last residual); only interior points are read or
- * written. With itmax <= 0 and iresid == 0 nothing runs. Reads one scalar
+ * doubles (r ends as the last residual): p is cleared first (its shell
+ * must read as zero), ap and r are used on the interior. With itmax <= 0
+ * and iresid == 0 nothing runs. Reads one scalar
  * back per iteration (synchronises the stream each time), as the reference
  * does. The reference's dot product returns x.x instead of x.y and its axpy
  * starts its range at index 0 (pmgc/mikpckd.cc:115-129, 192-222); this
@@ -311,6 +312,44 @@ int pmg_Vcghs_d(int nx, int ny, int nz, const int *ipc, const double *ac,
                 const double *cc, const double *fc, double *x, double *p,
                 double *ap, double *r, int itmax, int *iters, double errtol,
                 int iresid, pmg_stream_t stream);
+
+/* The APBS iparm/rparm multigrid driver, linear case: builds the box-method
+ * fine operator from the coefficient maps (as pmg_VbuildA_fv_d), the
+ * prolongations and Galerkin operators of nlev levels, then runs V-cycles
+ * from u = 0 until the stop test passes or itmax cycles ran, and writes the
+ * boundary values onto u's shell. iparm and rparm are 0-based copies of the
+ * reference's 1-based arrays (Vpackmg order, pmgc/mgsubd.cc:538-576):
+ *   iparm[2..5] nx ny nz nlev   iparm[6..7] nu1 nu2   iparm[8] mgkey (0|1)
+ *   iparm[9] itmax   iparm[10] istop (0 absolute L1 residual, 1 relative L1
+ *   residual, 2 L1 change of the iterate, 3 L2 error against tcf)
+ *   iparm[13] ipkey   iparm[15] mode (0)   iparm[16] mgprol (0 trilinear,
+ *   1 operator-based)   iparm[17] mgcoar (2 Galerkin)   iparm[18] mgdisc
+ *   (0 box method)   iparm[19] mgsmoo (1 red-black GS, 4 CG)   iparm[20]
+ *   mgsolv (0 CG on the coarsest level)   iparm[21] iperf (0)
+ *   rparm[0] errtol
+ * Other values of those parameters return PMG_ERR_ARG (the reference leaves
+ * them untranslated or cannot build them). Level 1 is the finest; each
+ * level's cycle follows Vmvcs: nu1 GS sweeps (colours forward) and the
+ * residual going down, 100 CG iterations on the coarsest level, the
+ * Hackbusch-Reusken damped correction and nu2 sweeps with the colours
+ * reversed going up. Device arrays: u (n^3), xf/yf/zf (mesh lines), the
+ * boundary maps gxcf/gycf/gzcf, a1cf a2cf a3cf ccf fcf (n^3), tcf (the true
+ * solution; needed for istop 2/3, which overwrites it with the iterate,
+ * else may be NULL). Host outputs (may be NULL): *iters cycles, *ierror 0
+ * or 1 (itmax reached), *rsnrm the final stop ratio. Reads one scalar back
+ * per cycle and per CG iteration; synchronises the stream. The reference's
+ * helpers compute x.x for x.y, start axpys at index 0 and fill only parts of
+ * the boundary faces (pmgc/mikpckd.cc:115-312); this follows what they
+ * document.
+ * Replaces pmgc::Vmgdriv (pmgc/mgdrvd.cc:60-491) with Vbuildops
+ * (pmgc/mgsubd.cc:63-265) and Vmvcs (pmgc/mgcsd.cc:61-531); the work
+ * arrays iwork/rwork are the library's own. */
+int pmg_Vmgdriv_d(const int *iparm, const double *rparm, double *u,
+                  const double *xf, const double *yf, const double *zf,
+                  const double *gxcf, const double *gycf, const double *gzcf,
+                  const double *a1cf, const double *a2cf, const double *a3cf,
+                  const double *ccf, const double *fcf, double *tcf,
+                  int *iters, int *ierror, double *rsnrm, pmg_stream_t stream);
 
 /* ======================================================================
  * Class-level helpers of PBE_linear_problem (device pointers)

@@ -154,6 +154,8 @@ int cghs(const Dims &d, const Op14<double> &A, const double *cc,
   PMG_CUDA_TRY(scratch_alloc((void **)&w.ticket, sizeof(unsigned), s));
   PMG_CUDA_TRY(scratch_alloc((void **)&w.res, 3 * sizeof(double), s));
   PMG_CUDA_TRY(cudaMemsetAsync(w.ticket, 0, sizeof(unsigned), s));
+  // p's shell must read as zero in A p; the interior is set before use
+  PMG_CUDA_TRY(cudaMemsetAsync(pv, 0, sizeof(double) * d.count(), s));
   double *rr[2] = {w.res, w.res + 1}, *pap = w.res + 2;
   auto slot = [&](double *out) {
     return ReduceSlot{w.partials, w.ticket, out};
@@ -203,6 +205,265 @@ int cghs(const Dims &d, const Op14<double> &A, const double *cc,
   }
   return PMG_OK;
 }
+
+// ---------------------------------------------------------------------------
+// The APBS driver, linear case: Vmgdriv / Vmgdriv2 (pmgc/mgdrvd.cc:60-491),
+// Vbuildops with Galerkin coarsening (pmgc/mgsubd.cc:63-265, 349-373) and
+// the V-cycle Vmvcs (pmgc/mgcsd.cc:61-531). Levels are numbered as APBS
+// numbers them: 1 finest .. nlev coarsest.
+// ---------------------------------------------------------------------------
+
+// Two opposite faces of x from a boundary map (VfboundPMG,
+// pmgc/mikpckd.cc:266-312) or zero when g is null (VfboundPMG00, :235-264).
+// group 0: i = 1 and nx over (j, k); 1: j = 1 and ny over (i, k); 2: k = 1
+// and nz over (i, j). Launched in that order, so edges keep the later
+// group's value.
+__global__ void apbs_face_kernel(Dims d, double *__restrict__ x,
+                                 const double *__restrict__ g, int group) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int b = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int na = group == 0 ? d.ny : d.nx;
+  const int nb = group == 2 ? d.ny : d.nz;
+  if (a > na || b > nb)
+    return;
+  const long face = (long)na * nb, q = (long)(b - 1) * na + (a - 1);
+  const double lo = g ? g[q] : 0.0, hi = g ? g[face + q] : 0.0;
+  if (group == 0) {
+    x[d.at(1, a, b)] = lo;
+    x[d.at(d.nx, a, b)] = hi;
+  } else if (group == 1) {
+    x[d.at(a, 1, b)] = lo;
+    x[d.at(a, d.ny, b)] = hi;
+  } else {
+    x[d.at(a, b, 1)] = lo;
+    x[d.at(a, b, d.nz)] = hi;
+  }
+}
+
+// Interior sums of the driver's norms: mode 0 sum |a| (Vxnrm1), 1 sum a*b
+// (Vxdot as documented), 2 sum |a - b| then a = b (istop 2), 3 sum
+// (a - b)^2 (istop 3).
+__global__ void __launch_bounds__(kReduceThreads)
+    apbs_sum_kernel(Dims d, double *__restrict__ a,
+                    const double *__restrict__ b, int mode, ReduceSlot s) {
+  __shared__ double sh[32];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
+  const int k0 = 2 + blockIdx.z * kReducePlanes;
+  const int k1 = min(k0 + kReducePlanes - 1, d.nz - 1);
+  double acc = 0.0;
+  if (i <= d.nx - 1 && j <= d.ny - 1)
+    for (int k = k0; k <= k1; ++k) {
+      const int p = d.at(i, j, k);
+      if (mode == 0) {
+        acc += fabs(a[p]);
+      } else if (mode == 1) {
+        acc += a[p] * b[p];
+      } else {
+        const double v = a[p] - b[p];
+        acc += mode == 2 ? fabs(v) : v * v;
+        if (mode == 2)
+          a[p] = b[p];
+      }
+    }
+  double v[1] = {block_sum_2d(acc, sh)};
+  reduce_finish<1>(v, s, nullptr);
+}
+
+// r = f - A x (Vmresid order) and its L1 norm: the stop test of istop 0/1
+// (mgcsd.cc:467-481).
+template <int KIND>
+__global__ void __launch_bounds__(kReduceThreads)
+    apbs_resid_l1_kernel(Dims d, Op14<double> A, const double *__restrict__ cc,
+                         const double *__restrict__ fc,
+                         const double *__restrict__ x, double *__restrict__ r,
+                         ReduceSlot s) {
+  __shared__ double sh[32];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
+  const int k0 = 2 + blockIdx.z * kReducePlanes;
+  const int k1 = min(k0 + kReducePlanes - 1, d.nz - 1);
+  double acc = 0.0;
+  if (i <= d.nx - 1 && j <= d.ny - 1)
+    for (int k = k0; k <= k1; ++k) {
+      const int p = d.at(i, j, k);
+      const double v = resid_at<KIND>(A, cc, fc, x, p, d.sy(), d.sz());
+      r[p] = v;
+      acc += fabs(v);
+    }
+  double v[1] = {block_sum_2d(acc, sh)};
+  reduce_finish<1>(v, s, nullptr);
+}
+
+// Hackbusch-Reusken damping of the coarse correction (mgcsd.cc:431-439):
+// w = (x . w0) / (x . A x), A with cc (Vmatvec), over the coarse interior.
+template <int KIND>
+__global__ void __launch_bounds__(kReduceThreads)
+    apbs_damp_kernel(Dims d, Op14<double> A, const double *__restrict__ cc,
+                     const double *__restrict__ x,
+                     const double *__restrict__ w0, ReduceSlot s,
+                     double *__restrict__ w) {
+  __shared__ double sh[32];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
+  const int k0 = 2 + blockIdx.z * kReducePlanes;
+  const int k1 = min(k0 + kReducePlanes - 1, d.nz - 1);
+  double up = 0.0, lo = 0.0;
+  if (i <= d.nx - 1 && j <= d.ny - 1)
+    for (int k = k0; k <= k1; ++k) {
+      const int p = d.at(i, j, k);
+      up += x[p] * w0[p];
+      lo += x[p] * apply_op<KIND>(A, cc, x, p, d.sy(), d.sz());
+    }
+  double v[2] = {block_sum_2d(up, sh), block_sum_2d(lo, sh)};
+  reduce_finish<2>(v, s, w);
+}
+
+struct ApbsLevel {
+  Dims d;
+  int kind;     // 7 (finest) or 27 (Galerkin levels)
+  int ipc[12];  // ipc[10] = kind, for the packed-operator entry points
+  double *ac;   // 4 or 14 columns of d.count()
+  double *cc, *fc, *x, *w0;
+  double *P[27]; // prolongation from this level to the next finer one
+  const double *a(int s) const { return ac + (size_t)s * d.count(); }
+  double *aw(int s) { return ac + (size_t)s * d.count(); }
+};
+
+#define APBS_P27(P)                                                            \
+  P[0], P[1], P[2], P[3], P[4], P[5], P[6], P[7], P[8], P[9], P[10], P[11],    \
+      P[12], P[13], P[14], P[15], P[16], P[17], P[18], P[19], P[20], P[21],    \
+      P[22], P[23], P[24], P[25], P[26]
+#define APBS_A14(L)                                                            \
+  (L).a(0), (L).a(1), (L).a(2), (L).a(3), (L).a(4), (L).a(5), (L).a(6),        \
+      (L).a(7), (L).a(8), (L).a(9), (L).a(10), (L).a(11), (L).a(12), (L).a(13)
+
+Op14<double> level_op(const ApbsLevel &L) {
+  Op14<double> A{};
+  for (int s = 0; s < (L.kind == 7 ? 4 : 14); ++s)
+    A.a[s] = L.a(s);
+  return A;
+}
+
+// Largest level count with exact coarsening and more than two points per
+// axis on every level (Vmaxlev, mgsubd.cc:456-484).
+int apbs_maxlev(int n1, int n2, int n3) {
+  int lev = 0;
+  for (;;) {
+    ++lev;
+    const int iden = 1 << (lev - 1);
+    const int c[3] = {(n1 - 1) / iden + 1, (n2 - 1) / iden + 1,
+                      (n3 - 1) / iden + 1};
+    const int n[3] = {n1, n2, n3};
+    bool done = false;
+    for (int a = 0; a < 3; ++a)
+      done |= (c[a] - 1) * iden != n[a] - 1 || c[a] <= 2;
+    if (done || lev > 30)
+      return lev - 1;
+  }
+}
+
+struct ApbsDriver {
+  cudaStream_t s;
+  int nlev, mgsmoo;
+  ApbsLevel lv[13];
+  double *w1 = nullptr, *w2 = nullptr, *w3 = nullptr;
+  void *block = nullptr; // every level array and work vector
+  double *partials = nullptr, *res = nullptr;
+  unsigned *ticket = nullptr;
+  dim3 rg0;
+
+  explicit ApbsDriver(cudaStream_t st) : s(st) {}
+  ~ApbsDriver() {
+    if (block)
+      scratch_free(block, s);
+  }
+
+  ReduceSlot slot(double *out) const { return ReduceSlot{partials, ticket, out}; }
+
+  int fetch(const double *dev, double *host) {
+    PMG_CUDA_TRY(cudaMemcpyAsync(host, dev, sizeof(double),
+                                 cudaMemcpyDeviceToHost, s));
+    PMG_CUDA_TRY(cudaStreamSynchronize(s));
+    return PMG_OK;
+  }
+
+  int faces(const ApbsLevel &L, double *x, const double *gx,
+            const double *gy, const double *gz) {
+    const Dims &d = L.d;
+    const dim3 b(32, 8);
+    apbs_face_kernel<<<dim3(cdiv(d.ny, 32), cdiv(d.nz, 8)), b, 0, s>>>(
+        d, x, gx, 0);
+    apbs_face_kernel<<<dim3(cdiv(d.nx, 32), cdiv(d.nz, 8)), b, 0, s>>>(
+        d, x, gy, 1);
+    apbs_face_kernel<<<dim3(cdiv(d.nx, 32), cdiv(d.ny, 8)), b, 0, s>>>(
+        d, x, gz, 2);
+    PMG_LAUNCH_CHECK();
+    return PMG_OK;
+  }
+
+  int sum(const ApbsLevel &L, double *a, const double *b, int mode,
+          double *host) {
+    apbs_sum_kernel<<<reduce_grid(L.d), interior_block(), 0, s>>>(
+        L.d, a, b, mode, slot(res));
+    PMG_LAUNCH_CHECK();
+    return fetch(res, host);
+  }
+
+  // Vsmooth (smoothd.cc:58-87): red-black GS (then the residual into w1
+  // when iresid) or the CG with errtol 0 (its residual is w1).
+  int smooth(ApbsLevel &L, const double *f, double *x, int nu, int iadjoint,
+             int iresid) {
+    const Dims &d = L.d;
+    int rc = PMG_OK;
+    if (mgsmoo == 4) {
+      int it = 0;
+      return pmg_Vcghs_d(d.nx, d.ny, d.nz, L.ipc, L.ac, L.cc, f, x, w2, w3,
+                         w1, nu, &it, 0.0, iresid, s);
+    }
+    if (L.kind == 7)
+      rc = pmg_Vgsrb7x_d(d.nx, d.ny, d.nz, L.a(0), L.cc, f, L.a(1), L.a(2),
+                         L.a(3), x, nu, iadjoint, 0, s);
+    else
+      rc = pmg_Vgsrb27x_d(d.nx, d.ny, d.nz, L.a(0), L.cc, f, L.a(1), L.a(2),
+                          L.a(3), L.a(4), L.a(5), L.a(6), L.a(7), L.a(8),
+                          L.a(9), L.a(10), L.a(11), L.a(12), L.a(13), x, nu,
+                          0, iadjoint, s);
+    if (rc != PMG_OK || !iresid)
+      return rc;
+    if (L.kind == 7)
+      return pmg_Vmresid7_1s_d(d.nx, d.ny, d.nz, L.a(0), L.cc, f, L.a(1),
+                               L.a(2), L.a(3), x, w1, s);
+    return pmg_Vmresid27_1s_d(d.nx, d.ny, d.nz, L.a(0), L.cc, f, L.a(1),
+                              L.a(2), L.a(3), L.a(4), L.a(5), L.a(6), L.a(7),
+                              L.a(8), L.a(9), L.a(10), L.a(11), L.a(12),
+                              L.a(13), x, w1, s);
+  }
+
+  // the coarsest level's solve (mgsolv 0): 100 CG iterations from zero,
+  // errtol epsiln = 0 (mgcsd.cc:362-378)
+  int coarse(ApbsLevel &C, const double *f) {
+    PMG_CUDA_TRY(cudaMemsetAsync(C.x, 0, sizeof(double) * C.d.count(), s));
+    int it = 0;
+    return pmg_Vcghs_d(C.d.nx, C.d.ny, C.d.nz, C.ipc, C.ac, C.cc, f, C.x, w1,
+                       w2, w3, 100, &it, 0.0, 0, s);
+  }
+
+  // the stop test's numerator after a cycle (mgcsd.cc:467-519)
+  int stop_norm(int istop, double *tru, double *out) {
+    ApbsLevel &F = lv[1];
+    if (istop == 0 || istop == 1) {
+      apbs_resid_l1_kernel<7><<<reduce_grid(F.d), interior_block(), 0, s>>>(
+          F.d, level_op(F), F.cc, F.fc, F.x, w1, slot(res));
+      PMG_LAUNCH_CHECK();
+      return fetch(res, out);
+    }
+    const int rc = sum(F, tru, F.x, istop == 2 ? 2 : 3, out);
+    if (rc == PMG_OK && istop == 3)
+      *out = sqrt(*out);
+    return rc;
+  }
+};
 
 } // namespace
 } // namespace pmg
@@ -272,6 +533,214 @@ int pmg_Vcghs_d(int nx, int ny, int nz, const int *ipc, const double *ac,
                              iresid, s)
                    : cghs<27>(d, A, cc, fc, x, p, ap, r, itmax, iters, errtol,
                               iresid, s);
+}
+
+int pmg_Vmgdriv_d(const int *iparm, const double *rparm, double *u,
+                  const double *xf, const double *yf, const double *zf,
+                  const double *gxcf, const double *gycf, const double *gzcf,
+                  const double *a1cf, const double *a2cf, const double *a3cf,
+                  const double *ccf, const double *fcf, double *tcf,
+                  int *iters, int *ierror, double *rsnrm, pmg_stream_t stream) {
+  PMG_REQUIRE(iparm && rparm && u, "Vmgdriv: null iparm, rparm or u");
+  const int nx = iparm[2], ny = iparm[3], nz = iparm[4], nlev = iparm[5];
+  const int nu1 = iparm[6], nu2 = iparm[7], mgkey = iparm[8];
+  const int itmax = iparm[9], istop = iparm[10], ipkey = iparm[13];
+  const int mode = iparm[15], mgprol = iparm[16], mgcoar = iparm[17];
+  const int mgdisc = iparm[18], mgsmoo = iparm[19], mgsolv = iparm[20];
+  const int iperf = iparm[21];
+  const double errtol = rparm[0];
+  PMG_REQUIRE(!bad_dims(nx, ny, nz), "Vmgdriv: grid size out of range");
+  PMG_REQUIRE(nlev >= 1 && nlev <= 12 && nlev <= apbs_maxlev(nx, ny, nz),
+              "Vmgdriv: nlev does not coarsen the grid exactly");
+  PMG_REQUIRE(mode == 0, "Vmgdriv: only the linear mode (iparm mode 0)");
+  PMG_REQUIRE(mgkey == 0 || mgkey == 1, "Vmgdriv: mgkey must be 0 or 1");
+  PMG_REQUIRE(mgdisc == 0, "Vmgdriv: only the box method (mgdisc 0)");
+  PMG_REQUIRE(mgcoar == 2, "Vmgdriv: only Galerkin coarsening (mgcoar 2)");
+  PMG_REQUIRE(mgprol == 0 || mgprol == 1, "Vmgdriv: mgprol must be 0 or 1");
+  PMG_REQUIRE(mgsmoo == 1 || mgsmoo == 4,
+              "Vmgdriv: mgsmoo must be 1 (red-black GS) or 4 (CG)");
+  PMG_REQUIRE(mgsolv == 0, "Vmgdriv: only the CG coarse solver (mgsolv 0)");
+  PMG_REQUIRE(iperf == 0, "Vmgdriv: no eigenvalue analysis (iperf 0)");
+  PMG_REQUIRE(istop >= 0 && istop <= 3, "Vmgdriv: istop must be 0 to 3");
+  PMG_REQUIRE(istop < 2 || tcf, "Vmgdriv: istop 2 and 3 need tcf");
+  PMG_REQUIRE(nu1 >= 0 && nu2 >= 0, "Vmgdriv: negative nu1 or nu2");
+  PMG_REQUIRE(xf && yf && zf && gxcf && gycf && gzcf && a1cf && a2cf &&
+                  a3cf && ccf && fcf,
+              "Vmgdriv: null input array");
+
+  ApbsDriver D((cudaStream_t)stream);
+  const cudaStream_t s = D.s;
+  D.nlev = nlev;
+  D.mgsmoo = mgsmoo;
+  // sizes and one block for everything
+  size_t total = 0;
+  for (int L = 1; L <= nlev; ++L) {
+    ApbsLevel &v = D.lv[L];
+    v.d = L == 1 ? Dims{nx, ny, nz}
+                 : Dims{(D.lv[L - 1].d.nx - 1) / 2 + 1,
+                        (D.lv[L - 1].d.ny - 1) / 2 + 1,
+                        (D.lv[L - 1].d.nz - 1) / 2 + 1};
+    v.kind = L == 1 ? 7 : 27;
+    for (int q = 0; q < 12; ++q)
+      v.ipc[q] = 0;
+    v.ipc[10] = v.kind;
+    const size_t n = (size_t)v.d.count();
+    total += n * ((v.kind == 7 ? 4 : 14) + 3 + (L > 1 ? 1 + 27 : 0));
+  }
+  const size_t nf = (size_t)D.lv[1].d.count();
+  D.rg0 = reduce_grid(D.lv[1].d);
+  const size_t nblk = (size_t)D.rg0.x * D.rg0.y * D.rg0.z;
+  total += 3 * nf + 2 * nblk + 4;
+  PMG_CUDA_TRY(scratch_alloc(&D.block, total * sizeof(double) + 64, s));
+  PMG_CUDA_TRY(
+      cudaMemsetAsync(D.block, 0, total * sizeof(double) + 64, s));
+  double *cur = (double *)D.block;
+  auto take = [&](size_t n) {
+    double *p = cur;
+    cur += n;
+    return p;
+  };
+  for (int L = 1; L <= nlev; ++L) {
+    ApbsLevel &v = D.lv[L];
+    const size_t n = (size_t)v.d.count();
+    v.ac = take(n * (v.kind == 7 ? 4 : 14));
+    v.cc = take(n);
+    v.fc = take(n);
+    v.w0 = take(n);
+    v.x = L == 1 ? u : take(n);
+    for (int q = 0; q < 27; ++q)
+      v.P[q] = L > 1 ? take(n) : nullptr;
+  }
+  D.w1 = take(nf);
+  D.w2 = take(nf);
+  D.w3 = take(nf);
+  D.partials = take(2 * nblk);
+  D.res = take(4);
+  D.ticket = (unsigned *)cur; // zeroed with the block
+
+  // Vbuildops: the box-method fine operator, then P and the Galerkin
+  // operator per level; the coarse cc and fc are the restricted fine ones
+  ApbsLevel &F1 = D.lv[1];
+  int rc = pmg_VbuildA_fv_d(nx, ny, nz, ipkey, nullptr, nullptr, F1.aw(0),
+                            F1.cc, F1.fc, F1.aw(1), F1.aw(2), F1.aw(3), xf, yf,
+                            zf, gxcf, gycf, gzcf, a1cf, a2cf, a3cf, ccf, fcf,
+                            stream);
+  for (int L = 2; L <= nlev && rc == PMG_OK; ++L) {
+    ApbsLevel &F = D.lv[L - 1], &C = D.lv[L];
+    const Dims &df = F.d, &dc = C.d;
+    if (mgprol == 0)
+      rc = pmg_VbuildPb_trilin_d(df.nx, df.ny, df.nz, dc.nx, dc.ny, dc.nz,
+                                 APBS_P27(C.P), stream);
+    else if (F.kind == 7)
+      rc = pmg_VbuildPb_op7_d(df.nx, df.ny, df.nz, dc.nx, dc.ny, dc.nz,
+                              F.a(0), F.a(1), F.a(2), F.a(3), APBS_P27(C.P),
+                              stream);
+    else
+      rc = pmg_VbuildPb_op27_d(df.nx, df.ny, df.nz, dc.nx, dc.ny, dc.nz,
+                               APBS_A14(F), APBS_P27(C.P), stream);
+    if (rc != PMG_OK)
+      break;
+    const double *pc[27];
+    double *out[14];
+    for (int q = 0; q < 27; ++q)
+      pc[q] = C.P[q];
+    for (int q = 0; q < 14; ++q)
+      out[q] = C.aw(q);
+    if (F.kind == 7) {
+      rc = pmg_VbuildG_7_d(df.nx, df.ny, df.nz, dc.nx, dc.ny, dc.nz, pc,
+                           F.a(0), F.a(1), F.a(2), F.a(3), out, stream);
+    } else {
+      const double *a14[14];
+      for (int q = 0; q < 14; ++q)
+        a14[q] = F.a(q);
+      rc = pmg_VbuildG_27_d(df.nx, df.ny, df.nz, dc.nx, dc.ny, dc.nz, pc, a14,
+                            out, stream);
+    }
+    if (rc == PMG_OK)
+      rc = pmg_Vrestrc2_d(df.nx, df.ny, df.nz, dc.nx, dc.ny, dc.nz, F.cc,
+                          C.cc, APBS_P27(C.P), stream);
+    if (rc == PMG_OK)
+      rc = pmg_Vrestrc2_d(df.nx, df.ny, df.nz, dc.nx, dc.ny, dc.nz, F.fc,
+                          C.fc, APBS_P27(C.P), stream);
+  }
+  if (rc != PMG_OK)
+    return rc;
+
+  // u starts from zero (mgdrvd.cc:419), then Vmvcs
+  PMG_CUDA_TRY(cudaMemsetAsync(u, 0, sizeof(double) * nf, s));
+  rc = D.faces(F1, u, nullptr, nullptr, nullptr);
+  if (rc != PMG_OK)
+    return rc;
+  double rsden = 1.0;
+  if (istop == 1) {
+    rc = D.sum(F1, F1.fc, nullptr, 0, &rsden);
+  } else if (istop == 2) {
+    rsden = sqrt((double)nx * ny * nz);
+  } else if (istop == 3) {
+    rc = D.sum(F1, tcf, tcf, 1, &rsden);
+    rsden = sqrt(rsden);
+  }
+  if (rc != PMG_OK)
+    return rc;
+  if (rsden == 0.0)
+    rsden = 1.0;
+  int it = 0;
+  double rn = 0.0;
+  if (nlev == 1) {
+    rc = D.coarse(F1, F1.fc);
+    it = 1;
+    if (rc == PMG_OK)
+      rc = D.stop_norm(istop, tcf, &rn);
+  } else {
+    do {
+      rc = D.smooth(F1, F1.fc, u, nu1, 0, 1);
+      for (int L = 2; L <= nlev && rc == PMG_OK; ++L) {
+        ApbsLevel &F = D.lv[L - 1], &C = D.lv[L];
+        rc = pmg_Vrestrc2_d(F.d.nx, F.d.ny, F.d.nz, C.d.nx, C.d.ny, C.d.nz,
+                            D.w1, C.w0, APBS_P27(C.P), stream);
+        if (rc == PMG_OK && L != nlev) {
+          PMG_CUDA_TRY(
+              cudaMemsetAsync(C.x, 0, sizeof(double) * C.d.count(), s));
+          rc = D.smooth(C, C.w0, C.x, nu1, 0, 1);
+        }
+      }
+      if (rc == PMG_OK)
+        rc = D.coarse(D.lv[nlev], D.lv[nlev].w0);
+      for (int L = nlev - 1; L >= 1 && rc == PMG_OK; --L) {
+        ApbsLevel &F = D.lv[L], &C = D.lv[L + 1];
+        if (C.kind == 7)
+          apbs_damp_kernel<7><<<reduce_grid(C.d), interior_block(), 0, s>>>(
+              C.d, level_op(C), C.cc, C.x, C.w0, D.slot(D.res), D.res + 3);
+        else
+          apbs_damp_kernel<27><<<reduce_grid(C.d), interior_block(), 0, s>>>(
+              C.d, level_op(C), C.cc, C.x, C.w0, D.slot(D.res), D.res + 3);
+        P27<double> P;
+        for (int q = 0; q < 27; ++q)
+          P.p[q] = C.P[q];
+        interp_add_kernel<double, false>
+            <<<interp_grid(C.d), interior_block(), 0, s>>>(C.d, F.d, C.x, P,
+                                                           F.x, D.res + 3);
+        PMG_LAUNCH_CHECK();
+        rc = D.smooth(F, L == 1 ? F.fc : F.w0, F.x, nu2, 1, 0);
+      }
+      ++it;
+      if (rc == PMG_OK)
+        rc = D.stop_norm(istop, tcf, &rn);
+    } while (rc == PMG_OK && it < itmax && rn / rsden > errtol);
+  }
+  if (rc != PMG_OK)
+    return rc;
+  rc = D.faces(F1, u, gxcf, gycf, gzcf);
+  if (rc != PMG_OK)
+    return rc;
+  PMG_CUDA_TRY(cudaStreamSynchronize(s));
+  if (iters)
+    *iters = it;
+  if (ierror)
+    *ierror = it < itmax ? 0 : 1;
+  if (rsnrm)
+    *rsnrm = rn / rsden;
+  return PMG_OK;
 }
 
 } // extern "C"

@@ -16,6 +16,7 @@ the reference's layout (x fastest, one-point shell). cc may be None (zero).
   VbuildA_fv     pmgc/buildAd.cc:63-212
   Vmatvec        pmgc/matvecd.cc:244-260   Vmresid      pmgc/matvecd.cc:513-529
   Vcghs          pmgc/cgd.cc:60-125 (packed operators, APBS layer)
+  Vmgdriv        pmgc/mgdrvd.cc:60-491 with Vbuildops and Vmvcs (linear)
   cg_level       CG_Solver.h:45-242 as run by PBE_pmgc_class.h:856-860
 """
 from __future__ import annotations
@@ -182,6 +183,22 @@ def Vcghs(nx, ny, nz, ac, cc, fc, x, p, ap, r, itmax, errtol, iresid=0,
               _p(p), _p(ap), _p(r), int(itmax), ctypes.byref(it),
               ctypes.c_double(errtol), int(iresid), _s(stream))
     return it.value
+
+
+def Vmgdriv(iparm, rparm, u, xf, yf, zf, gxcf, gycf, gzcf, a1cf, a2cf, a3cf,
+            ccf, fcf, tcf=None, stream=None):
+    """APBS driver (linear): iparm / rparm are 0-based sequences in the
+    reference's order; u (n^3) gets the solution with its boundary values.
+    Returns (cycles, ierror, final stop ratio)."""
+    ip = (ctypes.c_int * max(len(iparm), 25))(*iparm)
+    rp = (ctypes.c_double * max(len(rparm), 12))(*rparm)
+    it, ie, rs = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+    _lib.call("pmg_Vmgdriv_d", ip, rp, _p(u),
+              *[_p(t) for t in (xf, yf, zf, gxcf, gycf, gzcf, a1cf, a2cf,
+                                a3cf, ccf, fcf)],
+              _p(tcf) if tcf is not None else None, ctypes.byref(it),
+              ctypes.byref(ie), ctypes.byref(rs), _s(stream))
+    return it.value, ie.value, rs.value
 
 
 def cg_level(nx, ny, nz, op14, rhs, x, thresh=1e-8, max_iters=20000,

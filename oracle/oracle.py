@@ -130,6 +130,23 @@ class Restatement:
                                 float(errtol), int(iresid))
         return it, r
 
+    def mgdriv(self, iparm, rparm, u, maps, tcf=None):
+        """APBS driver (linear); iparm/rparm 0-based sequences, u updated in
+        place, maps: dict of BOX_IN arrays. Returns (iters, ierror,
+        final stop ratio)."""
+        ip = (ctypes.c_int * len(iparm))(*iparm)
+        rp = (ctypes.c_double * len(rparm))(*rparm)
+        it, ie, rs = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+        self.lib.pmgo_mgdriv.restype = ctypes.c_int
+        rc = self.lib.pmgo_mgdriv(ip, rp, _d(u),
+                                  *[_d(maps[k]) for k in self.BOX_IN],
+                                  _d(tcf) if tcf is not None else None,
+                                  ctypes.byref(it), ctypes.byref(ie),
+                                  ctypes.byref(rs))
+        if rc != 0:
+            raise RuntimeError(f"pmgo_mgdriv returned {rc}")
+        return it.value, ie.value, rs.value
+
     BOX_IN = ("xf", "yf", "zf", "gxcf", "gycf", "gzcf", "a1cf", "a2cf",
               "a3cf", "ccf", "fcf")
 

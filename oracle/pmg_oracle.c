@@ -596,13 +596,17 @@ static double idot(int nx, int ny, int nz, const double *a, const double *b) {
  * ||r||/denom <= errtol or iters >= itmax; p = r on the first step, else
  * p += (1/beta) r then p *= beta (beta = rho_k / rho_{k-1}); ap = A p
  * (Vmatvec order, cc included); alpha = rho_k / p.ap; x += alpha p;
- * r += (-alpha) ap. p, ap, r are caller work arrays; returns the count. */
+ * r += (-alpha) ap. p, ap, r are caller work arrays (p is cleared first,
+ * so that its shell reads as zero); returns the count. */
 int pmgo_cghs(int nx, int ny, int nz, const pmgo_op *A, const double *cc,
               const double *fc, double *x, double *p, double *ap, double *r,
               int itmax, double errtol, int iresid) {
   int iters = 0;
   if (iters >= itmax && iresid == 0)
     return 0;
+  /* p's shell must read as zero in A p (the reference leaves whatever the
+   * work array held there) */
+  memset(p, 0, sizeof(double) * (size_t)nx * ny * nz);
   pmgo_mresid(nx, ny, nz, A, cc, fc, x, r);
   const double denom = sqrt(idot(nx, ny, nz, r, r));
   if (denom == 0.0 || iters >= itmax)
@@ -637,6 +641,266 @@ int pmgo_cghs(int nx, int ny, int nz, const pmgo_op *A, const double *cc,
     ++iters;
   }
   return iters;
+}
+
+/* ------------------------------------------------------------------------
+ * APBS iparm/rparm driver, linear case: Vmgdriv / Vmgdriv2
+ * (pmgc/mgdrvd.cc:60-491) with Vbuildops (pmgc/mgsubd.cc:63-265, Galerkin
+ * coarsening) and the V-cycle Vmvcs (pmgc/mgcsd.cc:61-531), restated with
+ * the semantics the code documents where the reference's own helpers are
+ * wrong (x.y dot products, interior axpys, all six boundary faces).
+ * Levels are numbered as APBS does: 1 finest .. nlev coarsest.
+ * ---------------------------------------------------------------------- */
+typedef struct {
+  int nx, ny, nz, kind;
+  double *a[14], *cc, *fc, *x, *w0, *P[27];
+} alevel;
+
+static double inorm1(int nx, int ny, int nz, const double *a) {
+  double s = 0.0;
+  for (int k = 2; k <= nz - 1; ++k)
+    for (int j = 2; j <= ny - 1; ++j)
+      for (int i = 2; i <= nx - 1; ++i)
+        s += fabs(a[IX(nx, ny, i, j, k)]);
+  return s;
+}
+
+static pmgo_op aop(const alevel *L) {
+  pmgo_op o;
+  o.kind = L->kind;
+  for (int s = 0; s < 14; ++s)
+    o.a[s] = L->a[s];
+  return o;
+}
+
+/* Vsmooth (smoothd.cc:58-87): meth 1 red-black GS (nu sweeps, then the
+ * residual into r when iresid), meth 4 the CG Vcghs (nu iterations,
+ * errtol 0). */
+static void asmooth(const alevel *L, const double *f, double *x, int nu,
+                    int iadjoint, int iresid, int meth, double *r, double *w2,
+                    double *w3) {
+  const pmgo_op o = aop(L);
+  if (meth == 4) {
+    pmgo_cghs(L->nx, L->ny, L->nz, &o, L->cc, f, x, w2, w3, r, nu, 0.0,
+              iresid);
+    return;
+  }
+  if (L->kind == 7)
+    pmgo_gsrb7x(L->nx, L->ny, L->nz, L->a[0], L->cc, f, L->a[1], L->a[2],
+                L->a[3], x, nu, iadjoint, 0);
+  else
+    pmgo_gsrb27x(L->nx, L->ny, L->nz, (const double *const *)L->a, L->cc, f,
+                 x, nu, iadjoint, 0);
+  if (iresid)
+    pmgo_mresid(L->nx, L->ny, L->nz, &o, L->cc, f, x, r);
+}
+
+/* Six faces of x from the boundary maps (VfboundPMG, mikpckd.cc:266-312,
+ * ibound != 0), or zero (VfboundPMG00, :235-264) when gx is NULL. */
+static void afbound(int nx, int ny, int nz, double *x, const double *gx,
+                    const double *gy, const double *gz) {
+  for (int k = 1; k <= nz; ++k)
+    for (int j = 1; j <= ny; ++j) {
+      x[IX(nx, ny, 1, j, k)] = gx ? gx[(size_t)(k - 1) * ny + (j - 1)] : 0.0;
+      x[IX(nx, ny, nx, j, k)] =
+          gx ? gx[(size_t)ny * nz + (size_t)(k - 1) * ny + (j - 1)] : 0.0;
+    }
+  for (int k = 1; k <= nz; ++k)
+    for (int i = 1; i <= nx; ++i) {
+      x[IX(nx, ny, i, 1, k)] = gy ? gy[(size_t)(k - 1) * nx + (i - 1)] : 0.0;
+      x[IX(nx, ny, i, ny, k)] =
+          gy ? gy[(size_t)nx * nz + (size_t)(k - 1) * nx + (i - 1)] : 0.0;
+    }
+  for (int j = 1; j <= ny; ++j)
+    for (int i = 1; i <= nx; ++i) {
+      x[IX(nx, ny, i, j, 1)] = gz ? gz[(size_t)(j - 1) * nx + (i - 1)] : 0.0;
+      x[IX(nx, ny, i, j, nz)] =
+          gz ? gz[(size_t)nx * ny + (size_t)(j - 1) * nx + (i - 1)] : 0.0;
+    }
+}
+
+/* The stop test's numerator after a cycle (mgcsd.cc:467-519): istop 0/1
+ * the L1 norm of f - A u, 2 the L1 norm of tru - u (then tru = u), 3 the
+ * L2 norm of tru - u. */
+static double astop(const alevel *L, int istop, const double *u, double *tru,
+                    double *w1) {
+  const int nx = L->nx, ny = L->ny, nz = L->nz;
+  if (istop == 0 || istop == 1) {
+    const pmgo_op o = aop(L);
+    pmgo_mresid(nx, ny, nz, &o, L->cc, L->fc, u, w1);
+    return inorm1(nx, ny, nz, w1);
+  }
+  double s = 0.0;
+  for (int k = 2; k <= nz - 1; ++k)
+    for (int j = 2; j <= ny - 1; ++j)
+      for (int i = 2; i <= nx - 1; ++i) {
+        const size_t q = IX(nx, ny, i, j, k);
+        const double d = tru[q] - u[q];
+        s += istop == 2 ? fabs(d) : d * d;
+        if (istop == 2)
+          tru[q] = u[q];
+      }
+  return istop == 2 ? s : sqrt(s);
+}
+
+int pmgo_mgdriv(const int *iparm, const double *rparm, double *u,
+                const double *xf, const double *yf, const double *zf,
+                const double *gxcf, const double *gycf, const double *gzcf,
+                const double *a1cf, const double *a2cf, const double *a3cf,
+                const double *ccf, const double *fcf, double *tcf,
+                int *iters_out, int *ierror_out, double *rsnrm_out) {
+  const int nx = iparm[2], ny = iparm[3], nz = iparm[4], nlev = iparm[5];
+  const int nu1 = iparm[6], nu2 = iparm[7], itmax = iparm[9];
+  const int istop = iparm[10], ipkey = iparm[13], mgprol = iparm[16];
+  const int mgsmoo = iparm[19];
+  const double errtol = rparm[0];
+  if (nlev < 1 || nlev > 12)
+    return -1;
+  alevel lv[13];
+  memset(lv, 0, sizeof(lv));
+  int ok = 1;
+  for (int L = 1; L <= nlev; ++L) {
+    alevel *v = &lv[L];
+    v->nx = L == 1 ? nx : (lv[L - 1].nx - 1) / 2 + 1;
+    v->ny = L == 1 ? ny : (lv[L - 1].ny - 1) / 2 + 1;
+    v->nz = L == 1 ? nz : (lv[L - 1].nz - 1) / 2 + 1;
+    v->kind = L == 1 ? 7 : 27;
+    const size_t n = (size_t)v->nx * v->ny * v->nz;
+    for (int s = 0; s < (v->kind == 7 ? 4 : 14); ++s)
+      ok &= (v->a[s] = calloc(n, sizeof(double))) != NULL;
+    ok &= (v->cc = calloc(n, sizeof(double))) != NULL;
+    ok &= (v->fc = calloc(n, sizeof(double))) != NULL;
+    ok &= (v->w0 = calloc(n, sizeof(double))) != NULL;
+    v->x = L == 1 ? u : calloc(n, sizeof(double));
+    ok &= v->x != NULL;
+    if (L > 1)
+      for (int s = 0; s < 27; ++s)
+        ok &= (v->P[s] = calloc(n, sizeof(double))) != NULL;
+  }
+  const size_t nf = (size_t)nx * ny * nz;
+  double *w1 = calloc(nf, sizeof(double)), *w2 = calloc(nf, sizeof(double));
+  double *w3 = calloc(nf, sizeof(double));
+  double *tru = NULL;
+  ok &= w1 && w2 && w3;
+  int iters = 0;
+  double rsnrm = 0.0;
+  if (!ok)
+    goto done;
+  /* Vbuildops: fine operator from the maps, then P and Galerkin per level;
+   * the coarse cc and fc are the restricted fine ones (Vbuildgaler0,
+   * mgsubd.cc:349-373). */
+  pmgo_buildA_fv(nx, ny, nz, ipkey, NULL, NULL, lv[1].a[0], lv[1].cc,
+                 lv[1].fc, lv[1].a[1], lv[1].a[2], lv[1].a[3], xf, yf, zf,
+                 gxcf, gycf, gzcf, a1cf, a2cf, a3cf, ccf, fcf);
+  for (int L = 2; L <= nlev; ++L) {
+    const alevel *F = &lv[L - 1];
+    alevel *C = &lv[L];
+    const pmgo_op fo = aop(F);
+    if (mgprol == 0)
+      pmgo_buildP_trilin(C->nx, C->ny, C->nz, C->P);
+    else
+      pmgo_buildP_op(F->nx, F->ny, F->nz, C->nx, C->ny, C->nz, &fo, C->P);
+    pmgo_buildG(F->nx, F->ny, F->nz, C->nx, C->ny, C->nz,
+                (const double *const *)C->P, &fo, C->a);
+    pmgo_restrc2(F->nx, F->ny, F->nz, C->nx, C->ny, C->nz, F->cc, C->cc,
+                 (const double *const *)C->P);
+    pmgo_restrc2(F->nx, F->ny, F->nz, C->nx, C->ny, C->nz, F->fc, C->fc,
+                 (const double *const *)C->P);
+  }
+  /* u starts from zero (mgdrvd.cc:419) */
+  memset(u, 0, sizeof(double) * nf);
+  afbound(nx, ny, nz, u, NULL, NULL, NULL);
+  /* Vmvcs: the stop test's denominator */
+  double rsden = 1.0;
+  if (istop == 1)
+    rsden = inorm1(nx, ny, nz, lv[1].fc);
+  else if (istop == 2)
+    rsden = sqrt((double)nx * ny * nz);
+  else if (istop == 3)
+    rsden = sqrt(idot(nx, ny, nz, tcf, tcf));
+  if (rsden == 0.0)
+    rsden = 1.0;
+  if (istop == 2 || istop == 3) {
+    tru = tcf;
+  }
+  if (nlev == 1) {
+    /* direct solve on the only level: 100 CG iterations (mgsolv 0) */
+    for (size_t q = 0; q < nf; ++q)
+      u[q] = 0.0;
+    const pmgo_op o = aop(&lv[1]);
+    pmgo_cghs(nx, ny, nz, &o, lv[1].cc, lv[1].fc, u, w1, w2, w3, 100, 0.0, 0);
+    iters = 1;
+    rsnrm = astop(&lv[1], istop, u, tru, w1);
+  } else {
+    do {
+      asmooth(&lv[1], lv[1].fc, lv[1].x, nu1, 0, 1, mgsmoo, w1, w2, w3);
+      for (int L = 2; L <= nlev; ++L) {
+        const alevel *F = &lv[L - 1];
+        alevel *C = &lv[L];
+        pmgo_restrc2(F->nx, F->ny, F->nz, C->nx, C->ny, C->nz, w1, C->w0,
+                     (const double *const *)C->P);
+        if (L != nlev) {
+          memset(C->x, 0, sizeof(double) * C->nx * C->ny * C->nz);
+          asmooth(C, C->w0, C->x, nu1, 0, 1, mgsmoo, w1, w2, w3);
+        }
+      }
+      {
+        alevel *C = &lv[nlev];
+        const pmgo_op o = aop(C);
+        memset(C->x, 0, sizeof(double) * C->nx * C->ny * C->nz);
+        pmgo_cghs(C->nx, C->ny, C->nz, &o, C->cc, C->w0, C->x, w1, w2, w3,
+                  100, 0.0, 0);
+      }
+      for (int L = nlev - 1; L >= 1; --L) {
+        alevel *F = &lv[L];
+        const alevel *C = &lv[L + 1];
+        const pmgo_op co = aop(C);
+        pmgo_matvec(C->nx, C->ny, C->nz, &co, C->cc, C->x, w2);
+        const double xdamp = idot(C->nx, C->ny, C->nz, C->x, C->w0) /
+                             idot(C->nx, C->ny, C->nz, C->x, w2);
+        memset(w1, 0, sizeof(double) * nf);
+        pmgo_interp2(C->nx, C->ny, C->nz, F->nx, F->ny, F->nz, C->x, w1,
+                     (const double *const *)C->P);
+        for (int k = 2; k <= F->nz - 1; ++k)
+          for (int j = 2; j <= F->ny - 1; ++j)
+            for (int i = 2; i <= F->nx - 1; ++i) {
+              const size_t q = IX(F->nx, F->ny, i, j, k);
+              F->x[q] = F->x[q] + xdamp * w1[q];
+            }
+        asmooth(F, L == 1 ? F->fc : F->w0, F->x, nu2, 1, 0, mgsmoo, w1, w2,
+                w3);
+      }
+      ++iters;
+      rsnrm = astop(&lv[1], istop, u, tru, w1);
+    } while (iters < itmax && rsnrm / rsden > errtol);
+  }
+  afbound(nx, ny, nz, u, gxcf, gycf, gzcf);
+done:
+  for (int L = 1; L <= nlev; ++L) {
+    alevel *v = &lv[L];
+    for (int s = 0; s < 14; ++s)
+      free(v->a[s]);
+    free(v->cc);
+    free(v->fc);
+    free(v->w0);
+    if (L > 1) {
+      free(v->x);
+      for (int s = 0; s < 27; ++s)
+        free(v->P[s]);
+    }
+  }
+  free(w1);
+  free(w2);
+  free(w3);
+  if (!ok)
+    return -2;
+  if (iters_out)
+    *iters_out = iters;
+  if (ierror_out)
+    *ierror_out = iters < itmax ? 0 : 1;
+  if (rsnrm_out)
+    *rsnrm_out = rsnrm / rsden;
+  return 0;
 }
 
 int pmgo_cg(int nx, int ny, int nz, const pmgo_op *A, const double *rhs,

@@ -52,6 +52,17 @@ void pmgo_buildP_trilin(int nxc, int nyc, int nzc, double *const *p27);
 int pmgo_cghs(int nx, int ny, int nz, const pmgo_op *A, const double *cc,
               const double *fc, double *x, double *p, double *ap, double *r,
               int itmax, double errtol, int iresid);
+/* APBS iparm/rparm driver, linear case (Vmgdriv, Vbuildops with Galerkin
+ * coarsening, Vmvcs). iparm/rparm are 0-based copies of the reference's
+ * 1-based arrays. u: n^3 in/out (solution with the boundary values on the
+ * shell); tcf: the true solution for istop 2/3 (overwritten by istop 2),
+ * else may be NULL. Returns 0, -1 (bad nlev) or -2 (out of memory). */
+int pmgo_mgdriv(const int *iparm, const double *rparm, double *u,
+                const double *xf, const double *yf, const double *zf,
+                const double *gxcf, const double *gycf, const double *gzcf,
+                const double *a1cf, const double *a2cf, const double *a3cf,
+                const double *ccf, const double *fcf, double *tcf,
+                int *iters_out, int *ierror_out, double *rsnrm_out);
 /* Box-method fine operator from coefficient maps (VbuildA_fv). */
 void pmgo_buildA_fv(int nx, int ny, int nz, int ipkey, int *numdia, int *ipc,
                     double *oC, double *cc, double *fc, double *oE,

@@ -1,0 +1,119 @@
+"""The APBS driver on the GPU (pmg_Vmgdriv_d: Vmgdriv -> Vbuildops -> Vmvcs,
+pmgc/mgdrvd.cc, pmgc/mgsubd.cc, pmgc/mgcsd.cc) against the CPU restatement
+(oracle/pmg_oracle.c pmgo_mgdriv) on the same inputs.
+
+Every kernel of the driver matches the restatement bit for bit (builders,
+smoothers, residuals, transfers); the interior sums (damping, CG dot
+products, stop norms) are added in a different order, so the cycle counts
+must agree and the potential within 1e-12 relative; the boundary faces bit
+for bit.
+"""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+pytestmark = pytest.mark.gpu
+
+if not torch.cuda.is_available():  # pragma: no cover
+    pytest.skip("no CUDA device", allow_module_level=True)
+
+from multigrid_b200 import pmgc  # noqa: E402
+from multigrid_b200._lib import PmgError  # noqa: E402
+from test_oracle import apbs_maps, apbs_params  # noqa: E402
+
+DEV = torch.device("cuda:0")
+BOX_IN = ("xf", "yf", "zf", "gxcf", "gycf", "gzcf", "a1cf", "a2cf", "a3cf",
+          "ccf", "fcf")
+
+
+def T(a):
+    return torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float64,
+                           device=DEV)
+
+
+def run_gpu(iparm, rparm, maps, n, tcf=None):
+    u = torch.full((n ** 3,), 7.0, dtype=torch.float64, device=DEV)
+    t = T(tcf) if tcf is not None else None
+    it, ierr, ratio = pmgc.Vmgdriv(iparm, rparm, u,
+                                   *[T(maps[k]) for k in BOX_IN], tcf=t)
+    torch.cuda.synchronize()
+    return u.cpu().numpy(), it, ierr, ratio, (t.cpu().numpy()
+                                              if t is not None else None)
+
+
+def rel(a, b):
+    return np.abs(a - b).max() / np.abs(b).max()
+
+
+@pytest.mark.parametrize("n,nlev,kw", [
+    (17, 3, dict()),
+    (17, 3, dict(mgprol=0)),
+    (17, 3, dict(mgsmoo=4, itmax=80)),
+    (33, 4, dict(istop=0, errtol=1e-6)),
+    (17, 2, dict(nu1=1, nu2=3, mgkey=1)),
+])
+def test_apbs_driver_matches_restatement(restatement, n, nlev, kw):
+    maps = apbs_maps(n, n + nlev)
+    iparm, rparm = apbs_params(n, nlev, **kw)
+    uo = np.zeros(n ** 3)
+    it_o, ie_o, r_o = restatement.mgdriv(iparm, rparm, uo, maps)
+    u, it, ierr, ratio, _ = run_gpu(iparm, rparm, maps, n)
+    assert (it, ierr) == (it_o, ie_o) and it > 1
+    assert rel(u, uo) <= 1e-12
+    assert abs(ratio - r_o) <= 1e-6 * r_o
+    shell = np.ones((n, n, n), bool)
+    shell[1:-1, 1:-1, 1:-1] = False
+    assert np.array_equal(u.reshape(n, n, n)[shell],
+                          uo.reshape(n, n, n)[shell])
+
+
+@pytest.mark.parametrize("istop", [2, 3])
+def test_apbs_driver_iterate_stop_tests(restatement, istop):
+    """istop 2 (L1 change of the iterate, tcf overwritten with it) and 3
+    (L2 error against a given true solution)."""
+    n, nlev = 17, 3
+    maps = apbs_maps(n, 21)
+    if istop == 2:
+        tcf = np.random.default_rng(4).normal(size=n ** 3) * 1e-3
+    else:  # the converged solution as the true one
+        tcf = np.zeros(n ** 3)
+        restatement.mgdriv(*apbs_params(n, nlev, errtol=1e-14), tcf, maps)
+    iparm, rparm = apbs_params(n, nlev, istop=istop, errtol=1e-9)
+    to = tcf.copy()
+    uo = np.zeros(n ** 3)
+    it_o, ie_o, _ = restatement.mgdriv(iparm, rparm, uo, maps, to)
+    u, it, ierr, _, t = run_gpu(iparm, rparm, maps, n, tcf)
+    assert (it, ierr) == (it_o, ie_o) and ierr == 0
+    assert rel(u, uo) <= 1e-12
+    if istop == 2:
+        assert rel(t, to) <= 1e-12
+    else:
+        assert np.array_equal(t, tcf)
+
+
+def test_apbs_driver_one_level_and_itmax(restatement):
+    n = 9
+    maps = apbs_maps(n, 2)
+    iparm, rparm = apbs_params(n, 1)
+    uo = np.zeros(n ** 3)
+    assert restatement.mgdriv(iparm, rparm, uo, maps)[0] == 1
+    u, it, ierr, _, _ = run_gpu(iparm, rparm, maps, n)
+    assert it == 1 and rel(u, uo) <= 1e-12
+    iparm, rparm = apbs_params(17, 3, itmax=2, errtol=1e-30)
+    maps = apbs_maps(17, 2)
+    _, it, ierr, _, _ = run_gpu(iparm, rparm, maps, 17)
+    assert (it, ierr) == (2, 1)
+
+
+@pytest.mark.parametrize("kw", [dict(mgcoar=0), dict(mgsolv=1),
+                                dict(mgsmoo=0), dict(mode=1), dict(nlev=5),
+                                dict(istop=4), dict(mgdisc=1)])
+def test_apbs_driver_rejects_untranslated_options(kw):
+    n = 17
+    kw = dict(kw)
+    nlev = kw.pop("nlev", 3)
+    iparm, rparm = apbs_params(n, nlev, **kw)
+    with pytest.raises(PmgError) as e:
+        run_gpu(iparm, rparm, apbs_maps(n, 1), n)
+    assert e.value.status == -1

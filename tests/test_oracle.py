@@ -179,6 +179,74 @@ def test_cghs_restatement_solves_the_system(restatement, kind):
     assert not x0.any()
 
 
+def apbs_params(n, nlev, **kw):
+    """0-based iparm / rparm of the APBS driver (Vpackmg order,
+    mgsubd.cc:538-576): linear, Galerkin coarsening, CG coarse solve."""
+    p = dict(nx=n, ny=n, nz=n, nlev=nlev, nu1=2, nu2=2, mgkey=0, itmax=60,
+             istop=1, iinfo=0, ipkey=0, mode=0, mgprol=1, mgcoar=2,
+             mgdisc=0, mgsmoo=1, mgsolv=0, iperf=0, errtol=1e-10)
+    p.update(kw)
+    iparm = [0] * 25
+    for i, k in ((2, "nx"), (3, "ny"), (4, "nz"), (5, "nlev"), (6, "nu1"),
+                 (7, "nu2"), (8, "mgkey"), (9, "itmax"), (10, "istop"),
+                 (11, "iinfo"), (13, "ipkey"), (15, "mode"), (16, "mgprol"),
+                 (17, "mgcoar"), (18, "mgdisc"), (19, "mgsmoo"),
+                 (20, "mgsolv"), (21, "iperf")):
+        iparm[i] = p[k]
+    rparm = [0.0] * 12
+    rparm[0] = p["errtol"]
+    return iparm, rparm
+
+
+def apbs_maps(n, seed, h=0.5):
+    """Box-method inputs on a uniform mesh: smooth dielectric-like face maps,
+    kappa, source and boundary values."""
+    rng = np.random.default_rng(seed)
+    g = np.arange(n) * h
+    z, y, x = np.meshgrid(g, g, g, indexing="ij")
+    eps = 2.0 + 76.0 / (1.0 + np.exp(-(np.sqrt((x - g[-1] / 2) ** 2 +
+                                               (y - g[-1] / 2) ** 2 +
+                                               (z - g[-1] / 2) ** 2) - 2.0)))
+    eps = eps.ravel()
+    return dict(xf=g.copy(), yf=g.copy(), zf=g.copy(),
+                gxcf=rng.normal(0.0, 0.1, n * n * 2),
+                gycf=rng.normal(0.0, 0.1, n * n * 2),
+                gzcf=rng.normal(0.0, 0.1, n * n * 2),
+                a1cf=eps.copy(), a2cf=eps.copy(), a3cf=eps.copy(),
+                ccf=np.full(n ** 3, 0.05), fcf=rng.normal(0.0, 1.0, n ** 3))
+
+
+@pytest.mark.parametrize("mgsmoo,mgprol", [(1, 1), (1, 0), (4, 1)])
+def test_apbs_driver_restatement_solves_the_box_system(restatement, mgsmoo,
+                                                        mgprol):
+    """The restated APBS driver (Vmgdriv -> Vbuildops -> Vmvcs) converges
+    to the direct solution of the box-method system it builds, with the
+    boundary values on the shell."""
+    n, nlev = 17, 3
+    maps = apbs_maps(n, 3)
+    iparm, rparm = apbs_params(n, nlev, mgsmoo=mgsmoo, mgprol=mgprol)
+    u = np.zeros(n ** 3)
+    it, ierr, ratio = restatement.mgdriv(iparm, rparm, u, maps)
+    assert ierr == 0 and 1 < it < 60 and ratio <= 1e-10
+    out = [np.zeros(n ** 3) for _ in range(6)]
+    restatement.buildA_fv(n, n, n, 0, maps, out)
+    oC, cc, fc, oE, oN, uC = out
+    A, idx = dense_operator(n, [oC, oE, oN, uC], cc)
+    want = np.linalg.solve(A, fc[idx])
+    assert np.abs(u[idx] - want).max() <= 1e-8 * np.abs(want).max()
+    # faces written x, then y, then z (edges keep the later face's value)
+    u3 = u.reshape(n, n, n)
+    gx = maps["gxcf"].reshape(2, n, n)
+    gy = maps["gycf"].reshape(2, n, n)
+    gz = maps["gzcf"].reshape(2, n, n)
+    c = slice(1, -1)
+    assert np.array_equal(u3[c, c, 0], gx[0, c, c])
+    assert np.array_equal(u3[c, c, -1], gx[1, c, c])
+    assert np.array_equal(u3[c, 0, :], gy[0, c, :])
+    assert np.array_equal(u3[c, -1, :], gy[1, c, :])
+    assert np.array_equal(u3[0], gz[0]) and np.array_equal(u3[-1], gz[1])
+
+
 def test_hierarchy(restatement, golden_problem):
     g = golden_problem
     base, nlev = int(g["base"]), int(g["nlev"])
