@@ -313,6 +313,34 @@ int pmg_Vcghs_d(int nx, int ny, int nz, const int *ipc, const double *ac,
                 double *ap, double *r, int itmax, int *iters, double errtol,
                 int iresid, pmg_stream_t stream);
 
+/* Band storage of a level's interior operator and its R^T R factorisation,
+ * for the direct coarse solve: acB (device, lda*n doubles with n the
+ * interior unknowns, m = (nx-2)(ny-2) for 7-point and (nx-2)(ny-2)+(nx-2)+1
+ * for 27-point operators, lda = m + 1) is zeroed, filled in LINPACK upper
+ * band storage (unknowns x fastest) and factored in place. ipcB (host, 4
+ * ints) gets n, m, lda, 1; *key (host) 0, or 1 when a pivot was not
+ * positive (the operator is not positive definite). The factorisation runs
+ * in one GPU thread in LINPACK's order; synchronises the stream. For
+ * 27-point operators the couplings are stored where the matvec reads them;
+ * the reference reads ten of them at other points (buildBd.cc:170-245).
+ * Replaces pmgc::Vbuildband, pmgc/buildBd.cc:252-303. */
+int pmg_Vbuildband_d(int *key, int nx, int ny, int nz, const int *ipc,
+                     const double *ac, int *ipcB, double *acB,
+                     pmg_stream_t stream);
+
+/* In-place R^T R factorisation of a symmetric positive definite band matrix
+ * (device abd, LINPACK upper band storage, lda >= m + 1); *info (host) 0 or
+ * the first column whose pivot was not positive. One GPU thread;
+ * synchronises the stream. Replaces pmgc::Vdpbfa, pmgc/mlinpckd.cc:168-207. */
+int pmg_Vdpbfa_d(double *abd, int lda, int n, int m, int *info,
+                 pmg_stream_t stream);
+
+/* Solves R^T R x = b in place with a factor from pmg_Vdpbfa_d (device b, n
+ * values). One GPU thread. Replaces pmgc::Vdpbsl,
+ * pmgc/mlinpckd.cc:209-240. */
+int pmg_Vdpbsl_d(const double *abd, int lda, int n, int m, double *b,
+                 pmg_stream_t stream);
+
 /* The APBS iparm/rparm multigrid driver, linear case: builds the box-method
  * fine operator from the coefficient maps (as pmg_VbuildA_fv_d), the
  * prolongations and Galerkin operators of nlev levels, then runs V-cycles
@@ -325,12 +353,14 @@ int pmg_Vcghs_d(int nx, int ny, int nz, const int *ipc, const double *ac,
  *   iparm[13] ipkey   iparm[15] mode (0)   iparm[16] mgprol (0 trilinear,
  *   1 operator-based)   iparm[17] mgcoar (2 Galerkin)   iparm[18] mgdisc
  *   (0 box method)   iparm[19] mgsmoo (1 red-black GS, 4 CG)   iparm[20]
- *   mgsolv (0 CG on the coarsest level)   iparm[21] iperf (0)
+ *   mgsolv (0 CG on the coarsest level, 1 banded direct solve as
+ *   pmg_Vbuildband_d / pmg_Vdpbsl_d)   iparm[21] iperf (0)
  *   rparm[0] errtol
  * Other values of those parameters return PMG_ERR_ARG (the reference leaves
  * them untranslated or cannot build them). Level 1 is the finest; each
  * level's cycle follows Vmvcs: nu1 GS sweeps (colours forward) and the
- * residual going down, 100 CG iterations on the coarsest level, the
+ * residual going down, 100 CG iterations (or the band solve) on the
+ * coarsest level, the
  * Hackbusch-Reusken damped correction and nu2 sweeps with the colours
  * reversed going up. Device arrays: u (n^3), xf/yf/zf (mesh lines), the
  * boundary maps gxcf/gycf/gzcf, a1cf a2cf a3cf ccf fcf (n^3), tcf (the true

@@ -89,6 +89,9 @@ _sig("pmg_Vcghs_d", c_int, *([c_int] * 3 + [PI] + [_V] * 7 + [c_int, PI,
                                                                c_double,
                                                                c_int, _V]))
 _sig("pmg_Vmgdriv_d", c_int, PI, PD, *([_V] * 13), PI, PI, PD, _V)
+_sig("pmg_Vbuildband_d", c_int, PI, c_int, c_int, c_int, PI, _V, PI, _V, _V)
+_sig("pmg_Vdpbfa_d", c_int, _V, c_int, c_int, c_int, PI, _V)
+_sig("pmg_Vdpbsl_d", c_int, _V, c_int, c_int, c_int, _V, _V)
 _PP = ctypes.POINTER(c_void_p)
 _sig("pmg_VbuildG_7_d", c_int, *([c_int] * 6 + [_PP, _V, _V, _V, _V, _PP, _V]))
 _sig("pmg_VbuildG_27_d", c_int, *([c_int] * 6 + [_PP, _PP, _PP, _V]))

@@ -319,6 +319,171 @@ __global__ void __launch_bounds__(kReduceThreads)
   reduce_finish<2>(v, s, w);
 }
 
+// ---------------------------------------------------------------------------
+// Banded direct solve of a coarsest level (APBS mgsolv 1): Vbuildband
+// (pmgc/buildBd.cc:63-303) stores the interior operator in LINPACK upper
+// band storage, abd(kk, jj) = A(ii, jj) with kk = ii - jj + m + 1 (lda = m + 1
+// rows per column, unknowns x fastest); Vdpbfa / Vdpbsl
+// (pmgc/mlinpckd.cc:168-240) factor it as R^T R and solve. The factorisation
+// and the two triangular solves are recurrences along the unknowns; they run
+// in one thread in LINPACK's order (dot products unrolled by five, Vddot
+// :113-165), bit for bit the reference's arithmetic.
+// ---------------------------------------------------------------------------
+
+// One column of the band per interior point. For 27-point operators the
+// coupling with each earlier neighbour q is read where the matvec reads it
+// (at q); the reference reads those ten at the point below or south of p
+// (buildBd.cc:170-245), which is not the operator its matvec applies.
+template <int KIND>
+__global__ void band_kernel(Dims d, Op14<double> A, double *__restrict__ abd,
+                            int m, int lda) {
+  const Interior t = interior_point(d);
+  if (!t.ok)
+    return;
+  const int i = t.i, j = t.j, k = t.k;
+  const int mx = d.nx - 2, my = d.ny - 2;
+  const int jj = (k - 2) * mx * my + (j - 2) * mx + (i - 2) + 1;
+  double *col = abd + (size_t)(jj - 1) * lda + m; // col[off] = A(jj+off, jj)
+  const double *const *a = A.a;
+  auto at = [&](int arr, int di, int dj, int dk) {
+    return a[arr][d.at(i + di, j + dj, k + dk)];
+  };
+  col[0] = at(kOC, 0, 0, 0);
+  col[-1] = -at(kOE, -1, 0, 0);
+  col[-mx] = -at(kON, 0, -1, 0);
+  if (KIND == 7) {
+    col[-mx * my] = -at(kUC, 0, 0, -1);
+    return;
+  }
+  col[-mx + 1] = -at(kONW, 1, -1, 0);
+  col[-mx - 1] = -at(kONE, -1, -1, 0);
+  col[-mx * my] = -at(kUC, 0, 0, -1);
+  col[-mx * my + 1] = -at(kUW, 1, 0, -1);
+  col[-mx * my - 1] = -at(kUE, -1, 0, -1);
+  col[-mx * my + mx] = -at(kUS, 0, 1, -1);
+  col[-mx * my - mx] = -at(kUN, 0, -1, -1);
+  col[-mx * my + mx + 1] = -at(kUSW, 1, 1, -1);
+  col[-mx * my + mx - 1] = -at(kUSE, -1, 1, -1);
+  col[-mx * my - mx + 1] = -at(kUNW, 1, -1, -1);
+  col[-mx * my - mx - 1] = -at(kUNE, -1, -1, -1);
+}
+
+// LINPACK's unit-stride dot product: the first n % 5 terms one by one, then
+// five-term groups summed left to right and added (Vddot).
+__device__ double ddot5(int n, const double *x, const double *y) {
+  double t = 0.0;
+  if (n <= 0)
+    return 0.0;
+  const int r = n % 5;
+  for (int q = 0; q < r; ++q)
+    t += x[q] * y[q];
+  if (n < 5)
+    return t;
+  for (int q = r; q < n; q += 5)
+    t += x[q] * y[q] + x[q + 1] * y[q + 1] + x[q + 2] * y[q + 2] +
+         x[q + 3] * y[q + 3] + x[q + 4] * y[q + 4];
+  return t;
+}
+
+#define ABD(r, c) abd[(size_t)((c) - 1) * lda + ((r) - 1)]
+
+// Vdpbfa in one thread; *info = 0 or the first column with a pivot <= 0
+__global__ void dpbfa_kernel(double *abd, int lda, int n, int m, int *info) {
+  *info = 0;
+  for (int j = 1; j <= n; ++j) {
+    double s = 0.0;
+    int ik = m + 1;
+    int jk = max(j - m, 1);
+    const int mu = max(m + 2 - j, 1);
+    for (int k = mu; k <= m; ++k) {
+      double t = ABD(k, j) - ddot5(k - mu, &ABD(ik, jk), &ABD(mu, j));
+      t /= ABD(m + 1, jk);
+      ABD(k, j) = t;
+      s += t * t;
+      --ik;
+      ++jk;
+    }
+    s = ABD(m + 1, j) - s;
+    if (s <= 0.0) {
+      *info = j;
+      return;
+    }
+    ABD(m + 1, j) = sqrt(s);
+  }
+}
+
+// Vdpbsl in one thread: R^T y = b, then R x = y, in place
+__global__ void dpbsl_kernel(const double *abd, int lda, int n, int m,
+                             double *b) {
+  for (int k = 1; k <= n; ++k) {
+    const int lm = min(k - 1, m), la = m + 1 - lm, lb = k - lm;
+    const double t = ddot5(lm, &ABD(la, k), &b[lb - 1]);
+    b[k - 1] = (b[k - 1] - t) / ABD(m + 1, k);
+  }
+  for (int kb = 1; kb <= n; ++kb) {
+    const int k = n + 1 - kb;
+    const int lm = min(k - 1, m), la = m + 1 - lm, lb = k - lm;
+    b[k - 1] /= ABD(m + 1, k);
+    const double t = -b[k - 1];
+    if (lm > 0 && t != 0.0) // Vdaxpy returns early for a zero factor
+      for (int q = 0; q < lm; ++q)
+        b[lb - 1 + q] += t * ABD(la + q, k);
+  }
+}
+#undef ABD
+
+// interior of x <-> compact vector of the interior unknowns (Vxcopy_small
+// with to_compact, Vxcopy_large without; pmgc/mikpckd.cc:78-113)
+__global__ void compact_kernel(Dims d, double *__restrict__ x,
+                               double *__restrict__ b, int to_compact) {
+  const Interior t = interior_point(d);
+  if (!t.ok)
+    return;
+  const long q = ((long)(t.k - 2) * (d.ny - 2) + (t.j - 2)) * (d.nx - 2) +
+                 (t.i - 2);
+  const int p = d.at(t.i, t.j, t.k);
+  if (to_compact)
+    b[q] = x[p];
+  else
+    x[p] = b[q];
+}
+
+// band sizes of a grid's interior operator (Vbuildband, buildBd.cc:262-280)
+void band_dims(const Dims &d, int kind, int *n, int *m, int *lda) {
+  const int mx = d.nx - 2, my = d.ny - 2;
+  *n = mx * my * (d.nz - 2);
+  *m = kind == 7 ? mx * my : mx * my + mx + 1;
+  *lda = *m + 1;
+}
+
+// zeroes abd, stores the band and factors it; *info read back (synchronises)
+int band_factor(const Dims &d, int kind, const Op14<double> &A, double *abd,
+                int *info, cudaStream_t s) {
+  int n, m, lda;
+  band_dims(d, kind, &n, &m, &lda);
+  PMG_CUDA_TRY(cudaMemsetAsync(abd, 0, sizeof(double) * lda * n, s));
+  if (kind == 7)
+    band_kernel<7><<<interior_grid(d), interior_block(), 0, s>>>(d, A, abd, m,
+                                                                lda);
+  else
+    band_kernel<27><<<interior_grid(d), interior_block(), 0, s>>>(d, A, abd,
+                                                                 m, lda);
+  int *dinfo = nullptr;
+  PMG_CUDA_TRY(scratch_alloc((void **)&dinfo, sizeof(int), s));
+  dpbfa_kernel<<<1, 1, 0, s>>>(abd, lda, n, m, dinfo);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(info, dinfo, sizeof(int), cudaMemcpyDeviceToHost, s);
+  scratch_free(dinfo, s);
+  if (e == cudaSuccess)
+    e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) {
+    set_last_error(e, "Vbuildband", __FILE__, __LINE__);
+    return PMG_ERR_CUDA;
+  }
+  return PMG_OK;
+}
+
 struct ApbsLevel {
   Dims d;
   int kind;     // 7 (finest) or 27 (Galerkin levels)
@@ -365,7 +530,9 @@ int apbs_maxlev(int n1, int n2, int n3) {
 
 struct ApbsDriver {
   cudaStream_t s;
-  int nlev, mgsmoo;
+  int nlev, mgsmoo, mgsolv = 0;
+  double *band = nullptr; // factored band of the coarsest level (mgsolv 1)
+  int bn = 0, bm = 0, blda = 0;
   ApbsLevel lv[13];
   double *w1 = nullptr, *w2 = nullptr, *w3 = nullptr;
   void *block = nullptr; // every level array and work vector
@@ -440,9 +607,19 @@ struct ApbsDriver {
                               L.a(13), x, w1, s);
   }
 
-  // the coarsest level's solve (mgsolv 0): 100 CG iterations from zero,
-  // errtol epsiln = 0 (mgcsd.cc:362-378)
+  // the coarsest level's solve: mgsolv 0, 100 CG iterations from zero with
+  // errtol epsiln = 0 (mgcsd.cc:362-378); mgsolv 1, the banded direct solve
+  // of the interior, boundary zero (:380-405)
   int coarse(ApbsLevel &C, const double *f) {
+    if (mgsolv == 1) {
+      compact_kernel<<<interior_grid(C.d), interior_block(), 0, s>>>(
+          C.d, const_cast<double *>(f), w1, 1);
+      dpbsl_kernel<<<1, 1, 0, s>>>(band, blda, bn, bm, w1);
+      compact_kernel<<<interior_grid(C.d), interior_block(), 0, s>>>(
+          C.d, C.x, w1, 0);
+      PMG_LAUNCH_CHECK();
+      return faces(C, C.x, nullptr, nullptr, nullptr);
+    }
     PMG_CUDA_TRY(cudaMemsetAsync(C.x, 0, sizeof(double) * C.d.count(), s));
     int it = 0;
     return pmg_Vcghs_d(C.d.nx, C.d.ny, C.d.nz, C.ipc, C.ac, C.cc, f, C.x, w1,
@@ -535,6 +712,60 @@ int pmg_Vcghs_d(int nx, int ny, int nz, const int *ipc, const double *ac,
                               iresid, s);
 }
 
+int pmg_Vbuildband_d(int *key, int nx, int ny, int nz, const int *ipc,
+                     const double *ac, int *ipcB, double *acB,
+                     pmg_stream_t stream) {
+  PMG_REQUIRE(!bad_dims(nx, ny, nz), "Vbuildband: grid size out of range");
+  PMG_REQUIRE(key && ipcB && acB, "Vbuildband: null key, ipcB or acB");
+  const Dims d{nx, ny, nz};
+  int kind = 0;
+  Op14<double> A;
+  int rc = unpack(ipc, ac, d.count(), &kind, &A);
+  if (rc != PMG_OK)
+    return rc;
+  int n, m, lda, info = 0;
+  band_dims(d, kind, &n, &m, &lda);
+  rc = band_factor(d, kind, A, acB, &info, (cudaStream_t)stream);
+  if (rc != PMG_OK)
+    return rc;
+  ipcB[0] = n;
+  ipcB[1] = m;
+  ipcB[2] = lda;
+  ipcB[3] = 1; // factored
+  *key = info != 0;
+  return PMG_OK;
+}
+
+int pmg_Vdpbfa_d(double *abd, int lda, int n, int m, int *info,
+                 pmg_stream_t stream) {
+  PMG_REQUIRE(abd && info, "Vdpbfa: null abd or info");
+  PMG_REQUIRE(n >= 0 && m >= 0 && lda >= m + 1, "Vdpbfa: bad n, m or lda");
+  const cudaStream_t s = (cudaStream_t)stream;
+  int *dinfo = nullptr;
+  PMG_CUDA_TRY(scratch_alloc((void **)&dinfo, sizeof(int), s));
+  dpbfa_kernel<<<1, 1, 0, s>>>(abd, lda, n, m, dinfo);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(info, dinfo, sizeof(int), cudaMemcpyDeviceToHost, s);
+  scratch_free(dinfo, s);
+  if (e == cudaSuccess)
+    e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) {
+    set_last_error(e, "Vdpbfa", __FILE__, __LINE__);
+    return PMG_ERR_CUDA;
+  }
+  return PMG_OK;
+}
+
+int pmg_Vdpbsl_d(const double *abd, int lda, int n, int m, double *b,
+                 pmg_stream_t stream) {
+  PMG_REQUIRE(abd && b, "Vdpbsl: null abd or b");
+  PMG_REQUIRE(n >= 0 && m >= 0 && lda >= m + 1, "Vdpbsl: bad n, m or lda");
+  dpbsl_kernel<<<1, 1, 0, (cudaStream_t)stream>>>(abd, lda, n, m, b);
+  PMG_LAUNCH_CHECK();
+  return PMG_OK;
+}
+
 int pmg_Vmgdriv_d(const int *iparm, const double *rparm, double *u,
                   const double *xf, const double *yf, const double *zf,
                   const double *gxcf, const double *gycf, const double *gzcf,
@@ -559,7 +790,8 @@ int pmg_Vmgdriv_d(const int *iparm, const double *rparm, double *u,
   PMG_REQUIRE(mgprol == 0 || mgprol == 1, "Vmgdriv: mgprol must be 0 or 1");
   PMG_REQUIRE(mgsmoo == 1 || mgsmoo == 4,
               "Vmgdriv: mgsmoo must be 1 (red-black GS) or 4 (CG)");
-  PMG_REQUIRE(mgsolv == 0, "Vmgdriv: only the CG coarse solver (mgsolv 0)");
+  PMG_REQUIRE(mgsolv == 0 || mgsolv == 1,
+              "Vmgdriv: mgsolv must be 0 (CG) or 1 (banded direct)");
   PMG_REQUIRE(iperf == 0, "Vmgdriv: no eigenvalue analysis (iperf 0)");
   PMG_REQUIRE(istop >= 0 && istop <= 3, "Vmgdriv: istop must be 0 to 3");
   PMG_REQUIRE(istop < 2 || tcf, "Vmgdriv: istop 2 and 3 need tcf");
@@ -572,6 +804,7 @@ int pmg_Vmgdriv_d(const int *iparm, const double *rparm, double *u,
   const cudaStream_t s = D.s;
   D.nlev = nlev;
   D.mgsmoo = mgsmoo;
+  D.mgsolv = mgsolv;
   // sizes and one block for everything
   size_t total = 0;
   for (int L = 1; L <= nlev; ++L) {
@@ -591,6 +824,10 @@ int pmg_Vmgdriv_d(const int *iparm, const double *rparm, double *u,
   D.rg0 = reduce_grid(D.lv[1].d);
   const size_t nblk = (size_t)D.rg0.x * D.rg0.y * D.rg0.z;
   total += 3 * nf + 2 * nblk + 4;
+  if (mgsolv == 1) {
+    band_dims(D.lv[nlev].d, D.lv[nlev].kind, &D.bn, &D.bm, &D.blda);
+    total += (size_t)D.blda * D.bn;
+  }
   PMG_CUDA_TRY(scratch_alloc(&D.block, total * sizeof(double) + 64, s));
   PMG_CUDA_TRY(
       cudaMemsetAsync(D.block, 0, total * sizeof(double) + 64, s));
@@ -616,6 +853,8 @@ int pmg_Vmgdriv_d(const int *iparm, const double *rparm, double *u,
   D.w3 = take(nf);
   D.partials = take(2 * nblk);
   D.res = take(4);
+  if (mgsolv == 1)
+    D.band = take((size_t)D.blda * D.bn);
   D.ticket = (unsigned *)cur; // zeroed with the block
 
   // Vbuildops: the box-method fine operator, then P and the Galerkin
@@ -662,6 +901,14 @@ int pmg_Vmgdriv_d(const int *iparm, const double *rparm, double *u,
     if (rc == PMG_OK)
       rc = pmg_Vrestrc2_d(df.nx, df.ny, df.nz, dc.nx, dc.ny, dc.nz, F.fc,
                           C.fc, APBS_P27(C.P), stream);
+  }
+  if (rc == PMG_OK && mgsolv == 1) {
+    // Vbuildband on the coarsest level, factored (mgsubd.cc:245-262)
+    int info = 0;
+    ApbsLevel &C = D.lv[nlev];
+    rc = band_factor(C.d, C.kind, level_op(C), D.band, &info, s);
+    PMG_REQUIRE(rc != PMG_OK || info == 0,
+                "Vmgdriv: the coarsest operator is not positive definite");
   }
   if (rc != PMG_OK)
     return rc;

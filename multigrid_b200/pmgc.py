@@ -17,6 +17,7 @@ the reference's layout (x fastest, one-point shell). cc may be None (zero).
   Vmatvec        pmgc/matvecd.cc:244-260   Vmresid      pmgc/matvecd.cc:513-529
   Vcghs          pmgc/cgd.cc:60-125 (packed operators, APBS layer)
   Vmgdriv        pmgc/mgdrvd.cc:60-491 with Vbuildops and Vmvcs (linear)
+  Vbuildband     pmgc/buildBd.cc:252-303   Vdpbfa, Vdpbsl pmgc/mlinpckd.cc
   cg_level       CG_Solver.h:45-242 as run by PBE_pmgc_class.h:856-860
 """
 from __future__ import annotations
@@ -183,6 +184,28 @@ def Vcghs(nx, ny, nz, ac, cc, fc, x, p, ap, r, itmax, errtol, iresid=0,
               _p(p), _p(ap), _p(r), int(itmax), ctypes.byref(it),
               ctypes.c_double(errtol), int(iresid), _s(stream))
     return it.value
+
+
+def Vbuildband(nx, ny, nz, ac, acB, stream=None):
+    """Band storage and factorisation of the packed operator ac into acB;
+    returns (key, [n, m, lda, 1])."""
+    ipc, a = _packed(ac)
+    key = ctypes.c_int(-1)
+    ipcB = (ctypes.c_int * 4)()
+    _lib.call("pmg_Vbuildband_d", ctypes.byref(key), nx, ny, nz, ipc, a,
+              ipcB, _p(acB), _s(stream))
+    return key.value, list(ipcB)
+
+
+def Vdpbfa(abd, lda, n, m, stream=None):
+    info = ctypes.c_int(-1)
+    _lib.call("pmg_Vdpbfa_d", _p(abd), lda, n, m, ctypes.byref(info),
+              _s(stream))
+    return info.value
+
+
+def Vdpbsl(abd, lda, n, m, b, stream=None):
+    _lib.call("pmg_Vdpbsl_d", _p(abd), lda, n, m, _p(b), _s(stream))
 
 
 def Vmgdriv(iparm, rparm, u, xf, yf, zf, gxcf, gycf, gzcf, a1cf, a2cf, a3cf,

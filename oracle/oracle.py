@@ -147,6 +147,25 @@ class Restatement:
             raise RuntimeError(f"pmgo_mgdriv returned {rc}")
         return it.value, ie.value, rs.value
 
+    def buildband(self, n, ops):
+        """Band storage of the interior operator (not yet factored);
+        returns (abd, nb, m, lda)."""
+        o = self.op(ops)
+        mx = n - 2
+        m = mx * mx if len(ops) == 4 else mx * mx + mx + 1
+        abd = np.zeros((m + 1) * mx ** 3)
+        nn, mm, ll = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        self.lib.pmgo_buildband(n, n, n, ctypes.byref(o), ctypes.byref(nn),
+                                ctypes.byref(mm), ctypes.byref(ll), _d(abd))
+        return abd, nn.value, mm.value, ll.value
+
+    def dpbfa(self, abd, lda, n, m):
+        self.lib.pmgo_dpbfa.restype = ctypes.c_int
+        return self.lib.pmgo_dpbfa(_d(abd), lda, n, m)
+
+    def dpbsl(self, abd, lda, n, m, b):
+        self.lib.pmgo_dpbsl(_d(abd), lda, n, m, _d(b))
+
     BOX_IN = ("xf", "yf", "zf", "gxcf", "gycf", "gzcf", "a1cf", "a2cf",
               "a3cf", "ccf", "fcf")
 

@@ -644,6 +644,124 @@ int pmgo_cghs(int nx, int ny, int nz, const pmgo_op *A, const double *cc,
 }
 
 /* ------------------------------------------------------------------------
+ * Banded direct solve of a coarsest level (the APBS mgsolv 1 path):
+ * Vbuildband (pmgc/buildBd.cc:63-303) stores the interior operator in
+ * LINPACK upper band storage, abd(kk, jj) = A(ii, jj) with kk = ii - jj +
+ * m + 1 (1-based, lda = m + 1 rows per column), unknowns ordered x fastest;
+ * Vdpbfa / Vdpbsl (pmgc/mlinpckd.cc:168-240) factor it as R^T R and solve.
+ * The dot products keep LINPACK's unrolled order (Vddot, :113-165).
+ * ---------------------------------------------------------------------- */
+static double ddot5(int n, const double *x, const double *y) {
+  double t = 0.0;
+  if (n <= 0)
+    return 0.0;
+  const int r = n % 5;
+  for (int i = 0; i < r; ++i)
+    t += x[i] * y[i];
+  if (n < 5)
+    return t;
+  for (int i = r; i < n; i += 5)
+    t += x[i] * y[i] + x[i + 1] * y[i + 1] + x[i + 2] * y[i + 2] +
+         x[i + 3] * y[i + 3] + x[i + 4] * y[i + 4];
+  return t;
+}
+
+/* Band storage of the interior operator (the caller zeroes abd, lda*n).
+ * Couplings are written for every listed offset, also where the offset
+ * wraps to the previous row or plane (there the coefficient read is a shell
+ * one, zero for operators built on the interior), as the reference writes
+ * them. For 27-point operators the reference reads the ten diagonal
+ * couplings at the point below or south of p (buildBd.cc:170-245), which
+ * is not the operator its matvec applies; this stores the coupling with
+ * each earlier neighbour q where the matvec reads it, at q. */
+void pmgo_buildband(int nx, int ny, int nz, const pmgo_op *A, int *n_out,
+                    int *m_out, int *lda_out, double *abd) {
+  const int mx = nx - 2, my = ny - 2;
+  const int n = mx * my * (nz - 2);
+  const int m = A->kind == 7 ? mx * my : mx * my + mx + 1, lda = m + 1;
+  const double *const *a = A->a;
+  *n_out = n;
+  *m_out = m;
+  *lda_out = lda;
+  for (int k = 2; k <= nz - 1; ++k)
+    for (int j = 2; j <= ny - 1; ++j)
+      for (int i = 2; i <= nx - 1; ++i) {
+        const int jj = (k - 2) * mx * my + (j - 2) * mx + (i - 2) + 1;
+        double *col = abd + (size_t)(jj - 1) * lda;
+        /* row offset ii - jj, coefficient array, its point (di, dj, dk) */
+#define BAND(off, arr, di, dj, dk, sign)                                       \
+  col[(off) + m] = sign a[arr][IX(nx, ny, i + (di), j + (dj), k + (dk))]
+        BAND(0, 0, 0, 0, 0, +);
+        BAND(-1, 1, -1, 0, 0, -);
+        BAND(-mx, 2, 0, -1, 0, -);
+        if (A->kind == 7) {
+          BAND(-mx * my, 3, 0, 0, -1, -);
+          continue;
+        }
+        /* the coupling with the earlier neighbour q = p + d is stored at q
+         * as the diagonal pointing back to p (the matvec's convention) */
+        BAND(-mx + 1, 5, 1, -1, 0, -);      /* oNW(i+1, j-1, k)   */
+        BAND(-mx - 1, 4, -1, -1, 0, -);     /* oNE(i-1, j-1, k)   */
+        BAND(-mx * my, 3, 0, 0, -1, -);     /* uC(i, j, k-1)      */
+        BAND(-mx * my + 1, 7, 1, 0, -1, -); /* uW(i+1, j, k-1)    */
+        BAND(-mx * my - 1, 6, -1, 0, -1, -); /* uE(i-1, j, k-1)   */
+        BAND(-mx * my + mx, 9, 0, 1, -1, -); /* uS(i, j+1, k-1)   */
+        BAND(-mx * my - mx, 8, 0, -1, -1, -); /* uN(i, j-1, k-1)  */
+        BAND(-mx * my + mx + 1, 13, 1, 1, -1, -);  /* uSW(i+1, j+1)  */
+        BAND(-mx * my + mx - 1, 12, -1, 1, -1, -); /* uSE(i-1, j+1)  */
+        BAND(-mx * my - mx + 1, 11, 1, -1, -1, -); /* uNW(i+1, j-1)  */
+        BAND(-mx * my - mx - 1, 10, -1, -1, -1, -); /* uNE(i-1, j-1) */
+#undef BAND
+      }
+}
+
+/* R^T R factorisation in place; returns info (0, or the column whose pivot
+ * was not positive). */
+int pmgo_dpbfa(double *abd, int lda, int n, int m) {
+#define ABD(r, c) abd[(size_t)((c) - 1) * lda + ((r) - 1)]
+  for (int j = 1; j <= n; ++j) {
+    double s = 0.0;
+    int ik = m + 1;
+    int jk = j - m > 1 ? j - m : 1;
+    const int mu = m + 2 - j > 1 ? m + 2 - j : 1;
+    for (int k = mu; k <= m; ++k) {
+      double t = ABD(k, j) - ddot5(k - mu, &ABD(ik, jk), &ABD(mu, j));
+      t /= ABD(m + 1, jk);
+      ABD(k, j) = t;
+      s += t * t;
+      --ik;
+      ++jk;
+    }
+    s = ABD(m + 1, j) - s;
+    if (s <= 0.0)
+      return j;
+    ABD(m + 1, j) = sqrt(s);
+  }
+  return 0;
+}
+
+/* Solves R^T R x = b in place (b: n values). */
+void pmgo_dpbsl(const double *abd, int lda, int n, int m, double *b) {
+  for (int k = 1; k <= n; ++k) {
+    const int lm = k - 1 < m ? k - 1 : m;
+    const int la = m + 1 - lm, lb = k - lm;
+    const double t = ddot5(lm, &ABD(la, k), &b[lb - 1]);
+    b[k - 1] = (b[k - 1] - t) / ABD(m + 1, k);
+  }
+  for (int kb = 1; kb <= n; ++kb) {
+    const int k = n + 1 - kb;
+    const int lm = k - 1 < m ? k - 1 : m;
+    const int la = m + 1 - lm, lb = k - lm;
+    b[k - 1] /= ABD(m + 1, k);
+    const double t = -b[k - 1];
+    if (lm > 0 && t != 0.0)
+      for (int i = 0; i < lm; ++i)
+        b[lb - 1 + i] += t * ABD(la + i, k);
+  }
+#undef ABD
+}
+
+/* ------------------------------------------------------------------------
  * APBS iparm/rparm driver, linear case: Vmgdriv / Vmgdriv2
  * (pmgc/mgdrvd.cc:60-491) with Vbuildops (pmgc/mgsubd.cc:63-265, Galerkin
  * coarsening) and the V-cycle Vmvcs (pmgc/mgcsd.cc:61-531), restated with
@@ -719,6 +837,33 @@ static void afbound(int nx, int ny, int nz, double *x, const double *gx,
     }
 }
 
+/* The coarsest level's solve (mgcsd.cc:362-405): mgsolv 0, 100 CG
+ * iterations from zero with errtol epsiln = 0; mgsolv 1, the factored band
+ * applied to the interior of f, boundary zero. */
+static void acoarse(alevel *C, const double *f, int mgsolv,
+                    const double *band, int bn, int bm, int blda, double *w1,
+                    double *w2, double *w3) {
+  const size_t n = (size_t)C->nx * C->ny * C->nz;
+  if (mgsolv == 1) {
+    size_t q = 0;
+    for (int k = 2; k <= C->nz - 1; ++k)
+      for (int j = 2; j <= C->ny - 1; ++j)
+        for (int i = 2; i <= C->nx - 1; ++i)
+          w1[q++] = f[IX(C->nx, C->ny, i, j, k)];
+    pmgo_dpbsl(band, blda, bn, bm, w1);
+    q = 0;
+    for (int k = 2; k <= C->nz - 1; ++k)
+      for (int j = 2; j <= C->ny - 1; ++j)
+        for (int i = 2; i <= C->nx - 1; ++i)
+          C->x[IX(C->nx, C->ny, i, j, k)] = w1[q++];
+    afbound(C->nx, C->ny, C->nz, C->x, NULL, NULL, NULL);
+    return;
+  }
+  const pmgo_op o = aop(C);
+  memset(C->x, 0, sizeof(double) * n);
+  pmgo_cghs(C->nx, C->ny, C->nz, &o, C->cc, f, C->x, w1, w2, w3, 100, 0.0, 0);
+}
+
 /* The stop test's numerator after a cycle (mgcsd.cc:467-519): istop 0/1
  * the L1 norm of f - A u, 2 the L1 norm of tru - u (then tru = u), 3 the
  * L2 norm of tru - u. */
@@ -752,7 +897,7 @@ int pmgo_mgdriv(const int *iparm, const double *rparm, double *u,
   const int nx = iparm[2], ny = iparm[3], nz = iparm[4], nlev = iparm[5];
   const int nu1 = iparm[6], nu2 = iparm[7], itmax = iparm[9];
   const int istop = iparm[10], ipkey = iparm[13], mgprol = iparm[16];
-  const int mgsmoo = iparm[19];
+  const int mgsmoo = iparm[19], mgsolv = iparm[20];
   const double errtol = rparm[0];
   if (nlev < 1 || nlev > 12)
     return -1;
@@ -780,7 +925,8 @@ int pmgo_mgdriv(const int *iparm, const double *rparm, double *u,
   const size_t nf = (size_t)nx * ny * nz;
   double *w1 = calloc(nf, sizeof(double)), *w2 = calloc(nf, sizeof(double));
   double *w3 = calloc(nf, sizeof(double));
-  double *tru = NULL;
+  double *tru = NULL, *band = NULL;
+  int bn = 0, bm = 0, blda = 0;
   ok &= w1 && w2 && w3;
   int iters = 0;
   double rsnrm = 0.0;
@@ -807,6 +953,22 @@ int pmgo_mgdriv(const int *iparm, const double *rparm, double *u,
     pmgo_restrc2(F->nx, F->ny, F->nz, C->nx, C->ny, C->nz, F->fc, C->fc,
                  (const double *const *)C->P);
   }
+  if (mgsolv == 1) { /* Vbuildband on the coarsest level, factored */
+    const alevel *C = &lv[nlev];
+    const pmgo_op o = aop(C);
+    const int mx = C->nx - 2, my = C->ny - 2;
+    const int m = C->kind == 7 ? mx * my : mx * my + mx + 1;
+    band = calloc((size_t)(m + 1) * mx * my * (C->nz - 2), sizeof(double));
+    if (!band) {
+      ok = 0;
+      goto done;
+    }
+    pmgo_buildband(C->nx, C->ny, C->nz, &o, &bn, &bm, &blda, band);
+    if (pmgo_dpbfa(band, blda, bn, bm) != 0) {
+      ok = -1;
+      goto done;
+    }
+  }
   /* u starts from zero (mgdrvd.cc:419) */
   memset(u, 0, sizeof(double) * nf);
   afbound(nx, ny, nz, u, NULL, NULL, NULL);
@@ -825,10 +987,7 @@ int pmgo_mgdriv(const int *iparm, const double *rparm, double *u,
   }
   if (nlev == 1) {
     /* direct solve on the only level: 100 CG iterations (mgsolv 0) */
-    for (size_t q = 0; q < nf; ++q)
-      u[q] = 0.0;
-    const pmgo_op o = aop(&lv[1]);
-    pmgo_cghs(nx, ny, nz, &o, lv[1].cc, lv[1].fc, u, w1, w2, w3, 100, 0.0, 0);
+    acoarse(&lv[1], lv[1].fc, mgsolv, band, bn, bm, blda, w1, w2, w3);
     iters = 1;
     rsnrm = astop(&lv[1], istop, u, tru, w1);
   } else {
@@ -844,13 +1003,8 @@ int pmgo_mgdriv(const int *iparm, const double *rparm, double *u,
           asmooth(C, C->w0, C->x, nu1, 0, 1, mgsmoo, w1, w2, w3);
         }
       }
-      {
-        alevel *C = &lv[nlev];
-        const pmgo_op o = aop(C);
-        memset(C->x, 0, sizeof(double) * C->nx * C->ny * C->nz);
-        pmgo_cghs(C->nx, C->ny, C->nz, &o, C->cc, C->w0, C->x, w1, w2, w3,
-                  100, 0.0, 0);
-      }
+      acoarse(&lv[nlev], lv[nlev].w0, mgsolv, band, bn, bm, blda, w1, w2,
+              w3);
       for (int L = nlev - 1; L >= 1; --L) {
         alevel *F = &lv[L];
         const alevel *C = &lv[L + 1];
@@ -892,6 +1046,9 @@ done:
   free(w1);
   free(w2);
   free(w3);
+  free(band);
+  if (ok == -1)
+    return -3;
   if (!ok)
     return -2;
   if (iters_out)

@@ -56,13 +56,21 @@ int pmgo_cghs(int nx, int ny, int nz, const pmgo_op *A, const double *cc,
  * coarsening, Vmvcs). iparm/rparm are 0-based copies of the reference's
  * 1-based arrays. u: n^3 in/out (solution with the boundary values on the
  * shell); tcf: the true solution for istop 2/3 (overwritten by istop 2),
- * else may be NULL. Returns 0, -1 (bad nlev) or -2 (out of memory). */
+ * else may be NULL. Returns 0, -1 (bad nlev), -2 (out of memory) or -3
+ * (mgsolv 1: the coarsest operator is not positive definite). */
 int pmgo_mgdriv(const int *iparm, const double *rparm, double *u,
                 const double *xf, const double *yf, const double *zf,
                 const double *gxcf, const double *gycf, const double *gzcf,
                 const double *a1cf, const double *a2cf, const double *a3cf,
                 const double *ccf, const double *fcf, double *tcf,
                 int *iters_out, int *ierror_out, double *rsnrm_out);
+/* Banded direct solver of the APBS layer (Vbuildband, Vdpbfa, Vdpbsl):
+ * band storage (abd zeroed by the caller, (m+1)*n doubles), in-place
+ * factorisation (returns info), in-place solve. */
+void pmgo_buildband(int nx, int ny, int nz, const pmgo_op *A, int *n_out,
+                    int *m_out, int *lda_out, double *abd);
+int pmgo_dpbfa(double *abd, int lda, int n, int m);
+void pmgo_dpbsl(const double *abd, int lda, int n, int m, double *b);
 /* Box-method fine operator from coefficient maps (VbuildA_fv). */
 void pmgo_buildA_fv(int nx, int ny, int nz, int ipkey, int *numdia, int *ipc,
                     double *oC, double *cc, double *fc, double *oE,

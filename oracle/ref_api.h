@@ -137,6 +137,17 @@ int pmgref_VbuildA_fv(int nx, int ny, int nz, int ipkey, int *numdia,
                       const double *a3cf, const double *ccf,
                       const double *fcf);
 
+/* The reference's banded coarse solver as compiled: Vbuildband
+ * (pmgc/buildBd.cc:252-303: LINPACK band storage of the interior operator,
+ * then Vdpbfa, pmgc/mlinpckd.cc:168-207) and Vdpbsl (:209-240). ac: the
+ * packed operator (4 or 14 columns for numdia 7 or 27); ipcB gets n, m,
+ * lda, 1; acB (zeroed by the caller) lda*n doubles. Returns key (0, or 1
+ * when the factorisation met a non-positive pivot). */
+int pmgref_Vbuildband(int nx, int ny, int nz, int numdia, double *ac,
+                      int *ipcB, double *acB);
+int pmgref_Vdpbfa(double *abd, int lda, int n, int m);
+int pmgref_Vdpbsl(double *abd, int lda, int n, int m, double *b);
+
 #ifdef __cplusplus
 }
 #endif

@@ -4,10 +4,12 @@
 #include "ref_registry.h"
 
 #include "pmgc/buildAd.h"
+#include "pmgc/buildBd.h"
 #include "pmgc/buildGd.h"
 #include "pmgc/buildPd.h"
 #include "pmgc/gsd.h"
 #include "pmgc/matvecd.h"
+#include "pmgc/mlinpckd.h"
 
 #include <iostream>
 #include <vector>
@@ -265,6 +267,28 @@ int pmgref_VbuildA_fv(int nx, int ny, int nz, int ipkey, int *numdia,
                       fc, oE, oN, uC, m(xf), m(yf), m(zf), m(gxcf), m(gycf),
                       m(gzcf), m(a1cf), m(a2cf), m(a3cf), m(ccf), m(fcf),
                       kq());
+  return 0;
+}
+
+int pmgref_Vbuildband(int nx, int ny, int nz, int numdia, double *ac,
+                      int *ipcB, double *acB) {
+  quiet_cout q;
+  int ipc[12] = {0};
+  ipc[10] = numdia;
+  int key = -1;
+  pmgc::Vbuildband<D>(&key, &nx, &ny, &nz, ipc, nullptr, ac, ipcB, nullptr,
+                      acB, kq());
+  return key;
+}
+
+int pmgref_Vdpbfa(double *abd, int lda, int n, int m) {
+  int info = -1;
+  pmgc::Vdpbfa<D>(abd, &lda, &n, &m, &info);
+  return info;
+}
+
+int pmgref_Vdpbsl(double *abd, int lda, int n, int m, double *b) {
+  pmgc::Vdpbsl<D>(abd, &lda, &n, &m, b);
   return 0;
 }
 

@@ -31,6 +31,11 @@ def golden_box():
     return load_golden("buildA_fv.npz")
 
 
+@pytest.fixture(scope="session")
+def golden_band():
+    return load_golden("band.npz")
+
+
 def box_case(g, tag):
     """One VbuildA_fv case of buildA_fv.npz: sizes, ipkey, the input maps,
     the pre-filled output arrays and the reference's outputs."""

@@ -8,7 +8,7 @@ regenerate them:
 
     make -C oracle -j8 && python tests/golden/make_golden.py [group ...]
 
-(groups: kernels, problems, box_operator; all by default).
+(groups: kernels, problems, box_operator, band; all by default).
 """
 from __future__ import annotations
 
@@ -194,8 +194,59 @@ def box_operator(ref: Reference) -> None:
     np.savez_compressed(os.path.join(OUT, "buildA_fv.npz"), **out)
 
 
+def zero_shell_op(rng, n, kind):
+    """Symmetric positive definite operator with zero coefficients on the
+    shell (as operators built on the interior have them)."""
+    a = [rng.uniform(0.5, 2.0, n ** 3) for _ in range(4 if kind == 7 else 14)]
+    a[0] = rng.uniform(60.0, 80.0, n ** 3)
+    shell = np.ones((n, n, n), bool)
+    shell[1:-1, 1:-1, 1:-1] = False
+    for v in a:
+        v.reshape(n, n, n)[shell] = 0.0
+    return a
+
+
+def band(ref: Reference) -> None:
+    """The reference's banded coarse solver (buildBd.cc, mlinpckd.cc): its
+    Vbuildband (band storage + Vdpbfa) of a 7-point operator, and its Vdpbfa
+    and Vdpbsl on the band of a 27-point operator stored by the
+    restatement (whose 27-point band keeps the matvec's couplings)."""
+    import ctypes
+    from oracle.oracle import Restatement
+    D = ctypes.POINTER(ctypes.c_double)
+
+    def d(a):
+        return a.ctypes.data_as(D)
+
+    rng = np.random.default_rng(20261205)
+    n = 7
+    mx = n - 2
+    out = dict(n=n)
+    a7 = zero_shell_op(rng, n, 7)
+    ac = np.ascontiguousarray(np.stack(a7).ravel())
+    m = mx * mx
+    acB = np.zeros((m + 1) * mx ** 3)
+    ipcB = (ctypes.c_int * 4)()
+    key = ref.lib.pmgref_Vbuildband(n, n, n, 7, d(ac), ipcB, d(acB))
+    b = rng.normal(size=mx ** 3)
+    x = b.copy()
+    ref.lib.pmgref_Vdpbsl(d(acB), m + 1, mx ** 3, m, d(x))
+    out.update(op7=np.stack(a7), band7=acB, ipcB7=np.array(ipcB[:]),
+               key7=key, b7=b, x7=x)
+    a27 = zero_shell_op(rng, n, 27)
+    abd, nb, m, lda = Restatement().buildband(n, a27)
+    fac = abd.copy()
+    info = ref.lib.pmgref_Vdpbfa(d(fac), lda, nb, m)
+    b = rng.normal(size=nb)
+    x = b.copy()
+    ref.lib.pmgref_Vdpbsl(d(fac), lda, nb, m, d(x))
+    out.update(op27=np.stack(a27), band27=abd, fac27=fac, info27=info,
+               b27=b, x27=x)
+    np.savez_compressed(os.path.join(OUT, "band.npz"), **out)
+
+
 GROUPS = {"kernels": kernels, "problems": problems,
-          "box_operator": box_operator}
+          "box_operator": box_operator, "band": band}
 
 if __name__ == "__main__":
     ref = Reference()

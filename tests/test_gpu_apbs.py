@@ -52,6 +52,8 @@ def rel(a, b):
     (17, 3, dict(mgsmoo=4, itmax=80)),
     (33, 4, dict(istop=0, errtol=1e-6)),
     (17, 2, dict(nu1=1, nu2=3, mgkey=1)),
+    (17, 3, dict(mgsolv=1)),
+    (33, 4, dict(mgsolv=1, mgprol=0)),
 ])
 def test_apbs_driver_matches_restatement(restatement, n, nlev, kw):
     maps = apbs_maps(n, n + nlev)
@@ -106,7 +108,7 @@ def test_apbs_driver_one_level_and_itmax(restatement):
     assert (it, ierr) == (2, 1)
 
 
-@pytest.mark.parametrize("kw", [dict(mgcoar=0), dict(mgsolv=1),
+@pytest.mark.parametrize("kw", [dict(mgcoar=0), dict(mgsolv=2),
                                 dict(mgsmoo=0), dict(mode=1), dict(nlev=5),
                                 dict(istop=4), dict(mgdisc=1)])
 def test_apbs_driver_rejects_untranslated_options(kw):
@@ -117,3 +119,31 @@ def test_apbs_driver_rejects_untranslated_options(kw):
     with pytest.raises(PmgError) as e:
         run_gpu(iparm, rparm, apbs_maps(n, 1), n)
     assert e.value.status == -1
+
+
+def test_band_solver_matches_reference(golden_band):
+    """Vbuildband (band storage and Vdpbfa), Vdpbfa and Vdpbsl bit for bit
+    against the reference's (buildBd.cc, mlinpckd.cc); the 27-point band
+    stored where the matvec reads its couplings and factored as the
+    reference factors it."""
+    g = golden_band
+    n = int(g["n"])
+    nb = (n - 2) ** 3
+    for kind in (7, 27):
+        ac = T(g[f"op{kind}"])
+        m = (n - 2) ** 2 + (0 if kind == 7 else n - 1)
+        acB = torch.full(((m + 1) * nb,), 3.0, dtype=torch.float64,
+                         device=DEV)
+        key, ipcB = pmgc.Vbuildband(n, n, n, ac, acB)
+        want = g["band7"] if kind == 7 else g["fac27"]
+        assert key == 0 and ipcB == [nb, m, m + 1, 1]
+        assert np.array_equal(acB.cpu().numpy(), want)
+        x = T(g[f"b{kind}"])
+        pmgc.Vdpbsl(acB, m + 1, nb, m, x)
+        assert np.array_equal(x.cpu().numpy(), g[f"x{kind}"])
+    m = (n - 2) ** 2 + n - 1
+    abd = T(g["band27"])
+    assert pmgc.Vdpbfa(abd, m + 1, nb, m) == 0
+    assert np.array_equal(abd.cpu().numpy(), g["fac27"])
+    bad = T(-g["band27"])
+    assert pmgc.Vdpbfa(bad, m + 1, nb, m) == 1

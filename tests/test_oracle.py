@@ -216,15 +216,17 @@ def apbs_maps(n, seed, h=0.5):
                 ccf=np.full(n ** 3, 0.05), fcf=rng.normal(0.0, 1.0, n ** 3))
 
 
-@pytest.mark.parametrize("mgsmoo,mgprol", [(1, 1), (1, 0), (4, 1)])
+@pytest.mark.parametrize("mgsmoo,mgprol,mgsolv", [(1, 1, 0), (1, 0, 0),
+                                                   (4, 1, 0), (1, 1, 1)])
 def test_apbs_driver_restatement_solves_the_box_system(restatement, mgsmoo,
-                                                        mgprol):
+                                                        mgprol, mgsolv):
     """The restated APBS driver (Vmgdriv -> Vbuildops -> Vmvcs) converges
     to the direct solution of the box-method system it builds, with the
     boundary values on the shell."""
     n, nlev = 17, 3
     maps = apbs_maps(n, 3)
-    iparm, rparm = apbs_params(n, nlev, mgsmoo=mgsmoo, mgprol=mgprol)
+    iparm, rparm = apbs_params(n, nlev, mgsmoo=mgsmoo, mgprol=mgprol,
+                               mgsolv=mgsolv)
     u = np.zeros(n ** 3)
     it, ierr, ratio = restatement.mgdriv(iparm, rparm, u, maps)
     assert ierr == 0 and 1 < it < 60 and ratio <= 1e-10
@@ -245,6 +247,36 @@ def test_apbs_driver_restatement_solves_the_box_system(restatement, mgsmoo,
     assert np.array_equal(u3[c, 0, :], gy[0, c, :])
     assert np.array_equal(u3[c, -1, :], gy[1, c, :])
     assert np.array_equal(u3[0], gz[0]) and np.array_equal(u3[-1], gz[1])
+
+
+def test_band_solver_bitexact(restatement, golden_band):
+    """Vbuildband / Vdpbfa / Vdpbsl (buildBd.cc, mlinpckd.cc): the band of a
+    7-point operator and its factor bit for bit; the factor and the solve of
+    a 27-point band bit for bit; the 27-point band solves the dense
+    system."""
+    g = golden_band
+    n = int(g["n"])
+    abd, nb, m, lda = restatement.buildband(n, [np.ascontiguousarray(a)
+                                                for a in g["op7"]])
+    assert restatement.dpbfa(abd, lda, nb, m) == 0
+    assert np.array_equal(abd, g["band7"])
+    x = g["b7"].copy()
+    restatement.dpbsl(abd, lda, nb, m, x)
+    assert np.array_equal(x, g["x7"])
+    ops27 = [np.ascontiguousarray(a) for a in g["op27"]]
+    abd, nb, m, lda = restatement.buildband(n, ops27)
+    assert np.array_equal(abd, g["band27"])
+    assert restatement.dpbfa(abd, lda, nb, m) == int(g["info27"]) == 0
+    assert np.array_equal(abd, g["fac27"])
+    x = g["b27"].copy()
+    restatement.dpbsl(abd, lda, nb, m, x)
+    assert np.array_equal(x, g["x27"])
+    A, idx = dense_operator(n, ops27, np.zeros(n ** 3))
+    y = np.zeros(n ** 3)
+    y[idx] = x
+    Ax = np.zeros(n ** 3)
+    restatement.matvec(n, ops27, np.zeros(n ** 3), y, Ax)
+    assert np.abs(Ax[idx] - g["b27"]).max() <= 1e-12 * np.abs(g["b27"]).max()
 
 
 def test_hierarchy(restatement, golden_problem):
