@@ -351,7 +351,8 @@ int pmg_Vdpbsl_d(const double *abd, int lda, int n, int m, double *b,
  *   iparm[9] itmax   iparm[10] istop (0 absolute L1 residual, 1 relative L1
  *   residual, 2 L1 change of the iterate, 3 L2 error against tcf)
  *   iparm[13] ipkey   iparm[15] mode (0)   iparm[16] mgprol (0 trilinear,
- *   1 operator-based)   iparm[17] mgcoar (2 Galerkin)   iparm[18] mgdisc
+ *   1 operator-based)   iparm[17] mgcoar (0 coefficient maps injected and
+ *   the box method per level, 2 Galerkin)   iparm[18] mgdisc
  *   (0 box method)   iparm[19] mgsmoo (1 red-black GS, 4 CG)   iparm[20]
  *   mgsolv (0 CG on the coarsest level, 1 banded direct solve as
  *   pmg_Vbuildband_d / pmg_Vdpbsl_d)   iparm[21] iperf (0)

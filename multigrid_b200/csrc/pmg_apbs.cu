@@ -484,13 +484,34 @@ int band_factor(const Dims &d, int kind, const Op14<double> &A, double *abd,
   return PMG_OK;
 }
 
+// Injection of a coefficient map to the next coarser grid (Vbuildcopy0,
+// pmgc/mgsubd.cc:578-697): out(a, b, c) = in(2a-1, 2b-1, 2c-1) over the
+// whole coarse array, shell included; with keep_c the third index is a
+// layer (the two sides of a boundary map) and is not coarsened. Mesh lines
+// are (n, 1, 1) arrays.
+__global__ void inject_kernel(const double *__restrict__ in,
+                              double *__restrict__ out, int na, int nb,
+                              int nc, int naf, int nbf, int keep_c) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  const int b = blockIdx.y * blockDim.y + threadIdx.y;
+  const int c = blockIdx.z;
+  if (a >= na || b >= nb || c >= nc)
+    return;
+  const int cf = keep_c ? c : 2 * c;
+  out[((long)c * nb + b) * na + a] = in[((long)cf * nbf + 2 * b) * naf + 2 * a];
+}
+
+// the eleven inputs of the box-method builder, in BoxMaps order
+enum { kMx, kMy, kMz, kGx, kGy, kGz, kA1, kA2, kA3, kCcf, kFcf, kMaps };
+
 struct ApbsLevel {
   Dims d;
-  int kind;     // 7 (finest) or 27 (Galerkin levels)
+  int kind;     // 7 (box method: finest, or every level with mgcoar 0) or 27
   int ipc[12];  // ipc[10] = kind, for the packed-operator entry points
   double *ac;   // 4 or 14 columns of d.count()
   double *cc, *fc, *x, *w0;
   double *P[27]; // prolongation from this level to the next finer one
+  const double *m[kMaps]; // coefficient maps (mgcoar 0)
   const double *a(int s) const { return ac + (size_t)s * d.count(); }
   double *aw(int s) { return ac + (size_t)s * d.count(); }
 };
@@ -786,7 +807,9 @@ int pmg_Vmgdriv_d(const int *iparm, const double *rparm, double *u,
   PMG_REQUIRE(mode == 0, "Vmgdriv: only the linear mode (iparm mode 0)");
   PMG_REQUIRE(mgkey == 0 || mgkey == 1, "Vmgdriv: mgkey must be 0 or 1");
   PMG_REQUIRE(mgdisc == 0, "Vmgdriv: only the box method (mgdisc 0)");
-  PMG_REQUIRE(mgcoar == 2, "Vmgdriv: only Galerkin coarsening (mgcoar 2)");
+  PMG_REQUIRE(mgcoar == 0 || mgcoar == 2,
+              "Vmgdriv: mgcoar must be 0 (coefficient injection) or 2 "
+              "(Galerkin)");
   PMG_REQUIRE(mgprol == 0 || mgprol == 1, "Vmgdriv: mgprol must be 0 or 1");
   PMG_REQUIRE(mgsmoo == 1 || mgsmoo == 4,
               "Vmgdriv: mgsmoo must be 1 (red-black GS) or 4 (CG)");
@@ -813,12 +836,16 @@ int pmg_Vmgdriv_d(const int *iparm, const double *rparm, double *u,
                  : Dims{(D.lv[L - 1].d.nx - 1) / 2 + 1,
                         (D.lv[L - 1].d.ny - 1) / 2 + 1,
                         (D.lv[L - 1].d.nz - 1) / 2 + 1};
-    v.kind = L == 1 ? 7 : 27;
+    v.kind = L == 1 || mgcoar == 0 ? 7 : 27;
     for (int q = 0; q < 12; ++q)
       v.ipc[q] = 0;
     v.ipc[10] = v.kind;
     const size_t n = (size_t)v.d.count();
     total += n * ((v.kind == 7 ? 4 : 14) + 3 + (L > 1 ? 1 + 27 : 0));
+    if (mgcoar == 0 && L > 1) // coarse maps: 5 grids, lines, boundary maps
+      total += 5 * n + v.d.nx + v.d.ny + v.d.nz +
+               2 * ((size_t)v.d.ny * v.d.nz + (size_t)v.d.nx * v.d.nz +
+                    (size_t)v.d.nx * v.d.ny);
   }
   const size_t nf = (size_t)D.lv[1].d.count();
   D.rg0 = reduce_grid(D.lv[1].d);
@@ -847,6 +874,20 @@ int pmg_Vmgdriv_d(const int *iparm, const double *rparm, double *u,
     v.x = L == 1 ? u : take(n);
     for (int q = 0; q < 27; ++q)
       v.P[q] = L > 1 ? take(n) : nullptr;
+    if (L == 1) {
+      const double *in[kMaps] = {xf,   yf,   zf,   gxcf, gycf, gzcf,
+                                 a1cf, a2cf, a3cf, ccf,  fcf};
+      for (int q = 0; q < kMaps; ++q)
+        v.m[q] = in[q];
+    } else if (mgcoar == 0) {
+      const Dims &c = v.d;
+      const size_t sz[kMaps] = {(size_t)c.nx, (size_t)c.ny, (size_t)c.nz,
+                                2 * (size_t)c.ny * c.nz,
+                                2 * (size_t)c.nx * c.nz,
+                                2 * (size_t)c.nx * c.ny, n, n, n, n, n};
+      for (int q = 0; q < kMaps; ++q)
+        v.m[q] = take(sz[q]);
+    }
   }
   D.w1 = take(nf);
   D.w2 = take(nf);
@@ -885,6 +926,33 @@ int pmg_Vmgdriv_d(const int *iparm, const double *rparm, double *u,
       pc[q] = C.P[q];
     for (int q = 0; q < 14; ++q)
       out[q] = C.aw(q);
+    if (mgcoar == 0) {
+      // Vbuildcopy0: the maps injected, then the box method on this grid
+      // (mgsubd.cc:141-166); the restricted cc and fc of Galerkin levels do
+      // not apply
+      const dim3 b(32, 8);
+      auto inject = [&](int q, int na, int nb, int nc, int naf, int nbf,
+                        int keep) {
+        inject_kernel<<<dim3(cdiv(na, 32), cdiv(nb, 8), nc), b, 0, s>>>(
+            F.m[q], const_cast<double *>(C.m[q]), na, nb, nc, naf, nbf,
+            keep);
+      };
+      inject(kMx, dc.nx, 1, 1, df.nx, 1, 1);
+      inject(kMy, dc.ny, 1, 1, df.ny, 1, 1);
+      inject(kMz, dc.nz, 1, 1, df.nz, 1, 1);
+      inject(kGx, dc.ny, dc.nz, 2, df.ny, df.nz, 1);
+      inject(kGy, dc.nx, dc.nz, 2, df.nx, df.nz, 1);
+      inject(kGz, dc.nx, dc.ny, 2, df.nx, df.ny, 1);
+      for (int q = kA1; q <= kFcf; ++q)
+        inject(q, dc.nx, dc.ny, dc.nz, df.nx, df.ny, 0);
+      PMG_LAUNCH_CHECK();
+      rc = pmg_VbuildA_fv_d(dc.nx, dc.ny, dc.nz, ipkey, nullptr, nullptr,
+                            C.aw(0), C.cc, C.fc, C.aw(1), C.aw(2), C.aw(3),
+                            C.m[kMx], C.m[kMy], C.m[kMz], C.m[kGx], C.m[kGy],
+                            C.m[kGz], C.m[kA1], C.m[kA2], C.m[kA3], C.m[kCcf],
+                            C.m[kFcf], stream);
+      continue;
+    }
     if (F.kind == 7) {
       rc = pmg_VbuildG_7_d(df.nx, df.ny, df.nz, dc.nx, dc.ny, dc.nz, pc,
                            F.a(0), F.a(1), F.a(2), F.a(3), out, stream);

@@ -772,7 +772,19 @@ void pmgo_dpbsl(const double *abd, int lda, int n, int m, double *b) {
 typedef struct {
   int nx, ny, nz, kind;
   double *a[14], *cc, *fc, *x, *w0, *P[27];
+  double *m[11]; /* coarse coefficient maps (mgcoar 0), BOX_IN order */
 } alevel;
+
+/* Injection to the next coarser grid (Vbuildcopy0, mgsubd.cc:578-697):
+ * out(a, b, c) = in(2a-1, 2b-1, 2c-1); keep_c: c is a layer index. */
+static void inject(const double *in, double *out, int na, int nb, int nc,
+                   int naf, int nbf, int keep_c) {
+  for (int c = 0; c < nc; ++c)
+    for (int b = 0; b < nb; ++b)
+      for (int a = 0; a < na; ++a)
+        out[((size_t)c * nb + b) * na + a] =
+            in[((size_t)(keep_c ? c : 2 * c) * nbf + 2 * b) * naf + 2 * a];
+}
 
 static double inorm1(int nx, int ny, int nz, const double *a) {
   double s = 0.0;
@@ -897,7 +909,7 @@ int pmgo_mgdriv(const int *iparm, const double *rparm, double *u,
   const int nx = iparm[2], ny = iparm[3], nz = iparm[4], nlev = iparm[5];
   const int nu1 = iparm[6], nu2 = iparm[7], itmax = iparm[9];
   const int istop = iparm[10], ipkey = iparm[13], mgprol = iparm[16];
-  const int mgsmoo = iparm[19], mgsolv = iparm[20];
+  const int mgsmoo = iparm[19], mgsolv = iparm[20], mgcoar = iparm[17];
   const double errtol = rparm[0];
   if (nlev < 1 || nlev > 12)
     return -1;
@@ -909,7 +921,7 @@ int pmgo_mgdriv(const int *iparm, const double *rparm, double *u,
     v->nx = L == 1 ? nx : (lv[L - 1].nx - 1) / 2 + 1;
     v->ny = L == 1 ? ny : (lv[L - 1].ny - 1) / 2 + 1;
     v->nz = L == 1 ? nz : (lv[L - 1].nz - 1) / 2 + 1;
-    v->kind = L == 1 ? 7 : 27;
+    v->kind = L == 1 || mgcoar == 0 ? 7 : 27;
     const size_t n = (size_t)v->nx * v->ny * v->nz;
     for (int s = 0; s < (v->kind == 7 ? 4 : 14); ++s)
       ok &= (v->a[s] = calloc(n, sizeof(double))) != NULL;
@@ -921,6 +933,14 @@ int pmgo_mgdriv(const int *iparm, const double *rparm, double *u,
     if (L > 1)
       for (int s = 0; s < 27; ++s)
         ok &= (v->P[s] = calloc(n, sizeof(double))) != NULL;
+    if (L > 1 && mgcoar == 0) {
+      const size_t sz[11] = {(size_t)v->nx, (size_t)v->ny, (size_t)v->nz,
+                             2 * (size_t)v->ny * v->nz,
+                             2 * (size_t)v->nx * v->nz,
+                             2 * (size_t)v->nx * v->ny, n, n, n, n, n};
+      for (int q = 0; q < 11; ++q)
+        ok &= (v->m[q] = calloc(sz[q], sizeof(double))) != NULL;
+    }
   }
   const size_t nf = (size_t)nx * ny * nz;
   double *w1 = calloc(nf, sizeof(double)), *w2 = calloc(nf, sizeof(double));
@@ -946,6 +966,24 @@ int pmgo_mgdriv(const int *iparm, const double *rparm, double *u,
       pmgo_buildP_trilin(C->nx, C->ny, C->nz, C->P);
     else
       pmgo_buildP_op(F->nx, F->ny, F->nz, C->nx, C->ny, C->nz, &fo, C->P);
+    if (mgcoar == 0) { /* maps injected, box method on this grid */
+      const double *fm[11] = {xf,   yf,   zf,   gxcf, gycf, gzcf,
+                              a1cf, a2cf, a3cf, ccf,  fcf};
+      const double *const *src = L == 2 ? fm : (const double *const *)F->m;
+      inject(src[0], C->m[0], C->nx, 1, 1, F->nx, 1, 1);
+      inject(src[1], C->m[1], C->ny, 1, 1, F->ny, 1, 1);
+      inject(src[2], C->m[2], C->nz, 1, 1, F->nz, 1, 1);
+      inject(src[3], C->m[3], C->ny, C->nz, 2, F->ny, F->nz, 1);
+      inject(src[4], C->m[4], C->nx, C->nz, 2, F->nx, F->nz, 1);
+      inject(src[5], C->m[5], C->nx, C->ny, 2, F->nx, F->ny, 1);
+      for (int q = 6; q < 11; ++q)
+        inject(src[q], C->m[q], C->nx, C->ny, C->nz, F->nx, F->ny, 0);
+      pmgo_buildA_fv(C->nx, C->ny, C->nz, ipkey, NULL, NULL, C->a[0], C->cc,
+                     C->fc, C->a[1], C->a[2], C->a[3], C->m[0], C->m[1],
+                     C->m[2], C->m[3], C->m[4], C->m[5], C->m[6], C->m[7],
+                     C->m[8], C->m[9], C->m[10]);
+      continue;
+    }
     pmgo_buildG(F->nx, F->ny, F->nz, C->nx, C->ny, C->nz,
                 (const double *const *)C->P, &fo, C->a);
     pmgo_restrc2(F->nx, F->ny, F->nz, C->nx, C->ny, C->nz, F->cc, C->cc,
@@ -1041,6 +1079,8 @@ done:
       free(v->x);
       for (int s = 0; s < 27; ++s)
         free(v->P[s]);
+      for (int q = 0; q < 11; ++q)
+        free(v->m[q]);
     }
   }
   free(w1);

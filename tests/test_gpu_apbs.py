@@ -54,6 +54,8 @@ def rel(a, b):
     (17, 2, dict(nu1=1, nu2=3, mgkey=1)),
     (17, 3, dict(mgsolv=1)),
     (33, 4, dict(mgsolv=1, mgprol=0)),
+    (17, 3, dict(mgcoar=0)),
+    (33, 4, dict(mgcoar=0, mgsolv=1)),
 ])
 def test_apbs_driver_matches_restatement(restatement, n, nlev, kw):
     maps = apbs_maps(n, n + nlev)
@@ -108,7 +110,7 @@ def test_apbs_driver_one_level_and_itmax(restatement):
     assert (it, ierr) == (2, 1)
 
 
-@pytest.mark.parametrize("kw", [dict(mgcoar=0), dict(mgsolv=2),
+@pytest.mark.parametrize("kw", [dict(mgcoar=1), dict(mgsolv=2),
                                 dict(mgsmoo=0), dict(mode=1), dict(nlev=5),
                                 dict(istop=4), dict(mgdisc=1)])
 def test_apbs_driver_rejects_untranslated_options(kw):

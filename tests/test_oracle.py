@@ -216,17 +216,19 @@ def apbs_maps(n, seed, h=0.5):
                 ccf=np.full(n ** 3, 0.05), fcf=rng.normal(0.0, 1.0, n ** 3))
 
 
-@pytest.mark.parametrize("mgsmoo,mgprol,mgsolv", [(1, 1, 0), (1, 0, 0),
-                                                   (4, 1, 0), (1, 1, 1)])
+@pytest.mark.parametrize("mgsmoo,mgprol,mgsolv,mgcoar", [
+    (1, 1, 0, 2), (1, 0, 0, 2), (4, 1, 0, 2), (1, 1, 1, 2), (1, 1, 0, 0),
+    (1, 0, 1, 0)])
 def test_apbs_driver_restatement_solves_the_box_system(restatement, mgsmoo,
-                                                        mgprol, mgsolv):
+                                                        mgprol, mgsolv,
+                                                        mgcoar):
     """The restated APBS driver (Vmgdriv -> Vbuildops -> Vmvcs) converges
     to the direct solution of the box-method system it builds, with the
     boundary values on the shell."""
     n, nlev = 17, 3
     maps = apbs_maps(n, 3)
     iparm, rparm = apbs_params(n, nlev, mgsmoo=mgsmoo, mgprol=mgprol,
-                               mgsolv=mgsolv)
+                               mgsolv=mgsolv, mgcoar=mgcoar)
     u = np.zeros(n ** 3)
     it, ierr, ratio = restatement.mgdriv(iparm, rparm, u, maps)
     assert ierr == 0 and 1 < it < 60 and ratio <= 1e-10
