@@ -269,12 +269,20 @@ def phase_bytes(p, level: int, phase: str, esz: int) -> float | None:
     nf3 = float(p.n ** 3)
     fine = level == p.nlev
     nc3 = float(level_n(p.base, level - 1) ** 3) if level >= 2 else 0.0
+    coded = getattr(p, "_coded", False)
     if level == 0:
+        if phase == "residual" and coded:  # oC, code byte, f, x; float r
+            return nf3 * (3 * 8 + 1 + 4)
         if phase == "residual":  # 4 coefficients + f + x in double
             return nf3 * (6 * 8 + (4 if p.precision == "mixed" else 0))
         if phase == "refine-update":  # x64 read/write, e32 read
             return nf3 * (8 + 4 + 8)
         return None
+    if fine and coded and phase in ("pre-smooth", "post-smooth"):
+        # per sweep: oC, the code byte, f, x read once and written once
+        return 2 * (4 * esz + 1) * n3
+    if fine and coded and phase == "defect":  # oC, code, f, x, r
+        return (4 * esz + 1) * n3
     arrays = {"pre-smooth": 2 * (7 if fine else 17),
               "post-smooth": 2 * (7 if fine else 17),
               "defect": 7 if fine else 17}
@@ -294,9 +302,17 @@ def phase_kernel(p, level: int, phase: str):
     if phase in ("pre-smooth", "post-smooth"):
         if level < p.nlev:
             return ("gs27_phase_kernel", 4)
-        # the mixed path's finest float level is colour-split
-        return ("gs7_split_color_kernel" if p.precision == "mixed"
-                else "gs7_color_kernel", 4)
+        # the mixed path's finest float level is colour-split (and coded
+        # when its couplings have two values per direction)
+        if p.precision == "mixed":
+            return ("gs7_code_color_kernel" if getattr(p, "_coded", False)
+                    else "gs7_split_color_kernel", 4)
+        return ("gs7_color_kernel", 4)
+    coded = getattr(p, "_coded", False)
+    if phase == "defect" and level == p.nlev and coded:
+        return ("defect7_code_kernel", 1)
+    if phase == "residual" and coded:
+        return ("defect_norm_code_kernel", 1)
     return {"residual": ("defect_norm_kernel", 1),
             "defect": ("defect_kernel", 1),
             "restrict": ("restrict_kernel", 1),
@@ -326,6 +342,7 @@ def profiled_traffic(kernel: str | None, launches: int, workload: str,
 def profile_solve(p, step, dev, esz):
     """One extra solve with CUDA events recorded around every cycle phase
     inside the cycle graph; returns per-phase averages and bandwidths."""
+    p._coded = p.precision == "mixed" and p.coded_couplings()
     p.set_profiling(True)
     p.profile(reset=True)
     step(p, dev)
@@ -731,6 +748,11 @@ def main():
                                             args.precision),
                 "traffic_unit": "bytes per phase occurrence (ncu capture)",
                 "peak_source": peak_kind,
+                "bytes_basis": (
+                    "coded couplings: per point oC, one code byte, f, x"
+                    if getattr(p, "_coded", False) and dom["level"] >= 0
+                    and kname and "code" in kname else
+                    "coefficient arrays as stored (kernel table)"),
                 "algorithmic_bytes_per_launch": dom["bytes"],
                 "avg_launch_us": dom["us_avg"]}
 

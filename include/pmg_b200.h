@@ -594,6 +594,16 @@ int pmg_problem_set_coarse_rtol(pmg_problem *p, double rtol);
  * No reference counterpart. */
 int pmg_problem_set_host_loop(pmg_problem *p, int on);
 
+/* Mixed precision: the finest float smoother and defect read the couplings
+ * as one code byte per point with a two-value table per direction whenever
+ * the fine operator has two values per coupling direction (the class's
+ * dielectric faces do), and the coupling arrays otherwise; results are the
+ * same bits either way. on = 0 keeps the arrays (default 1). */
+int pmg_problem_set_coded_couplings(pmg_problem *p, int on);
+/* *coded = 1 when the built mixed problem's finest couplings are coded and
+ * in use. Synchronises the problem's stream. */
+int pmg_problem_coded_couplings(pmg_problem *p, int *coded);
+
 /* on != 0: choose kernels for many solves sharing the GPU rather than for
  * the latency of this one: the mixed path's lowest levels run in one CTA
  * instead of an 8-CTA cluster with its arrays in shared memory (a cluster

@@ -6,6 +6,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <climits>
 #include <new>
 
 #include "build_kernels.cuh"
@@ -36,6 +37,10 @@ struct LevelBuf {
   float *x32 = nullptr, *f32 = nullptr, *r32 = nullptr;
   float *xalt32 = nullptr;
   double *omega = nullptr; // damping computed on this level (device)
+  // mixed finest level: coded couplings (split_layout.cuh) and their table
+  unsigned char *code = nullptr;
+  int *code_info = nullptr; // device: ranges and the mismatch flags
+  double *lut64 = nullptr;  // device: the double couplings of the codes
 
   Op14<double> A64(int nops) const {
     Op14<double> A{};
@@ -132,6 +137,7 @@ struct pmg_problem {
   bool solve_pending = false;
   bool host_loop = false; // pmg_problem_set_host_loop
   bool throughput = false; // pmg_problem_set_throughput_mode
+  bool use_codes = true;   // pmg_problem_set_coded_couplings
   // MG-preconditioned CG on the finest level (allocated on first use):
   // right-hand side, iterate, residual, preconditioned residual, search
   // direction, A times it; three reduction slots; the iteration state.
@@ -194,6 +200,9 @@ void plan(pmg_problem *p, Arena &a) {
       v.f32 = a.take<float>(v.n3);
       v.r32 = L > 1 ? a.take<float>(v.n3) : nullptr;
       v.xalt32 = smoothed ? a.take<float>(v.n3) : nullptr;
+      v.code = fine ? a.take<unsigned char>(v.n3) : nullptr;
+      v.code_info = fine ? a.take<int>(8) : nullptr;
+      v.lut64 = fine ? a.take<double>(6) : nullptr;
     }
   }
   const long n1 = p->lv[1].n3;
@@ -388,6 +397,11 @@ double norm_from_sum(const pmg_problem *p, double s) {
 
 int smooth32(pmg_problem *p, int L, int nsweeps, int zero_init, float **cur) {
   LevelBuf &v = p->lv[L];
+  if (L == p->nlev && p->use_codes)
+    return launch_gs7_code<float>(v.d, v.op32[kOC], v.f32, v.op32[kOE],
+                                  v.op32[kON], v.op32[kUC], v.code,
+                                  v.code_info, *cur, nsweeps, 0, zero_init,
+                                  p->stream);
   if (L == p->nlev) // colour-split layout (split_layout.cuh)
     return launch_gs7_split<float>(v.d, v.op32[kOC], v.f32, v.op32[kOE],
                                    v.op32[kON], v.op32[kUC], *cur, nsweeps, 0,
@@ -469,7 +483,12 @@ int vcycle32(pmg_problem *p, int L) {
     return rc;
   prof_end(p, sl + kPhPre);
   prof_begin(p, sl + kPhDefect);
-  if (kind == 7) // split arrays in, reference-layout defect out
+  if (kind == 7 && p->use_codes)
+    defect7_code_kernel<float>
+        <<<defect7_code_grid(v.d), interior_block(), 0, s>>>(
+            v.d, v.op32[kOC], v.op32[kOE], v.op32[kON], v.op32[kUC], v.code,
+            v.code_info, v.f32, x, v.r32);
+  else if (kind == 7) // split arrays in, reference-layout defect out
     defect7_split_kernel<float>
         <<<interior_grid(v.d), interior_block(), 0, s>>>(
             v.d, v.op32[kOC], v.op32[kOE], v.op32[kON], v.op32[kUC], v.f32, x,
@@ -538,9 +557,15 @@ int vcycle32(pmg_problem *p, int L) {
 int mixed_residual_async(pmg_problem *p, bool to_host = true) {
   LevelBuf &v = p->lv[p->nlev];
   prof_begin(p, kPhResidual);
-  defect_norm_kernel<7, double, float, true>
-      <<<reduce_grid(v.d), interior_block(), 0, p->stream>>>(
-          v.d, v.A64(4), v.f, v.x, v.f32, p->red_norm);
+  if (p->use_codes)
+    defect_norm_code_kernel<double><<<reduce_grid(v.d), interior_block(), 0,
+                              p->stream>>>(v.d, v.A64(4), v.f, v.x, v.code,
+                                           v.lut64, v.code_info, v.f32,
+                                           p->red_norm);
+  else
+    defect_norm_kernel<7, double, float, true>
+        <<<reduce_grid(v.d), interior_block(), 0, p->stream>>>(
+            v.d, v.A64(4), v.f, v.x, v.f32, p->red_norm);
   prof_end(p, kPhResidual);
   PMG_LAUNCH_CHECK();
   if (to_host)
@@ -1089,6 +1114,30 @@ int pmg_problem_set_host_loop(pmg_problem *p, int on) {
   return PMG_OK;
 }
 
+int pmg_problem_set_coded_couplings(pmg_problem *p, int on) {
+  if (!p)
+    return PMG_ERR_ARG;
+  if ((bool)on != p->use_codes)
+    drop_graphs(p); // the captured cycles bake the kernel choice in
+  p->use_codes = on != 0;
+  return PMG_OK;
+}
+
+int pmg_problem_coded_couplings(pmg_problem *p, int *coded) {
+  if (!p || !coded)
+    return PMG_ERR_ARG;
+  *coded = 0;
+  const LevelBuf &v = p->lv[p->nlev];
+  if (!p->built || p->precision != PMG_PREC_MIXED || !p->use_codes)
+    return PMG_OK;
+  int flag = 1;
+  PMG_CUDA_TRY(cudaMemcpyAsync(&flag, v.code_info + 6, sizeof(int),
+                               cudaMemcpyDeviceToHost, p->stream));
+  PMG_CUDA_TRY(cudaStreamSynchronize(p->stream));
+  *coded = flag == 0;
+  return PMG_OK;
+}
+
 int pmg_problem_set_throughput_mode(pmg_problem *p, int on) {
   if (!p)
     return PMG_ERR_ARG;
@@ -1220,6 +1269,21 @@ int pmg_build_hierarchy(pmg_problem *p, int trilinear) {
                                                          v.op32[q]);
         ++p->launches;
       }
+    // coded couplings of the finest float operator, when it has two values
+    // per direction (split_layout.cuh)
+    const int init[8] = {INT_MAX, INT_MIN, INT_MAX, INT_MIN,
+                         INT_MAX, INT_MIN, 0,       0};
+    PMG_CUDA_TRY(cudaMemcpyAsync(v.code_info, init, sizeof(init),
+                                 cudaMemcpyHostToDevice, s));
+    coupling_range_kernel<float><<<interior_grid(v.d), interior_block(), 0, s>>>(
+        v.d, v.op32[kOE], v.op32[kON], v.op32[kUC], v.code_info);
+    coupling_code_kernel<float><<<interior_grid(v.d), interior_block(), 0, s>>>(
+        v.d, v.op32[kOE], v.op32[kON], v.op32[kUC], v.code_info, v.code);
+    lut64_store_kernel<double><<<interior_grid(v.d), interior_block(), 0, s>>>(
+        v.d, v.op[kOE], v.op[kON], v.op[kUC], v.code, v.lut64);
+    lut64_check_kernel<double><<<interior_grid(v.d), interior_block(), 0, s>>>(
+        v.d, v.op[kOE], v.op[kON], v.op[kUC], v.code, v.lut64, v.code_info);
+    p->launches += 4;
     if (trilinear) // the trilinear builder writes double only
       for (int L = 1; L < p->nlev; ++L) {
         LevelBuf &c = p->lv[L];

@@ -18,7 +18,11 @@
 // bit-identical.
 #pragma once
 
+#include <climits>
+#include <cstring>
+
 #include "launch.cuh"
+#include "reduce_kernels.cuh"
 
 namespace pmg {
 
@@ -148,6 +152,409 @@ __global__ void __launch_bounds__(256)
                oE[nb.w] * x[nb.w] - uC[nb.dn] * x[nb.dn] - uC[p] * x[nb.u] +
                (oC[p] + T(0)) * x[p];
   r[d.at(t.i, t.j, t.k)] = f[p] - ax;
+}
+
+// ---------------------------------------------------------------------------
+// Coded couplings. The class's fine operator has two-valued couplings per
+// direction (each face's dielectric is the inside or the outside value, so
+// oE, oN and uC each hold two values). A colour pass then needs, per point,
+// only which of the two each of its six couplings is: one byte
+// (bit 0 oE(p), 1 oE(west), 2 oN(p), 3 oN(south), 4 uC(p), 5 uC(down); a set
+// bit selects the larger value), stored in the split layout next to oC. The
+// pass reads the byte instead of three float arrays (per sweep 17 bytes per
+// point instead of 28) and takes the very same float values from a table,
+// so results are bit-identical to the uncoded kernels. The encoding checks
+// every coupling a pass reads bit for bit against the two table values;
+// for any other operator the kernels read the coupling arrays as before.
+// ---------------------------------------------------------------------------
+struct CodeLut {
+  float el, eh, nl, nh, ul, uh; // low / high value of oE, oN, uC
+};
+
+// order-preserving int image of a float (for atomicMin / atomicMax)
+__device__ __forceinline__ int float_order(float v) {
+  const int i = __float_as_int(v);
+  return i >= 0 ? i : i ^ 0x7fffffff;
+}
+__host__ __device__ inline float order_float(int i) {
+  const int b = i >= 0 ? i : i ^ 0x7fffffff;
+  float f;
+  memcpy(&f, &b, sizeof f);
+  return f;
+}
+
+// info[0..5] = min, max of oE, oN, uC over the couplings the interior
+// points read (ordered ints; info[0,2,4] start at INT_MAX, [1,3,5] at
+// INT_MIN)
+template <typename T>
+__global__ void __launch_bounds__(256)
+    coupling_range_kernel(Dims d, const T *__restrict__ oE,
+                          const T *__restrict__ oN,
+                          const T *__restrict__ uC, int *info) {
+  const Interior t = interior_point(d);
+  int v[6] = {INT_MAX, INT_MIN, INT_MAX, INT_MIN, INT_MAX, INT_MIN};
+  if (t.ok) {
+    const Split sp = Split::of(d);
+    const int p = sp.at(t.i, t.j, t.k);
+    const SplitNb nb = split_nb(sp, p, (t.i - 1) & 1);
+    const int e0 = float_order(oE[p]), e1 = float_order(oE[nb.w]);
+    const int n0 = float_order(oN[p]), n1 = float_order(oN[nb.s]);
+    const int u0 = float_order(uC[p]), u1 = float_order(uC[nb.dn]);
+    v[0] = min(e0, e1);
+    v[1] = max(e0, e1);
+    v[2] = min(n0, n1);
+    v[3] = max(n0, n1);
+    v[4] = min(u0, u1);
+    v[5] = max(u0, u1);
+  }
+#pragma unroll
+  for (int q = 0; q < 6; ++q) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const int w = __shfl_xor_sync(0xffffffffu, v[q], o);
+      v[q] = (q & 1) ? max(v[q], w) : min(v[q], w);
+    }
+  }
+  if ((threadIdx.x & 31) == 0)
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+      if (q & 1)
+        atomicMax(&info[q], v[q]);
+      else
+        atomicMin(&info[q], v[q]);
+    }
+}
+
+// code bytes of the interior points; info[6] |= 1 when a coupling is
+// neither table value bit for bit
+template <typename T>
+__global__ void __launch_bounds__(256)
+    coupling_code_kernel(Dims d, const T *__restrict__ oE,
+                         const T *__restrict__ oN,
+                         const T *__restrict__ uC, int *info,
+                         unsigned char *__restrict__ code) {
+  const Interior t = interior_point(d);
+  if (!t.ok)
+    return;
+  const Split sp = Split::of(d);
+  const int p = sp.at(t.i, t.j, t.k);
+  const SplitNb nb = split_nb(sp, p, (t.i - 1) & 1);
+  const T c[6] = {oE[p], oE[nb.w], oN[p], oN[nb.s], uC[p], uC[nb.dn]};
+  unsigned bits = 0;
+  bool bad = false;
+#pragma unroll
+  for (int q = 0; q < 6; ++q) {
+    const int v = __float_as_int(c[q]);
+    const int lo = __float_as_int(order_float(info[(q >> 1) * 2]));
+    const int hi = __float_as_int(order_float(info[(q >> 1) * 2 + 1]));
+    if (v == hi)
+      bits |= 1u << q;
+    else if (v != lo)
+      bad = true;
+  }
+  code[p] = (unsigned char)bits;
+  if (bad)
+    atomicOr(&info[6], 1);
+}
+
+// The table of a coded level, read on the device (info written by
+// coupling_range_kernel / coupling_code_kernel); false when the level's
+// couplings did not all match it, and the uncoded arrays must be used.
+__device__ __forceinline__ bool load_lut(const int *info, CodeLut &L) {
+  if (info[6] != 0)
+    return false;
+  L.el = order_float(info[0]);
+  L.eh = order_float(info[1]);
+  L.nl = order_float(info[2]);
+  L.nh = order_float(info[3]);
+  L.ul = order_float(info[4]);
+  L.uh = order_float(info[5]);
+  return true;
+}
+
+// the six couplings of point p: from the code byte when the level is coded,
+// else from the arrays (the same float values either way)
+template <typename T> struct Couplings {
+  T e, w, n, s, u, dn;
+};
+template <typename T>
+__device__ __forceinline__ Couplings<T>
+couplings(bool coded, const CodeLut &L, const unsigned char *code,
+          const T *oE, const T *oN, const T *uC, int p, const SplitNb &nb) {
+  Couplings<T> c;
+  if (coded) {
+    const unsigned b = code[p];
+    c.e = (b & 1u) ? L.eh : L.el;
+    c.w = (b & 2u) ? L.eh : L.el;
+    c.n = (b & 4u) ? L.nh : L.nl;
+    c.s = (b & 8u) ? L.nh : L.nl;
+    c.u = (b & 16u) ? L.uh : L.ul;
+    c.dn = (b & 32u) ? L.uh : L.ul;
+  } else {
+    c.e = oE[p];
+    c.w = oE[nb.w];
+    c.n = oN[p];
+    c.s = oN[nb.s];
+    c.u = uC[p];
+    c.dn = uC[nb.dn];
+  }
+  return c;
+}
+
+// gs7_split_color_kernel taking the couplings from the code byte when the
+// level is coded (a uniform branch on the device flag, so the choice needs
+// no host round trip and a captured graph serves either case). With the
+// couplings coded a point moves about 17 bytes, so each thread takes PTS
+// points of its half row (32 apart: a warp stays contiguous) and issues
+// all their loads before computing, to keep enough bytes in flight.
+template <typename T, int PTS>
+__global__ void __launch_bounds__(256)
+    gs7_code_color_kernel(Dims d, const T *__restrict__ oC,
+                          const T *__restrict__ fc, const T *__restrict__ oE,
+                          const T *__restrict__ oN, const T *__restrict__ uC,
+                          const unsigned char *__restrict__ code,
+                          const int *__restrict__ info, T *x, int want,
+                          T keep) {
+  const Split sp = Split::of(d);
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
+  const int k = blockIdx.z + 2;
+  if (j > d.ny - 1)
+    return;
+  const int i0 = 2 + ((2 + j + k + want) & 1) +
+                 2 * (int)(blockIdx.x * blockDim.x * PTS + threadIdx.x);
+  if (i0 > d.nx - 1)
+    return;
+  const int qp = (i0 - 1) & 1; // the same for every point of the thread
+  int p[PTS];
+  bool ok[PTS];
+  unsigned b[PTS];
+#pragma unroll
+  for (int r = 0; r < PTS; ++r) {
+    const int i = i0 + 64 * r;
+    ok[r] = i <= d.nx - 1;
+    p[r] = sp.at(ok[r] ? i : i0, j, k);
+    b[r] = code[p[r]]; // every interior point has a byte
+  }
+  CodeLut L;
+  const bool coded = load_lut(info, L);
+  T s[PTS], f[PTS], c[PTS];
+#pragma unroll
+  for (int r = 0; r < PTS; ++r) {
+    const SplitNb nb = split_nb(sp, p[r], qp);
+    Couplings<T> cp;
+    if (coded) {
+      cp.e = (b[r] & 1u) ? L.eh : L.el;
+      cp.w = (b[r] & 2u) ? L.eh : L.el;
+      cp.n = (b[r] & 4u) ? L.nh : L.nl;
+      cp.s = (b[r] & 8u) ? L.nh : L.nl;
+      cp.u = (b[r] & 16u) ? L.uh : L.ul;
+      cp.dn = (b[r] & 32u) ? L.uh : L.ul;
+    } else {
+      cp = couplings<T>(false, L, code, oE, oN, uC, p[r], nb);
+    }
+    s[r] = cp.n * x[nb.n] + cp.s * x[nb.s] + cp.e * x[nb.e] +
+           cp.w * x[nb.w] + cp.dn * x[nb.dn] + cp.u * x[nb.u];
+    f[r] = fc[p[r]];
+    c[r] = oC[p[r]];
+  }
+#pragma unroll
+  for (int r = 0; r < PTS; ++r)
+    if (ok[r])
+      x[p[r]] = (f[r] + keep * s[r]) / (c[r] + T(0));
+}
+
+// points per thread of the coded colour pass
+constexpr int kCodePts = 2;
+
+template <typename T>
+int launch_gs7_code(const Dims &d, const T *oC, const T *fc, const T *oE,
+                    const T *oN, const T *uC, const unsigned char *code,
+                    const int *info, T *x, int itmax, int iadjoint,
+                    int zero_init, cudaStream_t s) {
+  const dim3 g(cdiv(cdiv(d.nx - 2, 2), 32 * kCodePts), cdiv(d.ny - 2, 8),
+               (unsigned)(d.nz - 2));
+  for (int it = 0; it < itmax; ++it)
+    for (int c = 0; c <= 1; ++c) {
+      const int want = (1 - iadjoint) * c + iadjoint * (1 - c);
+      const T keep = zero_init ? T(0) : T(1);
+      gs7_code_color_kernel<T, kCodePts><<<g, interior_block(), 0, s>>>(
+          d, oC, fc, oE, oN, uC, code, info, x, want, keep);
+      zero_init = 0;
+    }
+  PMG_LAUNCH_CHECK();
+  return PMG_OK;
+}
+
+// defect7_split_kernel with the couplings from the code byte when coded;
+// two points per thread (32 apart in the row) for the same reason as the
+// colour pass
+template <typename T>
+__global__ void __launch_bounds__(256)
+    defect7_code_kernel(Dims d, const T *__restrict__ oC,
+                        const T *__restrict__ oE, const T *__restrict__ oN,
+                        const T *__restrict__ uC,
+                        const unsigned char *__restrict__ code,
+                        const int *__restrict__ info, const T *__restrict__ f,
+                        const T *__restrict__ x, T *__restrict__ r) {
+  const int i0 = blockIdx.x * blockDim.x * 2 + threadIdx.x + 2;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
+  const int k = blockIdx.z + 2;
+  if (i0 > d.nx - 1 || j > d.ny - 1)
+    return;
+  const Split sp = Split::of(d);
+  int ii[2], p[2];
+  bool ok[2];
+  unsigned b[2];
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    ii[q] = i0 + 32 * q;
+    ok[q] = ii[q] <= d.nx - 1;
+    if (!ok[q])
+      ii[q] = i0;
+    p[q] = sp.at(ii[q], j, k);
+    b[q] = code[p[q]];
+  }
+  CodeLut L;
+  const bool coded = load_lut(info, L);
+  T out[2];
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    const SplitNb nb = split_nb(sp, p[q], (ii[q] - 1) & 1);
+    Couplings<T> c;
+    if (coded) {
+      c.e = (b[q] & 1u) ? L.eh : L.el;
+      c.w = (b[q] & 2u) ? L.eh : L.el;
+      c.n = (b[q] & 4u) ? L.nh : L.nl;
+      c.s = (b[q] & 8u) ? L.nh : L.nl;
+      c.u = (b[q] & 16u) ? L.uh : L.ul;
+      c.dn = (b[q] & 32u) ? L.uh : L.ul;
+    } else {
+      c = couplings<T>(false, L, code, oE, oN, uC, p[q], nb);
+    }
+    const T ax = -c.n * x[nb.n] - c.s * x[nb.s] - c.e * x[nb.e] -
+                 c.w * x[nb.w] - c.dn * x[nb.dn] - c.u * x[nb.u] +
+                 (oC[p[q]] + T(0)) * x[p[q]];
+    out[q] = f[p[q]] - ax;
+  }
+#pragma unroll
+  for (int q = 0; q < 2; ++q)
+    if (ok[q])
+      r[d.at(ii[q], j, k)] = out[q];
+}
+
+// ---- the double operator of the same level (the refinement residual) ----
+// The double couplings take the code bytes of the float ones when each
+// direction's double values are two as well: lut64[2q + bit] holds the
+// double value of direction q (E, N, U) for a bit, and info[7] is set when
+// any double coupling differs from its entry bit for bit.
+template <typename T>
+__device__ __forceinline__ void couplings64_of(const Dims &d, const T *oE,
+                                               const T *oN, const T *uC,
+                                               int p, T (&c)[6]) {
+  c[0] = oE[p];
+  c[1] = oE[p - 1];
+  c[2] = oN[p];
+  c[3] = oN[p - d.sy()];
+  c[4] = uC[p];
+  c[5] = uC[p - d.sz()];
+}
+
+// pass 1: every point stores its double couplings under their bits (equal
+// values when the level is two-valued; pass 2 finds out)
+template <typename T>
+__global__ void __launch_bounds__(256)
+    lut64_store_kernel(Dims d, const T *__restrict__ oE,
+                       const T *__restrict__ oN, const T *__restrict__ uC,
+                       const unsigned char *__restrict__ code, T *lut64) {
+  const Interior t = interior_point(d);
+  if (!t.ok)
+    return;
+  const int p = d.at(t.i, t.j, t.k);
+  const unsigned b = code[Split::of(d).at(t.i, t.j, t.k)];
+  T c[6];
+  couplings64_of(d, oE, oN, uC, p, c);
+#pragma unroll
+  for (int q = 0; q < 6; ++q)
+    lut64[2 * (q >> 1) + ((b >> q) & 1u)] = c[q];
+}
+
+// pass 2: info[7] |= 1 on any double coupling that is not its entry
+template <typename T>
+__global__ void __launch_bounds__(256)
+    lut64_check_kernel(Dims d, const T *__restrict__ oE,
+                       const T *__restrict__ oN, const T *__restrict__ uC,
+                       const unsigned char *__restrict__ code,
+                       const T *__restrict__ lut64, int *info) {
+  const Interior t = interior_point(d);
+  if (!t.ok)
+    return;
+  const int p = d.at(t.i, t.j, t.k);
+  const unsigned b = code[Split::of(d).at(t.i, t.j, t.k)];
+  T c[6];
+  couplings64_of(d, oE, oN, uC, p, c);
+  bool bad = false;
+#pragma unroll
+  for (int q = 0; q < 6; ++q)
+    bad |= __double_as_longlong(c[q]) !=
+           __double_as_longlong(lut64[2 * (q >> 1) + ((b >> q) & 1u)]);
+  if (bad)
+    atomicOr(&info[7], 1);
+}
+
+// defect_norm_kernel<7, double, float, true> (the refinement residual r =
+// f - A x64, written to the split float right-hand side, and its sum of
+// squares) with the double couplings from the code bytes when both codings
+// hold: the same values, the same order, the same bits.
+template <typename T>
+__global__ void __launch_bounds__(kReduceThreads)
+    defect_norm_code_kernel(Dims d, Op14<T> A, const T *__restrict__ f,
+                            const T *__restrict__ x,
+                            const unsigned char *__restrict__ code,
+                            const T *__restrict__ lut64,
+                            const int *__restrict__ info,
+                            float *__restrict__ r, ReduceSlot s) {
+  __shared__ double sh[32];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
+  const int k0 = 2 + blockIdx.z * kReducePlanes;
+  const int k1 = min(k0 + kReducePlanes - 1, d.nz - 1);
+  const int sy = d.sy(), sz = d.sz();
+  const bool coded = info[6] == 0 && info[7] == 0;
+  T lut[6];
+#pragma unroll
+  for (int q = 0; q < 6; ++q)
+    lut[q] = coded ? lut64[q] : T(0);
+  const Split sp = Split::of(d);
+  double acc = 0.0;
+  if (i <= d.nx - 1 && j <= d.ny - 1) {
+    for (int k = k0; k <= k1; ++k) {
+      const int p = d.at(i, j, k);
+      const int sidx = sp.at(i, j, k);
+      T c[6];
+      if (coded) {
+        const unsigned b = code[sidx];
+#pragma unroll
+        for (int q = 0; q < 6; ++q)
+          c[q] = lut[2 * (q >> 1) + ((b >> q) & 1u)];
+      } else {
+        couplings64_of(d, A.a[kOE], A.a[kON], A.a[kUC], p, c);
+      }
+      // apply7's order: -oN x_n - oN_s x_s - oE x_e - oE_w x_w - uC_d x_d
+      // - uC x_u + (oC + 0) x
+      const T ax = -c[2] * x[p + sy] - c[3] * x[p - sy] - c[0] * x[p + 1] -
+                   c[1] * x[p - 1] - c[5] * x[p - sz] - c[4] * x[p + sz] +
+                   (A.a[kOC][p] + T(0)) * x[p];
+      const T dv = f[p] - ax;
+      r[sidx] = (float)dv;
+      acc += (double)dv * (double)dv;
+    }
+  }
+  double v[1] = {block_sum_2d(acc, sh)};
+  reduce_finish<1>(v, s, nullptr);
+}
+
+inline dim3 defect7_code_grid(const Dims &d) {
+  return dim3(cdiv(d.nx - 2, 64), cdiv(d.ny - 2, 8), (unsigned)(d.nz - 2));
 }
 
 } // namespace pmg

@@ -217,6 +217,21 @@ class PBELinearProblem:
         _lib.check("pmg_problem_set_throughput_mode",
                    _lib.lib.pmg_problem_set_throughput_mode(self._h, int(on)))
 
+    def set_coded_couplings(self, on: bool = True) -> None:
+        """Mixed precision: read the finest couplings as one code byte per
+        point when the operator has two values per direction (default on;
+        the same bits either way)."""
+        _lib.check("pmg_problem_set_coded_couplings",
+                   _lib.lib.pmg_problem_set_coded_couplings(self._h, int(on)))
+
+    def coded_couplings(self) -> bool:
+        """Whether the built mixed problem's finest couplings are coded."""
+        c = ctypes.c_int()
+        _lib.check("pmg_problem_coded_couplings",
+                   _lib.lib.pmg_problem_coded_couplings(self._h,
+                                                        ctypes.byref(c)))
+        return bool(c.value)
+
     def set_profiling(self, on: bool = True) -> None:
         """Time every cycle phase with CUDA events inside the cycle graph."""
         _lib.check("pmg_problem_set_profiling",

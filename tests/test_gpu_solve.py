@@ -315,6 +315,39 @@ def test_throughput_mode_same_solve_within_tolerance(pb65):
     assert np.linalg.norm(x1 - x0) <= 1e-9 * np.linalg.norm(x0)
 
 
+def test_coded_couplings_give_the_same_bits(pb65):
+    """The class's fine operator has two coupling values per direction, so
+    the mixed path's finest smoother and defect read code bytes; the solve
+    is bit-identical to the one reading the coupling arrays. An operator
+    with more values per direction is not coded and solves the same with
+    the switch on or off."""
+    w, fine = pb65
+    out = {}
+    for case in ("class", "random"):
+        f = dict(fine)
+        if case == "random":  # a third value in oE: no coding
+            rng = np.random.default_rng(1)
+            oE = np.array(f["oE"], copy=True)
+            flat = oE.reshape(-1)
+            pick = rng.choice(flat.size, 50, replace=False)
+            flat[pick] = flat[pick] * 1.01
+            f["oE"] = oE
+        for on in (True, False):
+            with PBELinearProblem(w.base, w.nlev, w.box, "mixed",
+                                  w.physics) as p:
+                p.set_coded_couplings(on)
+                p.set_fine(**f)
+                p.buildmultilevelops()
+                coded = p.coded_couplings()
+                r = p.solve(tol=1e-10, max_cycles=100)
+                out[case, on] = (coded, r.cycles, p.potential().ravel().copy())
+    assert out["class", True][0] and not out["class", False][0]
+    assert not out["random", True][0]
+    for case in ("class", "random"):
+        assert out[case, True][1] == out[case, False][1]
+        assert np.array_equal(out[case, True][2], out[case, False][2])
+
+
 @pytest.mark.parametrize("throughput", [False, True])
 @pytest.mark.parametrize("base,nlev", [(2, 2), (2, 3), (2, 4), (1, 5)])
 def test_mixed_lowest_levels_shapes(base, nlev, throughput):
