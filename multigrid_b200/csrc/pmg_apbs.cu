@@ -567,7 +567,9 @@ struct ApbsDriver {
       scratch_free(block, s);
   }
 
-  ReduceSlot slot(double *out) const { return ReduceSlot{partials, ticket, out}; }
+  ReduceSlot slot(double *out) const {
+    return ReduceSlot{partials, ticket, out};
+  }
 
   int fetch(const double *dev, double *host) {
     PMG_CUDA_TRY(cudaMemcpyAsync(host, dev, sizeof(double),

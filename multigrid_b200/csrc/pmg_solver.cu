@@ -1275,13 +1275,14 @@ int pmg_build_hierarchy(pmg_problem *p, int trilinear) {
                          INT_MAX, INT_MIN, 0,       0};
     PMG_CUDA_TRY(cudaMemcpyAsync(v.code_info, init, sizeof(init),
                                  cudaMemcpyHostToDevice, s));
-    coupling_range_kernel<float><<<interior_grid(v.d), interior_block(), 0, s>>>(
+    const dim3 ig = interior_grid(v.d), ib = interior_block();
+    coupling_range_kernel<float><<<ig, ib, 0, s>>>(
         v.d, v.op32[kOE], v.op32[kON], v.op32[kUC], v.code_info);
-    coupling_code_kernel<float><<<interior_grid(v.d), interior_block(), 0, s>>>(
+    coupling_code_kernel<float><<<ig, ib, 0, s>>>(
         v.d, v.op32[kOE], v.op32[kON], v.op32[kUC], v.code_info, v.code);
-    lut64_store_kernel<double><<<interior_grid(v.d), interior_block(), 0, s>>>(
+    lut64_store_kernel<double><<<ig, ib, 0, s>>>(
         v.d, v.op[kOE], v.op[kON], v.op[kUC], v.code, v.lut64);
-    lut64_check_kernel<double><<<interior_grid(v.d), interior_block(), 0, s>>>(
+    lut64_check_kernel<double><<<ig, ib, 0, s>>>(
         v.d, v.op[kOE], v.op[kON], v.op[kUC], v.code, v.lut64, v.code_info);
     p->launches += 4;
     if (trilinear) // the trilinear builder writes double only

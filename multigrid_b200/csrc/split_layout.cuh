@@ -520,22 +520,32 @@ __global__ void __launch_bounds__(kReduceThreads)
   const int k1 = min(k0 + kReducePlanes - 1, d.nz - 1);
   const int sy = d.sy(), sz = d.sz();
   const bool coded = info[6] == 0 && info[7] == 0;
-  T lut[6];
-#pragma unroll
-  for (int q = 0; q < 6; ++q)
-    lut[q] = coded ? lut64[q] : T(0);
+  // low / high double value per direction, in registers (selected below,
+  // never indexed at run time)
+  const T el = coded ? lut64[0] : T(0), eh = coded ? lut64[1] : T(0);
+  const T nl = coded ? lut64[2] : T(0), nh = coded ? lut64[3] : T(0);
+  const T ul = coded ? lut64[4] : T(0), uh = coded ? lut64[5] : T(0);
   const Split sp = Split::of(d);
   double acc = 0.0;
   if (i <= d.nx - 1 && j <= d.ny - 1) {
-    for (int k = k0; k <= k1; ++k) {
+    // unrolled over the block's planes so the loads of several planes are
+    // in flight together; acc still adds the planes in order
+#pragma unroll
+    for (int q = 0; q < kReducePlanes; ++q) {
+      const int k = k0 + q;
+      if (k > k1)
+        break;
       const int p = d.at(i, j, k);
       const int sidx = sp.at(i, j, k);
       T c[6];
       if (coded) {
         const unsigned b = code[sidx];
-#pragma unroll
-        for (int q = 0; q < 6; ++q)
-          c[q] = lut[2 * (q >> 1) + ((b >> q) & 1u)];
+        c[0] = (b & 1u) ? eh : el;
+        c[1] = (b & 2u) ? eh : el;
+        c[2] = (b & 4u) ? nh : nl;
+        c[3] = (b & 8u) ? nh : nl;
+        c[4] = (b & 16u) ? uh : ul;
+        c[5] = (b & 32u) ? uh : ul;
       } else {
         couplings64_of(d, A.a[kOE], A.a[kON], A.a[kUC], p, c);
       }
