@@ -1276,7 +1276,7 @@ int pmg_build_hierarchy(pmg_problem *p, int trilinear) {
     PMG_CUDA_TRY(cudaMemcpyAsync(v.code_info, init, sizeof(init),
                                  cudaMemcpyHostToDevice, s));
     const dim3 ig = interior_grid(v.d), ib = interior_block();
-    coupling_range_kernel<float><<<ig, ib, 0, s>>>(
+    coupling_range_kernel<float><<<coupling_range_blocks(v.d), 256, 0, s>>>(
         v.d, v.op32[kOE], v.op32[kON], v.op32[kUC], v.code_info);
     coupling_code_kernel<float><<<ig, ib, 0, s>>>(
         v.d, v.op32[kOE], v.op32[kON], v.op32[kUC], v.code_info, v.code);

@@ -185,28 +185,33 @@ __host__ __device__ inline float order_float(int i) {
 
 // info[0..5] = min, max of oE, oN, uC over the couplings the interior
 // points read (ordered ints; info[0,2,4] start at INT_MAX, [1,3,5] at
-// INT_MIN)
+// INT_MIN). A grid-stride loop, then warp and block reductions, so only
+// one thread per block touches the six global words.
 template <typename T>
 __global__ void __launch_bounds__(256)
     coupling_range_kernel(Dims d, const T *__restrict__ oE,
                           const T *__restrict__ oN,
                           const T *__restrict__ uC, int *info) {
-  const Interior t = interior_point(d);
+  __shared__ int sh[6][8];
   int v[6] = {INT_MAX, INT_MIN, INT_MAX, INT_MIN, INT_MAX, INT_MIN};
-  if (t.ok) {
-    const Split sp = Split::of(d);
-    const int p = sp.at(t.i, t.j, t.k);
-    const SplitNb nb = split_nb(sp, p, (t.i - 1) & 1);
-    const int e0 = float_order(oE[p]), e1 = float_order(oE[nb.w]);
-    const int n0 = float_order(oN[p]), n1 = float_order(oN[nb.s]);
-    const int u0 = float_order(uC[p]), u1 = float_order(uC[nb.dn]);
-    v[0] = min(e0, e1);
-    v[1] = max(e0, e1);
-    v[2] = min(n0, n1);
-    v[3] = max(n0, n1);
-    v[4] = min(u0, u1);
-    v[5] = max(u0, u1);
+  const Split sp = Split::of(d);
+  const int total = (d.nx - 2) * (d.ny - 2) * (d.nz - 2);
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < total;
+       q += gridDim.x * blockDim.x) {
+    int i, j, k;
+    interior_coords(d, q, i, j, k);
+    const int p = sp.at(i, j, k);
+    const SplitNb nb = split_nb(sp, p, (i - 1) & 1);
+    const int c[6] = {float_order(oE[p]), float_order(oE[nb.w]),
+                      float_order(oN[p]), float_order(oN[nb.s]),
+                      float_order(uC[p]), float_order(uC[nb.dn])};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      v[2 * a] = min(v[2 * a], min(c[2 * a], c[2 * a + 1]));
+      v[2 * a + 1] = max(v[2 * a + 1], max(c[2 * a], c[2 * a + 1]));
+    }
   }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
   for (int q = 0; q < 6; ++q) {
 #pragma unroll
@@ -214,15 +219,29 @@ __global__ void __launch_bounds__(256)
       const int w = __shfl_xor_sync(0xffffffffu, v[q], o);
       v[q] = (q & 1) ? max(v[q], w) : min(v[q], w);
     }
+    if (lane == 0)
+      sh[q][warp] = v[q];
   }
-  if ((threadIdx.x & 31) == 0)
-#pragma unroll
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int nw = blockDim.x >> 5;
     for (int q = 0; q < 6; ++q) {
+      int r = sh[q][0];
+      for (int w = 1; w < nw; ++w)
+        r = (q & 1) ? max(r, sh[q][w]) : min(r, sh[q][w]);
       if (q & 1)
-        atomicMax(&info[q], v[q]);
+        atomicMax(&info[q], r);
       else
-        atomicMin(&info[q], v[q]);
+        atomicMin(&info[q], r);
     }
+  }
+}
+
+// blocks of coupling_range_kernel: enough to fill the GPU a few times over
+inline unsigned coupling_range_blocks(const Dims &d) {
+  const long total = (long)(d.nx - 2) * (d.ny - 2) * (d.nz - 2);
+  const long want = (total + 255) / 256;
+  return (unsigned)(want < 148 * 8 ? want : 148 * 8);
 }
 
 // code bytes of the interior points; info[6] |= 1 when a coupling is
