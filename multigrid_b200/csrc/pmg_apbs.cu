@@ -330,10 +330,14 @@ __global__ void __launch_bounds__(kReduceThreads)
 // :113-165), bit for bit the reference's arithmetic.
 // ---------------------------------------------------------------------------
 
-// One column of the band per interior point. For 27-point operators the
-// coupling with each earlier neighbour q is read where the matvec reads it
-// (at q); the reference reads those ten at the point below or south of p
-// (buildBd.cc:170-245), which is not the operator its matvec applies.
+// One column of the band per interior point; cc is not part of it, as in
+// the reference (Vbuildband takes ac only). Only couplings with interior
+// neighbours are stored: the reference also writes the offsets of shell
+// neighbours, which on grids with one interior point along x alias the
+// diagonal or pass the end of the column (buildBd.cc:150-247). For
+// 27-point operators the coupling with each earlier neighbour q is read
+// where the matvec reads it (at q); the reference reads those ten at the
+// point below or south of p, which is not the operator its matvec applies.
 template <int KIND>
 __global__ void band_kernel(Dims d, Op14<double> A, double *__restrict__ abd,
                             int m, int lda) {
@@ -345,27 +349,34 @@ __global__ void band_kernel(Dims d, Op14<double> A, double *__restrict__ abd,
   const int jj = (k - 2) * mx * my + (j - 2) * mx + (i - 2) + 1;
   double *col = abd + (size_t)(jj - 1) * lda + m; // col[off] = A(jj+off, jj)
   const double *const *a = A.a;
-  auto at = [&](int arr, int di, int dj, int dk) {
-    return a[arr][d.at(i + di, j + dj, k + dk)];
+  // the coupling with the earlier neighbour (di, dj, dk), stored at offset
+  // di + dj mx + dk mx my, which lies in [-m, -1] for interior neighbours;
+  // shell neighbours are skipped
+  auto put = [&](int arr, int di, int dj, int dk) {
+    const int ii = i + di, jn = j + dj, kn = k + dk;
+    if (ii < 2 || ii > d.nx - 1 || jn < 2 || jn > d.ny - 1 || kn < 2 ||
+        kn > d.nz - 1)
+      return;
+    col[di + dj * mx + dk * mx * my] = -a[arr][d.at(ii, jn, kn)];
   };
-  col[0] = at(kOC, 0, 0, 0);
-  col[-1] = -at(kOE, -1, 0, 0);
-  col[-mx] = -at(kON, 0, -1, 0);
+  col[0] = a[kOC][d.at(i, j, k)];
+  put(kOE, -1, 0, 0);
+  put(kON, 0, -1, 0);
   if (KIND == 7) {
-    col[-mx * my] = -at(kUC, 0, 0, -1);
+    put(kUC, 0, 0, -1);
     return;
   }
-  col[-mx + 1] = -at(kONW, 1, -1, 0);
-  col[-mx - 1] = -at(kONE, -1, -1, 0);
-  col[-mx * my] = -at(kUC, 0, 0, -1);
-  col[-mx * my + 1] = -at(kUW, 1, 0, -1);
-  col[-mx * my - 1] = -at(kUE, -1, 0, -1);
-  col[-mx * my + mx] = -at(kUS, 0, 1, -1);
-  col[-mx * my - mx] = -at(kUN, 0, -1, -1);
-  col[-mx * my + mx + 1] = -at(kUSW, 1, 1, -1);
-  col[-mx * my + mx - 1] = -at(kUSE, -1, 1, -1);
-  col[-mx * my - mx + 1] = -at(kUNW, 1, -1, -1);
-  col[-mx * my - mx - 1] = -at(kUNE, -1, -1, -1);
+  put(kONW, 1, -1, 0);
+  put(kONE, -1, -1, 0);
+  put(kUC, 0, 0, -1);
+  put(kUW, 1, 0, -1);
+  put(kUE, -1, 0, -1);
+  put(kUS, 0, 1, -1);
+  put(kUN, 0, -1, -1);
+  put(kUSW, 1, 1, -1);
+  put(kUSE, -1, 1, -1);
+  put(kUNW, 1, -1, -1);
+  put(kUNE, -1, -1, -1);
 }
 
 // LINPACK's unit-stride dot product: the first n % 5 terms one by one, then

@@ -666,14 +666,17 @@ static double ddot5(int n, const double *x, const double *y) {
   return t;
 }
 
-/* Band storage of the interior operator (the caller zeroes abd, lda*n).
- * Couplings are written for every listed offset, also where the offset
- * wraps to the previous row or plane (there the coefficient read is a shell
- * one, zero for operators built on the interior), as the reference writes
- * them. For 27-point operators the reference reads the ten diagonal
- * couplings at the point below or south of p (buildBd.cc:170-245), which
- * is not the operator its matvec applies; this stores the coupling with
- * each earlier neighbour q where the matvec reads it, at q. */
+/* Band storage of the interior operator (the caller zeroes abd, lda*n);
+ * cc is not part of it, as in the reference (Vbuildband takes ac only).
+ * Only couplings with interior neighbours are stored. The reference also
+ * writes the offsets of shell neighbours, which wrap to the previous row or
+ * plane (a shell coefficient, zero for operators built on the interior);
+ * on grids with one interior point along x (3 points) some of those
+ * offsets alias the diagonal or pass the end of the column, i.e. of the
+ * array (buildBd.cc:150-247). For 27-point operators the reference reads
+ * the ten diagonal couplings at the point below or south of p, which is not
+ * the operator its matvec applies; this stores the coupling with each
+ * earlier neighbour q where the matvec reads it, at q. */
 void pmgo_buildband(int nx, int ny, int nz, const pmgo_op *A, int *n_out,
                     int *m_out, int *lda_out, double *abd) {
   const int mx = nx - 2, my = ny - 2;
@@ -689,8 +692,14 @@ void pmgo_buildband(int nx, int ny, int nz, const pmgo_op *A, int *n_out,
         const int jj = (k - 2) * mx * my + (j - 2) * mx + (i - 2) + 1;
         double *col = abd + (size_t)(jj - 1) * lda;
         /* row offset ii - jj, coefficient array, its point (di, dj, dk) */
+/* only couplings with interior neighbours (whose offset lies in [-m, -1]) */
 #define BAND(off, arr, di, dj, dk, sign)                                       \
-  col[(off) + m] = sign a[arr][IX(nx, ny, i + (di), j + (dj), k + (dk))]
+  do {                                                                         \
+    if (i + (di) >= 2 && i + (di) <= nx - 1 && j + (dj) >= 2 &&              \
+        j + (dj) <= ny - 1 && k + (dk) >= 2 && k + (dk) <= nz - 1)             \
+      col[(off) + m] =                                                         \
+          sign a[arr][IX(nx, ny, i + (di), j + (dj), k + (dk))];               \
+  } while (0)
         BAND(0, 0, 0, 0, 0, +);
         BAND(-1, 1, -1, 0, 0, -);
         BAND(-mx, 2, 0, -1, 0, -);

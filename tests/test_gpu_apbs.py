@@ -56,6 +56,7 @@ def rel(a, b):
     (33, 4, dict(mgsolv=1, mgprol=0)),
     (17, 3, dict(mgcoar=0)),
     (33, 4, dict(mgcoar=0, mgsolv=1)),
+    (17, 4, dict(mgsolv=1)),  # 3^3 coarsest level: one unknown in the band
 ])
 def test_apbs_driver_matches_restatement(restatement, n, nlev, kw):
     maps = apbs_maps(n, n + nlev)

@@ -281,6 +281,35 @@ def test_band_solver_bitexact(restatement, golden_band):
     assert np.abs(Ax[idx] - g["b27"]).max() <= 1e-12 * np.abs(g["b27"]).max()
 
 
+@pytest.mark.parametrize("nlev,mgsolv,mgcoar", [(4, 0, 2), (4, 1, 2),
+                                                 (4, 1, 0), (1, 1, 2)])
+def test_apbs_driver_restatement_extreme_levels(restatement, nlev, mgsolv,
+                                                 mgcoar):
+    """The restated driver down to a 3^3 coarsest level (one unknown) and
+    with a single level (the coarse solve alone), for both coarse solvers:
+    the same box-system solution."""
+    n = 17
+    maps = apbs_maps(n, 40 + nlev)
+    iparm, rparm = apbs_params(n, nlev, mgsolv=mgsolv, mgcoar=mgcoar,
+                               itmax=80)
+    u = np.zeros(n ** 3)
+    it, ierr, ratio = restatement.mgdriv(iparm, rparm, u, maps)
+    out = [np.zeros(n ** 3) for _ in range(6)]
+    restatement.buildA_fv(n, n, n, 0, maps, out)
+    oC, cc, fc, oE, oN, uC = out
+    if nlev == 1 and mgsolv == 1:
+        # one direct band solve of the operator without cc (the band holds
+        # ac only, as the reference's Vbuildband)
+        A0, idx = dense_operator(n, [oC, oE, oN, uC], np.zeros(n ** 3))
+        want = np.linalg.solve(A0, fc[idx])
+        assert it == 1
+    else:
+        A, idx = dense_operator(n, [oC, oE, oN, uC], cc)
+        want = np.linalg.solve(A, fc[idx])
+        assert ierr == 0 and ratio <= 1e-10
+    assert np.abs(u[idx] - want).max() <= 1e-8 * np.abs(want).max()
+
+
 def test_hierarchy(restatement, golden_problem):
     g = golden_problem
     base, nlev = int(g["base"]), int(g["nlev"])
