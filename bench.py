@@ -260,7 +260,8 @@ def workload_config(w, precision):
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
-def phase_bytes(p, level: int, phase: str, esz: int) -> float | None:
+def phase_bytes(p, level: int, phase: str, esz: int,
+                coded: bool = False) -> float | None:
     """Algorithmic bytes moved by one occurrence of a cycle phase (counted in
     arrays of the level's n^3 points; see the kernel table of the design
     notes)."""
@@ -269,7 +270,6 @@ def phase_bytes(p, level: int, phase: str, esz: int) -> float | None:
     nf3 = float(p.n ** 3)
     fine = level == p.nlev
     nc3 = float(level_n(p.base, level - 1) ** 3) if level >= 2 else 0.0
-    coded = getattr(p, "_coded", False)
     if level == 0:
         if phase == "residual" and coded:  # oC, code byte, f, x; float r
             return nf3 * (3 * 8 + 1 + 4)
@@ -298,17 +298,16 @@ def phase_bytes(p, level: int, phase: str, esz: int) -> float | None:
 
 
 # kernel launched by a cycle phase, and launches per phase occurrence
-def phase_kernel(p, level: int, phase: str):
+def phase_kernel(p, level: int, phase: str, coded: bool = False):
     if phase in ("pre-smooth", "post-smooth"):
         if level < p.nlev:
             return ("gs27_phase_kernel", 4)
         # the mixed path's finest float level is colour-split (and coded
         # when its couplings have two values per direction)
         if p.precision == "mixed":
-            return ("gs7_code_color_kernel" if getattr(p, "_coded", False)
+            return ("gs7_code_color_kernel" if coded
                     else "gs7_split_color_kernel", 4)
         return ("gs7_color_kernel", 4)
-    coded = getattr(p, "_coded", False)
     if phase == "defect" and level == p.nlev and coded:
         return ("defect7_code_kernel", 1)
     if phase == "residual" and coded:
@@ -339,10 +338,10 @@ def profiled_traffic(kernel: str | None, launches: int, workload: str,
     return float(m.group(1)) * launches if m else None
 
 
-def profile_solve(p, step, dev, esz):
+def profile_solve(p, step, dev, esz, coded=False):
     """One extra solve with CUDA events recorded around every cycle phase
-    inside the cycle graph; returns per-phase averages and bandwidths."""
-    p._coded = p.precision == "mixed" and p.coded_couplings()
+    inside the cycle graph; returns per-phase averages and bandwidths
+    (coded: the finest couplings are read as code bytes)."""
     p.set_profiling(True)
     p.profile(reset=True)
     step(p, dev)
@@ -351,7 +350,7 @@ def profile_solve(p, step, dev, esz):
     rows = []
     for (L, ph), (ms, cnt) in prof.items():
         avg_ms = ms / cnt
-        b = phase_bytes(p, L, ph, esz if L != 1 else 8)
+        b = phase_bytes(p, L, ph, esz if L != 1 else 8, coded)
         rows.append({"level": L, "phase": ph, "ms_total": ms, "count": cnt,
                      "us_avg": 1000 * avg_ms,
                      "gbs": (b / (avg_ms / 1000) / 1e9) if b else None,
@@ -736,9 +735,10 @@ def main():
     # roofline
     peak, peak_kind = peaks()
     esz = 4 if args.precision == "mixed" else 8
-    phases = profile_solve(p, step, dev, esz)
+    coded = args.precision == "mixed" and p.coded_couplings()
+    phases = profile_solve(p, step, dev, esz, coded)
     dom = next(r for r in phases if r["gbs"])
-    kname, klaunches = phase_kernel(p, dom["level"], dom["phase"])
+    kname, klaunches = phase_kernel(p, dom["level"], dom["phase"], coded)
     roofline = {"bound": "hbm",
                 "kernel": (f"{kname} x{klaunches}: level {dom['level']} "
                            f"{dom['phase']}"),
@@ -750,8 +750,7 @@ def main():
                 "peak_source": peak_kind,
                 "bytes_basis": (
                     "coded couplings: per point oC, one code byte, f, x"
-                    if getattr(p, "_coded", False) and dom["level"] >= 0
-                    and kname and "code" in kname else
+                    if coded and kname and "code" in kname else
                     "coefficient arrays as stored (kernel table)"),
                 "algorithmic_bytes_per_launch": dom["bytes"],
                 "avg_launch_us": dom["us_avg"]}
