@@ -257,3 +257,18 @@ def test_bench_phase_accounting():
         "defect_norm_code_kernel"
     assert bench.phase_kernel(p, 6, "pre-smooth", True)[0] == \
         "gs27_phase_kernel"
+
+
+def test_c_header_compiles_as_c99(tmp_path):
+    """include/pmg_b200.h is the C ABI: plain C99, no C++ or CUDA types."""
+    import shutil
+    import subprocess
+    gcc = shutil.which("gcc")
+    if not gcc:
+        pytest.skip("gcc not found")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    src = tmp_path / "abi.c"
+    src.write_text('#include "pmg_b200.h"\nint main(void) { return 0; }\n')
+    subprocess.run([gcc, "-std=c99", "-Wall", "-Werror", "-pedantic", "-I",
+                    os.path.join(root, "include"), "-c", str(src), "-o",
+                    str(tmp_path / "abi.o")], check=True)
