@@ -419,3 +419,22 @@ def test_pcg_restatement_converges_to_the_solve(golden_problem, restatement):
     assert 0 < c <= cs
     assert h[-1] / h[0] < 1e-10
     assert np.linalg.norm(xo - xs) <= 1e-9 * np.linalg.norm(xs)
+
+
+def test_reference_fine_couplings_are_two_valued(golden_problem):
+    """The property the mixed path's coded couplings rest on, checked on the
+    reference's own set-up (PBE_pmgc_class.h:248-318): over the couplings
+    the interior points read, oE, oN and uC each take two values (inside and
+    outside dielectric), in double and after rounding to float."""
+    g = golden_problem
+    n = int(g["base"]) * 2 ** int(g["nlev"]) + 1
+    f = fine_of(g)
+    sl = slice(1, n - 1)
+    a = {k: f[k].reshape(n, n, n) for k in ("oE", "oN", "uC")}
+    lo = slice(0, n - 1)  # along the coupling: the lower face of i = 2 too
+    read = {"oE": a["oE"][sl, sl, lo].ravel(),   # [k, j, i]
+            "oN": a["oN"][sl, lo, sl].ravel(),
+            "uC": a["uC"][lo, sl, sl].ravel()}
+    for k, v in read.items():
+        assert len(np.unique(v)) <= 2, k
+        assert len(np.unique(v.astype(np.float32))) <= 2, k
