@@ -272,3 +272,16 @@ def test_c_header_compiles_as_c99(tmp_path):
     subprocess.run([gcc, "-std=c99", "-Wall", "-Werror", "-pedantic", "-I",
                     os.path.join(root, "include"), "-c", str(src), "-o",
                     str(tmp_path / "abi.o")], check=True)
+
+
+def test_packed_operator_rows_checked():
+    """pmgc's packed-operator entry points take 4 (7-point) or 14 (27-point)
+    rows; anything else is refused before any device call."""
+    torch = pytest.importorskip("torch")
+    from multigrid_b200 import pmgc
+    with pytest.raises(ValueError):
+        pmgc._packed(torch.zeros(5, 8))
+    with pytest.raises(ValueError):
+        pmgc._packed(torch.zeros(14))
+    with pytest.raises(TypeError):  # host tensors are refused
+        pmgc._packed(torch.zeros(4, 8))
