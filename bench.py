@@ -163,21 +163,42 @@ def max_over_ranks(world, value: float) -> float:
 # ---------------------------------------------------------------------------
 # CPU baseline: reference class (or the restatement) on bounded samples
 # ---------------------------------------------------------------------------
+def workload_defs():
+    """The workload definitions (multigrid_b200/molecule.py: pure Python and
+    numpy), loaded by file path so that the reference arm never imports the
+    package and so never maps the CUDA library into its process."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location(
+        "pmg_workloads", os.path.join(ROOT, "multigrid_b200", "molecule.py"))
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[spec.name] = mod  # dataclasses look the module up
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def oracle_fine(w):
+    """Fine-level inputs of workload w built by the oracle's own set-up
+    (oracle/pmg_oracle_setup.c, bit for bit the product's host set-up)."""
+    from oracle.oracle import Restatement
+    return Restatement().setup_fine(w.n, w.h, w.atoms(), w.physics)
+
+
 def cpu_sample(w, fine, fp64_cycles: int, solves: int = 1):
     """Times complete solves of the reference class on the host cores (class
     construction, hierarchy build, V-cycles to rel. residual 1e-10; OpenMP,
     all cores). Without the reference build, the single-threaded restatement
     is timed on hierarchy build + 2 V-cycles and extrapolated to
-    fp64_cycles cycles (a full solve would take minutes)."""
+    fp64_cycles cycles (a full solve would take minutes). The reference's
+    potential of the last solve is returned under "x" (not printed)."""
     from oracle.oracle import Reference, Restatement, reference_available
     cores = os.cpu_count() or 1
     if reference_available(omp=True):
         os.environ.setdefault("OMP_NUM_THREADS", str(cores))
         ref = Reference(omp=True)
-        times, cycles = [], None
+        times, cycles, x = [], None, None
         for _ in range(max(1, solves)):
             t0 = time.perf_counter()
-            _, cycles, hist = ref.solve(w.base, w.nlev, fine, tol=TOL,
+            x, cycles, hist = ref.solve(w.base, w.nlev, fine, tol=TOL,
                                         max_cycles=MAX_CYCLES)
             times.append(time.perf_counter() - t0)
         t = statistics.median(times)
@@ -188,7 +209,7 @@ def cpu_sample(w, fine, fp64_cycles: int, solves: int = 1):
                        f"(class set-up, hierarchy build, {cycles} FP64 "
                        f"V-cycles to rel. residual {hist[-1] / hist[0]:.2e}),"
                        f" median {t:.2f} s"),
-            "cycles": cycles,
+            "cycles": cycles, "x": x,
         }
     ref = Restatement()
     t0 = time.perf_counter()
@@ -206,15 +227,22 @@ def cpu_sample(w, fine, fp64_cycles: int, solves: int = 1):
     }
 
 
+# A reference solve at 257^3 takes 5-11 s on 16 host cores: the arm times at
+# most this many steps after at most this many warm-up solves.
+REF_STEP_CAP = 10
+REF_WARMUP_CAP = 1
+
+
 def run_reference(args):
-    """The reference's own PMG class on the host cores (rank 0 only): one
-    untimed solve, then `steps` timed complete solves (at most 10)."""
+    """The reference's own PMG class on the host cores (rank 0 only): at
+    most REF_WARMUP_CAP untimed solves, then at most REF_STEP_CAP timed
+    complete solves. The inputs come from the oracle's set-up; nothing of
+    the product is loaded in this process."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    from multigrid_b200.molecule import WORKLOADS
-    from multigrid_b200.problem import setup_fine
+    WORKLOADS = workload_defs().WORKLOADS
     if args.workload not in WORKLOADS:
         print(json.dumps({"impl": "reference", "unavailable":
                           f"{args.workload}: the reference solves one "
@@ -222,22 +250,26 @@ def run_reference(args):
                           "single-solve workloads"}))
         return 0
     w = WORKLOADS[args.workload]
-    fine = setup_fine(w.n, w.h, w.atoms(), w.physics)
+    fine = oracle_fine(w)
     # FP64 cycle count of this workload (used only by the extrapolated
     # restatement fallback)
     cycles = {"pb65": 13, "pb161": 16, "pb257": 24}.get(w.name, 24)
-    warm = min(args.warmup, 1)
+    warm = min(args.warmup, REF_WARMUP_CAP)
     if warm:
-        cpu_sample(w, fine, cycles, solves=1)
-    steps = max(1, min(args.steps, 10))
+        cpu_sample(w, fine, cycles, solves=warm)
+    steps = max(1, min(args.steps, REF_STEP_CAP))
     base = cpu_sample(w, fine, cycles, solves=steps)
+    base.pop("x", None)
     v = base["value"]
     out = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT,
         "n_gpus": world, "steps": steps, "warmup": warm,
+        "steps_requested": args.steps, "warmup_requested": args.warmup,
+        "step_cap": REF_STEP_CAP, "warmup_cap": REF_WARMUP_CAP,
         "ms_per_step": 1000.0 / v, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "config": workload_config(w, "fp64"),
+        "precision": "fp64", "levels_used": w.nlev,
+        "data": "synthetic", "config": workload_config(w),
         "cpu_baseline": base,
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
@@ -246,13 +278,15 @@ def run_reference(args):
     return 0
 
 
-def workload_config(w, precision):
+def workload_config(w):
+    """The workload (the same dict in both arms; how a solve computes it,
+    precision and hierarchy depth, is reported beside the config)."""
     return {
         "workload": (f"{w.name}: {w.n}^3 grid, {w.nlev} levels, h {w.h} A, "
                      f"{w.natoms}-atom synthetic molecule, linearized PBE, "
                      f"Galerkin PMG V-cycles to rel. residual 1e-10"),
         "grid": w.n, "levels": w.nlev, "spacing_A": w.h, "atoms": w.natoms,
-        "precision": precision, "tol": TOL,
+        "tol": TOL,
         "l2_flush": "inputs larger than L2 (fine level 4+2 arrays of n^3)",
     }
 
@@ -755,15 +789,26 @@ def main():
                 "algorithmic_bytes_per_launch": dom["bytes"],
                 "avg_launch_us": dom["us_avg"]}
 
+    def error(x, ref):
+        return {"rel_l2": float(np.linalg.norm(x - ref) /
+                                np.linalg.norm(ref)),
+                "max_norm": float(np.abs(x - ref).max() /
+                                  np.abs(ref).max())}
+
     xm, xd = results["mixed"]["x"], results["fp64"]["x"]
-    err = {"rel_l2": float(np.linalg.norm(xm - xd) / np.linalg.norm(xd)),
-           "max_norm": float(np.abs(xm - xd).max() / np.abs(xd).max())}
+    err = error(xm, xd)
 
     cpu = None
+    err_oracle = {}
     if world == 1 and rank == 0 and not args.no_cpu_baseline:
         try:
             cpu_sample(w, fine, results["fp64"]["cycles"][-1])  # warm-up
             cpu = cpu_sample(w, fine, results["fp64"]["cycles"][-1])
+            # the reference's own FP64 potential of the same inputs
+            xr = cpu.pop("x", None)
+            if xr is not None:
+                err_oracle = {prec: error(r["x"], xr)
+                              for prec, r in results.items()}
         except Exception as e:  # reported, never silently replaced
             cpu = {"error": str(e)}
 
@@ -777,21 +822,30 @@ def main():
             "scaling": "weak", "vs_baseline": None,
             "dtype": "f32+f64" if args.precision == "mixed" else "f64",
             "data": "synthetic",
-            "config": dict(workload_config(w, args.precision),
-                           levels_used=results[args.precision]["p"].nlev,
-                           parallelism=f"replicas x{world}"),
+            "config": workload_config(w),
+            "precision": args.precision,
+            "levels_used": results[args.precision]["p"].nlev,
+            "parallelism": f"replicas x{world}",
             "cycles": prim["cycles"][-1],
             "relres": prim["relres"],
             "fp64": {"value": fp64_value, "cycles":
                      results["fp64"]["cycles"][-1],
                      "ms_per_step": results["fp64"]["ms"] / args.steps,
-                     "levels": results["fp64"]["p"].nlev},
+                     "levels": results["fp64"]["p"].nlev,
+                     "error_vs_oracle": err_oracle.get("fp64")},
             "mixed": {"value": mixed_value, "cycles":
                       results["mixed"]["cycles"][-1],
                       "ms_per_step": results["mixed"]["ms"] / args.steps,
                       "levels": results["mixed"]["p"].nlev,
-                      "error_vs_fp64": err},
+                      "error_vs_fp64": err,
+                      "error_vs_oracle": err_oracle.get("mixed")},
             "mixed_speedup_vs_fp64": mixed_value / fp64_value,
+            # against the reference class timed in this run (cpu_baseline):
+            # the FP64 GPU solve has the reference's hierarchy and arithmetic
+            "speedup_vs_cpu_baseline": (
+                {"mixed": mixed_value / cpu["value"],
+                 "fp64_same_hierarchy": fp64_value / cpu["value"]}
+                if cpu and "value" in cpu else None),
             "fine_unknowns_x_cycles_per_s": value * (w.n - 2) ** 3 *
             prim["cycles"][-1],
             "gpu_launches": prim["launches"],

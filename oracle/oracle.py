@@ -198,6 +198,30 @@ class Restatement:
         return self.lib.pmgo_ideal_lambda(n, n, n, ctypes.byref(o), _d(x),
                                           _d(r))
 
+    def setup_fine(self, n: int, h: float, atoms: np.ndarray,
+                   physics: dict) -> dict:
+        """Fine-level arrays (oC, oE, oN, uC, f, x0) from atoms with the
+        restated set-up (pmg_oracle_setup.c); physics as the product's dict
+        (eps_in, eps_out, ionic_strength, ion_radius, temperature,
+        probe_radius)."""
+        atoms = np.ascontiguousarray(atoms, dtype=np.float64)
+        out = {k: np.empty(n ** 3) for k in ("oC", "oE", "oN", "uC", "f",
+                                             "x0")}
+        L = self.lib
+        L.pmgo_setup_fine.restype = ctypes.c_int
+        L.pmgo_setup_fine.argtypes = [ctypes.c_int, ctypes.c_double, D,
+                                      ctypes.c_int] + [ctypes.c_double] * 6 \
+            + [D] * 6
+        rc = L.pmgo_setup_fine(
+            n, h, _d(atoms), int(atoms.shape[0]), physics["eps_in"],
+            physics["eps_out"], physics["ionic_strength"],
+            physics["ion_radius"], physics["temperature"],
+            physics.get("probe_radius", 0.0),
+            *[_d(out[k]) for k in ("oC", "oE", "oN", "uC", "f", "x0")])
+        if rc != 0:
+            raise ValueError(f"pmgo_setup_fine returned {rc}")
+        return out
+
     def cg(self, n, op14, rhs, x, thresh=1e-8) -> int:
         o = self.op(op14)
         return self.lib.pmgo_cg(n, n, n, ctypes.byref(o), _d(rhs), _d(x),

@@ -119,6 +119,23 @@ long pmgo_hierarchy(int base, int nlev, const double *oC, const double *oE,
                     const double *oN, const double *uC, int trilinear,
                     double *out, long cap);
 
+/* ---- fine-level set-up from atoms (pmg_oracle_setup.c) ---------------- */
+/* kappa (1/Angstrom) and eps0 (e^2 / (kT Angstrom)) of the physics
+ * (scientific_quantities.h:7-55). */
+void pmgo_physics(double eps_out, double ionic_strength, double temperature,
+                  double *kappa, double *eps0);
+/* Fine level of an n^3 grid from natoms rows (x, y, z, radius, charge) in
+ * the grid frame: face coefficients, oC with kappa^2 eps_out folded in,
+ * trilinear charges, multiple Debye-Hueckel boundary on the shell
+ * (PBE_pmgc_class.h:141-349). probe_radius 0 is the reference's van der
+ * Waals marking; > 0 the molecular surface. Returns 0, -1 on a bad argument
+ * or an atom outside the grid, -2 on allocation failure. */
+int pmgo_setup_fine(int n, double h, const double *atoms, int natoms,
+                    double eps_in, double eps_out, double ionic_strength,
+                    double ion_radius, double temperature,
+                    double probe_radius, double *oC, double *oE, double *oN,
+                    double *uC, double *f, double *x0);
+
 #ifdef __cplusplus
 }
 #endif

@@ -357,6 +357,51 @@ def test_setup_matches_reference(golden_problem):
         assert np.array_equal(out[k], g["fine_" + k]), k
 
 
+def test_oracle_setup_matches_reference_golden(golden_problem, restatement):
+    """The restated set-up (pmgo_setup_fine) at the reference's constants
+    gives the reference's own set-up bit for bit."""
+    from multigrid_b200.molecule import REFERENCE_PHYSICS
+    g = golden_problem
+    base, nlev, box = int(g["base"]), int(g["nlev"]), float(g["box"])
+    n = base * 2 ** nlev + 1
+    out = restatement.setup_fine(n, box / (n - 1), g["atoms"],
+                                 REFERENCE_PHYSICS)
+    for k in ("oC", "oE", "oN", "uC", "f", "x0"):
+        assert np.array_equal(out[k], g["fine_" + k]), k
+
+
+@pytest.mark.parametrize("probe", [0.0, 1.4])
+@pytest.mark.parametrize("n,h,natoms,radius", [(33, 0.5, 150, 5.0),
+                                               (41, 0.4, 400, 6.0)])
+def test_oracle_setup_bitexact_vs_product_host_setup(restatement, probe, n,
+                                                     h, natoms, radius):
+    """The oracle's own set-up (what the reference arm of the benchmark and
+    the parity tests feed the reference with) and the product's host set-up
+    give the same bits, with and without the probe surface, at the PB
+    workloads' physics."""
+    from multigrid_b200.molecule import DEFAULT_PHYSICS, synthetic_atoms
+    from multigrid_b200.problem import setup_fine
+    box = h * (n - 1)
+    atoms = synthetic_atoms(natoms, radius, 40 + n, (box / 2,) * 3)
+    phys = dict(DEFAULT_PHYSICS, probe_radius=probe)
+    a = restatement.setup_fine(n, h, atoms, phys)
+    b = setup_fine(n, h, atoms, phys)
+    for k in a:
+        assert np.array_equal(a[k], b[k]), (probe, k)
+    # the probe surface changes the dielectric maps (solute grows)
+    if probe > 0:
+        vdw = restatement.setup_fine(n, h, atoms,
+                                     dict(DEFAULT_PHYSICS, probe_radius=0.0))
+        assert (a["oE"] <= vdw["oE"]).all() and (a["oE"] < vdw["oE"]).any()
+
+
+def test_oracle_setup_rejects_atoms_outside(restatement):
+    from multigrid_b200.molecule import DEFAULT_PHYSICS
+    with pytest.raises(ValueError):
+        restatement.setup_fine(9, 0.5, np.array([[10.0, 1.0, 1.0, 1.5, 1.0]]),
+                               DEFAULT_PHYSICS)
+
+
 # -------- direct comparison with the reference-built oracle (if built) --------
 needs_ref = pytest.mark.skipif(not reference_available(),
                                reason="oracle/_ref not built")
