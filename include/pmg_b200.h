@@ -404,11 +404,15 @@ int pmg_cg_level_d(int nx, int ny, int nz, const double *const *a14,
  * time step). The work vectors live in a static device array of this
  * library (about 118 KB, held by every GPU that loads the library until the
  * process exits), so grids are limited to 17*17*17 points including the
- * shell; larger grids return PMG_ERR_ARG. The first call on a device looks
- * up the array's device address; make that first call before any stream
- * capture. All calls on a device share the array: each call clears the part
- * it uses, and calls that overlap on the GPU (e.g. on two streams) corrupt
- * each other. Synchronises the stream. No counterpart in the reference. */
+ * shell; larger grids return PMG_ERR_ARG. Every call looks up the array's
+ * device address in the current device's context (so a cudaDeviceReset
+ * between calls is harmless). All calls on a device share the array: each
+ * call clears the part it uses, and calls that overlap on the GPU (e.g. on
+ * two streams) corrupt each other. Grids of at most 17 points per axis run
+ * as the cluster kernel, which keeps its vectors on chip (only the array's
+ * two status words are used); the other accepted shapes (e.g. 19 x 13 x 19)
+ * run the one-CTA kernel on the array's work vectors. Synchronises the
+ * stream. No counterpart in the reference. */
 int pmg_cg_level_noalloc_d(int nx, int ny, int nz, const double *const *a14,
                            const double *rhs, double *x, double thresh,
                            int max_iters, int *iters, pmg_stream_t stream);
@@ -466,8 +470,10 @@ int pmg_setup_fine_d(int n, double h, const double *atoms, int natoms,
  * the file cannot be read or holds more than cap atoms. */
 int pmg_read_pqr(const char *path, double *atoms, int cap, int *count);
 /* OpenDX grid file of an nx x ny x nz array in array order (x fastest), the
- * reference's print_dx_to_stream (Domain.h:136-185): origin (xmin, ymin,
- * zmin), spacing box_length / (nx - 1), three values per line. */
+ * reference's print_dx_to_stream (Domain.h:136-185): counts slowest axis
+ * first (nz ny nx), origin (xmin, ymin, zmin), spacing box_length / (nz - 1)
+ * on every axis (box_length is the extent of the slowest axis, as in the
+ * reference), three values per line. */
 int pmg_write_dx(const char *path, const double *values, int nx, int ny,
                  int nz, double xmin, double ymin, double zmin,
                  double box_length);
@@ -482,7 +488,13 @@ typedef struct pmg_problem pmg_problem;
 
 typedef enum {
   PMG_PREC_FP64 = 0,  /* V-cycles in double (the reference's arithmetic)  */
-  PMG_PREC_MIXED = 1  /* float V-cycles inside double iterative refinement */
+  PMG_PREC_MIXED = 1, /* float V-cycles inside double iterative refinement */
+  /* double V-cycles with the mixed path's structure: zero-started V-cycles
+   * on the correction equation inside the same double refinement loop, the
+   * finest level on colour-split arrays with coded couplings; the fastest
+   * all-double solve (not the reference's cycle, so its potential agrees
+   * with the reference's to the stopping tolerance, not to rounding). */
+  PMG_PREC_FP64_FAST = 2
 } pmg_precision;
 
 /* Creates a problem on the current CUDA device; allocates its hierarchy.

@@ -36,6 +36,7 @@ STATUS = {
 globals().update({name: code for code, name in STATUS.items()})
 PREC_FP64 = 0
 PREC_MIXED = 1
+PREC_FP64_FAST = 2
 
 
 class PmgError(RuntimeError):

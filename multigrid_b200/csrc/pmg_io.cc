@@ -6,11 +6,13 @@
 // radius from field 10 (1-based). Blank lines are skipped (the reference
 // indexes an empty field list there).
 //
-// write: the reference's OpenDX writer (Domain::print_dx_to_stream,
-// Domain.h:136-185): gridpositions header with counts n, origin and the
-// three axis deltas box / (n - 1), then the values in array order, three per
-// line, each formatted as a left-aligned, explicitly signed, 13-wide
-// exponent number followed by a space, then the field trailer.
+// write: the reference's OpenDX writer (Grid::print_dx_to_stream,
+// Domain.h:136-185): gridpositions header with the counts slowest axis
+// first (nz ny nx, OpenDX's order: the last count varies fastest), origin,
+// and the three axis deltas box / (nz - 1) (the reference's spacing of its
+// first, slowest axis), then the values in array order, three per line,
+// each formatted as a left-aligned, explicitly signed, 13-wide exponent
+// number followed by a space, then the field trailer.
 #include <stdio.h>
 #include <string.h>
 
@@ -70,9 +72,9 @@ int pmg_write_dx(const char *path, const double *values, int nx, int ny,
   FILE *f = fopen(path, "w");
   if (!f)
     return PMG_ERR_ARG;
-  const double delta = box_length / (double)(nx - 1);
+  const double delta = box_length / (double)(nz - 1);
   const long count = (long)nx * ny * nz;
-  fprintf(f, "object 1 class gridpositions counts %d %d %d\n", nx, ny, nz);
+  fprintf(f, "object 1 class gridpositions counts %d %d %d\n", nz, ny, nx);
   fprintf(f, "origin ");
   put_value(f, xmin);
   put_value(f, ymin);
@@ -84,7 +86,7 @@ int pmg_write_dx(const char *path, const double *values, int nx, int ny,
       put_value(f, c == axis ? delta : 0.0);
     fprintf(f, "\n");
   }
-  fprintf(f, "object 2 class gridconnections count %d %d %d\n", nx, ny, nz);
+  fprintf(f, "object 2 class gridconnections count %d %d %d\n", nz, ny, nx);
   fprintf(f, "object 3 class array type double rank 0 items %ld data follows\n",
           count);
   for (long i = 0; i < count; ++i) {

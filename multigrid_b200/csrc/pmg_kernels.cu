@@ -188,15 +188,6 @@ __global__ void add_correction_kernel(Dims d, double *__restrict__ x,
   x[p] = x[p] + (double)e[p];
 }
 
-__global__ void add_correction_split_kernel(Dims d, double *__restrict__ x,
-                                            const float *__restrict__ e) {
-  const Interior t = interior_point(d);
-  if (!t.ok)
-    return;
-  const int p = d.at(t.i, t.j, t.k);
-  x[p] = x[p] + (double)e[Split::of(d).at(t.i, t.j, t.k)];
-}
-
 __global__ void buildP_trilin_kernel(Dims dc, P27W<double> P) {
   const Interior t = interior_point(dc);
   if (!t.ok)

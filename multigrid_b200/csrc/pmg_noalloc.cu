@@ -16,8 +16,6 @@
 // contents, so each call clears the part it uses (the kernel expects zero
 // shells), and two calls that run on the GPU at the same time (on different
 // streams) overwrite each other's work vectors.
-#include <mutex>
-
 #include "reduce_kernels.cuh"
 
 namespace {
@@ -30,28 +28,17 @@ constexpr size_t kNoAllocBytes =
 
 static __device__ __align__(256) unsigned char noalloc_scratch[kNoAllocBytes];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_mutex;
-void *g_addr[kMaxDevices] = {};
-
-// Device address of noalloc_scratch on the current device. In host code the
-// array's name is only a stand-in for the symbol, never an address a kernel
-// may use, so the address is looked up once per device (with that device
-// current) and cached.
+// Device address of noalloc_scratch in the current device's context. In
+// host code the array's name is only a stand-in for the symbol, never an
+// address a kernel may use. The address is looked up on every call, with
+// the caller's device current: a cached address would go stale when the
+// context that loaded the module is torn down (cudaDeviceReset) or when
+// another context is current, and the lookup is cheap next to the stream
+// synchronisation each call does anyway.
 int scratch_address(void **out) {
-  int dev = -1;
-  PMG_CUDA_TRY(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= kMaxDevices) {
-    pmg::set_last_message("cg_level_noalloc: device index out of range");
-    return PMG_ERR_ARG;
-  }
-  std::lock_guard<std::mutex> lock(g_mutex);
-  if (!g_addr[dev]) {
-    void *ptr = nullptr;
-    PMG_CUDA_TRY(cudaGetSymbolAddress(&ptr, noalloc_scratch));
-    g_addr[dev] = ptr;
-  }
-  *out = g_addr[dev];
+  void *ptr = nullptr;
+  PMG_CUDA_TRY(cudaGetSymbolAddress(&ptr, noalloc_scratch));
+  *out = ptr;
   return PMG_OK;
 }
 

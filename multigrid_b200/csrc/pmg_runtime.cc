@@ -450,7 +450,8 @@ int pmg_server_submit(pmg_server *s, const pmg_request *r) {
   if (!s || !r)
     return PMG_ERR_ARG;
   if (r->max_cycles < 0 || r->max_cycles > 1024 || !(r->tol >= 0.0) ||
-      (r->precision != PMG_PREC_FP64 && r->precision != PMG_PREC_MIXED))
+      (r->precision != PMG_PREC_FP64 && r->precision != PMG_PREC_MIXED &&
+       r->precision != PMG_PREC_FP64_FAST))
     return PMG_ERR_ARG;
   if (r->atoms) {
     if (r->natoms < 0)

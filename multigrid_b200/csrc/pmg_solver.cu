@@ -37,10 +37,15 @@ struct LevelBuf {
   float *x32 = nullptr, *f32 = nullptr, *r32 = nullptr;
   float *xalt32 = nullptr;
   double *omega = nullptr; // damping computed on this level (device)
-  // mixed finest level: coded couplings (split_layout.cuh) and their table
+  // mixed / fp64-fast finest level: coded couplings (split_layout.cuh) and
+  // their table
   unsigned char *code = nullptr;
   int *code_info = nullptr; // device: ranges and the mismatch flags
   double *lut64 = nullptr;  // device: the double couplings of the codes
+  // fp64-fast finest level: the correction, its right-hand side and the
+  // operator (oC oE oN uC) in the colour-split layout, double
+  double *xs = nullptr, *fs = nullptr;
+  double *ops[4] = {};
 
   Op14<double> A64(int nops) const {
     Op14<double> A{};
@@ -78,6 +83,31 @@ struct Arena {
     off += sizeof(T) * (size_t)count;
     return p;
   }
+};
+
+// The arrays a refinement-step V-cycle (vcycle_ref) works on, by its
+// arithmetic type: float copies on every level (mixed), or the double
+// arrays, with the colour-split copies on the finest level (fp64-fast).
+template <typename T> struct LevelArrays;
+template <> struct LevelArrays<float> {
+  static float *x(LevelBuf &v) { return v.x32; }
+  static float *f(LevelBuf &v) { return v.f32; }
+  static float *r(LevelBuf &v) { return v.r32; }
+  static float *alt(LevelBuf &v) { return v.xalt32; }
+  static float *fine_op(LevelBuf &v, int s) { return v.op32[s]; }
+  static const float *lut(LevelBuf &) { return nullptr; }
+  static Op14<float> A(const LevelBuf &v) { return v.A32(14); }
+  static P27<float> P(const LevelBuf &v) { return v.Pc32(); }
+};
+template <> struct LevelArrays<double> {
+  static double *x(LevelBuf &v) { return v.xs ? v.xs : v.x; }
+  static double *f(LevelBuf &v) { return v.fs ? v.fs : v.f; }
+  static double *r(LevelBuf &v) { return v.r; }
+  static double *alt(LevelBuf &v) { return v.xalt; }
+  static double *fine_op(LevelBuf &v, int s) { return v.ops[s]; }
+  static const double *lut(LevelBuf &v) { return v.lut64; }
+  static Op14<double> A(const LevelBuf &v) { return v.A64(14); }
+  static P27<double> P(const LevelBuf &v) { return v.Pc(); }
 };
 
 // Fine-level set-up from atoms on the GPU (pmg_setup_gpu.cu).
@@ -170,6 +200,7 @@ int level_n(int base, int L) { return base * (1 << L) + 1; }
 // counts bytes.
 void plan(pmg_problem *p, Arena &a) {
   const bool mixed = p->precision == PMG_PREC_MIXED;
+  const bool fast = p->precision == PMG_PREC_FP64_FAST;
   for (int L = 1; L <= p->nlev; ++L) {
     LevelBuf &v = p->lv[L];
     v.n = level_n(p->base, L);
@@ -203,6 +234,15 @@ void plan(pmg_problem *p, Arena &a) {
       v.code = fine ? a.take<unsigned char>(v.n3) : nullptr;
       v.code_info = fine ? a.take<int>(8) : nullptr;
       v.lut64 = fine ? a.take<double>(6) : nullptr;
+    }
+    if (fast && fine) {
+      for (int s = 0; s < 4; ++s)
+        v.ops[s] = a.take<double>(v.n3);
+      v.xs = a.take<double>(v.n3);
+      v.fs = a.take<double>(v.n3);
+      v.code = a.take<unsigned char>(v.n3);
+      v.code_info = a.take<int>(8);
+      v.lut64 = a.take<double>(6);
     }
   }
   const long n1 = p->lv[1].n3;
@@ -300,11 +340,12 @@ int smooth64(pmg_problem *p, int L, int nsweeps, int zero_init,
 }
 
 // Coarsest level: the class's CG (absolute 1e-8, first test on
-// sqrt(sqrt(r.r))) on the FP64 path; on the mixed path a zero-started CG to
-// coarse_rtol relative to its initial residual.
+// sqrt(sqrt(r.r))) on the FP64 path; on the refinement paths (mixed,
+// fp64-fast) a zero-started CG to coarse_rtol relative to its initial
+// residual.
 int cg_level1(pmg_problem *p, const double *rhs, double *x) {
   LevelBuf &v = p->lv[1];
-  if (p->precision == PMG_PREC_MIXED)
+  if (p->precision != PMG_PREC_FP64)
     return launch_cg_level(v.d, v.A64(14), rhs, x, p->cg_r, p->cg_p,
                            p->cg_ap, 0.0, p->coarse_rtol, 0, kCgMaxIters,
                            p->cg_status, p->stream);
@@ -393,22 +434,30 @@ double norm_from_sum(const pmg_problem *p, double s) {
   return sqrt(s / n3);
 }
 
-// ---- mixed precision -------------------------------------------------------
+// ---- refinement paths (mixed, fp64-fast) -----------------------------------
 
-int smooth32(pmg_problem *p, int L, int nsweeps, int zero_init, float **cur) {
+// Smoothing sweeps of a refinement-step V-cycle on level L in type T: on the
+// finest level the colour-split red-black pass, with the couplings from the
+// code bytes when they are coded; below, the eight-colour smoother with
+// ping-pong buffers. *cur holds the iterate on entry and on return.
+template <typename T>
+int smooth_ref(pmg_problem *p, int L, int nsweeps, int zero_init, T **cur) {
+  using A = LevelArrays<T>;
   LevelBuf &v = p->lv[L];
   if (L == p->nlev && p->use_codes)
-    return launch_gs7_code<float>(v.d, v.op32[kOC], v.f32, v.op32[kOE],
-                                  v.op32[kON], v.op32[kUC], v.code,
-                                  v.code_info, *cur, nsweeps, 0, zero_init,
-                                  p->stream);
+    return launch_gs7_code<T>(v.d, A::fine_op(v, kOC), A::f(v),
+                              A::fine_op(v, kOE), A::fine_op(v, kON),
+                              A::fine_op(v, kUC), v.code, v.code_info,
+                              A::lut(v), *cur, nsweeps, 0, zero_init,
+                              p->stream);
   if (L == p->nlev) // colour-split layout (split_layout.cuh)
-    return launch_gs7_split<float>(v.d, v.op32[kOC], v.f32, v.op32[kOE],
-                                   v.op32[kON], v.op32[kUC], *cur, nsweeps, 0,
-                                   zero_init, p->stream);
-  float *alt = *cur == v.x32 ? v.xalt32 : v.x32;
-  return launch_gs27_pp<float>(v.d, v.A32(14), nullptr, v.f32, *cur, alt,
-                               nsweeps, 0, zero_init, p->stream, cur);
+    return launch_gs7_split<T>(v.d, A::fine_op(v, kOC), A::f(v),
+                               A::fine_op(v, kOE), A::fine_op(v, kON),
+                               A::fine_op(v, kUC), *cur, nsweeps, 0,
+                               zero_init, p->stream);
+  T *alt = *cur == A::x(v) ? A::alt(v) : A::x(v);
+  return launch_gs27_pp<T>(v.d, A::A(v), nullptr, A::f(v), *cur, alt,
+                           nsweeps, 0, zero_init, p->stream, cur);
 }
 
 // Arguments of the one-CTA cycle over levels 1 .. top.
@@ -457,17 +506,20 @@ int launch_bottom(pmg_problem *p, int top) {
   return PMG_OK;
 }
 
-// V-cycle in float on the correction equation, every level zero-started
+// V-cycle in type T on the correction equation, every level zero-started
 // (v_cycle with as_preconditioner, PBE_pmgc_class.h:1070-1114); level 1 in
-// double.
-int vcycle32(pmg_problem *p, int L) {
+// double. T = float is the mixed path, T = double fp64-fast.
+template <typename T> int vcycle_ref(pmg_problem *p, int L) {
+  using A = LevelArrays<T>;
+  constexpr bool kFloat = sizeof(T) == sizeof(float);
   cudaStream_t s = p->stream;
   LevelBuf &v = p->lv[L];
   const int sl = L * 8;
   if (L == 1) {
     prof_begin(p, sl + kPhCoarse);
-    convert_kernel<float, double><<<flat_grid(v.n3), 256, 0, s>>>(v.n3, v.f32,
-                                                                 v.f);
+    if (kFloat)
+      convert_kernel<float, double><<<flat_grid(v.n3), 256, 0, s>>>(
+          v.n3, v.f32, v.f);
     PMG_CUDA_TRY(cudaMemsetAsync(v.x, 0, sizeof(double) * v.n3, s));
     int rc = cg_level1(p, v.f, v.x);
     prof_end(p, sl + kPhCoarse);
@@ -476,31 +528,30 @@ int vcycle32(pmg_problem *p, int L) {
   LevelBuf &c = p->lv[L - 1];
   const int kind = L == p->nlev ? 7 : 27;
   int rc;
-  float *x = v.x32;
-  const bool bottom_below = L - 1 <= p->bottom_top;
+  T *x = A::x(v);
+  const bool bottom_below = kFloat && L - 1 <= p->bottom_top;
   prof_begin(p, sl + kPhPre);
-  if ((rc = smooth32(p, L, 2, 1, &x)))
+  if ((rc = smooth_ref<T>(p, L, 2, 1, &x)))
     return rc;
   prof_end(p, sl + kPhPre);
   prof_begin(p, sl + kPhDefect);
   if (kind == 7 && p->use_codes)
-    defect7_code_kernel<float>
+    defect7_code_kernel<T>
         <<<defect7_code_grid(v.d), interior_block(), 0, s>>>(
-            v.d, v.op32[kOC], v.op32[kOE], v.op32[kON], v.op32[kUC], v.code,
-            v.code_info, v.f32, x, v.r32);
+            v.d, A::fine_op(v, kOC), A::fine_op(v, kOE), A::fine_op(v, kON),
+            A::fine_op(v, kUC), v.code, v.code_info, A::lut(v), A::f(v), x,
+            A::r(v));
   else if (kind == 7) // split arrays in, reference-layout defect out
-    defect7_split_kernel<float>
-        <<<interior_grid(v.d), interior_block(), 0, s>>>(
-            v.d, v.op32[kOC], v.op32[kOE], v.op32[kON], v.op32[kUC], v.f32, x,
-            v.r32);
+    defect7_split_kernel<T><<<interior_grid(v.d), interior_block(), 0, s>>>(
+        v.d, A::fine_op(v, kOC), A::fine_op(v, kOE), A::fine_op(v, kON),
+        A::fine_op(v, kUC), A::f(v), x, A::r(v));
   else
-    defect_kernel<27, float><<<interior_grid(v.d), interior_block(), 0, s>>>(
-        v.d, v.A32(14), v.f32, x, v.r32);
+    defect_kernel<27, T><<<interior_grid(v.d), interior_block(), 0, s>>>(
+        v.d, A::A(v), A::f(v), x, A::r(v));
   prof_end(p, sl + kPhDefect);
   prof_begin(p, sl + kPhRestrict);
-  restrict_kernel<float, float>
-      <<<interior_grid(c.d), interior_block(), 0, s>>>(v.d, c.d, v.r32, c.f32,
-                                                       c.Pc32());
+  restrict_kernel<T, T><<<interior_grid(c.d), interior_block(), 0, s>>>(
+      v.d, c.d, A::r(v), A::f(c), A::P(c));
   prof_end(p, sl + kPhRestrict);
   PMG_LAUNCH_CHECK();
   if (bottom_below) {
@@ -510,7 +561,7 @@ int vcycle32(pmg_problem *p, int L) {
       return rc;
     prof_end(p, sl + kPhCoarse);
     PMG_LAUNCH_CHECK();
-  } else if ((rc = vcycle32(p, L - 1))) {
+  } else if ((rc = vcycle_ref<T>(p, L - 1))) {
     return rc;
   }
   prof_begin(p, sl + kPhLambda);
@@ -520,52 +571,62 @@ int vcycle32(pmg_problem *p, int L) {
     ideal_lambda_kernel<double><<<lambda_grid(c.d), interior_block(), 0, s>>>(
         c.d, c.A64(14), c.x, c.f, p->red_lambda, c.omega,
         lambda_planes(c.d));
-    convert_kernel<double, float><<<flat_grid(c.n3), 256, 0, s>>>(c.n3, c.x,
-                                                                 c.x32);
+    if (kFloat)
+      convert_kernel<double, float><<<flat_grid(c.n3), 256, 0, s>>>(
+          c.n3, c.x, c.x32);
   } else {
-    ideal_lambda_kernel<float><<<lambda_grid(c.d), interior_block(), 0, s>>>(
-        c.d, c.A32(14), c.x32, c.f32, p->red_lambda, c.omega,
+    ideal_lambda_kernel<T><<<lambda_grid(c.d), interior_block(), 0, s>>>(
+        c.d, A::A(c), A::x(c), A::f(c), p->red_lambda, c.omega,
         lambda_planes(c.d));
   }
   prof_end(p, sl + kPhLambda);
   // x += w * (interpolated correction), one pass
   prof_begin(p, sl + kPhInterp);
-  if (kind == 7) // the finest float iterate is split
-    interp_add_kernel<float, true>
-        <<<interp_grid(c.d), interior_block(), 0, s>>>(c.d, v.d, c.x32,
-                                                       c.Pc32(), x, c.omega);
+  if (kind == 7) // the finest iterate is split
+    interp_add_kernel<T, true><<<interp_grid(c.d), interior_block(), 0, s>>>(
+        c.d, v.d, A::x(c), A::P(c), x, c.omega);
   else
-    interp_add_kernel<float, false>
-        <<<interp_grid(c.d), interior_block(), 0, s>>>(c.d, v.d, c.x32,
-                                                       c.Pc32(), x, c.omega);
+    interp_add_kernel<T, false>
+        <<<interp_grid(c.d), interior_block(), 0, s>>>(c.d, v.d, A::x(c),
+                                                       A::P(c), x, c.omega);
   prof_end(p, sl + kPhInterp);
   PMG_LAUNCH_CHECK();
   prof_begin(p, sl + kPhPost);
-  if ((rc = smooth32(p, L, 2, 0, &x)))
+  if ((rc = smooth_ref<T>(p, L, 2, 0, &x)))
     return rc;
   prof_end(p, sl + kPhPost);
-  if (x != v.x32) {
-    set_last_message("vcycle32: iterate left the level's buffer");
+  if (x != A::x(v)) {
+    set_last_message("vcycle_ref: iterate left the level's buffer");
     return PMG_ERR_STATE;
   }
   return PMG_OK;
 }
 
-// r64 = f - A x64 on the finest level, written as float into f32 (the
-// correction equation's right-hand side), its sum of squares into red_norm
-// and pinned host memory.
-int mixed_residual_async(pmg_problem *p, bool to_host = true) {
+// r64 = f - A x64 on the finest level, written into the correction
+// equation's split right-hand side (float for mixed, double for fp64-fast),
+// its sum of squares into red_norm and pinned host memory.
+int refine_residual_async(pmg_problem *p, bool to_host = true) {
   LevelBuf &v = p->lv[p->nlev];
+  const dim3 g = reduce_grid(v.d), b = interior_block();
+  cudaStream_t s = p->stream;
   prof_begin(p, kPhResidual);
-  if (p->use_codes)
-    defect_norm_code_kernel<double><<<reduce_grid(v.d), interior_block(), 0,
-                              p->stream>>>(v.d, v.A64(4), v.f, v.x, v.code,
-                                           v.lut64, v.code_info, v.f32,
-                                           p->red_norm);
-  else
-    defect_norm_kernel<7, double, float, true>
-        <<<reduce_grid(v.d), interior_block(), 0, p->stream>>>(
-            v.d, v.A64(4), v.f, v.x, v.f32, p->red_norm);
+  if (p->precision == PMG_PREC_MIXED) {
+    if (p->use_codes)
+      defect_norm_code_kernel<double, float><<<g, b, 0, s>>>(
+          v.d, v.A64(4), v.f, v.x, v.code, v.lut64, v.code_info, v.f32,
+          p->red_norm);
+    else
+      defect_norm_kernel<7, double, float, true><<<g, b, 0, s>>>(
+          v.d, v.A64(4), v.f, v.x, v.f32, p->red_norm);
+  } else {
+    if (p->use_codes)
+      defect_norm_code_kernel<double, double><<<g, b, 0, s>>>(
+          v.d, v.A64(4), v.f, v.x, v.code, v.lut64, v.code_info, v.fs,
+          p->red_norm);
+    else
+      defect_norm_kernel<7, double, double, true><<<g, b, 0, s>>>(
+          v.d, v.A64(4), v.f, v.x, v.fs, p->red_norm);
+  }
   prof_end(p, kPhResidual);
   PMG_LAUNCH_CHECK();
   if (to_host)
@@ -575,19 +636,27 @@ int mixed_residual_async(pmg_problem *p, bool to_host = true) {
   return PMG_OK;
 }
 
-// One refinement step: float V-cycle on the correction, x64 += e, new
-// residual.
-int mixed_step(pmg_problem *p, bool to_host = true) {
+// One refinement step: V-cycle on the correction (float or double), x64 +=
+// e, new residual.
+int refine_step(pmg_problem *p, bool to_host = true) {
   LevelBuf &v = p->lv[p->nlev];
-  int rc;
-  if ((rc = vcycle32(p, p->nlev)))
+  const bool mixed = p->precision == PMG_PREC_MIXED;
+  int rc = mixed ? vcycle_ref<float>(p, p->nlev)
+                 : vcycle_ref<double>(p, p->nlev);
+  if (rc)
     return rc;
   prof_begin(p, kPhCorrect);
-  add_correction_split_kernel<<<interior_grid(v.d), interior_block(), 0,
-                                p->stream>>>(v.d, v.x, v.x32);
+  if (mixed)
+    add_correction_split_kernel<float>
+        <<<interior_grid(v.d), interior_block(), 0, p->stream>>>(v.d, v.x,
+                                                                 v.x32);
+  else
+    add_correction_split_kernel<double>
+        <<<interior_grid(v.d), interior_block(), 0, p->stream>>>(v.d, v.x,
+                                                                 v.xs);
   prof_end(p, kPhCorrect);
   PMG_LAUNCH_CHECK();
-  return mixed_residual_async(p, to_host);
+  return refine_residual_async(p, to_host);
 }
 
 // Kernel nodes of a graph (conditional bodies are counted by their own
@@ -615,8 +684,8 @@ long long count_kernel_nodes(cudaGraph_t g) {
 // refinement step. to_host adds the copy of the residual sum to pinned
 // memory (the host-driven loop); the device-driven loop keeps it on the GPU.
 int cycle_with_residual(pmg_problem *p, bool to_host) {
-  if (p->precision == PMG_PREC_MIXED)
-    return mixed_step(p, to_host);
+  if (p->precision != PMG_PREC_FP64)
+    return refine_step(p, to_host);
   int rc = vcycle64(p, p->nlev, 0);
   return rc ? rc : residual_norm_async(p, to_host);
 }
@@ -804,11 +873,11 @@ int build_loop_graph(pmg_problem *p, Head head, Body body, Tail tail,
 int ensure_solve_graph(pmg_problem *p) {
   if (p->solve_exec)
     return PMG_OK;
-  const bool mixed = p->precision == PMG_PREC_MIXED;
+  const bool refine = p->precision != PMG_PREC_FP64;
   const double n3 = (double)p->lv[p->nlev].n3;
   auto head = [&](cudaGraphConditionalHandle h) -> int {
-    int rc = mixed ? mixed_residual_async(p, false)
-                   : residual_norm_async(p, false);
+    int rc = refine ? refine_residual_async(p, false)
+                    : residual_norm_async(p, false);
     if (rc)
       return rc;
     solve_init_kernel<<<1, 1, 0, p->stream>>>(p->d_state,
@@ -895,11 +964,23 @@ int precondition(pmg_problem *p, const double *r, double *z) {
     to_split_kernel<double, float><<<flat_grid(v.n3), 256, 0, s>>>(v.d, r,
                                                                    v.f32);
     PMG_LAUNCH_CHECK();
-    int rc = vcycle32(p, p->nlev);
+    int rc = vcycle_ref<float>(p, p->nlev);
     if (rc)
       return rc;
     from_split_kernel<float, double><<<flat_grid(v.n3), 256, 0, s>>>(
         v.d, v.x32, z);
+    PMG_LAUNCH_CHECK();
+    return PMG_OK;
+  }
+  if (p->precision == PMG_PREC_FP64_FAST) {
+    to_split_kernel<double, double><<<flat_grid(v.n3), 256, 0, s>>>(v.d, r,
+                                                                    v.fs);
+    PMG_LAUNCH_CHECK();
+    int rc = vcycle_ref<double>(p, p->nlev);
+    if (rc)
+      return rc;
+    from_split_kernel<double, double><<<flat_grid(v.n3), 256, 0, s>>>(
+        v.d, v.xs, z);
     PMG_LAUNCH_CHECK();
     return PMG_OK;
   }
@@ -1012,7 +1093,8 @@ long long pmg_problem_bytes(int base, int nlev, int precision) {
 int pmg_problem_create(int base, int nlev, double box, int precision,
                        pmg_stream_t stream, pmg_problem **out) {
   if (!out || check_shape(base, nlev) ||
-      (precision != PMG_PREC_FP64 && precision != PMG_PREC_MIXED)) {
+      (precision != PMG_PREC_FP64 && precision != PMG_PREC_MIXED &&
+       precision != PMG_PREC_FP64_FAST)) {
     set_last_message("pmg_problem_create: bad argument");
     return PMG_ERR_ARG;
   }
@@ -1128,13 +1210,15 @@ int pmg_problem_coded_couplings(pmg_problem *p, int *coded) {
     return PMG_ERR_ARG;
   *coded = 0;
   const LevelBuf &v = p->lv[p->nlev];
-  if (!p->built || p->precision != PMG_PREC_MIXED || !p->use_codes)
+  if (!p->built || p->precision == PMG_PREC_FP64 || !p->use_codes)
     return PMG_OK;
-  int flag = 1;
-  PMG_CUDA_TRY(cudaMemcpyAsync(&flag, v.code_info + 6, sizeof(int),
+  int flag[2] = {1, 1};
+  PMG_CUDA_TRY(cudaMemcpyAsync(flag, v.code_info + 6, sizeof(flag),
                                cudaMemcpyDeviceToHost, p->stream));
   PMG_CUDA_TRY(cudaStreamSynchronize(p->stream));
-  *coded = flag == 0;
+  // the float coding; fp64-fast also needs the double couplings to match
+  *coded = flag[0] == 0 &&
+           (p->precision == PMG_PREC_MIXED || flag[1] == 0);
   return PMG_OK;
 }
 
@@ -1296,6 +1380,33 @@ int pmg_build_hierarchy(pmg_problem *p, int trilinear) {
       }
     PMG_LAUNCH_CHECK();
   }
+  if (p->precision == PMG_PREC_FP64_FAST) {
+    // the finest double operator split by colour, and its coded couplings
+    // (classified by their float values, then checked bit for bit in
+    // double: info[7] keeps the arrays in use when they do not match)
+    LevelBuf &v = p->lv[p->nlev];
+    const unsigned g = flat_grid(v.n3);
+    for (int q = 0; q < 4; ++q) {
+      to_split_kernel<double, double><<<g, 256, 0, s>>>(v.d, v.op[q],
+                                                        v.ops[q]);
+      ++p->launches;
+    }
+    const int init[8] = {INT_MAX, INT_MIN, INT_MAX, INT_MIN,
+                         INT_MAX, INT_MIN, 0,       0};
+    PMG_CUDA_TRY(cudaMemcpyAsync(v.code_info, init, sizeof(init),
+                                 cudaMemcpyHostToDevice, s));
+    const dim3 ig = interior_grid(v.d), ib = interior_block();
+    coupling_range_kernel<double><<<coupling_range_blocks(v.d), 256, 0, s>>>(
+        v.d, v.ops[kOE], v.ops[kON], v.ops[kUC], v.code_info);
+    coupling_code_kernel<double><<<ig, ib, 0, s>>>(
+        v.d, v.ops[kOE], v.ops[kON], v.ops[kUC], v.code_info, v.code);
+    lut64_store_kernel<double><<<ig, ib, 0, s>>>(
+        v.d, v.op[kOE], v.op[kON], v.op[kUC], v.code, v.lut64);
+    lut64_check_kernel<double><<<ig, ib, 0, s>>>(
+        v.d, v.op[kOE], v.op[kON], v.op[kUC], v.code, v.lut64, v.code_info);
+    p->launches += 4;
+    PMG_LAUNCH_CHECK();
+  }
   // tile edge of the 27-point smoother, measured once per grid size (every
   // edge gives the same bits; the levels' iterates serve as scratch and are
   // cleared afterwards)
@@ -1354,8 +1465,8 @@ int pmg_compute_residual_2(pmg_problem *p, double *out) {
 // conditional body, and for histories longer than the device state holds).
 static int solve_host_loop(pmg_problem *p, double tol, int max_cycles,
                            int *cycles, double *relres, double *hist) {
-  const bool mixed = p->precision == PMG_PREC_MIXED;
-  int rc = mixed ? mixed_residual_async(p) : residual_norm_async(p);
+  const bool refine = p->precision != PMG_PREC_FP64;
+  int rc = refine ? refine_residual_async(p) : residual_norm_async(p);
   if (rc)
     return rc;
   ++p->launches;

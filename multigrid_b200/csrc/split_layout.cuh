@@ -68,9 +68,17 @@ __global__ void from_split_kernel(Dims d, const Tin *__restrict__ src,
     dst[g] = (Tout)src[sp.of_linear((int)g)];
 }
 
-// x64 (reference layout) += (double) e32 (split) on the interior
+// x64 (reference layout) += (double) e (split) on the interior: the
+// refinement update of the split correction (float or double)
+template <typename E>
 __global__ void add_correction_split_kernel(Dims d, double *__restrict__ x,
-                                            const float *__restrict__ e);
+                                            const E *__restrict__ e) {
+  const Interior t = interior_point(d);
+  if (!t.ok)
+    return;
+  const int p = d.at(t.i, t.j, t.k);
+  x[p] = x[p] + (double)e[Split::of(d).at(t.i, t.j, t.k)];
+}
 
 // Neighbour offsets of the point at split index s with q = i - 1 of parity
 // qp: west and east (the other half), north/south (one row), up/down (one
@@ -202,9 +210,11 @@ __global__ void __launch_bounds__(256)
     interior_coords(d, q, i, j, k);
     const int p = sp.at(i, j, k);
     const SplitNb nb = split_nb(sp, p, (i - 1) & 1);
-    const int c[6] = {float_order(oE[p]), float_order(oE[nb.w]),
-                      float_order(oN[p]), float_order(oN[nb.s]),
-                      float_order(uC[p]), float_order(uC[nb.dn])};
+    // classified by their float values (the double path checks its
+    // couplings against the table separately, lut64_check_kernel)
+    const int c[6] = {float_order((float)oE[p]), float_order((float)oE[nb.w]),
+                      float_order((float)oN[p]), float_order((float)oN[nb.s]),
+                      float_order((float)uC[p]), float_order((float)uC[nb.dn])};
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
       v[2 * a] = min(v[2 * a], min(c[2 * a], c[2 * a + 1]));
@@ -263,7 +273,7 @@ __global__ void __launch_bounds__(256)
   bool bad = false;
 #pragma unroll
   for (int q = 0; q < 6; ++q) {
-    const int v = __float_as_int(c[q]);
+    const int v = __float_as_int((float)c[q]);
     const int lo = __float_as_int(order_float(info[(q >> 1) * 2]));
     const int hi = __float_as_int(order_float(info[(q >> 1) * 2 + 1]));
     if (v == hi)
@@ -291,32 +301,51 @@ __device__ __forceinline__ bool load_lut(const int *info, CodeLut &L) {
   return true;
 }
 
-// the six couplings of point p: from the code byte when the level is coded,
-// else from the arrays (the same float values either way)
+// The table of a coded double level: lut64 (lut64_store_kernel) holds the
+// double value of each direction and bit; usable when the float
+// classification held (info[6]) and every double coupling matched its
+// entry (info[7]).
+struct CodeLut64 {
+  double el, eh, nl, nh, ul, uh;
+};
+__device__ __forceinline__ bool load_lut(const int *info, const float *,
+                                         CodeLut &L) {
+  return load_lut(info, L);
+}
+__device__ __forceinline__ bool load_lut(const int *info, const double *lut64,
+                                         CodeLut64 &L) {
+  if (info[6] != 0 || info[7] != 0)
+    return false;
+  L.el = lut64[0];
+  L.eh = lut64[1];
+  L.nl = lut64[2];
+  L.nh = lut64[3];
+  L.ul = lut64[4];
+  L.uh = lut64[5];
+  return true;
+}
+template <typename T> struct LutOf {
+  using type = CodeLut;
+};
+template <> struct LutOf<double> {
+  using type = CodeLut64;
+};
+
+// the six couplings of point p from the arrays (split layout)
 template <typename T> struct Couplings {
   T e, w, n, s, u, dn;
 };
 template <typename T>
 __device__ __forceinline__ Couplings<T>
-couplings(bool coded, const CodeLut &L, const unsigned char *code,
-          const T *oE, const T *oN, const T *uC, int p, const SplitNb &nb) {
+array_couplings(const T *oE, const T *oN, const T *uC, int p,
+                const SplitNb &nb) {
   Couplings<T> c;
-  if (coded) {
-    const unsigned b = code[p];
-    c.e = (b & 1u) ? L.eh : L.el;
-    c.w = (b & 2u) ? L.eh : L.el;
-    c.n = (b & 4u) ? L.nh : L.nl;
-    c.s = (b & 8u) ? L.nh : L.nl;
-    c.u = (b & 16u) ? L.uh : L.ul;
-    c.dn = (b & 32u) ? L.uh : L.ul;
-  } else {
-    c.e = oE[p];
-    c.w = oE[nb.w];
-    c.n = oN[p];
-    c.s = oN[nb.s];
-    c.u = uC[p];
-    c.dn = uC[nb.dn];
-  }
+  c.e = oE[p];
+  c.w = oE[nb.w];
+  c.n = oN[p];
+  c.s = oN[nb.s];
+  c.u = uC[p];
+  c.dn = uC[nb.dn];
   return c;
 }
 
@@ -325,14 +354,18 @@ couplings(bool coded, const CodeLut &L, const unsigned char *code,
 // no host round trip and a captured graph serves either case). With the
 // couplings coded a point moves about 17 bytes, so each thread takes PTS
 // points of its half row (32 apart: a warp stays contiguous) and issues
-// all their loads before computing, to keep enough bytes in flight.
+// all their loads before computing, to keep enough bytes in flight. The
+// loads that do not depend on the coding (x neighbours, f, oC, code bytes)
+// are issued before the table and its flag are read, so no load waits for
+// the flag.
 template <typename T, int PTS>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 6 : 4)
     gs7_code_color_kernel(Dims d, const T *__restrict__ oC,
                           const T *__restrict__ fc, const T *__restrict__ oE,
                           const T *__restrict__ oN, const T *__restrict__ uC,
                           const unsigned char *__restrict__ code,
-                          const int *__restrict__ info, T *x, int want,
+                          const int *__restrict__ info,
+                          const T *__restrict__ lut, T *x, int want,
                           T keep) {
   const Split sp = Split::of(d);
   const int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
@@ -347,19 +380,28 @@ __global__ void __launch_bounds__(256)
   int p[PTS];
   bool ok[PTS];
   unsigned b[PTS];
+  T xv[PTS][6], f[PTS], c[PTS];
 #pragma unroll
   for (int r = 0; r < PTS; ++r) {
     const int i = i0 + 64 * r;
     ok[r] = i <= d.nx - 1;
     p[r] = sp.at(ok[r] ? i : i0, j, k);
     b[r] = code[p[r]]; // every interior point has a byte
+    const SplitNb nb = split_nb(sp, p[r], qp);
+    xv[r][0] = x[nb.n];
+    xv[r][1] = x[nb.s];
+    xv[r][2] = x[nb.e];
+    xv[r][3] = x[nb.w];
+    xv[r][4] = x[nb.dn];
+    xv[r][5] = x[nb.u];
+    f[r] = fc[p[r]];
+    c[r] = oC[p[r]];
   }
-  CodeLut L;
-  const bool coded = load_lut(info, L);
-  T s[PTS], f[PTS], c[PTS];
+  typename LutOf<T>::type L;
+  const bool coded = load_lut(info, lut, L);
+  T s[PTS];
 #pragma unroll
   for (int r = 0; r < PTS; ++r) {
-    const SplitNb nb = split_nb(sp, p[r], qp);
     Couplings<T> cp;
     if (coded) {
       cp.e = (b[r] & 1u) ? L.eh : L.el;
@@ -369,12 +411,10 @@ __global__ void __launch_bounds__(256)
       cp.u = (b[r] & 16u) ? L.uh : L.ul;
       cp.dn = (b[r] & 32u) ? L.uh : L.ul;
     } else {
-      cp = couplings<T>(false, L, code, oE, oN, uC, p[r], nb);
+      cp = array_couplings<T>(oE, oN, uC, p[r], split_nb(sp, p[r], qp));
     }
-    s[r] = cp.n * x[nb.n] + cp.s * x[nb.s] + cp.e * x[nb.e] +
-           cp.w * x[nb.w] + cp.dn * x[nb.dn] + cp.u * x[nb.u];
-    f[r] = fc[p[r]];
-    c[r] = oC[p[r]];
+    s[r] = cp.n * xv[r][0] + cp.s * xv[r][1] + cp.e * xv[r][2] +
+           cp.w * xv[r][3] + cp.dn * xv[r][4] + cp.u * xv[r][5];
   }
 #pragma unroll
   for (int r = 0; r < PTS; ++r)
@@ -388,8 +428,8 @@ constexpr int kCodePts = 2;
 template <typename T>
 int launch_gs7_code(const Dims &d, const T *oC, const T *fc, const T *oE,
                     const T *oN, const T *uC, const unsigned char *code,
-                    const int *info, T *x, int itmax, int iadjoint,
-                    int zero_init, cudaStream_t s) {
+                    const int *info, const T *lut, T *x, int itmax,
+                    int iadjoint, int zero_init, cudaStream_t s) {
   const dim3 g(cdiv(cdiv(d.nx - 2, 2), 32 * kCodePts), cdiv(d.ny - 2, 8),
                (unsigned)(d.nz - 2));
   for (int it = 0; it < itmax; ++it)
@@ -397,7 +437,7 @@ int launch_gs7_code(const Dims &d, const T *oC, const T *fc, const T *oE,
       const int want = (1 - iadjoint) * c + iadjoint * (1 - c);
       const T keep = zero_init ? T(0) : T(1);
       gs7_code_color_kernel<T, kCodePts><<<g, interior_block(), 0, s>>>(
-          d, oC, fc, oE, oN, uC, code, info, x, want, keep);
+          d, oC, fc, oE, oN, uC, code, info, lut, x, want, keep);
       zero_init = 0;
     }
   PMG_LAUNCH_CHECK();
@@ -408,12 +448,13 @@ int launch_gs7_code(const Dims &d, const T *oC, const T *fc, const T *oE,
 // two points per thread (32 apart in the row) for the same reason as the
 // colour pass
 template <typename T>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 8 : 4)
     defect7_code_kernel(Dims d, const T *__restrict__ oC,
                         const T *__restrict__ oE, const T *__restrict__ oN,
                         const T *__restrict__ uC,
                         const unsigned char *__restrict__ code,
-                        const int *__restrict__ info, const T *__restrict__ f,
+                        const int *__restrict__ info,
+                        const T *__restrict__ lut, const T *__restrict__ f,
                         const T *__restrict__ x, T *__restrict__ r) {
   const int i0 = blockIdx.x * blockDim.x * 2 + threadIdx.x + 2;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
@@ -424,6 +465,8 @@ __global__ void __launch_bounds__(256)
   int ii[2], p[2];
   bool ok[2];
   unsigned b[2];
+  // loads independent of the coding first (see gs7_code_color_kernel)
+  T xv[2][7], fv[2], cv[2];
 #pragma unroll
   for (int q = 0; q < 2; ++q) {
     ii[q] = i0 + 32 * q;
@@ -432,13 +475,22 @@ __global__ void __launch_bounds__(256)
       ii[q] = i0;
     p[q] = sp.at(ii[q], j, k);
     b[q] = code[p[q]];
+    const SplitNb nb = split_nb(sp, p[q], (ii[q] - 1) & 1);
+    xv[q][0] = x[nb.n];
+    xv[q][1] = x[nb.s];
+    xv[q][2] = x[nb.e];
+    xv[q][3] = x[nb.w];
+    xv[q][4] = x[nb.dn];
+    xv[q][5] = x[nb.u];
+    xv[q][6] = x[p[q]];
+    fv[q] = f[p[q]];
+    cv[q] = oC[p[q]];
   }
-  CodeLut L;
-  const bool coded = load_lut(info, L);
+  typename LutOf<T>::type L;
+  const bool coded = load_lut(info, lut, L);
   T out[2];
 #pragma unroll
   for (int q = 0; q < 2; ++q) {
-    const SplitNb nb = split_nb(sp, p[q], (ii[q] - 1) & 1);
     Couplings<T> c;
     if (coded) {
       c.e = (b[q] & 1u) ? L.eh : L.el;
@@ -448,12 +500,13 @@ __global__ void __launch_bounds__(256)
       c.u = (b[q] & 16u) ? L.uh : L.ul;
       c.dn = (b[q] & 32u) ? L.uh : L.ul;
     } else {
-      c = couplings<T>(false, L, code, oE, oN, uC, p[q], nb);
+      c = array_couplings<T>(oE, oN, uC, p[q],
+                             split_nb(sp, p[q], (ii[q] - 1) & 1));
     }
-    const T ax = -c.n * x[nb.n] - c.s * x[nb.s] - c.e * x[nb.e] -
-                 c.w * x[nb.w] - c.dn * x[nb.dn] - c.u * x[nb.u] +
-                 (oC[p[q]] + T(0)) * x[p[q]];
-    out[q] = f[p[q]] - ax;
+    const T ax = -c.n * xv[q][0] - c.s * xv[q][1] - c.e * xv[q][2] -
+                 c.w * xv[q][3] - c.dn * xv[q][4] - c.u * xv[q][5] +
+                 (cv[q] + T(0)) * xv[q][6];
+    out[q] = fv[q] - ax;
   }
 #pragma unroll
   for (int q = 0; q < 2; ++q)
@@ -524,14 +577,14 @@ __global__ void __launch_bounds__(256)
 // f - A x64, written to the split float right-hand side, and its sum of
 // squares) with the double couplings from the code bytes when both codings
 // hold: the same values, the same order, the same bits.
-template <typename T>
+template <typename T, typename R>
 __global__ void __launch_bounds__(kReduceThreads)
     defect_norm_code_kernel(Dims d, Op14<T> A, const T *__restrict__ f,
                             const T *__restrict__ x,
                             const unsigned char *__restrict__ code,
                             const T *__restrict__ lut64,
                             const int *__restrict__ info,
-                            float *__restrict__ r, ReduceSlot s) {
+                            R *__restrict__ r, ReduceSlot s) {
   __shared__ double sh[32];
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
@@ -556,9 +609,13 @@ __global__ void __launch_bounds__(kReduceThreads)
         break;
       const int p = d.at(i, j, k);
       const int sidx = sp.at(i, j, k);
+      // loads independent of the coding first
+      const T xn = x[p + sy], xs = x[p - sy], xe = x[p + 1], xw = x[p - 1];
+      const T xd = x[p - sz], xu = x[p + sz], xc = x[p];
+      const T fv = f[p], oc = A.a[kOC][p];
+      const unsigned b = code[sidx];
       T c[6];
       if (coded) {
-        const unsigned b = code[sidx];
         c[0] = (b & 1u) ? eh : el;
         c[1] = (b & 2u) ? eh : el;
         c[2] = (b & 4u) ? nh : nl;
@@ -570,11 +627,10 @@ __global__ void __launch_bounds__(kReduceThreads)
       }
       // apply7's order: -oN x_n - oN_s x_s - oE x_e - oE_w x_w - uC_d x_d
       // - uC x_u + (oC + 0) x
-      const T ax = -c[2] * x[p + sy] - c[3] * x[p - sy] - c[0] * x[p + 1] -
-                   c[1] * x[p - 1] - c[5] * x[p - sz] - c[4] * x[p + sz] +
-                   (A.a[kOC][p] + T(0)) * x[p];
-      const T dv = f[p] - ax;
-      r[sidx] = (float)dv;
+      const T ax = -c[2] * xn - c[3] * xs - c[0] * xe - c[1] * xw -
+                   c[5] * xd - c[4] * xu + (oc + T(0)) * xc;
+      const T dv = fv - ax;
+      r[sidx] = (R)dv;
       acc += (double)dv * (double)dv;
     }
   }

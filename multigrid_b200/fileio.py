@@ -38,13 +38,14 @@ def read_pqr(path: str, origin=(0.0, 0.0, 0.0)) -> np.ndarray:
 def write_dx(path: str, values: np.ndarray, origin=(0.0, 0.0, 0.0),
              box_length: float | None = None) -> None:
     """Writes an (nz, ny, nx) array (x fastest in memory) as an OpenDX grid
-    with the given origin and spacing box_length / (nx - 1)."""
+    with the given origin and spacing box_length / (nz - 1) (box_length is
+    the extent of the slowest axis, as in the reference's writer)."""
     v = np.ascontiguousarray(values, dtype=np.float64)
     if v.ndim != 3:
         raise ValueError("values must be a 3-D array")
     nz, ny, nx = v.shape
     if box_length is None:
-        box_length = float(nx - 1)
+        box_length = float(nz - 1)
     _lib.check("pmg_write_dx", _lib.lib.pmg_write_dx(
         str(path).encode(), v.ctypes.data_as(_lib.PD), nx, ny, nz,
         float(origin[0]), float(origin[1]), float(origin[2]),

@@ -59,15 +59,17 @@ class SolveResult:
     history: np.ndarray  # residual norm before and after each cycle
 
 
-PRECISIONS = {"fp64": _lib.PREC_FP64, "mixed": _lib.PREC_MIXED}
+PRECISIONS = {"fp64": _lib.PREC_FP64, "mixed": _lib.PREC_MIXED,
+              "fp64-fast": _lib.PREC_FP64_FAST}
 
 
 class PBELinearProblem:
     """PBE_linear_problem<base, nlev, box> with runtime sizes.
 
-    precision: "fp64" (the reference's arithmetic) or "mixed" (float
+    precision: "fp64" (the reference's arithmetic), "mixed" (float
     V-cycles inside double iterative refinement; double residual, norms and
-    coarsest CG).
+    coarsest CG) or "fp64-fast" (double V-cycles in the mixed path's
+    structure: the fastest all-double solve).
     """
 
     def __init__(self, base: int, nlev: int, box: float,
@@ -77,10 +79,10 @@ class PBELinearProblem:
         L = 1..nlev); "deep" coarsens the same finest grid as far as a 5^3
         coarsest level allows (levels_for), which makes the coarsest CG
         cheap. Default: "reference" for fp64 (parity with the reference),
-        "deep" for mixed."""
+        "deep" for mixed and fp64-fast."""
         n = level_n(int(base), int(nlev))
         if hierarchy is None:
-            hierarchy = "deep" if precision == "mixed" else "reference"
+            hierarchy = "reference" if precision == "fp64" else "deep"
         if hierarchy == "deep":
             base, nlev = levels_for(n, max_levels=12, min_coarse=5)
         elif hierarchy != "reference":

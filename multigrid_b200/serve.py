@@ -141,8 +141,9 @@ def _request(base, nlev, box, precision, fine, out, tol, max_cycles, tag,
         keep.append(out)
         r.potential = _ptr(out)
     r.tol, r.max_cycles, r.tag = tol, max_cycles, tag
-    # same default as PBELinearProblem: the deepest hierarchy for mixed
-    r.hierarchy = 1 if precision == "mixed" else 0
+    # same default as PBELinearProblem: the deepest hierarchy except for
+    # the reference's FP64 cycle
+    r.hierarchy = 0 if precision == "fp64" else 1
     return r, keep
 
 

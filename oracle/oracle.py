@@ -280,6 +280,17 @@ class _RefFine(ctypes.Structure):
     _fields_ = [(k, D) for k in ("oC", "oE", "oN", "uC", "f", "x0")]
 
 
+def reference_tree() -> str | None:
+    """The reference tree oracle/_ref was built from, when it is present on
+    this machine (its data files, e.g. the PQR inputs); else None."""
+    try:
+        with open(os.path.join(HERE, "_ref", "reference_dir.txt")) as f:
+            path = f.read().strip()
+    except OSError:
+        return None
+    return path if path and os.path.isdir(path) else None
+
+
 def reference_available(omp: bool = False) -> bool:
     name = "libpmgc_ref_omp.so" if omp else "libpmgc_ref.so"
     return os.path.exists(os.path.join(HERE, "_ref", name))
@@ -362,6 +373,32 @@ class Reference:
         rc = self.lib.pmgref_cg_level1(base, nlev, _pp(op14), _d(rhs), _d(x))
         if rc != 0:
             raise KeyError(f"reference oracle has no ({base}, {nlev}) grid")
+
+    def read_pqr(self, path: str, cap: int = 1 << 20) -> np.ndarray:
+        """The reference's PQR reader: rows (x, y, z, radius, charge)."""
+        atoms = np.empty((cap, 5))
+        n = ctypes.c_int()
+        rc = self.lib.pmgref_read_pqr(path.encode(), _d(atoms), cap,
+                                      ctypes.byref(n))
+        if rc != 0:
+            raise ValueError("more atoms than cap")
+        return atoms[:n.value].copy()
+
+    DX_SHAPES = {0: (4, 5, 6), 1: (7, 7, 7)}
+
+    def write_dx(self, shape: int, values: np.ndarray, origin, box) -> str:
+        """The reference's OpenDX text of a grid of DX_SHAPES[shape] interior
+        points (slowest axis first) with a one-point padding (oracle/_ref/
+        ref_dx, a separate process)."""
+        import tempfile
+        exe = os.path.join(HERE, "_ref", "ref_dx")
+        with tempfile.NamedTemporaryFile(suffix=".bin") as f:
+            np.ascontiguousarray(values, dtype="<f8").tofile(f.name)
+            r = subprocess.run([exe, str(shape), f.name] +
+                               [repr(float(v)) for v in origin] +
+                               [repr(float(box))], capture_output=True,
+                               check=True)
+        return r.stdout.decode()
 
     def setup(self, base, nlev, atoms, ionic_strength, ion_radius) -> dict:
         n = base * 2 ** nlev + 1

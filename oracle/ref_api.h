@@ -148,6 +148,20 @@ int pmgref_Vbuildband(int nx, int ny, int nz, int numdia, double *ac,
 int pmgref_Vdpbfa(double *abd, int lda, int n, int m);
 int pmgref_Vdpbsl(double *abd, int lda, int n, int m, double *b);
 
+/* The reference's PQR reader (read_pqr_file, fileio.cc:10-53): rows (x, y,
+ * z, radius, charge) of up to cap atoms; *count gets the number read.
+ * Returns -1 when the file holds more than cap. */
+int pmgref_read_pqr(const char *path, double *atoms, int cap, int *count);
+
+/* The reference's OpenDX writer (Grid::print_dx_to_stream,
+ * Domain.h:136-185) on a grid of interior lengths (slowest axis first)
+ * 4 x 5 x 6 (shape 0) or 7 x 7 x 7 (shape 1) with a one-point padding,
+ * values in array order; the text goes to out (cap bytes). Returns its
+ * length, or minus the bytes needed. */
+long pmgref_write_dx(int shape, const double *values, double xmin,
+                     double ymin, double zmin, double box, char *out,
+                     long cap);
+
 #ifdef __cplusplus
 }
 #endif

@@ -315,25 +315,30 @@ def test_throughput_mode_same_solve_within_tolerance(pb65):
     assert np.linalg.norm(x1 - x0) <= 1e-9 * np.linalg.norm(x0)
 
 
-def test_coded_couplings_give_the_same_bits(pb65):
+@pytest.mark.parametrize("precision", ["mixed", "fp64-fast"])
+def test_coded_couplings_give_the_same_bits(pb65, precision):
     """The class's fine operator has two coupling values per direction, so
-    the mixed path's finest smoother and defect read code bytes; the solve
-    is bit-identical to the one reading the coupling arrays. An operator
-    with more values per direction is not coded and solves the same with
-    the switch on or off."""
+    the finest smoother and defect of the refinement paths read code bytes;
+    the solve is bit-identical to the one reading the coupling arrays. An
+    operator with more values per direction is not coded and solves the
+    same with the switch on or off; so does one whose double couplings take
+    a third value that rounds to a float table value (coded for the float
+    passes of the mixed path, not for fp64-fast)."""
     w, fine = pb65
     out = {}
-    for case in ("class", "random"):
+    for case in ("class", "random", "ulp"):
         f = dict(fine)
+        rng = np.random.default_rng(1)
+        oE = np.array(f["oE"], copy=True)
+        flat = oE.reshape(-1)
+        pick = rng.choice(flat.size, 50, replace=False)
         if case == "random":  # a third value in oE: no coding
-            rng = np.random.default_rng(1)
-            oE = np.array(f["oE"], copy=True)
-            flat = oE.reshape(-1)
-            pick = rng.choice(flat.size, 50, replace=False)
             flat[pick] = flat[pick] * 1.01
-            f["oE"] = oE
+        elif case == "ulp":  # a third double, the same float
+            flat[pick] = np.nextafter(flat[pick], np.inf)
+        f["oE"] = oE
         for on in (True, False):
-            with PBELinearProblem(w.base, w.nlev, w.box, "mixed",
+            with PBELinearProblem(w.base, w.nlev, w.box, precision,
                                   w.physics) as p:
                 p.set_coded_couplings(on)
                 p.set_fine(**f)
@@ -343,9 +348,52 @@ def test_coded_couplings_give_the_same_bits(pb65):
                 out[case, on] = (coded, r.cycles, p.potential().ravel().copy())
     assert out["class", True][0] and not out["class", False][0]
     assert not out["random", True][0]
-    for case in ("class", "random"):
+    assert out["ulp", True][0] == (precision == "mixed")
+    for case in ("class", "random", "ulp"):
         assert out[case, True][1] == out[case, False][1]
         assert np.array_equal(out[case, True][2], out[case, False][2])
+
+
+def test_fp64_fast_solves_golden_problems(golden_problem):
+    """fp64-fast (double V-cycles on the correction equation, deep
+    hierarchy, coded colour-split finest level) reaches relative residual
+    1e-10 and agrees with the reference's FP64 solve to the stopping
+    tolerance (1e-8 relative L2: it is not the reference's cycle, so it does
+    not agree to rounding)."""
+    g = golden_problem
+    base, nlev, box = int(g["base"]), int(g["nlev"]), float(g["box"])
+    with PBELinearProblem(base, nlev, box, "fp64-fast") as p:
+        p.set_fine(**fine_of(g))
+        p.buildmultilevelops()
+        res = p.solve(tol=1e-10, max_cycles=60)
+        x = p.potential().ravel()
+    assert res.relres < 1e-10
+    assert res.cycles <= int(g["cycles"]) + 3
+    assert rel_l2(x, g["x"]) <= TOL_MIXED
+
+
+def test_pb65_fp64_fast_vs_oracle_and_pcg(pb65, restatement):
+    """pb65: fp64-fast against the FP64 oracle (1e-8 relative L2 and
+    max-norm), and as the preconditioner of the outer CG."""
+    w, fine = pb65
+    xo, co, _ = restatement.solve(w.base, w.nlev, fine, tol=1e-10,
+                                  max_cycles=60)
+    with PBELinearProblem(w.base, w.nlev, w.box, "fp64-fast",
+                          w.physics) as p:
+        p.set_fine(**fine)
+        p.buildmultilevelops()
+        assert p.coded_couplings()
+        res = p.solve(tol=1e-10, max_cycles=60)
+        x = p.potential().ravel().copy()
+        assert res.relres < 1e-10 and res.cycles <= co + 3
+        assert rel_l2(x, xo) <= TOL_MIXED
+        assert np.abs(x - xo).max() / np.abs(xo).max() <= TOL_MIXED
+        p.set_fine(**fine)
+        p.buildmultilevelops()
+        pr = p.pcg_solve(tol=1e-10, max_iters=60)
+        xp = p.potential().ravel()
+    assert pr.relres < 1e-10
+    assert rel_l2(xp, xo) <= TOL_MIXED
 
 
 @pytest.mark.parametrize("throughput", [False, True])

@@ -8,6 +8,8 @@ reference's operation order and must match bit for bit; the builders are a
 generic formulation and must match to rounding; whole solves to 1e-12
 relative L2 with the same number of cycles.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -483,3 +485,66 @@ def test_reference_fine_couplings_are_two_valued(golden_problem):
     for k, v in read.items():
         assert len(np.unique(v)) <= 2, k
         assert len(np.unique(v.astype(np.float32))) <= 2, k
+
+
+# -------- file formats against the reference's own reader and writer --------
+PQR_TEXT = """REMARK   1 synthetic PQR for the reader comparison
+REMARK   6 Total charge on this protein: 0.0000 e
+ATOM      1  N   ARG     1      -8.544   3.578  14.046  0.1305 1.8240
+ATOM      2  CA  ARG     1      -7.776   3.484  12.790 -0.0223 1.9080
+HETATM    3  O   HOH     2       1.5e1  -0.25   7.125  -0.8340 1.7683
+ATOM      4  CB  ARG A   1      -7.640   2.025  12.309  0.0118 1.9080
+ATOM      5  CG  ARG     1      -6.000   2.000   3.000  0.0000 0.0000
+TER
+END
+"""
+
+
+@needs_ref
+def test_pqr_reader_matches_reference(tmp_path):
+    """pmg_read_pqr and the reference's read_pqr_file (fileio.cc:10-53) on
+    the same file: the same atoms, bit for bit (rows with a chain field have
+    eleven fields and are skipped by both)."""
+    from multigrid_b200.fileio import read_pqr
+    path = tmp_path / "mol.pqr"
+    path.write_text(PQR_TEXT)
+    ours = read_pqr(str(path))
+    ref = Reference().read_pqr(str(path))
+    assert ours.shape == (4, 5)
+    assert np.array_equal(ours, ref)
+
+
+@needs_ref
+def test_pqr_reader_matches_reference_on_its_molecule():
+    """The reference's own molecule file 1PIT.pqr, read by both readers."""
+    from oracle.oracle import reference_tree
+    from multigrid_b200.fileio import read_pqr
+    tree = reference_tree()
+    if tree is None or not os.path.exists(os.path.join(tree, "1PIT.pqr")):
+        pytest.skip("the reference tree is not on this machine")
+    path = os.path.join(tree, "1PIT.pqr")
+    ours = read_pqr(path)
+    ref = Reference().read_pqr(path)
+    assert len(ours) == 892
+    assert np.array_equal(ours, ref)
+
+
+@needs_ref
+@pytest.mark.parametrize("shape", [0, 1])
+def test_dx_writer_matches_reference_byte_for_byte(tmp_path, shape):
+    """pmg_write_dx and the reference's print_dx_to_stream
+    (Domain.h:136-185) write the same bytes for the same array, origin and
+    box, on a non-cubic and a cubic grid."""
+    from multigrid_b200.fileio import write_dx
+    ref = Reference()
+    n0, n1, n2 = (s + 2 for s in ref.DX_SHAPES[shape])  # slowest first
+    rng = np.random.default_rng(shape)
+    vals = rng.normal(size=(n0, n1, n2)) * 10.0 ** rng.integers(-5, 5,
+                                                                (n0, n1, n2))
+    vals[0, 0, :3] = [0.0, -0.0, 1.0]
+    origin, box = (-1.5, 2.25, 1e-3), 12.5
+    want = ref.write_dx(shape, vals.ravel(), origin, box)
+    path = tmp_path / "v.dx"
+    write_dx(str(path), vals, origin=origin, box_length=box)
+    got = path.read_text()
+    assert got == want
