@@ -7,8 +7,9 @@ the host cores; the GPU solves the same fine-level inputs:
 * pb161 (161^3, 5 levels, 5000 atoms) and pb257 (257^3, 5 levels): the plain
   FP64 GPU solve must take the same number of V-cycles and be within 1e-12
   relative L2 of the reference's potential; the mixed-precision solve
-  (float V-cycles inside double refinement, its deeper hierarchy) within
-  1e-8 relative L2 and 1e-8 relative max-norm, at relative residual 1e-10.
+  (float V-cycles inside double refinement, its deeper hierarchy) and the
+  fp64-fast solve (double V-cycles in the same structure) within 1e-8
+  relative L2 and 1e-8 relative max-norm, at relative residual 1e-10.
 * three molecules of the batched set (97^3, 129^3 and 161^3 grids at
   0.5 A): solved together through the batched runtime from their atoms
   (set-up on the GPU), each within 1e-8 of the reference's solve of the
@@ -83,9 +84,13 @@ def test_fp64_matches_reference_solve(workload):
     assert err <= TOL_FP64, (w.name, err)
 
 
-def test_mixed_within_tolerance_of_reference_solve(workload):
+@pytest.mark.parametrize("precision", ["mixed", "fp64-fast"])
+def test_refinement_paths_within_tolerance_of_reference_solve(workload,
+                                                              precision):
+    """The mixed solve and the fastest all-double solve (fp64-fast: not the
+    reference's cycle) against the reference's potential."""
     w, fine, xr, _ = workload
-    res, x, _ = gpu_solve(w, fine, "mixed")
+    res, x, _ = gpu_solve(w, fine, precision)
     assert res.relres < 1e-10
     e2, em = rel_l2(x, xr), rel_max(x, xr)
     assert e2 <= TOL_MIXED and em <= TOL_MIXED, (w.name, e2, em)
