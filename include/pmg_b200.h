@@ -341,6 +341,36 @@ int pmg_Vdpbfa_d(double *abd, int lda, int n, int m, int *info,
 int pmg_Vdpbsl_d(const double *abd, int lda, int n, int m, double *b,
                  pmg_stream_t stream);
 
+/* The APBS V-cycle loop on a hierarchy the caller built (Vbuildops or its
+ * own), in APBS's packed multilevel storage: for level lev the iterate,
+ * w0, cc, fc and tru start at offset iz(1,lev), the operator's ac at
+ * iz(7,lev) (4 or 14 columns of n_lev doubles), its ipc at iz(5,lev) (host;
+ * ipc(11) = 7 or 27), and the prolongation from lev+1 to lev at iz(11,lev)
+ * (27 columns of n_(lev+1)). iz is the host copy of the 50 x nlev_real
+ * integer table of Vbuildstr (pmgc/mgsubd.cc:266-345), column-major,
+ * 1-based offsets. Runs levels ilev .. ilev+nlev-1 with level ilev of size
+ * nx x ny x nz: per cycle nu1 red-black GS sweeps (mgsmoo 1) or CG steps
+ * (mgsmoo 4) and the residual going down, the coarsest level by 100 CG
+ * iterations to epsiln (mgsolv 0) or by the factored band stored one level
+ * further down (mgsolv 1: n, m, lda in that level's ipc, the band in its
+ * ac), the Hackbusch-Reusken damped correction and nu2 sweeps with the
+ * colours reversed going up; until itmax cycles or the stop ratio of istop
+ * 0-3 (tru needed for 2 and 3) is at most errtol. x (level ilev) is the
+ * starting iterate and the result. Device arrays: x, w0, pc, ac, cc, fc,
+ * tru (packed) and w1, w2, w3 (the finest size). Host outputs (may be
+ * NULL): *iters cycles, *ierror 0 or 1 (itmax reached). iok, iinfo, omega
+ * and rpc are accepted for the reference's signature and not used. Reads
+ * one scalar back per cycle and per CG iteration; synchronises the stream.
+ * Replaces pmgc::Vmvcs (pmgc/mgcsd.cc:61-531). */
+int pmg_Vmvcs_d(int nx, int ny, int nz, double *x, const int *iz, double *w0,
+                double *w1, double *w2, double *w3, int istop, int itmax,
+                int *iters, int *ierror, int nlev, int ilev, int nlev_real,
+                int mgsolv, int iok, int iinfo, double epsiln, double errtol,
+                double omega, int nu1, int nu2, int mgsmoo, const int *ipc,
+                const double *rpc, const double *pc, const double *ac,
+                const double *cc, const double *fc, double *tru,
+                pmg_stream_t stream);
+
 /* The APBS iparm/rparm multigrid driver, linear case: builds the box-method
  * fine operator from the coefficient maps (as pmg_VbuildA_fv_d), the
  * prolongations and Galerkin operators of nlev levels, then runs V-cycles

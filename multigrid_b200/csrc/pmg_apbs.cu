@@ -563,6 +563,7 @@ int apbs_maxlev(int n1, int n2, int n3) {
 struct ApbsDriver {
   cudaStream_t s;
   int nlev, mgsmoo, mgsolv = 0;
+  double epsiln = 0.0; // stop of the coarsest CG (mgcsd.cc:362-378)
   double *band = nullptr; // factored band of the coarsest level (mgsolv 1)
   int bn = 0, bm = 0, blda = 0;
   ApbsLevel lv[13];
@@ -657,7 +658,7 @@ struct ApbsDriver {
     PMG_CUDA_TRY(cudaMemsetAsync(C.x, 0, sizeof(double) * C.d.count(), s));
     int it = 0;
     return pmg_Vcghs_d(C.d.nx, C.d.ny, C.d.nz, C.ipc, C.ac, C.cc, f, C.x, w1,
-                       w2, w3, 100, &it, 0.0, 0, s);
+                       w2, w3, 100, &it, epsiln, 0, s);
   }
 
   // the stop test's numerator after a cycle (mgcsd.cc:467-519)
@@ -672,6 +673,83 @@ struct ApbsDriver {
     const int rc = sum(F, tru, F.x, istop == 2 ? 2 : 3, out);
     if (rc == PMG_OK && istop == 3)
       *out = sqrt(*out);
+    return rc;
+  }
+
+  // Vmvcs (pmgc/mgcsd.cc:61-531) from the finest iterate lv[1].x: the stop
+  // test's denominator, then V-cycles until itmax or the stop ratio is at
+  // most errtol (one cycle-free coarse solve when nlev is 1). Returns the
+  // cycles run and the final ratio.
+  int mvcs(int istop, int itmax, double errtol, int nu1, int nu2,
+           double *tcf, int *iters, double *ratio) {
+    ApbsLevel &F1 = lv[1];
+    const Dims &df = F1.d;
+    double rsden = 1.0;
+    int rc = PMG_OK;
+    if (istop == 1) {
+      rc = sum(F1, F1.fc, nullptr, 0, &rsden);
+    } else if (istop == 2) {
+      rsden = sqrt((double)df.nx * df.ny * df.nz);
+    } else if (istop == 3) {
+      rc = sum(F1, tcf, tcf, 1, &rsden);
+      rsden = sqrt(rsden);
+    }
+    if (rc != PMG_OK)
+      return rc;
+    if (rsden == 0.0)
+      rsden = 1.0;
+    int it = 0;
+    double rn = 0.0;
+    if (nlev == 1) {
+      rc = coarse(F1, F1.fc);
+      it = 1;
+      if (rc == PMG_OK)
+        rc = stop_norm(istop, tcf, &rn);
+    } else {
+      do {
+        rc = smooth(F1, F1.fc, F1.x, nu1, 0, 1);
+        // the finest residual is kept in the finest w0 (mgcsd.cc:324)
+        if (rc == PMG_OK)
+          PMG_CUDA_TRY(cudaMemcpyAsync(F1.w0, w1,
+                                       sizeof(double) * df.count(),
+                                       cudaMemcpyDeviceToDevice, s));
+        for (int L = 2; L <= nlev && rc == PMG_OK; ++L) {
+          ApbsLevel &F = lv[L - 1], &C = lv[L];
+          rc = pmg_Vrestrc2_d(F.d.nx, F.d.ny, F.d.nz, C.d.nx, C.d.ny, C.d.nz,
+                              w1, C.w0, APBS_P27(C.P), s);
+          if (rc == PMG_OK && L != nlev) {
+            PMG_CUDA_TRY(
+                cudaMemsetAsync(C.x, 0, sizeof(double) * C.d.count(), s));
+            rc = smooth(C, C.w0, C.x, nu1, 0, 1);
+          }
+        }
+        if (rc == PMG_OK)
+          rc = coarse(lv[nlev], lv[nlev].w0);
+        for (int L = nlev - 1; L >= 1 && rc == PMG_OK; --L) {
+          ApbsLevel &F = lv[L], &C = lv[L + 1];
+          if (C.kind == 7)
+            apbs_damp_kernel<7><<<reduce_grid(C.d), interior_block(), 0, s>>>(
+                C.d, level_op(C), C.cc, C.x, C.w0, slot(res), res + 3);
+          else
+            apbs_damp_kernel<27>
+                <<<reduce_grid(C.d), interior_block(), 0, s>>>(
+                    C.d, level_op(C), C.cc, C.x, C.w0, slot(res), res + 3);
+          P27<double> P;
+          for (int q = 0; q < 27; ++q)
+            P.p[q] = C.P[q];
+          interp_add_kernel<double, false>
+              <<<interp_grid(C.d), interior_block(), 0, s>>>(C.d, F.d, C.x, P,
+                                                             F.x, res + 3);
+          PMG_LAUNCH_CHECK();
+          rc = smooth(F, L == 1 ? F.fc : F.w0, F.x, nu2, 1, 0);
+        }
+        ++it;
+        if (rc == PMG_OK)
+          rc = stop_norm(istop, tcf, &rn);
+      } while (rc == PMG_OK && it < itmax && rn / rsden > errtol);
+    }
+    *iters = it;
+    *ratio = rn / rsden;
     return rc;
   }
 };
@@ -999,63 +1077,9 @@ int pmg_Vmgdriv_d(const int *iparm, const double *rparm, double *u,
   rc = D.faces(F1, u, nullptr, nullptr, nullptr);
   if (rc != PMG_OK)
     return rc;
-  double rsden = 1.0;
-  if (istop == 1) {
-    rc = D.sum(F1, F1.fc, nullptr, 0, &rsden);
-  } else if (istop == 2) {
-    rsden = sqrt((double)nx * ny * nz);
-  } else if (istop == 3) {
-    rc = D.sum(F1, tcf, tcf, 1, &rsden);
-    rsden = sqrt(rsden);
-  }
-  if (rc != PMG_OK)
-    return rc;
-  if (rsden == 0.0)
-    rsden = 1.0;
   int it = 0;
-  double rn = 0.0;
-  if (nlev == 1) {
-    rc = D.coarse(F1, F1.fc);
-    it = 1;
-    if (rc == PMG_OK)
-      rc = D.stop_norm(istop, tcf, &rn);
-  } else {
-    do {
-      rc = D.smooth(F1, F1.fc, u, nu1, 0, 1);
-      for (int L = 2; L <= nlev && rc == PMG_OK; ++L) {
-        ApbsLevel &F = D.lv[L - 1], &C = D.lv[L];
-        rc = pmg_Vrestrc2_d(F.d.nx, F.d.ny, F.d.nz, C.d.nx, C.d.ny, C.d.nz,
-                            D.w1, C.w0, APBS_P27(C.P), stream);
-        if (rc == PMG_OK && L != nlev) {
-          PMG_CUDA_TRY(
-              cudaMemsetAsync(C.x, 0, sizeof(double) * C.d.count(), s));
-          rc = D.smooth(C, C.w0, C.x, nu1, 0, 1);
-        }
-      }
-      if (rc == PMG_OK)
-        rc = D.coarse(D.lv[nlev], D.lv[nlev].w0);
-      for (int L = nlev - 1; L >= 1 && rc == PMG_OK; --L) {
-        ApbsLevel &F = D.lv[L], &C = D.lv[L + 1];
-        if (C.kind == 7)
-          apbs_damp_kernel<7><<<reduce_grid(C.d), interior_block(), 0, s>>>(
-              C.d, level_op(C), C.cc, C.x, C.w0, D.slot(D.res), D.res + 3);
-        else
-          apbs_damp_kernel<27><<<reduce_grid(C.d), interior_block(), 0, s>>>(
-              C.d, level_op(C), C.cc, C.x, C.w0, D.slot(D.res), D.res + 3);
-        P27<double> P;
-        for (int q = 0; q < 27; ++q)
-          P.p[q] = C.P[q];
-        interp_add_kernel<double, false>
-            <<<interp_grid(C.d), interior_block(), 0, s>>>(C.d, F.d, C.x, P,
-                                                           F.x, D.res + 3);
-        PMG_LAUNCH_CHECK();
-        rc = D.smooth(F, L == 1 ? F.fc : F.w0, F.x, nu2, 1, 0);
-      }
-      ++it;
-      if (rc == PMG_OK)
-        rc = D.stop_norm(istop, tcf, &rn);
-    } while (rc == PMG_OK && it < itmax && rn / rsden > errtol);
-  }
+  double ratio = 0.0;
+  rc = D.mvcs(istop, itmax, errtol, nu1, nu2, tcf, &it, &ratio);
   if (rc != PMG_OK)
     return rc;
   rc = D.faces(F1, u, gxcf, gycf, gzcf);
@@ -1067,7 +1091,111 @@ int pmg_Vmgdriv_d(const int *iparm, const double *rparm, double *u,
   if (ierror)
     *ierror = it < itmax ? 0 : 1;
   if (rsnrm)
-    *rsnrm = rn / rsden;
+    *rsnrm = ratio;
+  return PMG_OK;
+}
+
+int pmg_Vmvcs_d(int nx, int ny, int nz, double *x, const int *iz, double *w0,
+                double *w1, double *w2, double *w3, int istop, int itmax,
+                int *iters, int *ierror, int nlev, int ilev, int nlev_real,
+                int mgsolv, int iok, int iinfo, double epsiln, double errtol,
+                double omega, int nu1, int nu2, int mgsmoo, const int *ipc,
+                const double *rpc, const double *pc, const double *ac,
+                const double *cc, const double *fc, double *tru,
+                pmg_stream_t stream) {
+  (void)iok;   // the reference's loop always tests (mgcsd.cc:461)
+  (void)iinfo; // i/o only
+  (void)omega; // damping of the smoothers not offered (mgsmoo 0/2/3)
+  (void)rpc;   // no real parameters for the box-method operators
+  PMG_REQUIRE(!bad_dims(nx, ny, nz), "Vmvcs: grid size out of range");
+  PMG_REQUIRE(iz && ipc, "Vmvcs: null iz or ipc (host arrays)");
+  PMG_REQUIRE(x && w0 && w1 && w2 && w3 && ac && cc && fc,
+              "Vmvcs: null device array");
+  PMG_REQUIRE(nlev >= 1 && nlev <= 12 && ilev >= 1 &&
+                  ilev - 1 + nlev + (mgsolv == 1 ? 1 : 0) <= nlev_real,
+              "Vmvcs: levels ilev .. ilev+nlev-1 (and the band level for "
+              "mgsolv 1) must lie within nlev_real");
+  PMG_REQUIRE(nlev == 1 || pc, "Vmvcs: null pc");
+  PMG_REQUIRE(mgsmoo == 1 || mgsmoo == 4,
+              "Vmvcs: mgsmoo must be 1 (red-black GS) or 4 (CG)");
+  PMG_REQUIRE(mgsolv == 0 || mgsolv == 1,
+              "Vmvcs: mgsolv must be 0 (CG) or 1 (banded direct)");
+  PMG_REQUIRE(istop >= 0 && istop <= 3, "Vmvcs: istop must be 0 to 3");
+  PMG_REQUIRE(istop < 2 || tru, "Vmvcs: istop 2 and 3 need tru");
+  PMG_REQUIRE(nu1 >= 0 && nu2 >= 0 && itmax >= 0,
+              "Vmvcs: negative nu1, nu2 or itmax");
+  // iz(field, lev), 1-based, 50 fields per level (Vbuildstr,
+  // mgsubd.cc:266-345), as a 0-based offset
+  auto IZ = [&](int field, int lev) {
+    return (size_t)(iz[(size_t)(lev - 1) * 50 + (field - 1)] - 1);
+  };
+  ApbsDriver D((cudaStream_t)stream);
+  D.nlev = nlev;
+  D.mgsmoo = mgsmoo;
+  D.mgsolv = mgsolv;
+  D.epsiln = epsiln;
+  for (int L = 1; L <= nlev; ++L) {
+    const int lev = ilev - 1 + L;
+    ApbsLevel &v = D.lv[L];
+    v.d = L == 1 ? Dims{nx, ny, nz}
+                 : Dims{(D.lv[L - 1].d.nx - 1) / 2 + 1,
+                        (D.lv[L - 1].d.ny - 1) / 2 + 1,
+                        (D.lv[L - 1].d.nz - 1) / 2 + 1};
+    PMG_REQUIRE(!bad_dims(v.d.nx, v.d.ny, v.d.nz),
+                "Vmvcs: a coarse grid is too small");
+    const int *ip = ipc + IZ(5, lev);
+    v.kind = ip[10];
+    PMG_REQUIRE(v.kind == 7 || v.kind == 27,
+                "Vmvcs: ipc(11) of a level must be 7 or 27");
+    for (int q = 0; q < 12; ++q)
+      v.ipc[q] = ip[q];
+    const size_t n = (size_t)v.d.count();
+    v.ac = const_cast<double *>(ac) + IZ(7, lev);
+    v.cc = const_cast<double *>(cc) + IZ(1, lev);
+    v.fc = const_cast<double *>(fc) + IZ(1, lev);
+    v.x = x + IZ(1, lev);
+    v.w0 = w0 + IZ(1, lev);
+    for (int q = 0; q < 27; ++q)
+      v.P[q] = L > 1 ? const_cast<double *>(pc) + IZ(11, lev - 1) + q * n
+                     : nullptr;
+  }
+  if (mgsolv == 1) {
+    // the factored band sits one level below the coarsest (lpv,
+    // mgcsd.cc:380-392): n, m, lda in its ipc, the band in its ac
+    const int lpv = ilev - 1 + nlev + 1;
+    const int *ipb = ipc + IZ(5, lpv);
+    D.bn = ipb[0];
+    D.bm = ipb[1];
+    D.blda = ipb[2];
+    const Dims &c = D.lv[nlev].d;
+    PMG_REQUIRE(D.bn == (c.nx - 2) * (c.ny - 2) * (c.nz - 2) && D.bm >= 0 &&
+                    D.blda == D.bm + 1,
+                "Vmvcs: band sizes in ipc do not fit the coarsest level");
+    D.band = const_cast<double *>(ac) + IZ(7, lpv);
+  }
+  D.w1 = w1;
+  D.w2 = w2;
+  D.w3 = w3;
+  // the reductions' partial sums, result slots and ticket
+  cudaStream_t s = D.s;
+  D.rg0 = reduce_grid(D.lv[1].d);
+  const size_t nblk = (size_t)D.rg0.x * D.rg0.y * D.rg0.z;
+  const size_t bytes = (2 * nblk + 4) * sizeof(double) + 64;
+  PMG_CUDA_TRY(scratch_alloc(&D.block, bytes, s));
+  PMG_CUDA_TRY(cudaMemsetAsync(D.block, 0, bytes, s));
+  D.partials = (double *)D.block;
+  D.res = D.partials + 2 * nblk;
+  D.ticket = (unsigned *)(D.res + 4);
+  int it = 0;
+  double ratio = 0.0;
+  int rc = D.mvcs(istop, itmax, errtol, nu1, nu2, tru, &it, &ratio);
+  if (rc != PMG_OK)
+    return rc;
+  PMG_CUDA_TRY(cudaStreamSynchronize(s));
+  if (iters)
+    *iters = it;
+  if (ierror)
+    *ierror = it < itmax ? 0 : 1;
   return PMG_OK;
 }
 

@@ -354,12 +354,12 @@ array_couplings(const T *oE, const T *oN, const T *uC, int p,
 // no host round trip and a captured graph serves either case). With the
 // couplings coded a point moves about 17 bytes, so each thread takes PTS
 // points of its half row (32 apart: a warp stays contiguous) and issues
-// all their loads before computing, to keep enough bytes in flight. The
-// loads that do not depend on the coding (x neighbours, f, oC, code bytes)
-// are issued before the table and its flag are read, so no load waits for
-// the flag.
+// all their loads before computing, to keep enough bytes in flight.
+// (Issuing the x loads before the coding flag is read raised the float
+// kernel to 40 registers and 6 blocks per SM: 173 -> 186 us per four passes
+// at 257^3.)
 template <typename T, int PTS>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 6 : 4)
+__global__ void __launch_bounds__(256)
     gs7_code_color_kernel(Dims d, const T *__restrict__ oC,
                           const T *__restrict__ fc, const T *__restrict__ oE,
                           const T *__restrict__ oN, const T *__restrict__ uC,
@@ -380,28 +380,19 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 6 : 4)
   int p[PTS];
   bool ok[PTS];
   unsigned b[PTS];
-  T xv[PTS][6], f[PTS], c[PTS];
 #pragma unroll
   for (int r = 0; r < PTS; ++r) {
     const int i = i0 + 64 * r;
     ok[r] = i <= d.nx - 1;
     p[r] = sp.at(ok[r] ? i : i0, j, k);
     b[r] = code[p[r]]; // every interior point has a byte
-    const SplitNb nb = split_nb(sp, p[r], qp);
-    xv[r][0] = x[nb.n];
-    xv[r][1] = x[nb.s];
-    xv[r][2] = x[nb.e];
-    xv[r][3] = x[nb.w];
-    xv[r][4] = x[nb.dn];
-    xv[r][5] = x[nb.u];
-    f[r] = fc[p[r]];
-    c[r] = oC[p[r]];
   }
   typename LutOf<T>::type L;
   const bool coded = load_lut(info, lut, L);
-  T s[PTS];
+  T s[PTS], f[PTS], c[PTS];
 #pragma unroll
   for (int r = 0; r < PTS; ++r) {
+    const SplitNb nb = split_nb(sp, p[r], qp);
     Couplings<T> cp;
     if (coded) {
       cp.e = (b[r] & 1u) ? L.eh : L.el;
@@ -411,10 +402,12 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 6 : 4)
       cp.u = (b[r] & 16u) ? L.uh : L.ul;
       cp.dn = (b[r] & 32u) ? L.uh : L.ul;
     } else {
-      cp = array_couplings<T>(oE, oN, uC, p[r], split_nb(sp, p[r], qp));
+      cp = array_couplings<T>(oE, oN, uC, p[r], nb);
     }
-    s[r] = cp.n * xv[r][0] + cp.s * xv[r][1] + cp.e * xv[r][2] +
-           cp.w * xv[r][3] + cp.dn * xv[r][4] + cp.u * xv[r][5];
+    s[r] = cp.n * x[nb.n] + cp.s * x[nb.s] + cp.e * x[nb.e] +
+           cp.w * x[nb.w] + cp.dn * x[nb.dn] + cp.u * x[nb.u];
+    f[r] = fc[p[r]];
+    c[r] = oC[p[r]];
   }
 #pragma unroll
   for (int r = 0; r < PTS; ++r)
@@ -609,13 +602,9 @@ __global__ void __launch_bounds__(kReduceThreads)
         break;
       const int p = d.at(i, j, k);
       const int sidx = sp.at(i, j, k);
-      // loads independent of the coding first
-      const T xn = x[p + sy], xs = x[p - sy], xe = x[p + 1], xw = x[p - 1];
-      const T xd = x[p - sz], xu = x[p + sz], xc = x[p];
-      const T fv = f[p], oc = A.a[kOC][p];
-      const unsigned b = code[sidx];
       T c[6];
       if (coded) {
+        const unsigned b = code[sidx];
         c[0] = (b & 1u) ? eh : el;
         c[1] = (b & 2u) ? eh : el;
         c[2] = (b & 4u) ? nh : nl;
@@ -627,9 +616,10 @@ __global__ void __launch_bounds__(kReduceThreads)
       }
       // apply7's order: -oN x_n - oN_s x_s - oE x_e - oE_w x_w - uC_d x_d
       // - uC x_u + (oC + 0) x
-      const T ax = -c[2] * xn - c[3] * xs - c[0] * xe - c[1] * xw -
-                   c[5] * xd - c[4] * xu + (oc + T(0)) * xc;
-      const T dv = fv - ax;
+      const T ax = -c[2] * x[p + sy] - c[3] * x[p - sy] - c[0] * x[p + 1] -
+                   c[1] * x[p - 1] - c[5] * x[p - sz] - c[4] * x[p + sz] +
+                   (A.a[kOC][p] + T(0)) * x[p];
+      const T dv = f[p] - ax;
       r[sidx] = (R)dv;
       acc += (double)dv * (double)dv;
     }

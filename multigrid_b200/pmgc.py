@@ -224,6 +224,29 @@ def Vmgdriv(iparm, rparm, u, xf, yf, zf, gxcf, gycf, gzcf, a1cf, a2cf, a3cf,
     return it.value, ie.value, rs.value
 
 
+def Vmvcs(nx, ny, nz, x, iz, w0, w1, w2, w3, istop, itmax, nlev, ipc, pc,
+          ac, cc, fc, tru=None, ilev=1, nlev_real=None, mgsolv=0,
+          epsiln=0.0, errtol=1e-10, nu1=2, nu2=2, mgsmoo=1, stream=None):
+    """APBS V-cycle loop on a packed hierarchy the caller built: iz is the
+    Vbuildstr table (50 x nlev_real ints, column-major, 1-based offsets),
+    ipc the packed host integer parameters (100 per level); x, w0, pc, ac,
+    cc, fc, tru packed device arrays, w1..w3 finest-size work. Returns
+    (cycles, ierror)."""
+    nlev_real = nlev_real or nlev
+    izc = (ctypes.c_int * len(iz))(*[int(v) for v in iz])
+    ipcc = (ctypes.c_int * len(ipc))(*[int(v) for v in ipc])
+    it, ie = ctypes.c_int(), ctypes.c_int()
+    _lib.call("pmg_Vmvcs_d", nx, ny, nz, _p(x), izc, _p(w0), _p(w1), _p(w2),
+              _p(w3), int(istop), int(itmax), ctypes.byref(it),
+              ctypes.byref(ie), int(nlev), int(ilev), int(nlev_real),
+              int(mgsolv), 1, 0, ctypes.c_double(epsiln),
+              ctypes.c_double(errtol), ctypes.c_double(1.0), int(nu1),
+              int(nu2), int(mgsmoo), ipcc, None,
+              _p(pc) if pc is not None else None, _p(ac), _p(cc), _p(fc),
+              _p(tru) if tru is not None else None, _s(stream))
+    return it.value, ie.value
+
+
 def cg_level(nx, ny, nz, op14, rhs, x, thresh=1e-8, max_iters=20000,
              stream=None) -> int:
     """Coarsest-level CG of the class; returns the iteration count."""
