@@ -54,6 +54,9 @@ def parse():
     # one precision, no end-to-end or kernel legs, cycles driven from the
     # host: a short run for kernel profilers
     ap.add_argument("--quick", action="store_true")
+    # the mixed path's 27-point smoother with per-point loads instead of
+    # tiles staged by tensor-memory access (the same bits)
+    ap.add_argument("--no-tma", action="store_true")
     return ap.parse_args()
 
 
@@ -306,18 +309,19 @@ def phase_bytes(p, level: int, phase: str, esz: int,
     fine = level == p.nlev
     nc3 = float(level_n(p.base, level - 1) ** 3) if level >= 2 else 0.0
     if level == 0:
-        if phase == "residual" and coded:  # oC, code byte, f, x; split r
-            return nf3 * (3 * 8 + 1 + (4 if p.precision == "mixed" else 8))
+        if phase == "residual" and coded:  # code byte, f, x; split r
+            return nf3 * (2 * 8 + 1 + (4 if p.precision == "mixed" else 8))
         if phase == "residual":  # 4 coefficients + f + x in double
             return nf3 * (6 * 8 + (4 if p.precision == "mixed" else 0))
         if phase == "refine-update":  # x64 read/write, e32 read
             return nf3 * (8 + 4 + 8)
         return None
     if fine and coded and phase in ("pre-smooth", "post-smooth"):
-        # per sweep: oC, the code byte, f, x read once and written once
-        return 2 * (4 * esz + 1) * n3
-    if fine and coded and phase == "defect":  # oC, code, f, x, r
-        return (4 * esz + 1) * n3
+        # per sweep: the code byte (couplings and oC), f, x read once and
+        # written once
+        return 2 * (3 * esz + 1) * n3
+    if fine and coded and phase == "defect":  # code, f, x, r
+        return (3 * esz + 1) * n3
     arrays = {"pre-smooth": 2 * (7 if fine else 17),
               "post-smooth": 2 * (7 if fine else 17),
               "defect": 7 if fine else 17}
@@ -336,7 +340,10 @@ def phase_bytes(p, level: int, phase: str, esz: int,
 def phase_kernel(p, level: int, phase: str, coded: bool = False):
     if phase in ("pre-smooth", "post-smooth"):
         if level < p.nlev:
-            return ("gs27_phase_kernel", 4)
+            # the mixed path's padded float levels stage their tiles by
+            # tensor-memory access
+            return ("gs27_tma_kernel" if p.precision == "mixed"
+                    else "gs27_phase_kernel", 4)
         # the refinement paths' finest level is colour-split (and coded
         # when its couplings have two values per direction)
         if p.precision != "fp64":
@@ -663,6 +670,9 @@ def main():
         p.buildmultilevelops()
         return p.solve(TOL, MAX_CYCLES)
 
+    if args.no_tma:
+        from multigrid_b200.problem import set_tma_staging
+        set_tma_staging(False)
     if args.quick:
         # profiler runs: launches are serialised and replayed there, so the
         # smoother's tile timings would mean nothing; use the size rule
@@ -704,9 +714,19 @@ def main():
         barrier(world)
         ms = max_over_ranks(world, ms)
         x = p.potential().ravel()
+        # the set-up share of a step: fine-level copy and hierarchy build
+        b0 = torch.cuda.Event(enable_timing=True)
+        b1 = torch.cuda.Event(enable_timing=True)
+        b0.record(stream)
+        for _ in range(3):
+            p.set_fine(*[dev[k] for k in keys])
+            p.buildmultilevelops()
+        b1.record(stream)
+        torch.cuda.synchronize()
+        build_ms = b0.elapsed_time(b1) / 3
         results[precision] = dict(ms=ms, cycles=cyc, relres=res.relres,
                                   x=x, clocks=ck, p=p, stream=stream,
-                                  launches=launches)
+                                  launches=launches, build_ms=build_ms)
 
     prim = results[args.precision]
     value = world * args.steps / (prim["ms"] / 1000.0)
@@ -785,7 +805,8 @@ def main():
                 "traffic_unit": "bytes per phase occurrence (ncu capture)",
                 "peak_source": peak_kind,
                 "bytes_basis": (
-                    "coded couplings: per point oC, one code byte, f, x"
+                    "coded operator: per point one code byte (couplings and "
+                    "oC), f, x"
                     if coded and kname and "code" in kname else
                     "coefficient arrays as stored (kernel table)"),
                 "algorithmic_bytes_per_launch": dom["bytes"],
@@ -834,11 +855,13 @@ def main():
             "fp64": {"value": fp64_value, "cycles":
                      results["fp64"]["cycles"][-1],
                      "ms_per_step": results["fp64"]["ms"] / args.steps,
+                     "build_ms": results["fp64"]["build_ms"],
                      "levels": results["fp64"]["p"].nlev,
                      "error_vs_oracle": err_oracle.get("fp64")},
             "mixed": {"value": mixed_value, "cycles":
                       results["mixed"]["cycles"][-1],
                       "ms_per_step": results["mixed"]["ms"] / args.steps,
+                      "build_ms": results["mixed"]["build_ms"],
                       "levels": results["mixed"]["p"].nlev,
                       "error_vs_fp64": err,
                       "error_vs_oracle": err_oracle.get("mixed")},
@@ -848,6 +871,7 @@ def main():
                           results["fp64-fast"]["cycles"][-1],
                           "ms_per_step": results["fp64-fast"]["ms"] /
                           args.steps,
+                          "build_ms": results["fp64-fast"]["build_ms"],
                           "levels": results["fp64-fast"]["p"].nlev,
                           "error_vs_fp64": error(results["fp64-fast"]["x"],
                                                  xd),

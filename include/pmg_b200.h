@@ -527,6 +527,14 @@ typedef enum {
   PMG_PREC_FP64_FAST = 2
 } pmg_precision;
 
+/* The mixed path's 27-point smoother stages each tile's operator, right-hand
+ * side and iterate planes in shared memory with tensor-memory-access copies
+ * on the levels between its one-launch bottom levels and the finest level
+ * (their float rows are padded to a 16-byte multiple for it). on = 0 makes
+ * problems created afterwards use the per-point-load kernel instead; both
+ * give the same bits. No counterpart in the reference. */
+int pmg_set_tma_staging(int on);
+
 /* Creates a problem on the current CUDA device; allocates its hierarchy.
  * stream may be NULL (a private stream is created). */
 int pmg_problem_create(int base, int nlev, double box, int precision,

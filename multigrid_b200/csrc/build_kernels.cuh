@@ -25,7 +25,7 @@ namespace pmg {
 template <int KIND>
 __global__ void __launch_bounds__(128)
     buildP_op_kernel(Dims df, Dims dc, Op14<double> A, P27W<double> P,
-                     P27W<float> P32) {
+                     P27W<float> P32, Dims dc32) {
   const int ii = blockIdx.x * blockDim.x + threadIdx.x + 2;
   const int jj = blockIdx.y * blockDim.y + threadIdx.y + 2;
   const int kk = blockIdx.z + 2;
@@ -87,10 +87,12 @@ __global__ void __launch_bounds__(128)
 #pragma unroll
   for (int s = 0; s < 27; ++s)
     P.p[s][pc] = w[s];
-  if (P32.p[0]) // the mixed path's float copy
+  if (P32.p[0]) { // the mixed path's float copy (rows dc32.px apart)
+    const int pc32 = dc32.at(ii, jj, kk);
 #pragma unroll
     for (int s = 0; s < 27; ++s)
-      P32.p[s][pc] = (float)w[s];
+      P32.p[s][pc32] = (float)w[s];
+  }
 }
 
 // Constant weights 1, 1/2, 1/4, 1/8 (VbuildPb_trilin, pmgc/buildPd.cc:
@@ -158,11 +160,12 @@ __device__ __forceinline__ double galerkin_entry(const Dims &df,
   return S == 0 ? acc : -acc;
 }
 
-// out32 (all null: none) receives the float copy of each entry.
+// out32 (all null: none) receives the float copy of each entry (rows
+// dc32.px apart).
 template <int KIND>
 __global__ void __launch_bounds__(128)
     buildG_kernel(Dims df, Dims dc, P27<double> P, Op14<double> A,
-                  Op14W<double> out, Op14W<float> out32) {
+                  Op14W<double> out, Op14W<float> out32, Dims dc32) {
   const int ii = blockIdx.x * blockDim.x + threadIdx.x + 2;
   const int jj = blockIdx.y * blockDim.y + threadIdx.y + 2;
   const int kk = blockIdx.z + 2;
@@ -171,63 +174,64 @@ __global__ void __launch_bounds__(128)
   const int pc = dc.at(ii, jj, kk);
   const int c0 = df.at(2 * ii - 1, 2 * jj - 1, 2 * kk - 1);
   const bool f32 = out32.a[0] != nullptr; // the mixed path's float copy
+  const int pc32 = dc32.at(ii, jj, kk);
   double v;
   v = galerkin_entry<KIND, 0>(df, dc, P, A, pc, c0);
   out.a[0][pc] = v;
   if (f32)
-    out32.a[0][pc] = (float)v;
+    out32.a[0][pc32] = (float)v;
   v = galerkin_entry<KIND, 1>(df, dc, P, A, pc, c0);
   out.a[1][pc] = v;
   if (f32)
-    out32.a[1][pc] = (float)v;
+    out32.a[1][pc32] = (float)v;
   v = galerkin_entry<KIND, 2>(df, dc, P, A, pc, c0);
   out.a[2][pc] = v;
   if (f32)
-    out32.a[2][pc] = (float)v;
+    out32.a[2][pc32] = (float)v;
   v = galerkin_entry<KIND, 3>(df, dc, P, A, pc, c0);
   out.a[3][pc] = v;
   if (f32)
-    out32.a[3][pc] = (float)v;
+    out32.a[3][pc32] = (float)v;
   v = galerkin_entry<KIND, 4>(df, dc, P, A, pc, c0);
   out.a[4][pc] = v;
   if (f32)
-    out32.a[4][pc] = (float)v;
+    out32.a[4][pc32] = (float)v;
   v = galerkin_entry<KIND, 5>(df, dc, P, A, pc, c0);
   out.a[5][pc] = v;
   if (f32)
-    out32.a[5][pc] = (float)v;
+    out32.a[5][pc32] = (float)v;
   v = galerkin_entry<KIND, 6>(df, dc, P, A, pc, c0);
   out.a[6][pc] = v;
   if (f32)
-    out32.a[6][pc] = (float)v;
+    out32.a[6][pc32] = (float)v;
   v = galerkin_entry<KIND, 7>(df, dc, P, A, pc, c0);
   out.a[7][pc] = v;
   if (f32)
-    out32.a[7][pc] = (float)v;
+    out32.a[7][pc32] = (float)v;
   v = galerkin_entry<KIND, 8>(df, dc, P, A, pc, c0);
   out.a[8][pc] = v;
   if (f32)
-    out32.a[8][pc] = (float)v;
+    out32.a[8][pc32] = (float)v;
   v = galerkin_entry<KIND, 9>(df, dc, P, A, pc, c0);
   out.a[9][pc] = v;
   if (f32)
-    out32.a[9][pc] = (float)v;
+    out32.a[9][pc32] = (float)v;
   v = galerkin_entry<KIND, 10>(df, dc, P, A, pc, c0);
   out.a[10][pc] = v;
   if (f32)
-    out32.a[10][pc] = (float)v;
+    out32.a[10][pc32] = (float)v;
   v = galerkin_entry<KIND, 11>(df, dc, P, A, pc, c0);
   out.a[11][pc] = v;
   if (f32)
-    out32.a[11][pc] = (float)v;
+    out32.a[11][pc32] = (float)v;
   v = galerkin_entry<KIND, 12>(df, dc, P, A, pc, c0);
   out.a[12][pc] = v;
   if (f32)
-    out32.a[12][pc] = (float)v;
+    out32.a[12][pc32] = (float)v;
   v = galerkin_entry<KIND, 13>(df, dc, P, A, pc, c0);
   out.a[13][pc] = v;
   if (f32)
-    out32.a[13][pc] = (float)v;
+    out32.a[13][pc32] = (float)v;
 }
 
 // One Galerkin entry per thread (blockIdx.x: the output slot, so the
@@ -238,7 +242,7 @@ __global__ void __launch_bounds__(128)
 template <int KIND>
 __global__ void __launch_bounds__(128)
     buildG_entry_kernel(Dims df, Dims dc, P27<double> P, Op14<double> A,
-                        Op14W<double> out, Op14W<float> out32) {
+                        Op14W<double> out, Op14W<float> out32, Dims dc32) {
   const int mx = dc.nx - 2, my = dc.ny - 2;
   const int q = blockIdx.y * blockDim.x + threadIdx.x;
   if (q >= mx * my * (dc.nz - 2))
@@ -267,7 +271,7 @@ __global__ void __launch_bounds__(128)
   }
   out.a[S][pc] = v;
   if (out32.a[0])
-    out32.a[S][pc] = (float)v;
+    out32.a[S][dc32.at(ii, jj, kk)] = (float)v;
 }
 
 } // namespace pmg

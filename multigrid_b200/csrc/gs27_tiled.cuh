@@ -102,13 +102,14 @@ __device__ __forceinline__ T gs27_update(const Gs27Point<T> &c, const T *xc,
 
 // Sub-colour step with halo H (step 3 - H of the phase): the points of the
 // step's sub-colour within H of the tile, a fixed NU x NU grid of them
-// clipped to the interior.
-template <typename T, int TT, int H>
-__device__ __forceinline__ void gs27_step(const Dims &d, const Op14<T> &A,
-                                          const T *cc, const T *fc, T *xs,
-                                          int ti0, int tj0, int k,
-                                          int order) {
-  constexpr int W = Gs27Tile<TT>::W, NT = Gs27Tile<TT>::THREADS;
+// clipped to the interior. xk: the staged plane k, its entry 0 at
+// (ti0 - 4, tj0 - 4), rows W apart; planes k - 1 and k + 1 at xk -/+ PS.
+template <typename T, int TT, int W, int PS, int H>
+__device__ __forceinline__ void gs27_step_at(const Dims &d, const Op14<T> &A,
+                                             const T *cc, const T *fc, T *xk,
+                                             int ti0, int tj0, int k,
+                                             int order) {
+  constexpr int NT = Gs27Tile<TT>::THREADS;
   constexpr int NU = TT / 2 + H, NQ = NU * NU;
   const int sy = d.sy(), sz = d.sz();
   const int s = (order >> (2 * (3 - H))) & 3;
@@ -124,13 +125,25 @@ __device__ __forceinline__ void gs27_step(const Dims &d, const Op14<T> &A,
     const int v = q / NU, u = q - v * NU;
     const int i = ia + 2 * u, j = ja + 2 * v;
     if (q < NQ && i >= 2 && i <= i_max && j >= 2 && j <= j_max) {
-      const int sidx = W * W + (i - i_lo) + W * (j - j_lo);
+      const int sidx = (i - i_lo) + W * (j - j_lo);
       Gs27Point<T> c;
       gs27_load(A, cc, fc, d.at(i, j, k), sy, sz, c);
-      xs[sidx] = gs27_update<T, W>(c, &xs[sidx], &xs[sidx - W * W],
-                                   &xs[sidx + W * W]);
+      xk[sidx] =
+          gs27_update<T, W>(c, &xk[sidx], &xk[sidx - PS], &xk[sidx + PS]);
     }
   }
+}
+
+// gs27_step_at on the staged planes of gs27_phase_kernel (W x W each, plane
+// k - 1 first)
+template <typename T, int TT, int H>
+__device__ __forceinline__ void gs27_step(const Dims &d, const Op14<T> &A,
+                                          const T *cc, const T *fc, T *xs,
+                                          int ti0, int tj0, int k,
+                                          int order) {
+  constexpr int W = Gs27Tile<TT>::W;
+  gs27_step_at<T, TT, W, W * W, H>(d, A, cc, fc, xs + W * W, ti0, tj0, k,
+                                   order);
 }
 
 // One parity phase on TT x TT tiles. kfirst: first plane of the parity (2 or

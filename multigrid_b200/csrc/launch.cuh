@@ -85,12 +85,16 @@ int launch_gs27(const Dims &d, const Op14<T> &A, const T *cc, const T *fc,
 
 // Prolongation / Galerkin builders (pmg_build.cu). P32 / out32 (all null:
 // none) also receive the float copies of the interior entries written.
+// P32 / out32 (optional): float copies, rows dc32.px apart (dc32 defaults
+// to dc)
 int launch_buildP(const Dims &df, const Dims &dc, int kind,
                   const Op14<double> &A, const P27W<double> &P,
-                  cudaStream_t s, const P27W<float> &P32 = P27W<float>{});
+                  cudaStream_t s, const P27W<float> &P32 = P27W<float>{},
+                  const Dims *dc32 = nullptr);
 int launch_buildG(const Dims &df, const Dims &dc, int kind,
                   const P27<double> &P, const Op14<double> &A,
                   const Op14W<double> &out, cudaStream_t s,
-                  const Op14W<float> &out32 = Op14W<float>{});
+                  const Op14W<float> &out32 = Op14W<float>{},
+                  const Dims *dc32 = nullptr);
 
 } // namespace pmg

@@ -17,14 +17,22 @@ namespace pmg {
 
 constexpr int kMaxN = 1025;
 
+// nx, ny, nz points per axis; rows px >= nx entries apart (px > nx pads
+// the rows of an array to a 16-byte multiple for tensor-memory-access
+// copies; every point's index and every stencil offset follow px, the
+// entries past nx in a row are never read as grid points).
 struct Dims {
-  int nx, ny, nz;
-  __host__ __device__ int sy() const { return nx; }
-  __host__ __device__ int sz() const { return nx * ny; }
+  int nx, ny, nz, px;
+  Dims() = default;
+  __host__ __device__ Dims(int x, int y, int z, int pitch = 0)
+      : nx(x), ny(y), nz(z), px(pitch > x ? pitch : x) {}
+  __host__ __device__ int sy() const { return px; }
+  __host__ __device__ int sz() const { return px * ny; }
   __host__ __device__ int at(int i, int j, int k) const {
-    return ((k - 1) * ny + (j - 1)) * nx + (i - 1);
+    return ((k - 1) * ny + (j - 1)) * px + (i - 1);
   }
-  __host__ __device__ long count() const { return (long)nx * ny * nz; }
+  // entries of an array (the padding included)
+  __host__ __device__ long count() const { return (long)px * ny * nz; }
 };
 
 // The 14 upper diagonals of a symmetric 27-point operator in the reference's

@@ -6,6 +6,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <atomic>
 #include <climits>
 #include <new>
 
@@ -13,6 +14,9 @@
 #include "bottom_cluster.cuh"
 #include "bottom_cycle.cuh"
 #include "gs27_tiled.cuh"
+#include "gs27_tma.cuh"
+
+#include <cudaTypedefs.h>
 #include "launch.cuh"
 #include "pcg_kernels.cuh"
 #include "split_layout.cuh"
@@ -28,6 +32,18 @@ struct LevelBuf {
   int n = 0;
   Dims d{};
   long n3 = 0;
+  // the float arrays of the level (mixed path): rows padded to a 16-byte
+  // multiple on the levels the 27-point smoother stages by tensor-memory
+  // access (between the one-launch bottom levels and the finest level),
+  // else d
+  Dims d32{};
+  long n3_32 = 0;
+  // tensor maps of the padded float iterate and its ping-pong partner (the
+  // 27-point smoother's x staging)
+  struct TmaMaps {
+    CUtensorMap x, xalt;
+  } tma;
+  bool tma_ok = false;
   double *op[14] = {};
   double *P[27] = {}; // prolongation from this level to level+1
   double *x = nullptr, *f = nullptr, *r = nullptr;
@@ -42,6 +58,11 @@ struct LevelBuf {
   unsigned char *code = nullptr;
   int *code_info = nullptr; // device: ranges and the mismatch flags
   double *lut64 = nullptr;  // device: the double couplings of the codes
+  // device: the centre coefficient by code (bit 6 of the code byte) and the
+  // per-code ranges it is found from
+  double *octab64 = nullptr;
+  float *octab32 = nullptr;
+  long long *oc_range = nullptr;
   // fp64-fast finest level: the correction, its right-hand side and the
   // operator (oC oE oN uC) in the colour-split layout, double
   double *xs = nullptr, *fs = nullptr;
@@ -96,6 +117,8 @@ template <> struct LevelArrays<float> {
   static float *alt(LevelBuf &v) { return v.xalt32; }
   static float *fine_op(LevelBuf &v, int s) { return v.op32[s]; }
   static const float *lut(LevelBuf &) { return nullptr; }
+  static const float *octab(LevelBuf &v) { return v.octab32; }
+  static const Dims &dims(const LevelBuf &v) { return v.d32; }
   static Op14<float> A(const LevelBuf &v) { return v.A32(14); }
   static P27<float> P(const LevelBuf &v) { return v.Pc32(); }
 };
@@ -106,6 +129,8 @@ template <> struct LevelArrays<double> {
   static double *alt(LevelBuf &v) { return v.xalt; }
   static double *fine_op(LevelBuf &v, int s) { return v.ops[s]; }
   static const double *lut(LevelBuf &v) { return v.lut64; }
+  static const double *octab(LevelBuf &v) { return v.octab64; }
+  static const Dims &dims(const LevelBuf &v) { return v.d; }
   static Op14<double> A(const LevelBuf &v) { return v.A64(14); }
   static P27<double> P(const LevelBuf &v) { return v.Pc(); }
 };
@@ -124,7 +149,9 @@ struct SolveState {
   double tol;
   int max_cycles;
   int cycles;
-  int status; // 0 running / converged / capped, 1 diverged, 2 r0 not finite
+  // 0 running / converged / capped, 1 diverged, 2 r0 not finite, 3 a
+  // staged copy of the 27-point smoother did not arrive
+  int status;
   int pad;
   double r0, r;
   double hist[kMaxHist + 1];
@@ -145,6 +172,8 @@ struct pmg_problem {
   LevelBuf lv[kMaxLevels + 1];
   double *cg_r = nullptr, *cg_p = nullptr, *cg_ap = nullptr;
   int *cg_status = nullptr;
+  int *kernel_err = nullptr; // device: set by gs27_tma_kernel on a lost stage
+  int num_sms = 0;
   // Relative stopping threshold of the coarsest CG on the mixed path's
   // correction equation (the FP64 path keeps the class's absolute 1e-8).
   double coarse_rtol = 1e-4;
@@ -196,17 +225,32 @@ namespace {
 
 int level_n(int base, int L) { return base * (1 << L) + 1; }
 
+// Mixed path: the top level of the one-launch bottom cycle (the levels up
+// to 17 points per axis); 0 on the other paths.
+int bottom_top_of(int base, int nlev, int precision) {
+  int top = 0;
+  if (precision == PMG_PREC_MIXED)
+    for (int L = 1; L < nlev && L <= kBottomMaxLevels; ++L)
+      if (level_n(base, L) <= kBottomMaxN)
+        top = L;
+  return top;
+}
+
 // Lays out every device array of a problem; with a.base == nullptr only
 // counts bytes.
 void plan(pmg_problem *p, Arena &a) {
   const bool mixed = p->precision == PMG_PREC_MIXED;
   const bool fast = p->precision == PMG_PREC_FP64_FAST;
+  const int bottom_top = bottom_top_of(p->base, p->nlev, p->precision);
   for (int L = 1; L <= p->nlev; ++L) {
     LevelBuf &v = p->lv[L];
     v.n = level_n(p->base, L);
     v.d = Dims{v.n, v.n, v.n};
     v.n3 = v.d.count();
     const bool fine = L == p->nlev;
+    const bool pitched = mixed && !fine && L > bottom_top;
+    v.d32 = pitched ? Dims{v.n, v.n, v.n, (v.n + 3) & ~3} : v.d;
+    v.n3_32 = v.d32.count();
     const int nops = fine ? 4 : 14;
     for (int s = 0; s < 14; ++s)
       v.op[s] = s < nops ? a.take<double>(v.n3) : nullptr;
@@ -223,17 +267,21 @@ void plan(pmg_problem *p, Arena &a) {
     v.xalt = (smoothed && !mixed) ? a.take<double>(v.n3) : nullptr;
     v.omega = a.take<double>(1);
     if (mixed) {
+      const long m = v.n3_32;
       for (int s = 0; s < 14; ++s)
-        v.op32[s] = (L > 1 && s < nops) ? a.take<float>(v.n3) : nullptr;
+        v.op32[s] = (L > 1 && s < nops) ? a.take<float>(m) : nullptr;
       for (int s = 0; s < 27; ++s)
-        v.P32[s] = fine ? nullptr : a.take<float>(v.n3);
-      v.x32 = a.take<float>(v.n3);
-      v.f32 = a.take<float>(v.n3);
-      v.r32 = L > 1 ? a.take<float>(v.n3) : nullptr;
-      v.xalt32 = smoothed ? a.take<float>(v.n3) : nullptr;
+        v.P32[s] = fine ? nullptr : a.take<float>(m);
+      v.x32 = a.take<float>(m);
+      v.f32 = a.take<float>(m);
+      v.r32 = L > 1 ? a.take<float>(m) : nullptr;
+      v.xalt32 = smoothed ? a.take<float>(m) : nullptr;
       v.code = fine ? a.take<unsigned char>(v.n3) : nullptr;
-      v.code_info = fine ? a.take<int>(8) : nullptr;
+      v.code_info = fine ? a.take<int>(12) : nullptr;
       v.lut64 = fine ? a.take<double>(6) : nullptr;
+      v.octab64 = fine ? a.take<double>(128) : nullptr;
+      v.octab32 = fine ? a.take<float>(128) : nullptr;
+      v.oc_range = fine ? a.take<long long>(128) : nullptr;
     }
     if (fast && fine) {
       for (int s = 0; s < 4; ++s)
@@ -241,8 +289,10 @@ void plan(pmg_problem *p, Arena &a) {
       v.xs = a.take<double>(v.n3);
       v.fs = a.take<double>(v.n3);
       v.code = a.take<unsigned char>(v.n3);
-      v.code_info = a.take<int>(8);
+      v.code_info = a.take<int>(12);
       v.lut64 = a.take<double>(6);
+      v.octab64 = a.take<double>(128);
+      v.oc_range = a.take<long long>(128);
     }
   }
   const long n1 = p->lv[1].n3;
@@ -250,6 +300,7 @@ void plan(pmg_problem *p, Arena &a) {
   p->cg_p = a.take<double>(n1);
   p->cg_ap = a.take<double>(n1);
   p->cg_status = a.take<int>(2);
+  p->kernel_err = a.take<int>(1);
   p->d_state = a.take<SolveState>(1);
   // partials of the largest launch using each slot: the finest level's
   // reductions, and the damping on any coarse level
@@ -434,6 +485,94 @@ double norm_from_sum(const pmg_problem *p, double s) {
   return sqrt(s / n3);
 }
 
+// ---- the 27-point smoother by tensor-memory access (gs27_tma.cuh) -----------
+
+// pmg_set_tma_staging: problems created while it is off use gs27_tiled.cuh
+// on every level (the same bits)
+std::atomic<int> g_tma_on{1};
+bool tma_disabled() { return g_tma_on.load() == 0; }
+
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f,
+                                cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    (void)cudaGetLastError();
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+  }();
+  return fn;
+}
+
+// A 3-D map of one padded float array of the level: extent nx x ny x nz
+// (the padding reads as outside), rows px apart, boxes of
+// kTmaBX x kTmaBY x 1.
+bool encode_level_map(CUtensorMap *m, const float *base, const Dims &d) {
+  auto enc = tensor_map_encoder();
+  if (!enc || !base || (d.px * sizeof(float)) % 16 != 0)
+    return false;
+  const cuuint64_t dims[3] = {(cuuint64_t)d.nx, (cuuint64_t)d.ny,
+                              (cuuint64_t)d.nz};
+  const cuuint64_t strides[2] = {(cuuint64_t)d.px * sizeof(float),
+                                 (cuuint64_t)d.px * d.ny * sizeof(float)};
+  const cuuint32_t box[3] = {kTmaBX, kTmaBY, 1};
+  const cuuint32_t elem[3] = {1, 1, 1};
+  return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void *)base, dims,
+             strides, box, elem, CU_TENSOR_MAP_INTERLEAVE_NONE,
+             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// Tensor maps of every padded level (their arrays are fixed for the life
+// of the problem); a level whose maps cannot be made uses gs27_tiled.cuh.
+void encode_tma_maps(pmg_problem *p) {
+  for (int L = 2; L < p->nlev; ++L) {
+    LevelBuf &v = p->lv[L];
+    v.tma_ok = false;
+    if (v.d32.px == v.d.px || !v.xalt32 || v.d32.nx - 2 < 1)
+      continue;
+    bool ok = encode_level_map(&v.tma.x, v.x32, v.d32);
+    ok = ok && encode_level_map(&v.tma.xalt, v.xalt32, v.d32);
+    v.tma_ok = ok;
+  }
+}
+
+// nsweeps eight-colour sweeps of a padded float level (launch_gs27_pp's
+// order and ping-pong, the colours forward), *cur in and out.
+int launch_gs27_tma(pmg_problem *p, LevelBuf &v, int nsweeps, int zero_init,
+                    float **cur) {
+  cudaStream_t s = p->stream;
+  const Dims &d = v.d32;
+  if (zero_init)
+    PMG_CUDA_TRY(cudaMemsetAsync(*cur, 0, sizeof(float) * v.n3_32, s));
+  const int order = 0 | 1 << 2 | 2 << 4 | 3 << 6;
+  const unsigned tx = cdiv(d.nx - 2, kTmaTT), ty = cdiv(d.ny - 2, kTmaTT);
+  const Op14<float> A = v.A32(14);
+  float *c = *cur;
+  float *a = c == v.x32 ? v.xalt32 : v.x32;
+  for (int sw = 0; sw < nsweeps; ++sw) {
+    const CUtensorMap &mc = c == v.x32 ? v.tma.x : v.tma.xalt;
+    const CUtensorMap &ma = c == v.x32 ? v.tma.xalt : v.tma.x;
+    for (int ph = 0; ph < 2; ++ph) {
+      const int kfirst = ph == 0 ? 2 : 3;
+      const int planes = kfirst > d.nz - 1 ? 0 : (d.nz - 1 - kfirst) / 2 + 1;
+      if (planes == 0)
+        continue;
+      Gs27TmaMaps m;
+      m.own = mc;
+      m.nb = ph == 0 ? mc : ma;
+      gs27_tma_kernel<<<dim3(tx, ty, (unsigned)planes), kTmaThreads, 0, s>>>(
+          m, d, A, v.f32, a, kfirst, order, p->kernel_err);
+    }
+    std::swap(c, a);
+  }
+  PMG_LAUNCH_CHECK();
+  *cur = c;
+  return PMG_OK;
+}
+
 // ---- refinement paths (mixed, fp64-fast) -----------------------------------
 
 // Smoothing sweeps of a refinement-step V-cycle on level L in type T: on the
@@ -448,15 +587,18 @@ int smooth_ref(pmg_problem *p, int L, int nsweeps, int zero_init, T **cur) {
     return launch_gs7_code<T>(v.d, A::fine_op(v, kOC), A::f(v),
                               A::fine_op(v, kOE), A::fine_op(v, kON),
                               A::fine_op(v, kUC), v.code, v.code_info,
-                              A::lut(v), *cur, nsweeps, 0, zero_init,
-                              p->stream);
+                              A::lut(v), A::octab(v), *cur, nsweeps, 0,
+                              zero_init, p->stream);
   if (L == p->nlev) // colour-split layout (split_layout.cuh)
     return launch_gs7_split<T>(v.d, A::fine_op(v, kOC), A::f(v),
                                A::fine_op(v, kOE), A::fine_op(v, kON),
                                A::fine_op(v, kUC), *cur, nsweeps, 0,
                                zero_init, p->stream);
+  if constexpr (sizeof(T) == sizeof(float))
+    if (v.tma_ok)
+      return launch_gs27_tma(p, v, nsweeps, zero_init, cur);
   T *alt = *cur == A::x(v) ? A::alt(v) : A::x(v);
-  return launch_gs27_pp<T>(v.d, A::A(v), nullptr, A::f(v), *cur, alt,
+  return launch_gs27_pp<T>(A::dims(v), A::A(v), nullptr, A::f(v), *cur, alt,
                            nsweeps, 0, zero_init, p->stream, cur);
 }
 
@@ -539,19 +681,19 @@ template <typename T> int vcycle_ref(pmg_problem *p, int L) {
     defect7_code_kernel<T>
         <<<defect7_code_grid(v.d), interior_block(), 0, s>>>(
             v.d, A::fine_op(v, kOC), A::fine_op(v, kOE), A::fine_op(v, kON),
-            A::fine_op(v, kUC), v.code, v.code_info, A::lut(v), A::f(v), x,
-            A::r(v));
+            A::fine_op(v, kUC), v.code, v.code_info, A::lut(v), A::octab(v),
+            A::f(v), x, A::r(v));
   else if (kind == 7) // split arrays in, reference-layout defect out
     defect7_split_kernel<T><<<interior_grid(v.d), interior_block(), 0, s>>>(
         v.d, A::fine_op(v, kOC), A::fine_op(v, kOE), A::fine_op(v, kON),
         A::fine_op(v, kUC), A::f(v), x, A::r(v));
   else
     defect_kernel<27, T><<<interior_grid(v.d), interior_block(), 0, s>>>(
-        v.d, A::A(v), A::f(v), x, A::r(v));
+        A::dims(v), A::A(v), A::f(v), x, A::r(v));
   prof_end(p, sl + kPhDefect);
   prof_begin(p, sl + kPhRestrict);
   restrict_kernel<T, T><<<interior_grid(c.d), interior_block(), 0, s>>>(
-      v.d, c.d, A::r(v), A::f(c), A::P(c));
+      A::dims(v), A::dims(c), A::r(v), A::f(c), A::P(c));
   prof_end(p, sl + kPhRestrict);
   PMG_LAUNCH_CHECK();
   if (bottom_below) {
@@ -576,7 +718,7 @@ template <typename T> int vcycle_ref(pmg_problem *p, int L) {
           c.n3, c.x, c.x32);
   } else {
     ideal_lambda_kernel<T><<<lambda_grid(c.d), interior_block(), 0, s>>>(
-        c.d, A::A(c), A::x(c), A::f(c), p->red_lambda, c.omega,
+        A::dims(c), A::A(c), A::x(c), A::f(c), p->red_lambda, c.omega,
         lambda_planes(c.d));
   }
   prof_end(p, sl + kPhLambda);
@@ -584,11 +726,11 @@ template <typename T> int vcycle_ref(pmg_problem *p, int L) {
   prof_begin(p, sl + kPhInterp);
   if (kind == 7) // the finest iterate is split
     interp_add_kernel<T, true><<<interp_grid(c.d), interior_block(), 0, s>>>(
-        c.d, v.d, A::x(c), A::P(c), x, c.omega);
+        A::dims(c), v.d, A::x(c), A::P(c), x, c.omega);
   else
     interp_add_kernel<T, false>
-        <<<interp_grid(c.d), interior_block(), 0, s>>>(c.d, v.d, A::x(c),
-                                                       A::P(c), x, c.omega);
+        <<<interp_grid(c.d), interior_block(), 0, s>>>(
+            A::dims(c), A::dims(v), A::x(c), A::P(c), x, c.omega);
   prof_end(p, sl + kPhInterp);
   PMG_LAUNCH_CHECK();
   prof_begin(p, sl + kPhPost);
@@ -613,16 +755,16 @@ int refine_residual_async(pmg_problem *p, bool to_host = true) {
   if (p->precision == PMG_PREC_MIXED) {
     if (p->use_codes)
       defect_norm_code_kernel<double, float><<<g, b, 0, s>>>(
-          v.d, v.A64(4), v.f, v.x, v.code, v.lut64, v.code_info, v.f32,
-          p->red_norm);
+          v.d, v.A64(4), v.f, v.x, v.code, v.lut64, v.octab64, v.code_info,
+          v.f32, p->red_norm);
     else
       defect_norm_kernel<7, double, float, true><<<g, b, 0, s>>>(
           v.d, v.A64(4), v.f, v.x, v.f32, p->red_norm);
   } else {
     if (p->use_codes)
       defect_norm_code_kernel<double, double><<<g, b, 0, s>>>(
-          v.d, v.A64(4), v.f, v.x, v.code, v.lut64, v.code_info, v.fs,
-          p->red_norm);
+          v.d, v.A64(4), v.f, v.x, v.code, v.lut64, v.octab64, v.code_info,
+          v.fs, p->red_norm);
     else
       defect_norm_kernel<7, double, double, true><<<g, b, 0, s>>>(
           v.d, v.A64(4), v.f, v.x, v.fs, p->red_norm);
@@ -749,7 +891,8 @@ __global__ void solve_init_kernel(SolveState *st, const double *sum,
 }
 
 __global__ void solve_check_kernel(SolveState *st, const double *sum,
-                                   double n3, cudaGraphConditionalHandle h) {
+                                   double n3, const int *kernel_err,
+                                   cudaGraphConditionalHandle h) {
   const double r = sqrt(sum[0] / n3);
   const int c = ++st->cycles;
   if (c <= kMaxHist)
@@ -757,9 +900,13 @@ __global__ void solve_check_kernel(SolveState *st, const double *sum,
   st->r = r;
   const double r0 = st->r0;
   const bool diverged = !isfinite(r) || r > 1e6 * r0;
+  const bool lost = *kernel_err != 0;
   if (diverged)
     st->status = 1;
-  const bool go = !diverged && !(r / r0 < st->tol) && c < st->max_cycles;
+  if (lost)
+    st->status = 3;
+  const bool go =
+      !diverged && !lost && !(r / r0 < st->tol) && c < st->max_cycles;
   cudaGraphSetConditional(h, go ? 1u : 0u);
 }
 
@@ -889,8 +1036,8 @@ int ensure_solve_graph(pmg_problem *p) {
     int rc = cycle_with_residual(p, false);
     if (rc)
       return rc;
-    solve_check_kernel<<<1, 1, 0, p->stream>>>(p->d_state,
-                                               p->red_norm.result, n3, h);
+    solve_check_kernel<<<1, 1, 0, p->stream>>>(
+        p->d_state, p->red_norm.result, n3, p->kernel_err, h);
     PMG_LAUNCH_CHECK();
     return PMG_OK;
   };
@@ -1053,6 +1200,22 @@ int ensure_pcg_graph(pmg_problem *p) {
                           &c.body_kernels);
 }
 
+// Bit 6 of the finest code bytes and the centre-coefficient tables
+// (split_layout.cuh, oc_range_kernel ... oc_table_kernel), after the
+// coupling codes.
+int build_oc_codes(pmg_problem *p, LevelBuf &v) {
+  cudaStream_t s = p->stream;
+  oc_range_init_kernel<<<1, 128, 0, s>>>(v.oc_range);
+  oc_range_kernel<<<oc_range_blocks(v.d), 256, 0, s>>>(v.d, v.op[kOC],
+                                                       v.code, v.oc_range);
+  oc_code_kernel<<<interior_grid(v.d), interior_block(), 0, s>>>(
+      v.d, v.op[kOC], v.oc_range, v.code_info, v.code);
+  oc_table_kernel<<<1, 128, 0, s>>>(v.oc_range, v.octab64, v.octab32);
+  p->launches += 4;
+  PMG_LAUNCH_CHECK();
+  return PMG_OK;
+}
+
 // A new problem starts from the state of a freshly constructed class: the
 // coarse iterates are zero (the coarsest CG warm-starts from its level's
 // iterate, so a previous solve's values would change the result).
@@ -1064,7 +1227,7 @@ int new_problem_loaded(pmg_problem *p) {
           cudaMemsetAsync(c.x, 0, sizeof(double) * c.n3, p->stream));
     if (c.x32)
       PMG_CUDA_TRY(
-          cudaMemsetAsync(c.x32, 0, sizeof(float) * c.n3, p->stream));
+          cudaMemsetAsync(c.x32, 0, sizeof(float) * c.n3_32, p->stream));
   }
   p->fine_set = true;
   p->built = false;
@@ -1106,10 +1269,7 @@ int pmg_problem_create(int base, int nlev, double box, int precision,
   p->nlev = nlev;
   p->box = box;
   p->precision = precision;
-  if (precision == PMG_PREC_MIXED)
-    for (int L = 1; L < nlev && L <= kBottomMaxLevels; ++L)
-      if (level_n(base, L) <= kBottomMaxN)
-        p->bottom_top = L;
+  p->bottom_top = bottom_top_of(base, nlev, precision);
   Arena a;
   plan(p, a);
   p->arena_bytes = a.off;
@@ -1122,6 +1282,15 @@ int pmg_problem_create(int base, int nlev, double box, int precision,
   Arena b;
   b.base = p->arena;
   plan(p, b);
+  {
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess)
+      cudaDeviceGetAttribute(&p->num_sms, cudaDevAttrMultiProcessorCount,
+                             dev);
+    (void)cudaGetLastError();
+    if (!tma_disabled())
+      encode_tma_maps(p);
+  }
   if (stream) {
     p->stream = (cudaStream_t)stream;
   } else {
@@ -1186,6 +1355,11 @@ int pmg_problem_set_coarse_rtol(pmg_problem *p, double rtol) {
   }
   p->coarse_rtol = rtol;
   drop_graphs(p); // the captured cycles bake the threshold in
+  return PMG_OK;
+}
+
+int pmg_set_tma_staging(int on) {
+  g_tma_on.store(on != 0);
   return PMG_OK;
 }
 
@@ -1322,6 +1496,7 @@ int pmg_build_hierarchy(pmg_problem *p, int trilinear) {
     // entries; the shells stay zero from the arena's clearing)
     P27W<float> P32w{};
     Op14W<float> out32{};
+    // the builders write the float copies (rows c.d32.px apart)
     if (mixed) {
       for (int q = 0; q < 27; ++q)
         P32w.p[q] = c.P32[q];
@@ -1333,7 +1508,7 @@ int pmg_build_hierarchy(pmg_problem *p, int trilinear) {
           c.d, Pw);
       PMG_LAUNCH_CHECK();
     } else if ((rc = launch_buildP(f.d, c.d, kind, f.A64(kind == 7 ? 4 : 14),
-                                   Pw, s, P32w))) {
+                                   Pw, s, P32w, &c.d32))) {
       return rc;
     }
     p->launches += 2; // prolongation + Galerkin operator
@@ -1341,7 +1516,8 @@ int pmg_build_hierarchy(pmg_problem *p, int trilinear) {
     for (int q = 0; q < 14; ++q)
       out.a[q] = c.op[q];
     if ((rc = launch_buildG(f.d, c.d, kind, c.Pc(),
-                            f.A64(kind == 7 ? 4 : 14), out, s, out32)))
+                            f.A64(kind == 7 ? 4 : 14), out, s, out32,
+                            &c.d32)))
       return rc;
   }
   if (mixed) {
@@ -1355,8 +1531,8 @@ int pmg_build_hierarchy(pmg_problem *p, int trilinear) {
       }
     // coded couplings of the finest float operator, when it has two values
     // per direction (split_layout.cuh)
-    const int init[8] = {INT_MAX, INT_MIN, INT_MAX, INT_MIN,
-                         INT_MAX, INT_MIN, 0,       0};
+    const int init[12] = {INT_MAX, INT_MIN, INT_MAX, INT_MIN, INT_MAX, INT_MIN,
+                          0,       0,       0,       0,       0,       0};
     PMG_CUDA_TRY(cudaMemcpyAsync(v.code_info, init, sizeof(init),
                                  cudaMemcpyHostToDevice, s));
     const dim3 ig = interior_grid(v.d), ib = interior_block();
@@ -1369,12 +1545,14 @@ int pmg_build_hierarchy(pmg_problem *p, int trilinear) {
     lut64_check_kernel<double><<<ig, ib, 0, s>>>(
         v.d, v.op[kOE], v.op[kON], v.op[kUC], v.code, v.lut64, v.code_info);
     p->launches += 4;
+    if ((rc = build_oc_codes(p, v)))
+      return rc;
     if (trilinear) // the trilinear builder writes double only
       for (int L = 1; L < p->nlev; ++L) {
         LevelBuf &c = p->lv[L];
         for (int q = 0; q < 27; ++q) {
-          convert_kernel<double, float><<<flat_grid(c.n3), 256, 0, s>>>(
-              c.n3, c.P[q], c.P32[q]);
+          repitch_kernel<double, float><<<flat_grid(c.n3), 256, 0, s>>>(
+              c.d, c.d32, c.P[q], c.P32[q]);
           ++p->launches;
         }
       }
@@ -1391,8 +1569,8 @@ int pmg_build_hierarchy(pmg_problem *p, int trilinear) {
                                                         v.ops[q]);
       ++p->launches;
     }
-    const int init[8] = {INT_MAX, INT_MIN, INT_MAX, INT_MIN,
-                         INT_MAX, INT_MIN, 0,       0};
+    const int init[12] = {INT_MAX, INT_MIN, INT_MAX, INT_MIN, INT_MAX, INT_MIN,
+                          0,       0,       0,       0,       0,       0};
     PMG_CUDA_TRY(cudaMemcpyAsync(v.code_info, init, sizeof(init),
                                  cudaMemcpyHostToDevice, s));
     const dim3 ig = interior_grid(v.d), ib = interior_block();
@@ -1405,6 +1583,8 @@ int pmg_build_hierarchy(pmg_problem *p, int trilinear) {
     lut64_check_kernel<double><<<ig, ib, 0, s>>>(
         v.d, v.op[kOE], v.op[kON], v.op[kUC], v.code, v.lut64, v.code_info);
     p->launches += 4;
+    if ((rc = build_oc_codes(p, v)))
+      return rc;
     PMG_LAUNCH_CHECK();
   }
   // tile edge of the 27-point smoother, measured once per grid size (every
@@ -1414,12 +1594,14 @@ int pmg_build_hierarchy(pmg_problem *p, int trilinear) {
     LevelBuf &v = p->lv[L];
     const size_t n3 = (size_t)v.n3;
     if (p->precision == PMG_PREC_MIXED) {
-      if (L <= p->bottom_top || gs27_tile_known(v.d, 4) || !gs27_autotune_on())
+      if (L <= p->bottom_top || v.tma_ok || gs27_tile_known(v.d32, 4) ||
+          !gs27_autotune_on())
         continue;
-      if ((rc = gs27_tune<float>(v.d, v.A32(14), v.f32, v.x32, v.xalt32, s)))
+      if ((rc = gs27_tune<float>(v.d32, v.A32(14), v.f32, v.x32, v.xalt32,
+                                 s)))
         return rc;
-      PMG_CUDA_TRY(cudaMemsetAsync(v.x32, 0, sizeof(float) * n3, s));
-      PMG_CUDA_TRY(cudaMemsetAsync(v.xalt32, 0, sizeof(float) * n3, s));
+      PMG_CUDA_TRY(cudaMemsetAsync(v.x32, 0, sizeof(float) * v.n3_32, s));
+      PMG_CUDA_TRY(cudaMemsetAsync(v.xalt32, 0, sizeof(float) * v.n3_32, s));
     } else {
       if (gs27_tile_known(v.d, 8) || !gs27_autotune_on())
         continue;
@@ -1466,6 +1648,7 @@ int pmg_compute_residual_2(pmg_problem *p, double *out) {
 static int solve_host_loop(pmg_problem *p, double tol, int max_cycles,
                            int *cycles, double *relres, double *hist) {
   const bool refine = p->precision != PMG_PREC_FP64;
+  PMG_CUDA_TRY(cudaMemsetAsync(p->kernel_err, 0, sizeof(int), p->stream));
   int rc = refine ? refine_residual_async(p) : residual_norm_async(p);
   if (rc)
     return rc;
@@ -1508,6 +1691,14 @@ static int solve_host_loop(pmg_problem *p, double tol, int max_cycles,
     *cycles = c;
   if (relres)
     *relres = r0 > 0.0 ? r / r0 : 0.0;
+  int lost = 0;
+  PMG_CUDA_TRY(cudaMemcpy(&lost, p->kernel_err, sizeof(int),
+                          cudaMemcpyDeviceToHost));
+  if (rc == PMG_OK && lost) {
+    set_last_message("pmg_solve: a staged copy of the 27-point smoother did "
+                     "not arrive (bounded wait ran out)");
+    rc = PMG_ERR_TIMEOUT;
+  }
   return rc;
 }
 
@@ -1532,6 +1723,7 @@ int pmg_solve_start(pmg_problem *p, double tol, int max_cycles) {
   int rc = ensure_solve_graph(p);
   if (rc)
     return rc;
+  PMG_CUDA_TRY(cudaMemsetAsync(p->kernel_err, 0, sizeof(int), p->stream));
   solve_params_kernel<<<1, 1, 0, p->stream>>>(p->d_state, tol, max_cycles);
   PMG_LAUNCH_CHECK();
   PMG_CUDA_TRY(cudaGraphLaunch(p->solve_exec, p->stream));
@@ -1584,6 +1776,11 @@ int pmg_solve_finish(pmg_problem *p, int *cycles, double *relres,
   if (st.status == 1) {
     set_last_message("pmg_solve: residual diverged");
     return PMG_ERR_DIVERGED;
+  }
+  if (st.status == 3) {
+    set_last_message("pmg_solve: a staged copy of the 27-point smoother did "
+                     "not arrive (bounded wait ran out)");
+    return PMG_ERR_TIMEOUT;
   }
   return PMG_OK;
 }

@@ -314,14 +314,18 @@ __device__ __forceinline__ bool load_lut(const int *info, const float *,
 }
 __device__ __forceinline__ bool load_lut(const int *info, const double *lut64,
                                          CodeLut64 &L) {
-  if (info[6] != 0 || info[7] != 0)
+  const int2 f = *reinterpret_cast<const int2 *>(info + 6);
+  if (f.x != 0 || f.y != 0) // info[6], info[7]
     return false;
-  L.el = lut64[0];
-  L.eh = lut64[1];
-  L.nl = lut64[2];
-  L.nh = lut64[3];
-  L.ul = lut64[4];
-  L.uh = lut64[5];
+  const double2 e = *reinterpret_cast<const double2 *>(lut64);
+  const double2 n = *reinterpret_cast<const double2 *>(lut64 + 2);
+  const double2 u = *reinterpret_cast<const double2 *>(lut64 + 4);
+  L.el = e.x;
+  L.eh = e.y;
+  L.nl = n.x;
+  L.nh = n.y;
+  L.ul = u.x;
+  L.uh = u.y;
   return true;
 }
 template <typename T> struct LutOf {
@@ -330,6 +334,131 @@ template <typename T> struct LutOf {
 template <> struct LutOf<double> {
   using type = CodeLut64;
 };
+
+// ---- the centre coefficient of a coded level ----------------------------
+// The class's oC is the sum of a point's six couplings plus kappa^2 eps_out
+// outside the ion-exclusion spheres (PBE_pmgc_class.h:67-100, 283-313), so
+// for each six-bit coupling code it takes at most two values. Bit 6 of the
+// code byte says which; the passes then read oC from a 128-entry table
+// (index = the code's low seven bits) instead of an n^3 array. The table is
+// found on the device (per code: the least and the largest value), every
+// point's oC is checked against it bit for bit (info[8] |= 1 on a third
+// value), and the double table is rounded to float for the float passes,
+// whose oC is the double one rounded.
+__device__ __forceinline__ long long double_order(double v) {
+  const long long i = __double_as_longlong(v);
+  return i >= 0 ? i : i ^ 0x7fffffffffffffffLL;
+}
+__device__ __forceinline__ double order_double(long long i) {
+  return __longlong_as_double(i >= 0 ? i : i ^ 0x7fffffffffffffffLL);
+}
+
+// range[2c], range[2c + 1]: least and largest oC (ordered) of code c
+static __global__ void oc_range_init_kernel(long long *range) {
+  const int t = threadIdx.x;
+  if (t < 128)
+    range[t] = (t & 1) ? LLONG_MIN : LLONG_MAX;
+}
+
+// Each thread takes runs of kOcRun consecutive interior points of a row
+// and folds equal codes in registers (codes change only at the dielectric
+// and ion boundaries), then the block's table in shared memory, then one
+// global update per code and block.
+constexpr int kOcRun = 16;
+static __global__ void __launch_bounds__(256)
+    oc_range_kernel(Dims d, const double *__restrict__ oC,
+                    const unsigned char *__restrict__ code,
+                    long long *range) {
+  __shared__ long long sh[128];
+  for (int t = threadIdx.x; t < 128; t += blockDim.x)
+    sh[t] = (t & 1) ? LLONG_MIN : LLONG_MAX;
+  __syncthreads();
+  const Split sp = Split::of(d);
+  const int mx = d.nx - 2;
+  const int runs_per_row = (mx + kOcRun - 1) / kOcRun;
+  const long runs = (long)runs_per_row * (d.ny - 2) * (d.nz - 2);
+  for (long r = blockIdx.x * (long)blockDim.x + threadIdx.x; r < runs;
+       r += (long)gridDim.x * blockDim.x) {
+    const long row = r / runs_per_row;
+    const int i0 = 2 + (int)(r - row * runs_per_row) * kOcRun;
+    const int j = 2 + (int)(row % (d.ny - 2)), k = 2 + (int)(row / (d.ny - 2));
+    const int i1 = min(i0 + kOcRun - 1, d.nx - 1);
+    int cur = -1;
+    long long lo = LLONG_MAX, hi = LLONG_MIN;
+    for (int i = i0; i <= i1; ++i) {
+      const int c = code[sp.at(i, j, k)] & 63;
+      const long long v = double_order(oC[d.at(i, j, k)]);
+      if (c != cur) {
+        if (cur >= 0) {
+          atomicMin(&sh[2 * cur], lo);
+          atomicMax(&sh[2 * cur + 1], hi);
+        }
+        cur = c;
+        lo = hi = v;
+      } else {
+        lo = min(lo, v);
+        hi = max(hi, v);
+      }
+    }
+    if (cur >= 0) {
+      atomicMin(&sh[2 * cur], lo);
+      atomicMax(&sh[2 * cur + 1], hi);
+    }
+  }
+  __syncthreads();
+  for (int c = threadIdx.x; c < 64; c += blockDim.x)
+    if (sh[2 * c] != LLONG_MAX) {
+      atomicMin(&range[2 * c], sh[2 * c]);
+      atomicMax(&range[2 * c + 1], sh[2 * c + 1]);
+    }
+}
+
+inline unsigned oc_range_blocks(const Dims &d) {
+  const long runs = (long)((d.nx - 2 + kOcRun - 1) / kOcRun) * (d.ny - 2) *
+                    (d.nz - 2);
+  const long want = (runs + 255) / 256;
+  return (unsigned)(want < 148 * 4 ? want : 148 * 4);
+}
+
+// bit 6 of every interior code byte (oC is the code's larger value), and
+// info[8] |= 1 where oC is neither of the code's two values
+static __global__ void __launch_bounds__(256)
+    oc_code_kernel(Dims d, const double *__restrict__ oC,
+                   const long long *__restrict__ range, int *info,
+                   unsigned char *__restrict__ code) {
+  const Interior t = interior_point(d);
+  if (!t.ok)
+    return;
+  const int sidx = Split::of(d).at(t.i, t.j, t.k);
+  const unsigned b = code[sidx] & 63u;
+  const long long v = __double_as_longlong(oC[d.at(t.i, t.j, t.k)]);
+  const long long lo = __double_as_longlong(order_double(range[2 * b]));
+  const long long hi = __double_as_longlong(order_double(range[2 * b + 1]));
+  code[sidx] = (unsigned char)(b | (v == hi ? 64u : 0u));
+  if (v != lo && v != hi)
+    atomicOr(&info[8], 1);
+}
+
+// the tables: tab64[c + 64 bit] = the code's low (bit 0) or high (bit 1)
+// value, tab32 the same rounded to float; codes no point has read 0
+static __global__ void oc_table_kernel(const long long *__restrict__ range,
+                                double *tab64, float *tab32) {
+  const int t = threadIdx.x; // 128 threads: t = c + 64 bit
+  if (t >= 128)
+    return;
+  const int c = t & 63, bit = t >> 6;
+  const bool used = range[2 * c] != LLONG_MAX;
+  const double v = used ? order_double(range[2 * c + bit]) : 0.0;
+  tab64[t] = v;
+  if (tab32)
+    tab32[t] = (float)v;
+}
+
+// oC of a coded point: the table entry of the code's low seven bits
+template <typename T>
+__device__ __forceinline__ T oc_of(const T *tab, unsigned b) {
+  return tab[b & 127u];
+}
 
 // the six couplings of point p from the arrays (split layout)
 template <typename T> struct Couplings {
@@ -357,15 +486,16 @@ array_couplings(const T *oE, const T *oN, const T *uC, int p,
 // all their loads before computing, to keep enough bytes in flight.
 // (Issuing the x loads before the coding flag is read raised the float
 // kernel to 40 registers and 6 blocks per SM: 173 -> 186 us per four passes
-// at 257^3.)
+// at 257^3; with one point per thread, 32 registers, 178 us.)
 template <typename T, int PTS>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 8 : 4)
     gs7_code_color_kernel(Dims d, const T *__restrict__ oC,
                           const T *__restrict__ fc, const T *__restrict__ oE,
                           const T *__restrict__ oN, const T *__restrict__ uC,
                           const unsigned char *__restrict__ code,
                           const int *__restrict__ info,
-                          const T *__restrict__ lut, T *x, int want,
+                          const T *__restrict__ lut,
+                          const T *__restrict__ octab, T *x, int want,
                           T keep) {
   const Split sp = Split::of(d);
   const int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
@@ -389,6 +519,7 @@ __global__ void __launch_bounds__(256)
   }
   typename LutOf<T>::type L;
   const bool coded = load_lut(info, lut, L);
+  const bool oc_coded = coded && info[8] == 0;
   T s[PTS], f[PTS], c[PTS];
 #pragma unroll
   for (int r = 0; r < PTS; ++r) {
@@ -407,7 +538,7 @@ __global__ void __launch_bounds__(256)
     s[r] = cp.n * x[nb.n] + cp.s * x[nb.s] + cp.e * x[nb.e] +
            cp.w * x[nb.w] + cp.dn * x[nb.dn] + cp.u * x[nb.u];
     f[r] = fc[p[r]];
-    c[r] = oC[p[r]];
+    c[r] = oc_coded ? oc_of(octab, b[r]) : oC[p[r]];
   }
 #pragma unroll
   for (int r = 0; r < PTS; ++r)
@@ -421,8 +552,8 @@ constexpr int kCodePts = 2;
 template <typename T>
 int launch_gs7_code(const Dims &d, const T *oC, const T *fc, const T *oE,
                     const T *oN, const T *uC, const unsigned char *code,
-                    const int *info, const T *lut, T *x, int itmax,
-                    int iadjoint, int zero_init, cudaStream_t s) {
+                    const int *info, const T *lut, const T *octab, T *x,
+                    int itmax, int iadjoint, int zero_init, cudaStream_t s) {
   const dim3 g(cdiv(cdiv(d.nx - 2, 2), 32 * kCodePts), cdiv(d.ny - 2, 8),
                (unsigned)(d.nz - 2));
   for (int it = 0; it < itmax; ++it)
@@ -430,7 +561,7 @@ int launch_gs7_code(const Dims &d, const T *oC, const T *fc, const T *oE,
       const int want = (1 - iadjoint) * c + iadjoint * (1 - c);
       const T keep = zero_init ? T(0) : T(1);
       gs7_code_color_kernel<T, kCodePts><<<g, interior_block(), 0, s>>>(
-          d, oC, fc, oE, oN, uC, code, info, lut, x, want, keep);
+          d, oC, fc, oE, oN, uC, code, info, lut, octab, x, want, keep);
       zero_init = 0;
     }
   PMG_LAUNCH_CHECK();
@@ -447,7 +578,8 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 8 : 4)
                         const T *__restrict__ uC,
                         const unsigned char *__restrict__ code,
                         const int *__restrict__ info,
-                        const T *__restrict__ lut, const T *__restrict__ f,
+                        const T *__restrict__ lut,
+                        const T *__restrict__ octab, const T *__restrict__ f,
                         const T *__restrict__ x, T *__restrict__ r) {
   const int i0 = blockIdx.x * blockDim.x * 2 + threadIdx.x + 2;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
@@ -477,13 +609,14 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 8 : 4)
     xv[q][5] = x[nb.u];
     xv[q][6] = x[p[q]];
     fv[q] = f[p[q]];
-    cv[q] = oC[p[q]];
   }
   typename LutOf<T>::type L;
   const bool coded = load_lut(info, lut, L);
+  const bool oc_coded = coded && info[8] == 0;
   T out[2];
 #pragma unroll
   for (int q = 0; q < 2; ++q) {
+    cv[q] = oc_coded ? oc_of(octab, b[q]) : oC[p[q]];
     Couplings<T> c;
     if (coded) {
       c.e = (b[q] & 1u) ? L.eh : L.el;
@@ -571,11 +704,12 @@ __global__ void __launch_bounds__(256)
 // squares) with the double couplings from the code bytes when both codings
 // hold: the same values, the same order, the same bits.
 template <typename T, typename R>
-__global__ void __launch_bounds__(kReduceThreads)
+__global__ void __launch_bounds__(kReduceThreads, 6)
     defect_norm_code_kernel(Dims d, Op14<T> A, const T *__restrict__ f,
                             const T *__restrict__ x,
                             const unsigned char *__restrict__ code,
                             const T *__restrict__ lut64,
+                            const T *__restrict__ octab,
                             const int *__restrict__ info,
                             R *__restrict__ r, ReduceSlot s) {
   __shared__ double sh[32];
@@ -585,6 +719,7 @@ __global__ void __launch_bounds__(kReduceThreads)
   const int k1 = min(k0 + kReducePlanes - 1, d.nz - 1);
   const int sy = d.sy(), sz = d.sz();
   const bool coded = info[6] == 0 && info[7] == 0;
+  const bool oc_coded = coded && info[8] == 0;
   // low / high double value per direction, in registers (selected below,
   // never indexed at run time)
   const T el = coded ? lut64[0] : T(0), eh = coded ? lut64[1] : T(0);
@@ -603,8 +738,10 @@ __global__ void __launch_bounds__(kReduceThreads)
       const int p = d.at(i, j, k);
       const int sidx = sp.at(i, j, k);
       T c[6];
+      T oc;
       if (coded) {
         const unsigned b = code[sidx];
+        oc = oc_coded ? oc_of(octab, b) : A.a[kOC][p];
         c[0] = (b & 1u) ? eh : el;
         c[1] = (b & 2u) ? eh : el;
         c[2] = (b & 4u) ? nh : nl;
@@ -613,12 +750,13 @@ __global__ void __launch_bounds__(kReduceThreads)
         c[5] = (b & 32u) ? uh : ul;
       } else {
         couplings64_of(d, A.a[kOE], A.a[kON], A.a[kUC], p, c);
+        oc = A.a[kOC][p];
       }
       // apply7's order: -oN x_n - oN_s x_s - oE x_e - oE_w x_w - uC_d x_d
       // - uC x_u + (oC + 0) x
       const T ax = -c[2] * x[p + sy] - c[3] * x[p - sy] - c[0] * x[p + 1] -
                    c[1] * x[p - 1] - c[5] * x[p - sz] - c[4] * x[p + sz] +
-                   (A.a[kOC][p] + T(0)) * x[p];
+                   (oc + T(0)) * x[p];
       const T dv = f[p] - ax;
       r[sidx] = (R)dv;
       acc += (double)dv * (double)dv;

@@ -329,6 +329,21 @@ __global__ void convert_kernel(long n, const Tin *__restrict__ src,
     dst[q] = (Tout)src[q];
 }
 
+// dst (rows dd.px apart) = (Tout) src (rows ds.px apart), every point of
+// the grid (shell included); the two Dims differ only in their pitch
+template <typename Tin, typename Tout>
+__global__ void repitch_kernel(Dims ds, Dims dd, const Tin *__restrict__ src,
+                               Tout *__restrict__ dst) {
+  const long n = (long)ds.nx * ds.ny * ds.nz;
+  for (long g = blockIdx.x * (long)blockDim.x + threadIdx.x; g < n;
+       g += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(g % ds.nx) + 1;
+    const long r = g / ds.nx;
+    const int j = (int)(r % ds.ny) + 1, k = (int)(r / ds.ny) + 1;
+    dst[dd.at(i, j, k)] = (Tout)src[ds.at(i, j, k)];
+  }
+}
+
 // x64 += (double)e32 on the interior (mixed-precision refinement update).
 __global__ void add_correction_kernel(Dims d, double *__restrict__ x,
                                       const float *__restrict__ e);

@@ -52,6 +52,13 @@ def kappa(physics: dict) -> tuple[float, float]:
     return k.value, e.value
 
 
+def set_tma_staging(on: bool) -> None:
+    """Problems created afterwards stage the mixed path's 27-point smoother
+    tiles by tensor-memory access (default) or load per point (the same
+    bits; pmg_set_tma_staging)."""
+    _lib.check("pmg_set_tma_staging", _lib.lib.pmg_set_tma_staging(int(on)))
+
+
 @dataclasses.dataclass
 class SolveResult:
     cycles: int

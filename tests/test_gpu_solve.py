@@ -323,10 +323,12 @@ def test_coded_couplings_give_the_same_bits(pb65, precision):
     operator with more values per direction is not coded and solves the
     same with the switch on or off; so does one whose double couplings take
     a third value that rounds to a float table value (coded for the float
-    passes of the mixed path, not for fp64-fast)."""
+    passes of the mixed path, not for fp64-fast), and one whose centre
+    coefficient takes a third value for some coupling code (couplings coded,
+    oC read from its array)."""
     w, fine = pb65
     out = {}
-    for case in ("class", "random", "ulp"):
+    for case in ("class", "random", "ulp", "oc3"):
         f = dict(fine)
         rng = np.random.default_rng(1)
         oE = np.array(f["oE"], copy=True)
@@ -336,6 +338,10 @@ def test_coded_couplings_give_the_same_bits(pb65, precision):
             flat[pick] = flat[pick] * 1.01
         elif case == "ulp":  # a third double, the same float
             flat[pick] = np.nextafter(flat[pick], np.inf)
+        elif case == "oc3":  # oC off its code's two values at a few points
+            oC = np.array(f["oC"], copy=True).reshape(w.n, w.n, w.n)
+            oC[w.n // 2, w.n // 2, 5:9] *= 1.0001
+            f["oC"] = oC.reshape(-1)
         f["oE"] = oE
         for on in (True, False):
             with PBELinearProblem(w.base, w.nlev, w.box, precision,
@@ -349,7 +355,8 @@ def test_coded_couplings_give_the_same_bits(pb65, precision):
     assert out["class", True][0] and not out["class", False][0]
     assert not out["random", True][0]
     assert out["ulp", True][0] == (precision == "mixed")
-    for case in ("class", "random", "ulp"):
+    assert out["oc3", True][0]
+    for case in ("class", "random", "ulp", "oc3"):
         assert out[case, True][1] == out[case, False][1]
         assert np.array_equal(out[case, True][2], out[case, False][2])
 
@@ -419,3 +426,28 @@ def test_mixed_lowest_levels_shapes(base, nlev, throughput):
             out[prec] = p.potential().ravel().copy()
     x0, x1 = out["fp64"], out["mixed"]
     assert np.linalg.norm(x1 - x0) <= 1e-8 * np.linalg.norm(x0)
+
+
+@pytest.mark.parametrize("name", ["pb65", "pb161"])
+def test_tma_staged_smoother_gives_the_same_bits(name):
+    """The mixed path's 27-point smoother with each tile staged by
+    tensor-memory access (padded float levels: 33^3 of pb65; 21^3, 41^3,
+    81^3 of pb161) against the per-point-load kernel: the same cycles and
+    the same potential, bit for bit."""
+    from multigrid_b200.problem import set_tma_staging
+    w = WORKLOADS[name]
+    fine = setup_fine(w.n, w.h, w.atoms(), w.physics)
+    out = {}
+    try:
+        for tma in (True, False):
+            set_tma_staging(tma)
+            with PBELinearProblem(w.base, w.nlev, w.box, "mixed",
+                                  w.physics) as p:
+                p.set_fine(**fine)
+                p.buildmultilevelops()
+                r = p.solve(tol=1e-10, max_cycles=100)
+                out[tma] = (r.cycles, p.potential().ravel().copy())
+    finally:
+        set_tma_staging(True)
+    assert out[True][0] == out[False][0]
+    assert np.array_equal(out[True][1], out[False][1])

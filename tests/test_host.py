@@ -231,8 +231,9 @@ def test_dx_writer_format(tmp_path):
 def test_bench_phase_accounting():
     """bench.py's algorithmic bytes and kernel names per cycle phase: the
     coupling arrays (28 B per point and sweep in float, 7 arrays) or, with
-    coded couplings, oC + code byte + f + x read and written (17 B); the
-    refinement residual 52 B or 29 B per point."""
+    the operator coded (couplings and oC in one byte), code byte + f + x
+    read and written (13 B); the refinement residual 52 B or 21 B per
+    point."""
     import importlib
     import sys
     sys.path.insert(0, os.path.dirname(os.path.dirname(
@@ -245,10 +246,10 @@ def test_bench_phase_accounting():
     p = P()
     n3 = 257.0 ** 3
     assert bench.phase_bytes(p, 7, "pre-smooth", 4) == 2 * 7 * 4 * n3
-    assert bench.phase_bytes(p, 7, "pre-smooth", 4, True) == 2 * 17 * n3
-    assert bench.phase_bytes(p, 7, "defect", 4, True) == 17 * n3
+    assert bench.phase_bytes(p, 7, "pre-smooth", 4, True) == 2 * 13 * n3
+    assert bench.phase_bytes(p, 7, "defect", 4, True) == 13 * n3
     assert bench.phase_bytes(p, 0, "residual", 4) == 52 * n3
-    assert bench.phase_bytes(p, 0, "residual", 4, True) == 29 * n3
+    assert bench.phase_bytes(p, 0, "residual", 4, True) == 21 * n3
     assert bench.phase_kernel(p, 7, "pre-smooth", True)[0] == \
         "gs7_code_color_kernel"
     assert bench.phase_kernel(p, 7, "pre-smooth")[0] == \
@@ -256,7 +257,9 @@ def test_bench_phase_accounting():
     assert bench.phase_kernel(p, 0, "residual", True)[0] == \
         "defect_norm_code_kernel"
     assert bench.phase_kernel(p, 6, "pre-smooth", True)[0] == \
-        "gs27_phase_kernel"
+        "gs27_tma_kernel"
+    p.precision = "fp64"
+    assert bench.phase_kernel(p, 4, "pre-smooth")[0] == "gs27_phase_kernel"
 
 
 def test_c_header_compiles_as_c99(tmp_path):
