@@ -737,6 +737,10 @@ __global__ void __launch_bounds__(kReduceThreads, 6)
         break;
       const int p = d.at(i, j, k);
       const int sidx = sp.at(i, j, k);
+      // the loads that do not depend on the code byte first, so a plane
+      // costs one memory round trip
+      const T xn = x[p + sy], xs = x[p - sy], xe = x[p + 1], xw = x[p - 1];
+      const T xd = x[p - sz], xu = x[p + sz], xc = x[p], fv = f[p];
       T c[6];
       T oc;
       if (coded) {
@@ -754,10 +758,9 @@ __global__ void __launch_bounds__(kReduceThreads, 6)
       }
       // apply7's order: -oN x_n - oN_s x_s - oE x_e - oE_w x_w - uC_d x_d
       // - uC x_u + (oC + 0) x
-      const T ax = -c[2] * x[p + sy] - c[3] * x[p - sy] - c[0] * x[p + 1] -
-                   c[1] * x[p - 1] - c[5] * x[p - sz] - c[4] * x[p + sz] +
-                   (oc + T(0)) * x[p];
-      const T dv = f[p] - ax;
+      const T ax = -c[2] * xn - c[3] * xs - c[0] * xe - c[1] * xw -
+                   c[5] * xd - c[4] * xu + (oc + T(0)) * xc;
+      const T dv = fv - ax;
       r[sidx] = (R)dv;
       acc += (double)dv * (double)dv;
     }
