@@ -428,12 +428,13 @@ def test_mixed_lowest_levels_shapes(base, nlev, throughput):
     assert np.linalg.norm(x1 - x0) <= 1e-8 * np.linalg.norm(x0)
 
 
-@pytest.mark.parametrize("name", ["pb65", "pb161"])
+@pytest.mark.parametrize("name", ["pb65", "pb161", "pb257"])
 def test_tma_staged_smoother_gives_the_same_bits(name):
     """The mixed path's 27-point smoother with each tile staged by
-    tensor-memory access (padded float levels: 33^3 of pb65; 21^3, 41^3,
-    81^3 of pb161) against the per-point-load kernel: the same cycles and
-    the same potential, bit for bit."""
+    tensor-memory access (padded float levels, tile edges by size: 33^3 of
+    pb65; 21^3, 41^3, 81^3 of pb161; 33^3, 65^3, 129^3 of pb257) against the
+    per-point-load kernel: the same cycles and the same potential, bit for
+    bit."""
     from multigrid_b200.problem import set_tma_staging
     w = WORKLOADS[name]
     fine = setup_fine(w.n, w.h, w.atoms(), w.physics)
