@@ -4,7 +4,7 @@
 // one-launch bottom levels and the finest level.
 //
 // The sweep is gs27_tiled.cuh's: one launch per plane parity, one CTA per
-// 32 x 32 tile of a plane, four sub-colour steps with a recomputed halo of
+// TT x TT tile of a plane (TT 32, 16 or 8 by the level's size, as there), four sub-colour steps with a recomputed halo of
 // 3 - t points in step t, ping-pong buffers and the reference's per-point
 // arithmetic (sums27 order), so the bits are the same. The x planes k - 1,
 // k, k + 1 over the tile and its halo arrive as three tensor-map boxes on
@@ -24,7 +24,8 @@
 // at the 16-byte boundary at or below the tile's halo (x coordinate
 // 32 bx - 4, a multiple of four floats); coordinates before the array or
 // past its last point (the map's extent is nx, not px) read as zero, which
-// no update uses.
+// no update uses. A box is (TT + 12) x (TT + 8) floats, so the tensor maps
+// of a level are made for its tile edge.
 #pragma once
 
 #include <cuda.h>
@@ -33,12 +34,12 @@
 
 namespace pmg {
 
-constexpr int kTmaTT = 32;
-constexpr int kTmaThreads = Gs27Tile<kTmaTT>::THREADS;
-constexpr int kTmaBX = kTmaTT + 12; // 44 floats = 176 bytes per box row
-constexpr int kTmaBY = kTmaTT + 8;
-constexpr int kTmaBox = kTmaBX * kTmaBY; // floats per box
-constexpr unsigned kTmaStageBytes = 3 * kTmaBox * sizeof(float);
+// box of a TT x TT tile: rows of TT + 12 floats (a 16-byte multiple, from
+// the 16-byte boundary below the halo), TT + 8 rows
+template <int TT> struct TmaBox {
+  static constexpr int BX = TT + 12, BY = TT + 8, SIZE = BX * BY;
+  static constexpr unsigned BYTES = 3 * SIZE * sizeof(float); // 3 planes
+};
 // mbarrier polls before the stage counts as lost (far above any real wait)
 constexpr long kTmaMaxPolls = 1L << 24;
 
@@ -105,16 +106,19 @@ __device__ __forceinline__ void fence_mbar_init() {
   asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
 }
 
-// One plane-parity phase on 32 x 32 tiles (gs27_phase_kernel with the x
+// One plane-parity phase on TT x TT tiles (gs27_phase_kernel with the x
 // planes staged by three tensor-map boxes). err: set to 1 when the stage
 // did not arrive within the bounded wait (the block then waits once more,
 // also bounded, for its copies and returns).
-__global__ void __launch_bounds__(kTmaThreads, 8)
+template <int TT>
+__global__ void __launch_bounds__(Gs27Tile<TT>::THREADS, 2048 /
+                                  Gs27Tile<TT>::THREADS)
     gs27_tma_kernel(const __grid_constant__ Gs27TmaMaps maps, Dims d,
                     Op14<float> A, const float *__restrict__ fc, float *out,
                     int kfirst, int order, int *err) {
-  constexpr int W = kTmaBX, TT = kTmaTT, NT = kTmaThreads;
-  __shared__ __align__(128) float xs[3 * kTmaBox];
+  constexpr int W = TmaBox<TT>::BX, NT = Gs27Tile<TT>::THREADS;
+  constexpr int kBox = TmaBox<TT>::SIZE;
+  __shared__ __align__(128) float xs[3 * kBox];
   __shared__ uint64_t bar;
   const int ti0 = 2 + blockIdx.x * TT, tj0 = 2 + blockIdx.y * TT;
   const int k = kfirst + 2 * blockIdx.z;
@@ -127,10 +131,10 @@ __global__ void __launch_bounds__(kTmaThreads, 8)
     // box origin (0-based): x at the 16-byte boundary ti0 - 6, y five rows
     // above the tile (the 4-point halo starts at tj0 - 4, 1-based)
     const int cx = ti0 - 6, cy = tj0 - 5, z = k - 1;
-    mbar_expect_tx(&bar, kTmaStageBytes);
+    mbar_expect_tx(&bar, TmaBox<TT>::BYTES);
     tma_load_3d(xs, &maps.nb, cx, cy, z - 1, &bar);
-    tma_load_3d(xs + kTmaBox, &maps.own, cx, cy, z, &bar);
-    tma_load_3d(xs + 2 * kTmaBox, &maps.nb, cx, cy, z + 1, &bar);
+    tma_load_3d(xs + kBox, &maps.own, cx, cy, z, &bar);
+    tma_load_3d(xs + 2 * kBox, &maps.nb, cx, cy, z + 1, &bar);
   }
   const bool ok = mbar_wait(&bar, 0);
   if (__syncthreads_or(!ok)) {
@@ -142,14 +146,18 @@ __global__ void __launch_bounds__(kTmaThreads, 8)
   }
   // box column c holds 1-based i = ti0 - 5 + c, row r holds j = tj0 - 4 + r;
   // gs27_step_at's origin is (ti0 - 4, tj0 - 4): one column on
-  float *xc = xs + kTmaBox + 1;
-  gs27_step_at<float, TT, W, kTmaBox, 3>(d, A, nullptr, fc, xc, ti0, tj0, k, order);
+  float *xc = xs + kBox + 1;
+  gs27_step_at<float, TT, W, kBox, 3>(d, A, nullptr, fc, xc, ti0, tj0, k,
+                                      order);
   __syncthreads();
-  gs27_step_at<float, TT, W, kTmaBox, 2>(d, A, nullptr, fc, xc, ti0, tj0, k, order);
+  gs27_step_at<float, TT, W, kBox, 2>(d, A, nullptr, fc, xc, ti0, tj0, k,
+                                      order);
   __syncthreads();
-  gs27_step_at<float, TT, W, kTmaBox, 1>(d, A, nullptr, fc, xc, ti0, tj0, k, order);
+  gs27_step_at<float, TT, W, kBox, 1>(d, A, nullptr, fc, xc, ti0, tj0, k,
+                                      order);
   __syncthreads();
-  gs27_step_at<float, TT, W, kTmaBox, 0>(d, A, nullptr, fc, xc, ti0, tj0, k, order);
+  gs27_step_at<float, TT, W, kBox, 0>(d, A, nullptr, fc, xc, ti0, tj0, k,
+                                      order);
   __syncthreads();
   const int i_max = d.nx - 1, j_max = d.ny - 1;
 #pragma unroll

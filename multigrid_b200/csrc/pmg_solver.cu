@@ -44,6 +44,7 @@ struct LevelBuf {
     CUtensorMap x, xalt;
   } tma;
   bool tma_ok = false;
+  int tma_tile = 0; // the tile edge the maps' boxes are made for
   double *op[14] = {};
   double *P[27] = {}; // prolongation from this level to level+1
   double *x = nullptr, *f = nullptr, *r = nullptr;
@@ -507,9 +508,10 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 }
 
 // A 3-D map of one padded float array of the level: extent nx x ny x nz
-// (the padding reads as outside), rows px apart, boxes of
-// kTmaBX x kTmaBY x 1.
-bool encode_level_map(CUtensorMap *m, const float *base, const Dims &d) {
+// (the padding reads as outside), rows px apart, boxes of a tt x tt tile
+// (TmaBox).
+bool encode_level_map(CUtensorMap *m, const float *base, const Dims &d,
+                      int tt) {
   auto enc = tensor_map_encoder();
   if (!enc || !base || (d.px * sizeof(float)) % 16 != 0)
     return false;
@@ -517,7 +519,7 @@ bool encode_level_map(CUtensorMap *m, const float *base, const Dims &d) {
                               (cuuint64_t)d.nz};
   const cuuint64_t strides[2] = {(cuuint64_t)d.px * sizeof(float),
                                  (cuuint64_t)d.px * d.ny * sizeof(float)};
-  const cuuint32_t box[3] = {kTmaBX, kTmaBY, 1};
+  const cuuint32_t box[3] = {(cuuint32_t)tt + 12, (cuuint32_t)tt + 8, 1};
   const cuuint32_t elem[3] = {1, 1, 1};
   return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void *)base, dims,
              strides, box, elem, CU_TENSOR_MAP_INTERLEAVE_NONE,
@@ -533,8 +535,10 @@ void encode_tma_maps(pmg_problem *p) {
     v.tma_ok = false;
     if (v.d32.px == v.d.px || !v.xalt32 || v.d32.nx - 2 < 1)
       continue;
-    bool ok = encode_level_map(&v.tma.x, v.x32, v.d32);
-    ok = ok && encode_level_map(&v.tma.xalt, v.xalt32, v.d32);
+    // the size rule's tile edge (gs27_tiled.cuh)
+    v.tma_tile = gs27_tile_by_size(v.d32);
+    bool ok = encode_level_map(&v.tma.x, v.x32, v.d32, v.tma_tile);
+    ok = ok && encode_level_map(&v.tma.xalt, v.xalt32, v.d32, v.tma_tile);
     v.tma_ok = ok;
   }
 }
@@ -548,7 +552,8 @@ int launch_gs27_tma(pmg_problem *p, LevelBuf &v, int nsweeps, int zero_init,
   if (zero_init)
     PMG_CUDA_TRY(cudaMemsetAsync(*cur, 0, sizeof(float) * v.n3_32, s));
   const int order = 0 | 1 << 2 | 2 << 4 | 3 << 6;
-  const unsigned tx = cdiv(d.nx - 2, kTmaTT), ty = cdiv(d.ny - 2, kTmaTT);
+  const int tt = v.tma_tile;
+  const unsigned tx = cdiv(d.nx - 2, tt), ty = cdiv(d.ny - 2, tt);
   const Op14<float> A = v.A32(14);
   float *c = *cur;
   float *a = c == v.x32 ? v.xalt32 : v.x32;
@@ -563,8 +568,16 @@ int launch_gs27_tma(pmg_problem *p, LevelBuf &v, int nsweeps, int zero_init,
       Gs27TmaMaps m;
       m.own = mc;
       m.nb = ph == 0 ? mc : ma;
-      gs27_tma_kernel<<<dim3(tx, ty, (unsigned)planes), kTmaThreads, 0, s>>>(
-          m, d, A, v.f32, a, kfirst, order, p->kernel_err);
+      const dim3 g(tx, ty, (unsigned)planes);
+      if (tt == 32)
+        gs27_tma_kernel<32><<<g, Gs27Tile<32>::THREADS, 0, s>>>(
+            m, d, A, v.f32, a, kfirst, order, p->kernel_err);
+      else if (tt == 16)
+        gs27_tma_kernel<16><<<g, Gs27Tile<16>::THREADS, 0, s>>>(
+            m, d, A, v.f32, a, kfirst, order, p->kernel_err);
+      else
+        gs27_tma_kernel<8><<<g, Gs27Tile<8>::THREADS, 0, s>>>(
+            m, d, A, v.f32, a, kfirst, order, p->kernel_err);
     }
     std::swap(c, a);
   }
