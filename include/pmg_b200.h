@@ -535,6 +535,15 @@ typedef enum {
  * give the same bits. No counterpart in the reference. */
 int pmg_set_tma_staging(int on);
 
+/* For testing the staged smoother's error path: every tensor-memory-access
+ * stage of solves launched or captured afterwards waits for `bytes` more
+ * than its boxes deliver (a multiple of 16, 0 restores the normal count),
+ * so each bounded wait runs out (about 0.1 s), the kernel records the lost
+ * stage and returns, and the solve reports PMG_ERR_TIMEOUT with the context
+ * still usable. A captured solve graph keeps the value it was captured
+ * with: use new problems on both sides of the switch. */
+int pmg_test_tma_short_delivery(int bytes);
+
 /* Creates a problem on the current CUDA device; allocates its hierarchy.
  * stream may be NULL (a private stream is created). */
 int pmg_problem_create(int base, int nlev, double box, int precision,

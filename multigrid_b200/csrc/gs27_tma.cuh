@@ -40,8 +40,9 @@ template <int TT> struct TmaBox {
   static constexpr int BX = TT + 12, BY = TT + 8, SIZE = BX * BY;
   static constexpr unsigned BYTES = 3 * SIZE * sizeof(float); // 3 planes
 };
-// mbarrier polls before the stage counts as lost (far above any real wait)
-constexpr long kTmaMaxPolls = 1L << 24;
+// mbarrier polls before the stage counts as lost: about 0.1 s, some 10^4
+// times the longest real wait
+constexpr long kTmaMaxPolls = 1L << 20;
 
 // Tensor maps of the two iterate buffers in the roles of the launch.
 struct alignas(64) Gs27TmaMaps {
@@ -109,13 +110,14 @@ __device__ __forceinline__ void fence_mbar_init() {
 // One plane-parity phase on TT x TT tiles (gs27_phase_kernel with the x
 // planes staged by three tensor-map boxes). err: set to 1 when the stage
 // did not arrive within the bounded wait (the block then waits once more,
-// also bounded, for its copies and returns).
+// also bounded, for its copies and returns). extra_tx: bytes expected on
+// top of the boxes' (0; a test sets it so that every wait runs out).
 template <int TT>
 __global__ void __launch_bounds__(Gs27Tile<TT>::THREADS, 2048 /
                                   Gs27Tile<TT>::THREADS)
     gs27_tma_kernel(const __grid_constant__ Gs27TmaMaps maps, Dims d,
                     Op14<float> A, const float *__restrict__ fc, float *out,
-                    int kfirst, int order, int *err) {
+                    int kfirst, int order, int *err, unsigned extra_tx) {
   constexpr int W = TmaBox<TT>::BX, NT = Gs27Tile<TT>::THREADS;
   constexpr int kBox = TmaBox<TT>::SIZE;
   __shared__ __align__(128) float xs[3 * kBox];
@@ -131,7 +133,7 @@ __global__ void __launch_bounds__(Gs27Tile<TT>::THREADS, 2048 /
     // box origin (0-based): x at the 16-byte boundary ti0 - 6, y five rows
     // above the tile (the 4-point halo starts at tj0 - 4, 1-based)
     const int cx = ti0 - 6, cy = tj0 - 5, z = k - 1;
-    mbar_expect_tx(&bar, TmaBox<TT>::BYTES);
+    mbar_expect_tx(&bar, TmaBox<TT>::BYTES + extra_tx);
     tma_load_3d(xs, &maps.nb, cx, cy, z - 1, &bar);
     tma_load_3d(xs + kBox, &maps.own, cx, cy, z, &bar);
     tma_load_3d(xs + 2 * kBox, &maps.nb, cx, cy, z + 1, &bar);

@@ -492,6 +492,8 @@ double norm_from_sum(const pmg_problem *p, double s) {
 // on every level (the same bits)
 std::atomic<int> g_tma_on{1};
 bool tma_disabled() { return g_tma_on.load() == 0; }
+// pmg_test_tma_short_delivery: extra bytes every stage waits for
+std::atomic<unsigned> g_tma_extra_tx{0};
 
 PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
@@ -569,15 +571,16 @@ int launch_gs27_tma(pmg_problem *p, LevelBuf &v, int nsweeps, int zero_init,
       m.own = mc;
       m.nb = ph == 0 ? mc : ma;
       const dim3 g(tx, ty, (unsigned)planes);
+      const unsigned xt = g_tma_extra_tx.load();
       if (tt == 32)
         gs27_tma_kernel<32><<<g, Gs27Tile<32>::THREADS, 0, s>>>(
-            m, d, A, v.f32, a, kfirst, order, p->kernel_err);
+            m, d, A, v.f32, a, kfirst, order, p->kernel_err, xt);
       else if (tt == 16)
         gs27_tma_kernel<16><<<g, Gs27Tile<16>::THREADS, 0, s>>>(
-            m, d, A, v.f32, a, kfirst, order, p->kernel_err);
+            m, d, A, v.f32, a, kfirst, order, p->kernel_err, xt);
       else
         gs27_tma_kernel<8><<<g, Gs27Tile<8>::THREADS, 0, s>>>(
-            m, d, A, v.f32, a, kfirst, order, p->kernel_err);
+            m, d, A, v.f32, a, kfirst, order, p->kernel_err, xt);
     }
     std::swap(c, a);
   }
@@ -1373,6 +1376,16 @@ int pmg_problem_set_coarse_rtol(pmg_problem *p, double rtol) {
 
 int pmg_set_tma_staging(int on) {
   g_tma_on.store(on != 0);
+  return PMG_OK;
+}
+
+int pmg_test_tma_short_delivery(int bytes) {
+  if (bytes < 0 || bytes % 16 != 0 || bytes > (1 << 20)) {
+    set_last_message("pmg_test_tma_short_delivery: bytes must be a multiple "
+                     "of 16 in [0, 2^20]");
+    return PMG_ERR_ARG;
+  }
+  g_tma_extra_tx.store((unsigned)bytes);
   return PMG_OK;
 }
 

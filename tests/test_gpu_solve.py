@@ -452,3 +452,36 @@ def test_tma_staged_smoother_gives_the_same_bits(name):
         set_tma_staging(True)
     assert out[True][0] == out[False][0]
     assert np.array_equal(out[True][1], out[False][1])
+
+
+def test_tma_stage_wait_runs_out_and_reports(pb65):
+    """The staged smoother's waits are bounded: with every stage expecting
+    16 bytes more than its boxes deliver (pmg_test_tma_short_delivery), each
+    wait runs out, the kernel records it and returns, and the solve reports
+    PMG_ERR_TIMEOUT; a new problem afterwards solves normally on the same
+    context, bit for bit as before."""
+    from multigrid_b200 import _lib
+    w, fine = pb65
+
+    def solve():
+        with PBELinearProblem(w.base, w.nlev, w.box, "mixed",
+                              w.physics) as p:
+            p.set_fine(**fine)
+            p.buildmultilevelops()
+            r = p.solve(tol=1e-10, max_cycles=100)
+            return r.cycles, p.potential().ravel().copy()
+
+    before = solve()
+    _lib.check("pmg_test_tma_short_delivery",
+               _lib.lib.pmg_test_tma_short_delivery(16))
+    try:
+        with pytest.raises(PmgError) as e:
+            solve()
+        assert e.value.status == _lib.PMG_ERR_TIMEOUT
+        assert b"did not arrive" in _lib.lib.pmg_last_error()
+    finally:
+        _lib.check("pmg_test_tma_short_delivery",
+                   _lib.lib.pmg_test_tma_short_delivery(0))
+    after = solve()
+    assert after[0] == before[0]
+    assert np.array_equal(after[1], before[1])
