@@ -155,13 +155,22 @@ def barrier(world):
 
 
 def max_over_ranks(world, value: float) -> float:
+    """The slowest rank's time (every rank gets it): the job is done when
+    the last replica is."""
     if world == 1:
         return value
     import torch
     import torch.distributed as dist
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def replicas_value(world: int, steps: int, ms: float) -> float:
+    """Whole-job solves/s of `world` independent replicas that each ran
+    `steps` solves, the slowest in `ms` milliseconds."""
+    return world * steps / (ms / 1000.0)
 
 
 # ---------------------------------------------------------------------------
@@ -731,7 +740,7 @@ def main():
                                   launches=launches, build_ms=build_ms)
 
     prim = results[args.precision]
-    value = world * args.steps / (prim["ms"] / 1000.0)
+    value = replicas_value(world, args.steps, prim["ms"])
     if args.quick:
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT,
