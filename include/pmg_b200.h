@@ -535,6 +535,16 @@ typedef enum {
  * give the same bits. No counterpart in the reference. */
 int pmg_set_tma_staging(int on);
 
+/* The refinement paths' finest red-black colour passes stream the level's
+ * rows through shared memory: per plane, one bulk copy per row of the other
+ * colour's iterate and of the own colour's right-hand side and code bytes,
+ * into a ring of stages, so the bytes in flight are set by the ring and not
+ * by registers. on = 0 makes problems created afterwards use the
+ * per-point-load pass instead; both give the same bits. No counterpart in
+ * the reference (Vgsrb7x, pmgc/gsd.cc:61-111, is the arithmetic of both).
+ * A lost stage is reported like the staged 27-point smoother's. */
+int pmg_set_finest_streaming(int on);
+
 /* For testing the staged smoother's error path: every tensor-memory-access
  * stage of solves launched or captured afterwards waits for `bytes` more
  * than its boxes deliver (a multiple of 16, 0 restores the normal count),

@@ -122,6 +122,7 @@ _sig("pmg_pcg_solve", c_int, _V, c_double, c_int, PI, PD, PD)
 _sig("pmg_problem_set_host_loop", c_int, _V, c_int)
 _sig("pmg_set_autotune", c_int, c_int)
 _sig("pmg_set_tma_staging", c_int, c_int)
+_sig("pmg_set_finest_streaming", c_int, c_int)
 _sig("pmg_test_tma_short_delivery", c_int, c_int)
 _sig("pmg_problem_set_coded_couplings", c_int, _V, c_int)
 _sig("pmg_problem_coded_couplings", c_int, _V, PI)

@@ -15,6 +15,7 @@
 #include "bottom_cycle.cuh"
 #include "gs27_tiled.cuh"
 #include "gs27_tma.cuh"
+#include "gs7_stream.cuh"
 
 #include <cudaTypedefs.h>
 #include "launch.cuh"
@@ -45,6 +46,9 @@ struct LevelBuf {
   } tma;
   bool tma_ok = false;
   int tma_tile = 0; // the tile edge the maps' boxes are made for
+  // the refinement paths' finest level: tensor maps of the colour-split
+  // correction, right-hand side and code bytes (the streamed colour pass)
+  StreamMaps smaps;
   double *op[14] = {};
   double *P[27] = {}; // prolongation from this level to level+1
   double *x = nullptr, *f = nullptr, *r = nullptr;
@@ -151,7 +155,7 @@ struct SolveState {
   int max_cycles;
   int cycles;
   // 0 running / converged / capped, 1 diverged, 2 r0 not finite, 3 a
-  // staged copy of the 27-point smoother did not arrive
+  // staged copy (27-point smoother, streamed finest pass) did not arrive
   int status;
   int pad;
   double r0, r;
@@ -173,7 +177,8 @@ struct pmg_problem {
   LevelBuf lv[kMaxLevels + 1];
   double *cg_r = nullptr, *cg_p = nullptr, *cg_ap = nullptr;
   int *cg_status = nullptr;
-  int *kernel_err = nullptr; // device: set by gs27_tma_kernel on a lost stage
+  // device: set by gs27_tma_kernel and gs7_stream_kernel on a lost stage
+  int *kernel_err = nullptr;
   int num_sms = 0;
   // Relative stopping threshold of the coarsest CG on the mixed path's
   // correction equation (the FP64 path keeps the class's absolute 1e-8).
@@ -198,6 +203,9 @@ struct pmg_problem {
   bool host_loop = false; // pmg_problem_set_host_loop
   bool throughput = false; // pmg_problem_set_throughput_mode
   bool use_codes = true;   // pmg_problem_set_coded_couplings
+  // the finest colour passes stream their rows through shared memory
+  // (gs7_stream.cuh); fixed at creation by pmg_set_finest_streaming
+  bool stream_fine = false;
   // MG-preconditioned CG on the finest level (allocated on first use):
   // right-hand side, iterate, residual, preconditioned residual, search
   // direction, A times it; three reduction slots; the iteration state.
@@ -267,17 +275,21 @@ void plan(pmg_problem *p, Arena &a) {
     const bool smoothed = L > 1 && !fine;
     v.xalt = (smoothed && !mixed) ? a.take<double>(v.n3) : nullptr;
     v.omega = a.take<double>(1);
+    // the refinement paths' finest operator, correction, its right-hand
+    // side and the code bytes are colour-split (split_layout.cuh)
+    const long ns = fine ? Split::of(v.d).count() : 0;
     if (mixed) {
       const long m = v.n3_32;
+      const long mf = fine ? ns : m;
       for (int s = 0; s < 14; ++s)
-        v.op32[s] = (L > 1 && s < nops) ? a.take<float>(m) : nullptr;
+        v.op32[s] = (L > 1 && s < nops) ? a.take<float>(mf) : nullptr;
       for (int s = 0; s < 27; ++s)
         v.P32[s] = fine ? nullptr : a.take<float>(m);
-      v.x32 = a.take<float>(m);
-      v.f32 = a.take<float>(m);
-      v.r32 = L > 1 ? a.take<float>(m) : nullptr;
+      v.x32 = a.take<float>(mf);
+      v.f32 = a.take<float>(mf);
+      v.r32 = L > 1 ? a.take<float>(m) : nullptr; // reference layout
       v.xalt32 = smoothed ? a.take<float>(m) : nullptr;
-      v.code = fine ? a.take<unsigned char>(v.n3) : nullptr;
+      v.code = fine ? a.take<unsigned char>(ns) : nullptr;
       v.code_info = fine ? a.take<int>(12) : nullptr;
       v.lut64 = fine ? a.take<double>(6) : nullptr;
       v.octab64 = fine ? a.take<double>(128) : nullptr;
@@ -286,10 +298,10 @@ void plan(pmg_problem *p, Arena &a) {
     }
     if (fast && fine) {
       for (int s = 0; s < 4; ++s)
-        v.ops[s] = a.take<double>(v.n3);
-      v.xs = a.take<double>(v.n3);
-      v.fs = a.take<double>(v.n3);
-      v.code = a.take<unsigned char>(v.n3);
+        v.ops[s] = a.take<double>(ns);
+      v.xs = a.take<double>(ns);
+      v.fs = a.take<double>(ns);
+      v.code = a.take<unsigned char>(ns);
       v.code_info = a.take<int>(12);
       v.lut64 = a.take<double>(6);
       v.octab64 = a.take<double>(128);
@@ -492,6 +504,9 @@ double norm_from_sum(const pmg_problem *p, double s) {
 // on every level (the same bits)
 std::atomic<int> g_tma_on{1};
 bool tma_disabled() { return g_tma_on.load() == 0; }
+// pmg_set_finest_streaming: problems created while it is off use the
+// per-point-load colour pass (gs7_code_color_kernel) on the finest level
+std::atomic<int> g_stream_on{1};
 // pmg_test_tma_short_delivery: extra bytes every stage waits for
 std::atomic<unsigned> g_tma_extra_tx{0};
 
@@ -543,6 +558,55 @@ void encode_tma_maps(pmg_problem *p) {
     ok = ok && encode_level_map(&v.tma.xalt, v.xalt32, v.d32, v.tma_tile);
     v.tma_ok = ok;
   }
+}
+
+// A 4-D map {entry, half, row, plane} of one colour-split array of the
+// level (split_layout.cuh): boxes of bw entries of one half over `rows`
+// rows of one plane.
+bool encode_split_map(CUtensorMap *m, const void *base, CUtensorMapDataType t,
+                      int esz, const Dims &d, int bw, int rows) {
+  auto enc = tensor_map_encoder();
+  if (!enc || !base || ((uintptr_t)base & 15) != 0)
+    return false;
+  const Split sp = Split::of(d);
+  const cuuint64_t dims[4] = {(cuuint64_t)sp.hp, 2, (cuuint64_t)d.ny,
+                              (cuuint64_t)d.nz};
+  const cuuint64_t strides[3] = {(cuuint64_t)sp.hp * esz,
+                                 (cuuint64_t)sp.pitch() * esz,
+                                 (cuuint64_t)sp.plane() * esz};
+  const cuuint32_t box[4] = {(cuuint32_t)bw, 1, (cuuint32_t)rows, 1};
+  const cuuint32_t elem[4] = {1, 1, 1, 1};
+  return enc(m, t, 4, const_cast<void *>(base), dims, strides, box, elem,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+             CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// The finest colour passes of a refinement path can be streamed
+// (gs7_stream.cuh): the level fits the stage ring and the box width, and
+// the tensor maps of its correction, right-hand side and code bytes could
+// be made (their arrays are fixed for the life of the problem).
+template <typename T>
+bool encode_stream_maps(LevelBuf &v, const T *x, const T *f) {
+  if (!stream_fits<T>(v.d))
+    return false;
+  const StreamShape sh = stream_shape<T>(v.d, 1);
+  constexpr int J = StreamCfg<T>::J;
+  const CUtensorMapDataType t = sizeof(T) == 4
+                                    ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+                                    : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+  return encode_split_map(&v.smaps.x, x, t, sizeof(T), v.d, sh.bw, J + 2) &&
+         encode_split_map(&v.smaps.f, f, t, sizeof(T), v.d, sh.bw, J) &&
+         encode_split_map(&v.smaps.code, v.code,
+                          CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, v.d, sh.bwc, J);
+}
+bool stream_fine_ok(pmg_problem *p) {
+  LevelBuf &v = p->lv[p->nlev];
+  if (p->precision == PMG_PREC_MIXED)
+    return encode_stream_maps<float>(v, v.x32, v.f32);
+  if (p->precision == PMG_PREC_FP64_FAST)
+    return encode_stream_maps<double>(v, v.xs, v.fs);
+  return false;
 }
 
 // nsweeps eight-colour sweeps of a padded float level (launch_gs27_pp's
@@ -599,6 +663,15 @@ template <typename T>
 int smooth_ref(pmg_problem *p, int L, int nsweeps, int zero_init, T **cur) {
   using A = LevelArrays<T>;
   LevelBuf &v = p->lv[L];
+  // (the streamed pass's tensor maps cover the level's own correction and
+  // right-hand side)
+  if (L == p->nlev && p->use_codes && p->stream_fine && *cur == A::x(v))
+    return launch_gs7_stream<T>(v.smaps, v.d, A::fine_op(v, kOC),
+                                A::fine_op(v, kOE), A::fine_op(v, kON),
+                                A::fine_op(v, kUC), v.code_info, A::lut(v),
+                                A::octab(v), *cur, nsweeps, 0, zero_init,
+                                p->kernel_err, g_tma_extra_tx.load(),
+                                p->stream);
   if (L == p->nlev && p->use_codes)
     return launch_gs7_code<T>(v.d, A::fine_op(v, kOC), A::f(v),
                               A::fine_op(v, kOE), A::fine_op(v, kON),
@@ -1306,6 +1379,7 @@ int pmg_problem_create(int base, int nlev, double box, int precision,
     (void)cudaGetLastError();
     if (!tma_disabled())
       encode_tma_maps(p);
+    p->stream_fine = g_stream_on.load() != 0 && stream_fine_ok(p);
   }
   if (stream) {
     p->stream = (cudaStream_t)stream;
@@ -1371,6 +1445,11 @@ int pmg_problem_set_coarse_rtol(pmg_problem *p, double rtol) {
   }
   p->coarse_rtol = rtol;
   drop_graphs(p); // the captured cycles bake the threshold in
+  return PMG_OK;
+}
+
+int pmg_set_finest_streaming(int on) {
+  g_stream_on.store(on != 0);
   return PMG_OK;
 }
 
@@ -1721,8 +1800,9 @@ static int solve_host_loop(pmg_problem *p, double tol, int max_cycles,
   PMG_CUDA_TRY(cudaMemcpy(&lost, p->kernel_err, sizeof(int),
                           cudaMemcpyDeviceToHost));
   if (rc == PMG_OK && lost) {
-    set_last_message("pmg_solve: a staged copy of the 27-point smoother did "
-                     "not arrive (bounded wait ran out)");
+    set_last_message("pmg_solve: a staged copy (27-point smoother or "
+                     "streamed finest pass) did not arrive (bounded wait "
+                     "ran out)");
     rc = PMG_ERR_TIMEOUT;
   }
   return rc;
@@ -1804,8 +1884,9 @@ int pmg_solve_finish(pmg_problem *p, int *cycles, double *relres,
     return PMG_ERR_DIVERGED;
   }
   if (st.status == 3) {
-    set_last_message("pmg_solve: a staged copy of the 27-point smoother did "
-                     "not arrive (bounded wait ran out)");
+    set_last_message("pmg_solve: a staged copy (27-point smoother or "
+                     "streamed finest pass) did not arrive (bounded wait "
+                     "ran out)");
     return PMG_ERR_TIMEOUT;
   }
   return PMG_OK;

@@ -102,9 +102,12 @@ __global__ void __launch_bounds__(kReduceThreads)
       const T dv =
           f[p] - apply_op<KIND>(A, (const T *)nullptr, x, p, sy, sz);
       if (r) {
-        if constexpr (SPLIT_OUT) { // colour-split row layout (i-1 parity)
-          const int q = i - 1;
-          r[p - q + (q >> 1) + (q & 1) * ((d.nx + 1) / 2)] = (Tout)dv;
+        if constexpr (SPLIT_OUT) {
+          // colour-split rows (split_layout.cuh): halves of hp entries (a
+          // multiple of 16), point i at entry (i - 1) >> 1 of its colour's
+          const int hp = ((d.nx + 1) / 2 + 15) & ~15;
+          r[((k - 1) * d.ny + (j - 1)) * 2 * hp + ((i + j + k) & 1) * hp +
+            ((i - 1) >> 1)] = (Tout)dv;
         } else {
           r[p] = (Tout)dv;
         }

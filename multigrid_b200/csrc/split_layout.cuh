@@ -1,21 +1,27 @@
-// Colour-split layout of the mixed path's finest-level float arrays.
+// Colour-split layout of the refinement paths' finest-level arrays.
 //
 // In the reference layout a red-black colour pass touches every other point
 // of a row, so it streams whole cache sectors of every array it reads: one
-// sweep moves about twice the bytes it needs. The mixed path owns its float
-// copies of the finest operator, right-hand side and correction, so it keeps
-// them with every row split by the parity of i-1: points with even i-1 first,
-// then those with odd i-1. One colour of a row is then a contiguous run, and
-// a colour pass reads only its own half of oC and f and the other colour's
-// half of x (it still needs both halves of oE, oN, uC: the couplings to the
-// west, south and lower neighbours are stored at those neighbours). Per sweep
-// that is 10 arrays' worth of traffic instead of about 13.5.
+// sweep moves about twice the bytes it needs. The mixed and fp64-fast paths
+// own their copies of the finest operator, right-hand side and correction,
+// so they keep every row split by colour: the points with (i + j + k) even
+// in the first half of the row, the odd ones in the second, each half
+// padded to a multiple of 16 entries (`hp`) so that every half row starts
+// on a 16-byte boundary. Entry (i - 1) >> 1 of its colour's half holds
+// point i. A colour pass then reads one contiguous half of every row of f
+// and the code bytes, and the other colour's half of x, which is the same
+// half in every row, so the J rows a block needs of a plane form one
+// tensor-map box (gs7_stream.cuh). Its neighbours: i - 1 and i + 1 are
+// entries e - (i odd), e + (i even) of the other half of the row; j +- 1
+// and k +- 1 are entry e of the other half of the next or previous row or
+// plane.
 //
-// Only the arrays of the finest float level use this layout; the kernels
-// here read and write them, converting at the boundaries (the double
-// residual, the prolongation's correction, the refinement update). The
-// per-point arithmetic is the reference-layout kernels', so results are
-// bit-identical.
+// Only the arrays of the finest level use this layout; the kernels here
+// read and write them, converting at the boundaries (the double residual,
+// the prolongation's correction, the refinement update). The per-point
+// arithmetic is the reference-layout kernels', so results are
+// bit-identical. The padding entries are zero (the problem's arena is
+// cleared at creation) and no update reads them.
 #pragma once
 
 #include <climits>
@@ -27,22 +33,27 @@
 namespace pmg {
 
 struct Split {
-  int nx, ny, nz, hx; // hx = (nx + 1) / 2: entries of the even half
+  int nx, ny, nz, hp; // hp: entries per colour half (a multiple of 16)
   __host__ __device__ static Split of(const Dims &d) {
-    return Split{d.nx, d.ny, d.nz, (d.nx + 1) / 2};
+    return Split{d.nx, d.ny, d.nz, ((d.nx + 1) / 2 + 15) & ~15};
   }
+  // entries of a row and of a plane
+  __host__ __device__ int pitch() const { return 2 * hp; }
+  __host__ __device__ int plane() const { return 2 * hp * ny; }
+  __host__ __device__ long count() const { return (long)plane() * nz; }
+  // first entry of row (j, k) (its colour-0 half)
   __host__ __device__ int row(int j, int k) const {
-    return ((k - 1) * ny + (j - 1)) * nx;
+    return ((k - 1) * ny + (j - 1)) * pitch();
   }
   // split index of (i, j, k)
   __host__ __device__ int at(int i, int j, int k) const {
-    const int q = i - 1;
-    return row(j, k) + (q >> 1) + (q & 1) * hx;
+    return row(j, k) + ((i + j + k) & 1) * hp + ((i - 1) >> 1);
   }
   // split index of the reference-layout linear index g
-  __host__ __device__ int of_linear(int g) const {
-    const int r = g / nx, q = g - r * nx;
-    return r * nx + (q >> 1) + (q & 1) * hx;
+  __host__ __device__ int of_linear(long g) const {
+    const int i = (int)(g % nx) + 1;
+    const long r = g / nx;
+    return at(i, (int)(r % ny) + 1, (int)(r / ny) + 1);
   }
 };
 
@@ -54,7 +65,7 @@ __global__ void to_split_kernel(Dims d, const Tin *__restrict__ src,
   const long n = d.count();
   for (long g = blockIdx.x * (long)blockDim.x + threadIdx.x; g < n;
        g += (long)gridDim.x * blockDim.x)
-    dst[sp.of_linear((int)g)] = (Tout)src[g];
+    dst[sp.of_linear(g)] = (Tout)src[g];
 }
 
 // dst (reference layout) = (Tout) src (split), every entry
@@ -65,7 +76,7 @@ __global__ void from_split_kernel(Dims d, const Tin *__restrict__ src,
   const long n = d.count();
   for (long g = blockIdx.x * (long)blockDim.x + threadIdx.x; g < n;
        g += (long)gridDim.x * blockDim.x)
-    dst[g] = (Tout)src[sp.of_linear((int)g)];
+    dst[g] = (Tout)src[sp.of_linear(g)];
 }
 
 // x64 (reference layout) += (double) e (split) on the interior: the
@@ -80,27 +91,29 @@ __global__ void add_correction_split_kernel(Dims d, double *__restrict__ x,
   x[p] = x[p] + (double)e[Split::of(d).at(t.i, t.j, t.k)];
 }
 
-// Neighbour offsets of the point at split index s with q = i - 1 of parity
-// qp: west and east (the other half), north/south (one row), up/down (one
-// plane).
+// Neighbour offsets of point i of colour c at split index s: every
+// neighbour has the other colour, so it lies in the other half; west and
+// east in the same row (entries e - 1, e for odd i; e, e + 1 for even i),
+// north / south one row on, up / down one plane on, at entry e.
 struct SplitNb {
   int w, e, n, s, u, dn;
 };
-__device__ __forceinline__ SplitNb split_nb(const Split &sp, int s, int qp) {
+__device__ __forceinline__ SplitNb split_nb(const Split &sp, int s, int i,
+                                            int c) {
+  const int o = s + (1 - 2 * c) * sp.hp; // entry e of the other half
+  const int odd = i & 1;
   SplitNb nb;
-  // even q: west (q-1) and east (q+1) sit at q/2 - 1 and q/2 of the odd half;
-  // odd q: at (q-1)/2 and (q+1)/2 of the even half
-  nb.w = qp ? s - sp.hx : s + sp.hx - 1;
-  nb.e = qp ? s - sp.hx + 1 : s + sp.hx;
-  nb.n = s + sp.nx;
-  nb.s = s - sp.nx;
-  nb.u = s + sp.nx * sp.ny;
-  nb.dn = s - sp.nx * sp.ny;
+  nb.w = o - odd;
+  nb.e = o + 1 - odd;
+  nb.n = o + sp.pitch();
+  nb.s = o - sp.pitch();
+  nb.u = o + sp.plane();
+  nb.dn = o - sp.plane();
   return nb;
 }
 
 // One colour of the red-black sweep (gs7_color_kernel) on split arrays: the
-// points of a row with (i + j + k) % 2 == want are one contiguous run. One
+// points of a row with (i + j + k) % 2 == want are one half of it. One
 // thread per point; blockIdx.z is the plane.
 template <typename T>
 __global__ void __launch_bounds__(256)
@@ -117,9 +130,8 @@ __global__ void __launch_bounds__(256)
                 2 * (int)(blockIdx.x * blockDim.x + threadIdx.x);
   if (i > d.nx - 1)
     return;
-  const int qp = (i - 1) & 1;
   const int p = sp.at(i, j, k);
-  const SplitNb nb = split_nb(sp, p, qp);
+  const SplitNb nb = split_nb(sp, p, i, want);
   const T s = oN[p] * x[nb.n] + oN[nb.s] * x[nb.s] + oE[p] * x[nb.e] +
               oE[nb.w] * x[nb.w] + uC[nb.dn] * x[nb.dn] + uC[p] * x[nb.u];
   x[p] = (fc[p] + keep * s) / (oC[p] + T(0));
@@ -155,7 +167,7 @@ __global__ void __launch_bounds__(256)
     return;
   const Split sp = Split::of(d);
   const int p = sp.at(t.i, t.j, t.k);
-  const SplitNb nb = split_nb(sp, p, (t.i - 1) & 1);
+  const SplitNb nb = split_nb(sp, p, t.i, (t.i + t.j + t.k) & 1);
   const T ax = -oN[p] * x[nb.n] - oN[nb.s] * x[nb.s] - oE[p] * x[nb.e] -
                oE[nb.w] * x[nb.w] - uC[nb.dn] * x[nb.dn] - uC[p] * x[nb.u] +
                (oC[p] + T(0)) * x[p];
@@ -209,7 +221,7 @@ __global__ void __launch_bounds__(256)
     int i, j, k;
     interior_coords(d, q, i, j, k);
     const int p = sp.at(i, j, k);
-    const SplitNb nb = split_nb(sp, p, (i - 1) & 1);
+    const SplitNb nb = split_nb(sp, p, i, (i + j + k) & 1);
     // classified by their float values (the double path checks its
     // couplings against the table separately, lut64_check_kernel)
     const int c[6] = {float_order((float)oE[p]), float_order((float)oE[nb.w]),
@@ -267,7 +279,7 @@ __global__ void __launch_bounds__(256)
     return;
   const Split sp = Split::of(d);
   const int p = sp.at(t.i, t.j, t.k);
-  const SplitNb nb = split_nb(sp, p, (t.i - 1) & 1);
+  const SplitNb nb = split_nb(sp, p, t.i, (t.i + t.j + t.k) & 1);
   const T c[6] = {oE[p], oE[nb.w], oN[p], oN[nb.s], uC[p], uC[nb.dn]};
   unsigned bits = 0;
   bool bad = false;
@@ -506,7 +518,6 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 8 : 4)
                  2 * (int)(blockIdx.x * blockDim.x * PTS + threadIdx.x);
   if (i0 > d.nx - 1)
     return;
-  const int qp = (i0 - 1) & 1; // the same for every point of the thread
   int p[PTS];
   bool ok[PTS];
   unsigned b[PTS];
@@ -523,7 +534,8 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 8 : 4)
   T s[PTS], f[PTS], c[PTS];
 #pragma unroll
   for (int r = 0; r < PTS; ++r) {
-    const SplitNb nb = split_nb(sp, p[r], qp);
+    // every point of the thread has colour want and the parity of i0
+    const SplitNb nb = split_nb(sp, p[r], i0, want);
     Couplings<T> cp;
     if (coded) {
       cp.e = (b[r] & 1u) ? L.eh : L.el;
@@ -600,7 +612,8 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 8 : 4)
       ii[q] = i0;
     p[q] = sp.at(ii[q], j, k);
     b[q] = code[p[q]];
-    const SplitNb nb = split_nb(sp, p[q], (ii[q] - 1) & 1);
+    const SplitNb nb =
+        split_nb(sp, p[q], ii[q], (ii[q] + j + k) & 1);
     xv[q][0] = x[nb.n];
     xv[q][1] = x[nb.s];
     xv[q][2] = x[nb.e];
@@ -627,7 +640,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 8 : 4)
       c.dn = (b[q] & 32u) ? L.uh : L.ul;
     } else {
       c = array_couplings<T>(oE, oN, uC, p[q],
-                             split_nb(sp, p[q], (ii[q] - 1) & 1));
+                             split_nb(sp, p[q], ii[q], (ii[q] + j + k) & 1));
     }
     const T ax = -c.n * xv[q][0] - c.s * xv[q][1] - c.e * xv[q][2] -
                  c.w * xv[q][3] - c.dn * xv[q][4] - c.u * xv[q][5] +

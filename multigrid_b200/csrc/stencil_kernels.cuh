@@ -281,13 +281,21 @@ __global__ void __launch_bounds__(256)
     return;
   const T ww = (T)(*w);
   const int cy = dc.sy(), cz = dc.sz();
-  const int fy = df.sy(), fz = df.sz();
   const int c = dc.at(ii, jj, kk);
-  const int f = df.at(2 * ii - 1, 2 * jj - 1, 2 * kk - 1);
-  // fine points 2ii-1 and 2ii of a row: reference layout f, f + 1; split
-  // layout (i - 1 = 2ii-2 even, 2ii-1 odd) row + ii-1 and row + hx + ii-1
-  const int e0 = SPLIT_X ? f - (2 * ii - 2) + (ii - 1) : f;
-  const int e1 = SPLIT_X ? e0 + (df.nx + 1) / 2 : f + 1;
+  // fine point (2ii-1 + a, 2jj-1 + b, 2kk-1 + c): reference layout
+  // f0 + a + b fy + c fz; colour-split layout (split_layout.cuh: halves of
+  // hp entries, a multiple of 16) entry ii - 1 of the half of its colour
+  // (1 + a + b + c) & 1 in row f0 + b fy + c fz
+  const int hp = SPLIT_X ? ((df.nx + 1) / 2 + 15) & ~15 : 0;
+  const int fy = SPLIT_X ? 2 * hp : df.sy();
+  const int fz = SPLIT_X ? 2 * hp * df.ny : df.sz();
+  const int f0 = SPLIT_X ? ((2 * kk - 2) * df.ny + (2 * jj - 2)) * fy + ii - 1
+                         : df.at(2 * ii - 1, 2 * jj - 1, 2 * kk - 1);
+  // offsets of the points with a = 0 and a = 1 in the rows with b + c even
+  // (in the other rows the two swap halves)
+  const int ev0 = SPLIT_X ? hp : 0, ev1 = SPLIT_X ? 0 : 1;
+  const int od0 = 0, od1 = SPLIT_X ? hp : 1;
+  const int e0 = f0 + ev0, e1 = f0 + ev1;
   const T *const *p = P.p;
   const T x000 = xin[c], x100 = xin[c + 1], x010 = xin[c + cy],
           x001 = xin[c + cz], x110 = xin[c + 1 + cy], x101 = xin[c + 1 + cz],
@@ -306,12 +314,13 @@ __global__ void __launch_bounds__(256)
                  p[16][c + cy] * x010 + p[17][c + 1 + cy] * x110 +
                  p[23][c + cz] * x001 + p[24][c + 1 + cz] * x101 +
                  p[25][c + cy + cz] * x011 + p[26][c + 1 + cy + cz] * x111;
+  const int o0 = f0 + od0, o1 = f0 + od1; // rows with b + c odd
   x[e0] = x[e0] + ww * v000;
   x[e1] = x[e1] + ww * v100;
-  x[e0 + fy] = x[e0 + fy] + ww * v010;
-  x[e0 + fz] = x[e0 + fz] + ww * v001;
-  x[e1 + fy] = x[e1 + fy] + ww * v110;
-  x[e1 + fz] = x[e1 + fz] + ww * v101;
+  x[o0 + fy] = x[o0 + fy] + ww * v010;
+  x[o0 + fz] = x[o0 + fz] + ww * v001;
+  x[o1 + fy] = x[o1 + fy] + ww * v110;
+  x[o1 + fz] = x[o1 + fz] + ww * v101;
   x[e0 + fy + fz] = x[e0 + fy + fz] + ww * v011;
   x[e1 + fy + fz] = x[e1 + fy + fz] + ww * v111;
 }

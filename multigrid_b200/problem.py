@@ -59,6 +59,14 @@ def set_tma_staging(on: bool) -> None:
     _lib.check("pmg_set_tma_staging", _lib.lib.pmg_set_tma_staging(int(on)))
 
 
+def set_finest_streaming(on: bool) -> None:
+    """Problems created afterwards stream the refinement paths' finest
+    colour passes through shared memory by bulk copies (default) or load
+    per point (the same bits; pmg_set_finest_streaming)."""
+    _lib.check("pmg_set_finest_streaming",
+               _lib.lib.pmg_set_finest_streaming(int(on)))
+
+
 @dataclasses.dataclass
 class SolveResult:
     cycles: int

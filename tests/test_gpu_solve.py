@@ -485,3 +485,67 @@ def test_tma_stage_wait_runs_out_and_reports(pb65):
     after = solve()
     assert after[0] == before[0]
     assert np.array_equal(after[1], before[1])
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64-fast"])
+@pytest.mark.parametrize("name", ["pb49", "pb65", "pb161", "pb257"])
+def test_streamed_finest_pass_gives_the_same_bits(name, precision):
+    """The refinement paths' finest colour passes with the level's rows
+    streamed through shared memory by bulk copies (row blocks of 8, planes
+    in chunks that fill the GPU once) against the per-point-load pass: the
+    same cycles and the same potential, bit for bit. 49^3 leaves a last row
+    block of 7 rows; 161^3 and 257^3 are the benchmark grids."""
+    from multigrid_b200.molecule import Workload
+    from multigrid_b200.problem import set_finest_streaming
+    w = (Workload("pb49", 3, 4, 0.5, 300, 8.0, 5) if name == "pb49"
+         else WORKLOADS[name])
+    fine = setup_fine(w.n, w.h, w.atoms(), w.physics)
+    out = {}
+    try:
+        for on in (True, False):
+            set_finest_streaming(on)
+            with PBELinearProblem(w.base, w.nlev, w.box, precision,
+                                  w.physics) as p:
+                p.set_fine(**fine)
+                p.buildmultilevelops()
+                assert p.coded_couplings()
+                r = p.solve(tol=1e-10, max_cycles=100)
+                assert r.relres < 1e-10
+                out[on] = (r.cycles, p.potential().ravel().copy())
+    finally:
+        set_finest_streaming(True)
+    assert out[True][0] == out[False][0]
+    assert np.array_equal(out[True][1], out[False][1])
+
+
+def test_streamed_pass_wait_runs_out_and_reports(pb65):
+    """The streamed finest pass's stage waits are bounded: fp64-fast (whose
+    coarse smoother stages nothing, so the finest pass is the only staged
+    kernel) with every stage expecting 16 bytes more than its copies
+    deliver reports PMG_ERR_TIMEOUT; a new problem afterwards solves bit for
+    bit as before on the same context."""
+    from multigrid_b200 import _lib
+    w, fine = pb65
+
+    def solve():
+        with PBELinearProblem(w.base, w.nlev, w.box, "fp64-fast",
+                              w.physics) as p:
+            p.set_fine(**fine)
+            p.buildmultilevelops()
+            r = p.solve(tol=1e-10, max_cycles=100)
+            return r.cycles, p.potential().ravel().copy()
+
+    before = solve()
+    _lib.check("pmg_test_tma_short_delivery",
+               _lib.lib.pmg_test_tma_short_delivery(16))
+    try:
+        with pytest.raises(PmgError) as e:
+            solve()
+        assert e.value.status == _lib.PMG_ERR_TIMEOUT
+        assert b"did not arrive" in _lib.lib.pmg_last_error()
+    finally:
+        _lib.check("pmg_test_tma_short_delivery",
+                   _lib.lib.pmg_test_tma_short_delivery(0))
+    after = solve()
+    assert after[0] == before[0]
+    assert np.array_equal(after[1], before[1])
