@@ -9,8 +9,11 @@
 // only what its registers hold in flight, so it runs issue- and
 // latency-bound at ~2.6 TB/s (ncu: 77% issue, 38 M warp instructions per
 // 257^3 pass). Here each CTA owns J rows of a chunk of planes and marches
-// along k. Per plane one thread issues three tensor-map boxes onto one
-// mbarrier of a ring of S stages: the other colour's half of x over J + 2
+// along k. Per plane a producer warp issues three tensor-map boxes onto
+// the "full" mbarrier of a slot of a ring of S stages, once every consumer
+// warp has released the slot's previous plane on its "empty" mbarrier (no
+// block-wide barrier per plane; each consumer warp waits only for the
+// planes it reads): the other colour's half of x over J + 2
 // rows (the rows above and below the block for the north and south
 // neighbours), and the own colour's half of f and of the code bytes over
 // the block's J rows. In the colour-split layout the other colour is the
@@ -33,9 +36,11 @@
 // the box and are never used. The tensor maps cover this GPU's own arrays
 // (no multicast).
 //
-// Every wait on a stage is bounded (gs27_tma.cuh's poll limit); a CTA whose
-// stage did not arrive sets *err, waits (also bounded) for every copy it
-// issued, and returns; the solve's stop test reports PMG_ERR_TIMEOUT.
+// Every wait is bounded (gs27_tma.cuh's poll limit): a consumer warp whose
+// plane did not arrive sets *err and returns; the producer, whose slot is
+// then never released, sets *err, waits (also bounded) for the copies it
+// has in flight, and returns; the solve's stop test reports
+// PMG_ERR_TIMEOUT.
 #pragma once
 
 #include <atomic>
@@ -46,11 +51,11 @@
 namespace pmg {
 
 // Rows per CTA, ring stages and threads of the streamed pass by element
-// type; one warp per row.
+// type: one consumer warp per row and one producer warp.
 template <typename T> struct StreamCfg {
   static constexpr int J = 8;
   static constexpr int S = sizeof(T) == 4 ? 6 : 4;
-  static constexpr int THREADS = 32 * J;
+  static constexpr int THREADS = 32 * (J + 1);
   // CTAs per SM the ring's shared memory allows at 257^3 (registers capped
   // to match)
   static constexpr int MIN_CTAS = sizeof(T) == 4 ? 3 : 2;
@@ -85,6 +90,32 @@ __device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map,
       : "memory");
 }
 
+// a plain arrival on an mbarrier (no transaction bytes)
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(
+                   smem_addr(bar))
+               : "memory");
+}
+
+// num / (c + 0), rounded to T, with c the divisor of table entry b.
+// Double: IEEE division. Float: num times the double reciprocal of the
+// divisor, rounded to float. That product is within 2^-51 (relative) of
+// num / c (two double roundings), while a quotient of two 24-bit floats
+// that is not itself a float lies at least 2^-49 (relative) from every
+// rounding midpoint between floats ((a - c m) is a nonzero multiple of the
+// smallest exponent's unit), so both round to the same float: the bits of
+// the division, without its special-case branch. Quotients that are
+// floats, zeros, infinities and NaNs come out the same too.
+__device__ __forceinline__ double div_by_table(double num, double c,
+                                               const double *, unsigned) {
+  return num / (c + 0.0);
+}
+__device__ __forceinline__ float div_by_table(float num, float,
+                                              const double *rtab,
+                                              unsigned b) {
+  return (float)((double)num * rtab[b]);
+}
+
 // four consecutive entries
 template <typename T> struct alignas(16) Quad {
   T x, y, z, w;
@@ -105,7 +136,13 @@ __global__ void __launch_bounds__(StreamCfg<T>::THREADS,
   // per code byte (its low seven bits) the point's seven coefficients in
   // the order the update uses them: n, s, e, w, down, up, oC (one spare)
   __shared__ __align__(16) T ctab[128][8];
-  uint64_t *bar = reinterpret_cast<uint64_t *>(sm + S * sh.slot);
+  // float: the double reciprocal of each code's divisor oC + 0 (see
+  // div_by_table)
+  __shared__ double rtab[sizeof(T) == 4 ? 128 : 1];
+  // full[s]: the slot's boxes landed (the producer's arrival and their
+  // bytes); empty[s]: every consumer warp is done with it
+  uint64_t *full = reinterpret_cast<uint64_t *>(sm + S * sh.slot);
+  uint64_t *empty = full + S;
   const Split sp = Split::of(d);
   const int jb = blockIdx.x % sh.nj, kc = blockIdx.x / sh.nj;
   const int j0 = 2 + jb * J;
@@ -116,8 +153,10 @@ __global__ void __launch_bounds__(StreamCfg<T>::THREADS,
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
 #pragma unroll
-    for (int s = 0; s < S; ++s)
-      mbar_init(&bar[s], 1);
+    for (int s = 0; s < S; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], J);
+    }
     fence_mbar_init();
   }
   // the coding (uniform): couplings from the code byte, oC from the table
@@ -135,52 +174,72 @@ __global__ void __launch_bounds__(StreamCfg<T>::THREADS,
     t[5] = (b & 16u) ? L.uh : L.ul;
     t[6] = octab[b];
     t[7] = T(0);
+    if constexpr (sizeof(T) == 4)
+      rtab[b] = 1.0 / (double)(t[6] + T(0));
   }
   __syncthreads();
+  auto slot_of = [&](int kk) { return (kk - kfirst) % S; };
+  auto use_of = [&](int kk) { return (kk - kfirst) / S; };
 
-  // thread 0: the boxes of plane kk into its slot (0-based coordinates:
-  // entry 0, the half, row j - 1, plane k - 1); the planes the block
-  // computes also bring their f and code rows
-  auto issue = [&](int kk) {
-    const int s = (kk - kfirst) % S;
-    unsigned char *slot = sm + s * sh.slot;
-    const bool own = kk >= ka && kk <= kb;
-    mbar_expect_tx(&bar[s], sh.xbytes + (own ? sh.fcbytes : 0u) + extra_tx);
-    tma_load_4d(slot + sh.xoff, &maps.x, 0, 1 - want, j0 - 2, kk - 1,
-                &bar[s]);
-    if (own) {
-      tma_load_4d(slot + sh.foff, &maps.f, 0, want, j0 - 1, kk - 1, &bar[s]);
-      tma_load_4d(slot + sh.coff, &maps.code, 0, want, j0 - 1, kk - 1,
-                  &bar[s]);
+  if (warp == J) {
+    // producer: the boxes of plane kk into its slot once the slot's
+    // previous plane is released (0-based coordinates: entry 0, the half,
+    // row j - 1, plane k - 1); the planes the block computes also bring
+    // their f and code rows
+    if (lane != 0)
+      return;
+    // every copy still in flight (planes last - S + 1 .. last) lands
+    // before the producer leaves; one poll budget for all of them
+    auto drain = [&](int last) {
+      long polls = 0;
+      for (int kk = max(kfirst, last - S + 1); kk <= last; ++kk)
+        while (!mbar_try_wait(&full[slot_of(kk)], use_of(kk) & 1u)) {
+          if (++polls > kTmaMaxPolls)
+            return;
+          if (polls > 64)
+            __nanosleep(64);
+        }
+    };
+    for (int kk = kfirst; kk <= klast; ++kk) {
+      const int s = slot_of(kk), u = use_of(kk);
+      if (u > 0 && !mbar_wait(&empty[s], (u - 1) & 1u)) {
+        atomicOr(err, 1);
+        drain(kk - 1);
+        return;
+      }
+      unsigned char *slot = sm + s * sh.slot;
+      const bool own = kk >= ka && kk <= kb;
+      mbar_expect_tx(&full[s],
+                     sh.xbytes + (own ? sh.fcbytes : 0u) + extra_tx);
+      tma_load_4d(slot + sh.xoff, &maps.x, 0, 1 - want, j0 - 2, kk - 1,
+                  &full[s]);
+      if (own) {
+        tma_load_4d(slot + sh.foff, &maps.f, 0, want, j0 - 1, kk - 1,
+                    &full[s]);
+        tma_load_4d(slot + sh.coff, &maps.code, 0, want, j0 - 1, kk - 1,
+                    &full[s]);
+      }
     }
-  };
-  auto parity = [&](int kk) { return (unsigned)((kk - kfirst) / S) & 1u; };
+    drain(klast);
+    return;
+  }
 
-  if (threadIdx.x == 0)
-    for (int kk = kfirst; kk <= klast && kk < kfirst + S; ++kk)
-      issue(kk);
-  int issued = min(klast, kfirst + S - 1); // last plane issued
-  int ready = kfirst - 1;                   // last plane waited for
+  // consumers: warp r computes row j0 + r of each plane (a warp past the
+  // last row keeps the pace and releases its slots)
+  int ready = kfirst - 1; // last plane waited for
   const int bw = sh.bw, bwc = sh.bwc;
   for (int k = ka; k <= kb; ++k) {
     // planes k - 1, k, k + 1 complete
-    bool ok = true;
     for (int kk = ready + 1; kk <= k + 1; ++kk)
-      ok = ok && mbar_wait(&bar[(kk - kfirst) % S], parity(kk));
-    if (__syncthreads_or(!ok)) {
-      if (threadIdx.x == 0) {
-        atomicOr(err, 1);
-        // every issued copy lands before the block leaves
-        for (int kk = ready + 1; kk <= issued; ++kk)
-          (void)mbar_wait(&bar[(kk - kfirst) % S], parity(kk));
+      if (!mbar_wait(&full[slot_of(kk)], use_of(kk) & 1u)) {
+        if (lane == 0)
+          atomicOr(err, 1);
+        return;
       }
-      __syncthreads();
-      return;
-    }
     ready = k + 1;
-    const unsigned char *sd = sm + ((k - 1 - kfirst) % S) * sh.slot;
-    const unsigned char *sc = sm + ((k - kfirst) % S) * sh.slot;
-    const unsigned char *su = sm + ((k + 1 - kfirst) % S) * sh.slot;
+    const unsigned char *sd = sm + slot_of(k - 1) * sh.slot;
+    const unsigned char *sc = sm + slot_of(k) * sh.slot;
+    const unsigned char *su = sm + slot_of(k + 1) * sh.slot;
     if (warp < jn) { // warp-uniform
       const int r = warp, j = j0 + r;
       // x stage row rr holds row j0 - 1 + rr: row j is rr = r + 1
@@ -244,7 +303,8 @@ __global__ void __launch_bounds__(StreamCfg<T>::THREADS,
             const Quad<T> c1 = *reinterpret_cast<const Quad<T> *>(t + 4);
             const T sum = c0.x * an[m] + c0.y * as[m] + c0.z * xe[m] +
                           c0.w * xw[m] + c1.x * ad[m] + c1.y * au[m];
-            out[m] = (af[m] + keep * sum) / (c1.z + T(0));
+            out[m] = div_by_table(af[m] + keep * sum, c1.z, rtab,
+                                  (cb >> (8 * m)) & 127u);
           }
         } else {
 #pragma unroll
@@ -289,12 +349,10 @@ __global__ void __launch_bounds__(StreamCfg<T>::THREADS,
         }
       }
     }
-    __syncthreads(); // the slot of plane k - 1 is free
-    if (issued < klast && issued + 1 == k - 1 + S) {
-      if (threadIdx.x == 0)
-        issue(issued + 1);
-      ++issued;
-    }
+    // plane k - 1 is no longer needed by this warp
+    __syncwarp();
+    if (lane == 0)
+      mbar_arrive(&empty[slot_of(k - 1)]);
   }
 }
 
@@ -327,7 +385,7 @@ StreamShape stream_shape(const Dims &d, int resident_ctas) {
 }
 template <typename T> size_t stream_smem_bytes(const StreamShape &sh) {
   return (size_t)StreamCfg<T>::S * sh.slot +
-         StreamCfg<T>::S * sizeof(uint64_t);
+         2 * StreamCfg<T>::S * sizeof(uint64_t);
 }
 inline unsigned stream_grid(const Dims &d, const StreamShape &sh) {
   return (unsigned)sh.nj * cdiv(d.nz - 2, sh.kchunk);
