@@ -346,7 +346,8 @@ def phase_bytes(p, level: int, phase: str, esz: int,
 
 
 # kernel launched by a cycle phase, and launches per phase occurrence
-def phase_kernel(p, level: int, phase: str, coded: bool = False):
+def phase_kernel(p, level: int, phase: str, coded: bool = False,
+                 streamed: bool = False):
     if phase in ("pre-smooth", "post-smooth"):
         if level < p.nlev:
             # the mixed path's padded float levels stage their tiles by
@@ -354,13 +355,18 @@ def phase_kernel(p, level: int, phase: str, coded: bool = False):
             return ("gs27_tma_kernel" if p.precision == "mixed"
                     else "gs27_phase_kernel", 4)
         # the refinement paths' finest level is colour-split (and coded
-        # when its couplings have two values per direction)
+        # when its couplings have two values per direction); its colour
+        # passes stream their rows through shared memory
         if p.precision != "fp64":
+            if streamed:
+                return ("gs7_stream_kernel", 4)
             return ("gs7_code_color_kernel" if coded
                     else "gs7_split_color_kernel", 4)
         return ("gs7_color_kernel", 4)
     if phase == "defect" and level == p.nlev and coded:
         return ("defect7_code_kernel", 1)
+    if phase == "residual" and streamed:
+        return ("defect_norm_stream_kernel", 1)
     if phase == "residual" and coded:
         return ("defect_norm_code_kernel", 1)
     return {"residual": ("defect_norm_kernel", 1),
@@ -805,7 +811,9 @@ def main():
     coded = args.precision != "fp64" and p.coded_couplings()
     phases = profile_solve(p, step, dev, esz, coded)
     dom = next(r for r in phases if r["gbs"])
-    kname, klaunches = phase_kernel(p, dom["level"], dom["phase"], coded)
+    streamed = args.precision != "fp64" and p.finest_streamed()
+    kname, klaunches = phase_kernel(p, dom["level"], dom["phase"], coded,
+                                    streamed)
     roofline = {"bound": "hbm",
                 "kernel": (f"{kname} x{klaunches}: level {dom['level']} "
                            f"{dom['phase']}"),
@@ -818,7 +826,8 @@ def main():
                 "bytes_basis": (
                     "coded operator: per point one code byte (couplings and "
                     "oC), f, x"
-                    if coded and kname and "code" in kname else
+                    if coded and kname and ("code" in kname or
+                                            "stream" in kname) else
                     "coefficient arrays as stored (kernel table)"),
                 "algorithmic_bytes_per_launch": dom["bytes"],
                 "avg_launch_us": dom["us_avg"]}

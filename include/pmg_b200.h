@@ -672,6 +672,11 @@ int pmg_problem_set_coded_couplings(pmg_problem *p, int on);
 /* *coded = 1 when the built mixed problem's finest couplings are coded and
  * in use. Synchronises the problem's stream. */
 int pmg_problem_coded_couplings(pmg_problem *p, int *coded);
+/* *streamed = 1 when the problem's finest colour passes and refinement
+ * residual stream their rows through shared memory (mixed and fp64-fast
+ * problems created with pmg_set_finest_streaming on, levels that fit the
+ * stage ring). No reference counterpart. */
+int pmg_problem_finest_streamed(pmg_problem *p, int *streamed);
 
 /* on != 0: choose kernels for many solves sharing the GPU rather than for
  * the latency of this one: the mixed path's lowest levels run in one CTA

@@ -126,6 +126,7 @@ _sig("pmg_set_finest_streaming", c_int, c_int)
 _sig("pmg_test_tma_short_delivery", c_int, c_int)
 _sig("pmg_problem_set_coded_couplings", c_int, _V, c_int)
 _sig("pmg_problem_coded_couplings", c_int, _V, PI)
+_sig("pmg_problem_finest_streamed", c_int, _V, PI)
 _sig("pmg_problem_set_throughput_mode", c_int, _V, c_int)
 _sig("pmg_solve_start", c_int, _V, c_double, c_int)
 _sig("pmg_solve_poll", c_int, _V, PI)

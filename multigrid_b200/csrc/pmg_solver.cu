@@ -16,6 +16,7 @@
 #include "gs27_tiled.cuh"
 #include "gs27_tma.cuh"
 #include "gs7_stream.cuh"
+#include "resid_stream.cuh"
 
 #include <cudaTypedefs.h>
 #include "launch.cuh"
@@ -155,7 +156,8 @@ struct SolveState {
   int max_cycles;
   int cycles;
   // 0 running / converged / capped, 1 diverged, 2 r0 not finite, 3 a
-  // staged copy (27-point smoother, streamed finest pass) did not arrive
+  // staged copy (27-point smoother, streamed finest pass or residual) did
+  // not arrive
   int status;
   int pad;
   double r0, r;
@@ -177,7 +179,8 @@ struct pmg_problem {
   LevelBuf lv[kMaxLevels + 1];
   double *cg_r = nullptr, *cg_p = nullptr, *cg_ap = nullptr;
   int *cg_status = nullptr;
-  // device: set by gs27_tma_kernel and gs7_stream_kernel on a lost stage
+  // device: set by the staged kernels (gs27_tma_kernel, gs7_stream_kernel,
+  // defect_norm_stream_kernel) on a lost stage
   int *kernel_err = nullptr;
   int num_sms = 0;
   // Relative stopping threshold of the coarsest CG on the mixed path's
@@ -319,6 +322,8 @@ void plan(pmg_problem *p, Arena &a) {
   // reductions, and the damping on any coarse level
   const dim3 gf = reduce_grid(p->lv[p->nlev].d);
   long blocks = (long)gf.x * gf.y * gf.z;
+  // the streamed refinement residual's CTAs (resid_stream.cuh)
+  blocks = std::max(blocks, resid_max_ctas(p->lv[p->nlev].d));
   for (int L = 1; L < p->nlev; ++L) {
     const dim3 g = lambda_grid(p->lv[L].d);
     blocks = std::max(blocks, (long)g.x * g.y * g.z);
@@ -841,7 +846,22 @@ int refine_residual_async(pmg_problem *p, bool to_host = true) {
   const dim3 g = reduce_grid(v.d), b = interior_block();
   cudaStream_t s = p->stream;
   prof_begin(p, kPhResidual);
-  if (p->precision == PMG_PREC_MIXED) {
+  // the streamed residual (resid_stream.cuh) on the problems whose colour
+  // passes stream; the same r, the sum of squares in another fixed order
+  const bool streamed = p->use_codes && p->stream_fine && resid_fits(v.d);
+  if (streamed && p->precision == PMG_PREC_MIXED) {
+    int rc = launch_resid_stream<float>(
+        v.d, v.A64(4), v.f, v.x, v.code, v.lut64, v.octab64, v.code_info,
+        v.f32, p->red_norm, p->kernel_err, g_tma_extra_tx.load(), s);
+    if (rc)
+      return rc;
+  } else if (streamed) {
+    int rc = launch_resid_stream<double>(
+        v.d, v.A64(4), v.f, v.x, v.code, v.lut64, v.octab64, v.code_info,
+        v.fs, p->red_norm, p->kernel_err, g_tma_extra_tx.load(), s);
+    if (rc)
+      return rc;
+  } else if (p->precision == PMG_PREC_MIXED) {
     if (p->use_codes)
       defect_norm_code_kernel<double, float><<<g, b, 0, s>>>(
           v.d, v.A64(4), v.f, v.x, v.code, v.lut64, v.octab64, v.code_info,
@@ -967,16 +987,19 @@ __global__ void solve_params_kernel(SolveState *st, double tol,
 }
 
 __global__ void solve_init_kernel(SolveState *st, const double *sum,
-                                  double n3, cudaGraphConditionalHandle h) {
+                                  double n3, const int *kernel_err,
+                                  cudaGraphConditionalHandle h) {
   const double r0 = sqrt(sum[0] / n3);
   st->r0 = r0;
   st->r = r0;
   st->hist[0] = r0;
   const bool finite = isfinite(r0);
-  st->status = finite ? 0 : 2;
-  cudaGraphSetConditional(h, (finite && r0 > 0.0 && st->max_cycles > 0)
-                                 ? 1u
-                                 : 0u);
+  // a staged copy of the initial residual that did not arrive leaves its
+  // sum incomplete: no cycle runs, the solve reports the lost stage
+  const bool lost = *kernel_err != 0;
+  st->status = lost ? 3 : finite ? 0 : 2;
+  cudaGraphSetConditional(
+      h, (!lost && finite && r0 > 0.0 && st->max_cycles > 0) ? 1u : 0u);
 }
 
 __global__ void solve_check_kernel(SolveState *st, const double *sum,
@@ -1116,8 +1139,8 @@ int ensure_solve_graph(pmg_problem *p) {
                     : residual_norm_async(p, false);
     if (rc)
       return rc;
-    solve_init_kernel<<<1, 1, 0, p->stream>>>(p->d_state,
-                                              p->red_norm.result, n3, h);
+    solve_init_kernel<<<1, 1, 0, p->stream>>>(
+        p->d_state, p->red_norm.result, n3, p->kernel_err, h);
     PMG_LAUNCH_CHECK();
     return PMG_OK;
   };
@@ -1501,6 +1524,13 @@ int pmg_problem_coded_couplings(pmg_problem *p, int *coded) {
   return PMG_OK;
 }
 
+int pmg_problem_finest_streamed(pmg_problem *p, int *streamed) {
+  if (!p || !streamed)
+    return PMG_ERR_ARG;
+  *streamed = p->stream_fine && p->use_codes;
+  return PMG_OK;
+}
+
 int pmg_problem_set_throughput_mode(pmg_problem *p, int on) {
   if (!p)
     return PMG_ERR_ARG;
@@ -1800,9 +1830,9 @@ static int solve_host_loop(pmg_problem *p, double tol, int max_cycles,
   PMG_CUDA_TRY(cudaMemcpy(&lost, p->kernel_err, sizeof(int),
                           cudaMemcpyDeviceToHost));
   if (rc == PMG_OK && lost) {
-    set_last_message("pmg_solve: a staged copy (27-point smoother or "
-                     "streamed finest pass) did not arrive (bounded wait "
-                     "ran out)");
+    set_last_message("pmg_solve: a staged copy (27-point smoother, "
+                     "streamed finest pass or residual) did not arrive "
+                     "(bounded wait ran out)");
     rc = PMG_ERR_TIMEOUT;
   }
   return rc;
@@ -1884,9 +1914,9 @@ int pmg_solve_finish(pmg_problem *p, int *cycles, double *relres,
     return PMG_ERR_DIVERGED;
   }
   if (st.status == 3) {
-    set_last_message("pmg_solve: a staged copy (27-point smoother or "
-                     "streamed finest pass) did not arrive (bounded wait "
-                     "ran out)");
+    set_last_message("pmg_solve: a staged copy (27-point smoother, "
+                     "streamed finest pass or residual) did not arrive "
+                     "(bounded wait ran out)");
     return PMG_ERR_TIMEOUT;
   }
   return PMG_OK;

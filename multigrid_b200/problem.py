@@ -249,6 +249,15 @@ class PBELinearProblem:
                                                         ctypes.byref(c)))
         return bool(c.value)
 
+    def finest_streamed(self) -> bool:
+        """Whether the finest colour passes and refinement residual stream
+        their rows through shared memory (pmg_problem_finest_streamed)."""
+        c = ctypes.c_int()
+        _lib.check("pmg_problem_finest_streamed",
+                   _lib.lib.pmg_problem_finest_streamed(self._h,
+                                                        ctypes.byref(c)))
+        return bool(c.value)
+
     def set_profiling(self, on: bool = True) -> None:
         """Time every cycle phase with CUDA events inside the cycle graph."""
         _lib.check("pmg_problem_set_profiling",
