@@ -17,6 +17,7 @@
 #include "gs27_tma.cuh"
 #include "gs7_stream.cuh"
 #include "resid_stream.cuh"
+#include "defect_stream.cuh"
 
 #include <cudaTypedefs.h>
 #include "launch.cuh"
@@ -50,6 +51,10 @@ struct LevelBuf {
   // the refinement paths' finest level: tensor maps of the colour-split
   // correction, right-hand side and code bytes (the streamed colour pass)
   StreamMaps smaps;
+  // the same arrays in boxes of both colour halves (the streamed defect,
+  // defect_stream.cuh); dmaps_ok when they could be made
+  StreamMaps dmaps;
+  bool dmaps_ok = false;
   double *op[14] = {};
   double *P[27] = {}; // prolongation from this level to level+1
   double *x = nullptr, *f = nullptr, *r = nullptr;
@@ -566,10 +571,11 @@ void encode_tma_maps(pmg_problem *p) {
 }
 
 // A 4-D map {entry, half, row, plane} of one colour-split array of the
-// level (split_layout.cuh): boxes of bw entries of one half over `rows`
-// rows of one plane.
+// level (split_layout.cuh): boxes of bw entries of one half (or of both)
+// over `rows` rows of one plane.
 bool encode_split_map(CUtensorMap *m, const void *base, CUtensorMapDataType t,
-                      int esz, const Dims &d, int bw, int rows) {
+                      int esz, const Dims &d, int bw, int rows,
+                      int halves = 1) {
   auto enc = tensor_map_encoder();
   if (!enc || !base || ((uintptr_t)base & 15) != 0)
     return false;
@@ -579,7 +585,8 @@ bool encode_split_map(CUtensorMap *m, const void *base, CUtensorMapDataType t,
   const cuuint64_t strides[3] = {(cuuint64_t)sp.hp * esz,
                                  (cuuint64_t)sp.pitch() * esz,
                                  (cuuint64_t)sp.plane() * esz};
-  const cuuint32_t box[4] = {(cuuint32_t)bw, 1, (cuuint32_t)rows, 1};
+  const cuuint32_t box[4] = {(cuuint32_t)bw, (cuuint32_t)halves,
+                             (cuuint32_t)rows, 1};
   const cuuint32_t elem[4] = {1, 1, 1, 1};
   return enc(m, t, 4, const_cast<void *>(base), dims, strides, box, elem,
              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -600,6 +607,15 @@ bool encode_stream_maps(LevelBuf &v, const T *x, const T *f) {
   const CUtensorMapDataType t = sizeof(T) == 4
                                     ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
                                     : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+  if (defect_fits<T>(v.d)) {
+    const StreamShape ds = defect_shape<T>(v.d, 1);
+    constexpr int JD = DefectCfg<T>::J;
+    v.dmaps_ok =
+        encode_split_map(&v.dmaps.x, x, t, sizeof(T), v.d, ds.bw, JD + 2, 2) &&
+        encode_split_map(&v.dmaps.f, f, t, sizeof(T), v.d, ds.bw, JD, 2) &&
+        encode_split_map(&v.dmaps.code, v.code, CU_TENSOR_MAP_DATA_TYPE_UINT8,
+                         1, v.d, ds.bwc, JD, 2);
+  }
   return encode_split_map(&v.smaps.x, x, t, sizeof(T), v.d, sh.bw, J + 2) &&
          encode_split_map(&v.smaps.f, f, t, sizeof(T), v.d, sh.bw, J) &&
          encode_split_map(&v.smaps.code, v.code,
@@ -771,7 +787,17 @@ template <typename T> int vcycle_ref(pmg_problem *p, int L) {
     return rc;
   prof_end(p, sl + kPhPre);
   prof_begin(p, sl + kPhDefect);
-  if (kind == 7 && p->use_codes)
+  if (kFloat && kind == 7 && p->use_codes && p->stream_fine && v.dmaps_ok &&
+      x == A::x(v)) {
+    // streamed (defect_stream.cuh): the maps cover the level's own arrays;
+    // float only (the double version, two CTAs per SM, was slower than the
+    // per-thread kernel: 114 against 110 us at 257^3)
+    if ((rc = launch_defect7_stream<T>(
+             v.dmaps, v.d, A::fine_op(v, kOC), A::fine_op(v, kOE),
+             A::fine_op(v, kON), A::fine_op(v, kUC), v.code_info, A::lut(v),
+             A::octab(v), A::r(v), p->kernel_err, g_tma_extra_tx.load(), s)))
+      return rc;
+  } else if (kind == 7 && p->use_codes)
     defect7_code_kernel<T>
         <<<defect7_code_grid(v.d), interior_block(), 0, s>>>(
             v.d, A::fine_op(v, kOC), A::fine_op(v, kOE), A::fine_op(v, kON),
