@@ -490,11 +490,13 @@ def test_tma_stage_wait_runs_out_and_reports(pb65):
 @pytest.mark.parametrize("precision", ["mixed", "fp64-fast"])
 @pytest.mark.parametrize("name", ["pb49", "pb65", "pb161", "pb257"])
 def test_streamed_finest_pass_gives_the_same_bits(name, precision):
-    """The refinement paths' finest colour passes with the level's rows
-    streamed through shared memory by bulk copies (row blocks of 8, planes
-    in chunks that fill the GPU once) against the per-point-load pass: the
+    """The refinement paths' finest colour passes, defect (mixed) and
+    refinement residual with the level's rows streamed through shared memory
+    by tensor-map boxes and bulk copies (row blocks of 8 or 4, planes in
+    chunks that fill the GPU once) against the per-point-load kernels: the
     same cycles and the same potential, bit for bit. 49^3 leaves a last row
-    block of 7 rows; 161^3 and 257^3 are the benchmark grids."""
+    block of 7 rows (3 for blocks of 4); 161^3 and 257^3 are the benchmark
+    grids."""
     from multigrid_b200.molecule import Workload
     from multigrid_b200.problem import set_finest_streaming
     w = (Workload("pb49", 3, 4, 0.5, 300, 8.0, 5) if name == "pb49"
@@ -509,6 +511,7 @@ def test_streamed_finest_pass_gives_the_same_bits(name, precision):
                 p.set_fine(**fine)
                 p.buildmultilevelops()
                 assert p.coded_couplings()
+                assert p.finest_streamed() == on
                 r = p.solve(tol=1e-10, max_cycles=100)
                 assert r.relres < 1e-10
                 out[on] = (r.cycles, p.potential().ravel().copy())
