@@ -22,6 +22,7 @@
 #include <cudaTypedefs.h>
 #include "launch.cuh"
 #include "pcg_kernels.cuh"
+#include "pcg_split.cuh"
 #include "split_layout.cuh"
 #include "reduce_kernels.cuh"
 
@@ -1292,6 +1293,20 @@ int ensure_pcg_graph(pmg_problem *p) {
   const size_t b = sizeof(double) * v.n3;
   auto &c = p->pcg;
   const dim3 rg = reduce_grid(v.d), rb = interior_block();
+  const bool mixed = p->precision == PMG_PREC_MIXED;
+  const bool split = p->precision != PMG_PREC_FP64;
+  // the refinement paths' finest operator as code bytes (pcg_split.cuh);
+  // the device flags say whether the coding holds
+  const bool coded = split && p->use_codes;
+  auto matvec = [&]() {
+    if (coded)
+      pcg_matvec_dot_code_kernel<<<rg, rb, 0, s>>>(
+          v.d, v.A64(4), v.code, v.lut64, v.octab64, v.code_info, c.pv, c.ap,
+          c.pap);
+    else
+      pcg_matvec_dot_kernel<<<rg, rb, 0, s>>>(v.d, v.A64(4), c.pv, c.ap,
+                                              c.pap);
+  };
   auto head = [&](cudaGraphConditionalHandle h) -> int {
     PMG_CUDA_TRY(cudaMemcpyAsync(c.xs, v.x, b, cudaMemcpyDeviceToDevice, s));
     PMG_CUDA_TRY(cudaMemcpyAsync(c.b, v.f, b, cudaMemcpyDeviceToDevice, s));
@@ -1303,25 +1318,45 @@ int ensure_pcg_graph(pmg_problem *p) {
       return rc;
     PMG_CUDA_TRY(cudaMemcpyAsync(c.pv, c.z, b, cudaMemcpyDeviceToDevice, s));
     pcg_dot_kernel<<<rg, rb, 0, s>>>(v.d, c.r, c.z, c.rz);
-    pcg_matvec_dot_kernel<<<rg, rb, 0, s>>>(v.d, v.A64(4), c.pv, c.ap,
-                                            c.pap);
+    matvec();
     pcg_init_kernel<<<1, 1, 0, s>>>(c.d_st, c.rr.result, c.rz.result,
                                     c.pap.result, n3, h);
     PMG_LAUNCH_CHECK();
     return PMG_OK;
   };
   auto body = [&](cudaGraphConditionalHandle h) -> int {
-    pcg_update_xr_kernel<<<rg, rb, 0, s>>>(v.d, c.pv, c.ap, c.xs, c.r,
-                                           c.d_st, c.rr);
-    PMG_LAUNCH_CHECK();
-    int rc = precondition(p, c.r, c.z);
-    if (rc)
-      return rc;
-    pcg_dot_kernel<<<rg, rb, 0, s>>>(v.d, c.r, c.z, c.rz);
+    int rc;
+    if (split) {
+      // r and the split right-hand side in one pass, the V-cycle, then z
+      // from the split correction inside r.z
+      if (mixed)
+        pcg_update_xr_split_kernel<float><<<rg, rb, 0, s>>>(
+            v.d, c.pv, c.ap, c.xs, c.r, v.f32, c.d_st, c.rr);
+      else
+        pcg_update_xr_split_kernel<double><<<rg, rb, 0, s>>>(
+            v.d, c.pv, c.ap, c.xs, c.r, v.fs, c.d_st, c.rr);
+      PMG_LAUNCH_CHECK();
+      rc = mixed ? vcycle_ref<float>(p, p->nlev)
+                 : vcycle_ref<double>(p, p->nlev);
+      if (rc)
+        return rc;
+      if (mixed)
+        pcg_dot_split_kernel<float>
+            <<<rg, rb, 0, s>>>(v.d, c.r, v.x32, c.z, c.rz);
+      else
+        pcg_dot_split_kernel<double>
+            <<<rg, rb, 0, s>>>(v.d, c.r, v.xs, c.z, c.rz);
+    } else {
+      pcg_update_xr_kernel<<<rg, rb, 0, s>>>(v.d, c.pv, c.ap, c.xs, c.r,
+                                             c.d_st, c.rr);
+      PMG_LAUNCH_CHECK();
+      if ((rc = precondition(p, c.r, c.z)))
+        return rc;
+      pcg_dot_kernel<<<rg, rb, 0, s>>>(v.d, c.r, c.z, c.rz);
+    }
     pcg_beta_kernel<<<1, 1, 0, s>>>(c.d_st, c.rz.result);
     pcg_update_p_kernel<<<rg, rb, 0, s>>>(v.d, c.z, c.pv, c.d_st);
-    pcg_matvec_dot_kernel<<<rg, rb, 0, s>>>(v.d, v.A64(4), c.pv, c.ap,
-                                            c.pap);
+    matvec();
     pcg_check_kernel<<<1, 1, 0, s>>>(c.d_st, c.pap.result, c.rr.result, n3,
                                      h);
     PMG_LAUNCH_CHECK();
