@@ -318,7 +318,9 @@ def phase_bytes(p, level: int, phase: str, esz: int,
     fine = level == p.nlev
     nc3 = float(level_n(p.base, level - 1) ** 3) if level >= 2 else 0.0
     if level == 0:
-        if phase == "residual" and coded:  # code byte, f, x; split r
+        # the refinement paths' residual reads the code byte and writes the
+        # split right-hand side; FP64's stop-test norm reads the arrays
+        if phase == "residual" and coded and p.precision != "fp64":
             return nf3 * (2 * 8 + 1 + (4 if p.precision == "mixed" else 8))
         if phase == "residual":  # 4 coefficients + f + x in double
             return nf3 * (6 * 8 + (4 if p.precision == "mixed" else 0))
@@ -357,11 +359,12 @@ def phase_kernel(p, level: int, phase: str, coded: bool = False,
         # the refinement paths' finest level is colour-split (and coded
         # when its couplings have two values per direction); its colour
         # passes stream their rows through shared memory
+        if streamed:
+            return ("gs7_stream_kernel", 4)
+        if coded:
+            return ("gs7_code_color_kernel", 4)
         if p.precision != "fp64":
-            if streamed:
-                return ("gs7_stream_kernel", 4)
-            return ("gs7_code_color_kernel" if coded
-                    else "gs7_split_color_kernel", 4)
+            return ("gs7_split_color_kernel", 4)
         return ("gs7_color_kernel", 4)
     if phase == "defect" and level == p.nlev and coded:
         return ("defect7_code_kernel", 1)
@@ -812,10 +815,10 @@ def main():
     # roofline
     peak, peak_kind = peaks()
     esz = 4 if args.precision == "mixed" else 8
-    coded = args.precision != "fp64" and p.coded_couplings()
+    coded = p.coded_couplings()
     phases = profile_solve(p, step, dev, esz, coded)
     dom = next(r for r in phases if r["gbs"])
-    streamed = args.precision != "fp64" and p.finest_streamed()
+    streamed = p.finest_streamed()
     kname, klaunches = phase_kernel(p, dom["level"], dom["phase"], coded,
                                     streamed)
     roofline = {"bound": "hbm",

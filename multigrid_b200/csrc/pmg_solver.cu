@@ -241,6 +241,16 @@ struct pmg_problem {
 
 namespace {
 
+// pmg_set_tma_staging: problems created while it is off use gs27_tiled.cuh
+// on every level (the same bits)
+std::atomic<int> g_tma_on{1};
+bool tma_disabled() { return g_tma_on.load() == 0; }
+// pmg_set_finest_streaming: problems created while it is off use the
+// per-point-load colour pass (gs7_code_color_kernel) on the finest level
+std::atomic<int> g_stream_on{1};
+// pmg_test_tma_short_delivery: extra bytes every stage waits for
+std::atomic<unsigned> g_tma_extra_tx{0};
+
 int level_n(int base, int L) { return base * (1 << L) + 1; }
 
 // Mixed path: the top level of the one-launch bottom cycle (the levels up
@@ -258,7 +268,11 @@ int bottom_top_of(int base, int nlev, int precision) {
 // counts bytes.
 void plan(pmg_problem *p, Arena &a) {
   const bool mixed = p->precision == PMG_PREC_MIXED;
-  const bool fast = p->precision == PMG_PREC_FP64_FAST;
+  // the finest level's colour-split double copies and code bytes: fp64-fast
+  // (its correction equation) and FP64 (the class's cycle on split copies
+  // of x and f, converted at the level's V-cycle)
+  const bool fast = p->precision == PMG_PREC_FP64_FAST ||
+                    p->precision == PMG_PREC_FP64;
   const int bottom_top = bottom_top_of(p->base, p->nlev, p->precision);
   for (int L = 1; L <= p->nlev; ++L) {
     LevelBuf &v = p->lv[L];
@@ -405,6 +419,17 @@ void prof_collect(pmg_problem *p) {
 int smooth64(pmg_problem *p, int L, int nsweeps, int zero_init,
              double **cur) {
   LevelBuf &v = p->lv[L];
+  if (L == p->nlev && *cur == v.xs) { // the split coded copies
+    if (p->stream_fine)
+      return launch_gs7_stream<double>(
+          v.smaps, v.d, v.ops[kOC], v.ops[kOE], v.ops[kON], v.ops[kUC],
+          v.code_info, v.lut64, v.octab64, v.xs, nsweeps, 0, zero_init,
+          p->kernel_err, g_tma_extra_tx.load(), p->stream);
+    return launch_gs7_code<double>(v.d, v.ops[kOC], v.fs, v.ops[kOE],
+                                   v.ops[kON], v.ops[kUC], v.code,
+                                   v.code_info, v.lut64, v.octab64, v.xs,
+                                   nsweeps, 0, zero_init, p->stream);
+  }
   if (L == p->nlev)
     return launch_gs7<double>(v.d, v.op[kOC], nullptr, v.f, v.op[kOE],
                               v.op[kON], v.op[kUC], *cur, nsweeps, 0,
@@ -442,14 +467,31 @@ int vcycle64(pmg_problem *p, int L, int as_preconditioner) {
   LevelBuf &c = p->lv[L - 1];
   const int kind = L == p->nlev ? 7 : 27;
   int rc;
-  double *x = v.x;
+  // the finest level runs on its colour-split coded copies (the kernels of
+  // the refinement paths, the class's per-point arithmetic: the same bits);
+  // x and f are converted at the level's V-cycle (f each time: the
+  // preconditioner's right-hand side changes per call)
+  const bool split = kind == 7 && p->use_codes && v.xs != nullptr;
+  double *x = split ? v.xs : v.x;
   const int zero_init = (L != p->nlev) || as_preconditioner;
+  if (split) {
+    to_split_kernel<double, double><<<flat_grid(v.n3), 256, 0, s>>>(v.d, v.f,
+                                                                    v.fs);
+    to_split_kernel<double, double><<<flat_grid(v.n3), 256, 0, s>>>(v.d, v.x,
+                                                                    v.xs);
+    PMG_LAUNCH_CHECK();
+  }
   prof_begin(p, sl + kPhPre);
   if ((rc = smooth64(p, L, 2, zero_init, &x)))
     return rc;
   prof_end(p, sl + kPhPre);
   prof_begin(p, sl + kPhDefect);
-  if (kind == 7)
+  if (split)
+    defect7_code_kernel<double>
+        <<<defect7_code_grid(v.d), interior_block(), 0, s>>>(
+            v.d, v.ops[kOC], v.ops[kOE], v.ops[kON], v.ops[kUC], v.code,
+            v.code_info, v.lut64, v.octab64, v.fs, x, v.r);
+  else if (kind == 7)
     defect_kernel<7, double><<<interior_grid(v.d), interior_block(), 0, s>>>(
         v.d, v.A64(4), v.f, x, v.r);
   else
@@ -471,18 +513,28 @@ int vcycle64(pmg_problem *p, int L, int as_preconditioner) {
   prof_end(p, sl + kPhLambda);
   // x += w * (interpolated correction), one pass
   prof_begin(p, sl + kPhInterp);
-  interp_add_kernel<double, false>
-      <<<interp_grid(c.d), interior_block(), 0, s>>>(c.d, v.d, c.x, c.Pc(), x,
-                                                     c.omega);
+  if (split)
+    interp_add_kernel<double, true>
+        <<<interp_grid(c.d), interior_block(), 0, s>>>(c.d, v.d, c.x, c.Pc(),
+                                                       x, c.omega);
+  else
+    interp_add_kernel<double, false>
+        <<<interp_grid(c.d), interior_block(), 0, s>>>(c.d, v.d, c.x, c.Pc(),
+                                                       x, c.omega);
   prof_end(p, sl + kPhInterp);
   PMG_LAUNCH_CHECK();
   prof_begin(p, sl + kPhPost);
   if ((rc = smooth64(p, L, 2, 0, &x)))
     return rc;
   prof_end(p, sl + kPhPost);
-  if (x != v.x) {
+  if (x != (split ? v.xs : v.x)) {
     set_last_message("vcycle64: iterate left the level's buffer");
     return PMG_ERR_STATE;
+  }
+  if (split) {
+    from_split_kernel<double, double><<<flat_grid(v.n3), 256, 0, s>>>(
+        v.d, v.xs, v.x);
+    PMG_LAUNCH_CHECK();
   }
   return PMG_OK;
 }
@@ -511,15 +563,6 @@ double norm_from_sum(const pmg_problem *p, double s) {
 
 // ---- the 27-point smoother by tensor-memory access (gs27_tma.cuh) -----------
 
-// pmg_set_tma_staging: problems created while it is off use gs27_tiled.cuh
-// on every level (the same bits)
-std::atomic<int> g_tma_on{1};
-bool tma_disabled() { return g_tma_on.load() == 0; }
-// pmg_set_finest_streaming: problems created while it is off use the
-// per-point-load colour pass (gs7_code_color_kernel) on the finest level
-std::atomic<int> g_stream_on{1};
-// pmg_test_tma_short_delivery: extra bytes every stage waits for
-std::atomic<unsigned> g_tma_extra_tx{0};
 
 PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
@@ -626,9 +669,7 @@ bool stream_fine_ok(pmg_problem *p) {
   LevelBuf &v = p->lv[p->nlev];
   if (p->precision == PMG_PREC_MIXED)
     return encode_stream_maps<float>(v, v.x32, v.f32);
-  if (p->precision == PMG_PREC_FP64_FAST)
-    return encode_stream_maps<double>(v, v.xs, v.fs);
-  return false;
+  return encode_stream_maps<double>(v, v.xs, v.fs);
 }
 
 // nsweeps eight-colour sweeps of a padded float level (launch_gs27_pp's
@@ -1573,13 +1614,14 @@ int pmg_problem_coded_couplings(pmg_problem *p, int *coded) {
     return PMG_ERR_ARG;
   *coded = 0;
   const LevelBuf &v = p->lv[p->nlev];
-  if (!p->built || p->precision == PMG_PREC_FP64 || !p->use_codes)
+  if (!p->built || !p->use_codes)
     return PMG_OK;
   int flag[2] = {1, 1};
   PMG_CUDA_TRY(cudaMemcpyAsync(flag, v.code_info + 6, sizeof(flag),
                                cudaMemcpyDeviceToHost, p->stream));
   PMG_CUDA_TRY(cudaStreamSynchronize(p->stream));
-  // the float coding; fp64-fast also needs the double couplings to match
+  // the float coding; the double paths also need the double couplings to
+  // match
   *coded = flag[0] == 0 &&
            (p->precision == PMG_PREC_MIXED || flag[1] == 0);
   return PMG_OK;
@@ -1754,8 +1796,9 @@ int pmg_build_hierarchy(pmg_problem *p, int trilinear) {
       }
     PMG_LAUNCH_CHECK();
   }
-  if (p->precision == PMG_PREC_FP64_FAST) {
-    // the finest double operator split by colour, and its coded couplings
+  if (p->precision != PMG_PREC_MIXED) {
+    // fp64-fast and FP64: the finest double operator split by colour, and
+    // its coded couplings
     // (classified by their float values, then checked bit for bit in
     // double: info[7] keeps the arrays in use when they do not match)
     LevelBuf &v = p->lv[p->nlev];

@@ -315,11 +315,13 @@ def test_throughput_mode_same_solve_within_tolerance(pb65):
     assert np.linalg.norm(x1 - x0) <= 1e-9 * np.linalg.norm(x0)
 
 
-@pytest.mark.parametrize("precision", ["mixed", "fp64-fast"])
+@pytest.mark.parametrize("precision", ["mixed", "fp64-fast", "fp64"])
 def test_coded_couplings_give_the_same_bits(pb65, precision):
     """The class's fine operator has two coupling values per direction, so
-    the finest smoother and defect of the refinement paths read code bytes;
-    the solve is bit-identical to the one reading the coupling arrays. An
+    the finest smoother and defect read code bytes (on the refinement paths'
+    correction and on the FP64 cycle's colour-split copies of x and f); the
+    solve is bit-identical to the one reading the coupling arrays (for FP64:
+    the reference layout's kernels). An
     operator with more values per direction is not coded and solves the
     same with the switch on or off; so does one whose double couplings take
     a third value that rounds to a float table value (coded for the float
@@ -487,7 +489,7 @@ def test_tma_stage_wait_runs_out_and_reports(pb65):
     assert np.array_equal(after[1], before[1])
 
 
-@pytest.mark.parametrize("precision", ["mixed", "fp64-fast"])
+@pytest.mark.parametrize("precision", ["mixed", "fp64-fast", "fp64"])
 @pytest.mark.parametrize("name", ["pb49", "pb65", "pb161", "pb257"])
 def test_streamed_finest_pass_gives_the_same_bits(name, precision):
     """The refinement paths' finest colour passes, defect (mixed) and
