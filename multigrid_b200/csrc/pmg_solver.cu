@@ -544,9 +544,19 @@ int vcycle64(pmg_problem *p, int L, int as_preconditioner) {
 int residual_norm_async(pmg_problem *p, bool to_host = true) {
   LevelBuf &v = p->lv[p->nlev];
   prof_begin(p, kPhResidual);
-  defect_norm_kernel<7, double, double>
-      <<<reduce_grid(v.d), interior_block(), 0, p->stream>>>(
-          v.d, v.A64(4), v.f, v.x, (double *)nullptr, p->red_norm);
+  if (p->use_codes && p->stream_fine && resid_fits(v.d)) {
+    // the streamed coded residual, its sum only (resid_stream.cuh)
+    int rc = launch_resid_stream<double>(
+        v.d, v.A64(4), v.f, v.x, v.code, v.lut64, v.octab64, v.code_info,
+        (double *)nullptr, p->red_norm, p->kernel_err, g_tma_extra_tx.load(),
+        p->stream);
+    if (rc)
+      return rc;
+  } else {
+    defect_norm_kernel<7, double, double>
+        <<<reduce_grid(v.d), interior_block(), 0, p->stream>>>(
+            v.d, v.A64(4), v.f, v.x, (double *)nullptr, p->red_norm);
+  }
   prof_end(p, kPhResidual);
   PMG_LAUNCH_CHECK();
   if (to_host)

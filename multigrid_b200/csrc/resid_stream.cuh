@@ -3,7 +3,8 @@
 // Convolution.h:137-139, with the couplings and oC from the code bytes),
 // written rounded to the correction equation's colour-split right-hand side
 // (float or double), and its sum of squares (compute_residual_map,
-// Convolution.h:156-185).
+// Convolution.h:156-185). With r null only the sum: the FP64 cycle's stop
+// test.
 //
 // The per-thread kernel (defect_norm_code_kernel) moves the coded format's
 // 21 bytes per point and no more but is bound by load latency (ncu: long-
@@ -265,7 +266,8 @@ __global__ void __launch_bounds__(ResidCfg::THREADS, 2)
                               c[1] * xw - c[5] * xdn - c[4] * xup +
                               (oc + 0.0) * xcc;
             const double dv = fv - ax;
-            r[sp.at(i, jj, k)] = (R)dv;
+            if (r)
+              r[sp.at(i, jj, k)] = (R)dv;
             acc += dv * dv;
           }
         }
