@@ -8,6 +8,8 @@
 // rounding.
 #pragma once
 
+#include <utility>
+
 #include "pmg_common.cuh"
 
 namespace pmg {
@@ -115,9 +117,42 @@ __host__ __device__ constexpr int upper_dz(int s) {
   return (s == 3 || s >= 6) ? 1 : 0;
 }
 
+// The terms of Galerkin entry S that the fine neighbour f = c + (dx,dy,dz)
+// contributes: sum_e P_d(C) A_f(f, f+e) P_{d+e-2D}(C+D), added to acc in e
+// order, with A_f(f,f) = oC(f) and A_f(f,g) = -a(f,g) (VbuildG_7
+// pmgc/buildGd.cc:438-1361, VbuildG_27 :1364-3274).
+template <int KIND, int S>
+__device__ __forceinline__ void galerkin_terms(double &acc, const Dims &df,
+                                               const Dims &dc,
+                                               const P27<double> &P,
+                                               const Op14<double> &A, int pc,
+                                               int fp, double pw, int dx,
+                                               int dy, int dz) {
+  constexpr int Dx = upper_dx(S), Dy = upper_dy(S), Dz = upper_dz(S);
+  const int pn = pc + Dx + Dy * dc.sy() + Dz * dc.sz();
+#pragma unroll
+  for (int ez = -1; ez <= 1; ++ez)
+#pragma unroll
+    for (int ey = -1; ey <= 1; ++ey)
+#pragma unroll
+      for (int ex = -1; ex <= 1; ++ex) {
+        const int tx = dx + ex - 2 * Dx, ty = dy + ey - 2 * Dy,
+                  tz = dz + ez - 2 * Dz;
+        if (tx < -1 || tx > 1 || ty < -1 || ty > 1 || tz < -1 || tz > 1)
+          continue;
+        const int nnz = (ex != 0) + (ey != 0) + (ez != 0);
+        if (KIND == 7 && nnz > 1)
+          continue;
+        const double af = nnz == 0 ? A.a[kOC][fp]
+                                   : -coupling(A, df, fp, ex, ey, ez);
+        if (af == 0.0)
+          continue;
+        acc += pw * af * P.p[pslot(tx, ty, tz)][pn];
+      }
+}
+
 // One Galerkin entry: A_c(C, C+D) = sum_{d,e} P_d(C) A_f(c+d, c+d+e)
-// P_{d+e-2D}(C+D), with A_f(f,f) = oC(f) and A_f(f,g) = -a(f,g)
-// (VbuildG_7 pmgc/buildGd.cc:438-1361, VbuildG_27 :1364-3274). Returns the
+// P_{d+e-2D}(C+D), the fine neighbours d in (z, y, x) order. Returns the
 // stored value: A_c(C,C) for S = 0, -A_c(C,C+D) otherwise.
 template <int KIND, int S>
 __device__ __forceinline__ double galerkin_entry(const Dims &df,
@@ -125,8 +160,6 @@ __device__ __forceinline__ double galerkin_entry(const Dims &df,
                                                  const P27<double> &P,
                                                  const Op14<double> &A,
                                                  int pc, int c0) {
-  constexpr int Dx = upper_dx(S), Dy = upper_dy(S), Dz = upper_dz(S);
-  const int pn = pc + Dx + Dy * dc.sy() + Dz * dc.sz();
   const int sy = df.sy(), sz = df.sz();
   double acc = 0.0;
 #pragma unroll
@@ -136,32 +169,28 @@ __device__ __forceinline__ double galerkin_entry(const Dims &df,
 #pragma unroll
       for (int dx = -1; dx <= 1; ++dx) {
         const int fp = c0 + dx + dy * sy + dz * sz;
-        const double pw = P.p[pslot(dx, dy, dz)][pc];
-#pragma unroll
-        for (int ez = -1; ez <= 1; ++ez)
-#pragma unroll
-          for (int ey = -1; ey <= 1; ++ey)
-#pragma unroll
-            for (int ex = -1; ex <= 1; ++ex) {
-              const int tx = dx + ex - 2 * Dx, ty = dy + ey - 2 * Dy,
-                        tz = dz + ez - 2 * Dz;
-              if (tx < -1 || tx > 1 || ty < -1 || ty > 1 || tz < -1 || tz > 1)
-                continue;
-              const int nnz = (ex != 0) + (ey != 0) + (ez != 0);
-              if (KIND == 7 && nnz > 1)
-                continue;
-              const double af = nnz == 0 ? A.a[kOC][fp]
-                                         : -coupling(A, df, fp, ex, ey, ez);
-              if (af == 0.0)
-                continue;
-              acc += pw * af * P.p[pslot(tx, ty, tz)][pn];
-            }
+        galerkin_terms<KIND, S>(acc, df, dc, P, A, pc, fp,
+                                P.p[pslot(dx, dy, dz)][pc], dx, dy, dz);
       }
   return S == 0 ? acc : -acc;
 }
 
-// out32 (all null: none) receives the float copy of each entry (rows
-// dc32.px apart).
+template <int KIND, int... S>
+__device__ __forceinline__ void
+galerkin_terms_all(double *acc, const Dims &df, const Dims &dc,
+                   const P27<double> &P, const Op14<double> &A, int pc,
+                   int fp, double pw, int dx, int dy, int dz,
+                   std::integer_sequence<int, S...>) {
+  (galerkin_terms<KIND, S>(acc[S], df, dc, P, A, pc, fp, pw, dx, dy, dz),
+   ...);
+}
+
+// All fourteen entries of one coarse point, the fine neighbour d outermost:
+// each entry still adds its terms in galerkin_entry's (d, e) order, so the
+// values are the same bits, while P_d(C) and the fine operator around c + d
+// are loaded once for the fourteen instead of once per entry, and the
+// stores come after all loads. out32 (all null: none) receives the float
+// copy of each entry (rows dc32.px apart).
 template <int KIND>
 __global__ void __launch_bounds__(128)
     buildG_kernel(Dims df, Dims dc, P27<double> P, Op14<double> A,
@@ -173,72 +202,39 @@ __global__ void __launch_bounds__(128)
     return;
   const int pc = dc.at(ii, jj, kk);
   const int c0 = df.at(2 * ii - 1, 2 * jj - 1, 2 * kk - 1);
+  const int sy = df.sy(), sz = df.sz();
+  double acc[14];
+#pragma unroll
+  for (int s = 0; s < 14; ++s)
+    acc[s] = 0.0;
+#pragma unroll
+  for (int dz = -1; dz <= 1; ++dz)
+#pragma unroll
+    for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
+      for (int dx = -1; dx <= 1; ++dx) {
+        const int fp = c0 + dx + dy * sy + dz * sz;
+        galerkin_terms_all<KIND>(acc, df, dc, P, A, pc, fp,
+                                 P.p[pslot(dx, dy, dz)][pc], dx, dy, dz,
+                                 std::make_integer_sequence<int, 14>{});
+      }
   const bool f32 = out32.a[0] != nullptr; // the mixed path's float copy
   const int pc32 = dc32.at(ii, jj, kk);
-  double v;
-  v = galerkin_entry<KIND, 0>(df, dc, P, A, pc, c0);
-  out.a[0][pc] = v;
-  if (f32)
-    out32.a[0][pc32] = (float)v;
-  v = galerkin_entry<KIND, 1>(df, dc, P, A, pc, c0);
-  out.a[1][pc] = v;
-  if (f32)
-    out32.a[1][pc32] = (float)v;
-  v = galerkin_entry<KIND, 2>(df, dc, P, A, pc, c0);
-  out.a[2][pc] = v;
-  if (f32)
-    out32.a[2][pc32] = (float)v;
-  v = galerkin_entry<KIND, 3>(df, dc, P, A, pc, c0);
-  out.a[3][pc] = v;
-  if (f32)
-    out32.a[3][pc32] = (float)v;
-  v = galerkin_entry<KIND, 4>(df, dc, P, A, pc, c0);
-  out.a[4][pc] = v;
-  if (f32)
-    out32.a[4][pc32] = (float)v;
-  v = galerkin_entry<KIND, 5>(df, dc, P, A, pc, c0);
-  out.a[5][pc] = v;
-  if (f32)
-    out32.a[5][pc32] = (float)v;
-  v = galerkin_entry<KIND, 6>(df, dc, P, A, pc, c0);
-  out.a[6][pc] = v;
-  if (f32)
-    out32.a[6][pc32] = (float)v;
-  v = galerkin_entry<KIND, 7>(df, dc, P, A, pc, c0);
-  out.a[7][pc] = v;
-  if (f32)
-    out32.a[7][pc32] = (float)v;
-  v = galerkin_entry<KIND, 8>(df, dc, P, A, pc, c0);
-  out.a[8][pc] = v;
-  if (f32)
-    out32.a[8][pc32] = (float)v;
-  v = galerkin_entry<KIND, 9>(df, dc, P, A, pc, c0);
-  out.a[9][pc] = v;
-  if (f32)
-    out32.a[9][pc32] = (float)v;
-  v = galerkin_entry<KIND, 10>(df, dc, P, A, pc, c0);
-  out.a[10][pc] = v;
-  if (f32)
-    out32.a[10][pc32] = (float)v;
-  v = galerkin_entry<KIND, 11>(df, dc, P, A, pc, c0);
-  out.a[11][pc] = v;
-  if (f32)
-    out32.a[11][pc32] = (float)v;
-  v = galerkin_entry<KIND, 12>(df, dc, P, A, pc, c0);
-  out.a[12][pc] = v;
-  if (f32)
-    out32.a[12][pc32] = (float)v;
-  v = galerkin_entry<KIND, 13>(df, dc, P, A, pc, c0);
-  out.a[13][pc] = v;
-  if (f32)
-    out32.a[13][pc32] = (float)v;
+#pragma unroll
+  for (int s = 0; s < 14; ++s) {
+    const double v = s == 0 ? acc[s] : -acc[s];
+    out.a[s][pc] = v;
+    if (f32)
+      out32.a[s][pc32] = (float)v;
+  }
 }
 
 // One Galerkin entry per thread (blockIdx.x: the output slot, so the
 // fourteen blocks of the same 128 coarse points run back to back and share
-// the fine operator in L2), for the 27-point input, whose fourteen entries
-// in one thread spill: a block evaluates one entry's unrolled sum for 128
-// coarse points.
+// the fine operator in L2), for the 27-point input: a block evaluates one
+// entry's unrolled sum for 128 coarse points. With 27 couplings per fine
+// point, buildG_kernel's fourteen accumulators need 216 registers (two CTAs
+// per SM) and two entries per thread 168; both measured slower than this.
 template <int KIND>
 __global__ void __launch_bounds__(128)
     buildG_entry_kernel(Dims df, Dims dc, P27<double> P, Op14<double> A,
