@@ -8,9 +8,9 @@
 // points in step t, ping-pong buffers and the reference's per-point
 // arithmetic (sums27 order), so the bits are the same. Two things differ:
 //
-// - The tiles are TI x TJ = 2 TT x TT / 2 (TT 32, 16 or 8 by the level's
-//   size, as there), so one sub-colour row of a tile is TT + H points and a
-//   warp's points lie along one row. The couplings are read from copies of
+// - The tiles are TI x TJ = 2 TT x TT / 2 (TT 32, the size class of levels
+//   from 97 points per axis), so one sub-colour row of a tile is TT + H
+//   points and a warp's points lie along one row. The couplings are read from copies of
 //   the level's fourteen arrays split by the parity of i (CoefSplit): the
 //   points of a sub-colour row and each of their 26 couplings are
 //   consecutive floats, where the reference layout puts them two apart and
@@ -21,6 +21,10 @@
 //   points read in shared memory are consecutive words (no bank conflicts
 //   between the even and odd columns). The tensor maps cover this GPU's own
 //   arrays (no multicast).
+//
+// Levels of the 16 and 8 size classes (65^3 and 33^3 of pb257) use
+// gs27_tma_square_kernel: TT x TT tiles, the couplings in the level's own
+// layout, the staged rows as they arrive.
 //
 // Staging the operator as well (27 boxes per tile: 114 KB, one CTA per SM
 // with two stages, persistent) was built and measured slower: 69 against
@@ -60,13 +64,24 @@ template <int TT> struct TmaBox {
                 "box destinations must be 128-byte aligned");
 };
 
+// box of a TT x TT tile (gs27_tma_square_kernel): rows of TT + 12 floats
+// (a 16-byte multiple, from the 16-byte boundary below the halo), TT + 8
+// rows; SIZE is a multiple of 32 floats for TT = 8, 16, 32
+template <int TT> struct TmaSqBox {
+  static constexpr int BX = TT + 12, BY = TT + 8, SIZE = BX * BY;
+  static constexpr unsigned BYTES = 3 * SIZE * sizeof(float); // 3 planes
+  static_assert(SIZE * sizeof(float) % 128 == 0,
+                "box destinations must be 128-byte aligned");
+};
+
 // The i-parity split layout of a padded float level's coupling copies: row
 // (j, k) holds the even i at [0, hx) and the odd i at [hx, 2 hx), entry i >> 1
-// (i = 1 .. nx, 1-based as Dims). hx is a multiple of 8 floats (one sector).
+// (i = 1 .. nx, 1-based as Dims). hx is a multiple of 4 floats (16 bytes):
+// 68 for 129 points, where a sector multiple (72) would read 6% more.
 struct CoefSplit {
   int hx, ny;
   __host__ __device__ static CoefSplit of(const Dims &d) {
-    return CoefSplit{(((d.nx >> 1) + 1) + 7) & ~7, d.ny};
+    return CoefSplit{(((d.nx >> 1) + 1) + 3) & ~3, d.ny};
   }
   __host__ __device__ int row() const { return 2 * hx; }
   __host__ __device__ int plane() const { return 2 * hx * ny; }
@@ -331,6 +346,74 @@ __global__ void __launch_bounds__(Gs27Tile<TT>::THREADS, 2048 /
     if (q < B::TI * B::TJ && i <= i_max && j <= j_max)
       out[d.at(i, j, k)] =
           xk[(jj + 4) * B::BX + (c & 1) * B::HB + (c >> 1)];
+  }
+}
+
+// One plane-parity phase on TT x TT tiles (gs27_phase_kernel with the x
+// planes staged by three tensor-map boxes, the couplings read in the
+// level's own layout): the 16 and 8 tile classes, where the wide tiles'
+// extra rows (a second round of loads in the first step at TT = 16) and the
+// row split cost more than the split reads save (ncu, cold cache: 10.5
+// against 13.9 us per launch at 65^3, 8.1 against 9.5 at 33^3). err and
+// extra_tx as gs27_tma_kernel's.
+template <int TT>
+__global__ void __launch_bounds__(Gs27Tile<TT>::THREADS, 2048 /
+                                  Gs27Tile<TT>::THREADS)
+    gs27_tma_square_kernel(const __grid_constant__ Gs27TmaMaps maps, Dims d,
+                           Op14<float> A, const float *__restrict__ fc,
+                           float *out, int kfirst, int order, int *err,
+                           unsigned extra_tx) {
+  constexpr int W = TmaSqBox<TT>::BX, NT = Gs27Tile<TT>::THREADS;
+  constexpr int kBox = TmaSqBox<TT>::SIZE;
+  __shared__ __align__(128) float xs[3 * kBox];
+  __shared__ uint64_t bar;
+  const int ti0 = 2 + blockIdx.x * TT, tj0 = 2 + blockIdx.y * TT;
+  const int k = kfirst + 2 * blockIdx.z;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    // box origin (0-based): x at the 16-byte boundary ti0 - 6, y five rows
+    // above the tile (the 4-point halo starts at tj0 - 4, 1-based)
+    const int cx = ti0 - 6, cy = tj0 - 5, z = k - 1;
+    mbar_expect_tx(&bar, TmaSqBox<TT>::BYTES + extra_tx);
+    tma_load_3d(xs, &maps.nb, cx, cy, z - 1, &bar);
+    tma_load_3d(xs + kBox, &maps.own, cx, cy, z, &bar);
+    tma_load_3d(xs + 2 * kBox, &maps.nb, cx, cy, z + 1, &bar);
+  }
+  const bool ok = mbar_wait(&bar, 0);
+  if (__syncthreads_or(!ok)) {
+    if (threadIdx.x == 0) {
+      atomicOr(err, 1);
+      (void)mbar_wait(&bar, 0); // the copies land before the block leaves
+    }
+    return;
+  }
+  // box column c holds 1-based i = ti0 - 5 + c, row r holds j = tj0 - 4 + r;
+  // gs27_step_at's origin is (ti0 - 4, tj0 - 4): one column on
+  float *xc = xs + kBox + 1;
+  gs27_step_at<float, TT, W, kBox, 3>(d, A, nullptr, fc, xc, ti0, tj0, k,
+                                      order);
+  __syncthreads();
+  gs27_step_at<float, TT, W, kBox, 2>(d, A, nullptr, fc, xc, ti0, tj0, k,
+                                      order);
+  __syncthreads();
+  gs27_step_at<float, TT, W, kBox, 1>(d, A, nullptr, fc, xc, ti0, tj0, k,
+                                      order);
+  __syncthreads();
+  gs27_step_at<float, TT, W, kBox, 0>(d, A, nullptr, fc, xc, ti0, tj0, k,
+                                      order);
+  __syncthreads();
+  const int i_max = d.nx - 1, j_max = d.ny - 1;
+#pragma unroll
+  for (int m = 0; m < (TT * TT + NT - 1) / NT; ++m) {
+    const int q = threadIdx.x + m * NT;
+    const int jj = q / TT, ii = q - jj * TT;
+    const int i = ti0 + ii, j = tj0 + jj;
+    if (q < TT * TT && i <= i_max && j <= j_max)
+      out[d.at(i, j, k)] = xc[(i - (ti0 - 4)) + W * (j - (tj0 - 4))];
   }
 }
 

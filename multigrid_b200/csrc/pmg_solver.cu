@@ -49,8 +49,8 @@ struct LevelBuf {
   } tma;
   bool tma_ok = false;
   int tma_tile = 0; // the tile edge the maps' boxes are made for
-  // the padded float levels: the fourteen couplings again, split by the
-  // parity of i (the staged 27-point smoother's copies, gs27_tma.cuh)
+  // the padded float levels of the 32 tile class: the fourteen couplings
+  // again, split by the parity of i (gs27_tma_kernel's copies)
   CoefSplit cs{};
   float *opc[14] = {};
   // the refinement paths' finest level: tensor maps of the colour-split
@@ -317,8 +317,9 @@ void plan(pmg_problem *p, Arena &a) {
       v.r32 = L > 1 ? a.take<float>(m) : nullptr; // reference layout
       v.xalt32 = smoothed ? a.take<float>(m) : nullptr;
       v.cs = CoefSplit::of(v.d32);
+      const bool wide = pitched && gs27_tile_by_size(v.d32) == 32;
       for (int s = 0; s < 14; ++s)
-        v.opc[s] = pitched ? a.take<float>(v.cs.count(v.d32.nz)) : nullptr;
+        v.opc[s] = wide ? a.take<float>(v.cs.count(v.d32.nz)) : nullptr;
       v.code = fine ? a.take<unsigned char>(ns) : nullptr;
       v.code_info = fine ? a.take<int>(12) : nullptr;
       v.lut64 = fine ? a.take<double>(6) : nullptr;
@@ -597,7 +598,8 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 
 // A 3-D map of one padded float array of the level: extent nx x ny x nz
 // (the padding reads as outside), rows px apart, boxes of a tile of size
-// class tt (TmaBox: 2 tt + 12 by tt / 2 + 8).
+// class tt (TmaBox, 2 tt + 12 by tt / 2 + 8, for tt = 32; TmaSqBox,
+// tt + 12 by tt + 8, below).
 bool encode_level_map(CUtensorMap *m, const float *base, const Dims &d,
                       int tt) {
   auto enc = tensor_map_encoder();
@@ -607,8 +609,9 @@ bool encode_level_map(CUtensorMap *m, const float *base, const Dims &d,
                               (cuuint64_t)d.nz};
   const cuuint64_t strides[2] = {(cuuint64_t)d.px * sizeof(float),
                                  (cuuint64_t)d.px * d.ny * sizeof(float)};
-  const cuuint32_t box[3] = {(cuuint32_t)(2 * tt + 12),
-                             (cuuint32_t)(tt / 2 + 8), 1};
+  const cuuint32_t box[3] = {
+      (cuuint32_t)(tt == 32 ? 2 * tt + 12 : tt + 12),
+      (cuuint32_t)(tt == 32 ? tt / 2 + 8 : tt + 8), 1};
   const cuuint32_t elem[3] = {1, 1, 1};
   return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void *)base, dims,
              strides, box, elem, CU_TENSOR_MAP_INTERLEAVE_NONE,
@@ -622,10 +625,12 @@ void encode_tma_maps(pmg_problem *p) {
   for (int L = 2; L < p->nlev; ++L) {
     LevelBuf &v = p->lv[L];
     v.tma_ok = false;
-    if (v.d32.px == v.d.px || !v.xalt32 || !v.opc[0] || v.d32.nx - 2 < 1)
+    if (v.d32.px == v.d.px || !v.xalt32 || v.d32.nx - 2 < 1)
       continue;
     // the size rule's tile edge (gs27_tiled.cuh)
     v.tma_tile = gs27_tile_by_size(v.d32);
+    if (v.tma_tile == 32 && !v.opc[0])
+      continue;
     bool ok = encode_level_map(&v.tma.x, v.x32, v.d32, v.tma_tile);
     ok = ok && encode_level_map(&v.tma.xalt, v.xalt32, v.d32, v.tma_tile);
     v.tma_ok = ok;
@@ -699,11 +704,14 @@ int launch_gs27_tma(pmg_problem *p, LevelBuf &v, int nsweeps, int zero_init,
   if (zero_init)
     PMG_CUDA_TRY(cudaMemsetAsync(*cur, 0, sizeof(float) * v.n3_32, s));
   const int tt = v.tma_tile;
-  // tiles of 2 tt x tt / 2 points (TmaBox)
-  const unsigned tx = cdiv(d.nx - 2, 2 * tt), ty = cdiv(d.ny - 2, tt / 2);
-  Op14<float> A{};
+  // tiles of 2 tt x tt / 2 points (TmaBox) for tt = 32, else tt x tt
+  const unsigned tx = tt == 32 ? cdiv(d.nx - 2, 2 * tt) : cdiv(d.nx - 2, tt);
+  const unsigned ty = tt == 32 ? cdiv(d.ny - 2, tt / 2) : cdiv(d.ny - 2, tt);
+  const int order = 0 | 1 << 2 | 2 << 4 | 3 << 6;
+  Op14<float> Ac{};
   for (int q = 0; q < 14; ++q)
-    A.a[q] = v.opc[q];
+    Ac.a[q] = v.opc[q];
+  const Op14<float> A = v.A32(14);
   float *c = *cur;
   float *a = c == v.x32 ? v.xalt32 : v.x32;
   for (int sw = 0; sw < nsweeps; ++sw) {
@@ -721,13 +729,13 @@ int launch_gs27_tma(pmg_problem *p, LevelBuf &v, int nsweeps, int zero_init,
       const unsigned xt = g_tma_extra_tx.load();
       if (tt == 32)
         gs27_tma_kernel<32><<<g, Gs27Tile<32>::THREADS, 0, s>>>(
-            m, d, v.cs, A, v.f32, a, kfirst, p->kernel_err, xt);
+            m, d, v.cs, Ac, v.f32, a, kfirst, p->kernel_err, xt);
       else if (tt == 16)
-        gs27_tma_kernel<16><<<g, Gs27Tile<16>::THREADS, 0, s>>>(
-            m, d, v.cs, A, v.f32, a, kfirst, p->kernel_err, xt);
+        gs27_tma_square_kernel<16><<<g, Gs27Tile<16>::THREADS, 0, s>>>(
+            m, d, A, v.f32, a, kfirst, order, p->kernel_err, xt);
       else
-        gs27_tma_kernel<8><<<g, Gs27Tile<8>::THREADS, 0, s>>>(
-            m, d, v.cs, A, v.f32, a, kfirst, p->kernel_err, xt);
+        gs27_tma_square_kernel<8><<<g, Gs27Tile<8>::THREADS, 0, s>>>(
+            m, d, A, v.f32, a, kfirst, order, p->kernel_err, xt);
     }
     std::swap(c, a);
   }
@@ -1808,7 +1816,7 @@ int pmg_build_hierarchy(pmg_problem *p, int trilinear) {
     // the staged smoother's split copies of the padded levels' couplings
     for (int L = 2; L < p->nlev; ++L) {
       LevelBuf &c = p->lv[L];
-      if (!c.tma_ok)
+      if (!c.tma_ok || !c.opc[0])
         continue;
       Op14W<float> o;
       for (int q = 0; q < 14; ++q)
