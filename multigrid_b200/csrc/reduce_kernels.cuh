@@ -60,11 +60,25 @@ __device__ void reduce_finish(const double (&v)[NV], ReduceSlot s,
   if (!last)
     return;
   __threadfence();
+  const volatile double *pv = s.partials;
 #pragma unroll
   for (int q = 0; q < NV; ++q) {
+    // each thread adds partials tid, tid + nt, ... in that order; eight
+    // loads are issued before their adds, so the tail waits on one load
+    // latency per eight partials instead of one per partial
     double acc = 0.0;
-    for (unsigned k = tid; k < nb; k += nt)
-      acc += ((volatile double *)s.partials)[(size_t)k * NV + q];
+    unsigned k = tid;
+    for (; k + 7 * nt < nb; k += 8 * nt) {
+      double v[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+        v[u] = pv[(size_t)(k + u * nt) * NV + q];
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+        acc += v[u];
+    }
+    for (; k < nb; k += nt)
+      acc += pv[(size_t)k * NV + q];
     acc = block_sum_2d(acc, sh);
     if (tid == 0)
       s.result[q] = acc;
