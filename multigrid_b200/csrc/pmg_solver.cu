@@ -199,6 +199,9 @@ struct pmg_problem {
   // Mixed path: levels 1 .. bottom_top (n <= 17) run in one CTA
   // (bottom_cycle_kernel); 0 when level 1 is too large.
   int bottom_top = 0;
+  // pmg_set_tma_staging when the problem was created (read once, so that
+  // both passes of plan() lay out the same arrays)
+  bool tma_on = true;
   ReduceSlot red_norm{}, red_lambda{};
   double *h_pinned = nullptr; // [0] residual sum, [1..] spare
   int *h_status = nullptr;
@@ -317,7 +320,8 @@ void plan(pmg_problem *p, Arena &a) {
       v.r32 = L > 1 ? a.take<float>(m) : nullptr; // reference layout
       v.xalt32 = smoothed ? a.take<float>(m) : nullptr;
       v.cs = CoefSplit::of(v.d32);
-      const bool wide = pitched && gs27_tile_by_size(v.d32) == 32;
+      const bool wide =
+          pitched && gs27_tile_by_size(v.d32) == 32 && p->tma_on;
       for (int s = 0; s < 14; ++s)
         v.opc[s] = wide ? a.take<float>(v.cs.count(v.d32.nz)) : nullptr;
       v.code = fine ? a.take<unsigned char>(ns) : nullptr;
@@ -1490,6 +1494,7 @@ long long pmg_problem_bytes(int base, int nlev, int precision) {
   tmp.base = base;
   tmp.nlev = nlev;
   tmp.precision = precision;
+  tmp.tma_on = !tma_disabled();
   Arena a;
   plan(&tmp, a);
   return (long long)a.off;
@@ -1512,6 +1517,7 @@ int pmg_problem_create(int base, int nlev, double box, int precision,
   p->box = box;
   p->precision = precision;
   p->bottom_top = bottom_top_of(base, nlev, precision);
+  p->tma_on = !tma_disabled();
   Arena a;
   plan(p, a);
   p->arena_bytes = a.off;
@@ -1530,7 +1536,7 @@ int pmg_problem_create(int base, int nlev, double box, int precision,
       cudaDeviceGetAttribute(&p->num_sms, cudaDevAttrMultiProcessorCount,
                              dev);
     (void)cudaGetLastError();
-    if (!tma_disabled())
+    if (p->tma_on)
       encode_tma_maps(p);
     p->stream_fine = g_stream_on.load() != 0 && stream_fine_ok(p);
   }
