@@ -168,6 +168,16 @@ __device__ __forceinline__ void tma_load_3d(float *dst, const CUtensorMap *map,
       "l"(map), "r"(x), "r"(y), "r"(z), "r"(smem_addr(bar))
       : "memory");
 }
+// bulk copy of `bytes` (a multiple of 16) from 16-byte aligned global
+// memory into shared memory, completing on bar
+__device__ __forceinline__ void bulk_load(void *dst, const void *src,
+                                          unsigned bytes, uint64_t *bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx"
+               "::bytes [%0], [%1], %2, [%3];\n" ::"r"(smem_addr(dst)),
+               "l"(src), "r"(bytes), "r"(smem_addr(bar))
+               : "memory");
+}
+
 __device__ __forceinline__ void fence_proxy_async_smem() {
   asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
 }

@@ -15,11 +15,15 @@
 // block-wide barrier per plane; each consumer warp waits only for the
 // planes it reads): the other colour's half of x over J + 2
 // rows (the rows above and below the block for the north and south
-// neighbours), and the own colour's half of f and of the code bytes over
-// the block's J rows. In the colour-split layout the other colour is the
-// same half of every row, so each is one box (half-row copies cost the
-// copy engine ~20 ns each whatever their size below ~1 KB, measured, which
-// bounds a pass of ~15 copies per plane at ~30 us). Plane k is computed
+// neighbours), and the own colour's half of f over the block's J rows. In
+// the colour-split layout the other colour is the same half of every row,
+// so each is one box; but a box moves row by row, and half-row copies cost
+// the copy engine ~20 ns each whatever their size below ~1 KB (measured).
+// The own colour's code bytes of the J rows therefore come from a copy of
+// the code array blocked by (plane, row block, colour) (code_block_kernel),
+// where they are one contiguous run: one bulk copy instead of J rows
+// (measured at 257^3: 131 -> 129 us per four float passes, 263 -> 262 us
+// double; the pass is bound more by instruction issue than by the copies). Plane k is computed
 // from the stages of k - 1, k and k + 1 while the next S - 3 planes are in
 // flight, so the bytes in flight are set by the ring, not by registers.
 // A warp computes a row: each lane four consecutive points from 16-byte
@@ -67,6 +71,48 @@ template <typename T> struct StreamCfg {
 struct alignas(64) StreamMaps {
   CUtensorMap x, f, code;
 };
+
+// The code bytes blocked for the streamed pass: per plane k, row block jb
+// (rows 2 + J jb ..) and colour half h, the J rows' entries 0 .. bwc - 1 of
+// half h in a run of J bwc bytes at ((k - 1) nj + jb) 2 + h runs; rows past
+// the grid read as zero, as in a box.
+static_assert(StreamCfg<float>::J == StreamCfg<double>::J,
+              "one blocking serves both element types");
+struct CodeBlocks {
+  int nj, bwc;
+  static CodeBlocks of(const Dims &d) {
+    constexpr int J = StreamCfg<float>::J;
+    return CodeBlocks{(int)cdiv(d.ny - 2, J),
+                      (((d.nx + 1) / 2) + 15) & ~15};
+  }
+  __host__ __device__ long run() const {
+    return (long)StreamCfg<float>::J * bwc;
+  }
+  __host__ __device__ long bytes(const Dims &d) const {
+    return (long)d.nz * nj * 2 * run();
+  }
+};
+
+__global__ void code_block_kernel(Dims d, CodeBlocks cb,
+                                  const unsigned char *__restrict__ code,
+                                  unsigned char *__restrict__ out) {
+  constexpr int J = StreamCfg<float>::J;
+  const Split sp = Split::of(d);
+  const long n = cb.bytes(d);
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n;
+       t += (long)gridDim.x * blockDim.x) {
+    const int e = (int)(t % cb.bwc);
+    long q = t / cb.bwc;
+    const int r = (int)(q % J);
+    q /= J;
+    const int h = (int)(q % 2);
+    q /= 2;
+    const int jb = (int)(q % cb.nj), k = (int)(q / cb.nj) + 1;
+    const int j = 2 + jb * J + r;
+    out[t] = (j <= d.ny && e < sp.hp) ? code[sp.row(j, k) + h * sp.hp + e]
+                                      : (unsigned char)0;
+  }
+}
 
 // Geometry of one streamed launch (host-computed).
 struct StreamShape {
@@ -129,8 +175,9 @@ __global__ void __launch_bounds__(StreamCfg<T>::THREADS,
                       const T *__restrict__ oE, const T *__restrict__ oN,
                       const T *__restrict__ uC, const int *__restrict__ info,
                       const T *__restrict__ lut,
-                      const T *__restrict__ octab, T *x, int want, T keep,
-                      int *err, unsigned extra_tx) {
+                      const T *__restrict__ octab,
+                      const unsigned char *__restrict__ codeb, T *x,
+                      int want, T keep, int *err, unsigned extra_tx) {
   using V = Quad<T>;
   extern __shared__ __align__(128) unsigned char sm[];
   // per code byte (its low seven bits) the point's seven coefficients in
@@ -216,8 +263,10 @@ __global__ void __launch_bounds__(StreamCfg<T>::THREADS,
       if (own) {
         tma_load_4d(slot + sh.foff, &maps.f, 0, want, j0 - 1, kk - 1,
                     &full[s]);
-        tma_load_4d(slot + sh.coff, &maps.code, 0, want, j0 - 1, kk - 1,
-                    &full[s]);
+        bulk_load(slot + sh.coff,
+                  codeb + ((long)((kk - 1) * sh.nj + jb) * 2 + want) *
+                              (J * sh.bwc),
+                  (unsigned)(J * sh.bwc), &full[s]);
       }
     }
     drain(klast);
@@ -406,12 +455,14 @@ template <typename T> constexpr auto stream_kernel_of() {
 }
 
 // itmax red-black sweeps on the coded split arrays (launch_gs7_code's
-// semantics) with the streamed pass; maps: the level's x, f and code maps
-// (boxes of stream_shape's widths); err as in gs7_stream_kernel.
+// semantics) with the streamed pass; maps: the level's x and f maps (boxes
+// of stream_shape's widths); codeb: the level's code bytes blocked by
+// code_block_kernel; err as in gs7_stream_kernel.
 template <typename T>
 int launch_gs7_stream(const StreamMaps &maps, const Dims &d, const T *oC,
                       const T *oE, const T *oN, const T *uC, const int *info,
-                      const T *lut, const T *octab, T *x, int itmax,
+                      const T *lut, const T *octab,
+                      const unsigned char *codeb, T *x, int itmax,
                       int iadjoint, int zero_init, int *err,
                       unsigned extra_tx, cudaStream_t s) {
   constexpr int NT = StreamCfg<T>::THREADS;
@@ -438,7 +489,7 @@ int launch_gs7_stream(const StreamMaps &maps, const Dims &d, const T *oC,
       const int want = (1 - iadjoint) * c + iadjoint * (1 - c);
       const T keep = zero_init ? T(0) : T(1);
       kern<<<g, NT, smem, s>>>(maps, d, sh, oC, oE, oN, uC, info, lut, octab,
-                               x, want, keep, err, extra_tx);
+                               codeb, x, want, keep, err, extra_tx);
       zero_init = 0;
     }
   PMG_LAUNCH_CHECK();

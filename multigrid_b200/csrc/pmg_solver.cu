@@ -54,7 +54,8 @@ struct LevelBuf {
   CoefSplit cs{};
   float *opc[14] = {};
   // the refinement paths' finest level: tensor maps of the colour-split
-  // correction, right-hand side and code bytes (the streamed colour pass)
+  // correction and right-hand side (the streamed colour pass; its code
+  // bytes come from codeb)
   StreamMaps smaps;
   // the same arrays in boxes of both colour halves (the streamed defect,
   // defect_stream.cuh); dmaps_ok when they could be made
@@ -72,6 +73,8 @@ struct LevelBuf {
   // mixed / fp64-fast finest level: coded couplings (split_layout.cuh) and
   // their table
   unsigned char *code = nullptr;
+  // the code bytes blocked for the streamed colour pass (CodeBlocks)
+  unsigned char *codeb = nullptr;
   int *code_info = nullptr; // device: ranges and the mismatch flags
   double *lut64 = nullptr;  // device: the double couplings of the codes
   // device: the centre coefficient by code (bit 6 of the code byte) and the
@@ -325,6 +328,8 @@ void plan(pmg_problem *p, Arena &a) {
       for (int s = 0; s < 14; ++s)
         v.opc[s] = wide ? a.take<float>(v.cs.count(v.d32.nz)) : nullptr;
       v.code = fine ? a.take<unsigned char>(ns) : nullptr;
+      v.codeb = fine ? a.take<unsigned char>(CodeBlocks::of(v.d).bytes(v.d))
+                     : nullptr;
       v.code_info = fine ? a.take<int>(12) : nullptr;
       v.lut64 = fine ? a.take<double>(6) : nullptr;
       v.octab64 = fine ? a.take<double>(128) : nullptr;
@@ -337,6 +342,7 @@ void plan(pmg_problem *p, Arena &a) {
       v.xs = a.take<double>(ns);
       v.fs = a.take<double>(ns);
       v.code = a.take<unsigned char>(ns);
+      v.codeb = a.take<unsigned char>(CodeBlocks::of(v.d).bytes(v.d));
       v.code_info = a.take<int>(12);
       v.lut64 = a.take<double>(6);
       v.octab64 = a.take<double>(128);
@@ -435,8 +441,8 @@ int smooth64(pmg_problem *p, int L, int nsweeps, int zero_init,
     if (p->stream_fine)
       return launch_gs7_stream<double>(
           v.smaps, v.d, v.ops[kOC], v.ops[kOE], v.ops[kON], v.ops[kUC],
-          v.code_info, v.lut64, v.octab64, v.xs, nsweeps, 0, zero_init,
-          p->kernel_err, g_tma_extra_tx.load(), p->stream);
+          v.code_info, v.lut64, v.octab64, v.codeb, v.xs, nsweeps, 0,
+          zero_init, p->kernel_err, g_tma_extra_tx.load(), p->stream);
     return launch_gs7_code<double>(v.d, v.ops[kOC], v.fs, v.ops[kOE],
                                    v.ops[kON], v.ops[kUC], v.code,
                                    v.code_info, v.lut64, v.octab64, v.xs,
@@ -687,10 +693,10 @@ bool encode_stream_maps(LevelBuf &v, const T *x, const T *f) {
         encode_split_map(&v.dmaps.code, v.code, CU_TENSOR_MAP_DATA_TYPE_UINT8,
                          1, v.d, ds.bwc, JD, 2);
   }
+  // (the streamed pass reads its code bytes by bulk copies of the blocked
+  // copy, not by a map)
   return encode_split_map(&v.smaps.x, x, t, sizeof(T), v.d, sh.bw, J + 2) &&
-         encode_split_map(&v.smaps.f, f, t, sizeof(T), v.d, sh.bw, J) &&
-         encode_split_map(&v.smaps.code, v.code,
-                          CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, v.d, sh.bwc, J);
+         encode_split_map(&v.smaps.f, f, t, sizeof(T), v.d, sh.bw, J);
 }
 bool stream_fine_ok(pmg_problem *p) {
   LevelBuf &v = p->lv[p->nlev];
@@ -764,9 +770,9 @@ int smooth_ref(pmg_problem *p, int L, int nsweeps, int zero_init, T **cur) {
     return launch_gs7_stream<T>(v.smaps, v.d, A::fine_op(v, kOC),
                                 A::fine_op(v, kOE), A::fine_op(v, kON),
                                 A::fine_op(v, kUC), v.code_info, A::lut(v),
-                                A::octab(v), *cur, nsweeps, 0, zero_init,
-                                p->kernel_err, g_tma_extra_tx.load(),
-                                p->stream);
+                                A::octab(v), v.codeb, *cur, nsweeps, 0,
+                                zero_init, p->kernel_err,
+                                g_tma_extra_tx.load(), p->stream);
   if (L == p->nlev && p->use_codes)
     return launch_gs7_code<T>(v.d, A::fine_op(v, kOC), A::f(v),
                               A::fine_op(v, kOE), A::fine_op(v, kON),
@@ -1819,6 +1825,10 @@ int pmg_build_hierarchy(pmg_problem *p, int trilinear) {
     p->launches += 4;
     if ((rc = build_oc_codes(p, v)))
       return rc;
+    // the streamed pass's blocked copy of the finished code bytes
+    code_block_kernel<<<flat_grid(CodeBlocks::of(v.d).bytes(v.d)), 256, 0,
+                        s>>>(v.d, CodeBlocks::of(v.d), v.code, v.codeb);
+    ++p->launches;
     // the staged smoother's split copies of the padded levels' couplings
     for (int L = 2; L < p->nlev; ++L) {
       LevelBuf &c = p->lv[L];
@@ -1870,6 +1880,10 @@ int pmg_build_hierarchy(pmg_problem *p, int trilinear) {
     p->launches += 4;
     if ((rc = build_oc_codes(p, v)))
       return rc;
+    // the streamed pass's blocked copy of the finished code bytes
+    code_block_kernel<<<flat_grid(CodeBlocks::of(v.d).bytes(v.d)), 256, 0,
+                        s>>>(v.d, CodeBlocks::of(v.d), v.code, v.codeb);
+    ++p->launches;
     PMG_LAUNCH_CHECK();
   }
   // tile edge of the 27-point smoother, measured once per grid size (every

@@ -77,16 +77,6 @@ inline long resid_max_ctas(const Dims &d) {
   return (long)cdiv(d.ny - 2, ResidCfg::J) * (d.nz - 2);
 }
 
-// bulk copy of `bytes` (a multiple of 16) from 16-byte aligned global
-// memory into shared memory, completing on bar
-__device__ __forceinline__ void bulk_load(void *dst, const void *src,
-                                          unsigned bytes, uint64_t *bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx"
-               "::bytes [%0], [%1], %2, [%3];\n" ::"r"(smem_addr(dst)),
-               "l"(src), "r"(bytes), "r"(smem_addr(bar))
-               : "memory");
-}
-
 // a bulk copy of elements [g0, g1) of an array of esz-byte entries, from the
 // 16-byte boundary at or below g0 to the one at or above g1, into the image
 // of the array whose element gb (16-byte aligned) is at dst
