@@ -167,7 +167,10 @@ template <typename T> struct alignas(16) Quad {
   T x, y, z, w;
 };
 
-template <typename T, int J, int S>
+// KEEP false: the first pass from a zero iterate (zero_initialize), whose
+// neighbour sum is multiplied by 0 as in the per-point pass; true: the sum
+// is added as it is (1 * sum is sum, so the multiply is left out).
+template <typename T, int J, int S, bool KEEP>
 __global__ void __launch_bounds__(StreamCfg<T>::THREADS,
                                   StreamCfg<T>::MIN_CTAS)
     gs7_stream_kernel(const __grid_constant__ StreamMaps maps, Dims d,
@@ -177,7 +180,7 @@ __global__ void __launch_bounds__(StreamCfg<T>::THREADS,
                       const T *__restrict__ lut,
                       const T *__restrict__ octab,
                       const unsigned char *__restrict__ codeb, T *x,
-                      int want, T keep, int *err, unsigned extra_tx) {
+                      int want, int *err, unsigned extra_tx) {
   using V = Quad<T>;
   extern __shared__ __align__(128) unsigned char sm[];
   // per code byte (its low seven bits) the point's seven coefficients in
@@ -352,7 +355,8 @@ __global__ void __launch_bounds__(StreamCfg<T>::THREADS,
             const Quad<T> c1 = *reinterpret_cast<const Quad<T> *>(t + 4);
             const T sum = c0.x * an[m] + c0.y * as[m] + c0.z * xe[m] +
                           c0.w * xw[m] + c1.x * ad[m] + c1.y * au[m];
-            out[m] = div_by_table(af[m] + keep * sum, c1.z, rtab,
+            out[m] = div_by_table(KEEP ? af[m] + sum : af[m] + T(0) * sum,
+                                  c1.z, rtab,
                                   (cb >> (8 * m)) & 127u);
           }
         } else {
@@ -377,7 +381,7 @@ __global__ void __launch_bounds__(StreamCfg<T>::THREADS,
             const T sum = cp.n * an[m] + cp.s * as[m] + cp.e * xe[m] +
                           cp.w * xw[m] + cp.dn * ad[m] + cp.u * au[m];
             const T c = in ? oC[p] : T(1);
-            out[m] = (af[m] + keep * sum) / (c + T(0));
+            out[m] = (KEEP ? af[m] + sum : af[m] + T(0) * sum) / (c + T(0));
           }
         }
         if (act) {
@@ -450,8 +454,8 @@ template <typename T> bool stream_fits(const Dims &d) {
          stream_smem_bytes<T>(sh) <= kStreamMaxSmem;
 }
 
-template <typename T> constexpr auto stream_kernel_of() {
-  return gs7_stream_kernel<T, StreamCfg<T>::J, StreamCfg<T>::S>;
+template <typename T, bool KEEP = true> constexpr auto stream_kernel_of() {
+  return gs7_stream_kernel<T, StreamCfg<T>::J, StreamCfg<T>::S, KEEP>;
 }
 
 // itmax red-black sweeps on the coded split arrays (launch_gs7_code's
@@ -474,7 +478,9 @@ int launch_gs7_stream(const StreamMaps &maps, const Dims &d, const T *oC,
   StreamShape sh = stream_shape<T>(d, 1);
   const size_t smem = stream_smem_bytes<T>(sh);
   {
-    const cudaError_t e = set_smem_limit<stream_kernel_of<T>()>((int)smem);
+    cudaError_t e = set_smem_limit<stream_kernel_of<T, true>()>((int)smem);
+    PMG_CUDA_TRY(e);
+    e = set_smem_limit<stream_kernel_of<T, false>()>((int)smem);
     PMG_CUDA_TRY(e);
   }
   int per_sm = 0, sms = 0;
@@ -487,9 +493,9 @@ int launch_gs7_stream(const StreamMaps &maps, const Dims &d, const T *oC,
   for (int it = 0; it < itmax; ++it)
     for (int c = 0; c <= 1; ++c) {
       const int want = (1 - iadjoint) * c + iadjoint * (1 - c);
-      const T keep = zero_init ? T(0) : T(1);
-      kern<<<g, NT, smem, s>>>(maps, d, sh, oC, oE, oN, uC, info, lut, octab,
-                               codeb, x, want, keep, err, extra_tx);
+      auto k = zero_init ? stream_kernel_of<T, false>() : kern;
+      k<<<g, NT, smem, s>>>(maps, d, sh, oC, oE, oN, uC, info, lut, octab,
+                            codeb, x, want, err, extra_tx);
       zero_init = 0;
     }
   PMG_LAUNCH_CHECK();
