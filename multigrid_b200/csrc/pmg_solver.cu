@@ -263,6 +263,22 @@ std::atomic<unsigned> g_tma_extra_tx{0};
 
 int level_n(int base, int L) { return base * (1 << L) + 1; }
 
+// The damping reduction of a coarse level (ideal_lambda_kernel with the
+// level's planes per block)
+template <typename T>
+void launch_ideal_lambda(const Dims &d, const Op14<T> &A, const T *x,
+                         const T *r, ReduceSlot red, double *w,
+                         cudaStream_t s) {
+  const dim3 g = lambda_grid(d), b = interior_block();
+  const int pl = lambda_planes(d);
+  if (pl == 4)
+    ideal_lambda_kernel<T, 4><<<g, b, 0, s>>>(d, A, x, r, red, w);
+  else if (pl == 2)
+    ideal_lambda_kernel<T, 2><<<g, b, 0, s>>>(d, A, x, r, red, w);
+  else
+    ideal_lambda_kernel<T, 1><<<g, b, 0, s>>>(d, A, x, r, red, w);
+}
+
 // Mixed path: the top level of the one-launch bottom cycle (the levels up
 // to 17 points per axis); 0 on the other paths.
 int bottom_top_of(int base, int nlev, int precision) {
@@ -525,9 +541,8 @@ int vcycle64(pmg_problem *p, int L, int as_preconditioner) {
   if ((rc = vcycle64(p, L - 1, 0)))
     return rc;
   prof_begin(p, sl + kPhLambda);
-  ideal_lambda_kernel<double><<<lambda_grid(c.d), interior_block(), 0, s>>>(
-      c.d, c.A64(14), c.x, c.f, p->red_lambda, c.omega,
-      lambda_planes(c.d));
+  launch_ideal_lambda<double>(c.d, c.A64(14), c.x, c.f, p->red_lambda,
+                              c.omega, s);
   prof_end(p, sl + kPhLambda);
   // x += w * (interpolated correction), one pass
   prof_begin(p, sl + kPhInterp);
@@ -910,16 +925,14 @@ template <typename T> int vcycle_ref(pmg_problem *p, int L) {
   if (bottom_below) {
     // damping computed by the bottom kernel
   } else if (L - 1 == 1) {
-    ideal_lambda_kernel<double><<<lambda_grid(c.d), interior_block(), 0, s>>>(
-        c.d, c.A64(14), c.x, c.f, p->red_lambda, c.omega,
-        lambda_planes(c.d));
+    launch_ideal_lambda<double>(c.d, c.A64(14), c.x, c.f, p->red_lambda,
+                                c.omega, s);
     if (kFloat)
       convert_kernel<double, float><<<flat_grid(c.n3), 256, 0, s>>>(
           c.n3, c.x, c.x32);
   } else {
-    ideal_lambda_kernel<T><<<lambda_grid(c.d), interior_block(), 0, s>>>(
-        A::dims(c), A::A(c), A::x(c), A::f(c), p->red_lambda, c.omega,
-        lambda_planes(c.d));
+    launch_ideal_lambda<T>(A::dims(c), A::A(c), A::x(c), A::f(c),
+                           p->red_lambda, c.omega, s);
   }
   prof_end(p, sl + kPhLambda);
   // x += w * (interpolated correction), one pass

@@ -148,26 +148,31 @@ __global__ void __launch_bounds__(256)
 
 // Hackbusch-Reusken damping w = (r . x) / (x . A x) over the interior of a
 // 27-point level (get_ideal_lambda, MultigridDomain.h:327-352), accumulated
-// in double; the last block stores w. Grid: lambda_grid, `planes` =
-// lambda_planes.
-template <typename T>
+// in double; the last block stores w. Grid: lambda_grid with PL =
+// lambda_planes planes per block. The plane loop has a compile-time length,
+// so the loads of a thread's planes can be in flight together; each
+// thread's sums still run over its planes in order.
+template <typename T, int PL>
 __global__ void __launch_bounds__(kReduceThreads)
     ideal_lambda_kernel(Dims d, Op14<T> A, const T *__restrict__ x,
                         const T *__restrict__ r, ReduceSlot s,
-                        double *__restrict__ w, int planes) {
+                        double *__restrict__ w) {
   __shared__ double sh[32];
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
-  const int k0 = 2 + blockIdx.z * planes;
-  const int k1 = min(k0 + planes - 1, d.nz - 1);
+  const int k0 = 2 + blockIdx.z * PL;
   const int sy = d.sy(), sz = d.sz();
   double up = 0.0, lo = 0.0;
   if (i <= d.nx - 1 && j <= d.ny - 1) {
-    for (int k = k0; k <= k1; ++k) {
-      const int p = d.at(i, j, k);
-      up += (double)r[p] * (double)x[p];
-      lo += (double)x[p] *
-            (double)apply27(A, (const T *)nullptr, x, p, sy, sz);
+#pragma unroll
+    for (int q = 0; q < PL; ++q) {
+      const int k = k0 + q;
+      if (k <= d.nz - 1) {
+        const int p = d.at(i, j, k);
+        up += (double)r[p] * (double)x[p];
+        lo += (double)x[p] *
+              (double)apply27(A, (const T *)nullptr, x, p, sy, sz);
+      }
     }
   }
   double v[2];
