@@ -6,10 +6,13 @@
 // The per-thread kernel (defect7_code_kernel) moves the coded format's 13
 // bytes per point at ~2.5 TB/s, bound by load latency. Here, as in the
 // streamed colour pass (gs7_stream.cuh), each CTA owns J rows of a chunk of
-// planes and marches along k: per plane a producer warp issues three
-// tensor-map boxes that take both colour halves (x over the J + 2 rows
-// around the block, f and the code bytes over its J rows) into a ring slot
-// with full / empty mbarriers, and consumer warps (two per row, lanes over
+// planes and marches along k: per plane a producer warp issues three bulk
+// copies (cp.async.bulk) that take both colour halves, x over the J + 2 rows
+// around the block, f and the code bytes over its J rows: in the
+// colour-split layout a row's two halves are adjacent and rows follow one
+// another, so each is one contiguous run (a tensor box would move it half
+// row by half row, ~20 ns each). They land in a ring slot with full / empty
+// mbarriers, and consumer warps (two per row, lanes over
 // 32 consecutive points, so the reference-layout stores coalesce) compute
 // plane k from the slots of k - 1, k and k + 1. A point's seven
 // coefficients come from the 128-entry table indexed by its code byte.
@@ -29,19 +32,20 @@ template <typename T> struct DefectCfg {
   static constexpr int J = 4;   // rows per CTA
   static constexpr int WPR = 2; // consumer warps per row
   static constexpr int NC = J * WPR;
-  static constexpr int S = sizeof(T) == 4 ? 6 : 4;
+  // stages: three float CTAs per SM at 257^3 (a stage holds rows of 2 hp
+  // entries, the global layout)
+  static constexpr int S = sizeof(T) == 4 ? 5 : 4;
   static constexpr int THREADS = 32 * (NC + 1);
   static constexpr int MIN_CTAS = sizeof(T) == 4 ? 3 : 2;
 };
 
-// Geometry of a streamed defect launch: boxes take both halves, so a stage
-// row holds 2 bw entries (2 bwc code bytes).
+// Geometry of a streamed defect launch: a stage row is a row of the
+// colour-split array, two halves of hp entries (bw = bwc = hp).
 template <typename T> StreamShape defect_shape(const Dims &d, int resident) {
   constexpr int J = DefectCfg<T>::J;
   StreamShape sh{};
-  const int hx = (d.nx + 1) / 2;
-  sh.bw = (hx + 3) & ~3;
-  sh.bwc = (hx + 15) & ~15;
+  sh.bw = Split::of(d).hp;
+  sh.bwc = sh.bw;
   sh.nj = (int)cdiv(d.ny - 2, J);
   const int planes = d.nz - 2;
   int nkc = resident / sh.nj;
@@ -71,8 +75,10 @@ template <typename T> bool defect_fits(const Dims &d) {
 template <typename T>
 __global__ void __launch_bounds__(DefectCfg<T>::THREADS,
                                   DefectCfg<T>::MIN_CTAS)
-    defect7_stream_kernel(const __grid_constant__ StreamMaps maps, Dims d,
-                          StreamShape sh, const T *__restrict__ oC,
+    defect7_stream_kernel(Dims d, StreamShape sh, const T *__restrict__ xg,
+                          const T *__restrict__ fg,
+                          const unsigned char *__restrict__ codeg,
+                          const T *__restrict__ oC,
                           const T *__restrict__ oE, const T *__restrict__ oN,
                           const T *__restrict__ uC,
                           const int *__restrict__ info,
@@ -123,10 +129,15 @@ __global__ void __launch_bounds__(DefectCfg<T>::THREADS,
   auto use_of = [&](int kk) { return (kk - kfirst) / S; };
 
   if (warp == NC) {
-    // producer: both halves of x over rows j0 - 1 .. j0 + J, of f and the
-    // code bytes over rows j0 .. j0 + J - 1 (planes the block computes)
+    // producer: both halves of x over rows j0 - 1 .. min(j0 + J, ny), of f
+    // and the code bytes over rows j0 .. j0 + jn - 1 (planes the block
+    // computes); the stage rows past them are never read
     if (lane != 0)
       return;
+    const int nrx = min(J + 2, d.ny - j0 + 2);
+    const unsigned xb = (unsigned)(nrx * sp.pitch() * sizeof(T));
+    const unsigned fb = (unsigned)(jn * sp.pitch() * sizeof(T));
+    const unsigned cb = (unsigned)(jn * sp.pitch());
     auto drain = [&](int last) {
       long polls = 0;
       for (int kk = max(kfirst, last - S + 1); kk <= last; ++kk)
@@ -146,13 +157,11 @@ __global__ void __launch_bounds__(DefectCfg<T>::THREADS,
       }
       unsigned char *slot = sm + s * sh.slot;
       const bool own = kk >= ka && kk <= kb;
-      mbar_expect_tx(&full[s],
-                     sh.xbytes + (own ? sh.fcbytes : 0u) + extra_tx);
-      tma_load_4d(slot + sh.xoff, &maps.x, 0, 0, j0 - 2, kk - 1, &full[s]);
+      mbar_expect_tx(&full[s], xb + (own ? fb + cb : 0u) + extra_tx);
+      bulk_load(slot + sh.xoff, xg + sp.row(j0 - 1, kk), xb, &full[s]);
       if (own) {
-        tma_load_4d(slot + sh.foff, &maps.f, 0, 0, j0 - 1, kk - 1, &full[s]);
-        tma_load_4d(slot + sh.coff, &maps.code, 0, 0, j0 - 1, kk - 1,
-                    &full[s]);
+        bulk_load(slot + sh.foff, fg + sp.row(j0, kk), fb, &full[s]);
+        bulk_load(slot + sh.coff, codeg + sp.row(j0, kk), cb, &full[s]);
       }
     }
     drain(klast);
@@ -242,10 +251,10 @@ template <typename T> constexpr auto defect_kernel_of() {
 }
 
 // r (reference layout) = f - A x on the coded split level d (defect_fits);
-// maps: x, f and code maps of both halves (boxes of defect_shape's widths,
-// J + 2 and J rows).
+// x, f, code: the level's colour-split arrays (16-byte aligned).
 template <typename T>
-int launch_defect7_stream(const StreamMaps &maps, const Dims &d, const T *oC,
+int launch_defect7_stream(const T *x, const T *f, const unsigned char *code,
+                          const Dims &d, const T *oC,
                           const T *oE, const T *oN, const T *uC,
                           const int *info, const T *lut, const T *octab,
                           T *r, int *err, unsigned extra_tx,
@@ -266,8 +275,8 @@ int launch_defect7_stream(const StreamMaps &maps, const Dims &d, const T *oC,
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem));
   sh = defect_shape<T>(d, sms * (per_sm < 1 ? 1 : per_sm));
   const unsigned g = (unsigned)sh.nj * cdiv(d.nz - 2, sh.kchunk);
-  kern<<<g, NT, smem, s>>>(maps, d, sh, oC, oE, oN, uC, info, lut, octab, r,
-                           err, extra_tx);
+  kern<<<g, NT, smem, s>>>(d, sh, x, f, code, oC, oE, oN, uC, info, lut,
+                           octab, r, err, extra_tx);
   PMG_LAUNCH_CHECK();
   return PMG_OK;
 }

@@ -57,10 +57,9 @@ struct LevelBuf {
   // correction and right-hand side (the streamed colour pass; its code
   // bytes come from codeb)
   StreamMaps smaps;
-  // the same arrays in boxes of both colour halves (the streamed defect,
-  // defect_stream.cuh); dmaps_ok when they could be made
-  StreamMaps dmaps;
-  bool dmaps_ok = false;
+  // the streamed defect (defect_stream.cuh, bulk copies of the same
+  // arrays) fits the level
+  bool defect_ok = false;
   double *op[14] = {};
   double *P[27] = {}; // prolongation from this level to level+1
   double *x = nullptr, *f = nullptr, *r = nullptr;
@@ -699,15 +698,7 @@ bool encode_stream_maps(LevelBuf &v, const T *x, const T *f) {
   const CUtensorMapDataType t = sizeof(T) == 4
                                     ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
                                     : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
-  if (defect_fits<T>(v.d)) {
-    const StreamShape ds = defect_shape<T>(v.d, 1);
-    constexpr int JD = DefectCfg<T>::J;
-    v.dmaps_ok =
-        encode_split_map(&v.dmaps.x, x, t, sizeof(T), v.d, ds.bw, JD + 2, 2) &&
-        encode_split_map(&v.dmaps.f, f, t, sizeof(T), v.d, ds.bw, JD, 2) &&
-        encode_split_map(&v.dmaps.code, v.code, CU_TENSOR_MAP_DATA_TYPE_UINT8,
-                         1, v.d, ds.bwc, JD, 2);
-  }
+  v.defect_ok = defect_fits<T>(v.d);
   // (the streamed pass reads its code bytes by bulk copies of the blocked
   // copy, not by a map)
   return encode_split_map(&v.smaps.x, x, t, sizeof(T), v.d, sh.bw, J + 2) &&
@@ -882,13 +873,13 @@ template <typename T> int vcycle_ref(pmg_problem *p, int L) {
     return rc;
   prof_end(p, sl + kPhPre);
   prof_begin(p, sl + kPhDefect);
-  if (kFloat && kind == 7 && p->use_codes && p->stream_fine && v.dmaps_ok &&
+  if (kFloat && kind == 7 && p->use_codes && p->stream_fine && v.defect_ok &&
       x == A::x(v)) {
-    // streamed (defect_stream.cuh): the maps cover the level's own arrays;
-    // float only (the double version, two CTAs per SM, was slower than the
-    // per-thread kernel: 114 against 110 us at 257^3)
+    // streamed (defect_stream.cuh); float only (the double version, two
+    // CTAs per SM, was slower than the per-thread kernel: 114 against
+    // 110 us at 257^3)
     if ((rc = launch_defect7_stream<T>(
-             v.dmaps, v.d, A::fine_op(v, kOC), A::fine_op(v, kOE),
+             x, A::f(v), v.code, v.d, A::fine_op(v, kOC), A::fine_op(v, kOE),
              A::fine_op(v, kON), A::fine_op(v, kUC), v.code_info, A::lut(v),
              A::octab(v), A::r(v), p->kernel_err, g_tma_extra_tx.load(), s)))
       return rc;
