@@ -48,6 +48,7 @@
 #pragma once
 
 #include <atomic>
+#include <type_traits>
 
 #include "gs27_tma.cuh"
 #include "split_layout.cuh"
@@ -160,6 +161,14 @@ __device__ __forceinline__ float div_by_table(float num, float,
                                               const double *rtab,
                                               unsigned b) {
   return (float)((double)num * rtab[b]);
+}
+
+// a row parity given at compile time (std::true_type / std::false_type) or
+// at run time (bool)
+__device__ __forceinline__ bool row_parity(bool b) { return b; }
+template <bool B>
+__device__ __forceinline__ bool row_parity(std::integral_constant<bool, B>) {
+  return B;
 }
 
 // four consecutive entries
@@ -304,102 +313,117 @@ __global__ void __launch_bounds__(StreamCfg<T>::THREADS,
       // own points: i = 1 + 2e (odd i, when point 1 of the row has the
       // pass's colour) or 2 + 2e; interior e in [elo, ehi]. West and east
       // are entries e - 1, e (odd i) or e, e + 1 (even i) of the other half.
-      const bool odd = ((1 + j + k) & 1) == want;
-      const int elo = odd ? 1 : 0;
-      const int ehi = odd ? (d.nx - 2) / 2 : (d.nx - 3) / 2;
       const long row = (long)sp.row(j, k) + want * sp.hp;
-      // every lane takes part in each round (the shuffles); lane g of the
-      // round takes entries 4g .. 4g + 3
-      for (int g0 = 0; 4 * g0 <= ehi; g0 += 32) {
-        const int g = g0 + lane, e4 = 4 * g;
-        const bool act = e4 <= ehi;
-        V vn{}, vs{}, vu{}, vd{}, vo{}, vf{};
-        unsigned cb = 0;
-        if (act) {
-          vn = *reinterpret_cast<const V *>(xn + e4);
-          vs = *reinterpret_cast<const V *>(xs + e4);
-          vu = *reinterpret_cast<const V *>(xu + e4);
-          vd = *reinterpret_cast<const V *>(xd + e4);
-          vo = *reinterpret_cast<const V *>(xo + e4);
-          vf = *reinterpret_cast<const V *>(fr + e4);
-          cb = *reinterpret_cast<const unsigned *>(cr + e4);
-        }
-        // the other-half entry just outside the four: e4 - 1 (odd i, the
-        // previous lane's last) or e4 + 4 (even i, the next lane's first);
-        // read directly where that lane is in another round or idle
-        const T up = __shfl_up_sync(0xffffffffu, vo.w, 1);
-        const T down = __shfl_down_sync(0xffffffffu, vo.x, 1);
-        T edge = odd ? up : down;
-        if (act && odd && lane == 0 && e4 > 0)
-          edge = xo[e4 - 1];
-        if (act && !odd && (lane == 31 || e4 + 4 > ehi))
-          edge = xo[e4 + 4];
-        const T xw[4] = {odd ? edge : vo.x, odd ? vo.x : vo.y,
-                         odd ? vo.y : vo.z, odd ? vo.z : vo.w};
-        const T xe[4] = {odd ? vo.x : vo.y, odd ? vo.y : vo.z,
-                         odd ? vo.z : vo.w, odd ? vo.w : edge};
-        const T an[4] = {vn.x, vn.y, vn.z, vn.w};
-        const T as[4] = {vs.x, vs.y, vs.z, vs.w};
-        const T au[4] = {vu.x, vu.y, vu.z, vu.w};
-        const T ad[4] = {vd.x, vd.y, vd.z, vd.w};
-        const T af[4] = {vf.x, vf.y, vf.z, vf.w};
-        T out[4];
-        if (oc_coded) {
-          // every coefficient from the code byte's table entry (the same
-          // values gs7_code_color_kernel selects); points outside the row's
-          // interior compute from table entries too and are not stored
-#pragma unroll
-          for (int m = 0; m < 4; ++m) {
-            const T *t = ctab[(cb >> (8 * m)) & 127u];
-            const Quad<T> c0 = *reinterpret_cast<const Quad<T> *>(t);
-            const Quad<T> c1 = *reinterpret_cast<const Quad<T> *>(t + 4);
-            const T sum = c0.x * an[m] + c0.y * as[m] + c0.z * xe[m] +
-                          c0.w * xw[m] + c1.x * ad[m] + c1.y * au[m];
-            out[m] = div_by_table(KEEP ? af[m] + sum : af[m] + T(0) * sum,
-                                  c1.z, rtab,
-                                  (cb >> (8 * m)) & 127u);
+      // the row's parity is the same for the whole warp. Float: each case
+      // compiled on its own, so the per-point selects between them fold away
+      // (1-2% per pass at 257^3); double keeps one body, whose two copies
+      // would spill (258 against 254 us per four passes)
+      auto row_pass = [&](auto odd_c) {
+        const bool odd = row_parity(odd_c);
+        const int elo = odd ? 1 : 0;
+        const int ehi = odd ? (d.nx - 2) / 2 : (d.nx - 3) / 2;
+        // every lane takes part in each round (the shuffles); lane g of the
+        // round takes entries 4g .. 4g + 3
+        for (int g0 = 0; 4 * g0 <= ehi; g0 += 32) {
+          const int g = g0 + lane, e4 = 4 * g;
+          const bool act = e4 <= ehi;
+          V vn{}, vs{}, vu{}, vd{}, vo{}, vf{};
+          unsigned cb = 0;
+          if (act) {
+            vn = *reinterpret_cast<const V *>(xn + e4);
+            vs = *reinterpret_cast<const V *>(xs + e4);
+            vu = *reinterpret_cast<const V *>(xu + e4);
+            vd = *reinterpret_cast<const V *>(xd + e4);
+            vo = *reinterpret_cast<const V *>(xo + e4);
+            vf = *reinterpret_cast<const V *>(fr + e4);
+            cb = *reinterpret_cast<const unsigned *>(cr + e4);
           }
-        } else {
-#pragma unroll
-          for (int m = 0; m < 4; ++m) {
-            const int e = e4 + m;
-            const bool in = act && e >= elo && e <= ehi;
-            const unsigned b = (cb >> (8 * m)) & 0xffu;
-            const int p = (int)(row + e);
-            Couplings<T> cp{};
-            if (coded) {
-              cp.e = (b & 1u) ? L.eh : L.el;
-              cp.w = (b & 2u) ? L.eh : L.el;
-              cp.n = (b & 4u) ? L.nh : L.nl;
-              cp.s = (b & 8u) ? L.nh : L.nl;
-              cp.u = (b & 16u) ? L.uh : L.ul;
-              cp.dn = (b & 32u) ? L.uh : L.ul;
-            } else if (in) {
-              cp = array_couplings<T>(oE, oN, uC, p,
-                                      split_nb(sp, p, odd ? 1 : 2, want));
+          // the other-half entry just outside the four: e4 - 1 (odd i, the
+          // previous lane's last) or e4 + 4 (even i, the next lane's first);
+          // read directly where that lane is in another round or idle
+          const T up = __shfl_up_sync(0xffffffffu, vo.w, 1);
+          const T down = __shfl_down_sync(0xffffffffu, vo.x, 1);
+          T edge = odd ? up : down;
+          if (act && odd && lane == 0 && e4 > 0)
+            edge = xo[e4 - 1];
+          if (act && !odd && (lane == 31 || e4 + 4 > ehi))
+            edge = xo[e4 + 4];
+          const T xw[4] = {odd ? edge : vo.x, odd ? vo.x : vo.y,
+                           odd ? vo.y : vo.z, odd ? vo.z : vo.w};
+          const T xe[4] = {odd ? vo.x : vo.y, odd ? vo.y : vo.z,
+                           odd ? vo.z : vo.w, odd ? vo.w : edge};
+          const T an[4] = {vn.x, vn.y, vn.z, vn.w};
+          const T as[4] = {vs.x, vs.y, vs.z, vs.w};
+          const T au[4] = {vu.x, vu.y, vu.z, vu.w};
+          const T ad[4] = {vd.x, vd.y, vd.z, vd.w};
+          const T af[4] = {vf.x, vf.y, vf.z, vf.w};
+          T out[4];
+          if (oc_coded) {
+            // every coefficient from the code byte's table entry (the same
+            // values gs7_code_color_kernel selects); points outside the row's
+            // interior compute from table entries too and are not stored
+  #pragma unroll
+            for (int m = 0; m < 4; ++m) {
+              const T *t = ctab[(cb >> (8 * m)) & 127u];
+              const Quad<T> c0 = *reinterpret_cast<const Quad<T> *>(t);
+              const Quad<T> c1 = *reinterpret_cast<const Quad<T> *>(t + 4);
+              const T sum = c0.x * an[m] + c0.y * as[m] + c0.z * xe[m] +
+                            c0.w * xw[m] + c1.x * ad[m] + c1.y * au[m];
+              out[m] = div_by_table(KEEP ? af[m] + sum : af[m] + T(0) * sum,
+                                    c1.z, rtab,
+                                    (cb >> (8 * m)) & 127u);
             }
-            const T sum = cp.n * an[m] + cp.s * as[m] + cp.e * xe[m] +
-                          cp.w * xw[m] + cp.dn * ad[m] + cp.u * au[m];
-            const T c = in ? oC[p] : T(1);
-            out[m] = (KEEP ? af[m] + sum : af[m] + T(0) * sum) / (c + T(0));
-          }
-        }
-        if (act) {
-          T *dst = x + row + e4;
-          if (e4 >= elo && e4 + 3 <= ehi) {
-            V v;
-            v.x = out[0];
-            v.y = out[1];
-            v.z = out[2];
-            v.w = out[3];
-            *reinterpret_cast<V *>(dst) = v;
           } else {
-#pragma unroll
-            for (int m = 0; m < 4; ++m)
-              if (e4 + m >= elo && e4 + m <= ehi)
-                dst[m] = out[m];
+  #pragma unroll
+            for (int m = 0; m < 4; ++m) {
+              const int e = e4 + m;
+              const bool in = act && e >= elo && e <= ehi;
+              const unsigned b = (cb >> (8 * m)) & 0xffu;
+              const int p = (int)(row + e);
+              Couplings<T> cp{};
+              if (coded) {
+                cp.e = (b & 1u) ? L.eh : L.el;
+                cp.w = (b & 2u) ? L.eh : L.el;
+                cp.n = (b & 4u) ? L.nh : L.nl;
+                cp.s = (b & 8u) ? L.nh : L.nl;
+                cp.u = (b & 16u) ? L.uh : L.ul;
+                cp.dn = (b & 32u) ? L.uh : L.ul;
+              } else if (in) {
+                cp = array_couplings<T>(oE, oN, uC, p,
+                                        split_nb(sp, p, odd ? 1 : 2, want));
+              }
+              const T sum = cp.n * an[m] + cp.s * as[m] + cp.e * xe[m] +
+                            cp.w * xw[m] + cp.dn * ad[m] + cp.u * au[m];
+              const T c = in ? oC[p] : T(1);
+              out[m] = (KEEP ? af[m] + sum : af[m] + T(0) * sum) / (c + T(0));
+            }
+          }
+          if (act) {
+            T *dst = x + row + e4;
+            if (e4 >= elo && e4 + 3 <= ehi) {
+              V v;
+              v.x = out[0];
+              v.y = out[1];
+              v.z = out[2];
+              v.w = out[3];
+              *reinterpret_cast<V *>(dst) = v;
+            } else {
+  #pragma unroll
+              for (int m = 0; m < 4; ++m)
+                if (e4 + m >= elo && e4 + m <= ehi)
+                  dst[m] = out[m];
+            }
           }
         }
+      };
+      const bool row_odd = ((1 + j + k) & 1) == want;
+      if constexpr (sizeof(T) == 4) {
+        if (row_odd)
+          row_pass(std::true_type{});
+        else
+          row_pass(std::false_type{});
+      } else {
+        row_pass(row_odd);
       }
     }
     // plane k - 1 is no longer needed by this warp
