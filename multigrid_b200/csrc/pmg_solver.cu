@@ -270,12 +270,16 @@ void launch_ideal_lambda(const Dims &d, const Op14<T> &A, const T *x,
                          cudaStream_t s) {
   const dim3 g = lambda_grid(d), b = interior_block();
   const int pl = lambda_planes(d);
-  if (pl == 4)
-    ideal_lambda_kernel<T, 4><<<g, b, 0, s>>>(d, A, x, r, red, w);
-  else if (pl == 2)
+  if (pl == 4) {
+    if constexpr (sizeof(T) == sizeof(float))
+      ideal_lambda_r32_kernel<4><<<g, b, 0, s>>>(d, A, x, r, red, w);
+    else
+      ideal_lambda_kernel<T, 4><<<g, b, 0, s>>>(d, A, x, r, red, w);
+  } else if (pl == 2) {
     ideal_lambda_kernel<T, 2><<<g, b, 0, s>>>(d, A, x, r, red, w);
-  else
+  } else {
     ideal_lambda_kernel<T, 1><<<g, b, 0, s>>>(d, A, x, r, red, w);
+  }
 }
 
 // Mixed path: the top level of the one-launch bottom cycle (the levels up
